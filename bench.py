@@ -1,0 +1,297 @@
+"""Closest-hit microbenchmark of the B200 path tracer (one JSON line on rank 0).
+
+Workload: 2,097,152 random triangles (centroids uniform in the unit cube,
+lognormal edge lengths around 0.005, random orientation) and 4,194,304
+incoherent rays (origins uniform in the cube, directions uniform on the
+sphere, tmax = 1e30), all seeded. A step traces every ray once through the
+scene's GPU-built BVH and writes (prim, t, u, v) per ray.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+For N > 1 (torchrun) every rank holds a full scene replica and traces its
+own seeded ray set (weak scaling); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_TRIS = 2097152
+N_RAYS = 4194304
+METRIC = "closest-hit Mrays/s (2M random tris, 4M incoherent rays, bit-exact vs Ref)"
+UNIT = "Mrays/s"
+WORKLOAD = "closest-hit BVH microbench: 2,097,152 random triangles, 4,194,304 incoherent rays"
+
+
+def peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "50"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.1)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def make_workload(rank: int):
+    from raydemo_b200 import scenes
+
+    tris = scenes.random_triangles(N_TRIS, seed=0)
+    rays = scenes.incoherent_rays(N_RAYS, seed=1 + rank)
+    return tris, rays
+
+
+def cpu_reference(tris, rays, sample: int, steps: int, warmup: int):
+    """Times the reference's AVX2 closest-hit traversal (oracle/_ref) on all
+    host threads. Returns (Mrays/s per step list, threads, build seconds)."""
+    from oracle.oracle import RefLib, RefScene
+    from raydemo_b200 import scenes
+
+    ref = RefLib()
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    sc = RefScene(ref, True)
+    attrs, idx = scenes.triangle_soup_mesh(tris)
+    m = sc.add_material(0)
+    sc.add_instance(sc.add_mesh(attrs, idx, [(m, 0xFFFFFFFF, 0, len(idx))]))
+    build_s = time.perf_counter() - t0
+    rng = np.random.default_rng(123)
+    vals = []
+    for s in range(warmup + steps):
+        sub = rays[rng.integers(0, len(rays), sample)]
+        t0 = time.perf_counter()
+        sc.trace_closest(sub, nthreads=threads, backend=1)
+        dt = time.perf_counter() - t0
+        if s >= warmup:
+            vals.append(sample / dt / 1e6)
+    return vals, threads, build_s
+
+
+def run_reference_arm(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    tris, rays = make_workload(0)
+    sample = args.cpu_sample
+    vals, threads, build_s = cpu_reference(tris, rays, sample, max(1, args.steps), max(0, args.warmup))
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(sample / (v * 1e6) * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene and rays)",
+            "config": {"workload": WORKLOAD, "rays_per_step": sample, "tris": N_TRIS, "bvh_build_s": round(build_s, 2)},
+            "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{sample} rays drawn from the 4,194,304-ray set per step; Ref SAH wide BVH; AVX2 8-ray packets"},
+            "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu_arm(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    from raydemo_b200.api import Renderer
+    from raydemo_b200 import scenes
+
+    tris, rays = make_workload(rank)
+    r = Renderer(64, 64, device=local)
+    sc = r.CreateScene()
+    attrs, idx = scenes.triangle_soup_mesh(tris)
+    mat = sc.AddMaterial()
+    sc.AddMeshInstance(sc.AddMesh(attrs, idx, [(mat, 0, len(idx))]))
+    t0 = time.perf_counter()
+    sc.Commit()
+    build_s = time.perf_counter() - t0
+    info = sc.mesh_bvh_info(0)
+
+    rays_d = torch.from_numpy(rays).to(dev)
+    hits_d = torch.empty((N_RAYS, 4), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+
+    def step():
+        sc.trace_closest_device(rays_d.data_ptr(), N_RAYS, hits_d.data_ptr(), 0, sptr)
+
+    # counting pass: node visits and triangle tests of this BVH (algorithmic bytes)
+    sc.set_counting(True)
+    step()
+    cnt = sc.last_trace_info()
+    sc.set_counting(False)
+    if cnt.error_flags:
+        raise RuntimeError(f"trace reported error flags {cnt.error_flags}")
+    node_visits, tri_tests = cnt.node_visits, cnt.tri_tests
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    if sc.last_trace_info().error_flags:
+        raise RuntimeError("trace reported an error during the timed steps")
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_step = ms_max / args.steps
+    value = world * N_RAYS / (ms_step * 1e-3) / 1e6
+
+    # end to end through the C ABI with pinned host buffers (H2D + kernel + D2H)
+    rays_h = torch.from_numpy(rays).pin_memory()
+    hits_h = torch.empty((N_RAYS, 4), dtype=torch.float32).pin_memory()
+    from raydemo_b200 import capi
+
+    def e2e_step():
+        capi.check(capi.lib().ray_scene_trace_closest(sc.handle, rays_h.data_ptr(), N_RAYS, hits_h.data_ptr(), None,
+                                                      capi.RAY_MEM_HOST, sptr))
+
+    for _ in range(2):
+        e2e_step()
+    e_steps = max(3, min(args.steps, 20))
+    if world > 1:
+        dist.barrier()
+    ev0.record(stream)
+    for _ in range(e_steps):
+        e2e_step()
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    te = torch.tensor([ev0.elapsed_time(ev1) / e_steps], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * N_RAYS / (float(te.item()) * 1e-3) / 1e6
+    ok = np.array_equal(hits_h.numpy().view(np.uint32), hits_d.cpu().numpy().view(np.uint32))
+
+    # roofline of the traversal kernel (the only kernel in the timed region)
+    p = peaks()
+    bytes_per_launch = N_RAYS * 44 + node_visits * 80 + tri_tests * 48
+    achieved = bytes_per_launch / (ms / args.steps * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": p["hbm_gbs"], "unit": "GB/s",
+                "frac": round(achieved / p["hbm_gbs"], 4), "traffic": args.traffic_bytes, "peak_source": p["source"],
+                "alg_bytes_per_launch": int(bytes_per_launch), "node_visits_per_ray": round(node_visits / N_RAYS, 3),
+                "tri_tests_per_ray": round(tri_tests / N_RAYS, 3)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            vals, threads, bs = cpu_reference(tris, rays, args.cpu_sample, 3, 1)
+            cpu = {"value": round(statistics.median(vals), 4), "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"{args.cpu_sample} rays x 3 steps from the same 4,194,304-ray set; Ref SAH wide BVH "
+                             f"(build {bs:.1f} s, excluded); AVX2 8-ray packets"}
+        except FileNotFoundError as e:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded procedural scene and rays)",
+                "config": {"workload": WORKLOAD, "rays_per_step_per_gpu": N_RAYS, "tris": N_TRIS,
+                           "l2": "inputs larger than L2 (rays 128 MiB per step, hits 64 MiB)", "bvh_build_s": round(build_s, 3),
+                           "bvh_nodes": info.nodes, "bvh_depth": info.depth, "parallelism": f"replicas x{world}"},
+                "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": N_RAYS * 32, "d2h_bytes_per_step": N_RAYS * 16,
+                        "matches_device_path": bool(ok)},
+                "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    del sc, r
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=262144)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traffic-bytes", type=float, default=None,
+                    help="DRAM bytes per launch of the traversal kernel from an ncu capture (reported as roofline.traffic)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,222 @@
+/*
+ * raygpu -- C ABI of the B200 wavefront path tracer.
+ *
+ * A drop-in for the renderer/scene interface of the Ray library embedded in
+ * SerhiiY-94/RayDemo (src/Ray). Every entry point returns an int status
+ * (RAY_OK or a negative RAY_ERR_* code); ray_last_error() gives a message for
+ * the calling thread. Descriptors are borrowed for the call only: all data is
+ * copied, as the reference does (src/Ray/SceneBase.h).
+ *
+ * Struct layouts: plain C PODs. The 16-byte ray_pixel matches pixel_color_t
+ * (src/Ray/Types.h:14-18); the descriptor structs carry the fields of the
+ * reference descriptors in the same order, with C types (ints for bools and
+ * enums, uint64_t for size_t).
+ */
+#ifndef RAYGPU_H
+#define RAYGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RAY_OK 0
+#define RAY_ERR_INVALID_ARG (-1)
+#define RAY_ERR_CUDA (-2)
+#define RAY_ERR_OUT_OF_MEMORY (-3)
+#define RAY_ERR_NOT_FOUND (-4)
+#define RAY_ERR_STACK_OVERFLOW (-5)
+#define RAY_ERR_TIMEOUT (-6)
+#define RAY_ERR_UNSUPPORTED (-7)
+
+#define RAY_INVALID_INDEX 0xffffffffu
+
+/* Memory space of the buffers handed to the batch entry points. */
+#define RAY_MEM_HOST 0
+#define RAY_MEM_DEVICE 1
+
+typedef struct ray_renderer ray_renderer;
+typedef struct ray_scene ray_scene;
+
+/* Ray::eRendererType (RendererBase.h:15-22); this library reports its own bit. */
+#define RAY_RENDERER_CUDA_SM100 (1 << 6)
+
+/* settings_t (RendererBase.h:25-31); device selects the CUDA device. */
+typedef struct ray_settings {
+    int w, h;
+    int use_wide_bvh; /* accepted for compatibility; the GPU always builds its own wide BVH */
+    int device;
+} ray_settings;
+
+typedef struct ray_rect { int x, y, w, h; } ray_rect;     /* rect_t, Types.h:31 */
+typedef struct ray_pixel { float r, g, b, a; } ray_pixel; /* pixel_color_t, Types.h:14-18 */
+typedef struct ray_shl1 { float coeff_r[4], coeff_g[4], coeff_b[4]; } ray_shl1; /* shl1_data_t, Types.h:25-28 */
+
+/* RegionContext (RendererBase.h:35-51): the caller owns it; ray_render
+ * increments `iteration` and regenerates the sample table itself. */
+typedef struct ray_region {
+    ray_rect rect; /* w == 0 or h == 0: whole image */
+    int iteration;
+} ray_region;
+
+/* stats_t (RendererBase.h:93-100), microseconds, cumulative. */
+typedef struct ray_stats {
+    unsigned long long time_primary_ray_gen_us, time_primary_trace_us, time_primary_shade_us;
+    unsigned long long time_secondary_sort_us, time_secondary_trace_us, time_secondary_shade_us;
+} ray_stats;
+
+/* eMaterialType (SceneBase.h:45-52) */
+enum { RAY_MAT_DIFFUSE = 0, RAY_MAT_GLOSSY, RAY_MAT_REFRACTIVE, RAY_MAT_EMISSIVE, RAY_MAT_MIX, RAY_MAT_TRANSPARENT };
+/* eVertexLayout (SceneBase.h:27-32) */
+enum { RAY_LAYOUT_PNT = 0, RAY_LAYOUT_PNTT, RAY_LAYOUT_PNBT, RAY_LAYOUT_PNBTT };
+/* eLightType (SceneBase.h:108-112) */
+enum { RAY_LIGHT_POINT = 0, RAY_LIGHT_SPOT, RAY_LIGHT_DIRECTIONAL };
+
+/* mat_desc_t (SceneBase.h:55-67) */
+typedef struct ray_mat_desc {
+    int type;
+    float main_color[3];
+    uint32_t main_texture, normal_map, mix_materials[2];
+    float roughness, strength, fresnel, int_ior, ext_ior;
+} ray_mat_desc;
+
+/* shape_desc_t (SceneBase.h:70-81) */
+typedef struct ray_shape_desc {
+    uint32_t mat_index, back_mat_index;
+    uint64_t vtx_start, vtx_count;
+} ray_shape_desc;
+
+/* mesh_desc_t (SceneBase.h:84-95) */
+typedef struct ray_mesh_desc {
+    int prim_type; /* 0: indexed triangle list */
+    int layout;
+    const float *vtx_attrs;
+    uint64_t vtx_attrs_count; /* number of vertices */
+    const uint32_t *vtx_indices;
+    uint64_t vtx_indices_count;
+    int base_vertex;
+    const ray_shape_desc *shapes;
+    uint64_t shapes_count;
+    int allow_spatial_splits, use_fast_bvh_build;
+} ray_mesh_desc;
+
+/* tex_desc_t (SceneBase.h:98-104); data: w*h RGBA8 pixels */
+typedef struct ray_tex_desc {
+    const uint8_t *data;
+    int w, h;
+    int is_srgb, generate_mipmaps;
+} ray_tex_desc;
+
+/* light_desc_t (SceneBase.h:114-119) */
+typedef struct ray_light_desc {
+    int type;
+    float position[3], radius;
+    float color[3];
+    float direction[3], angle;
+} ray_light_desc;
+
+/* camera_desc_t (SceneBase.h:122-145) */
+typedef struct ray_camera_desc {
+    int type, filter, dtype; /* eCamType, eFilterType, eDeviceType (Types.h:33-37) */
+    float origin[3], fwd[3], up[3];
+    float fov, gamma, focus_distance, focus_factor;
+    uint32_t mi_index, uv_index;
+    int lighting_only, skip_direct_lighting, skip_indirect_lighting, no_background, clamp, output_sh, use_coherent_sampling;
+    int max_diff_depth, max_glossy_depth, max_refr_depth, max_transp_depth, max_total_depth, termination_start_depth;
+} ray_camera_desc;
+
+/* environment_desc_t (SceneBase.h:148-152) */
+typedef struct ray_environment_desc {
+    float env_col[3];
+    float env_clamp;
+    uint32_t env_map;
+} ray_environment_desc;
+
+/* One closest hit. prim: global triangle index in scene insertion order
+ * (the reference's tris_ index), -1 on a miss; t, u, v as computed by the
+ * reference's intersection (CoreRef.cpp:11-42). */
+typedef struct ray_hit {
+    int32_t prim;
+    float t, u, v;
+} ray_hit;
+
+const char *ray_last_error(void);
+int ray_version(void);
+
+/* ---- renderer (RendererBase.h:55-103, RendererFactory.h:19) */
+/* Ray::CreateRenderer: the flags argument of the reference picks a CPU or
+ * OpenCL backend; there is one backend here, so it takes none. */
+int ray_create_renderer(const ray_settings *s, ray_renderer **out);
+int ray_destroy_renderer(ray_renderer *r);
+int ray_renderer_type(const ray_renderer *r, int *out_type);           /* RendererBase::type */
+int ray_renderer_size(const ray_renderer *r, int *w, int *h);          /* RendererBase::size */
+int ray_resize(ray_renderer *r, int w, int h);                        /* RendererBase::Resize */
+int ray_clear(ray_renderer *r, const ray_pixel *c);                   /* RendererBase::Clear (NULL: black) */
+int ray_create_scene(ray_renderer *r, ray_scene **out);               /* RendererBase::CreateScene */
+int ray_destroy_scene(ray_scene *s);
+/* RendererBase::RenderScene: one sample per pixel over region->rect. */
+int ray_render(ray_renderer *r, ray_scene *s, ray_region *region);
+/* RendererBase::get_pixels_ref: RGBA f32 row-major w*h; host pointer valid
+ * until the next render/resize/clear (on_device != 0: device pointer). */
+int ray_get_pixels(ray_renderer *r, const ray_pixel **out, int on_device);
+int ray_get_sh_data(ray_renderer *r, const ray_shl1 **out); /* get_sh_data_ref */
+int ray_get_stats(ray_renderer *r, ray_stats *out);          /* GetStats */
+int ray_reset_stats(ray_renderer *r);                        /* ResetStats */
+
+/* ---- scene (SceneBase.h:157-285) */
+int ray_scene_get_environment(ray_scene *s, ray_environment_desc *out);
+int ray_scene_set_environment(ray_scene *s, const ray_environment_desc *env);
+int ray_scene_add_texture(ray_scene *s, const ray_tex_desc *t, uint32_t *out_index);
+int ray_scene_remove_texture(ray_scene *s, uint32_t i);
+int ray_scene_add_material(ray_scene *s, const ray_mat_desc *m, uint32_t *out_index);
+int ray_scene_remove_material(ray_scene *s, uint32_t i);
+int ray_scene_add_mesh(ray_scene *s, const ray_mesh_desc *m, uint32_t *out_index);
+int ray_scene_remove_mesh(ray_scene *s, uint32_t i);
+int ray_scene_add_light(ray_scene *s, const ray_light_desc *l, uint32_t *out_index);
+int ray_scene_remove_light(ray_scene *s, uint32_t i);
+int ray_scene_add_mesh_instance(ray_scene *s, uint32_t mesh_index, const float xform[16], uint32_t *out_index);
+int ray_scene_set_mesh_instance_transform(ray_scene *s, uint32_t mi_index, const float xform[16]);
+int ray_scene_remove_mesh_instance(ray_scene *s, uint32_t mi_index);
+int ray_scene_add_camera(ray_scene *s, const ray_camera_desc *c, uint32_t *out_index);     /* SceneBase::AddCamera */
+int ray_scene_get_camera(ray_scene *s, uint32_t i, ray_camera_desc *out);                 /* SceneBase::GetCamera */
+int ray_scene_set_camera(ray_scene *s, uint32_t i, const ray_camera_desc *c);             /* SceneBase::SetCamera */
+int ray_scene_remove_camera(ray_scene *s, uint32_t i);                                    /* SceneBase::RemoveCamera */
+int ray_scene_current_cam(ray_scene *s, uint32_t *out);
+int ray_scene_set_current_cam(ray_scene *s, uint32_t i);
+int ray_scene_triangle_count(ray_scene *s, uint32_t *out);
+int ray_scene_node_count(ray_scene *s, uint32_t *out);
+/* Uploads pending changes and builds the BVHs on the GPU (done implicitly by
+ * ray_render and the trace entry points). */
+int ray_scene_commit(ray_scene *s);
+
+/* ---- batch closest hit: Traverse_MacroTree_WithStack_ClosestHit over a batch
+ * (CoreRef.cpp:1133-1222). rays: n records of 8 floats
+ * (ox, oy, oz, tmax, dx, dy, dz, unused); hits: n ray_hit; obj (optional, may be
+ * NULL): n mesh-instance indices (-1 on a miss). mem: RAY_MEM_HOST or
+ * RAY_MEM_DEVICE for all three buffers. stream: a cudaStream_t or NULL. */
+int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit *hits, int32_t *obj, int mem, void *stream);
+
+/* Statistics of the last trace call on this scene: error flags OR-ed over rays
+ * (bit 0: a ray's traversal stack overflowed), node and triangle visit totals
+ * (counted only when counting was enabled with ray_scene_set_counting). */
+typedef struct ray_trace_info {
+    uint32_t error_flags;
+    uint64_t node_visits, tri_tests;
+} ray_trace_info;
+int ray_scene_set_counting(ray_scene *s, int enable);
+int ray_scene_last_trace_info(ray_scene *s, ray_trace_info *out);
+
+/* BVH summary of one mesh (for tests and the roofline): node count, leaf
+ * triangle records, maximum wide depth. */
+typedef struct ray_bvh_info {
+    uint32_t nodes, tris, depth, root;
+    float bbox_min[3], bbox_max[3];
+} ray_bvh_info;
+int ray_scene_mesh_bvh_info(ray_scene *s, uint32_t mesh, ray_bvh_info *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

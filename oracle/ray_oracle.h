@@ -1,0 +1,92 @@
+/*
+ * CPU oracle for the wavefront path tracer: a plain-C restatement of the Ray
+ * library's hot-path arithmetic (SerhiiY-94/RayDemo, src/Ray). It is test
+ * infrastructure only: tests, the smoke check and the CPU-baseline leg of the
+ * benchmark may call it as a checker; the product never links or runs it.
+ *
+ * Build with -ffp-contract=off: the reference results depend on products and
+ * sums being rounded separately (no FMA contraction).
+ */
+#ifndef RAY_ORACLE_H
+#define RAY_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same 48-byte layout as tri_accel_t (src/Ray/internal/Core.h:27-36). */
+typedef struct orc_tri {
+    float nu, nv, np, pu, pv;
+    int32_t ci;
+    float e0u, e0v, e1u, e1v;
+    uint32_t mi, back_mi;
+} orc_tri;
+
+/* One closest hit: prim = -1 on a miss (t then holds the input tmax). */
+typedef struct orc_hit {
+    int32_t prim;
+    float t, u, v;
+} orc_hit;
+
+/* Same field order as Ref::ray_packet_t (src/Ray/internal/CoreRef.h:34-45). */
+typedef struct orc_ray_packet {
+    float o[3], d[3], c[3], ior;
+    float do_dx[3], dd_dx[3], do_dy[3], dd_dy[3];
+    int32_t xy;
+    int32_t ray_depth;
+} orc_ray_packet;
+
+typedef struct orc_camera {
+    int filter; /* 0 Box, 1 Tent (Types.h eFilterType) */
+    float fov, gamma, focus_distance, focus_factor;
+    float origin[3], fwd[3], side[3], up[3];
+} orc_camera;
+
+/* PreprocessTri (src/Ray/internal/Core.cpp:162-214) for an indexed mesh.
+ * pos: vertex positions with `stride` floats between vertices. Returns the
+ * number of degenerate triangles (written as the reference's InvalidTriangle). */
+int64_t orc_preprocess_tris(const float *pos, int64_t stride, const uint32_t *idx, int64_t ntris, orc_tri *out);
+
+/* Closest hit over all triangles with _IntersectTri arithmetic
+ * (src/Ray/internal/CoreRef.cpp:11-42). rays: 8 floats per ray
+ * (ox, oy, oz, tmax, dx, dy, dz, unused). Ties on t keep the lowest index. */
+void orc_closest_hit_brute(const orc_tri *tris, int64_t ntris, const float *rays, int64_t nrays, orc_hit *hits, int nthreads);
+
+/* Same result through an oracle-owned binary BVH (conservative boxes, so the
+ * result equals the brute-force one). aabbs: 6 floats per triangle. */
+typedef struct orc_bvh orc_bvh;
+orc_bvh *orc_bvh_build(const float *aabbs, int64_t ntris);
+void orc_bvh_free(orc_bvh *b);
+void orc_closest_hit_bvh(const orc_bvh *b, const orc_tri *tris, const float *rays, int64_t nrays, orc_hit *hits, int nthreads);
+
+/* get_ray_hash (src/Ray/internal/CoreRef.cpp:316-333) for rays given as
+ * 8 floats (o, tmax, d, unused). */
+void orc_ray_hash(const float *rays, int64_t nrays, const float root_min[3], const float cell_size[3], uint32_t *keys);
+/* The permutation SortRays_CPU (CoreRef.cpp:615-657) applies: a stable sort
+ * by 32-bit key. perm[i] = source index of the ray that lands at position i. */
+void orc_sort_perm(const uint32_t *keys, int64_t n, uint32_t *perm);
+
+/* ConstructCamera, perspective case (src/Ray/internal/Core.cpp:856-886). */
+void orc_construct_camera(int filter, const float origin[3], const float fwd[3], const float up[3], float fov, float gamma,
+                          float focus_distance, float focus_factor, orc_camera *cam);
+/* GeneratePrimaryRays (src/Ray/internal/CoreRef.cpp:427-505). */
+void orc_generate_primary_rays(const orc_camera *cam, int iteration, int rx, int ry, int rw, int rh, int w, int h,
+                               const float *halton, orc_ray_packet *out);
+
+/* Halton permutations (src/Ray/internal/Halton.h:7-43 with the generator of
+ * RendererRef.cpp:10-13) and the 24 x 256 sample table
+ * (RendererRef.cpp:327-358). perms: 1,002 entries. */
+void orc_halton_perms(uint16_t *perms);
+void orc_halton_table(int iteration, const uint16_t *perms, float *out);
+
+/* Integer hash and [0,1) float construction used for per-pixel scrambling
+ * (CoreRef.cpp:264-270, 359-368). */
+int32_t orc_hash(int32_t x);
+float orc_construct_float(uint32_t m);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

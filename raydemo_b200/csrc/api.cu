@@ -1,0 +1,798 @@
+// C ABI: scene storage, lazy GPU build, batch closest-hit tracing.
+// Scene semantics follow the reference Ref::Scene (src/Ray/internal/SceneRef.cpp)
+// and SceneBase (src/Ray/SceneBase.cpp); file:line citations per function.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <new>
+
+#include "../../include/raygpu.h"
+#include "scene.hpp"
+#include "trace.cuh"
+
+namespace rg {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+cudaError_t DeviceBuf::ensure(size_t n) {
+    if (n <= bytes && p) return cudaSuccess;
+    release();
+    const size_t want = std::max<size_t>(n, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        bytes = 0;
+        return e;
+    }
+    bytes = want;
+    return cudaSuccess;
+}
+
+void DeviceBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+// InverseMatrix, src/Ray/internal/Core.cpp:909-949 (same operation order).
+static void inverse_matrix(const float m[16], float o[16]) {
+    const float A2323 = m[10] * m[15] - m[11] * m[14];
+    const float A1323 = m[9] * m[15] - m[11] * m[13];
+    const float A1223 = m[9] * m[14] - m[10] * m[13];
+    const float A0323 = m[8] * m[15] - m[11] * m[12];
+    const float A0223 = m[8] * m[14] - m[10] * m[12];
+    const float A0123 = m[8] * m[13] - m[9] * m[12];
+    const float A2313 = m[6] * m[15] - m[7] * m[14];
+    const float A1313 = m[5] * m[15] - m[7] * m[13];
+    const float A1213 = m[5] * m[14] - m[6] * m[13];
+    const float A2312 = m[6] * m[11] - m[7] * m[10];
+    const float A1312 = m[5] * m[11] - m[7] * m[9];
+    const float A1212 = m[5] * m[10] - m[6] * m[9];
+    const float A0313 = m[4] * m[15] - m[7] * m[12];
+    const float A0213 = m[4] * m[14] - m[6] * m[12];
+    const float A0312 = m[4] * m[11] - m[7] * m[8];
+    const float A0212 = m[4] * m[10] - m[6] * m[8];
+    const float A0113 = m[4] * m[13] - m[5] * m[12];
+    const float A0112 = m[4] * m[9] - m[5] * m[8];
+    const float det = m[0] * (m[5] * A2323 - m[6] * A1323 + m[7] * A1223) - m[1] * (m[4] * A2323 - m[6] * A0323 + m[7] * A0223) +
+                      m[2] * (m[4] * A1323 - m[5] * A0323 + m[7] * A0123) - m[3] * (m[4] * A1223 - m[5] * A0223 + m[6] * A0123);
+    const float inv_det = 1.0f / det;
+    o[0] = inv_det * (m[5] * A2323 - m[6] * A1323 + m[7] * A1223);
+    o[1] = inv_det * -(m[1] * A2323 - m[2] * A1323 + m[3] * A1223);
+    o[2] = inv_det * (m[1] * A2313 - m[2] * A1313 + m[3] * A1213);
+    o[3] = inv_det * -(m[1] * A2312 - m[2] * A1312 + m[3] * A1212);
+    o[4] = inv_det * -(m[4] * A2323 - m[6] * A0323 + m[7] * A0223);
+    o[5] = inv_det * (m[0] * A2323 - m[2] * A0323 + m[3] * A0223);
+    o[6] = inv_det * -(m[0] * A2313 - m[2] * A0313 + m[3] * A0213);
+    o[7] = inv_det * (m[0] * A2312 - m[2] * A0312 + m[3] * A0212);
+    o[8] = inv_det * (m[4] * A1323 - m[5] * A0323 + m[7] * A0123);
+    o[9] = inv_det * -(m[0] * A1323 - m[1] * A0323 + m[3] * A0123);
+    o[10] = inv_det * (m[0] * A1313 - m[1] * A0313 + m[3] * A0113);
+    o[11] = inv_det * -(m[0] * A1312 - m[1] * A0312 + m[3] * A0112);
+    o[12] = inv_det * -(m[4] * A1223 - m[5] * A0223 + m[6] * A0123);
+    o[13] = inv_det * (m[0] * A1223 - m[1] * A0223 + m[2] * A0123);
+    o[14] = inv_det * -(m[0] * A1213 - m[1] * A0213 + m[2] * A0113);
+    o[15] = inv_det * (m[0] * A1212 - m[1] * A0212 + m[2] * A0112);
+}
+
+// TransformBoundingBox, src/Ray/internal/Core.cpp:888-907
+static void transform_bbox(const float bmin[3], const float bmax[3], const float *x, float omin[3], float omax[3]) {
+    for (int j = 0; j < 3; j++) omin[j] = omax[j] = x[12 + j];
+    for (int j = 0; j < 3; j++) {
+        for (int i = 0; i < 3; i++) {
+            const float a = x[i * 4 + j] * bmin[i];
+            const float b = x[i * 4 + j] * bmax[i];
+            if (a < b) {
+                omin[j] += a;
+                omax[j] += b;
+            } else {
+                omin[j] += b;
+                omax[j] += a;
+            }
+        }
+    }
+}
+
+static float len3(const float *v) {
+    float t = 0.0f;
+    t += v[0] * v[0];
+    t += v[1] * v[1];
+    t += v[2] * v[2];
+    return std::sqrt(t);
+}
+
+// ConstructCamera, src/Ray/internal/Core.cpp:856-886 (perspective)
+static void construct_camera(CameraRec &c) {
+    const ray_camera_desc &d = c.desc;
+    float u[3] = {d.up[0], d.up[1], d.up[2]};
+    float l2 = 0.0f;
+    l2 += u[0] * u[0];
+    l2 += u[1] * u[1];
+    l2 += u[2] * u[2];
+    if (l2 < FLT_EPS_) {
+        if (std::abs(d.fwd[1]) >= 0.999f) {
+            u[0] = 1.0f; u[1] = 0.0f; u[2] = 0.0f;
+        } else {
+            u[0] = 0.0f; u[1] = 1.0f; u[2] = 0.0f;
+        }
+    }
+    const float *f = d.fwd;
+    float s[3] = {f[1] * u[2] - f[2] * u[1], f[2] * u[0] - f[0] * u[2], f[0] * u[1] - f[1] * u[0]};
+    const float ls = len3(s);
+    for (int k = 0; k < 3; k++) s[k] = s[k] / ls;
+    const float nu[3] = {s[1] * f[2] - s[2] * f[1], s[2] * f[0] - s[0] * f[2], s[0] * f[1] - s[1] * f[0]};
+    for (int k = 0; k < 3; k++) {
+        c.origin[k] = d.origin[k];
+        c.fwd[k] = f[k];
+        c.side[k] = s[k];
+        c.up[k] = nu[k];
+    }
+}
+
+static int upload_texture_host(ray_scene *s, const uint8_t *data, int w, int h, bool srgb, bool mips, uint32_t *out) {
+    if (!data || w <= 0 || h <= 0 || w > 16384 || h > 16384) {
+        set_error("invalid texture description");
+        return RAY_ERR_INVALID_ARG;
+    }
+    TextureRec t;
+    t.w = w;
+    t.h = h;
+    t.srgb = srgb;
+    t.mips = mips;
+    t.rgba.assign(data, data + (size_t)w * h * 4);
+    t.level_offset.push_back(0);
+    t.level_w.push_back((uint32_t)w);
+    t.level_h.push_back((uint32_t)h);
+    s->textures.push_back(std::move(t));
+    *out = (uint32_t)(s->textures.size() - 1);
+    return RAY_OK;
+}
+
+int commit(ray_scene *s) {
+    if (!s->geom_dirty) return RAY_OK;
+    RG_CUDA_TRY(cudaSetDevice(s->device));
+    cudaStream_t st = s->stream;
+    // 1. build the meshes that have no BVH yet
+    for (MeshRec &m : s->meshes) {
+        if (m.built) continue;
+        const uint32_t n = m.tris_count;
+        if (m.tris_ref) {
+            cudaFree(m.tris_ref);
+            m.tris_ref = nullptr;
+        }
+        if (n) {
+            DeviceBuf verts, mat, aabb;
+            RG_CUDA_TRY(verts.ensure(m.verts.size() * sizeof(float)));
+            RG_CUDA_TRY(mat.ensure(m.mat.size() * sizeof(uint32_t)));
+            RG_CUDA_TRY(aabb.ensure((size_t)n * 6 * sizeof(float)));
+            RG_CUDA_TRY(cudaMalloc(&m.tris_ref, (size_t)n * sizeof(TriRec)));
+            RG_CUDA_TRY(cudaMemcpyAsync(verts.p, m.verts.data(), m.verts.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+            RG_CUDA_TRY(cudaMemcpyAsync(mat.p, m.mat.data(), m.mat.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+            RG_CUDA_TRY(launch_preprocess_tris(static_cast<const float *>(verts.p), static_cast<const uint32_t *>(mat.p), n, m.tris_ref,
+                                               static_cast<float *>(aabb.p), st));
+            const int rc = build_mesh_bvh(m.tris_ref, static_cast<const float *>(aabb.p), n, m.bvh, st);
+            if (rc != RAY_OK) return rc;
+            RG_CUDA_TRY(cudaStreamSynchronize(st));
+        }
+        m.built = true;
+    }
+    // 2. assemble the scene arrays
+    uint64_t nodes = 0, tris = 0;
+    for (const MeshRec &m : s->meshes) {
+        nodes += m.bvh.node_count;
+        tris += m.tris_count;
+    }
+    if (nodes > 0xffffffffull || tris > 0x7fffffffull) {
+        set_error("scene too large");
+        return RAY_ERR_INVALID_ARG;
+    }
+    RG_CUDA_TRY(s->d_nodes.ensure(nodes * sizeof(WideNode)));
+    RG_CUDA_TRY(s->d_leaf.ensure(tris * sizeof(TriRec)));
+    RG_CUDA_TRY(s->d_tris_ref.ensure(tris * sizeof(TriRec)));
+    std::vector<uint32_t> node_base(s->meshes.size()), tri_base(s->meshes.size());
+    uint64_t nb = 0, tb = 0;
+    for (size_t i = 0; i < s->meshes.size(); i++) {
+        const MeshRec &m = s->meshes[i];
+        node_base[i] = (uint32_t)nb;
+        tri_base[i] = (uint32_t)tb;
+        if (m.bvh.node_count) {
+            RG_CUDA_TRY(cudaMemcpyAsync(static_cast<WideNode *>(s->d_nodes.p) + nb, m.bvh.nodes, m.bvh.node_count * sizeof(WideNode),
+                                        cudaMemcpyDeviceToDevice, st));
+            RG_CUDA_TRY(cudaMemcpyAsync(static_cast<TriRec *>(s->d_leaf.p) + tb, m.bvh.leaf_tris, m.bvh.tri_count * sizeof(TriRec),
+                                        cudaMemcpyDeviceToDevice, st));
+            RG_CUDA_TRY(cudaMemcpyAsync(static_cast<TriRec *>(s->d_tris_ref.p) + m.tris_index, m.tris_ref, m.tris_count * sizeof(TriRec),
+                                        cudaMemcpyDeviceToDevice, st));
+        }
+        nb += m.bvh.node_count;
+        tb += m.bvh.tri_count;
+    }
+    // 3. instances (SetMeshInstanceTransform, SceneRef.cpp:370-414)
+    std::vector<InstanceRec> inst;
+    for (const InstanceRecHost &ih : s->instances) {
+        const MeshRec &m = s->meshes[ih.mesh];
+        if (m.tris_count == 0) continue;
+        InstanceRec r{};
+        const float *x = ih.inv_xform;
+        const int sel[12] = {0, 1, 2, 4, 5, 6, 8, 9, 10, 12, 13, 14};
+        for (int k = 0; k < 12; k++) r.inv_xform[k] = x[sel[k]];
+        float bmn[3], bmx[3];
+        transform_bbox(m.bvh.bmin, m.bvh.bmax, ih.xform, bmn, bmx);
+        for (int k = 0; k < 3; k++) {
+            r.bbox_min[k] = bmn[k];
+            r.bbox_max[k] = bmx[k];
+        }
+        r.node_base = node_base[ih.mesh];
+        r.tri_base = tri_base[ih.mesh];
+        r.prim_base = m.tris_index;
+        r.mesh = ih.mesh;
+        inst.push_back(r);
+    }
+    // keep the instance index the reference reports (mesh_instances_ position)
+    RG_CUDA_TRY(s->d_inst.ensure(std::max<size_t>(inst.size(), 1) * sizeof(InstanceRec)));
+    if (!inst.empty())
+        RG_CUDA_TRY(cudaMemcpyAsync(s->d_inst.p, inst.data(), inst.size() * sizeof(InstanceRec), cudaMemcpyHostToDevice, st));
+    s->n_inst_dev = (uint32_t)inst.size();
+    RG_CUDA_TRY(cudaStreamSynchronize(st));
+    s->total_nodes = (uint32_t)nodes;
+    s->geom_dirty = false;
+    return RAY_OK;
+}
+
+} // namespace rg
+
+using namespace rg;
+
+#define RG_CHECK(cond, msg)                                                                                            \
+    do {                                                                                                               \
+        if (!(cond)) {                                                                                                 \
+            set_error(msg);                                                                                            \
+            return RAY_ERR_INVALID_ARG;                                                                                \
+        }                                                                                                              \
+    } while (0)
+
+#define RG_GUARD_BEGIN try {
+#define RG_GUARD_END                                                                                                   \
+    }                                                                                                                  \
+    catch (const std::bad_alloc &) {                                                                                   \
+        set_error("host allocation failed");                                                                           \
+        return RAY_ERR_OUT_OF_MEMORY;                                                                                  \
+    }                                                                                                                  \
+    catch (const std::exception &e) {                                                                                  \
+        set_error(e.what());                                                                                           \
+        return RAY_ERR_INVALID_ARG;                                                                                    \
+    }
+
+ray_scene::~ray_scene() {
+    cudaSetDevice(device);
+    for (MeshRec &m : meshes) {
+        free_mesh_bvh(m.bvh);
+        if (m.tris_ref) cudaFree(m.tris_ref);
+    }
+    if (stream) cudaStreamDestroy(stream);
+}
+
+ray_renderer::~ray_renderer() {
+    cudaSetDevice(device);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+extern "C" {
+
+const char *ray_last_error(void) { return g_last_error.c_str(); }
+int ray_version(void) { return 1; }
+
+int ray_create_renderer(const ray_settings *s, ray_renderer **out) {
+    RG_CHECK(s && out, "null argument");
+    RG_CHECK(s->w > 0 && s->h > 0 && s->w <= 32768 && s->h <= 32768, "invalid framebuffer size");
+    RG_GUARD_BEGIN
+    int ndev = 0;
+    RG_CUDA_TRY(cudaGetDeviceCount(&ndev));
+    RG_CHECK(s->device >= 0 && s->device < ndev, "invalid CUDA device index");
+    RG_CUDA_TRY(cudaSetDevice(s->device));
+    auto *r = new ray_renderer;
+    r->device = s->device;
+    r->w = s->w;
+    r->h = s->h;
+    cudaError_t e = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete r;
+        set_error(cudaGetErrorString(e));
+        return RAY_ERR_CUDA;
+    }
+    *out = r;
+    return RAY_OK;
+    RG_GUARD_END
+}
+
+int ray_destroy_renderer(ray_renderer *r) {
+    delete r;
+    return RAY_OK;
+}
+
+int ray_renderer_type(const ray_renderer *r, int *out_type) {
+    RG_CHECK(r && out_type, "null argument");
+    *out_type = RAY_RENDERER_CUDA_SM100;
+    return RAY_OK;
+}
+
+int ray_renderer_size(const ray_renderer *r, int *w, int *h) {
+    RG_CHECK(r && w && h, "null argument");
+    *w = r->w;
+    *h = r->h;
+    return RAY_OK;
+}
+
+int ray_create_scene(ray_renderer *r, ray_scene **out) {
+    RG_CHECK(r && out, "null argument");
+    RG_GUARD_BEGIN
+    RG_CUDA_TRY(cudaSetDevice(r->device));
+    auto *s = new ray_scene;
+    s->device = r->device;
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete s;
+        set_error(cudaGetErrorString(e));
+        return RAY_ERR_CUDA;
+    }
+    // Ref::Scene::Scene (SceneRef.cpp:8-44): a 1-pixel white RGBE environment
+    // map and a 1-pixel flat normal map are textures 0 and 1.
+    static const uint8_t env_px[4] = {255, 255, 255, 128};
+    static const uint8_t nrm_px[4] = {127, 127, 255, 0};
+    upload_texture_host(s, env_px, 1, 1, true, false, &s->default_env_texture);
+    upload_texture_host(s, nrm_px, 1, 1, true, false, &s->default_normals_texture);
+    s->env.env_col[0] = s->env.env_col[1] = s->env.env_col[2] = 0.0f;
+    s->env.env_clamp = 0.0f;
+    s->env.env_map = s->default_env_texture;
+    *out = s;
+    return RAY_OK;
+    RG_GUARD_END
+}
+
+int ray_destroy_scene(ray_scene *s) {
+    delete s;
+    return RAY_OK;
+}
+
+int ray_scene_get_environment(ray_scene *s, ray_environment_desc *out) {
+    RG_CHECK(s && out, "null argument");
+    *out = s->env;
+    return RAY_OK;
+}
+
+int ray_scene_set_environment(ray_scene *s, const ray_environment_desc *env) {
+    RG_CHECK(s && env, "null argument");
+    s->env = *env;
+    if (s->env.env_map == RAY_INVALID_INDEX) s->env.env_map = s->default_env_texture; // SceneRef.cpp:52-59
+    return RAY_OK;
+}
+
+int ray_scene_add_texture(ray_scene *s, const ray_tex_desc *t, uint32_t *out_index) {
+    RG_CHECK(s && t && out_index, "null argument");
+    RG_GUARD_BEGIN
+    return upload_texture_host(s, t->data, t->w, t->h, t->is_srgb != 0, t->generate_mipmaps != 0, out_index);
+    RG_GUARD_END
+}
+
+int ray_scene_remove_texture(ray_scene *s, uint32_t i) {
+    RG_CHECK(s, "null argument");
+    (void)i; // no-op in the reference too (SceneRef.h:84)
+    return RAY_OK;
+}
+
+int ray_scene_add_material(ray_scene *s, const ray_mat_desc *m, uint32_t *out_index) {
+    RG_CHECK(s && m && out_index, "null argument");
+    RG_CHECK(m->type >= RAY_MAT_DIFFUSE && m->type <= RAY_MAT_TRANSPARENT, "invalid material type");
+    RG_GUARD_BEGIN
+    // AddMaterial, SceneRef.cpp:118-150
+    MaterialRec r{};
+    r.type = (uint32_t)m->type;
+    r.textures[1] = m->main_texture;
+    r.textures[2] = r.textures[3] = RAY_INVALID_INDEX;
+    for (int k = 0; k < 3; k++) r.main_color[k] = m->main_color[k];
+    r.int_ior = m->int_ior;
+    r.ext_ior = m->ext_ior;
+    if (m->type == RAY_MAT_DIFFUSE || m->type == RAY_MAT_GLOSSY || m->type == RAY_MAT_REFRACTIVE) {
+        r.roughness_or_strength = m->roughness;
+    } else if (m->type == RAY_MAT_EMISSIVE) {
+        r.roughness_or_strength = m->strength;
+    } else if (m->type == RAY_MAT_MIX) {
+        r.roughness_or_strength = m->strength;
+        r.textures[2] = m->mix_materials[0];
+        r.textures[3] = m->mix_materials[1];
+    }
+    r.textures[0] = (m->normal_map != RAY_INVALID_INDEX) ? m->normal_map : s->default_normals_texture;
+    s->materials.push_back(r);
+    *out_index = (uint32_t)(s->materials.size() - 1);
+    return RAY_OK;
+    RG_GUARD_END
+}
+
+int ray_scene_remove_material(ray_scene *s, uint32_t i) {
+    RG_CHECK(s, "null argument");
+    (void)i; // no-op in the reference too (SceneRef.h:87)
+    return RAY_OK;
+}
+
+int ray_scene_add_mesh(ray_scene *s, const ray_mesh_desc *d, uint32_t *out_index) {
+    RG_CHECK(s && d && out_index, "null argument");
+    RG_CHECK(d->prim_type == 0, "only indexed triangle lists are supported");
+    RG_CHECK(d->layout >= RAY_LAYOUT_PNT && d->layout <= RAY_LAYOUT_PNBTT, "invalid vertex layout");
+    RG_CHECK(d->vtx_indices_count % 3 == 0, "index count must be a multiple of 3");
+    RG_CHECK(d->vtx_indices_count == 0 || (d->vtx_indices && d->vtx_attrs), "null vertex data");
+    RG_GUARD_BEGIN
+    static const size_t strides[4] = {8, 10, 11, 13}; // AttrStrides, SceneBase.h:38-43
+    const size_t stride = strides[d->layout];
+    const uint64_t ntris = d->vtx_indices_count / 3;
+    RG_CHECK((uint64_t)s->total_tris + ntris <= 0x7fffffffull, "too many triangles");
+    for (uint64_t j = 0; j < d->vtx_indices_count; j++) {
+        const int64_t v = (int64_t)d->vtx_indices[j] + d->base_vertex;
+        RG_CHECK(v >= 0 && (uint64_t)v < d->vtx_attrs_count, "vertex index out of range");
+    }
+    // material of every triangle: AddMesh, SceneRef.cpp:184-215
+    std::vector<uint32_t> mat(ntris * 3, 0u);
+    for (uint64_t i = 0; i < ntris; i++) {
+        mat[3 * i + 0] = 0;
+        mat[3 * i + 1] = 0;
+        mat[3 * i + 2] = 0;
+    }
+    for (uint64_t k = 0; k < d->shapes_count; k++) {
+        const ray_shape_desc &sh = d->shapes[k];
+        RG_CHECK(sh.mat_index < s->materials.size(), "shape material out of range");
+        bool solid = true;
+        uint32_t stack[32];
+        uint32_t cnt = 0;
+        stack[cnt++] = sh.mat_index;
+        while (cnt) {
+            const uint32_t mi = stack[--cnt];
+            RG_CHECK(mi < s->materials.size(), "mix material out of range");
+            const MaterialRec &mr = s->materials[mi];
+            if (mr.type == RAY_MAT_MIX) {
+                RG_CHECK(cnt + 2 <= 32, "mix materials nested too deeply");
+                stack[cnt++] = mr.textures[2];
+                stack[cnt++] = mr.textures[3];
+            } else if (mr.type == RAY_MAT_TRANSPARENT) {
+                solid = false;
+                break;
+            }
+        }
+        for (uint64_t i = sh.vtx_start; i < sh.vtx_start + sh.vtx_count && i / 3 < ntris; i += 3) {
+            mat[3 * (i / 3) + 0] = sh.mat_index;
+            mat[3 * (i / 3) + 1] = sh.back_mat_index;
+            mat[3 * (i / 3) + 2] = solid ? 1u : 0u;
+        }
+    }
+    MeshRec m;
+    m.tris_index = s->total_tris;
+    m.tris_count = (uint32_t)ntris;
+    m.verts.resize(ntris * 9);
+    m.mat = std::move(mat);
+    for (uint64_t j = 0; j < d->vtx_indices_count; j++) {
+        const size_t v = (size_t)((int64_t)d->vtx_indices[j] + d->base_vertex);
+        memcpy(&m.verts[3 * j], d->vtx_attrs + v * stride, 3 * sizeof(float));
+    }
+    // shading attributes (SceneRef.cpp:220-260); tangents are filled in by the
+    // shading setup when the layout has none
+    const uint32_t vbase = (uint32_t)s->vertices.size();
+    s->vertices.resize(vbase + d->vtx_attrs_count);
+    for (uint64_t i = 0; i < d->vtx_attrs_count; i++) {
+        VertexRec &v = s->vertices[vbase + i];
+        memset(&v, 0, sizeof(v));
+        const float *a = d->vtx_attrs + i * stride;
+        memcpy(v.p, a, 12);
+        memcpy(v.n, a + 3, 12);
+        if (d->layout == RAY_LAYOUT_PNT) {
+            memcpy(v.t[0], a + 6, 8);
+        } else if (d->layout == RAY_LAYOUT_PNTT) {
+            memcpy(v.t[0], a + 6, 8);
+            memcpy(v.t[1], a + 8, 8);
+        } else if (d->layout == RAY_LAYOUT_PNBT) {
+            memcpy(v.b, a + 6, 12);
+            memcpy(v.t[0], a + 9, 8);
+        } else {
+            memcpy(v.b, a + 6, 12);
+            memcpy(v.t[0], a + 9, 8);
+            memcpy(v.t[1], a + 11, 8);
+        }
+    }
+    for (uint64_t j = 0; j < d->vtx_indices_count; j++) s->vtx_indices.push_back((uint32_t)(d->vtx_indices[j] + d->base_vertex) + vbase);
+    s->meshes.push_back(std::move(m));
+    s->total_tris += (uint32_t)ntris;
+    s->geom_dirty = true;
+    *out_index = (uint32_t)(s->meshes.size() - 1);
+    return RAY_OK;
+    RG_GUARD_END
+}
+
+int ray_scene_remove_mesh(ray_scene *s, uint32_t i) {
+    RG_CHECK(s && i < s->meshes.size(), "invalid mesh index");
+    RG_GUARD_BEGIN
+    // RemoveMesh, SceneRef.cpp:263-303: swap with the last mesh, drop the
+    // instances that then refer to index i (this includes the instances of the
+    // mesh that was moved into slot i, as in the reference), remove the
+    // triangles and shift the triangle ranges of later meshes.
+    const uint32_t last = (uint32_t)s->meshes.size() - 1;
+    const uint32_t tris_index = s->meshes[i].tris_index, tris_count = s->meshes[i].tris_count;
+    free_mesh_bvh(s->meshes[i].bvh);
+    if (s->meshes[i].tris_ref) cudaFree(s->meshes[i].tris_ref);
+    s->meshes[i].tris_ref = nullptr;
+    std::swap(s->meshes[i], s->meshes[last]);
+    s->meshes.pop_back();
+    for (auto it = s->instances.begin(); it != s->instances.end();) {
+        if (it->mesh == last) it->mesh = i;
+        if (it->mesh == i) it = s->instances.erase(it);
+        else ++it;
+    }
+    for (MeshRec &m : s->meshes)
+        if (m.tris_index > tris_index) m.tris_index -= tris_count;
+    // shading arrays keep insertion order: remove the triangle indices of the range
+    s->vtx_indices.erase(s->vtx_indices.begin() + 3ull * tris_index, s->vtx_indices.begin() + 3ull * (tris_index + tris_count));
+    s->total_tris -= tris_count;
+    s->geom_dirty = true;
+    return RAY_OK;
+    RG_GUARD_END
+}
+
+int ray_scene_add_light(ray_scene *s, const ray_light_desc *d, uint32_t *out_index) {
+    RG_CHECK(s && d && out_index, "null argument");
+    RG_CHECK(d->type >= RAY_LIGHT_POINT && d->type <= RAY_LIGHT_DIRECTIONAL, "invalid light type");
+    RG_GUARD_BEGIN
+    // AddLight, SceneRef.cpp:305-349
+    const float PI = 3.141592653589793238463f;
+    LightRec l{};
+    memcpy(l.pos, d->position, 12);
+    l.radius = d->radius;
+    memcpy(l.col, d->color, 12);
+    if (d->type == RAY_LIGHT_SPOT) {
+        for (int k = 0; k < 3; k++) l.dir[k] = -d->direction[k];
+        l.spot = std::cos(d->angle * PI / 180.0f);
+    } else if (d->type == RAY_LIGHT_POINT) {
+        l.dir[0] = l.dir[2] = 0.0f;
+        l.dir[1] = 1.0f;
+        l.spot = -1.0f;
+    } else {
+        const float dist = 9999999.0f;
+        for (int k = 0; k < 3; k++) l.dir[k] = -d->direction[k];
+        for (int k = 0; k < 3; k++) l.pos[k] = l.dir[k] * dist;
+        l.radius = dist * std::tan(d->angle * PI / 180.0f) + 1.0f;
+        float kk = 1.0f + dist / l.radius;
+        kk *= kk;
+        for (int k = 0; k < 3; k++) l.col[k] = d->color[k] * kk;
+        l.spot = 0.0f;
+    }
+    l.brightness = std::max(l.col[0], std::max(l.col[1], l.col[2]));
+    s->lights.push_back(l);
+    *out_index = (uint32_t)(s->lights.size() - 1);
+    return RAY_OK;
+    RG_GUARD_END
+}
+
+int ray_scene_remove_light(ray_scene *s, uint32_t i) {
+    RG_CHECK(s, "null argument");
+    (void)i; // a no-op in the reference (SceneRef.cpp:351-354)
+    return RAY_OK;
+}
+
+int ray_scene_add_mesh_instance(ray_scene *s, uint32_t mesh_index, const float xform[16], uint32_t *out_index) {
+    RG_CHECK(s && xform && out_index, "null argument");
+    RG_CHECK(mesh_index < s->meshes.size(), "invalid mesh index");
+    RG_GUARD_BEGIN
+    InstanceRecHost ih{};
+    ih.mesh = mesh_index;
+    memcpy(ih.xform, xform, 64);
+    inverse_matrix(ih.xform, ih.inv_xform);
+    s->instances.push_back(ih);
+    s->geom_dirty = true;
+    *out_index = (uint32_t)(s->instances.size() - 1);
+    return RAY_OK;
+    RG_GUARD_END
+}
+
+int ray_scene_set_mesh_instance_transform(ray_scene *s, uint32_t mi, const float xform[16]) {
+    RG_CHECK(s && xform && mi < s->instances.size(), "invalid instance");
+    memcpy(s->instances[mi].xform, xform, 64);
+    inverse_matrix(s->instances[mi].xform, s->instances[mi].inv_xform);
+    s->geom_dirty = true;
+    return RAY_OK;
+}
+
+int ray_scene_remove_mesh_instance(ray_scene *s, uint32_t mi) {
+    RG_CHECK(s && mi < s->instances.size(), "invalid instance");
+    s->instances.erase(s->instances.begin() + mi);
+    s->geom_dirty = true;
+    return RAY_OK;
+}
+
+int ray_scene_add_camera(ray_scene *s, const ray_camera_desc *c, uint32_t *out_index) {
+    RG_CHECK(s && c && out_index, "null argument");
+    RG_GUARD_BEGIN
+    // SceneBase::AddCamera, SceneBase.cpp:8-20
+    uint32_t i;
+    if (s->cam_first_free == RAY_INVALID_INDEX) {
+        i = (uint32_t)s->cameras.size();
+        s->cameras.emplace_back();
+    } else {
+        i = s->cam_first_free;
+        s->cam_first_free = s->cameras[i].next_free;
+    }
+    s->cameras[i].desc = *c;
+    s->cameras[i].alive = true;
+    construct_camera(s->cameras[i]);
+    if (s->current_cam == RAY_INVALID_INDEX) s->current_cam = i;
+    *out_index = i;
+    return RAY_OK;
+    RG_GUARD_END
+}
+
+int ray_scene_get_camera(ray_scene *s, uint32_t i, ray_camera_desc *out) {
+    RG_CHECK(s && out && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");
+    *out = s->cameras[i].desc;
+    return RAY_OK;
+}
+
+int ray_scene_set_camera(ray_scene *s, uint32_t i, const ray_camera_desc *c) {
+    RG_CHECK(s && c && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");
+    s->cameras[i].desc = *c;
+    construct_camera(s->cameras[i]);
+    return RAY_OK;
+}
+
+int ray_scene_remove_camera(ray_scene *s, uint32_t i) {
+    RG_CHECK(s && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");
+    s->cameras[i].alive = false;
+    s->cameras[i].next_free = s->cam_first_free;
+    s->cam_first_free = i;
+    return RAY_OK;
+}
+
+int ray_scene_current_cam(ray_scene *s, uint32_t *out) {
+    RG_CHECK(s && out, "null argument");
+    *out = s->current_cam;
+    return RAY_OK;
+}
+
+int ray_scene_set_current_cam(ray_scene *s, uint32_t i) {
+    RG_CHECK(s, "null argument");
+    s->current_cam = i;
+    return RAY_OK;
+}
+
+int ray_scene_triangle_count(ray_scene *s, uint32_t *out) {
+    RG_CHECK(s && out, "null argument");
+    *out = s->total_tris;
+    return RAY_OK;
+}
+
+int ray_scene_node_count(ray_scene *s, uint32_t *out) {
+    RG_CHECK(s && out, "null argument");
+    RG_GUARD_BEGIN
+    const int rc = commit(s);
+    if (rc != RAY_OK) return rc;
+    *out = s->total_nodes;
+    return RAY_OK;
+    RG_GUARD_END
+}
+
+int ray_scene_commit(ray_scene *s) {
+    RG_CHECK(s, "null argument");
+    RG_GUARD_BEGIN
+    return commit(s);
+    RG_GUARD_END
+}
+
+int ray_scene_mesh_bvh_info(ray_scene *s, uint32_t mesh, ray_bvh_info *out) {
+    RG_CHECK(s && out && mesh < s->meshes.size(), "invalid mesh");
+    RG_GUARD_BEGIN
+    const int rc = commit(s);
+    if (rc != RAY_OK) return rc;
+    const MeshRec &m = s->meshes[mesh];
+    out->nodes = m.bvh.node_count;
+    out->tris = m.bvh.tri_count;
+    out->depth = m.bvh.depth;
+    out->root = 0;
+    for (int k = 0; k < 3; k++) {
+        out->bbox_min[k] = m.bvh.bmin[k];
+        out->bbox_max[k] = m.bvh.bmax[k];
+    }
+    return RAY_OK;
+    RG_GUARD_END
+}
+
+int ray_scene_set_counting(ray_scene *s, int enable) {
+    RG_CHECK(s, "null argument");
+    s->counting = enable != 0;
+    return RAY_OK;
+}
+
+int ray_scene_last_trace_info(ray_scene *s, ray_trace_info *out) {
+    RG_CHECK(s && out, "null argument");
+    if (s->info_pending) {
+        RG_CUDA_TRY(cudaSetDevice(s->device));
+        RG_CUDA_TRY(cudaStreamSynchronize(s->info_stream));
+        uint32_t err = 0;
+        unsigned long long cnt[2] = {0, 0};
+        RG_CUDA_TRY(cudaMemcpy(&err, s->d_err.p, 4, cudaMemcpyDeviceToHost));
+        RG_CUDA_TRY(cudaMemcpy(cnt, s->d_counters.p, 16, cudaMemcpyDeviceToHost));
+        s->last_info.error_flags = err;
+        s->last_info.node_visits = cnt[0];
+        s->last_info.tri_tests = cnt[1];
+        s->info_pending = false;
+    }
+    *out = s->last_info;
+    return RAY_OK;
+}
+
+int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit *hits, int32_t *obj, int mem, void *stream) {
+    RG_CHECK(s, "null scene");
+    RG_CHECK(n == 0 || (rays && hits), "null buffer");
+    RG_CHECK(mem == RAY_MEM_HOST || mem == RAY_MEM_DEVICE, "invalid memory space");
+    RG_CHECK(n <= 0xffffffffull, "too many rays in one call");
+    RG_GUARD_BEGIN
+    RG_CUDA_TRY(cudaSetDevice(s->device));
+    int rc = commit(s);
+    if (rc != RAY_OK) return rc;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+    RG_CUDA_TRY(s->d_err.ensure(4));
+    RG_CUDA_TRY(s->d_counters.ensure(16));
+    RG_CUDA_TRY(cudaMemsetAsync(s->d_err.p, 0, 4, st));
+    RG_CUDA_TRY(cudaMemsetAsync(s->d_counters.p, 0, 16, st));
+    const float4 *d_rays = reinterpret_cast<const float4 *>(rays);
+    float4 *d_hits = reinterpret_cast<float4 *>(hits);
+    int32_t *d_obj = obj;
+    if (mem == RAY_MEM_HOST && n) {
+        RG_CUDA_TRY(s->d_rays.ensure(n * 32));
+        RG_CUDA_TRY(s->d_hits.ensure(n * 16));
+        if (obj) RG_CUDA_TRY(s->d_obj.ensure(n * 4));
+        RG_CUDA_TRY(cudaMemcpyAsync(s->d_rays.p, rays, n * 32, cudaMemcpyHostToDevice, st));
+        d_rays = static_cast<const float4 *>(s->d_rays.p);
+        d_hits = static_cast<float4 *>(s->d_hits.p);
+        d_obj = obj ? static_cast<int32_t *>(s->d_obj.p) : nullptr;
+    }
+    SceneView sv{static_cast<const WideNode *>(s->d_nodes.p), static_cast<const TriRec *>(s->d_leaf.p),
+                 static_cast<const InstanceRec *>(s->d_inst.p), s->n_inst_dev};
+    RG_CUDA_TRY(launch_trace_closest(sv, d_rays, (uint32_t)n, d_hits, d_obj, static_cast<uint32_t *>(s->d_err.p),
+                                     static_cast<unsigned long long *>(s->d_counters.p), s->counting, st));
+    s->info_pending = true;
+    s->info_stream = st;
+    if (mem == RAY_MEM_HOST) {
+        if (n) {
+            RG_CUDA_TRY(cudaMemcpyAsync(hits, s->d_hits.p, n * 16, cudaMemcpyDeviceToHost, st));
+            if (obj) RG_CUDA_TRY(cudaMemcpyAsync(obj, s->d_obj.p, n * 4, cudaMemcpyDeviceToHost, st));
+        }
+        ray_trace_info info;
+        rc = ray_scene_last_trace_info(s, &info);
+        if (rc != RAY_OK) return rc;
+        if (info.error_flags & TRACE_ERR_STACK) {
+            set_error("traversal stack overflow");
+            return RAY_ERR_STACK_OVERFLOW;
+        }
+    }
+    return RAY_OK;
+    RG_GUARD_END
+}
+
+// ---- renderer entry points that do not need the render loop
+int ray_resize(ray_renderer *r, int w, int h) {
+    RG_CHECK(r && w > 0 && h > 0 && w <= 32768 && h <= 32768, "invalid size");
+    r->w = w;
+    r->h = h;
+    return RAY_OK;
+}
+
+int ray_get_stats(ray_renderer *r, ray_stats *out) {
+    RG_CHECK(r && out, "null argument");
+    *out = r->stats;
+    return RAY_OK;
+}
+
+int ray_reset_stats(ray_renderer *r) {
+    RG_CHECK(r, "null argument");
+    r->stats = ray_stats{};
+    return RAY_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,86 @@
+// Shared device-side types and helpers of the B200 path tracer.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+namespace rg {
+
+// Precomputed triangle in the layout of tri_accel_t (src/Ray/internal/Core.h:27-36),
+// 48 bytes = three 16-byte loads. In the leaf-ordered copy used by traversal
+// the last two words hold the global triangle index instead of the materials.
+struct alignas(16) TriRec {
+    float nu, nv, np, pu;
+    float pv;
+    int32_t ci;
+    float e0u, e0v;
+    float e1u, e1v;
+    uint32_t mi, back_mi; // leaf copy: mi = global triangle index, back_mi unused
+};
+static_assert(sizeof(TriRec) == 48, "TriRec must stay 48 bytes");
+
+constexpr int TRI_W_BITS = 3;
+constexpr int TRI_AXIS_ALIGNED_BIT = 4;
+constexpr int TRI_INV_NORMAL_BIT = 8;
+constexpr int TRI_SOLID_BIT = 16;
+constexpr float HIT_EPS = 0.000001f;
+constexpr float FLT_EPS_ = 0.0000001f;
+constexpr float MAX_DIST = 3.402823466e+38F;
+
+// Compressed 8-wide node (80 bytes). Child boxes are quantised to 8 bits per
+// plane against a per-node origin p and per-axis power-of-two scale 2^(e-127).
+// The build picks p and e so that every decoded plane p + q * 2^e is an exact
+// float and lies outside the exact child box by at least one quantum, so the
+// slab test on the decoded box never rejects what a test on the exact box
+// accepts.
+//
+// meta[i] (slot i): 0 = empty. Internal child: 0b001 << 5 | (24 + i). Leaf:
+// unary triangle count (0b001, 0b011, 0b111) << 5 | offset of its first
+// triangle from tri_base (0..21). Internal children are stored contiguously
+// from child_base in slot order.
+struct alignas(16) WideNode {
+    float p[3];
+    uint8_t e[3];
+    uint8_t imask;
+    uint32_t child_base;
+    uint32_t tri_base;
+    uint8_t meta[8];
+    uint8_t qlo[3][8];
+    uint8_t qhi[3][8];
+};
+static_assert(sizeof(WideNode) == 80, "WideNode must stay 80 bytes");
+
+// Mesh instance as the traversal sees it (96 bytes).
+struct alignas(16) InstanceRec {
+    // inverse transform, column-major 4x4 without its last row:
+    // [0..2] column 0, [3..5] column 1, [6..8] column 2, [9..11] translation
+    float inv_xform[12];
+    float bbox_min[3];
+    uint32_t node_base; // first wide node of the mesh BVH in the scene node array
+    float bbox_max[3];
+    uint32_t tri_base;  // first leaf triangle of the mesh in the scene leaf array
+    uint32_t prim_base; // global index of the mesh's first triangle
+    uint32_t mesh;
+    uint32_t pad[2];
+};
+static_assert(sizeof(InstanceRec) == 96, "InstanceRec must stay 96 bytes");
+
+constexpr int LEAF_MAX_TRIS = 3;
+
+} // namespace rg
+
+// Error helpers for host code.
+namespace rg {
+void set_error(const std::string &msg);
+}
+
+#define RG_CUDA_TRY(expr)                                                                                              \
+    do {                                                                                                               \
+        cudaError_t _e = (expr);                                                                                       \
+        if (_e != cudaSuccess) {                                                                                       \
+            ::rg::set_error(std::string(#expr " failed: ") + cudaGetErrorString(_e));                                 \
+            return RAY_ERR_CUDA;                                                                                       \
+        }                                                                                                              \
+    } while (0)

@@ -1,0 +1,225 @@
+// Closest-hit traversal (compiled with --fmad=false).
+//
+// One thread per ray. World level: for every mesh instance, the reference's
+// instance box test (bbox_test with safe_invert, CoreRef.cpp:64-86, 272-294)
+// and TransformRay (CoreRef.cpp:1605-1617), both reproduced operation for
+// operation. Mesh level: the compressed 8-wide BVH, traversed with node
+// groups (a base index plus a hit mask of up to 8 children) on a per-thread
+// stack in shared memory; children are visited in octant order, which is
+// roughly front to back. Triangles use the reference's intersection
+// arithmetic (CoreRef.cpp:11-42) with every product and sum rounded on its
+// own, so t, u, v are bit-exact; a tie on t goes to the lower triangle index,
+// which makes the result independent of the visiting order.
+#include "trace.cuh"
+
+namespace rg {
+namespace {
+
+constexpr int TRACE_BLOCK = 128;
+constexpr int STACK_SIZE = 32;
+
+__device__ __forceinline__ float byte_to_float(uint32_t word, uint32_t sel) {
+    // 0x4B0000bb is 2^23 + bb as a float; subtracting 2^23 leaves bb exactly.
+    return __fsub_rn(__uint_as_float(__byte_perm(word, 0x4B000000u, sel)), 8388608.0f);
+}
+
+// The reference's slab test, exactly (bbox_test, CoreRef.cpp:64-86).
+__device__ __forceinline__ bool ref_bbox_test(float ox, float oy, float oz, float ix, float iy, float iz, float t, const float *bmin,
+                                              const float *bmax) {
+    float lo_x = __fmul_rn(ix, __fsub_rn(bmin[0], ox)), hi_x = __fmul_rn(ix, __fsub_rn(bmax[0], ox));
+    if (lo_x > hi_x) { const float tmp = lo_x; lo_x = hi_x; hi_x = tmp; }
+    float lo_y = __fmul_rn(iy, __fsub_rn(bmin[1], oy)), hi_y = __fmul_rn(iy, __fsub_rn(bmax[1], oy));
+    if (lo_y > hi_y) { const float tmp = lo_y; lo_y = hi_y; hi_y = tmp; }
+    float lo_z = __fmul_rn(iz, __fsub_rn(bmin[2], oz)), hi_z = __fmul_rn(iz, __fsub_rn(bmax[2], oz));
+    if (lo_z > hi_z) { const float tmp = lo_z; lo_z = hi_z; hi_z = tmp; }
+    float tmin = lo_x > lo_y ? lo_x : lo_y;
+    if (lo_z > tmin) tmin = lo_z;
+    float tmax = hi_x < hi_y ? hi_x : hi_y;
+    if (hi_z < tmax) tmax = hi_z;
+    tmax = __fmul_rn(tmax, 1.00000024f);
+    return tmin <= tmax && tmin <= t && tmax > 0;
+}
+
+// safe_invert, CoreRef.cpp:272-294
+__device__ __forceinline__ float safe_inv(float v) {
+    float r = __frcp_rn(v);
+    if (v <= FLT_EPS_ && v >= 0) r = 3.402823466e+38F;
+    else if (v >= -FLT_EPS_ && v < 0) r = -3.402823466e+38F;
+    return r;
+}
+
+struct Best {
+    float t, u, v;
+    int prim, obj;
+};
+
+template <bool COUNT>
+__device__ __forceinline__ void trace_mesh(const WideNode *__restrict__ nodes, const TriRec *__restrict__ tris, uint32_t prim_base, int obj,
+                                           float ox, float oy, float oz, float dx, float dy, float dz, Best &best, uint2 *stack,
+                                           uint32_t &err, uint32_t &nvis, uint32_t &ntri) {
+    const float ix = __frcp_rn(dx), iy = __frcp_rn(dy), iz = __frcp_rn(dz); // 1.0f / d, CoreRef.cpp:1215
+    const uint32_t oct = (ix < 0.0f ? 1u : 0u) | (iy < 0.0f ? 2u : 0u) | (iz < 0.0f ? 4u : 0u);
+    // Near/far plane selection by direction sign: a NaN slab value (origin on
+    // a plane of a box the ray runs parallel to) then leaves that axis
+    // unbounded, which keeps the test conservative.
+    const bool nx = ix < 0.0f, ny = iy < 0.0f, nz = iz < 0.0f;
+    uint32_t ng_base = 0, ng_bits = (1u << (24 + oct)) | 1u; // the root as slot 0 of a virtual parent
+    int sp = 0;
+    while (true) {
+        // ---- next child of the current node group
+        const uint32_t j = __ffs(ng_bits >> 24) - 1;
+        ng_bits &= ~(1u << (24 + j));
+        const uint32_t s = j ^ oct;
+        const uint32_t ni = ng_base + __popc((ng_bits & 0xFFu) & ((1u << s) - 1u));
+        if (ng_bits > 0x00FFFFFFu) {
+            if (sp >= STACK_SIZE) {
+                err |= TRACE_ERR_STACK;
+                break;
+            }
+            stack[sp * TRACE_BLOCK] = make_uint2(ng_base, ng_bits);
+            sp++;
+        }
+        const uint4 *np = reinterpret_cast<const uint4 *>(nodes + ni);
+        const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+        if (COUNT) nvis++;
+        const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+        const float sx = __uint_as_float((w0.w & 0xFFu) << 23), sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23),
+                    sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
+        const uint32_t imask = w0.w >> 24;
+        // quantised planes: lo x = w2.xy, lo y = w2.zw, lo z = w3.xy, hi x = w3.zw, hi y = w4.xy, hi z = w4.zw
+        const uint32_t nxa = nx ? w3.z : w2.x, nxb = nx ? w3.w : w2.y, fxa = nx ? w2.x : w3.z, fxb = nx ? w2.y : w3.w;
+        const uint32_t nya = ny ? w4.x : w2.z, nyb = ny ? w4.y : w2.w, fya = ny ? w2.z : w4.x, fyb = ny ? w2.w : w4.y;
+        const uint32_t nza = nz ? w4.z : w3.x, nzb = nz ? w4.w : w3.y, fza = nz ? w3.x : w4.z, fzb = nz ? w3.y : w4.w;
+        uint32_t hitmask = 0;
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            const uint32_t meta = ((c < 4 ? w1.z : w1.w) >> (8 * (c & 3))) & 0xFFu;
+            const uint32_t sel = 0x7540u | (uint32_t)(c & 3);
+            const float tnx = __fmul_rn(__fsub_rn(__fmaf_rn(byte_to_float(c < 4 ? nxa : nxb, sel), sx, px), ox), ix);
+            const float tfx = __fmul_rn(__fsub_rn(__fmaf_rn(byte_to_float(c < 4 ? fxa : fxb, sel), sx, px), ox), ix);
+            const float tny = __fmul_rn(__fsub_rn(__fmaf_rn(byte_to_float(c < 4 ? nya : nyb, sel), sy, py), oy), iy);
+            const float tfy = __fmul_rn(__fsub_rn(__fmaf_rn(byte_to_float(c < 4 ? fya : fyb, sel), sy, py), oy), iy);
+            const float tnz = __fmul_rn(__fsub_rn(__fmaf_rn(byte_to_float(c < 4 ? nza : nzb, sel), sz, pz), oz), iz);
+            const float tfz = __fmul_rn(__fsub_rn(__fmaf_rn(byte_to_float(c < 4 ? fza : fzb, sel), sz, pz), oz), iz);
+            const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
+            const float tmax = __fmul_rn(fminf(fminf(tfx, tfy), tfz), 1.00000024f);
+            if (meta != 0 && tmin <= tmax && tmin <= best.t && tmax > 0.0f) {
+                uint32_t bit = meta & 31u;
+                if (bit >= 24u) bit ^= oct;
+                hitmask |= (meta >> 5) << bit;
+            }
+        }
+        // ---- triangles of this node's leaf children
+        uint32_t tbits = hitmask & 0x00FFFFFFu;
+        const uint32_t tbase = w1.y;
+        while (tbits) {
+            const uint32_t k = __ffs(tbits) - 1;
+            tbits &= tbits - 1;
+            const float4 *tp = reinterpret_cast<const float4 *>(tris + tbase + k);
+            const float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
+            if (COUNT) ntri++;
+            const float nu = t0.x, nv = t0.y, npl = t0.z, pu = t0.w, pv = t1.x, e0u = t1.z, e0v = t1.w, e1u = t2.x, e1v = t2.y;
+            const int iw = __float_as_int(t1.y) & TRI_W_BITS;
+            const float du = iw == 0 ? dy : dx, dv = iw == 2 ? dy : dz, dw = iw == 0 ? dx : (iw == 1 ? dy : dz);
+            const float ou = iw == 0 ? oy : ox, ov = iw == 2 ? oy : oz, ow = iw == 0 ? ox : (iw == 1 ? oy : oz);
+            // _IntersectTri, CoreRef.cpp:18-40
+            const float det = __fadd_rn(__fadd_rn(__fmul_rn(du, nu), __fmul_rn(dv, nv)), dw);
+            const float dett = __fsub_rn(npl, __fadd_rn(__fadd_rn(__fmul_rn(ou, nu), __fmul_rn(ov, nv)), ow));
+            const float Du = __fsub_rn(__fmul_rn(du, dett), __fmul_rn(__fsub_rn(pu, ou), det));
+            const float Dv = __fsub_rn(__fmul_rn(dv, dett), __fmul_rn(__fsub_rn(pv, ov), det));
+            const float detu = __fsub_rn(__fmul_rn(e1v, Du), __fmul_rn(e1u, Dv));
+            const float detv = __fsub_rn(__fmul_rn(e0u, Dv), __fmul_rn(e0v, Du));
+            const float tmpdet0 = __fsub_rn(__fsub_rn(det, detu), detv);
+            if ((tmpdet0 > -HIT_EPS && detu > -HIT_EPS && detv > -HIT_EPS) || (tmpdet0 < HIT_EPS && detu < HIT_EPS && detv < HIT_EPS)) {
+                const float rdet = __frcp_rn(det); // 1.0f / det, correctly rounded
+                const float t = __fmul_rn(dett, rdet);
+                const int gp = (int)(prim_base + __float_as_uint(t2.z));
+                if (t > 0.0f && (t < best.t || (t == best.t && best.prim >= 0 && gp < best.prim))) {
+                    best.t = t;
+                    best.u = __fmul_rn(detu, rdet);
+                    best.v = __fmul_rn(detv, rdet);
+                    best.prim = gp;
+                    best.obj = obj;
+                }
+            }
+        }
+        // ---- next node group
+        ng_base = w1.x;
+        ng_bits = (hitmask & 0xFF000000u) | imask;
+        if (ng_bits <= 0x00FFFFFFu) {
+            if (sp == 0) break;
+            sp--;
+            const uint2 e = stack[sp * TRACE_BLOCK];
+            ng_base = e.x;
+            ng_bits = e.y;
+        }
+    }
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, const float4 *__restrict__ rays, uint32_t n, float4 *__restrict__ hits,
+                                                               int32_t *__restrict__ obj_out, uint32_t *__restrict__ err_out,
+                                                               unsigned long long *__restrict__ counters) {
+    __shared__ uint2 s_stack[STACK_SIZE * TRACE_BLOCK];
+    const uint32_t i = blockIdx.x * TRACE_BLOCK + threadIdx.x;
+    uint32_t err = 0, nvis = 0, ntri = 0;
+    if (i < n) {
+        const float4 r0 = __ldg(rays + 2ull * i), r1 = __ldg(rays + 2ull * i + 1);
+        Best best;
+        best.t = r0.w;
+        best.u = best.v = 0.0f;
+        best.prim = -1;
+        best.obj = -1;
+        const float sx = safe_inv(r1.x), sy = safe_inv(r1.y), sz = safe_inv(r1.z);
+        for (uint32_t m = 0; m < sv.n_inst; m++) {
+            const InstanceRec *ir = sv.inst + m;
+            float bmin[3], bmax[3], x[12];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                bmin[k] = __ldg(&ir->bbox_min[k]);
+                bmax[k] = __ldg(&ir->bbox_max[k]);
+            }
+            if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
+#pragma unroll
+            for (int k = 0; k < 12; k++) x[k] = __ldg(&ir->inv_xform[k]);
+            // TransformRay, CoreRef.cpp:1605-1617
+            const float tox = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(x[0], r0.x), __fmul_rn(x[3], r0.y)), __fmul_rn(x[6], r0.z)), x[9]);
+            const float toy = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(x[1], r0.x), __fmul_rn(x[4], r0.y)), __fmul_rn(x[7], r0.z)), x[10]);
+            const float toz = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(x[2], r0.x), __fmul_rn(x[5], r0.y)), __fmul_rn(x[8], r0.z)), x[11]);
+            const float tdx = __fadd_rn(__fadd_rn(__fmul_rn(x[0], r1.x), __fmul_rn(x[3], r1.y)), __fmul_rn(x[6], r1.z));
+            const float tdy = __fadd_rn(__fadd_rn(__fmul_rn(x[1], r1.x), __fmul_rn(x[4], r1.y)), __fmul_rn(x[7], r1.z));
+            const float tdz = __fadd_rn(__fadd_rn(__fmul_rn(x[2], r1.x), __fmul_rn(x[5], r1.y)), __fmul_rn(x[8], r1.z));
+            trace_mesh<COUNT>(sv.nodes + __ldg(&ir->node_base), sv.leaf_tris + __ldg(&ir->tri_base), __ldg(&ir->prim_base), (int)m, tox, toy,
+                              toz, tdx, tdy, tdz, best, s_stack + threadIdx.x, err, nvis, ntri);
+        }
+        hits[i] = make_float4(__int_as_float(best.prim), best.t, best.prim >= 0 ? best.u : 0.0f, best.prim >= 0 ? best.v : 0.0f);
+        if (obj_out) obj_out[i] = best.obj;
+    }
+    if (err) atomicOr(err_out, err);
+    if (COUNT) {
+        unsigned long long a = nvis, b = ntri;
+        for (int off = 16; off; off >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, off);
+            b += __shfl_xor_sync(0xffffffffu, b, off);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&counters[0], a);
+            atomicAdd(&counters[1], b);
+        }
+    }
+}
+
+} // namespace
+
+cudaError_t launch_trace_closest(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
+                                 unsigned long long *counters, bool count, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    const uint32_t grid = (n + TRACE_BLOCK - 1) / TRACE_BLOCK;
+    if (count)
+        k_trace_closest<true><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters);
+    else
+        k_trace_closest<false><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters);
+    return cudaGetLastError();
+}
+
+} // namespace rg

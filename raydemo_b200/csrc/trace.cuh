@@ -1,0 +1,25 @@
+// Closest-hit traversal entry points (device side of the batch trace and of
+// the render loop).
+#pragma once
+
+#include "common.cuh"
+
+namespace rg {
+
+struct SceneView {
+    const WideNode *nodes;
+    const TriRec *leaf_tris;
+    const InstanceRec *inst;
+    uint32_t n_inst;
+};
+
+// Error bits written (OR-ed) to *err by the traversal.
+constexpr uint32_t TRACE_ERR_STACK = 1u;
+
+// rays: n x 8 floats (ox, oy, oz, tmax, dx, dy, dz, unused).
+// hits: n x {prim, t, u, v}; obj may be null. counters (may be null when
+// count == false): [0] node visits, [1] triangle tests.
+cudaError_t launch_trace_closest(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
+                                 unsigned long long *counters, bool count, cudaStream_t st);
+
+} // namespace rg
