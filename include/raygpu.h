@@ -216,6 +216,12 @@ typedef struct ray_bvh_info {
 } ray_bvh_info;
 int ray_scene_mesh_bvh_info(ray_scene *s, uint32_t mesh, ray_bvh_info *out);
 
+/* Diagnostics: copies one of the scene's device arrays to host memory (after
+ * committing). what: 0 wide nodes (80 bytes each), 1 leaf-ordered triangles
+ * (48 bytes each), 2 instance records (96 bytes each). Copies at most `bytes`
+ * bytes; *out_bytes receives the array size. */
+int ray_scene_debug_read(ray_scene *s, int what, void *dst, uint64_t bytes, uint64_t *out_bytes);
+
 #ifdef __cplusplus
 }
 #endif

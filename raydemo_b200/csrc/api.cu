@@ -230,6 +230,8 @@ int commit(ray_scene *s) {
         r.tri_base = tri_base[ih.mesh];
         r.prim_base = m.tris_index;
         r.mesh = ih.mesh;
+        r.node_count = m.bvh.node_count;
+        r.tri_count = m.bvh.tri_count;
         inst.push_back(r);
     }
     // keep the instance index the reference reports (mesh_instances_ position)
@@ -770,7 +772,37 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
             set_error("traversal stack overflow");
             return RAY_ERR_STACK_OVERFLOW;
         }
+        if (info.error_flags) {
+            set_error("traversal found a corrupt BVH (index or visit bound)");
+            return RAY_ERR_CUDA;
+        }
     }
+    return RAY_OK;
+    RG_GUARD_END
+}
+
+int ray_scene_debug_read(ray_scene *s, int what, void *dst, uint64_t bytes, uint64_t *out_bytes) {
+    RG_CHECK(s && out_bytes, "null argument");
+    RG_CHECK(what >= 0 && what <= 2, "invalid array selector");
+    RG_GUARD_BEGIN
+    RG_CUDA_TRY(cudaSetDevice(s->device));
+    const int rc = commit(s);
+    if (rc != RAY_OK) return rc;
+    uint64_t total = 0;
+    const void *src = nullptr;
+    if (what == 0) {
+        total = (uint64_t)s->total_nodes * sizeof(WideNode);
+        src = s->d_nodes.p;
+    } else if (what == 1) {
+        total = (uint64_t)s->total_tris * sizeof(TriRec);
+        src = s->d_leaf.p;
+    } else {
+        total = (uint64_t)s->n_inst_dev * sizeof(InstanceRec);
+        src = s->d_inst.p;
+    }
+    *out_bytes = total;
+    const uint64_t n = std::min(total, bytes);
+    if (n && dst) RG_CUDA_TRY(cudaMemcpy(dst, src, n, cudaMemcpyDeviceToHost));
     return RAY_OK;
     RG_GUARD_END
 }

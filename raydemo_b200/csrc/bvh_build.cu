@@ -207,7 +207,7 @@ __global__ void k_bottom_up(const float *__restrict__ aabb, const uint32_t *__re
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     uint32_t node = parent[n - 1 + j];
-    while (true) {
+    for (int climb = 0; climb < n; climb++) { // a path to the root has fewer than n nodes
         __threadfence();
         if (atomicAdd(&flags[node], 1u) == 0) return; // the sibling subtree is not done yet
         float a0[3], a1[3], b0[3], b1[3];
@@ -218,7 +218,7 @@ __global__ void k_bottom_up(const float *__restrict__ aabb, const uint32_t *__re
             __stcg(nb + 6ull * node + 3 + k, fmaxf(a1[k], b1[k]));
         }
         if (node == 0) return;
-        node = parent[n - 1 + node];
+        node = parent[node];
     }
 }
 

@@ -61,9 +61,10 @@ struct alignas(16) InstanceRec {
     uint32_t node_base; // first wide node of the mesh BVH in the scene node array
     float bbox_max[3];
     uint32_t tri_base;  // first leaf triangle of the mesh in the scene leaf array
-    uint32_t prim_base; // global index of the mesh's first triangle
+    uint32_t prim_base;  // global index of the mesh's first triangle
     uint32_t mesh;
-    uint32_t pad[2];
+    uint32_t node_count; // bounds for the traversal's index checks
+    uint32_t tri_count;
 };
 static_assert(sizeof(InstanceRec) == 96, "InstanceRec must stay 96 bytes");
 

@@ -54,7 +54,8 @@ struct Best {
 };
 
 template <bool COUNT>
-__device__ __forceinline__ void trace_mesh(const WideNode *__restrict__ nodes, const TriRec *__restrict__ tris, uint32_t prim_base, int obj,
+__device__ __forceinline__ void trace_mesh(const WideNode *__restrict__ nodes, const TriRec *__restrict__ tris, uint32_t prim_base,
+                                           uint32_t node_count, uint32_t tri_count, int obj,
                                            float ox, float oy, float oz, float dx, float dy, float dz, Best &best, uint2 *stack,
                                            uint32_t &err, uint32_t &nvis, uint32_t &ntri) {
     const float ix = __frcp_rn(dx), iy = __frcp_rn(dy), iz = __frcp_rn(dz); // 1.0f / d, CoreRef.cpp:1215
@@ -65,6 +66,7 @@ __device__ __forceinline__ void trace_mesh(const WideNode *__restrict__ nodes, c
     const bool nx = ix < 0.0f, ny = iy < 0.0f, nz = iz < 0.0f;
     uint32_t ng_base = 0, ng_bits = (1u << (24 + oct)) | 1u; // the root as slot 0 of a virtual parent
     int sp = 0;
+    uint32_t visits = 0;
     while (true) {
         // ---- next child of the current node group
         const uint32_t j = __ffs(ng_bits >> 24) - 1;
@@ -78,6 +80,12 @@ __device__ __forceinline__ void trace_mesh(const WideNode *__restrict__ nodes, c
             }
             stack[sp * TRACE_BLOCK] = make_uint2(ng_base, ng_bits);
             sp++;
+        }
+        // A tree visits each node at most once; a bad index or a longer walk
+        // means a corrupt structure: flag it and stop this ray.
+        if (ni >= node_count || ++visits > node_count) {
+            err |= (ni >= node_count) ? TRACE_ERR_BOUNDS : TRACE_ERR_LIMIT;
+            break;
         }
         const uint4 *np = reinterpret_cast<const uint4 *>(nodes + ni);
         const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
@@ -115,6 +123,10 @@ __device__ __forceinline__ void trace_mesh(const WideNode *__restrict__ nodes, c
         while (tbits) {
             const uint32_t k = __ffs(tbits) - 1;
             tbits &= tbits - 1;
+            if (tbase + k >= tri_count) {
+                err |= TRACE_ERR_BOUNDS;
+                continue;
+            }
             const float4 *tp = reinterpret_cast<const float4 *>(tris + tbase + k);
             const float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
             if (COUNT) ntri++;
@@ -189,7 +201,8 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
             const float tdx = __fadd_rn(__fadd_rn(__fmul_rn(x[0], r1.x), __fmul_rn(x[3], r1.y)), __fmul_rn(x[6], r1.z));
             const float tdy = __fadd_rn(__fadd_rn(__fmul_rn(x[1], r1.x), __fmul_rn(x[4], r1.y)), __fmul_rn(x[7], r1.z));
             const float tdz = __fadd_rn(__fadd_rn(__fmul_rn(x[2], r1.x), __fmul_rn(x[5], r1.y)), __fmul_rn(x[8], r1.z));
-            trace_mesh<COUNT>(sv.nodes + __ldg(&ir->node_base), sv.leaf_tris + __ldg(&ir->tri_base), __ldg(&ir->prim_base), (int)m, tox, toy,
+            trace_mesh<COUNT>(sv.nodes + __ldg(&ir->node_base), sv.leaf_tris + __ldg(&ir->tri_base), __ldg(&ir->prim_base),
+                              __ldg(&ir->node_count), __ldg(&ir->tri_count), (int)m, tox, toy,
                               toz, tdx, tdy, tdz, best, s_stack + threadIdx.x, err, nvis, ntri);
         }
         hits[i] = make_float4(__int_as_float(best.prim), best.t, best.prim >= 0 ? best.u : 0.0f, best.prim >= 0 ? best.v : 0.0f);

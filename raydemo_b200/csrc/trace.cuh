@@ -15,6 +15,8 @@ struct SceneView {
 
 // Error bits written (OR-ed) to *err by the traversal.
 constexpr uint32_t TRACE_ERR_STACK = 1u;
+constexpr uint32_t TRACE_ERR_BOUNDS = 2u; // a node or triangle index outside the mesh's arrays
+constexpr uint32_t TRACE_ERR_LIMIT = 4u;  // more node visits than the mesh has nodes
 
 // rays: n x 8 floats (ox, oy, oz, tmax, dx, dy, dz, unused).
 // hits: n x {prim, t, u, v}; obj may be null. counters (may be null when
