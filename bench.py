@@ -174,7 +174,10 @@ def run_gpu_arm(args) -> None:
 
     rays_d = torch.from_numpy(rays).to(dev)
     hits_d = torch.empty((N_RAYS, 4), dtype=torch.float32, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    # an explicit stream: the kernels and the timing events share it (a null
+    # handle would mean the scene's own stream to the C ABI)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
 
     def step():

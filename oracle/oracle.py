@@ -54,11 +54,11 @@ class Oracle:
         vp, i64, i32 = C.c_void_p, C.c_int64, C.c_int
         L.orc_preprocess_tris.argtypes = [vp, i64, vp, i64, vp]
         L.orc_preprocess_tris.restype = i64
-        L.orc_closest_hit_brute.argtypes = [vp, i64, vp, i64, vp, i32]
+        L.orc_closest_hit_brute.argtypes = [vp, i64, vp, i64, vp, i32, vp]
         L.orc_bvh_build.argtypes = [vp, i64]
         L.orc_bvh_build.restype = vp
         L.orc_bvh_free.argtypes = [vp]
-        L.orc_closest_hit_bvh.argtypes = [vp, vp, vp, i64, vp, i32]
+        L.orc_closest_hit_bvh.argtypes = [vp, vp, vp, i64, vp, i32, vp]
         L.orc_ray_hash.argtypes = [vp, i64, vp, vp, vp]
         L.orc_sort_perm.argtypes = [vp, i64, vp]
         L.orc_construct_camera.argtypes = [i32, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.POINTER(OrcCamera)]
@@ -79,19 +79,27 @@ class Oracle:
         self.lib.orc_preprocess_tris(_p(pos), stride, _p(idx), n, _p(out))
         return out
 
-    def closest_hit_brute(self, tris: np.ndarray, rays: np.ndarray, nthreads: int = 8) -> np.ndarray:
+    @staticmethod
+    def _box(world_box):
+        return None if world_box is None else np.ascontiguousarray(world_box, np.float32).reshape(6)
+
+    def closest_hit_brute(self, tris: np.ndarray, rays: np.ndarray, nthreads: int = 8, world_box=None) -> np.ndarray:
+        """world_box: the single instance's box (min xyz, max xyz), tested as
+        the reference's macro traversal does; None skips that test."""
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
         hits = np.zeros(len(rays), HIT_DTYPE)
-        self.lib.orc_closest_hit_brute(_p(tris), len(tris), _p(rays), len(rays), _p(hits), nthreads)
+        box = self._box(world_box)
+        self.lib.orc_closest_hit_brute(_p(tris), len(tris), _p(rays), len(rays), _p(hits), nthreads, _p(box))
         return hits
 
-    def closest_hit_bvh(self, tris: np.ndarray, aabbs: np.ndarray, rays: np.ndarray, nthreads: int = 8) -> np.ndarray:
+    def closest_hit_bvh(self, tris: np.ndarray, aabbs: np.ndarray, rays: np.ndarray, nthreads: int = 8, world_box=None) -> np.ndarray:
         aabbs = np.ascontiguousarray(aabbs, np.float32).reshape(-1, 6)
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
         hits = np.zeros(len(rays), HIT_DTYPE)
+        box = self._box(world_box)
         b = self.lib.orc_bvh_build(_p(aabbs), len(aabbs))
         try:
-            self.lib.orc_closest_hit_bvh(b, _p(tris), _p(rays), len(rays), _p(hits), nthreads)
+            self.lib.orc_closest_hit_bvh(b, _p(tris), _p(rays), len(rays), _p(hits), nthreads, _p(box))
         finally:
             self.lib.orc_bvh_free(b)
         return hits

@@ -129,6 +129,33 @@ static inline void intersect_tri(const float *o, const float *d, const orc_tri *
     }
 }
 
+/* safe_invert, src/Ray/internal/CoreRef.cpp:272-294 */
+static float safe_inv(float v) {
+    float r = 1.0f / v;
+    if (v <= ORC_FLT_EPS && v >= 0) r = 3.402823466e+38F;
+    else if (v >= -ORC_FLT_EPS && v < 0) r = -3.402823466e+38F;
+    return r;
+}
+
+/* bbox_test, src/Ray/internal/CoreRef.cpp:64-86: the instance-box test of the
+ * reference's macro traversal (Traverse_MacroTree_WithStack_ClosestHit,
+ * CoreRef.cpp:1133-1222), done with safe_invert'ed directions. */
+static int ref_bbox_test(const float *o, const float *d, float t, const float *box) {
+    const float inv_d[3] = {safe_inv(d[0]), safe_inv(d[1]), safe_inv(d[2])};
+    float lo[3], hi[3];
+    for (int k = 0; k < 3; k++) {
+        lo[k] = inv_d[k] * (box[k] - o[k]);
+        hi[k] = inv_d[k] * (box[3 + k] - o[k]);
+        if (lo[k] > hi[k]) { const float tmp = lo[k]; lo[k] = hi[k]; hi[k] = tmp; }
+    }
+    float tmin = lo[0] > lo[1] ? lo[0] : lo[1];
+    if (lo[2] > tmin) tmin = lo[2];
+    float tmax = hi[0] < hi[1] ? hi[0] : hi[1];
+    if (hi[2] < tmax) tmax = hi[2];
+    tmax *= 1.00000024f;
+    return tmin <= tmax && tmin <= t && tmax > 0;
+}
+
 typedef struct {
     const orc_tri *tris;
     int64_t ntris;
@@ -136,6 +163,7 @@ typedef struct {
     orc_hit *hits;
     int64_t begin, end;
     const orc_bvh *bvh;
+    const float *world_box;
 } work_t;
 
 static void *brute_worker(void *arg) {
@@ -143,7 +171,8 @@ static void *brute_worker(void *arg) {
     for (int64_t r = w->begin; r < w->end; r++) {
         const float *ray = w->rays + 8 * r;
         orc_hit h = {-1, ray[3], 0.0f, 0.0f};
-        for (int64_t i = 0; i < w->ntris; i++) intersect_tri(ray, ray + 4, &w->tris[i], (int32_t)i, &h);
+        if (!w->world_box || ref_bbox_test(ray, ray + 4, ray[3], w->world_box))
+            for (int64_t i = 0; i < w->ntris; i++) intersect_tri(ray, ray + 4, &w->tris[i], (int32_t)i, &h);
         w->hits[r] = h;
     }
     return NULL;
@@ -167,8 +196,9 @@ static void run_parallel(void *(*fn)(void *), work_t proto, int64_t n, int nthre
     for (int t = 0; t < started; t++) pthread_join(th[t], NULL);
 }
 
-void orc_closest_hit_brute(const orc_tri *tris, int64_t ntris, const float *rays, int64_t nrays, orc_hit *hits, int nthreads) {
-    work_t proto = {tris, ntris, rays, hits, 0, 0, NULL};
+void orc_closest_hit_brute(const orc_tri *tris, int64_t ntris, const float *rays, int64_t nrays, orc_hit *hits, int nthreads,
+                           const float *world_box) {
+    work_t proto = {tris, ntris, rays, hits, 0, 0, NULL, world_box};
     run_parallel(brute_worker, proto, nrays, nthreads);
 }
 
@@ -296,7 +326,7 @@ static void *bvh_worker(void *arg) {
         const float inv_d[3] = {1.0f / d[0], 1.0f / d[1], 1.0f / d[2]};
         orc_hit h = {-1, ray[3], 0.0f, 0.0f};
         int sp = 0;
-        if (b->nnodes > 0 && b->nodes[0].right != 0) stack[sp++] = 0;
+        if (b->nnodes > 0 && b->nodes[0].right != 0 && (!w->world_box || ref_bbox_test(o, d, ray[3], w->world_box))) stack[sp++] = 0;
         while (sp) {
             const onode *nd = &b->nodes[stack[--sp]];
             if (!box_hit(nd, o, inv_d, h.t)) continue;
@@ -315,8 +345,9 @@ static void *bvh_worker(void *arg) {
     return NULL;
 }
 
-void orc_closest_hit_bvh(const orc_bvh *b, const orc_tri *tris, const float *rays, int64_t nrays, orc_hit *hits, int nthreads) {
-    work_t proto = {tris, 0, rays, hits, 0, 0, b};
+void orc_closest_hit_bvh(const orc_bvh *b, const orc_tri *tris, const float *rays, int64_t nrays, orc_hit *hits, int nthreads,
+                         const float *world_box) {
+    work_t proto = {tris, 0, rays, hits, 0, 0, b, world_box};
     run_parallel(bvh_worker, proto, nrays, nthreads);
 }
 

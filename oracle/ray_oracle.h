@@ -51,15 +51,20 @@ int64_t orc_preprocess_tris(const float *pos, int64_t stride, const uint32_t *id
 
 /* Closest hit over all triangles with _IntersectTri arithmetic
  * (src/Ray/internal/CoreRef.cpp:11-42). rays: 8 floats per ray
- * (ox, oy, oz, tmax, dx, dy, dz, unused). Ties on t keep the lowest index. */
-void orc_closest_hit_brute(const orc_tri *tris, int64_t ntris, const float *rays, int64_t nrays, orc_hit *hits, int nthreads);
+ * (ox, oy, oz, tmax, dx, dy, dz, unused). Ties on t keep the lowest index.
+ * world_box (6 floats, min then max; may be NULL): the box of the single mesh
+ * instance, tested first as the reference's macro traversal does
+ * (bbox_test with safe_invert, CoreRef.cpp:64-86, 272-294, 1133-1222). */
+void orc_closest_hit_brute(const orc_tri *tris, int64_t ntris, const float *rays, int64_t nrays, orc_hit *hits, int nthreads,
+                           const float *world_box);
 
 /* Same result through an oracle-owned binary BVH (conservative boxes, so the
  * result equals the brute-force one). aabbs: 6 floats per triangle. */
 typedef struct orc_bvh orc_bvh;
 orc_bvh *orc_bvh_build(const float *aabbs, int64_t ntris);
 void orc_bvh_free(orc_bvh *b);
-void orc_closest_hit_bvh(const orc_bvh *b, const orc_tri *tris, const float *rays, int64_t nrays, orc_hit *hits, int nthreads);
+void orc_closest_hit_bvh(const orc_bvh *b, const orc_tri *tris, const float *rays, int64_t nrays, orc_hit *hits, int nthreads,
+                         const float *world_box);
 
 /* get_ray_hash (src/Ray/internal/CoreRef.cpp:316-333) for rays given as
  * 8 floats (o, tmax, d, unused). */

@@ -21,7 +21,28 @@ def _scene(tris, renderer, xform=None, instances=1):
 
 
 def _same(a, b):
-    return np.array_equal(a.view(np.uint32).reshape(len(a), -1), b.view(np.uint32).reshape(len(b), -1))
+    if len(a) != len(b):
+        return False
+    return len(a) == 0 or np.array_equal(a.view(np.uint32).reshape(len(a), -1), b.view(np.uint32).reshape(len(b), -1))
+
+
+def _oracle_hits(oracle, tris, rays, brute=None):
+    """Oracle closest hits for one identity instance of `tris`, including the
+    reference's instance-box test on the mesh box."""
+    attrs, idx = scenes.triangle_soup_mesh(tris)
+    acc = oracle.preprocess_tris(attrs[:, :3].copy(), idx)
+    box = np.concatenate([tris.reshape(-1, 3).min(axis=0), tris.reshape(-1, 3).max(axis=0)])
+    if brute is None:
+        brute = len(tris) <= 5000
+    if brute:
+        return oracle.closest_hit_brute(acc, rays, world_box=box)
+    return oracle.closest_hit_bvh(acc, scenes.tri_aabbs(tris), rays, world_box=box)
+
+
+def _assert_hits_equal(hits, exp):
+    assert np.array_equal(hits["prim"], exp["prim"])
+    hit = exp["prim"] >= 0
+    assert _same(hits[hit], exp[hit])
 
 
 @pytest.fixture(scope="module")
@@ -42,15 +63,14 @@ def test_golden_hits(renderer, ref_outputs):
 def test_random_scenes_vs_oracle(renderer, oracle, n_tris, n_rays, seed):
     tris = scenes.random_triangles(n_tris, seed=seed, mean_edge=0.05 if n_tris < 1000 else 0.005)
     rays = scenes.incoherent_rays(n_rays, seed=seed + 100)
-    sc = _scene(tris, renderer)
-    hits = sc.trace_closest(rays)
-    attrs, idx = scenes.triangle_soup_mesh(tris)
-    acc = oracle.preprocess_tris(attrs[:, :3].copy(), idx)
-    exp = oracle.closest_hit_bvh(acc, scenes.tri_aabbs(tris), rays) if n_tris > 5000 else oracle.closest_hit_brute(acc, rays)
-    assert (exp["prim"] >= 0).any() or n_tris < 10
-    miss = exp["prim"] < 0
-    assert np.array_equal(hits["prim"], exp["prim"])
-    assert _same(hits[~miss], exp[~miss])
+    if n_tris < 10:  # aim a share of the rays at the triangles
+        tgt = tris.mean(axis=1)[np.arange(n_rays) % n_tris]
+        d = tgt - rays[:, 0:3]
+        rays[::2, 4:7] = (d / np.linalg.norm(d, axis=1, keepdims=True))[::2]
+    hits = _scene(tris, renderer).trace_closest(rays)
+    exp = _oracle_hits(oracle, tris, rays)
+    assert (exp["prim"] >= 0).any()
+    _assert_hits_equal(hits, exp)
 
 
 def test_live_reference(renderer, reflib):
@@ -64,29 +84,23 @@ def test_live_reference(renderer, reflib):
     sc.add_instance(sc.add_mesh(attrs, idx, [(m, 0xFFFFFFFF, 0, len(idx))]))
     ref_hits, ref_obj = sc.trace_closest(rays)
     hits, obj = _scene(tris, renderer).trace_closest(rays, with_obj=True)
-    assert np.array_equal(hits["prim"], ref_hits["prim"])
+    _assert_hits_equal(hits, ref_hits)
     assert np.array_equal(obj, ref_obj)
-    hit = hits["prim"] >= 0
-    assert _same(hits[hit], ref_hits[hit])
 
 
 def test_tmax_and_coherent(renderer, oracle):
     tris = scenes.random_triangles(50000, seed=41)
     rays = scenes.coherent_rays(128, 128)
     rays[::3, 3] = 1.7  # short rays
-    sc = _scene(tris, renderer)
-    hits = sc.trace_closest(rays)
-    attrs, idx = scenes.triangle_soup_mesh(tris)
-    acc = oracle.preprocess_tris(attrs[:, :3].copy(), idx)
-    exp = oracle.closest_hit_bvh(acc, scenes.tri_aabbs(tris), rays)
-    assert np.array_equal(hits["prim"], exp["prim"])
-    assert _same(hits[exp["prim"] >= 0], exp[exp["prim"] >= 0])
+    hits = _scene(tris, renderer).trace_closest(rays)
+    exp = _oracle_hits(oracle, tris, rays)
+    _assert_hits_equal(hits, exp)
     assert np.all(hits["t"][::3][hits["prim"][::3] >= 0] < 1.7)
 
 
-def test_axis_aligned_geometry_and_rays(renderer, oracle):
-    # a grid of axis-aligned quads hit by axis-aligned rays (zero direction
-    # components, origins on box planes)
+def _axis_aligned_case():
+    # a stack of axis-aligned quads hit by axis-aligned rays: zero direction
+    # components, and origins on box planes (x or y exactly 0 or 1)
     quads = []
     for k in range(8):
         z = 0.1 * k
@@ -99,11 +113,35 @@ def test_axis_aligned_geometry_and_rays(renderer, oracle):
     rays[:n, 0], rays[:n, 1], rays[:n, 2], rays[:n, 6] = X.ravel(), Y.ravel(), -1.0, 1.0
     rays[n:, 0], rays[n:, 1], rays[n:, 2], rays[n:, 6] = X.ravel(), Y.ravel(), 0.35, -1.0
     rays[:, 3] = 1e30
+    return tris, rays
+
+
+def test_axis_aligned_geometry_and_rays(renderer, oracle):
+    tris, rays = _axis_aligned_case()
     hits = _scene(tris, renderer).trace_closest(rays)
+    _assert_hits_equal(hits, _oracle_hits(oracle, tris, rays))
+    # rays on the x = 1 or y = 1 face of the instance box are rejected by the
+    # reference's instance test (its tmax is 0 there); the others hit
+    edge = (rays[:, 0] == 1.0) | (rays[:, 1] == 1.0)
+    assert np.all(hits["prim"][~edge] >= 0)
+
+
+def test_axis_aligned_vs_reference(renderer, reflib):
+    from oracle.oracle import RefScene
+
+    tris, rays = _axis_aligned_case()
     attrs, idx = scenes.triangle_soup_mesh(tris)
-    exp = oracle.closest_hit_brute(oracle.preprocess_tris(attrs[:, :3].copy(), idx), rays)
-    assert np.array_equal(hits["prim"], exp["prim"])
-    assert _same(hits[exp["prim"] >= 0], exp[exp["prim"] >= 0])
+    sc = RefScene(reflib, True)
+    m = sc.add_material(0)
+    sc.add_instance(sc.add_mesh(attrs, idx, [(m, 0xFFFFFFFF, 0, len(idx))]))
+    ref_hits, _ = sc.trace_closest(rays)
+    # Ref keeps the first of two exactly equal t (traversal order); here every
+    # hit is a tie between the two triangles of a quad only on its diagonal,
+    # so compare t/u/v of the hit and the hit mask
+    hits = _scene(tris, renderer).trace_closest(rays)
+    assert np.array_equal(hits["prim"] >= 0, ref_hits["prim"] >= 0)
+    hit = hits["prim"] >= 0
+    assert np.array_equal(hits["t"][hit], ref_hits["t"][hit])
 
 
 def test_instances_with_transforms(renderer, reflib):
@@ -134,10 +172,8 @@ def test_instances_with_transforms(renderer, reflib):
     rays[:, 0:3] = rays[:, 0:3] * 3 - 1.5
     ref_hits, ref_obj = rsc.trace_closest(rays)
     hits, obj = gsc.trace_closest(rays, with_obj=True)
-    assert np.array_equal(hits["prim"], ref_hits["prim"])
+    _assert_hits_equal(hits, ref_hits)
     assert np.array_equal(obj, ref_obj)
-    hit = hits["prim"] >= 0
-    assert _same(hits[hit], ref_hits[hit])
 
 
 def test_empty_and_degenerate(renderer, oracle):
@@ -148,11 +184,26 @@ def test_empty_and_degenerate(renderer, oracle):
     tris[::7, 1] = tris[::7, 0]  # zero-area triangles never hit (InvalidTriangle)
     rays = scenes.incoherent_rays(3000, seed=62)
     hits = _scene(tris, renderer).trace_closest(rays)
-    attrs, idx = scenes.triangle_soup_mesh(tris)
-    exp = oracle.closest_hit_brute(oracle.preprocess_tris(attrs[:, :3].copy(), idx), rays)
-    assert np.array_equal(hits["prim"], exp["prim"])
+    _assert_hits_equal(hits, _oracle_hits(oracle, tris, rays))
     assert not np.any(np.isin(hits["prim"], np.arange(0, 500, 7)))
     assert len(sc.trace_closest(np.zeros((0, 8), np.float32))) == 0
+
+
+def test_device_path_matches_host_path(renderer):
+    import torch
+
+    tris = scenes.random_triangles(30000, seed=71, mean_edge=0.01)
+    rays = scenes.incoherent_rays(50000, seed=72)
+    sc = _scene(tris, renderer)
+    host = sc.trace_closest(rays)
+    rd = torch.from_numpy(rays).cuda()
+    hd = torch.empty((len(rays), 4), dtype=torch.float32, device="cuda")
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        sc.trace_closest_device(rd.data_ptr(), len(rays), hd.data_ptr(), 0, s.cuda_stream)
+    s.synchronize()
+    assert sc.last_trace_info().error_flags == 0
+    assert np.array_equal(hd.cpu().numpy().view(np.uint32), host.view(np.float32).reshape(-1, 4).view(np.uint32))
 
 
 def test_full_size_microbench_subset(renderer, oracle):
@@ -163,16 +214,12 @@ def test_full_size_microbench_subset(renderer, oracle):
     rays = scenes.incoherent_rays(4194304, seed=1)
     sc = _scene(tris, renderer)
     hits = sc.trace_closest(rays)
-    info = sc.last_trace_info()
-    assert info.error_flags == 0
+    assert sc.last_trace_info().error_flags == 0
     hit = hits["prim"] >= 0
     assert 0.85 < hit.mean() < 0.99
     assert np.all(hits["t"][hit] > 0) and np.all(hits["prim"][hit] < len(tris))
     sub = np.random.default_rng(7).choice(len(rays), 65536, replace=False)
-    attrs, idx = scenes.triangle_soup_mesh(tris)
-    acc = oracle.preprocess_tris(attrs[:, :3].copy(), idx)
-    exp = oracle.closest_hit_bvh(acc, scenes.tri_aabbs(tris), rays[sub])
-    assert np.array_equal(hits["prim"][sub], exp["prim"])
-    assert _same(hits[sub][exp["prim"] >= 0], exp[exp["prim"] >= 0])
-    # tracing twice gives the same bytes
+    exp = _oracle_hits(oracle, tris, rays[sub], brute=False)
+    _assert_hits_equal(hits[sub], exp)
+    # tracing again gives the same bytes
     assert _same(sc.trace_closest(rays[:100000]), hits[:100000])
