@@ -90,10 +90,26 @@ __device__ __forceinline__ void trace_mesh(const WideNode *__restrict__ nodes, c
         const uint4 *np = reinterpret_cast<const uint4 *>(nodes + ni);
         const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
         if (COUNT) nvis++;
-        const float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
-        const float sx = __uint_as_float((w0.w & 0xFFu) << 23), sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23),
-                    sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
         const uint32_t imask = w0.w >> 24;
+        // Slab parameter of plane q on one axis: t(q) = q * A + B with
+        // A = 2^e * inv_d (exact: a power-of-two scaling) and B = (p - o) * inv_d,
+        // one FMA per plane. Its rounding error is below 2u(|B| + 256|A|)
+        // (u = 2^-24); the slack 2^-21 (|B| + 256|A|) moves the near planes
+        // down and the far planes up by more than that, so the test accepts
+        // every box that the exact slab test on the decoded box accepts.
+        float A[3], Bn[3], Bf[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const float p = __uint_as_float(a == 0 ? w0.x : (a == 1 ? w0.y : w0.z));
+            const float sc = __uint_as_float(((w0.w >> (8 * a)) & 0xFFu) << 23);
+            const float inv = a == 0 ? ix : (a == 1 ? iy : iz);
+            const float o = a == 0 ? ox : (a == 1 ? oy : oz);
+            A[a] = __fmul_rn(sc, inv);
+            const float B = __fmul_rn(__fsub_rn(p, o), inv);
+            const float slack = __fmul_rn(__fmaf_rn(fabsf(A[a]), 256.0f, fabsf(B)), 4.76837158203125e-07f);
+            Bn[a] = __fsub_rn(B, slack);
+            Bf[a] = __fadd_rn(B, slack);
+        }
         // quantised planes: lo x = w2.xy, lo y = w2.zw, lo z = w3.xy, hi x = w3.zw, hi y = w4.xy, hi z = w4.zw
         const uint32_t nxa = nx ? w3.z : w2.x, nxb = nx ? w3.w : w2.y, fxa = nx ? w2.x : w3.z, fxb = nx ? w2.y : w3.w;
         const uint32_t nya = ny ? w4.x : w2.z, nyb = ny ? w4.y : w2.w, fya = ny ? w2.z : w4.x, fyb = ny ? w2.w : w4.y;
@@ -103,15 +119,15 @@ __device__ __forceinline__ void trace_mesh(const WideNode *__restrict__ nodes, c
         for (int c = 0; c < 8; c++) {
             const uint32_t meta = ((c < 4 ? w1.z : w1.w) >> (8 * (c & 3))) & 0xFFu;
             const uint32_t sel = 0x7540u | (uint32_t)(c & 3);
-            const float tnx = __fmul_rn(__fsub_rn(__fmaf_rn(byte_to_float(c < 4 ? nxa : nxb, sel), sx, px), ox), ix);
-            const float tfx = __fmul_rn(__fsub_rn(__fmaf_rn(byte_to_float(c < 4 ? fxa : fxb, sel), sx, px), ox), ix);
-            const float tny = __fmul_rn(__fsub_rn(__fmaf_rn(byte_to_float(c < 4 ? nya : nyb, sel), sy, py), oy), iy);
-            const float tfy = __fmul_rn(__fsub_rn(__fmaf_rn(byte_to_float(c < 4 ? fya : fyb, sel), sy, py), oy), iy);
-            const float tnz = __fmul_rn(__fsub_rn(__fmaf_rn(byte_to_float(c < 4 ? nza : nzb, sel), sz, pz), oz), iz);
-            const float tfz = __fmul_rn(__fsub_rn(__fmaf_rn(byte_to_float(c < 4 ? fza : fzb, sel), sz, pz), oz), iz);
+            const float tnx = __fmaf_rn(byte_to_float(c < 4 ? nxa : nxb, sel), A[0], Bn[0]);
+            const float tfx = __fmaf_rn(byte_to_float(c < 4 ? fxa : fxb, sel), A[0], Bf[0]);
+            const float tny = __fmaf_rn(byte_to_float(c < 4 ? nya : nyb, sel), A[1], Bn[1]);
+            const float tfy = __fmaf_rn(byte_to_float(c < 4 ? fya : fyb, sel), A[1], Bf[1]);
+            const float tnz = __fmaf_rn(byte_to_float(c < 4 ? nza : nzb, sel), A[2], Bn[2]);
+            const float tfz = __fmaf_rn(byte_to_float(c < 4 ? fza : fzb, sel), A[2], Bf[2]);
             const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
-            const float tmax = __fmul_rn(fminf(fminf(tfx, tfy), tfz), 1.00000024f);
-            if (meta != 0 && tmin <= tmax && tmin <= best.t && tmax > 0.0f) {
+            const float tmax = fminf(fminf(tfx, tfy), tfz);
+            if (meta != 0 && tmin <= tmax && tmin <= best.t && tmax >= 0.0f) {
                 uint32_t bit = meta & 31u;
                 if (bit >= 24u) bit ^= oct;
                 hitmask |= (meta >> 5) << bit;

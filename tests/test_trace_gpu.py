@@ -135,13 +135,19 @@ def test_axis_aligned_vs_reference(renderer, reflib):
     m = sc.add_material(0)
     sc.add_instance(sc.add_mesh(attrs, idx, [(m, 0xFFFFFFFF, 0, len(idx))]))
     ref_hits, _ = sc.trace_closest(rays)
-    # Ref keeps the first of two exactly equal t (traversal order); here every
-    # hit is a tie between the two triangles of a quad only on its diagonal,
-    # so compare t/u/v of the hit and the hit mask
     hits = _scene(tris, renderer).trace_closest(rays)
-    assert np.array_equal(hits["prim"] >= 0, ref_hits["prim"] >= 0)
-    hit = hits["prim"] >= 0
-    assert np.array_equal(hits["t"][hit], ref_hits["t"][hit])
+    # Where the reference hits, the GPU returns the same t (the prim may be
+    # the other triangle of a quad on its diagonal, an exact tie that Ref
+    # resolves by traversal order).
+    both = (ref_hits["prim"] >= 0)
+    assert np.all(hits["prim"][both] >= 0)
+    assert np.array_equal(hits["t"][both].view(np.uint32), ref_hits["t"][both].view(np.uint32))
+    # Where they differ, the reference misses a ray that runs inside the y = 0
+    # face of its leaf boxes (d.y = 0 makes its slab test 0 * inf = NaN, which
+    # culls): a box false negative of the reference, not a GPU miss.
+    diff = (hits["prim"] >= 0) != (ref_hits["prim"] >= 0)
+    assert np.all(ref_hits["prim"][diff] < 0)
+    assert np.all((rays[diff, 1] == 0.0) & (rays[diff, 5] == 0.0))
 
 
 def test_instances_with_transforms(renderer, reflib):
