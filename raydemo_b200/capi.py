@@ -91,6 +91,10 @@ class TraceInfo(C.Structure):
     _fields_ = [("error_flags", C.c_uint32), ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64)]
 
 
+class TraceTuning(C.Structure):
+    _fields_ = [("kernel", C.c_int), ("refill_min", C.c_int), ("postpone_min", C.c_int)]
+
+
 class BvhInfo(C.Structure):
     _fields_ = [("nodes", C.c_uint32), ("tris", C.c_uint32), ("depth", C.c_uint32), ("root", C.c_uint32), ("bbox_min", f3),
                 ("bbox_max", f3)]
@@ -150,6 +154,8 @@ _SIGS = {
     "ray_scene_last_trace_info": ([_P, C.POINTER(TraceInfo)], C.c_int),
     "ray_scene_mesh_bvh_info": ([_P, C.c_uint32, C.POINTER(BvhInfo)], C.c_int),
     "ray_scene_debug_read": ([_P, C.c_int, _P, C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
+    "ray_scene_set_trace_tuning": ([_P, C.POINTER(TraceTuning)], C.c_int),
+    "ray_scene_get_trace_tuning": ([_P, C.POINTER(TraceTuning)], C.c_int),
 }
 
 

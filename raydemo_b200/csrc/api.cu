@@ -704,6 +704,22 @@ int ray_scene_mesh_bvh_info(ray_scene *s, uint32_t mesh, ray_bvh_info *out) {
     RG_GUARD_END
 }
 
+int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t) {
+    RG_CHECK(s && t, "null argument");
+    RG_CHECK(t->kernel >= 0 && t->kernel <= 2, "kernel must be 1 (per ray) or 2 (persistent)");
+    RG_CHECK(t->refill_min <= 32 && t->postpone_min <= 32, "lane counts are at most 32");
+    if (t->kernel > 0) s->tuning.kernel = t->kernel;
+    if (t->refill_min >= 0) s->tuning.refill_min = t->refill_min < 1 ? 1 : t->refill_min;
+    if (t->postpone_min >= 0) s->tuning.postpone_min = t->postpone_min;
+    return RAY_OK;
+}
+
+int ray_scene_get_trace_tuning(ray_scene *s, ray_trace_tuning *out) {
+    RG_CHECK(s && out, "null argument");
+    *out = s->tuning;
+    return RAY_OK;
+}
+
 int ray_scene_set_counting(ray_scene *s, int enable) {
     RG_CHECK(s, "null argument");
     s->counting = enable != 0;
@@ -756,8 +772,14 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
     }
     SceneView sv{static_cast<const WideNode *>(s->d_nodes.p), static_cast<const TriRec *>(s->d_leaf.p),
                  static_cast<const InstanceRec *>(s->d_inst.p), s->n_inst_dev};
+    RG_CUDA_TRY(s->d_next_ray.ensure(4));
+    TraceParams tp;
+    tp.persistent = s->tuning.kernel == 2;
+    tp.refill_min = s->tuning.refill_min;
+    tp.postpone_min = s->tuning.postpone_min;
+    tp.next_ray = static_cast<uint32_t *>(s->d_next_ray.p);
     RG_CUDA_TRY(launch_trace_closest(sv, d_rays, (uint32_t)n, d_hits, d_obj, static_cast<uint32_t *>(s->d_err.p),
-                                     static_cast<unsigned long long *>(s->d_counters.p), s->counting, st));
+                                     static_cast<unsigned long long *>(s->d_counters.p), s->counting, st, tp));
     s->info_pending = true;
     s->info_stream = st;
     if (mem == RAY_MEM_HOST) {

@@ -104,7 +104,8 @@ struct ray_scene {
     uint32_t n_inst_dev = 0;
 
     // batch-trace staging and diagnostics
-    rg::DeviceBuf d_rays, d_hits, d_obj, d_err, d_counters;
+    rg::DeviceBuf d_rays, d_hits, d_obj, d_err, d_counters, d_next_ray;
+    ray_trace_tuning tuning{2, 8, 8};
     bool counting = false;
     ray_trace_info last_info{};
     bool info_pending = false;

@@ -1,22 +1,33 @@
 // Closest-hit traversal (compiled with --fmad=false).
 //
-// One thread per ray. World level: for every mesh instance, the reference's
-// instance box test (bbox_test with safe_invert, CoreRef.cpp:64-86, 272-294)
-// and TransformRay (CoreRef.cpp:1605-1617), both reproduced operation for
-// operation. Mesh level: the compressed 8-wide BVH, traversed with node
-// groups (a base index plus a hit mask of up to 8 children) on a per-thread
-// stack in shared memory; children are visited in octant order, which is
-// roughly front to back. Triangles use the reference's intersection
-// arithmetic (CoreRef.cpp:11-42) with every product and sum rounded on its
-// own, so t, u, v are bit-exact; a tie on t goes to the lower triangle index,
-// which makes the result independent of the visiting order.
+// World level: for every mesh instance, the reference's instance box test
+// (bbox_test with safe_invert, CoreRef.cpp:64-86, 272-294) and TransformRay
+// (CoreRef.cpp:1605-1617), both reproduced operation for operation. Mesh
+// level: the compressed 8-wide BVH, traversed with node groups (a base index
+// plus a hit mask of up to 8 children) and triangle groups (a base index plus
+// a mask of up to 24 triangles) on a per-thread stack; children are visited
+// in octant order, which is roughly front to back. Triangles use the
+// reference's intersection arithmetic (CoreRef.cpp:11-42) with every product
+// and sum rounded on its own, so t, u, v are bit-exact; a tie on t goes to the
+// lower triangle index, which makes the result independent of visiting order.
+//
+// Two kernels share the traversal step:
+//   k_trace_closest     one thread per ray (a grid over the rays)
+//   k_trace_persistent  a resident grid; a lane whose ray is done takes the
+//                       next one from a global counter (warp-aggregated), and
+//                       a warp postpones triangle groups while few of its
+//                       lanes have any, so more lanes do useful work per
+//                       instruction on incoherent rays.
 #include "trace.cuh"
 
 namespace rg {
 namespace {
 
 constexpr int TRACE_BLOCK = 128;
-constexpr int STACK_SIZE = 32;
+constexpr int SMEM_STACK = 24;  // entries per thread in shared memory
+constexpr int LMEM_STACK = 40;  // further entries in local memory (rarely used)
+constexpr int STACK_SIZE = SMEM_STACK + LMEM_STACK;
+constexpr uint32_t NO_RAY = 0xffffffffu;
 
 __device__ __forceinline__ float byte_to_float(uint32_t word, uint32_t sel) {
     // 0x4B0000bb is 2^23 + bb as a float; subtracting 2^23 leaves bb exactly.
@@ -53,131 +64,212 @@ struct Best {
     int prim, obj;
 };
 
+// Ray in the space of the instance being traversed.
+struct LocalRay {
+    float ox, oy, oz, dx, dy, dz, ix, iy, iz;
+    uint32_t oct; // bit a set: direction negative on axis a
+};
+
+struct MeshRef {
+    const WideNode *nodes;
+    const TriRec *tris;
+    uint32_t prim_base, node_count, tri_count;
+    int obj;
+};
+
+// Two-tier per-thread stack: the first SMEM_STACK entries in shared memory
+// (strided by the block size), the rest in a local array.
+struct Stack {
+    uint2 *smem;
+    uint2 lmem[LMEM_STACK];
+    int sp;
+    __device__ __forceinline__ bool push(uint2 e) {
+        if (sp >= STACK_SIZE) return false;
+        if (sp < SMEM_STACK) smem[sp * TRACE_BLOCK] = e;
+        else lmem[sp - SMEM_STACK] = e;
+        sp++;
+        return true;
+    }
+    __device__ __forceinline__ uint2 pop() {
+        sp--;
+        return sp < SMEM_STACK ? smem[sp * TRACE_BLOCK] : lmem[sp - SMEM_STACK];
+    }
+};
+
+__device__ __forceinline__ LocalRay make_local_ray(float ox, float oy, float oz, float dx, float dy, float dz) {
+    LocalRay r;
+    r.ox = ox; r.oy = oy; r.oz = oz;
+    r.dx = dx; r.dy = dy; r.dz = dz;
+    r.ix = __frcp_rn(dx); // 1.0f / d, CoreRef.cpp:1215
+    r.iy = __frcp_rn(dy);
+    r.iz = __frcp_rn(dz);
+    r.oct = (r.ix < 0.0f ? 1u : 0u) | (r.iy < 0.0f ? 2u : 0u) | (r.iz < 0.0f ? 4u : 0u);
+    return r;
+}
+
+// TransformRay, CoreRef.cpp:1605-1617, with the instance's inverse transform.
+__device__ __forceinline__ LocalRay transform_ray(const InstanceRec *ir, float4 r0, float4 r1) {
+    float x[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) x[k] = __ldg(&ir->inv_xform[k]);
+    const float tox = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(x[0], r0.x), __fmul_rn(x[3], r0.y)), __fmul_rn(x[6], r0.z)), x[9]);
+    const float toy = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(x[1], r0.x), __fmul_rn(x[4], r0.y)), __fmul_rn(x[7], r0.z)), x[10]);
+    const float toz = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(x[2], r0.x), __fmul_rn(x[5], r0.y)), __fmul_rn(x[8], r0.z)), x[11]);
+    const float tdx = __fadd_rn(__fadd_rn(__fmul_rn(x[0], r1.x), __fmul_rn(x[3], r1.y)), __fmul_rn(x[6], r1.z));
+    const float tdy = __fadd_rn(__fadd_rn(__fmul_rn(x[1], r1.x), __fmul_rn(x[4], r1.y)), __fmul_rn(x[7], r1.z));
+    const float tdz = __fadd_rn(__fadd_rn(__fmul_rn(x[2], r1.x), __fmul_rn(x[5], r1.y)), __fmul_rn(x[8], r1.z));
+    return make_local_ray(tox, toy, toz, tdx, tdy, tdz);
+}
+
+__device__ __forceinline__ MeshRef mesh_of(const SceneView &sv, const InstanceRec *ir, int m) {
+    MeshRef mr;
+    mr.nodes = sv.nodes + __ldg(&ir->node_base);
+    mr.tris = sv.leaf_tris + __ldg(&ir->tri_base);
+    mr.prim_base = __ldg(&ir->prim_base);
+    mr.node_count = __ldg(&ir->node_count);
+    mr.tri_count = __ldg(&ir->tri_count);
+    mr.obj = m;
+    return mr;
+}
+
+// Node step: takes the next child of node group (ng_base, ng_bits), tests
+// its 8 children and returns their hits as a node group (internal children,
+// bits 24..31, with the node's imask in bits 0..7) and a triangle group
+// (bits 0..23). Returns false (and sets err) on a corrupt index.
 template <bool COUNT>
-__device__ __forceinline__ void trace_mesh(const WideNode *__restrict__ nodes, const TriRec *__restrict__ tris, uint32_t prim_base,
-                                           uint32_t node_count, uint32_t tri_count, int obj,
-                                           float ox, float oy, float oz, float dx, float dy, float dz, Best &best, uint2 *stack,
-                                           uint32_t &err, uint32_t &nvis, uint32_t &ntri) {
-    const float ix = __frcp_rn(dx), iy = __frcp_rn(dy), iz = __frcp_rn(dz); // 1.0f / d, CoreRef.cpp:1215
-    const uint32_t oct = (ix < 0.0f ? 1u : 0u) | (iy < 0.0f ? 2u : 0u) | (iz < 0.0f ? 4u : 0u);
-    // Near/far plane selection by direction sign: a NaN slab value (origin on
-    // a plane of a box the ray runs parallel to) then leaves that axis
-    // unbounded, which keeps the test conservative.
-    const bool nx = ix < 0.0f, ny = iy < 0.0f, nz = iz < 0.0f;
-    uint32_t ng_base = 0, ng_bits = (1u << (24 + oct)) | 1u; // the root as slot 0 of a virtual parent
-    int sp = 0;
-    uint32_t visits = 0;
+__device__ __forceinline__ bool node_step(const MeshRef &mr, const LocalRay &r, float best_t, uint32_t &ng_base, uint32_t &ng_bits,
+                                          uint32_t &tg_base, uint32_t &tg_bits, Stack &st, uint32_t &visits, uint32_t &err,
+                                          uint32_t &nvis) {
+    const uint32_t j = __ffs(ng_bits >> 24) - 1;
+    ng_bits &= ~(1u << (24 + j));
+    const uint32_t s = j ^ r.oct;
+    const uint32_t ni = ng_base + __popc((ng_bits & 0xFFu) & ((1u << s) - 1u));
+    if (ng_bits > 0x00FFFFFFu && !st.push(make_uint2(ng_base, ng_bits))) {
+        err |= TRACE_ERR_STACK;
+        return false;
+    }
+    // A tree visits each node at most once; a bad index or a longer walk
+    // means a corrupt structure: flag it and stop this ray.
+    if (ni >= mr.node_count || ++visits > mr.node_count) {
+        err |= (ni >= mr.node_count) ? TRACE_ERR_BOUNDS : TRACE_ERR_LIMIT;
+        return false;
+    }
+    const uint4 *np = reinterpret_cast<const uint4 *>(mr.nodes + ni);
+    const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+    if (COUNT) nvis++;
+    const uint32_t imask = w0.w >> 24;
+    // Slab parameter of plane q on one axis: t(q) = q * A + B with
+    // A = 2^e * inv_d (exact: a power-of-two scaling) and B = (p - o) * inv_d,
+    // one FMA per plane. Its rounding error is below 2u(|B| + 256|A|)
+    // (u = 2^-24); the slack 2^-21 (|B| + 256|A|) moves the near planes
+    // down and the far planes up by more than that, so the test accepts
+    // every box that the exact slab test on the decoded box accepts.
+    float A[3], Bn[3], Bf[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float p = __uint_as_float(a == 0 ? w0.x : (a == 1 ? w0.y : w0.z));
+        const float sc = __uint_as_float(((w0.w >> (8 * a)) & 0xFFu) << 23);
+        const float inv = a == 0 ? r.ix : (a == 1 ? r.iy : r.iz);
+        const float o = a == 0 ? r.ox : (a == 1 ? r.oy : r.oz);
+        A[a] = __fmul_rn(sc, inv);
+        const float B = __fmul_rn(__fsub_rn(p, o), inv);
+        const float slack = __fmul_rn(__fmaf_rn(fabsf(A[a]), 256.0f, fabsf(B)), 4.76837158203125e-07f);
+        Bn[a] = __fsub_rn(B, slack);
+        Bf[a] = __fadd_rn(B, slack);
+    }
+    // Near/far plane words by direction sign, so that a NaN slab value
+    // (origin on a plane of a box the ray runs parallel to) leaves that axis
+    // unbounded, which keeps the test conservative. Planes: lo x = w2.xy,
+    // lo y = w2.zw, lo z = w3.xy, hi x = w3.zw, hi y = w4.xy, hi z = w4.zw.
+    const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
+    const uint32_t nxa = nx ? w3.z : w2.x, nxb = nx ? w3.w : w2.y, fxa = nx ? w2.x : w3.z, fxb = nx ? w2.y : w3.w;
+    const uint32_t nya = ny ? w4.x : w2.z, nyb = ny ? w4.y : w2.w, fya = ny ? w2.z : w4.x, fyb = ny ? w2.w : w4.y;
+    const uint32_t nza = nz ? w4.z : w3.x, nzb = nz ? w4.w : w3.y, fza = nz ? w3.x : w4.z, fzb = nz ? w3.y : w4.w;
+    uint32_t hitmask = 0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        const uint32_t meta = ((c < 4 ? w1.z : w1.w) >> (8 * (c & 3))) & 0xFFu;
+        const uint32_t sel = 0x7540u | (uint32_t)(c & 3);
+        const float tnx = __fmaf_rn(byte_to_float(c < 4 ? nxa : nxb, sel), A[0], Bn[0]);
+        const float tfx = __fmaf_rn(byte_to_float(c < 4 ? fxa : fxb, sel), A[0], Bf[0]);
+        const float tny = __fmaf_rn(byte_to_float(c < 4 ? nya : nyb, sel), A[1], Bn[1]);
+        const float tfy = __fmaf_rn(byte_to_float(c < 4 ? fya : fyb, sel), A[1], Bf[1]);
+        const float tnz = __fmaf_rn(byte_to_float(c < 4 ? nza : nzb, sel), A[2], Bn[2]);
+        const float tfz = __fmaf_rn(byte_to_float(c < 4 ? fza : fzb, sel), A[2], Bf[2]);
+        const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
+        const float tmax = fminf(fminf(tfx, tfy), tfz);
+        if (meta != 0 && tmin <= tmax && tmin <= best_t && tmax >= 0.0f) {
+            uint32_t bit = meta & 31u;
+            if (bit >= 24u) bit ^= r.oct;
+            hitmask |= (meta >> 5) << bit;
+        }
+    }
+    ng_base = w1.x;
+    ng_bits = (hitmask & 0xFF000000u) | imask;
+    tg_base = w1.y;
+    tg_bits = hitmask & 0x00FFFFFFu;
+    return true;
+}
+
+// One triangle test; updates best when it is the closer hit.
+template <bool COUNT>
+__device__ __forceinline__ void tri_test(const MeshRef &mr, const LocalRay &r, uint32_t li, Best &best, uint32_t &err, uint32_t &ntri) {
+    if (li >= mr.tri_count) {
+        err |= TRACE_ERR_BOUNDS;
+        return;
+    }
+    const float4 *tp = reinterpret_cast<const float4 *>(mr.tris + li);
+    const float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
+    if (COUNT) ntri++;
+    const float nu = t0.x, nv = t0.y, npl = t0.z, pu = t0.w, pv = t1.x, e0u = t1.z, e0v = t1.w, e1u = t2.x, e1v = t2.y;
+    const int iw = __float_as_int(t1.y) & TRI_W_BITS;
+    const float du = iw == 0 ? r.dy : r.dx, dv = iw == 2 ? r.dy : r.dz, dw = iw == 0 ? r.dx : (iw == 1 ? r.dy : r.dz);
+    const float ou = iw == 0 ? r.oy : r.ox, ov = iw == 2 ? r.oy : r.oz, ow = iw == 0 ? r.ox : (iw == 1 ? r.oy : r.oz);
+    // _IntersectTri, CoreRef.cpp:18-40
+    const float det = __fadd_rn(__fadd_rn(__fmul_rn(du, nu), __fmul_rn(dv, nv)), dw);
+    const float dett = __fsub_rn(npl, __fadd_rn(__fadd_rn(__fmul_rn(ou, nu), __fmul_rn(ov, nv)), ow));
+    const float Du = __fsub_rn(__fmul_rn(du, dett), __fmul_rn(__fsub_rn(pu, ou), det));
+    const float Dv = __fsub_rn(__fmul_rn(dv, dett), __fmul_rn(__fsub_rn(pv, ov), det));
+    const float detu = __fsub_rn(__fmul_rn(e1v, Du), __fmul_rn(e1u, Dv));
+    const float detv = __fsub_rn(__fmul_rn(e0u, Dv), __fmul_rn(e0v, Du));
+    const float tmpdet0 = __fsub_rn(__fsub_rn(det, detu), detv);
+    if ((tmpdet0 > -HIT_EPS && detu > -HIT_EPS && detv > -HIT_EPS) || (tmpdet0 < HIT_EPS && detu < HIT_EPS && detv < HIT_EPS)) {
+        const float rdet = __frcp_rn(det); // 1.0f / det, correctly rounded
+        const float t = __fmul_rn(dett, rdet);
+        const int gp = (int)(mr.prim_base + __float_as_uint(t2.z));
+        if (t > 0.0f && (t < best.t || (t == best.t && best.prim >= 0 && gp < best.prim))) {
+            best.t = t;
+            best.u = __fmul_rn(detu, rdet);
+            best.v = __fmul_rn(detv, rdet);
+            best.prim = gp;
+            best.obj = mr.obj;
+        }
+    }
+}
+
+// Whole traversal of one mesh for one ray (the one-thread-per-ray kernel).
+template <bool COUNT>
+__device__ __forceinline__ void trace_mesh(const MeshRef &mr, const LocalRay &r, Best &best, Stack &st, uint32_t &err, uint32_t &nvis,
+                                           uint32_t &ntri) {
+    uint32_t ng_base = 0, ng_bits = (1u << (24 + r.oct)) | 1u; // the root as slot 0 of a virtual parent
+    uint32_t tg_base = 0, tg_bits = 0, visits = 0;
+    st.sp = 0;
     while (true) {
-        // ---- next child of the current node group
-        const uint32_t j = __ffs(ng_bits >> 24) - 1;
-        ng_bits &= ~(1u << (24 + j));
-        const uint32_t s = j ^ oct;
-        const uint32_t ni = ng_base + __popc((ng_bits & 0xFFu) & ((1u << s) - 1u));
         if (ng_bits > 0x00FFFFFFu) {
-            if (sp >= STACK_SIZE) {
-                err |= TRACE_ERR_STACK;
-                break;
-            }
-            stack[sp * TRACE_BLOCK] = make_uint2(ng_base, ng_bits);
-            sp++;
+            if (!node_step<COUNT>(mr, r, best.t, ng_base, ng_bits, tg_base, tg_bits, st, visits, err, nvis)) return;
+        } else {
+            tg_base = ng_base;
+            tg_bits = ng_bits;
+            ng_bits = 0;
         }
-        // A tree visits each node at most once; a bad index or a longer walk
-        // means a corrupt structure: flag it and stop this ray.
-        if (ni >= node_count || ++visits > node_count) {
-            err |= (ni >= node_count) ? TRACE_ERR_BOUNDS : TRACE_ERR_LIMIT;
-            break;
+        while (tg_bits) {
+            const uint32_t k = __ffs(tg_bits) - 1;
+            tg_bits &= tg_bits - 1;
+            tri_test<COUNT>(mr, r, tg_base + k, best, err, ntri);
         }
-        const uint4 *np = reinterpret_cast<const uint4 *>(nodes + ni);
-        const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
-        if (COUNT) nvis++;
-        const uint32_t imask = w0.w >> 24;
-        // Slab parameter of plane q on one axis: t(q) = q * A + B with
-        // A = 2^e * inv_d (exact: a power-of-two scaling) and B = (p - o) * inv_d,
-        // one FMA per plane. Its rounding error is below 2u(|B| + 256|A|)
-        // (u = 2^-24); the slack 2^-21 (|B| + 256|A|) moves the near planes
-        // down and the far planes up by more than that, so the test accepts
-        // every box that the exact slab test on the decoded box accepts.
-        float A[3], Bn[3], Bf[3];
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            const float p = __uint_as_float(a == 0 ? w0.x : (a == 1 ? w0.y : w0.z));
-            const float sc = __uint_as_float(((w0.w >> (8 * a)) & 0xFFu) << 23);
-            const float inv = a == 0 ? ix : (a == 1 ? iy : iz);
-            const float o = a == 0 ? ox : (a == 1 ? oy : oz);
-            A[a] = __fmul_rn(sc, inv);
-            const float B = __fmul_rn(__fsub_rn(p, o), inv);
-            const float slack = __fmul_rn(__fmaf_rn(fabsf(A[a]), 256.0f, fabsf(B)), 4.76837158203125e-07f);
-            Bn[a] = __fsub_rn(B, slack);
-            Bf[a] = __fadd_rn(B, slack);
-        }
-        // quantised planes: lo x = w2.xy, lo y = w2.zw, lo z = w3.xy, hi x = w3.zw, hi y = w4.xy, hi z = w4.zw
-        const uint32_t nxa = nx ? w3.z : w2.x, nxb = nx ? w3.w : w2.y, fxa = nx ? w2.x : w3.z, fxb = nx ? w2.y : w3.w;
-        const uint32_t nya = ny ? w4.x : w2.z, nyb = ny ? w4.y : w2.w, fya = ny ? w2.z : w4.x, fyb = ny ? w2.w : w4.y;
-        const uint32_t nza = nz ? w4.z : w3.x, nzb = nz ? w4.w : w3.y, fza = nz ? w3.x : w4.z, fzb = nz ? w3.y : w4.w;
-        uint32_t hitmask = 0;
-#pragma unroll
-        for (int c = 0; c < 8; c++) {
-            const uint32_t meta = ((c < 4 ? w1.z : w1.w) >> (8 * (c & 3))) & 0xFFu;
-            const uint32_t sel = 0x7540u | (uint32_t)(c & 3);
-            const float tnx = __fmaf_rn(byte_to_float(c < 4 ? nxa : nxb, sel), A[0], Bn[0]);
-            const float tfx = __fmaf_rn(byte_to_float(c < 4 ? fxa : fxb, sel), A[0], Bf[0]);
-            const float tny = __fmaf_rn(byte_to_float(c < 4 ? nya : nyb, sel), A[1], Bn[1]);
-            const float tfy = __fmaf_rn(byte_to_float(c < 4 ? fya : fyb, sel), A[1], Bf[1]);
-            const float tnz = __fmaf_rn(byte_to_float(c < 4 ? nza : nzb, sel), A[2], Bn[2]);
-            const float tfz = __fmaf_rn(byte_to_float(c < 4 ? fza : fzb, sel), A[2], Bf[2]);
-            const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
-            const float tmax = fminf(fminf(tfx, tfy), tfz);
-            if (meta != 0 && tmin <= tmax && tmin <= best.t && tmax >= 0.0f) {
-                uint32_t bit = meta & 31u;
-                if (bit >= 24u) bit ^= oct;
-                hitmask |= (meta >> 5) << bit;
-            }
-        }
-        // ---- triangles of this node's leaf children
-        uint32_t tbits = hitmask & 0x00FFFFFFu;
-        const uint32_t tbase = w1.y;
-        while (tbits) {
-            const uint32_t k = __ffs(tbits) - 1;
-            tbits &= tbits - 1;
-            if (tbase + k >= tri_count) {
-                err |= TRACE_ERR_BOUNDS;
-                continue;
-            }
-            const float4 *tp = reinterpret_cast<const float4 *>(tris + tbase + k);
-            const float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
-            if (COUNT) ntri++;
-            const float nu = t0.x, nv = t0.y, npl = t0.z, pu = t0.w, pv = t1.x, e0u = t1.z, e0v = t1.w, e1u = t2.x, e1v = t2.y;
-            const int iw = __float_as_int(t1.y) & TRI_W_BITS;
-            const float du = iw == 0 ? dy : dx, dv = iw == 2 ? dy : dz, dw = iw == 0 ? dx : (iw == 1 ? dy : dz);
-            const float ou = iw == 0 ? oy : ox, ov = iw == 2 ? oy : oz, ow = iw == 0 ? ox : (iw == 1 ? oy : oz);
-            // _IntersectTri, CoreRef.cpp:18-40
-            const float det = __fadd_rn(__fadd_rn(__fmul_rn(du, nu), __fmul_rn(dv, nv)), dw);
-            const float dett = __fsub_rn(npl, __fadd_rn(__fadd_rn(__fmul_rn(ou, nu), __fmul_rn(ov, nv)), ow));
-            const float Du = __fsub_rn(__fmul_rn(du, dett), __fmul_rn(__fsub_rn(pu, ou), det));
-            const float Dv = __fsub_rn(__fmul_rn(dv, dett), __fmul_rn(__fsub_rn(pv, ov), det));
-            const float detu = __fsub_rn(__fmul_rn(e1v, Du), __fmul_rn(e1u, Dv));
-            const float detv = __fsub_rn(__fmul_rn(e0u, Dv), __fmul_rn(e0v, Du));
-            const float tmpdet0 = __fsub_rn(__fsub_rn(det, detu), detv);
-            if ((tmpdet0 > -HIT_EPS && detu > -HIT_EPS && detv > -HIT_EPS) || (tmpdet0 < HIT_EPS && detu < HIT_EPS && detv < HIT_EPS)) {
-                const float rdet = __frcp_rn(det); // 1.0f / det, correctly rounded
-                const float t = __fmul_rn(dett, rdet);
-                const int gp = (int)(prim_base + __float_as_uint(t2.z));
-                if (t > 0.0f && (t < best.t || (t == best.t && best.prim >= 0 && gp < best.prim))) {
-                    best.t = t;
-                    best.u = __fmul_rn(detu, rdet);
-                    best.v = __fmul_rn(detv, rdet);
-                    best.prim = gp;
-                    best.obj = obj;
-                }
-            }
-        }
-        // ---- next node group
-        ng_base = w1.x;
-        ng_bits = (hitmask & 0xFF000000u) | imask;
         if (ng_bits <= 0x00FFFFFFu) {
-            if (sp == 0) break;
-            sp--;
-            const uint2 e = stack[sp * TRACE_BLOCK];
+            if (st.sp == 0) return;
+            const uint2 e = st.pop();
             ng_base = e.x;
             ng_bits = e.y;
         }
@@ -185,45 +277,7 @@ __device__ __forceinline__ void trace_mesh(const WideNode *__restrict__ nodes, c
 }
 
 template <bool COUNT>
-__global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, const float4 *__restrict__ rays, uint32_t n, float4 *__restrict__ hits,
-                                                               int32_t *__restrict__ obj_out, uint32_t *__restrict__ err_out,
-                                                               unsigned long long *__restrict__ counters) {
-    __shared__ uint2 s_stack[STACK_SIZE * TRACE_BLOCK];
-    const uint32_t i = blockIdx.x * TRACE_BLOCK + threadIdx.x;
-    uint32_t err = 0, nvis = 0, ntri = 0;
-    if (i < n) {
-        const float4 r0 = __ldg(rays + 2ull * i), r1 = __ldg(rays + 2ull * i + 1);
-        Best best;
-        best.t = r0.w;
-        best.u = best.v = 0.0f;
-        best.prim = -1;
-        best.obj = -1;
-        const float sx = safe_inv(r1.x), sy = safe_inv(r1.y), sz = safe_inv(r1.z);
-        for (uint32_t m = 0; m < sv.n_inst; m++) {
-            const InstanceRec *ir = sv.inst + m;
-            float bmin[3], bmax[3], x[12];
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                bmin[k] = __ldg(&ir->bbox_min[k]);
-                bmax[k] = __ldg(&ir->bbox_max[k]);
-            }
-            if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
-#pragma unroll
-            for (int k = 0; k < 12; k++) x[k] = __ldg(&ir->inv_xform[k]);
-            // TransformRay, CoreRef.cpp:1605-1617
-            const float tox = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(x[0], r0.x), __fmul_rn(x[3], r0.y)), __fmul_rn(x[6], r0.z)), x[9]);
-            const float toy = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(x[1], r0.x), __fmul_rn(x[4], r0.y)), __fmul_rn(x[7], r0.z)), x[10]);
-            const float toz = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(x[2], r0.x), __fmul_rn(x[5], r0.y)), __fmul_rn(x[8], r0.z)), x[11]);
-            const float tdx = __fadd_rn(__fadd_rn(__fmul_rn(x[0], r1.x), __fmul_rn(x[3], r1.y)), __fmul_rn(x[6], r1.z));
-            const float tdy = __fadd_rn(__fadd_rn(__fmul_rn(x[1], r1.x), __fmul_rn(x[4], r1.y)), __fmul_rn(x[7], r1.z));
-            const float tdz = __fadd_rn(__fadd_rn(__fmul_rn(x[2], r1.x), __fmul_rn(x[5], r1.y)), __fmul_rn(x[8], r1.z));
-            trace_mesh<COUNT>(sv.nodes + __ldg(&ir->node_base), sv.leaf_tris + __ldg(&ir->tri_base), __ldg(&ir->prim_base),
-                              __ldg(&ir->node_count), __ldg(&ir->tri_count), (int)m, tox, toy,
-                              toz, tdx, tdy, tdz, best, s_stack + threadIdx.x, err, nvis, ntri);
-        }
-        hits[i] = make_float4(__int_as_float(best.prim), best.t, best.prim >= 0 ? best.u : 0.0f, best.prim >= 0 ? best.v : 0.0f);
-        if (obj_out) obj_out[i] = best.obj;
-    }
+__device__ __forceinline__ void flush_counters(uint32_t err, uint32_t nvis, uint32_t ntri, uint32_t *err_out, unsigned long long *counters) {
     if (err) atomicOr(err_out, err);
     if (COUNT) {
         unsigned long long a = nvis, b = ntri;
@@ -238,16 +292,191 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
     }
 }
 
+template <bool COUNT>
+__global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, const float4 *__restrict__ rays, uint32_t n, float4 *__restrict__ hits,
+                                                               int32_t *__restrict__ obj_out, uint32_t *__restrict__ err_out,
+                                                               unsigned long long *__restrict__ counters) {
+    __shared__ uint2 s_stack[SMEM_STACK * TRACE_BLOCK];
+    Stack st;
+    st.smem = s_stack + threadIdx.x;
+    st.sp = 0;
+    const uint32_t i = blockIdx.x * TRACE_BLOCK + threadIdx.x;
+    uint32_t err = 0, nvis = 0, ntri = 0;
+    if (i < n) {
+        const float4 r0 = __ldg(rays + 2ull * i), r1 = __ldg(rays + 2ull * i + 1);
+        Best best;
+        best.t = r0.w;
+        best.u = best.v = 0.0f;
+        best.prim = -1;
+        best.obj = -1;
+        const float sx = safe_inv(r1.x), sy = safe_inv(r1.y), sz = safe_inv(r1.z);
+        for (uint32_t m = 0; m < sv.n_inst; m++) {
+            const InstanceRec *ir = sv.inst + m;
+            float bmin[3], bmax[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                bmin[k] = __ldg(&ir->bbox_min[k]);
+                bmax[k] = __ldg(&ir->bbox_max[k]);
+            }
+            if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
+            trace_mesh<COUNT>(mesh_of(sv, ir, (int)m), transform_ray(ir, r0, r1), best, st, err, nvis, ntri);
+        }
+        hits[i] = make_float4(__int_as_float(best.prim), best.t, best.prim >= 0 ? best.u : 0.0f, best.prim >= 0 ? best.v : 0.0f);
+        if (obj_out) obj_out[i] = best.obj;
+    }
+    flush_counters<COUNT>(err, nvis, ntri, err_out, counters);
+}
+
+// Persistent variant. Per lane: the ray it owns (index ri), the next instance
+// to try (mi) and, while a mesh is being traversed (in_mesh), the traversal
+// state. Each loop iteration of a warp: refill lanes without a ray when
+// enough of them are idle, advance lanes to their next instance (or finish
+// their ray), then one node step plus the triangles it hit.
+template <bool COUNT>
+__global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, const float4 *__restrict__ rays, uint32_t n,
+                                                                  float4 *__restrict__ hits, int32_t *__restrict__ obj_out,
+                                                                  uint32_t *__restrict__ err_out, unsigned long long *__restrict__ counters,
+                                                                  uint32_t *__restrict__ next_ray, int refill_min, int postpone_min) {
+    __shared__ uint2 s_stack[SMEM_STACK * TRACE_BLOCK];
+    Stack st;
+    st.smem = s_stack + threadIdx.x;
+    st.sp = 0;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lanemask_lt = (1u << lane) - 1u;
+    uint32_t err = 0, nvis = 0, ntri = 0;
+    uint32_t ri = NO_RAY, mi = 0, visits = 0;
+    bool in_mesh = false, pool_empty = false;
+    Best best;
+    best.t = 0.0f;
+    best.u = best.v = 0.0f;
+    best.prim = best.obj = -1;
+    LocalRay r = make_local_ray(0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f);
+    MeshRef mr{};
+    uint32_t ng_base = 0, ng_bits = 0, tg_base = 0, tg_bits = 0;
+    while (true) {
+        // ---- refill lanes that have no ray
+        const uint32_t need = __ballot_sync(0xffffffffu, ri == NO_RAY);
+        if (!pool_empty && need != 0 && (__popc(need) >= refill_min || need == 0xffffffffu)) {
+            const uint32_t leader = __ffs(need) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(next_ray, (uint32_t)__popc(need));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + __popc(need) >= n) pool_empty = true;
+            if (ri == NO_RAY) {
+                const uint32_t idx = base + __popc(need & lanemask_lt);
+                if (idx < n) {
+                    ri = idx;
+                    mi = 0;
+                    in_mesh = false;
+                    best.t = __ldg(&rays[2ull * idx].w);
+                    best.u = best.v = 0.0f;
+                    best.prim = best.obj = -1;
+                }
+            }
+        }
+        if (pool_empty && __all_sync(0xffffffffu, ri == NO_RAY)) break;
+        if (ri == NO_RAY) continue;
+        // ---- next instance whose box the ray enters, or the end of the ray
+        if (!in_mesh) {
+            const float4 r0 = __ldg(rays + 2ull * ri), r1 = __ldg(rays + 2ull * ri + 1);
+            const float sx = safe_inv(r1.x), sy = safe_inv(r1.y), sz = safe_inv(r1.z);
+            while (mi < sv.n_inst) {
+                const InstanceRec *ir = sv.inst + mi;
+                float bmin[3], bmax[3];
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    bmin[k] = __ldg(&ir->bbox_min[k]);
+                    bmax[k] = __ldg(&ir->bbox_max[k]);
+                }
+                mi++;
+                if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
+                mr = mesh_of(sv, ir, (int)mi - 1);
+                r = transform_ray(ir, r0, r1);
+                ng_base = 0;
+                ng_bits = (1u << (24 + r.oct)) | 1u;
+                tg_bits = 0;
+                st.sp = 0;
+                visits = 0;
+                in_mesh = true;
+                break;
+            }
+            if (!in_mesh) {
+                hits[ri] = make_float4(__int_as_float(best.prim), best.t, best.prim >= 0 ? best.u : 0.0f, best.prim >= 0 ? best.v : 0.0f);
+                if (obj_out) obj_out[ri] = best.obj;
+                ri = NO_RAY;
+                continue;
+            }
+        }
+        // ---- one traversal step
+        bool ok = true;
+        if (ng_bits > 0x00FFFFFFu) {
+            ok = node_step<COUNT>(mr, r, best.t, ng_base, ng_bits, tg_base, tg_bits, st, visits, err, nvis);
+        } else {
+            tg_base = ng_base; // a postponed triangle group came off the stack
+            tg_bits = ng_bits;
+            ng_bits = 0;
+        }
+        if (!ok) {
+            in_mesh = false;
+            mi = sv.n_inst; // abandon the ray; the error flag reports it
+            continue;
+        }
+        while (tg_bits) {
+            // few lanes with triangles: put the group back and keep traversing
+            if (__popc(__activemask()) < postpone_min && st.push(make_uint2(tg_base, tg_bits))) {
+                tg_bits = 0;
+                break;
+            }
+            const uint32_t k = __ffs(tg_bits) - 1;
+            tg_bits &= tg_bits - 1;
+            tri_test<COUNT>(mr, r, tg_base + k, best, err, ntri);
+        }
+        if (ng_bits <= 0x00FFFFFFu) {
+            if (st.sp == 0) {
+                in_mesh = false;
+            } else {
+                const uint2 e = st.pop();
+                ng_base = e.x;
+                ng_bits = e.y;
+            }
+        }
+    }
+    flush_counters<COUNT>(err, nvis, ntri, err_out, counters);
+}
+
+int g_persistent_blocks = 0;
+
 } // namespace
 
 cudaError_t launch_trace_closest(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
-                                 unsigned long long *counters, bool count, cudaStream_t st) {
+                                 unsigned long long *counters, bool count, cudaStream_t st, const TraceParams &tp) {
     if (n == 0) return cudaSuccess;
-    const uint32_t grid = (n + TRACE_BLOCK - 1) / TRACE_BLOCK;
+    if (!tp.persistent) {
+        const uint32_t grid = (n + TRACE_BLOCK - 1) / TRACE_BLOCK;
+        if (count)
+            k_trace_closest<true><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters);
+        else
+            k_trace_closest<false><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters);
+        return cudaGetLastError();
+    }
+    if (!tp.next_ray) return cudaErrorInvalidValue;
+    if (g_persistent_blocks == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_persistent<false>, TRACE_BLOCK, 0);
+        if (e != cudaSuccess) return e;
+        g_persistent_blocks = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    cudaError_t e = cudaMemsetAsync(tp.next_ray, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    const uint32_t grid = (uint32_t)g_persistent_blocks;
     if (count)
-        k_trace_closest<true><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters);
+        k_trace_persistent<true><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min,
+                                                               tp.postpone_min);
     else
-        k_trace_closest<false><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters);
+        k_trace_persistent<false><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min,
+                                                                tp.postpone_min);
     return cudaGetLastError();
 }
 

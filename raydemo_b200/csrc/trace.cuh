@@ -18,10 +18,18 @@ constexpr uint32_t TRACE_ERR_STACK = 1u;
 constexpr uint32_t TRACE_ERR_BOUNDS = 2u; // a node or triangle index outside the mesh's arrays
 constexpr uint32_t TRACE_ERR_LIMIT = 4u;  // more node visits than the mesh has nodes
 
+// Kernel choice and its knobs (picked by the tuner).
+struct TraceParams {
+    bool persistent = true; // resident grid with per-lane ray refill
+    int refill_min = 8;     // refill a warp's idle lanes once at least this many are idle
+    int postpone_min = 8;   // postpone triangle groups while fewer lanes than this test triangles
+    uint32_t *next_ray = nullptr; // device work counter for the persistent kernel
+};
+
 // rays: n x 8 floats (ox, oy, oz, tmax, dx, dy, dz, unused).
 // hits: n x {prim, t, u, v}; obj may be null. counters (may be null when
 // count == false): [0] node visits, [1] triangle tests.
 cudaError_t launch_trace_closest(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
-                                 unsigned long long *counters, bool count, cudaStream_t st);
+                                 unsigned long long *counters, bool count, cudaStream_t st, const TraceParams &tp);
 
 } // namespace rg
