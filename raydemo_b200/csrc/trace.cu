@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lanemask_lt = (1u << lane) - 1u;
     uint32_t err = 0, nvis = 0, ntri = 0;
-    uint32_t ri = NO_RAY, mi = 0, visits = 0;
+    uint32_t ri = NO_RAY, mi = 0, visits = 0, steps = 0;
     bool in_mesh = false, pool_empty = false;
     Best best;
     best.t = 0.0f;
@@ -397,6 +397,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
                 tg_bits = 0;
                 st.sp = 0;
                 visits = 0;
+                steps = 0;
                 in_mesh = true;
                 break;
             }
@@ -407,11 +408,15 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
                 continue;
             }
         }
-        // ---- one traversal step
-        bool ok = true;
-        if (ng_bits > 0x00FFFFFFu) {
+        // ---- one traversal step. Every step either visits a node or
+        // consumes a postponed triangle group, and each node yields at most
+        // one of each, so a mesh takes at most 2 * node_count steps; more
+        // means a corrupt structure.
+        bool ok = ++steps <= 2u * mr.node_count + 8u;
+        if (!ok) err |= TRACE_ERR_LIMIT;
+        if (ok && ng_bits > 0x00FFFFFFu) {
             ok = node_step<COUNT>(mr, r, best.t, ng_base, ng_bits, tg_base, tg_bits, st, visits, err, nvis);
-        } else {
+        } else if (ok) {
             tg_base = ng_base; // a postponed triangle group came off the stack
             tg_bits = ng_bits;
             ng_bits = 0;
@@ -422,8 +427,11 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
             continue;
         }
         while (tg_bits) {
-            // few lanes with triangles: put the group back and keep traversing
-            if (__popc(__activemask()) < postpone_min && st.push(make_uint2(tg_base, tg_bits))) {
+            // Few lanes with triangles while this lane still has nodes to
+            // visit: put the group back and keep traversing. A group without
+            // node work behind it is always tested, so every group is tested
+            // the second time it comes off the stack at the latest.
+            if (ng_bits > 0x00FFFFFFu && __popc(__activemask()) < postpone_min && st.push(make_uint2(tg_base, tg_bits))) {
                 tg_bits = 0;
                 break;
             }
