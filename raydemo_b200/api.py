@@ -92,9 +92,12 @@ class Scene:
         self._renderer = renderer  # keeps the device context's owner alive
 
     def __del__(self):
-        if getattr(self, "_h", None) and self._h.value:
-            lib().ray_destroy_scene(self._h)
-            self._h = C.c_void_p()
+        try:
+            if getattr(self, "_h", None) and self._h.value:
+                lib().ray_destroy_scene(self._h)
+                self._h = C.c_void_p()
+        except Exception:  # interpreter shutdown: the module state may be gone
+            pass
 
     @property
     def handle(self) -> C.c_void_p:
@@ -258,9 +261,12 @@ class Renderer:
         self._h = out
 
     def __del__(self):
-        if getattr(self, "_h", None) and self._h.value:
-            lib().ray_destroy_renderer(self._h)
-            self._h = C.c_void_p()
+        try:
+            if getattr(self, "_h", None) and self._h.value:
+                lib().ray_destroy_renderer(self._h)
+                self._h = C.c_void_p()
+        except Exception:  # interpreter shutdown: the module state may be gone
+            pass
 
     @property
     def handle(self) -> C.c_void_p:
