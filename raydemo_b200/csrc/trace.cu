@@ -24,10 +24,11 @@ namespace rg {
 namespace {
 
 constexpr int TRACE_BLOCK = 128;
-constexpr int SMEM_STACK = 24;  // entries per thread in shared memory
-constexpr int LMEM_STACK = 40;  // further entries in local memory (rarely used)
+constexpr int SMEM_STACK = 16;  // entries per thread in shared memory
+constexpr int LMEM_STACK = 48;  // further entries in local memory (rarely used)
 constexpr int STACK_SIZE = SMEM_STACK + LMEM_STACK;
 constexpr uint32_t NO_RAY = 0xffffffffu;
+constexpr uint32_t NO_NODE = 0xffffffffu;
 
 __device__ __forceinline__ float byte_to_float(uint32_t word, uint32_t sel) {
     // 0x4B0000bb is 2^23 + bb as a float; subtracting 2^23 leaves bb exactly.
@@ -77,22 +78,36 @@ struct MeshRef {
     int obj;
 };
 
-// Two-tier per-thread stack: the first SMEM_STACK entries in shared memory
-// (strided by the block size), the rest in a local array.
+// Two-tier per-thread stack of groups: the first SMEM_STACK entries in shared
+// memory (strided by the block size), the rest in local arrays. An entry is a
+// group (base, bits) plus a lower bound on the entry distance of everything
+// in it, so that a group starting beyond the closest hit so far is dropped.
 struct Stack {
     uint2 *smem;
+    float *sdist;
     uint2 lmem[LMEM_STACK];
+    float ldist[LMEM_STACK];
     int sp;
-    __device__ __forceinline__ bool push(uint2 e) {
+    __device__ __forceinline__ bool push(uint2 e, float d) {
         if (sp >= STACK_SIZE) return false;
-        if (sp < SMEM_STACK) smem[sp * TRACE_BLOCK] = e;
-        else lmem[sp - SMEM_STACK] = e;
+        if (sp < SMEM_STACK) {
+            smem[sp * TRACE_BLOCK] = e;
+            sdist[sp * TRACE_BLOCK] = d;
+        } else {
+            lmem[sp - SMEM_STACK] = e;
+            ldist[sp - SMEM_STACK] = d;
+        }
         sp++;
         return true;
     }
-    __device__ __forceinline__ uint2 pop() {
+    __device__ __forceinline__ uint2 pop(float &d) {
         sp--;
-        return sp < SMEM_STACK ? smem[sp * TRACE_BLOCK] : lmem[sp - SMEM_STACK];
+        if (sp < SMEM_STACK) {
+            d = sdist[sp * TRACE_BLOCK];
+            return smem[sp * TRACE_BLOCK];
+        }
+        d = ldist[sp - SMEM_STACK];
+        return lmem[sp - SMEM_STACK];
     }
 };
 
@@ -132,84 +147,13 @@ __device__ __forceinline__ MeshRef mesh_of(const SceneView &sv, const InstanceRe
     return mr;
 }
 
-// Node step: takes the next child of node group (ng_base, ng_bits), tests
-// its 8 children and returns their hits as a node group (internal children,
-// bits 24..31, with the node's imask in bits 0..7) and a triangle group
-// (bits 0..23). Returns false (and sets err) on a corrupt index.
-template <bool COUNT>
-__device__ __forceinline__ bool node_step(const MeshRef &mr, const LocalRay &r, float best_t, uint32_t &ng_base, uint32_t &ng_bits,
-                                          uint32_t &tg_base, uint32_t &tg_bits, Stack &st, uint32_t &visits, uint32_t &err,
-                                          uint32_t &nvis) {
-    const uint32_t j = __ffs(ng_bits >> 24) - 1;
-    ng_bits &= ~(1u << (24 + j));
-    const uint32_t s = j ^ r.oct;
-    const uint32_t ni = ng_base + __popc((ng_bits & 0xFFu) & ((1u << s) - 1u));
-    if (ng_bits > 0x00FFFFFFu && !st.push(make_uint2(ng_base, ng_bits))) {
-        err |= TRACE_ERR_STACK;
-        return false;
-    }
-    // A tree visits each node at most once; a bad index or a longer walk
-    // means a corrupt structure: flag it and stop this ray.
-    if (ni >= mr.node_count || ++visits > mr.node_count) {
-        err |= (ni >= mr.node_count) ? TRACE_ERR_BOUNDS : TRACE_ERR_LIMIT;
-        return false;
-    }
-    const uint4 *np = reinterpret_cast<const uint4 *>(mr.nodes + ni);
-    const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
-    if (COUNT) nvis++;
-    const uint32_t imask = w0.w >> 24;
-    // Slab parameter of plane q on one axis: t(q) = q * A + B with
-    // A = 2^e * inv_d (exact: a power-of-two scaling) and B = (p - o) * inv_d,
-    // one FMA per plane. Its rounding error is below 2u(|B| + 256|A|)
-    // (u = 2^-24); the slack 2^-21 (|B| + 256|A|) moves the near planes
-    // down and the far planes up by more than that, so the test accepts
-    // every box that the exact slab test on the decoded box accepts.
-    float A[3], Bn[3], Bf[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        const float p = __uint_as_float(a == 0 ? w0.x : (a == 1 ? w0.y : w0.z));
-        const float sc = __uint_as_float(((w0.w >> (8 * a)) & 0xFFu) << 23);
-        const float inv = a == 0 ? r.ix : (a == 1 ? r.iy : r.iz);
-        const float o = a == 0 ? r.ox : (a == 1 ? r.oy : r.oz);
-        A[a] = __fmul_rn(sc, inv);
-        const float B = __fmul_rn(__fsub_rn(p, o), inv);
-        const float slack = __fmul_rn(__fmaf_rn(fabsf(A[a]), 256.0f, fabsf(B)), 4.76837158203125e-07f);
-        Bn[a] = __fsub_rn(B, slack);
-        Bf[a] = __fadd_rn(B, slack);
-    }
-    // Near/far plane words by direction sign, so that a NaN slab value
-    // (origin on a plane of a box the ray runs parallel to) leaves that axis
-    // unbounded, which keeps the test conservative. Planes: lo x = w2.xy,
-    // lo y = w2.zw, lo z = w3.xy, hi x = w3.zw, hi y = w4.xy, hi z = w4.zw.
-    const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
-    const uint32_t nxa = nx ? w3.z : w2.x, nxb = nx ? w3.w : w2.y, fxa = nx ? w2.x : w3.z, fxb = nx ? w2.y : w3.w;
-    const uint32_t nya = ny ? w4.x : w2.z, nyb = ny ? w4.y : w2.w, fya = ny ? w2.z : w4.x, fyb = ny ? w2.w : w4.y;
-    const uint32_t nza = nz ? w4.z : w3.x, nzb = nz ? w4.w : w3.y, fza = nz ? w3.x : w4.z, fzb = nz ? w3.y : w4.w;
-    uint32_t hitmask = 0;
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
-        const uint32_t meta = ((c < 4 ? w1.z : w1.w) >> (8 * (c & 3))) & 0xFFu;
-        const uint32_t sel = 0x7540u | (uint32_t)(c & 3);
-        const float tnx = __fmaf_rn(byte_to_float(c < 4 ? nxa : nxb, sel), A[0], Bn[0]);
-        const float tfx = __fmaf_rn(byte_to_float(c < 4 ? fxa : fxb, sel), A[0], Bf[0]);
-        const float tny = __fmaf_rn(byte_to_float(c < 4 ? nya : nyb, sel), A[1], Bn[1]);
-        const float tfy = __fmaf_rn(byte_to_float(c < 4 ? fya : fyb, sel), A[1], Bf[1]);
-        const float tnz = __fmaf_rn(byte_to_float(c < 4 ? nza : nzb, sel), A[2], Bn[2]);
-        const float tfz = __fmaf_rn(byte_to_float(c < 4 ? fza : fzb, sel), A[2], Bf[2]);
-        const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
-        const float tmax = fminf(fminf(tfx, tfy), tfz);
-        if (meta != 0 && tmin <= tmax && tmin <= best_t && tmax >= 0.0f) {
-            uint32_t bit = meta & 31u;
-            if (bit >= 24u) bit ^= r.oct;
-            hitmask |= (meta >> 5) << bit;
-        }
-    }
-    ng_base = w1.x;
-    ng_bits = (hitmask & 0xFF000000u) | imask;
-    tg_base = w1.y;
-    tg_bits = hitmask & 0x00FFFFFFu;
-    return true;
-}
+// Traversal state of one ray in one mesh: the node to visit next (NO_NODE:
+// take a group from the stack) and the counters of the corruption guards.
+struct Trav {
+    uint32_t ni, visits, steps;
+};
+
+enum { STEP_CONTINUE = 0, STEP_DONE = 1, STEP_ERROR = 2 };
 
 // One triangle test; updates best when it is the closer hit.
 template <bool COUNT>
@@ -247,33 +191,142 @@ __device__ __forceinline__ void tri_test(const MeshRef &mr, const LocalRay &r, u
     }
 }
 
-// Whole traversal of one mesh for one ray (the one-thread-per-ray kernel).
 template <bool COUNT>
-__device__ __forceinline__ void trace_mesh(const MeshRef &mr, const LocalRay &r, Best &best, Stack &st, uint32_t &err, uint32_t &nvis,
-                                           uint32_t &ntri) {
-    uint32_t ng_base = 0, ng_bits = (1u << (24 + r.oct)) | 1u; // the root as slot 0 of a virtual parent
-    uint32_t tg_base = 0, tg_bits = 0, visits = 0;
-    st.sp = 0;
-    while (true) {
-        if (ng_bits > 0x00FFFFFFu) {
-            if (!node_step<COUNT>(mr, r, best.t, ng_base, ng_bits, tg_base, tg_bits, st, visits, err, nvis)) return;
-        } else {
-            tg_base = ng_base;
-            tg_bits = ng_bits;
-            ng_bits = 0;
+__device__ __forceinline__ void tri_group(const MeshRef &mr, const LocalRay &r, uint32_t base, uint32_t bits, Best &best, uint32_t &err,
+                                          uint32_t &ntri) {
+    while (bits) {
+        const uint32_t k = __ffs(bits) - 1;
+        bits &= bits - 1;
+        tri_test<COUNT>(mr, r, base + k, best, err, ntri);
+    }
+}
+
+// One traversal step: visits one node (taking a group off the stack first
+// when there is no node to visit) and tests the triangles it hits. The
+// nearest internal child that the ray enters becomes the next node; the
+// other hit internal children are pushed as one node group (bits 24..31,
+// octant order, with the node's imask in bits 0..7) tagged with the least
+// entry distance among them, and a group whose tag exceeds the closest hit
+// when it comes off the stack is dropped: a triangle in it could only be hit
+// at a larger t. Triangle groups are tested at once, unless fewer than
+// postpone_min lanes of the warp have triangles while this lane has a node to
+// visit next: then the group is pushed (tagged the same way) and tested when
+// it comes off the stack.
+template <bool COUNT>
+__device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, Best &best, Stack &st, Trav &tv, int postpone_min,
+                                         uint32_t &err, uint32_t &nvis, uint32_t &ntri) {
+    // Each node yields at most one node visit, one pushed node group (whose
+    // pops each visit a node or drop the group) and one triangle group, so a
+    // mesh takes fewer than 4 * node_count steps; more means a corrupt
+    // structure.
+    if (++tv.steps > 4u * mr.node_count + 8u) {
+        err |= TRACE_ERR_LIMIT;
+        return STEP_ERROR;
+    }
+    if (tv.ni == NO_NODE) {
+        if (st.sp == 0) return STEP_DONE;
+        float dist;
+        uint2 e = st.pop(dist);
+        if (dist > best.t) return STEP_CONTINUE;
+        if (e.y <= 0x00FFFFFFu) { // a postponed triangle group
+            tri_group<COUNT>(mr, r, e.x, e.y, best, err, ntri);
+            return STEP_CONTINUE;
         }
-        while (tg_bits) {
-            const uint32_t k = __ffs(tg_bits) - 1;
-            tg_bits &= tg_bits - 1;
-            tri_test<COUNT>(mr, r, tg_base + k, best, err, ntri);
-        }
-        if (ng_bits <= 0x00FFFFFFu) {
-            if (st.sp == 0) return;
-            const uint2 e = st.pop();
-            ng_base = e.x;
-            ng_bits = e.y;
+        const uint32_t j = __ffs(e.y >> 24) - 1;
+        e.y &= ~(1u << (24 + j));
+        const uint32_t s = j ^ r.oct;
+        tv.ni = e.x + __popc((e.y & 0xFFu) & ((1u << s) - 1u));
+        if (e.y > 0x00FFFFFFu) st.push(e, dist); // fits: an entry was just taken
+    }
+    const uint32_t ni = tv.ni;
+    // A tree visits each node at most once; a bad index or a longer walk
+    // means a corrupt structure: flag it and stop this ray.
+    if (ni >= mr.node_count || ++tv.visits > mr.node_count) {
+        err |= (ni >= mr.node_count) ? TRACE_ERR_BOUNDS : TRACE_ERR_LIMIT;
+        return STEP_ERROR;
+    }
+    const uint4 *np = reinterpret_cast<const uint4 *>(mr.nodes + ni);
+    const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+    if (COUNT) nvis++;
+    // Slab parameter of plane q on one axis: t(q) = q * A + B with
+    // A = 2^e * inv_d (exact: a power-of-two scaling) and B = (p - o) * inv_d,
+    // one FMA per plane. Its rounding error is below 2u(|B| + 256|A|)
+    // (u = 2^-24); the slack 2^-21 (|B| + 256|A|) moves the near planes
+    // down and the far planes up by more than that, so the test accepts
+    // every box that the exact slab test on the decoded box accepts, and the
+    // near distance it gives is a lower bound of the exact one.
+    float A[3], Bn[3], Bf[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float p = __uint_as_float(a == 0 ? w0.x : (a == 1 ? w0.y : w0.z));
+        const float sc = __uint_as_float(((w0.w >> (8 * a)) & 0xFFu) << 23);
+        const float inv = a == 0 ? r.ix : (a == 1 ? r.iy : r.iz);
+        const float o = a == 0 ? r.ox : (a == 1 ? r.oy : r.oz);
+        A[a] = __fmul_rn(sc, inv);
+        const float B = __fmul_rn(__fsub_rn(p, o), inv);
+        const float slack = __fmul_rn(__fmaf_rn(fabsf(A[a]), 256.0f, fabsf(B)), 4.76837158203125e-07f);
+        Bn[a] = __fsub_rn(B, slack);
+        Bf[a] = __fadd_rn(B, slack);
+    }
+    // Near/far plane words by direction sign, so that a NaN slab value
+    // (origin on a plane of a box the ray runs parallel to) leaves that axis
+    // unbounded, which keeps the test conservative. Planes: lo x = w2.xy,
+    // lo y = w2.zw, lo z = w3.xy, hi x = w3.zw, hi y = w4.xy, hi z = w4.zw.
+    const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
+    const uint32_t nxa = nx ? w3.z : w2.x, nxb = nx ? w3.w : w2.y, fxa = nx ? w2.x : w3.z, fxb = nx ? w2.y : w3.w;
+    const uint32_t nya = ny ? w4.x : w2.z, nyb = ny ? w4.y : w2.w, fya = ny ? w2.z : w4.x, fyb = ny ? w2.w : w4.y;
+    const uint32_t nza = nz ? w4.z : w3.x, nzb = nz ? w4.w : w3.y, fza = nz ? w3.x : w4.z, fzb = nz ? w3.y : w4.w;
+    uint32_t node_hits = 0, tri_hits = 0;
+    float d1 = INFINITY, d2 = INFINITY, dt = INFINITY;
+    int c1 = -1;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        const uint32_t meta = ((c < 4 ? w1.z : w1.w) >> (8 * (c & 3))) & 0xFFu;
+        const uint32_t sel = 0x7540u | (uint32_t)(c & 3);
+        const float tnx = __fmaf_rn(byte_to_float(c < 4 ? nxa : nxb, sel), A[0], Bn[0]);
+        const float tfx = __fmaf_rn(byte_to_float(c < 4 ? fxa : fxb, sel), A[0], Bf[0]);
+        const float tny = __fmaf_rn(byte_to_float(c < 4 ? nya : nyb, sel), A[1], Bn[1]);
+        const float tfy = __fmaf_rn(byte_to_float(c < 4 ? fya : fyb, sel), A[1], Bf[1]);
+        const float tnz = __fmaf_rn(byte_to_float(c < 4 ? nza : nzb, sel), A[2], Bn[2]);
+        const float tfz = __fmaf_rn(byte_to_float(c < 4 ? fza : fzb, sel), A[2], Bf[2]);
+        const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
+        const float tmax = fminf(fminf(tfx, tfy), tfz);
+        if (meta != 0 && tmin <= tmax && tmin <= best.t && tmax >= 0.0f) {
+            const uint32_t bit = meta & 31u;
+            if (bit >= 24u) {
+                node_hits |= 1u << (bit ^ r.oct);
+                if (tmin < d1) {
+                    d2 = d1;
+                    d1 = tmin;
+                    c1 = c;
+                } else if (tmin < d2) {
+                    d2 = tmin;
+                }
+            } else {
+                tri_hits |= (meta >> 5) << bit;
+                dt = fminf(dt, tmin);
+            }
         }
     }
+    const uint32_t imask = w0.w >> 24;
+    if (c1 >= 0) {
+        tv.ni = w1.x + __popc(imask & ((1u << c1) - 1u));
+        node_hits &= ~(1u << ((24u + (uint32_t)c1) ^ r.oct));
+    } else {
+        tv.ni = NO_NODE;
+    }
+    if (node_hits && !st.push(make_uint2(w1.x, node_hits | imask), d2)) {
+        err |= TRACE_ERR_STACK;
+        return STEP_ERROR;
+    }
+    if (tri_hits) {
+        if (postpone_min > 0 && tv.ni != NO_NODE) {
+            const uint32_t with_tris = __popc(__ballot_sync(__activemask(), true));
+            if ((int)with_tris < postpone_min && st.push(make_uint2(w1.y, tri_hits), dt)) return STEP_CONTINUE;
+        }
+        tri_group<COUNT>(mr, r, w1.y, tri_hits, best, err, ntri);
+    }
+    return STEP_CONTINUE;
 }
 
 template <bool COUNT>
@@ -297,8 +350,10 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
                                                                int32_t *__restrict__ obj_out, uint32_t *__restrict__ err_out,
                                                                unsigned long long *__restrict__ counters) {
     __shared__ uint2 s_stack[SMEM_STACK * TRACE_BLOCK];
+    __shared__ float s_dist[SMEM_STACK * TRACE_BLOCK];
     Stack st;
     st.smem = s_stack + threadIdx.x;
+    st.sdist = s_dist + threadIdx.x;
     st.sp = 0;
     const uint32_t i = blockIdx.x * TRACE_BLOCK + threadIdx.x;
     uint32_t err = 0, nvis = 0, ntri = 0;
@@ -319,7 +374,12 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
                 bmax[k] = __ldg(&ir->bbox_max[k]);
             }
             if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
-            trace_mesh<COUNT>(mesh_of(sv, ir, (int)m), transform_ray(ir, r0, r1), best, st, err, nvis, ntri);
+            const MeshRef mr = mesh_of(sv, ir, (int)m);
+            const LocalRay r = transform_ray(ir, r0, r1);
+            Trav tv{0u, 0u, 0u};
+            st.sp = 0;
+            while (trav_step<COUNT>(mr, r, best, st, tv, 0, err, nvis, ntri) == STEP_CONTINUE) {
+            }
         }
         hits[i] = make_float4(__int_as_float(best.prim), best.t, best.prim >= 0 ? best.u : 0.0f, best.prim >= 0 ? best.v : 0.0f);
         if (obj_out) obj_out[i] = best.obj;
@@ -331,20 +391,22 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
 // to try (mi) and, while a mesh is being traversed (in_mesh), the traversal
 // state. Each loop iteration of a warp: refill lanes without a ray when
 // enough of them are idle, advance lanes to their next instance (or finish
-// their ray), then one node step plus the triangles it hit.
+// their ray), then one traversal step.
 template <bool COUNT>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, const float4 *__restrict__ rays, uint32_t n,
                                                                   float4 *__restrict__ hits, int32_t *__restrict__ obj_out,
                                                                   uint32_t *__restrict__ err_out, unsigned long long *__restrict__ counters,
                                                                   uint32_t *__restrict__ next_ray, int refill_min, int postpone_min) {
     __shared__ uint2 s_stack[SMEM_STACK * TRACE_BLOCK];
+    __shared__ float s_dist[SMEM_STACK * TRACE_BLOCK];
     Stack st;
     st.smem = s_stack + threadIdx.x;
+    st.sdist = s_dist + threadIdx.x;
     st.sp = 0;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lanemask_lt = (1u << lane) - 1u;
     uint32_t err = 0, nvis = 0, ntri = 0;
-    uint32_t ri = NO_RAY, mi = 0, visits = 0, steps = 0;
+    uint32_t ri = NO_RAY, mi = 0;
     bool in_mesh = false, pool_empty = false;
     Best best;
     best.t = 0.0f;
@@ -352,7 +414,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
     best.prim = best.obj = -1;
     LocalRay r = make_local_ray(0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f);
     MeshRef mr{};
-    uint32_t ng_base = 0, ng_bits = 0, tg_base = 0, tg_bits = 0;
+    Trav tv{NO_NODE, 0u, 0u};
     while (true) {
         // ---- refill lanes that have no ray
         const uint32_t need = __ballot_sync(0xffffffffu, ri == NO_RAY);
@@ -392,12 +454,8 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
                 if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
                 mr = mesh_of(sv, ir, (int)mi - 1);
                 r = transform_ray(ir, r0, r1);
-                ng_base = 0;
-                ng_bits = (1u << (24 + r.oct)) | 1u;
-                tg_bits = 0;
+                tv = Trav{0u, 0u, 0u};
                 st.sp = 0;
-                visits = 0;
-                steps = 0;
                 in_mesh = true;
                 break;
             }
@@ -408,45 +466,13 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
                 continue;
             }
         }
-        // ---- one traversal step. Every step either visits a node or
-        // consumes a postponed triangle group, and each node yields at most
-        // one of each, so a mesh takes at most 2 * node_count steps; more
-        // means a corrupt structure.
-        bool ok = ++steps <= 2u * mr.node_count + 8u;
-        if (!ok) err |= TRACE_ERR_LIMIT;
-        if (ok && ng_bits > 0x00FFFFFFu) {
-            ok = node_step<COUNT>(mr, r, best.t, ng_base, ng_bits, tg_base, tg_bits, st, visits, err, nvis);
-        } else if (ok) {
-            tg_base = ng_base; // a postponed triangle group came off the stack
-            tg_bits = ng_bits;
-            ng_bits = 0;
-        }
-        if (!ok) {
+        // ---- one traversal step
+        const int res = trav_step<COUNT>(mr, r, best, st, tv, postpone_min, err, nvis, ntri);
+        if (res == STEP_DONE) {
+            in_mesh = false;
+        } else if (res == STEP_ERROR) {
             in_mesh = false;
             mi = sv.n_inst; // abandon the ray; the error flag reports it
-            continue;
-        }
-        while (tg_bits) {
-            // Few lanes with triangles while this lane still has nodes to
-            // visit: put the group back and keep traversing. A group without
-            // node work behind it is always tested, so every group is tested
-            // the second time it comes off the stack at the latest.
-            if (ng_bits > 0x00FFFFFFu && __popc(__activemask()) < postpone_min && st.push(make_uint2(tg_base, tg_bits))) {
-                tg_bits = 0;
-                break;
-            }
-            const uint32_t k = __ffs(tg_bits) - 1;
-            tg_bits &= tg_bits - 1;
-            tri_test<COUNT>(mr, r, tg_base + k, best, err, ntri);
-        }
-        if (ng_bits <= 0x00FFFFFFu) {
-            if (st.sp == 0) {
-                in_mesh = false;
-            } else {
-                const uint2 e = st.pop();
-                ng_base = e.x;
-                ng_bits = e.y;
-            }
         }
     }
     flush_counters<COUNT>(err, nvis, ntri, err_out, counters);
