@@ -291,22 +291,20 @@ __device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, B
         const float tfz = __fmaf_rn(byte_to_float(c < 4 ? fza : fzb, sel), A[2], Bf[2]);
         const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
         const float tmax = fminf(fminf(tfx, tfy), tfz);
-        if (meta != 0 && tmin <= tmax && tmin <= best.t && tmax >= 0.0f) {
-            const uint32_t bit = meta & 31u;
-            if (bit >= 24u) {
-                node_hits |= 1u << (bit ^ r.oct);
-                if (tmin < d1) {
-                    d2 = d1;
-                    d1 = tmin;
-                    c1 = c;
-                } else if (tmin < d2) {
-                    d2 = tmin;
-                }
-            } else {
-                tri_hits |= (meta >> 5) << bit;
-                dt = fminf(dt, tmin);
-            }
-        }
+        // branch-free bookkeeping (selects only): hit masks, the nearest
+        // internal child and the two least entry distances
+        const bool hit = meta != 0 && tmin <= tmax && tmin <= best.t && tmax >= 0.0f;
+        const uint32_t bit = meta & 31u;
+        const bool inner = hit && bit >= 24u;
+        const bool leaf = hit && bit < 24u;
+        node_hits |= inner ? (1u << (bit ^ r.oct)) : 0u;
+        tri_hits |= leaf ? ((meta >> 5) << bit) : 0u;
+        const float key = inner ? tmin : INFINITY;
+        const bool closer = key < d1;
+        d2 = closer ? d1 : fminf(d2, key);
+        c1 = closer ? c : c1;
+        d1 = closer ? key : d1;
+        dt = leaf ? fminf(dt, tmin) : dt;
     }
     const uint32_t imask = w0.w >> 24;
     if (c1 >= 0) {
