@@ -224,10 +224,14 @@ __device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, B
         return STEP_ERROR;
     }
     if (tv.ni == NO_NODE) {
-        if (st.sp == 0) return STEP_DONE;
+        // Drop groups that start beyond the closest hit within this step, so
+        // that a lane does not spend a whole warp step on each of them.
         float dist;
-        uint2 e = st.pop(dist);
-        if (dist > best.t) return STEP_CONTINUE;
+        uint2 e;
+        do {
+            if (st.sp == 0) return STEP_DONE;
+            e = st.pop(dist);
+        } while (dist > best.t);
         if (e.y <= 0x00FFFFFFu) { // a postponed triangle group
             tri_group<COUNT>(mr, r, e.x, e.y, best, err, ntri);
             return STEP_CONTINUE;
