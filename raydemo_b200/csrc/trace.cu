@@ -28,7 +28,6 @@ constexpr int SMEM_STACK = 16;  // entries per thread in shared memory
 constexpr int LMEM_STACK = 48;  // further entries in local memory (rarely used)
 constexpr int STACK_SIZE = SMEM_STACK + LMEM_STACK;
 constexpr uint32_t NO_RAY = 0xffffffffu;
-constexpr uint32_t NO_NODE = 0xffffffffu;
 
 __device__ __forceinline__ float byte_to_float(uint32_t word, uint32_t sel) {
     // 0x4B0000bb is 2^23 + bb as a float; subtracting 2^23 leaves bb exactly.
@@ -147,11 +146,19 @@ __device__ __forceinline__ MeshRef mesh_of(const SceneView &sv, const InstanceRe
     return mr;
 }
 
-// Traversal state of one ray in one mesh: the node to visit next (NO_NODE:
-// take a group from the stack) and the counters of the corruption guards.
+// Traversal state of one ray in one mesh: the current node group (base,
+// bits 24..31 = hit internal children in octant order, bits 0..7 = imask)
+// with the least entry distance of its members, and the counters of the
+// corruption guards.
 struct Trav {
-    uint32_t ni, visits, steps;
+    uint32_t ng_base, ng_bits;
+    float ng_dist;
+    uint32_t visits, steps;
 };
+
+__device__ __forceinline__ Trav trav_root(const LocalRay &r) {
+    return Trav{0u, (1u << (24 + r.oct)) | 1u, -INFINITY, 0u, 0u}; // the root as slot 0 of a virtual parent
+}
 
 enum { STEP_CONTINUE = 0, STEP_DONE = 1, STEP_ERROR = 2 };
 
@@ -201,31 +208,28 @@ __device__ __forceinline__ void tri_group(const MeshRef &mr, const LocalRay &r, 
     }
 }
 
-// One traversal step: visits one node (taking a group off the stack first
-// when there is no node to visit) and tests the triangles it hits. The
-// nearest internal child that the ray enters becomes the next node; the
-// other hit internal children are pushed as one node group (bits 24..31,
-// octant order, with the node's imask in bits 0..7) tagged with the least
-// entry distance among them, and a group whose tag exceeds the closest hit
-// when it comes off the stack is dropped: a triangle in it could only be hit
-// at a larger t. Triangle groups are tested at once, unless fewer than
-// postpone_min lanes of the warp have triangles while this lane has a node to
-// visit next: then the group is pushed (tagged the same way) and tested when
-// it comes off the stack.
+// One traversal step: visits one node and tests the triangles it hits.
+// Node groups are taken in octant order, which is roughly front to back; a
+// group, in registers or on the stack, carries the least entry distance of
+// its members and is dropped once that exceeds the closest hit so far (a
+// triangle in it could only be hit at a larger t). Triangle groups are tested
+// at once, unless fewer than postpone_min lanes of the warp have triangles
+// while this lane has nodes left: then the group is pushed (tagged the same
+// way) and tested when it comes off the stack.
 template <bool COUNT>
 __device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, Best &best, Stack &st, Trav &tv, int postpone_min,
                                          uint32_t &err, uint32_t &nvis, uint32_t &ntri) {
-    // Each node yields at most one node visit, one pushed node group (whose
-    // pops each visit a node or drop the group) and one triangle group, so a
-    // mesh takes fewer than 4 * node_count steps; more means a corrupt
-    // structure.
+    // Each node yields at most one node visit, one pushed group remainder and
+    // one triangle group, so a mesh takes fewer than 4 * node_count steps;
+    // more means a corrupt structure.
     if (++tv.steps > 4u * mr.node_count + 8u) {
         err |= TRACE_ERR_LIMIT;
         return STEP_ERROR;
     }
-    if (tv.ni == NO_NODE) {
-        // Drop groups that start beyond the closest hit within this step, so
-        // that a lane does not spend a whole warp step on each of them.
+    if (tv.ng_bits <= 0x00FFFFFFu || tv.ng_dist > best.t) {
+        // Next group from the stack; groups that start beyond the closest hit
+        // are dropped within this step, so that a lane does not spend a whole
+        // warp step on each of them.
         float dist;
         uint2 e;
         do {
@@ -233,16 +237,22 @@ __device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, B
             e = st.pop(dist);
         } while (dist > best.t);
         if (e.y <= 0x00FFFFFFu) { // a postponed triangle group
+            tv.ng_bits = 0;
             tri_group<COUNT>(mr, r, e.x, e.y, best, err, ntri);
             return STEP_CONTINUE;
         }
-        const uint32_t j = __ffs(e.y >> 24) - 1;
-        e.y &= ~(1u << (24 + j));
-        const uint32_t s = j ^ r.oct;
-        tv.ni = e.x + __popc((e.y & 0xFFu) & ((1u << s) - 1u));
-        if (e.y > 0x00FFFFFFu) st.push(e, dist); // fits: an entry was just taken
+        tv.ng_base = e.x;
+        tv.ng_bits = e.y;
+        tv.ng_dist = dist;
     }
-    const uint32_t ni = tv.ni;
+    const uint32_t j = __ffs(tv.ng_bits >> 24) - 1;
+    tv.ng_bits &= ~(1u << (24 + j));
+    const uint32_t s = j ^ r.oct;
+    const uint32_t ni = tv.ng_base + __popc((tv.ng_bits & 0xFFu) & ((1u << s) - 1u));
+    if (tv.ng_bits > 0x00FFFFFFu && !st.push(make_uint2(tv.ng_base, tv.ng_bits), tv.ng_dist)) {
+        err |= TRACE_ERR_STACK;
+        return STEP_ERROR;
+    }
     // A tree visits each node at most once; a bad index or a longer walk
     // means a corrupt structure: flag it and stop this ray.
     if (ni >= mr.node_count || ++tv.visits > mr.node_count) {
@@ -281,8 +291,7 @@ __device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, B
     const uint32_t nya = ny ? w4.x : w2.z, nyb = ny ? w4.y : w2.w, fya = ny ? w2.z : w4.x, fyb = ny ? w2.w : w4.y;
     const uint32_t nza = nz ? w4.z : w3.x, nzb = nz ? w4.w : w3.y, fza = nz ? w3.x : w4.z, fzb = nz ? w3.y : w4.w;
     uint32_t node_hits = 0, tri_hits = 0;
-    float d1 = INFINITY, d2 = INFINITY, dt = INFINITY;
-    int c1 = -1;
+    float dn = INFINITY, dt = INFINITY;
 #pragma unroll
     for (int c = 0; c < 8; c++) {
         const uint32_t meta = ((c < 4 ? w1.z : w1.w) >> (8 * (c & 3))) & 0xFFu;
@@ -295,34 +304,22 @@ __device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, B
         const float tfz = __fmaf_rn(byte_to_float(c < 4 ? fza : fzb, sel), A[2], Bf[2]);
         const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
         const float tmax = fminf(fminf(tfx, tfy), tfz);
-        // branch-free bookkeeping (selects only): hit masks, the nearest
-        // internal child and the two least entry distances
+        // branch-free bookkeeping (selects only): hit masks and the least
+        // entry distance of the hit internal and of the hit leaf children
         const bool hit = meta != 0 && tmin <= tmax && tmin <= best.t && tmax >= 0.0f;
         const uint32_t bit = meta & 31u;
         const bool inner = hit && bit >= 24u;
         const bool leaf = hit && bit < 24u;
         node_hits |= inner ? (1u << (bit ^ r.oct)) : 0u;
         tri_hits |= leaf ? ((meta >> 5) << bit) : 0u;
-        const float key = inner ? tmin : INFINITY;
-        const bool closer = key < d1;
-        d2 = closer ? d1 : fminf(d2, key);
-        c1 = closer ? c : c1;
-        d1 = closer ? key : d1;
-        dt = leaf ? fminf(dt, tmin) : dt;
+        dn = fminf(dn, inner ? tmin : INFINITY);
+        dt = fminf(dt, leaf ? tmin : INFINITY);
     }
-    const uint32_t imask = w0.w >> 24;
-    if (c1 >= 0) {
-        tv.ni = w1.x + __popc(imask & ((1u << c1) - 1u));
-        node_hits &= ~(1u << ((24u + (uint32_t)c1) ^ r.oct));
-    } else {
-        tv.ni = NO_NODE;
-    }
-    if (node_hits && !st.push(make_uint2(w1.x, node_hits | imask), d2)) {
-        err |= TRACE_ERR_STACK;
-        return STEP_ERROR;
-    }
+    tv.ng_base = w1.x;
+    tv.ng_bits = node_hits | (w0.w >> 24);
+    tv.ng_dist = dn;
     if (tri_hits) {
-        if (postpone_min > 0 && tv.ni != NO_NODE) {
+        if (postpone_min > 0 && node_hits) {
             const uint32_t with_tris = __popc(__ballot_sync(__activemask(), true));
             if ((int)with_tris < postpone_min && st.push(make_uint2(w1.y, tri_hits), dt)) return STEP_CONTINUE;
         }
@@ -378,7 +375,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
             if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
             const MeshRef mr = mesh_of(sv, ir, (int)m);
             const LocalRay r = transform_ray(ir, r0, r1);
-            Trav tv{0u, 0u, 0u};
+            Trav tv = trav_root(r);
             st.sp = 0;
             while (trav_step<COUNT>(mr, r, best, st, tv, 0, err, nvis, ntri) == STEP_CONTINUE) {
             }
@@ -416,7 +413,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
     best.prim = best.obj = -1;
     LocalRay r = make_local_ray(0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f);
     MeshRef mr{};
-    Trav tv{NO_NODE, 0u, 0u};
+    Trav tv = trav_root(r);
     while (true) {
         // ---- refill lanes that have no ray
         const uint32_t need = __ballot_sync(0xffffffffu, ri == NO_RAY);
@@ -456,7 +453,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
                 if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
                 mr = mesh_of(sv, ir, (int)mi - 1);
                 r = transform_ray(ir, r0, r1);
-                tv = Trav{0u, 0u, 0u};
+                tv = trav_root(r);
                 st.sp = 0;
                 in_mesh = true;
                 break;
