@@ -211,11 +211,10 @@ int ray_scene_last_trace_info(ray_scene *s, ray_trace_info *out);
 /* Traversal kernel choice for this scene (no counterpart in the reference,
  * which has one CPU loop): kernel 1 = one thread per ray, 2 = resident grid
  * whose lanes take new rays as theirs finish (refill once at least
- * refill_min lanes of a warp are idle) and postpone triangle tests while
- * fewer than postpone_min lanes of the warp have any (0 = never). Negative
- * values (and kernel 0) keep the current setting. */
+ * refill_min lanes of a warp are idle, 1..32). kernel 0 or refill_min <= 0
+ * keep the current setting. */
 typedef struct ray_trace_tuning {
-    int kernel, refill_min, postpone_min;
+    int kernel, refill_min;
 } ray_trace_tuning;
 int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t);
 int ray_scene_get_trace_tuning(ray_scene *s, ray_trace_tuning *out);

@@ -4,28 +4,26 @@
 // (bbox_test with safe_invert, CoreRef.cpp:64-86, 272-294) and TransformRay
 // (CoreRef.cpp:1605-1617), both reproduced operation for operation. Mesh
 // level: the compressed 8-wide BVH, traversed with node groups (a base index
-// plus a hit mask of up to 8 children) and triangle groups (a base index plus
-// a mask of up to 24 triangles) on a per-thread stack; children are visited
-// in octant order, which is roughly front to back. Triangles use the
-// reference's intersection arithmetic (CoreRef.cpp:11-42) with every product
-// and sum rounded on its own, so t, u, v are bit-exact; a tie on t goes to the
-// lower triangle index, which makes the result independent of visiting order.
+// plus a hit mask of up to 8 children, visited in octant order, which is
+// roughly front to back) on a per-thread stack. Triangles use the reference's
+// intersection arithmetic (CoreRef.cpp:11-42) with every product and sum
+// rounded on its own, so t, u, v are bit-exact; a tie on t goes to the lower
+// triangle index, which makes the result independent of visiting order.
 //
 // Two kernels share the traversal step:
 //   k_trace_closest     one thread per ray (a grid over the rays)
 //   k_trace_persistent  a resident grid; a lane whose ray is done takes the
-//                       next one from a global counter (warp-aggregated), and
-//                       a warp postpones triangle groups while few of its
-//                       lanes have any, so more lanes do useful work per
-//                       instruction on incoherent rays.
+//                       next one from a global counter (warp-aggregated), so
+//                       more lanes do useful work per instruction on
+//                       incoherent rays of very different lengths.
 #include "trace.cuh"
 
 namespace rg {
 namespace {
 
 constexpr int TRACE_BLOCK = 128;
-constexpr int SMEM_STACK = 16;  // entries per thread in shared memory
-constexpr int LMEM_STACK = 48;  // further entries in local memory (rarely used)
+constexpr int SMEM_STACK = 28; // entries per thread in shared memory (8 bytes each)
+constexpr int LMEM_STACK = 36; // further entries in a local array, touched only by deeper trees
 constexpr int STACK_SIZE = SMEM_STACK + LMEM_STACK;
 constexpr uint32_t NO_RAY = 0xffffffffu;
 
@@ -77,38 +75,16 @@ struct MeshRef {
     int obj;
 };
 
-// Two-tier per-thread stack of groups: the first SMEM_STACK entries in shared
-// memory (strided by the block size), the rest in local arrays. An entry is a
-// group (base, bits) plus a lower bound on the entry distance of everything
-// in it, so that a group starting beyond the closest hit so far is dropped.
-struct Stack {
-    uint2 *smem;
-    float *sdist;
-    uint2 lmem[LMEM_STACK];
-    float ldist[LMEM_STACK];
-    int sp;
-    __device__ __forceinline__ bool push(uint2 e, float d) {
-        if (sp >= STACK_SIZE) return false;
-        if (sp < SMEM_STACK) {
-            smem[sp * TRACE_BLOCK] = e;
-            sdist[sp * TRACE_BLOCK] = d;
-        } else {
-            lmem[sp - SMEM_STACK] = e;
-            ldist[sp - SMEM_STACK] = d;
-        }
-        sp++;
-        return true;
-    }
-    __device__ __forceinline__ uint2 pop(float &d) {
-        sp--;
-        if (sp < SMEM_STACK) {
-            d = sdist[sp * TRACE_BLOCK];
-            return smem[sp * TRACE_BLOCK];
-        }
-        d = ldist[sp - SMEM_STACK];
-        return lmem[sp - SMEM_STACK];
-    }
-};
+// Stack entry: a node group (x = base, y bits 24..31 = hit internal
+// children in octant order, bits 0..7 = the node's imask) and, in y bits
+// 8..23, the upper half of the float bits of the least entry distance among
+// its members. Dropping the low half rounds a non-negative distance down and
+// a negative one towards zero, so the stored value is a lower bound whenever
+// it can matter (a group is dropped only when it exceeds a positive t).
+__device__ __forceinline__ uint2 pack_group(uint32_t base, uint32_t bits, float dist) {
+    return make_uint2(base, (bits & 0xFF0000FFu) | ((__float_as_uint(dist) >> 16) << 8));
+}
+__device__ __forceinline__ float group_dist(uint2 e) { return __uint_as_float(((e.y >> 8) & 0xFFFFu) << 16); }
 
 __device__ __forceinline__ LocalRay make_local_ray(float ox, float oy, float oz, float dx, float dy, float dz) {
     LocalRay r;
@@ -144,20 +120,6 @@ __device__ __forceinline__ MeshRef mesh_of(const SceneView &sv, const InstanceRe
     mr.tri_count = __ldg(&ir->tri_count);
     mr.obj = m;
     return mr;
-}
-
-// Traversal state of one ray in one mesh: the current node group (base,
-// bits 24..31 = hit internal children in octant order, bits 0..7 = imask)
-// with the least entry distance of its members, and the counters of the
-// corruption guards.
-struct Trav {
-    uint32_t ng_base, ng_bits;
-    float ng_dist;
-    uint32_t visits, steps;
-};
-
-__device__ __forceinline__ Trav trav_root(const LocalRay &r) {
-    return Trav{0u, (1u << (24 + r.oct)) | 1u, -INFINITY, 0u, 0u}; // the root as slot 0 of a virtual parent
 }
 
 enum { STEP_CONTINUE = 0, STEP_DONE = 1, STEP_ERROR = 2 };
@@ -198,60 +160,64 @@ __device__ __forceinline__ void tri_test(const MeshRef &mr, const LocalRay &r, u
     }
 }
 
-template <bool COUNT>
-__device__ __forceinline__ void tri_group(const MeshRef &mr, const LocalRay &r, uint32_t base, uint32_t bits, Best &best, uint32_t &err,
-                                          uint32_t &ntri) {
-    while (bits) {
-        const uint32_t k = __ffs(bits) - 1;
-        bits &= bits - 1;
-        tri_test<COUNT>(mr, r, base + k, best, err, ntri);
-    }
+// Per-thread traversal state of one ray in one mesh. The stack's lower part
+// lives in shared memory (entry k of this thread at smem[k * TRACE_BLOCK]),
+// the rest in the caller's local array; sp and the current group stay in
+// registers.
+struct Trav {
+    uint32_t ng_base, ng_bits; // current node group
+    float ng_dist;             // least entry distance of its members
+    int sp;
+    uint32_t visits, steps;
+};
+
+__device__ __forceinline__ void trav_init(Trav &tv, const LocalRay &r) {
+    tv.ng_base = 0; // the root as slot 0 of a virtual parent
+    tv.ng_bits = (1u << (24 + r.oct)) | 1u;
+    tv.ng_dist = -INFINITY;
+    tv.sp = 0;
+    tv.visits = 0;
+    tv.steps = 0;
 }
 
-// One traversal step: visits one node and tests the triangles it hits.
-// Node groups are taken in octant order, which is roughly front to back; a
-// group, in registers or on the stack, carries the least entry distance of
-// its members and is dropped once that exceeds the closest hit so far (a
-// triangle in it could only be hit at a larger t). Triangle groups are tested
-// at once, unless fewer than postpone_min lanes of the warp have triangles
-// while this lane has nodes left: then the group is pushed (tagged the same
-// way) and tested when it comes off the stack.
+// One traversal step: visits one node and tests the triangles it hits. A
+// group, in registers or on the stack, is dropped once its least entry
+// distance exceeds the closest hit so far: a triangle in it could only be
+// hit at a larger t. Groups dropped on the way down the stack cost no extra
+// step, so that a lane does not spend a whole warp step on each of them.
 template <bool COUNT>
-__device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, Best &best, Stack &st, Trav &tv, int postpone_min,
+__device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, Best &best, uint2 *smem, uint2 *lmem, Trav &tv,
                                          uint32_t &err, uint32_t &nvis, uint32_t &ntri) {
-    // Each node yields at most one node visit, one pushed group remainder and
-    // one triangle group, so a mesh takes fewer than 4 * node_count steps;
-    // more means a corrupt structure.
-    if (++tv.steps > 4u * mr.node_count + 8u) {
+    // Each node yields at most one node visit and one pushed group, so a mesh
+    // takes fewer than 2 * node_count steps; more means a corrupt structure.
+    if (++tv.steps > 2u * mr.node_count + 8u) {
         err |= TRACE_ERR_LIMIT;
         return STEP_ERROR;
     }
     if (tv.ng_bits <= 0x00FFFFFFu || tv.ng_dist > best.t) {
-        // Next group from the stack; groups that start beyond the closest hit
-        // are dropped within this step, so that a lane does not spend a whole
-        // warp step on each of them.
-        float dist;
         uint2 e;
         do {
-            if (st.sp == 0) return STEP_DONE;
-            e = st.pop(dist);
-        } while (dist > best.t);
-        if (e.y <= 0x00FFFFFFu) { // a postponed triangle group
-            tv.ng_bits = 0;
-            tri_group<COUNT>(mr, r, e.x, e.y, best, err, ntri);
-            return STEP_CONTINUE;
-        }
+            if (tv.sp == 0) return STEP_DONE;
+            tv.sp--;
+            e = tv.sp < SMEM_STACK ? smem[tv.sp * TRACE_BLOCK] : lmem[tv.sp - SMEM_STACK];
+        } while (group_dist(e) > best.t);
         tv.ng_base = e.x;
-        tv.ng_bits = e.y;
-        tv.ng_dist = dist;
+        tv.ng_bits = e.y & 0xFF0000FFu;
+        tv.ng_dist = group_dist(e);
     }
     const uint32_t j = __ffs(tv.ng_bits >> 24) - 1;
     tv.ng_bits &= ~(1u << (24 + j));
     const uint32_t s = j ^ r.oct;
     const uint32_t ni = tv.ng_base + __popc((tv.ng_bits & 0xFFu) & ((1u << s) - 1u));
-    if (tv.ng_bits > 0x00FFFFFFu && !st.push(make_uint2(tv.ng_base, tv.ng_bits), tv.ng_dist)) {
-        err |= TRACE_ERR_STACK;
-        return STEP_ERROR;
+    if (tv.ng_bits > 0x00FFFFFFu) {
+        if (tv.sp >= STACK_SIZE) {
+            err |= TRACE_ERR_STACK;
+            return STEP_ERROR;
+        }
+        const uint2 e = pack_group(tv.ng_base, tv.ng_bits, tv.ng_dist);
+        if (tv.sp < SMEM_STACK) smem[tv.sp * TRACE_BLOCK] = e;
+        else lmem[tv.sp - SMEM_STACK] = e;
+        tv.sp++;
     }
     // A tree visits each node at most once; a bad index or a longer walk
     // means a corrupt structure: flag it and stop this ray.
@@ -290,8 +256,8 @@ __device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, B
     const uint32_t nxa = nx ? w3.z : w2.x, nxb = nx ? w3.w : w2.y, fxa = nx ? w2.x : w3.z, fxb = nx ? w2.y : w3.w;
     const uint32_t nya = ny ? w4.x : w2.z, nyb = ny ? w4.y : w2.w, fya = ny ? w2.z : w4.x, fyb = ny ? w2.w : w4.y;
     const uint32_t nza = nz ? w4.z : w3.x, nzb = nz ? w4.w : w3.y, fza = nz ? w3.x : w4.z, fzb = nz ? w3.y : w4.w;
-    uint32_t node_hits = 0, tri_hits = 0;
-    float dn = INFINITY, dt = INFINITY;
+    uint32_t hitmask = 0;
+    float dn = INFINITY;
 #pragma unroll
     for (int c = 0; c < 8; c++) {
         const uint32_t meta = ((c < 4 ? w1.z : w1.w) >> (8 * (c & 3))) & 0xFFu;
@@ -304,26 +270,22 @@ __device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, B
         const float tfz = __fmaf_rn(byte_to_float(c < 4 ? fza : fzb, sel), A[2], Bf[2]);
         const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
         const float tmax = fminf(fminf(tfx, tfy), tfz);
-        // branch-free bookkeeping (selects only): hit masks and the least
-        // entry distance of the hit internal and of the hit leaf children
         const bool hit = meta != 0 && tmin <= tmax && tmin <= best.t && tmax >= 0.0f;
-        const uint32_t bit = meta & 31u;
-        const bool inner = hit && bit >= 24u;
-        const bool leaf = hit && bit < 24u;
-        node_hits |= inner ? (1u << (bit ^ r.oct)) : 0u;
-        tri_hits |= leaf ? ((meta >> 5) << bit) : 0u;
-        dn = fminf(dn, inner ? tmin : INFINITY);
-        dt = fminf(dt, leaf ? tmin : INFINITY);
+        uint32_t bit = meta & 31u;
+        const bool inner = bit >= 24u;
+        bit = inner ? (bit ^ r.oct) : bit;
+        hitmask |= hit ? ((meta >> 5) << bit) : 0u;
+        dn = fminf(dn, (hit && inner) ? tmin : INFINITY);
     }
     tv.ng_base = w1.x;
-    tv.ng_bits = node_hits | (w0.w >> 24);
+    tv.ng_bits = (hitmask & 0xFF000000u) | (w0.w >> 24);
     tv.ng_dist = dn;
-    if (tri_hits) {
-        if (postpone_min > 0 && node_hits) {
-            const uint32_t with_tris = __popc(__ballot_sync(__activemask(), true));
-            if ((int)with_tris < postpone_min && st.push(make_uint2(w1.y, tri_hits), dt)) return STEP_CONTINUE;
-        }
-        tri_group<COUNT>(mr, r, w1.y, tri_hits, best, err, ntri);
+    uint32_t tbits = hitmask & 0x00FFFFFFu;
+    const uint32_t tbase = w1.y;
+    while (tbits) {
+        const uint32_t k = __ffs(tbits) - 1;
+        tbits &= tbits - 1;
+        tri_test<COUNT>(mr, r, tbase + k, best, err, ntri);
     }
     return STEP_CONTINUE;
 }
@@ -344,16 +306,24 @@ __device__ __forceinline__ void flush_counters(uint32_t err, uint32_t nvis, uint
     }
 }
 
+__device__ __forceinline__ bool enter_instance(const SceneView &sv, uint32_t m, float4 r0, float4 sinv, float best_t) {
+    const InstanceRec *ir = sv.inst + m;
+    float bmin[3], bmax[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        bmin[k] = __ldg(&ir->bbox_min[k]);
+        bmax[k] = __ldg(&ir->bbox_max[k]);
+    }
+    return ref_bbox_test(r0.x, r0.y, r0.z, sinv.x, sinv.y, sinv.z, best_t, bmin, bmax);
+}
+
 template <bool COUNT>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, const float4 *__restrict__ rays, uint32_t n, float4 *__restrict__ hits,
                                                                int32_t *__restrict__ obj_out, uint32_t *__restrict__ err_out,
                                                                unsigned long long *__restrict__ counters) {
     __shared__ uint2 s_stack[SMEM_STACK * TRACE_BLOCK];
-    __shared__ float s_dist[SMEM_STACK * TRACE_BLOCK];
-    Stack st;
-    st.smem = s_stack + threadIdx.x;
-    st.sdist = s_dist + threadIdx.x;
-    st.sp = 0;
+    uint2 l_stack[LMEM_STACK];
+    uint2 *smem = s_stack + threadIdx.x;
     const uint32_t i = blockIdx.x * TRACE_BLOCK + threadIdx.x;
     uint32_t err = 0, nvis = 0, ntri = 0;
     if (i < n) {
@@ -363,21 +333,15 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
         best.u = best.v = 0.0f;
         best.prim = -1;
         best.obj = -1;
-        const float sx = safe_inv(r1.x), sy = safe_inv(r1.y), sz = safe_inv(r1.z);
+        const float4 sinv = make_float4(safe_inv(r1.x), safe_inv(r1.y), safe_inv(r1.z), 0.0f);
         for (uint32_t m = 0; m < sv.n_inst; m++) {
+            if (!enter_instance(sv, m, r0, sinv, best.t)) continue;
             const InstanceRec *ir = sv.inst + m;
-            float bmin[3], bmax[3];
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                bmin[k] = __ldg(&ir->bbox_min[k]);
-                bmax[k] = __ldg(&ir->bbox_max[k]);
-            }
-            if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
             const MeshRef mr = mesh_of(sv, ir, (int)m);
             const LocalRay r = transform_ray(ir, r0, r1);
-            Trav tv = trav_root(r);
-            st.sp = 0;
-            while (trav_step<COUNT>(mr, r, best, st, tv, 0, err, nvis, ntri) == STEP_CONTINUE) {
+            Trav tv;
+            trav_init(tv, r);
+            while (trav_step<COUNT>(mr, r, best, smem, l_stack, tv, err, nvis, ntri) == STEP_CONTINUE) {
             }
         }
         hits[i] = make_float4(__int_as_float(best.prim), best.t, best.prim >= 0 ? best.u : 0.0f, best.prim >= 0 ? best.v : 0.0f);
@@ -388,20 +352,17 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
 
 // Persistent variant. Per lane: the ray it owns (index ri), the next instance
 // to try (mi) and, while a mesh is being traversed (in_mesh), the traversal
-// state. Each loop iteration of a warp: refill lanes without a ray when
-// enough of them are idle, advance lanes to their next instance (or finish
+// state. Each loop iteration of a warp: refill lanes without a ray when at
+// least refill_min are idle, advance lanes to their next instance (or finish
 // their ray), then one traversal step.
 template <bool COUNT>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, const float4 *__restrict__ rays, uint32_t n,
                                                                   float4 *__restrict__ hits, int32_t *__restrict__ obj_out,
                                                                   uint32_t *__restrict__ err_out, unsigned long long *__restrict__ counters,
-                                                                  uint32_t *__restrict__ next_ray, int refill_min, int postpone_min) {
+                                                                  uint32_t *__restrict__ next_ray, int refill_min) {
     __shared__ uint2 s_stack[SMEM_STACK * TRACE_BLOCK];
-    __shared__ float s_dist[SMEM_STACK * TRACE_BLOCK];
-    Stack st;
-    st.smem = s_stack + threadIdx.x;
-    st.sdist = s_dist + threadIdx.x;
-    st.sp = 0;
+    uint2 l_stack[LMEM_STACK];
+    uint2 *smem = s_stack + threadIdx.x;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lanemask_lt = (1u << lane) - 1u;
     uint32_t err = 0, nvis = 0, ntri = 0;
@@ -413,7 +374,8 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
     best.prim = best.obj = -1;
     LocalRay r = make_local_ray(0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f);
     MeshRef mr{};
-    Trav tv = trav_root(r);
+    Trav tv;
+    trav_init(tv, r);
     while (true) {
         // ---- refill lanes that have no ray
         const uint32_t need = __ballot_sync(0xffffffffu, ri == NO_RAY);
@@ -440,21 +402,14 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
         // ---- next instance whose box the ray enters, or the end of the ray
         if (!in_mesh) {
             const float4 r0 = __ldg(rays + 2ull * ri), r1 = __ldg(rays + 2ull * ri + 1);
-            const float sx = safe_inv(r1.x), sy = safe_inv(r1.y), sz = safe_inv(r1.z);
+            const float4 sinv = make_float4(safe_inv(r1.x), safe_inv(r1.y), safe_inv(r1.z), 0.0f);
             while (mi < sv.n_inst) {
-                const InstanceRec *ir = sv.inst + mi;
-                float bmin[3], bmax[3];
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    bmin[k] = __ldg(&ir->bbox_min[k]);
-                    bmax[k] = __ldg(&ir->bbox_max[k]);
-                }
-                mi++;
-                if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
-                mr = mesh_of(sv, ir, (int)mi - 1);
+                const uint32_t m = mi++;
+                if (!enter_instance(sv, m, r0, sinv, best.t)) continue;
+                const InstanceRec *ir = sv.inst + m;
+                mr = mesh_of(sv, ir, (int)m);
                 r = transform_ray(ir, r0, r1);
-                tv = trav_root(r);
-                st.sp = 0;
+                trav_init(tv, r);
                 in_mesh = true;
                 break;
             }
@@ -466,7 +421,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
             }
         }
         // ---- one traversal step
-        const int res = trav_step<COUNT>(mr, r, best, st, tv, postpone_min, err, nvis, ntri);
+        const int res = trav_step<COUNT>(mr, r, best, smem, l_stack, tv, err, nvis, ntri);
         if (res == STEP_DONE) {
             in_mesh = false;
         } else if (res == STEP_ERROR) {
@@ -505,11 +460,9 @@ cudaError_t launch_trace_closest(const SceneView &sv, const float4 *rays, uint32
     if (e != cudaSuccess) return e;
     const uint32_t grid = (uint32_t)g_persistent_blocks;
     if (count)
-        k_trace_persistent<true><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min,
-                                                               tp.postpone_min);
+        k_trace_persistent<true><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min);
     else
-        k_trace_persistent<false><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min,
-                                                                tp.postpone_min);
+        k_trace_persistent<false><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min);
     return cudaGetLastError();
 }
 

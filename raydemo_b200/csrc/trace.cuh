@@ -22,7 +22,6 @@ constexpr uint32_t TRACE_ERR_LIMIT = 4u;  // more node visits than the mesh has 
 struct TraceParams {
     bool persistent = true; // resident grid with per-lane ray refill
     int refill_min = 8;     // refill a warp's idle lanes once at least this many are idle
-    int postpone_min = 0;   // postpone triangle groups while fewer lanes than this test triangles
     uint32_t *next_ray = nullptr; // device work counter for the persistent kernel
 };
 
