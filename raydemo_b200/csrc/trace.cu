@@ -180,11 +180,14 @@ __device__ __forceinline__ void trav_init(Trav &tv, const LocalRay &r) {
     tv.steps = 0;
 }
 
-// One traversal step: visits one node and tests the triangles it hits. A
-// group, in registers or on the stack, is dropped once its least entry
-// distance exceeds the closest hit so far: a triangle in it could only be
-// hit at a larger t. Groups dropped on the way down the stack cost no extra
-// step, so that a lane does not spend a whole warp step on each of them.
+// One traversal step: takes the next child of the current node group (which
+// always has one on entry), visits it, tests the triangles it hits, and then
+// makes sure that a node group is ready for the next step, taking one from
+// the stack if needed (STEP_DONE when there is none left). A group, in
+// registers or on the stack, is dropped once its least entry distance
+// exceeds the closest hit so far: a triangle in it could only be hit at a
+// larger t. The stack work comes last so that the node visit at the start of
+// every step runs on all lanes of a warp together.
 template <bool COUNT>
 __device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, Best &best, uint2 *smem, uint2 *lmem, Trav &tv,
                                          uint32_t &err, uint32_t &nvis, uint32_t &ntri) {
@@ -193,17 +196,6 @@ __device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, B
     if (++tv.steps > 2u * mr.node_count + 8u) {
         err |= TRACE_ERR_LIMIT;
         return STEP_ERROR;
-    }
-    if (tv.ng_bits <= 0x00FFFFFFu || tv.ng_dist > best.t) {
-        uint2 e;
-        do {
-            if (tv.sp == 0) return STEP_DONE;
-            tv.sp--;
-            e = tv.sp < SMEM_STACK ? smem[tv.sp * TRACE_BLOCK] : lmem[tv.sp - SMEM_STACK];
-        } while (group_dist(e) > best.t);
-        tv.ng_base = e.x;
-        tv.ng_bits = e.y & 0xFF0000FFu;
-        tv.ng_dist = group_dist(e);
     }
     const uint32_t j = __ffs(tv.ng_bits >> 24) - 1;
     tv.ng_bits &= ~(1u << (24 + j));
@@ -287,7 +279,17 @@ __device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, B
         tbits &= tbits - 1;
         tri_test<COUNT>(mr, r, tbase + k, best, err, ntri);
     }
-    return STEP_CONTINUE;
+    // ---- a node group for the next step
+    bool ready = tv.ng_bits > 0x00FFFFFFu && tv.ng_dist <= best.t;
+    while (!ready && tv.sp > 0) {
+        tv.sp--;
+        const uint2 e = tv.sp < SMEM_STACK ? smem[tv.sp * TRACE_BLOCK] : lmem[tv.sp - SMEM_STACK];
+        tv.ng_base = e.x;
+        tv.ng_bits = e.y & 0xFF0000FFu;
+        tv.ng_dist = group_dist(e);
+        ready = tv.ng_dist <= best.t;
+    }
+    return ready ? STEP_CONTINUE : STEP_DONE;
 }
 
 template <bool COUNT>
