@@ -212,9 +212,11 @@ int ray_scene_last_trace_info(ray_scene *s, ray_trace_info *out);
  * which has one CPU loop): kernel 1 = one thread per ray, 2 = resident grid
  * whose lanes take new rays as theirs finish (refill once at least
  * refill_min lanes of a warp are idle, 1..32). kernel 0 or refill_min <= 0
- * keep the current setting. */
+ * keep the current setting. deep_stack: 0 = size the traversal stack by the
+ * BVH depth (shared memory only unless a tree is deeper than it holds),
+ * 1 = always continue it in local memory. */
 typedef struct ray_trace_tuning {
-    int kernel, refill_min;
+    int kernel, refill_min, deep_stack;
 } ray_trace_tuning;
 int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t);
 int ray_scene_get_trace_tuning(ray_scene *s, ray_trace_tuning *out);

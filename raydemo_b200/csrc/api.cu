@@ -708,8 +708,10 @@ int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t) {
     RG_CHECK(s && t, "null argument");
     RG_CHECK(t->kernel >= 0 && t->kernel <= 2, "kernel must be 1 (per ray) or 2 (persistent)");
     RG_CHECK(t->refill_min <= 32, "refill_min is a lane count, at most 32");
+    RG_CHECK(t->deep_stack == 0 || t->deep_stack == 1, "deep_stack is 0 or 1");
     if (t->kernel > 0) s->tuning.kernel = t->kernel;
     if (t->refill_min > 0) s->tuning.refill_min = t->refill_min;
+    s->tuning.deep_stack = t->deep_stack;
     return RAY_OK;
 }
 
@@ -775,6 +777,8 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
     TraceParams tp;
     tp.persistent = s->tuning.kernel == 2;
     tp.refill_min = s->tuning.refill_min;
+    for (const MeshRec &m : s->meshes) tp.max_depth = std::max(tp.max_depth, m.bvh.depth);
+    if (s->tuning.deep_stack) tp.max_depth = 0xffffffffu;
     tp.next_ray = static_cast<uint32_t *>(s->d_next_ray.p);
     RG_CUDA_TRY(launch_trace_closest(sv, d_rays, (uint32_t)n, d_hits, d_obj, static_cast<uint32_t *>(s->d_err.p),
                                      static_cast<unsigned long long *>(s->d_counters.p), s->counting, st, tp));

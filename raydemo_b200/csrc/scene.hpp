@@ -105,7 +105,7 @@ struct ray_scene {
 
     // batch-trace staging and diagnostics
     rg::DeviceBuf d_rays, d_hits, d_obj, d_err, d_counters, d_next_ray;
-    ray_trace_tuning tuning{2, 8};
+    ray_trace_tuning tuning{2, 8, 0};
     bool counting = false;
     ray_trace_info last_info{};
     bool info_pending = false;

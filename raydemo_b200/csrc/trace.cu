@@ -4,11 +4,12 @@
 // (bbox_test with safe_invert, CoreRef.cpp:64-86, 272-294) and TransformRay
 // (CoreRef.cpp:1605-1617), both reproduced operation for operation. Mesh
 // level: the compressed 8-wide BVH, traversed with node groups (a base index
-// plus a hit mask of up to 8 children, visited in octant order, which is
-// roughly front to back) on a per-thread stack. Triangles use the reference's
-// intersection arithmetic (CoreRef.cpp:11-42) with every product and sum
-// rounded on its own, so t, u, v are bit-exact; a tie on t goes to the lower
-// triangle index, which makes the result independent of visiting order.
+// plus a hit mask of up to 8 children) on a per-thread stack, children in
+// octant order, which is roughly front to back; the triangles of the leaf
+// children a node step hits (up to 24) are tested at once. Triangles use the
+// reference's intersection arithmetic (CoreRef.cpp:11-42) with every product
+// and sum rounded on its own, so t, u, v are bit-exact; a tie on t goes to the
+// lower triangle index, which makes the result independent of visiting order.
 //
 // Two kernels share the traversal step:
 //   k_trace_closest     one thread per ray (a grid over the rays)
@@ -16,15 +17,17 @@
 //                       next one from a global counter (warp-aggregated), so
 //                       more lanes do useful work per instruction on
 //                       incoherent rays of very different lengths.
+// The stack holds one node group per tree level at most. It lives in shared
+// memory; meshes deeper than that use the DEEP instances, which continue it
+// in a local array.
 #include "trace.cuh"
 
 namespace rg {
 namespace {
 
 constexpr int TRACE_BLOCK = 128;
-constexpr int SMEM_STACK = 28; // entries per thread in shared memory (8 bytes each)
-constexpr int LMEM_STACK = 36; // further entries in a local array, touched only by deeper trees
-constexpr int STACK_SIZE = SMEM_STACK + LMEM_STACK;
+constexpr int SMEM_STACK = 24; // entries per thread in shared memory
+constexpr int LMEM_STACK = 40; // further entries in a local array (DEEP instances only)
 constexpr uint32_t NO_RAY = 0xffffffffu;
 
 __device__ __forceinline__ float byte_to_float(uint32_t word, uint32_t sel) {
@@ -75,16 +78,44 @@ struct MeshRef {
     int obj;
 };
 
-// Stack entry: a node group (x = base, y bits 24..31 = hit internal
-// children in octant order, bits 0..7 = the node's imask) and, in y bits
-// 8..23, the upper half of the float bits of the least entry distance among
-// its members. Dropping the low half rounds a non-negative distance down and
-// a negative one towards zero, so the stored value is a lower bound whenever
-// it can matter (a group is dropped only when it exceeds a positive t).
-__device__ __forceinline__ uint2 pack_group(uint32_t base, uint32_t bits, float dist) {
-    return make_uint2(base, (bits & 0xFF0000FFu) | ((__float_as_uint(dist) >> 16) << 8));
-}
-__device__ __forceinline__ float group_dist(uint2 e) { return __uint_as_float(((e.y >> 8) & 0xFFFFu) << 16); }
+// Per-thread stack of node groups: entry k of this thread at
+// smem[k * TRACE_BLOCK]; the DEEP variant continues in a local array.
+template <bool DEEP>
+struct Stack;
+
+template <>
+struct Stack<false> {
+    uint2 *smem;
+    int sp;
+    __device__ __forceinline__ bool push(uint2 e) {
+        if (sp >= SMEM_STACK) return false;
+        smem[sp * TRACE_BLOCK] = e;
+        sp++;
+        return true;
+    }
+    __device__ __forceinline__ uint2 pop() {
+        sp--;
+        return smem[sp * TRACE_BLOCK];
+    }
+};
+
+template <>
+struct Stack<true> {
+    uint2 *smem;
+    uint2 lmem[LMEM_STACK];
+    int sp;
+    __device__ __forceinline__ bool push(uint2 e) {
+        if (sp >= SMEM_STACK + LMEM_STACK) return false;
+        if (sp < SMEM_STACK) smem[sp * TRACE_BLOCK] = e;
+        else lmem[sp - SMEM_STACK] = e;
+        sp++;
+        return true;
+    }
+    __device__ __forceinline__ uint2 pop() {
+        sp--;
+        return sp < SMEM_STACK ? smem[sp * TRACE_BLOCK] : lmem[sp - SMEM_STACK];
+    }
+};
 
 __device__ __forceinline__ LocalRay make_local_ray(float ox, float oy, float oz, float dx, float dy, float dz) {
     LocalRay r;
@@ -122,7 +153,84 @@ __device__ __forceinline__ MeshRef mesh_of(const SceneView &sv, const InstanceRe
     return mr;
 }
 
-enum { STEP_CONTINUE = 0, STEP_DONE = 1, STEP_ERROR = 2 };
+// Node step: takes the next child of node group (ng_base, ng_bits), tests
+// its 8 children and returns their hits as a node group (internal children,
+// bits 24..31, with the node's imask in bits 0..7) and a triangle group
+// (bits 0..23). Returns false (and sets err) on a corrupt index.
+template <bool COUNT, bool DEEP>
+__device__ __forceinline__ bool node_step(const MeshRef &mr, const LocalRay &r, float best_t, uint32_t &ng_base, uint32_t &ng_bits,
+                                          uint32_t &tg_base, uint32_t &tg_bits, Stack<DEEP> &st, uint32_t &visits, uint32_t &err,
+                                          uint32_t &nvis) {
+    const uint32_t j = __ffs(ng_bits >> 24) - 1;
+    ng_bits &= ~(1u << (24 + j));
+    const uint32_t s = j ^ r.oct;
+    const uint32_t ni = ng_base + __popc((ng_bits & 0xFFu) & ((1u << s) - 1u));
+    if (ng_bits > 0x00FFFFFFu && !st.push(make_uint2(ng_base, ng_bits))) {
+        err |= TRACE_ERR_STACK;
+        return false;
+    }
+    // A tree visits each node at most once; a bad index or a longer walk
+    // means a corrupt structure: flag it and stop this ray.
+    if (ni >= mr.node_count || ++visits > mr.node_count) {
+        err |= (ni >= mr.node_count) ? TRACE_ERR_BOUNDS : TRACE_ERR_LIMIT;
+        return false;
+    }
+    const uint4 *np = reinterpret_cast<const uint4 *>(mr.nodes + ni);
+    const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+    if (COUNT) nvis++;
+    const uint32_t imask = w0.w >> 24;
+    // Slab parameter of plane q on one axis: t(q) = q * A + B with
+    // A = 2^e * inv_d (exact: a power-of-two scaling) and B = (p - o) * inv_d,
+    // one FMA per plane. Its rounding error is below 2u(|B| + 256|A|)
+    // (u = 2^-24); the slack 2^-21 (|B| + 256|A|) moves the near planes
+    // down and the far planes up by more than that, so the test accepts
+    // every box that the exact slab test on the decoded box accepts.
+    float A[3], Bn[3], Bf[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float p = __uint_as_float(a == 0 ? w0.x : (a == 1 ? w0.y : w0.z));
+        const float sc = __uint_as_float(((w0.w >> (8 * a)) & 0xFFu) << 23);
+        const float inv = a == 0 ? r.ix : (a == 1 ? r.iy : r.iz);
+        const float o = a == 0 ? r.ox : (a == 1 ? r.oy : r.oz);
+        A[a] = __fmul_rn(sc, inv);
+        const float B = __fmul_rn(__fsub_rn(p, o), inv);
+        const float slack = __fmul_rn(__fmaf_rn(fabsf(A[a]), 256.0f, fabsf(B)), 4.76837158203125e-07f);
+        Bn[a] = __fsub_rn(B, slack);
+        Bf[a] = __fadd_rn(B, slack);
+    }
+    // Near/far plane words by direction sign, so that a NaN slab value
+    // (origin on a plane of a box the ray runs parallel to) leaves that axis
+    // unbounded, which keeps the test conservative. Planes: lo x = w2.xy,
+    // lo y = w2.zw, lo z = w3.xy, hi x = w3.zw, hi y = w4.xy, hi z = w4.zw.
+    const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
+    const uint32_t nxa = nx ? w3.z : w2.x, nxb = nx ? w3.w : w2.y, fxa = nx ? w2.x : w3.z, fxb = nx ? w2.y : w3.w;
+    const uint32_t nya = ny ? w4.x : w2.z, nyb = ny ? w4.y : w2.w, fya = ny ? w2.z : w4.x, fyb = ny ? w2.w : w4.y;
+    const uint32_t nza = nz ? w4.z : w3.x, nzb = nz ? w4.w : w3.y, fza = nz ? w3.x : w4.z, fzb = nz ? w3.y : w4.w;
+    uint32_t hitmask = 0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        const uint32_t meta = ((c < 4 ? w1.z : w1.w) >> (8 * (c & 3))) & 0xFFu;
+        const uint32_t sel = 0x7540u | (uint32_t)(c & 3);
+        const float tnx = __fmaf_rn(byte_to_float(c < 4 ? nxa : nxb, sel), A[0], Bn[0]);
+        const float tfx = __fmaf_rn(byte_to_float(c < 4 ? fxa : fxb, sel), A[0], Bf[0]);
+        const float tny = __fmaf_rn(byte_to_float(c < 4 ? nya : nyb, sel), A[1], Bn[1]);
+        const float tfy = __fmaf_rn(byte_to_float(c < 4 ? fya : fyb, sel), A[1], Bf[1]);
+        const float tnz = __fmaf_rn(byte_to_float(c < 4 ? nza : nzb, sel), A[2], Bn[2]);
+        const float tfz = __fmaf_rn(byte_to_float(c < 4 ? fza : fzb, sel), A[2], Bf[2]);
+        const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
+        const float tmax = fminf(fminf(tfx, tfy), tfz);
+        if (meta != 0 && tmin <= tmax && tmin <= best_t && tmax >= 0.0f) {
+            uint32_t bit = meta & 31u;
+            if (bit >= 24u) bit ^= r.oct;
+            hitmask |= (meta >> 5) << bit;
+        }
+    }
+    ng_base = w1.x;
+    ng_bits = (hitmask & 0xFF000000u) | imask;
+    tg_base = w1.y;
+    tg_bits = hitmask & 0x00FFFFFFu;
+    return true;
+}
 
 // One triangle test; updates best when it is the closer hit.
 template <bool COUNT>
@@ -160,136 +268,29 @@ __device__ __forceinline__ void tri_test(const MeshRef &mr, const LocalRay &r, u
     }
 }
 
-// Per-thread traversal state of one ray in one mesh. The stack's lower part
-// lives in shared memory (entry k of this thread at smem[k * TRACE_BLOCK]),
-// the rest in the caller's local array; sp and the current group stay in
-// registers.
-struct Trav {
-    uint32_t ng_base, ng_bits; // current node group
-    float ng_dist;             // least entry distance of its members
-    int sp;
-    uint32_t visits, steps;
-};
-
-__device__ __forceinline__ void trav_init(Trav &tv, const LocalRay &r) {
-    tv.ng_base = 0; // the root as slot 0 of a virtual parent
-    tv.ng_bits = (1u << (24 + r.oct)) | 1u;
-    tv.ng_dist = -INFINITY;
-    tv.sp = 0;
-    tv.visits = 0;
-    tv.steps = 0;
-}
-
-// One traversal step: takes the next child of the current node group (which
-// always has one on entry), visits it, tests the triangles it hits, and then
-// makes sure that a node group is ready for the next step, taking one from
-// the stack if needed (STEP_DONE when there is none left). A group, in
-// registers or on the stack, is dropped once its least entry distance
-// exceeds the closest hit so far: a triangle in it could only be hit at a
-// larger t. The stack work comes last so that the node visit at the start of
-// every step runs on all lanes of a warp together.
-template <bool COUNT>
-__device__ __forceinline__ int trav_step(const MeshRef &mr, const LocalRay &r, Best &best, uint2 *smem, uint2 *lmem, Trav &tv,
-                                         uint32_t &err, uint32_t &nvis, uint32_t &ntri) {
-    // Each node yields at most one node visit and one pushed group, so a mesh
-    // takes fewer than 2 * node_count steps; more means a corrupt structure.
-    if (++tv.steps > 2u * mr.node_count + 8u) {
-        err |= TRACE_ERR_LIMIT;
-        return STEP_ERROR;
-    }
-    const uint32_t j = __ffs(tv.ng_bits >> 24) - 1;
-    tv.ng_bits &= ~(1u << (24 + j));
-    const uint32_t s = j ^ r.oct;
-    const uint32_t ni = tv.ng_base + __popc((tv.ng_bits & 0xFFu) & ((1u << s) - 1u));
-    if (tv.ng_bits > 0x00FFFFFFu) {
-        if (tv.sp >= STACK_SIZE) {
-            err |= TRACE_ERR_STACK;
-            return STEP_ERROR;
+// Whole traversal of one mesh for one ray (the one-thread-per-ray kernel).
+// The current node group always has a child left at the top of the loop: the
+// root's, then the group a node step returns or one taken from the stack.
+template <bool COUNT, bool DEEP>
+__device__ __forceinline__ void trace_mesh(const MeshRef &mr, const LocalRay &r, Best &best, Stack<DEEP> &st, uint32_t &err,
+                                           uint32_t &nvis, uint32_t &ntri) {
+    uint32_t ng_base = 0, ng_bits = (1u << (24 + r.oct)) | 1u; // the root as slot 0 of a virtual parent
+    uint32_t tg_base = 0, tg_bits = 0, visits = 0;
+    st.sp = 0;
+    while (true) {
+        if (!node_step<COUNT>(mr, r, best.t, ng_base, ng_bits, tg_base, tg_bits, st, visits, err, nvis)) return;
+        while (tg_bits) {
+            const uint32_t k = __ffs(tg_bits) - 1;
+            tg_bits &= tg_bits - 1;
+            tri_test<COUNT>(mr, r, tg_base + k, best, err, ntri);
         }
-        const uint2 e = pack_group(tv.ng_base, tv.ng_bits, tv.ng_dist);
-        if (tv.sp < SMEM_STACK) smem[tv.sp * TRACE_BLOCK] = e;
-        else lmem[tv.sp - SMEM_STACK] = e;
-        tv.sp++;
+        if (ng_bits <= 0x00FFFFFFu) {
+            if (st.sp == 0) return;
+            const uint2 e = st.pop();
+            ng_base = e.x;
+            ng_bits = e.y;
+        }
     }
-    // A tree visits each node at most once; a bad index or a longer walk
-    // means a corrupt structure: flag it and stop this ray.
-    if (ni >= mr.node_count || ++tv.visits > mr.node_count) {
-        err |= (ni >= mr.node_count) ? TRACE_ERR_BOUNDS : TRACE_ERR_LIMIT;
-        return STEP_ERROR;
-    }
-    const uint4 *np = reinterpret_cast<const uint4 *>(mr.nodes + ni);
-    const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
-    if (COUNT) nvis++;
-    // Slab parameter of plane q on one axis: t(q) = q * A + B with
-    // A = 2^e * inv_d (exact: a power-of-two scaling) and B = (p - o) * inv_d,
-    // one FMA per plane. Its rounding error is below 2u(|B| + 256|A|)
-    // (u = 2^-24); the slack 2^-21 (|B| + 256|A|) moves the near planes
-    // down and the far planes up by more than that, so the test accepts
-    // every box that the exact slab test on the decoded box accepts, and the
-    // near distance it gives is a lower bound of the exact one.
-    float A[3], Bn[3], Bf[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        const float p = __uint_as_float(a == 0 ? w0.x : (a == 1 ? w0.y : w0.z));
-        const float sc = __uint_as_float(((w0.w >> (8 * a)) & 0xFFu) << 23);
-        const float inv = a == 0 ? r.ix : (a == 1 ? r.iy : r.iz);
-        const float o = a == 0 ? r.ox : (a == 1 ? r.oy : r.oz);
-        A[a] = __fmul_rn(sc, inv);
-        const float B = __fmul_rn(__fsub_rn(p, o), inv);
-        const float slack = __fmul_rn(__fmaf_rn(fabsf(A[a]), 256.0f, fabsf(B)), 4.76837158203125e-07f);
-        Bn[a] = __fsub_rn(B, slack);
-        Bf[a] = __fadd_rn(B, slack);
-    }
-    // Near/far plane words by direction sign, so that a NaN slab value
-    // (origin on a plane of a box the ray runs parallel to) leaves that axis
-    // unbounded, which keeps the test conservative. Planes: lo x = w2.xy,
-    // lo y = w2.zw, lo z = w3.xy, hi x = w3.zw, hi y = w4.xy, hi z = w4.zw.
-    const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
-    const uint32_t nxa = nx ? w3.z : w2.x, nxb = nx ? w3.w : w2.y, fxa = nx ? w2.x : w3.z, fxb = nx ? w2.y : w3.w;
-    const uint32_t nya = ny ? w4.x : w2.z, nyb = ny ? w4.y : w2.w, fya = ny ? w2.z : w4.x, fyb = ny ? w2.w : w4.y;
-    const uint32_t nza = nz ? w4.z : w3.x, nzb = nz ? w4.w : w3.y, fza = nz ? w3.x : w4.z, fzb = nz ? w3.y : w4.w;
-    uint32_t hitmask = 0;
-    float dn = INFINITY;
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
-        const uint32_t meta = ((c < 4 ? w1.z : w1.w) >> (8 * (c & 3))) & 0xFFu;
-        const uint32_t sel = 0x7540u | (uint32_t)(c & 3);
-        const float tnx = __fmaf_rn(byte_to_float(c < 4 ? nxa : nxb, sel), A[0], Bn[0]);
-        const float tfx = __fmaf_rn(byte_to_float(c < 4 ? fxa : fxb, sel), A[0], Bf[0]);
-        const float tny = __fmaf_rn(byte_to_float(c < 4 ? nya : nyb, sel), A[1], Bn[1]);
-        const float tfy = __fmaf_rn(byte_to_float(c < 4 ? fya : fyb, sel), A[1], Bf[1]);
-        const float tnz = __fmaf_rn(byte_to_float(c < 4 ? nza : nzb, sel), A[2], Bn[2]);
-        const float tfz = __fmaf_rn(byte_to_float(c < 4 ? fza : fzb, sel), A[2], Bf[2]);
-        const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
-        const float tmax = fminf(fminf(tfx, tfy), tfz);
-        const bool hit = meta != 0 && tmin <= tmax && tmin <= best.t && tmax >= 0.0f;
-        uint32_t bit = meta & 31u;
-        const bool inner = bit >= 24u;
-        bit = inner ? (bit ^ r.oct) : bit;
-        hitmask |= hit ? ((meta >> 5) << bit) : 0u;
-        dn = fminf(dn, (hit && inner) ? tmin : INFINITY);
-    }
-    tv.ng_base = w1.x;
-    tv.ng_bits = (hitmask & 0xFF000000u) | (w0.w >> 24);
-    tv.ng_dist = dn;
-    uint32_t tbits = hitmask & 0x00FFFFFFu;
-    const uint32_t tbase = w1.y;
-    while (tbits) {
-        const uint32_t k = __ffs(tbits) - 1;
-        tbits &= tbits - 1;
-        tri_test<COUNT>(mr, r, tbase + k, best, err, ntri);
-    }
-    // ---- a node group for the next step
-    bool ready = tv.ng_bits > 0x00FFFFFFu && tv.ng_dist <= best.t;
-    while (!ready && tv.sp > 0) {
-        tv.sp--;
-        const uint2 e = tv.sp < SMEM_STACK ? smem[tv.sp * TRACE_BLOCK] : lmem[tv.sp - SMEM_STACK];
-        tv.ng_base = e.x;
-        tv.ng_bits = e.y & 0xFF0000FFu;
-        tv.ng_dist = group_dist(e);
-        ready = tv.ng_dist <= best.t;
-    }
-    return ready ? STEP_CONTINUE : STEP_DONE;
 }
 
 template <bool COUNT>
@@ -308,24 +309,14 @@ __device__ __forceinline__ void flush_counters(uint32_t err, uint32_t nvis, uint
     }
 }
 
-__device__ __forceinline__ bool enter_instance(const SceneView &sv, uint32_t m, float4 r0, float4 sinv, float best_t) {
-    const InstanceRec *ir = sv.inst + m;
-    float bmin[3], bmax[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        bmin[k] = __ldg(&ir->bbox_min[k]);
-        bmax[k] = __ldg(&ir->bbox_max[k]);
-    }
-    return ref_bbox_test(r0.x, r0.y, r0.z, sinv.x, sinv.y, sinv.z, best_t, bmin, bmax);
-}
-
-template <bool COUNT>
+template <bool COUNT, bool DEEP>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, const float4 *__restrict__ rays, uint32_t n, float4 *__restrict__ hits,
                                                                int32_t *__restrict__ obj_out, uint32_t *__restrict__ err_out,
                                                                unsigned long long *__restrict__ counters) {
     __shared__ uint2 s_stack[SMEM_STACK * TRACE_BLOCK];
-    uint2 l_stack[LMEM_STACK];
-    uint2 *smem = s_stack + threadIdx.x;
+    Stack<DEEP> st;
+    st.smem = s_stack + threadIdx.x;
+    st.sp = 0;
     const uint32_t i = blockIdx.x * TRACE_BLOCK + threadIdx.x;
     uint32_t err = 0, nvis = 0, ntri = 0;
     if (i < n) {
@@ -335,16 +326,17 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
         best.u = best.v = 0.0f;
         best.prim = -1;
         best.obj = -1;
-        const float4 sinv = make_float4(safe_inv(r1.x), safe_inv(r1.y), safe_inv(r1.z), 0.0f);
+        const float sx = safe_inv(r1.x), sy = safe_inv(r1.y), sz = safe_inv(r1.z);
         for (uint32_t m = 0; m < sv.n_inst; m++) {
-            if (!enter_instance(sv, m, r0, sinv, best.t)) continue;
             const InstanceRec *ir = sv.inst + m;
-            const MeshRef mr = mesh_of(sv, ir, (int)m);
-            const LocalRay r = transform_ray(ir, r0, r1);
-            Trav tv;
-            trav_init(tv, r);
-            while (trav_step<COUNT>(mr, r, best, smem, l_stack, tv, err, nvis, ntri) == STEP_CONTINUE) {
+            float bmin[3], bmax[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                bmin[k] = __ldg(&ir->bbox_min[k]);
+                bmax[k] = __ldg(&ir->bbox_max[k]);
             }
+            if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
+            trace_mesh<COUNT, DEEP>(mesh_of(sv, ir, (int)m), transform_ray(ir, r0, r1), best, st, err, nvis, ntri);
         }
         hits[i] = make_float4(__int_as_float(best.prim), best.t, best.prim >= 0 ? best.u : 0.0f, best.prim >= 0 ? best.v : 0.0f);
         if (obj_out) obj_out[i] = best.obj;
@@ -354,21 +346,22 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
 
 // Persistent variant. Per lane: the ray it owns (index ri), the next instance
 // to try (mi) and, while a mesh is being traversed (in_mesh), the traversal
-// state. Each loop iteration of a warp: refill lanes without a ray when at
-// least refill_min are idle, advance lanes to their next instance (or finish
-// their ray), then one traversal step.
-template <bool COUNT>
+// state. Each loop iteration of a warp: refill lanes without a ray when
+// enough of them are idle, advance lanes to their next instance (or finish
+// their ray), then one node step plus the triangles it hit.
+template <bool COUNT, bool DEEP>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, const float4 *__restrict__ rays, uint32_t n,
                                                                   float4 *__restrict__ hits, int32_t *__restrict__ obj_out,
                                                                   uint32_t *__restrict__ err_out, unsigned long long *__restrict__ counters,
                                                                   uint32_t *__restrict__ next_ray, int refill_min) {
     __shared__ uint2 s_stack[SMEM_STACK * TRACE_BLOCK];
-    uint2 l_stack[LMEM_STACK];
-    uint2 *smem = s_stack + threadIdx.x;
+    Stack<DEEP> st;
+    st.smem = s_stack + threadIdx.x;
+    st.sp = 0;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lanemask_lt = (1u << lane) - 1u;
     uint32_t err = 0, nvis = 0, ntri = 0;
-    uint32_t ri = NO_RAY, mi = 0;
+    uint32_t ri = NO_RAY, mi = 0, visits = 0, steps = 0;
     bool in_mesh = false, pool_empty = false;
     Best best;
     best.t = 0.0f;
@@ -376,8 +369,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
     best.prim = best.obj = -1;
     LocalRay r = make_local_ray(0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f);
     MeshRef mr{};
-    Trav tv;
-    trav_init(tv, r);
+    uint32_t ng_base = 0, ng_bits = 0, tg_base = 0, tg_bits = 0;
     while (true) {
         // ---- refill lanes that have no ray
         const uint32_t need = __ballot_sync(0xffffffffu, ri == NO_RAY);
@@ -404,14 +396,25 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
         // ---- next instance whose box the ray enters, or the end of the ray
         if (!in_mesh) {
             const float4 r0 = __ldg(rays + 2ull * ri), r1 = __ldg(rays + 2ull * ri + 1);
-            const float4 sinv = make_float4(safe_inv(r1.x), safe_inv(r1.y), safe_inv(r1.z), 0.0f);
+            const float sx = safe_inv(r1.x), sy = safe_inv(r1.y), sz = safe_inv(r1.z);
             while (mi < sv.n_inst) {
-                const uint32_t m = mi++;
-                if (!enter_instance(sv, m, r0, sinv, best.t)) continue;
-                const InstanceRec *ir = sv.inst + m;
-                mr = mesh_of(sv, ir, (int)m);
+                const InstanceRec *ir = sv.inst + mi;
+                float bmin[3], bmax[3];
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    bmin[k] = __ldg(&ir->bbox_min[k]);
+                    bmax[k] = __ldg(&ir->bbox_max[k]);
+                }
+                mi++;
+                if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
+                mr = mesh_of(sv, ir, (int)mi - 1);
                 r = transform_ray(ir, r0, r1);
-                trav_init(tv, r);
+                ng_base = 0;
+                ng_bits = (1u << (24 + r.oct)) | 1u;
+                tg_bits = 0;
+                st.sp = 0;
+                visits = 0;
+                steps = 0;
                 in_mesh = true;
                 break;
             }
@@ -422,50 +425,75 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
                 continue;
             }
         }
-        // ---- one traversal step
-        const int res = trav_step<COUNT>(mr, r, best, smem, l_stack, tv, err, nvis, ntri);
-        if (res == STEP_DONE) {
-            in_mesh = false;
-        } else if (res == STEP_ERROR) {
+        // ---- one traversal step: a node visit (the current group always has
+        // a child left here) and the triangles it hits. A mesh takes at most
+        // node_count steps; more means a corrupt structure.
+        bool ok = ++steps <= mr.node_count + 8u;
+        if (!ok) err |= TRACE_ERR_LIMIT;
+        if (ok) ok = node_step<COUNT>(mr, r, best.t, ng_base, ng_bits, tg_base, tg_bits, st, visits, err, nvis);
+        if (!ok) {
             in_mesh = false;
             mi = sv.n_inst; // abandon the ray; the error flag reports it
+            continue;
+        }
+        while (tg_bits) {
+            const uint32_t k = __ffs(tg_bits) - 1;
+            tg_bits &= tg_bits - 1;
+            tri_test<COUNT>(mr, r, tg_base + k, best, err, ntri);
+        }
+        if (ng_bits <= 0x00FFFFFFu) {
+            if (st.sp == 0) {
+                in_mesh = false;
+            } else {
+                const uint2 e = st.pop();
+                ng_base = e.x;
+                ng_bits = e.y;
+            }
         }
     }
     flush_counters<COUNT>(err, nvis, ntri, err_out, counters);
 }
 
-int g_persistent_blocks = 0;
+int g_persistent_blocks[2] = {0, 0};
+
+template <bool DEEP>
+cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
+                        unsigned long long *counters, bool count, cudaStream_t st, const TraceParams &tp) {
+    if (!tp.persistent) {
+        const uint32_t grid = (n + TRACE_BLOCK - 1) / TRACE_BLOCK;
+        if (count)
+            k_trace_closest<true, DEEP><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters);
+        else
+            k_trace_closest<false, DEEP><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters);
+        return cudaGetLastError();
+    }
+    if (!tp.next_ray) return cudaErrorInvalidValue;
+    int &blocks = g_persistent_blocks[DEEP ? 1 : 0];
+    if (blocks == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_persistent<false, DEEP>, TRACE_BLOCK, 0);
+        if (e != cudaSuccess) return e;
+        blocks = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    cudaError_t e = cudaMemsetAsync(tp.next_ray, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    if (count)
+        k_trace_persistent<true, DEEP><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min);
+    else
+        k_trace_persistent<false, DEEP><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min);
+    return cudaGetLastError();
+}
 
 } // namespace
 
 cudaError_t launch_trace_closest(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
                                  unsigned long long *counters, bool count, cudaStream_t st, const TraceParams &tp) {
     if (n == 0) return cudaSuccess;
-    if (!tp.persistent) {
-        const uint32_t grid = (n + TRACE_BLOCK - 1) / TRACE_BLOCK;
-        if (count)
-            k_trace_closest<true><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters);
-        else
-            k_trace_closest<false><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters);
-        return cudaGetLastError();
-    }
-    if (!tp.next_ray) return cudaErrorInvalidValue;
-    if (g_persistent_blocks == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaError_t e = cudaGetDevice(&dev);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_persistent<false>, TRACE_BLOCK, 0);
-        if (e != cudaSuccess) return e;
-        g_persistent_blocks = sms * (per_sm > 0 ? per_sm : 1);
-    }
-    cudaError_t e = cudaMemsetAsync(tp.next_ray, 0, sizeof(uint32_t), st);
-    if (e != cudaSuccess) return e;
-    const uint32_t grid = (uint32_t)g_persistent_blocks;
-    if (count)
-        k_trace_persistent<true><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min);
-    else
-        k_trace_persistent<false><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min);
-    return cudaGetLastError();
+    // one group per level at most: the shared-memory stack suffices up to SMEM_STACK levels
+    if (tp.max_depth < (uint32_t)SMEM_STACK) return launch_impl<false>(sv, rays, n, hits, obj, err, counters, count, st, tp);
+    return launch_impl<true>(sv, rays, n, hits, obj, err, counters, count, st, tp);
 }
 
 } // namespace rg

@@ -22,6 +22,7 @@ constexpr uint32_t TRACE_ERR_LIMIT = 4u;  // more node visits than the mesh has 
 struct TraceParams {
     bool persistent = true; // resident grid with per-lane ray refill
     int refill_min = 8;     // refill a warp's idle lanes once at least this many are idle
+    uint32_t max_depth = 0; // deepest wide BVH among the traced meshes (sizes the stack)
     uint32_t *next_ray = nullptr; // device work counter for the persistent kernel
 };
 

@@ -195,6 +195,17 @@ def test_empty_and_degenerate(renderer, oracle):
     assert len(sc.trace_closest(np.zeros((0, 8), np.float32))) == 0
 
 
+@pytest.mark.parametrize("kernel,refill,deep", [(1, 8, 0), (1, 8, 1), (2, 1, 0), (2, 8, 0), (2, 32, 0), (2, 8, 1)])
+def test_kernel_variants_agree(renderer, oracle, kernel, refill, deep):
+    """Every traversal kernel and stack placement gives the same bytes."""
+    tris = scenes.random_triangles(100000, seed=81)
+    rays = scenes.incoherent_rays(60000, seed=82)
+    sc = _scene(tris, renderer)
+    sc.set_trace_tuning(kernel, refill, deep)
+    assert sc.get_trace_tuning() == (kernel, refill, deep)
+    _assert_hits_equal(sc.trace_closest(rays), _oracle_hits(oracle, tris, rays))
+
+
 def test_device_path_matches_host_path(renderer):
     import torch
 
