@@ -198,6 +198,19 @@ int ray_scene_commit(ray_scene *s);
  * RAY_MEM_DEVICE for all three buffers. stream: a cudaStream_t or NULL. */
 int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit *hits, int32_t *obj, int mem, void *stream);
 
+/* ---- ray sorting: SortRays_CPU (CoreRef.cpp:615-657) on device buffers.
+ * rays: n records of 8 floats (as for ray_scene_trace_closest). root_min,
+ * cell_size: the origin grid of get_ray_hash (CoreRef.cpp:316-333); the
+ * reference renderer uses the scene's root box and (max - min) / 255
+ * (RendererRef.cpp:48-77). keys_out (may be NULL): the hash of every input
+ * ray, bit-exact; perm_out: perm_out[k] = input index of the ray that lands at
+ * position k (a stable sort on the hash, the order SortRays_CPU produces);
+ * rays_out (may be NULL): the rays in that order. Device memory only;
+ * stream-ordered (stream: a cudaStream_t or NULL for the renderer's stream).
+ * The sort's scratch memory belongs to the renderer. */
+int ray_sort_rays(ray_renderer *r, const float *rays, uint64_t n, const float root_min[3], const float cell_size[3], uint32_t *keys_out,
+                  uint32_t *perm_out, float *rays_out, void *stream);
+
 /* Statistics of the last trace call on this scene: error flags OR-ed over rays
  * (bit 0: a ray's traversal stack overflowed), node and triangle visit totals
  * (counted only when counting was enabled with ray_scene_set_counting). */

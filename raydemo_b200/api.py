@@ -303,6 +303,14 @@ class Renderer:
         check(lib().ray_get_pixels(self._h, C.byref(out), 0))
         return np.ctypeslib.as_array(C.cast(out, C.POINTER(C.c_float)), shape=(h, w, 4)).copy()
 
+    def sort_rays_device(self, rays_ptr: int, n: int, root_min, cell_size, perm_ptr: int, keys_ptr: int = 0, rays_out_ptr: int = 0,
+                         stream: int = 0) -> None:
+        """SortRays_CPU (CoreRef.cpp:615-657) on device buffers: keys (optional),
+        the stable-sort permutation and (optional) the reordered rays."""
+        rm = (C.c_float * 3)(*root_min)
+        cs = (C.c_float * 3)(*cell_size)
+        check(lib().ray_sort_rays(self._h, rays_ptr, n, rm, cs, keys_ptr or None, perm_ptr, rays_out_ptr or None, stream or None))
+
     def GetStats(self) -> dict:
         st = capi.Stats()
         check(lib().ray_get_stats(self._h, C.byref(st)))

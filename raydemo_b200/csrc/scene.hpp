@@ -120,5 +120,6 @@ struct ray_renderer {
     cudaStream_t stream = nullptr;
     ray_stats stats{};
     std::vector<ray_pixel> host_pixels;
+    rg::DeviceBuf d_sort_scratch;
     ~ray_renderer();
 };

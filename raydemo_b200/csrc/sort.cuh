@@ -1,0 +1,20 @@
+// Ray hashing and sorting (the reference's SortRays_CPU, CoreRef.cpp:615-657).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rg {
+
+// Scratch bytes sort_rays needs for n rays.
+size_t sort_rays_scratch_bytes(uint64_t n);
+
+// keys_out[i] = get_ray_hash(ray i) (CoreRef.cpp:316-333); perm_out = the
+// order SortRays_CPU puts the rays in (a stable sort on the key: perm_out[k]
+// is the input index of the ray at position k); rays_out (may be null) = the
+// rays in that order. rays / rays_out: n records of 8 floats
+// (ox, oy, oz, tmax, dx, dy, dz, unused). All pointers are device memory.
+cudaError_t sort_rays(const float4 *rays, uint64_t n, const float root_min[3], const float cell_size[3], uint32_t *keys_out,
+                      uint32_t *perm_out, float4 *rays_out, void *scratch, cudaStream_t st);
+
+} // namespace rg
