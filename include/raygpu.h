@@ -211,6 +211,22 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
 int ray_sort_rays(ray_renderer *r, const float *rays, uint64_t n, const float root_min[3], const float cell_size[3], uint32_t *keys_out,
                   uint32_t *perm_out, float *rays_out, void *stream);
 
+/* Allocation-free variant of ray_sort_rays; it has no counterpart in the
+ * reference. For callers that cannot call cudaMalloc: hosts whose GPU memory
+ * belongs to their own allocator and budget, and frame loops that must not
+ * stall on cudaMalloc's implicit device-wide synchronisation. Same inputs,
+ * outputs and results as ray_sort_rays, without a renderer: the scratch
+ * memory is a fixed array of about 12.3 MB that every GPU loading this
+ * library holds until the process exits, so n is limited to
+ * RAY_SORT_NOALLOC_MAX_RAYS (larger n: RAY_ERR_INVALID_ARG). The first call on
+ * a device looks the array up on the current device; make that first call
+ * before any stream capture begins. All calls share the array: calls that
+ * overlap on the GPU (other streams, other host threads) race. stream: a
+ * cudaStream_t, or NULL for the default stream. */
+#define RAY_SORT_NOALLOC_MAX_RAYS (1u << 20)
+int ray_sort_rays_noalloc(const float *rays, uint64_t n, const float root_min[3], const float cell_size[3], uint32_t *keys_out,
+                          uint32_t *perm_out, float *rays_out, void *stream);
+
 /* Statistics of the last trace call on this scene: error flags OR-ed over rays
  * (bit 0: a ray's traversal stack overflowed), node and triangle visit totals
  * (counted only when counting was enabled with ray_scene_set_counting). */
