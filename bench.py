@@ -35,6 +35,18 @@ UNIT = "Mrays/s"
 WORKLOAD = "closest-hit BVH microbench: 2,097,152 random triangles, 4,194,304 incoherent rays"
 
 
+def profiled_traffic() -> float | None:
+    """DRAM bytes per launch of the traversal kernel, from the committed ncu
+    summary of this workload (profiles/trace_closest_microbench.txt)."""
+    p = os.path.join(ROOT, "profiles", "trace_closest_microbench.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("dram_bytes_per_launch:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
 def peaks() -> dict:
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -248,8 +260,9 @@ def run_gpu_arm(args) -> None:
     p = peaks()
     bytes_per_launch = N_RAYS * 44 + node_visits * 80 + tri_tests * 48
     achieved = bytes_per_launch / (ms / args.steps * 1e-3) / 1e9
+    traffic = args.traffic_bytes if args.traffic_bytes is not None else profiled_traffic()
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": p["hbm_gbs"], "unit": "GB/s",
-                "frac": round(achieved / p["hbm_gbs"], 4), "traffic": args.traffic_bytes, "peak_source": p["source"],
+                "frac": round(achieved / p["hbm_gbs"], 4), "traffic": traffic, "peak_source": p["source"],
                 "alg_bytes_per_launch": int(bytes_per_launch), "node_visits_per_ray": round(node_visits / N_RAYS, 3),
                 "tri_tests_per_ray": round(tri_tests / N_RAYS, 3)}
 
