@@ -1,0 +1,280 @@
+// Device-side traversal shared by the trace kernels and the shading kernels:
+// the instance-level test and transform, the compressed wide-BVH node step,
+// the triangle test and whole-mesh traversal. See trace.cu for the design.
+#pragma once
+
+#include "trace.cuh"
+
+namespace rg {
+namespace trav {
+
+constexpr int TRACE_BLOCK = 128;
+constexpr int SMEM_STACK = 24; // entries per thread in shared memory
+constexpr int LMEM_STACK = 40; // further entries in a local array (DEEP instances only)
+constexpr uint32_t NO_RAY = 0xffffffffu;
+
+__device__ __forceinline__ float byte_to_float(uint32_t word, uint32_t sel) {
+    // 0x4B0000bb is 2^23 + bb as a float; subtracting 2^23 leaves bb exactly.
+    return __fsub_rn(__uint_as_float(__byte_perm(word, 0x4B000000u, sel)), 8388608.0f);
+}
+
+// The reference's slab test, exactly (bbox_test, CoreRef.cpp:64-86).
+__device__ __forceinline__ bool ref_bbox_test(float ox, float oy, float oz, float ix, float iy, float iz, float t, const float *bmin,
+                                              const float *bmax) {
+    float lo_x = __fmul_rn(ix, __fsub_rn(bmin[0], ox)), hi_x = __fmul_rn(ix, __fsub_rn(bmax[0], ox));
+    if (lo_x > hi_x) { const float tmp = lo_x; lo_x = hi_x; hi_x = tmp; }
+    float lo_y = __fmul_rn(iy, __fsub_rn(bmin[1], oy)), hi_y = __fmul_rn(iy, __fsub_rn(bmax[1], oy));
+    if (lo_y > hi_y) { const float tmp = lo_y; lo_y = hi_y; hi_y = tmp; }
+    float lo_z = __fmul_rn(iz, __fsub_rn(bmin[2], oz)), hi_z = __fmul_rn(iz, __fsub_rn(bmax[2], oz));
+    if (lo_z > hi_z) { const float tmp = lo_z; lo_z = hi_z; hi_z = tmp; }
+    float tmin = lo_x > lo_y ? lo_x : lo_y;
+    if (lo_z > tmin) tmin = lo_z;
+    float tmax = hi_x < hi_y ? hi_x : hi_y;
+    if (hi_z < tmax) tmax = hi_z;
+    tmax = __fmul_rn(tmax, 1.00000024f);
+    return tmin <= tmax && tmin <= t && tmax > 0;
+}
+
+// safe_invert, CoreRef.cpp:272-294
+__device__ __forceinline__ float safe_inv(float v) {
+    float r = __frcp_rn(v);
+    if (v <= FLT_EPS_ && v >= 0) r = 3.402823466e+38F;
+    else if (v >= -FLT_EPS_ && v < 0) r = -3.402823466e+38F;
+    return r;
+}
+
+struct Best {
+    float t, u, v;
+    int prim, obj;
+};
+
+// Ray in the space of the instance being traversed.
+struct LocalRay {
+    float ox, oy, oz, dx, dy, dz, ix, iy, iz;
+    uint32_t oct; // bit a set: direction negative on axis a
+};
+
+struct MeshRef {
+    const WideNode *nodes;
+    const TriRec *tris;
+    uint32_t prim_base, node_count, tri_count;
+    int obj;
+};
+
+// Per-thread stack of node groups: entry k of this thread at
+// smem[k * TRACE_BLOCK]; the DEEP variant continues in a local array.
+template <bool DEEP>
+struct Stack;
+
+template <>
+struct Stack<false> {
+    uint2 *smem;
+    int sp;
+    __device__ __forceinline__ bool push(uint2 e) {
+        if (sp >= SMEM_STACK) return false;
+        smem[sp * TRACE_BLOCK] = e;
+        sp++;
+        return true;
+    }
+    __device__ __forceinline__ uint2 pop() {
+        sp--;
+        return smem[sp * TRACE_BLOCK];
+    }
+};
+
+template <>
+struct Stack<true> {
+    uint2 *smem;
+    uint2 lmem[LMEM_STACK];
+    int sp;
+    __device__ __forceinline__ bool push(uint2 e) {
+        if (sp >= SMEM_STACK + LMEM_STACK) return false;
+        if (sp < SMEM_STACK) smem[sp * TRACE_BLOCK] = e;
+        else lmem[sp - SMEM_STACK] = e;
+        sp++;
+        return true;
+    }
+    __device__ __forceinline__ uint2 pop() {
+        sp--;
+        return sp < SMEM_STACK ? smem[sp * TRACE_BLOCK] : lmem[sp - SMEM_STACK];
+    }
+};
+
+__device__ __forceinline__ LocalRay make_local_ray(float ox, float oy, float oz, float dx, float dy, float dz) {
+    LocalRay r;
+    r.ox = ox; r.oy = oy; r.oz = oz;
+    r.dx = dx; r.dy = dy; r.dz = dz;
+    r.ix = __frcp_rn(dx); // 1.0f / d, CoreRef.cpp:1215
+    r.iy = __frcp_rn(dy);
+    r.iz = __frcp_rn(dz);
+    r.oct = (r.ix < 0.0f ? 1u : 0u) | (r.iy < 0.0f ? 2u : 0u) | (r.iz < 0.0f ? 4u : 0u);
+    return r;
+}
+
+// TransformRay, CoreRef.cpp:1605-1617, with the instance's inverse transform.
+__device__ __forceinline__ LocalRay transform_ray(const InstanceRec *ir, float4 r0, float4 r1) {
+    float x[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) x[k] = __ldg(&ir->inv_xform[k]);
+    const float tox = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(x[0], r0.x), __fmul_rn(x[3], r0.y)), __fmul_rn(x[6], r0.z)), x[9]);
+    const float toy = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(x[1], r0.x), __fmul_rn(x[4], r0.y)), __fmul_rn(x[7], r0.z)), x[10]);
+    const float toz = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(x[2], r0.x), __fmul_rn(x[5], r0.y)), __fmul_rn(x[8], r0.z)), x[11]);
+    const float tdx = __fadd_rn(__fadd_rn(__fmul_rn(x[0], r1.x), __fmul_rn(x[3], r1.y)), __fmul_rn(x[6], r1.z));
+    const float tdy = __fadd_rn(__fadd_rn(__fmul_rn(x[1], r1.x), __fmul_rn(x[4], r1.y)), __fmul_rn(x[7], r1.z));
+    const float tdz = __fadd_rn(__fadd_rn(__fmul_rn(x[2], r1.x), __fmul_rn(x[5], r1.y)), __fmul_rn(x[8], r1.z));
+    return make_local_ray(tox, toy, toz, tdx, tdy, tdz);
+}
+
+__device__ __forceinline__ MeshRef mesh_of(const SceneView &sv, const InstanceRec *ir, int m) {
+    MeshRef mr;
+    mr.nodes = sv.nodes + __ldg(&ir->node_base);
+    mr.tris = sv.leaf_tris + __ldg(&ir->tri_base);
+    mr.prim_base = __ldg(&ir->prim_base);
+    mr.node_count = __ldg(&ir->node_count);
+    mr.tri_count = __ldg(&ir->tri_count);
+    mr.obj = m;
+    return mr;
+}
+
+// Node step: takes the next child of node group (ng_base, ng_bits), tests
+// its 8 children and returns their hits as a node group (internal children,
+// bits 24..31, with the node's imask in bits 0..7) and a triangle group
+// (bits 0..23). Returns false (and sets err) on a corrupt index.
+template <bool COUNT, bool DEEP>
+__device__ __forceinline__ bool node_step(const MeshRef &mr, const LocalRay &r, float best_t, uint32_t &ng_base, uint32_t &ng_bits,
+                                          uint32_t &tg_base, uint32_t &tg_bits, Stack<DEEP> &st, uint32_t &visits, uint32_t &err,
+                                          uint32_t &nvis) {
+    const uint32_t j = __ffs(ng_bits >> 24) - 1;
+    ng_bits &= ~(1u << (24 + j));
+    const uint32_t s = j ^ r.oct;
+    const uint32_t ni = ng_base + __popc((ng_bits & 0xFFu) & ((1u << s) - 1u));
+    if (ng_bits > 0x00FFFFFFu && !st.push(make_uint2(ng_base, ng_bits))) {
+        err |= TRACE_ERR_STACK;
+        return false;
+    }
+    // A tree visits each node at most once; a bad index or a longer walk
+    // means a corrupt structure: flag it and stop this ray.
+    if (ni >= mr.node_count || ++visits > mr.node_count) {
+        err |= (ni >= mr.node_count) ? TRACE_ERR_BOUNDS : TRACE_ERR_LIMIT;
+        return false;
+    }
+    const uint4 *np = reinterpret_cast<const uint4 *>(mr.nodes + ni);
+    const uint4 w0 = __ldg(np), w1 = __ldg(np + 1), w2 = __ldg(np + 2), w3 = __ldg(np + 3), w4 = __ldg(np + 4);
+    if (COUNT) nvis++;
+    const uint32_t imask = w0.w >> 24;
+    // Slab parameter of plane q on one axis: t(q) = q * A + B with
+    // A = 2^e * inv_d (exact: a power-of-two scaling) and B = (p - o) * inv_d,
+    // one FMA per plane. Its rounding error is below 2u(|B| + 256|A|)
+    // (u = 2^-24); the slack 2^-21 (|B| + 256|A|) moves the near planes
+    // down and the far planes up by more than that, so the test accepts
+    // every box that the exact slab test on the decoded box accepts.
+    float A[3], Bn[3], Bf[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float p = __uint_as_float(a == 0 ? w0.x : (a == 1 ? w0.y : w0.z));
+        const float sc = __uint_as_float(((w0.w >> (8 * a)) & 0xFFu) << 23);
+        const float inv = a == 0 ? r.ix : (a == 1 ? r.iy : r.iz);
+        const float o = a == 0 ? r.ox : (a == 1 ? r.oy : r.oz);
+        A[a] = __fmul_rn(sc, inv);
+        const float B = __fmul_rn(__fsub_rn(p, o), inv);
+        const float slack = __fmul_rn(__fmaf_rn(fabsf(A[a]), 256.0f, fabsf(B)), 4.76837158203125e-07f);
+        Bn[a] = __fsub_rn(B, slack);
+        Bf[a] = __fadd_rn(B, slack);
+    }
+    // Near/far plane words by direction sign, so that a NaN slab value
+    // (origin on a plane of a box the ray runs parallel to) leaves that axis
+    // unbounded, which keeps the test conservative. Planes: lo x = w2.xy,
+    // lo y = w2.zw, lo z = w3.xy, hi x = w3.zw, hi y = w4.xy, hi z = w4.zw.
+    const bool nx = r.oct & 1u, ny = r.oct & 2u, nz = r.oct & 4u;
+    const uint32_t nxa = nx ? w3.z : w2.x, nxb = nx ? w3.w : w2.y, fxa = nx ? w2.x : w3.z, fxb = nx ? w2.y : w3.w;
+    const uint32_t nya = ny ? w4.x : w2.z, nyb = ny ? w4.y : w2.w, fya = ny ? w2.z : w4.x, fyb = ny ? w2.w : w4.y;
+    const uint32_t nza = nz ? w4.z : w3.x, nzb = nz ? w4.w : w3.y, fza = nz ? w3.x : w4.z, fzb = nz ? w3.y : w4.w;
+    uint32_t hitmask = 0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        const uint32_t meta = ((c < 4 ? w1.z : w1.w) >> (8 * (c & 3))) & 0xFFu;
+        const uint32_t sel = 0x7540u | (uint32_t)(c & 3);
+        const float tnx = __fmaf_rn(byte_to_float(c < 4 ? nxa : nxb, sel), A[0], Bn[0]);
+        const float tfx = __fmaf_rn(byte_to_float(c < 4 ? fxa : fxb, sel), A[0], Bf[0]);
+        const float tny = __fmaf_rn(byte_to_float(c < 4 ? nya : nyb, sel), A[1], Bn[1]);
+        const float tfy = __fmaf_rn(byte_to_float(c < 4 ? fya : fyb, sel), A[1], Bf[1]);
+        const float tnz = __fmaf_rn(byte_to_float(c < 4 ? nza : nzb, sel), A[2], Bn[2]);
+        const float tfz = __fmaf_rn(byte_to_float(c < 4 ? fza : fzb, sel), A[2], Bf[2]);
+        const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
+        const float tmax = fminf(fminf(tfx, tfy), tfz);
+        if (meta != 0 && tmin <= tmax && tmin <= best_t && tmax >= 0.0f) {
+            uint32_t bit = meta & 31u;
+            if (bit >= 24u) bit ^= r.oct;
+            hitmask |= (meta >> 5) << bit;
+        }
+    }
+    ng_base = w1.x;
+    ng_bits = (hitmask & 0xFF000000u) | imask;
+    tg_base = w1.y;
+    tg_bits = hitmask & 0x00FFFFFFu;
+    return true;
+}
+
+// One triangle test; updates best when it is the closer hit.
+template <bool COUNT>
+__device__ __forceinline__ void tri_test(const MeshRef &mr, const LocalRay &r, uint32_t li, Best &best, uint32_t &err, uint32_t &ntri) {
+    if (li >= mr.tri_count) {
+        err |= TRACE_ERR_BOUNDS;
+        return;
+    }
+    const float4 *tp = reinterpret_cast<const float4 *>(mr.tris + li);
+    const float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
+    if (COUNT) ntri++;
+    const float nu = t0.x, nv = t0.y, npl = t0.z, pu = t0.w, pv = t1.x, e0u = t1.z, e0v = t1.w, e1u = t2.x, e1v = t2.y;
+    const int iw = __float_as_int(t1.y) & TRI_W_BITS;
+    const float du = iw == 0 ? r.dy : r.dx, dv = iw == 2 ? r.dy : r.dz, dw = iw == 0 ? r.dx : (iw == 1 ? r.dy : r.dz);
+    const float ou = iw == 0 ? r.oy : r.ox, ov = iw == 2 ? r.oy : r.oz, ow = iw == 0 ? r.ox : (iw == 1 ? r.oy : r.oz);
+    // _IntersectTri, CoreRef.cpp:18-40
+    const float det = __fadd_rn(__fadd_rn(__fmul_rn(du, nu), __fmul_rn(dv, nv)), dw);
+    const float dett = __fsub_rn(npl, __fadd_rn(__fadd_rn(__fmul_rn(ou, nu), __fmul_rn(ov, nv)), ow));
+    const float Du = __fsub_rn(__fmul_rn(du, dett), __fmul_rn(__fsub_rn(pu, ou), det));
+    const float Dv = __fsub_rn(__fmul_rn(dv, dett), __fmul_rn(__fsub_rn(pv, ov), det));
+    const float detu = __fsub_rn(__fmul_rn(e1v, Du), __fmul_rn(e1u, Dv));
+    const float detv = __fsub_rn(__fmul_rn(e0u, Dv), __fmul_rn(e0v, Du));
+    const float tmpdet0 = __fsub_rn(__fsub_rn(det, detu), detv);
+    if ((tmpdet0 > -HIT_EPS && detu > -HIT_EPS && detv > -HIT_EPS) || (tmpdet0 < HIT_EPS && detu < HIT_EPS && detv < HIT_EPS)) {
+        const float rdet = __frcp_rn(det); // 1.0f / det, correctly rounded
+        const float t = __fmul_rn(dett, rdet);
+        const int gp = (int)(mr.prim_base + __float_as_uint(t2.z));
+        if (t > 0.0f && (t < best.t || (t == best.t && best.prim >= 0 && gp < best.prim))) {
+            best.t = t;
+            best.u = __fmul_rn(detu, rdet);
+            best.v = __fmul_rn(detv, rdet);
+            best.prim = gp;
+            best.obj = mr.obj;
+        }
+    }
+}
+
+// Whole traversal of one mesh for one ray (the one-thread-per-ray kernel).
+// The current node group always has a child left at the top of the loop: the
+// root's, then the group a node step returns or one taken from the stack.
+template <bool COUNT, bool DEEP>
+__device__ __forceinline__ void trace_mesh(const MeshRef &mr, const LocalRay &r, Best &best, Stack<DEEP> &st, uint32_t &err,
+                                           uint32_t &nvis, uint32_t &ntri) {
+    uint32_t ng_base = 0, ng_bits = (1u << (24 + r.oct)) | 1u; // the root as slot 0 of a virtual parent
+    uint32_t tg_base = 0, tg_bits = 0, visits = 0;
+    st.sp = 0;
+    while (true) {
+        if (!node_step<COUNT>(mr, r, best.t, ng_base, ng_bits, tg_base, tg_bits, st, visits, err, nvis)) return;
+        while (tg_bits) {
+            const uint32_t k = __ffs(tg_bits) - 1;
+            tg_bits &= tg_bits - 1;
+            tri_test<COUNT>(mr, r, tg_base + k, best, err, ntri);
+        }
+        if (ng_bits <= 0x00FFFFFFu) {
+            if (st.sp == 0) return;
+            const uint2 e = st.pop();
+            ng_base = e.x;
+            ng_bits = e.y;
+        }
+    }
+}
+
+} // namespace trav
+} // namespace rg
