@@ -264,6 +264,16 @@ int ray_scene_mesh_bvh_info(ray_scene *s, uint32_t mesh, ray_bvh_info *out);
  * bytes; *out_bytes receives the array size. */
 int ray_scene_debug_read(ray_scene *s, int what, void *dst, uint64_t bytes, uint64_t *out_bytes);
 
+/* Diagnostics: copies one of the renderer's device arrays to host memory after
+ * the last ray_render. what: 0 the first ray buffer (32 bytes per ray: ox, oy,
+ * oz, tmax, dx, dy, dz, pixel as (x << 16) | y), 1 its payloads (80 bytes per
+ * ray: c[3], ior, do_dx[3], dd_dx[3], do_dy[3], dd_dy[3], ray_depth, 3 unused),
+ * 2 the sample table (6144 floats, RendererRef.cpp:327-358), 3 the frame's
+ * sample buffer (16 bytes per pixel). The first ray buffer holds the primary
+ * rays when the frame traced no bounce (skip_indirect_lighting). Copies at most
+ * `bytes` bytes; *out_bytes receives the array size. */
+int ray_renderer_debug_read(ray_renderer *r, int what, void *dst, uint64_t bytes, uint64_t *out_bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,7 +16,7 @@
 #include <functional>
 #include <memory>
 #include <random>
-#include <sstream>
+#include <ostream>
 #include <thread>
 #include <vector>
 
@@ -349,7 +349,11 @@ void *rb_renderer_new(int type, int w, int h, int use_wide) {
     s.w = w;
     s.h = h;
     s.use_wide_bvh = use_wide != 0;
-    std::ostringstream log;
+    // A stream without a buffer: CreateRenderer's log lines are dropped before
+    // they reach the locale machinery, which is not safe to use when the host
+    // process carries a second copy of the C++ runtime (a Python interpreter
+    // that has loaded numpy, for one).
+    std::ostream log(nullptr);
     rh->r = Ray::CreateRenderer(s, (uint32_t)type, log);
     rh->w = w;
     rh->h = h;

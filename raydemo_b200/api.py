@@ -311,6 +311,32 @@ class Renderer:
         cs = (C.c_float * 3)(*cell_size)
         check(lib().ray_sort_rays(self._h, rays_ptr, n, rm, cs, keys_ptr or None, perm_ptr, rays_out_ptr or None, stream or None))
 
+    def get_sh_data_ref(self):
+        """get_sh_data_ref: (h, w, 12) float32 (coeff_r[4], coeff_g[4], coeff_b[4]) or None."""
+        w, h = self.size()
+        out = C.c_void_p()
+        check(lib().ray_get_sh_data(self._h, C.byref(out)))
+        if not out.value:
+            return None
+        return np.ctypeslib.as_array(C.cast(out, C.POINTER(C.c_float)), shape=(h, w, 12)).copy()
+
+    def debug_read(self, what: int) -> np.ndarray:
+        """Renderer device arrays (ray_renderer_debug_read): 0 first ray buffer
+        (n, 8) float32, 1 payloads (n, 20) float32, 2 sample table (6144,),
+        3 sample buffer (h, w, 4)."""
+        size = C.c_uint64()
+        check(lib().ray_renderer_debug_read(self._h, what, None, 0, C.byref(size)))
+        buf = np.zeros(size.value // 4, np.float32)
+        check(lib().ray_renderer_debug_read(self._h, what, buf.ctypes.data, size.value, C.byref(size)))
+        if what == 0:
+            return buf.reshape(-1, 8)
+        if what == 1:
+            return buf.reshape(-1, 20)
+        if what == 3:
+            w, h = self.size()
+            return buf.reshape(h, w, 4)
+        return buf
+
     def GetStats(self) -> dict:
         st = capi.Stats()
         check(lib().ray_get_stats(self._h, C.byref(st)))

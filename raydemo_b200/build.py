@@ -19,7 +19,8 @@ OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libraygpu.so")
 OBJ_DIR = os.path.join(OUT_DIR, "obj")
 
-SOURCES = ["api.cu", "bvh_build.cu", "radix_sort.cu", "trace.cu", "sort.cu", "sort_noalloc.cu", "render.cu"]
+SOURCES = ["api.cu", "bvh_build.cu", "radix_sort.cu", "trace.cu", "sort.cu", "sort_noalloc.cu", "render.cu", "render_kernels.cu",
+           "scene_shading.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off",

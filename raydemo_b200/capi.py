@@ -154,6 +154,7 @@ _SIGS = {
     "ray_scene_last_trace_info": ([_P, C.POINTER(TraceInfo)], C.c_int),
     "ray_scene_mesh_bvh_info": ([_P, C.c_uint32, C.POINTER(BvhInfo)], C.c_int),
     "ray_scene_debug_read": ([_P, C.c_int, _P, C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
+    "ray_renderer_debug_read": ([_P, C.c_int, _P, C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
     "ray_sort_rays": ([_P, _P, C.c_uint64, C.POINTER(C.c_float), C.POINTER(C.c_float), _P, _P, _P, _P], C.c_int),
     "ray_sort_rays_noalloc": ([_P, C.c_uint64, C.POINTER(C.c_float), C.POINTER(C.c_float), _P, _P, _P, _P], C.c_int),
     "ray_scene_set_trace_tuning": ([_P, C.POINTER(TraceTuning)], C.c_int),

@@ -134,27 +134,8 @@ static void construct_camera(CameraRec &c) {
     }
 }
 
-static int upload_texture_host(ray_scene *s, const uint8_t *data, int w, int h, bool srgb, bool mips, uint32_t *out) {
-    if (!data || w <= 0 || h <= 0 || w > 16384 || h > 16384) {
-        set_error("invalid texture description");
-        return RAY_ERR_INVALID_ARG;
-    }
-    TextureRec t;
-    t.w = w;
-    t.h = h;
-    t.srgb = srgb;
-    t.mips = mips;
-    t.rgba.assign(data, data + (size_t)w * h * 4);
-    t.level_offset.push_back(0);
-    t.level_w.push_back((uint32_t)w);
-    t.level_h.push_back((uint32_t)h);
-    s->textures.push_back(std::move(t));
-    *out = (uint32_t)(s->textures.size() - 1);
-    return RAY_OK;
-}
-
 int commit(ray_scene *s) {
-    if (!s->geom_dirty) return RAY_OK;
+    if (!s->geom_dirty) return upload_shading(s);
     RG_CUDA_TRY(cudaSetDevice(s->device));
     cudaStream_t st = s->stream;
     // 1. build the meshes that have no BVH yet
@@ -241,8 +222,10 @@ int commit(ray_scene *s) {
     s->n_inst_dev = (uint32_t)inst.size();
     RG_CUDA_TRY(cudaStreamSynchronize(st));
     s->total_nodes = (uint32_t)nodes;
+    s->max_depth = 0;
+    for (const MeshRec &m : s->meshes) s->max_depth = std::max(s->max_depth, m.bvh.depth);
     s->geom_dirty = false;
-    return RAY_OK;
+    return upload_shading(s);
 }
 
 } // namespace rg
@@ -275,11 +258,6 @@ ray_scene::~ray_scene() {
         free_mesh_bvh(m.bvh);
         if (m.tris_ref) cudaFree(m.tris_ref);
     }
-    if (stream) cudaStreamDestroy(stream);
-}
-
-ray_renderer::~ray_renderer() {
-    cudaSetDevice(device);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -345,8 +323,8 @@ int ray_create_scene(ray_renderer *r, ray_scene **out) {
     // map and a 1-pixel flat normal map are textures 0 and 1.
     static const uint8_t env_px[4] = {255, 255, 255, 128};
     static const uint8_t nrm_px[4] = {127, 127, 255, 0};
-    upload_texture_host(s, env_px, 1, 1, true, false, &s->default_env_texture);
-    upload_texture_host(s, nrm_px, 1, 1, true, false, &s->default_normals_texture);
+    add_texture(s, env_px, 1, 1, true, false, &s->default_env_texture);
+    add_texture(s, nrm_px, 1, 1, true, false, &s->default_normals_texture);
     s->env.env_col[0] = s->env.env_col[1] = s->env.env_col[2] = 0.0f;
     s->env.env_clamp = 0.0f;
     s->env.env_map = s->default_env_texture;
@@ -376,7 +354,7 @@ int ray_scene_set_environment(ray_scene *s, const ray_environment_desc *env) {
 int ray_scene_add_texture(ray_scene *s, const ray_tex_desc *t, uint32_t *out_index) {
     RG_CHECK(s && t && out_index, "null argument");
     RG_GUARD_BEGIN
-    return upload_texture_host(s, t->data, t->w, t->h, t->is_srgb != 0, t->generate_mipmaps != 0, out_index);
+    return add_texture(s, t->data, t->w, t->h, t->is_srgb != 0, t->generate_mipmaps != 0, out_index);
     RG_GUARD_END
 }
 
@@ -409,6 +387,7 @@ int ray_scene_add_material(ray_scene *s, const ray_mat_desc *m, uint32_t *out_in
     }
     r.textures[0] = (m->normal_map != RAY_INVALID_INDEX) ? m->normal_map : s->default_normals_texture;
     s->materials.push_back(r);
+    s->shade_dirty = true;
     *out_index = (uint32_t)(s->materials.size() - 1);
     return RAY_OK;
     RG_GUARD_END
@@ -477,8 +456,8 @@ int ray_scene_add_mesh(ray_scene *s, const ray_mesh_desc *d, uint32_t *out_index
         const size_t v = (size_t)((int64_t)d->vtx_indices[j] + d->base_vertex);
         memcpy(&m.verts[3 * j], d->vtx_attrs + v * stride, 3 * sizeof(float));
     }
-    // shading attributes (SceneRef.cpp:220-260); tangents are filled in by the
-    // shading setup when the layout has none
+    // shading attributes (SceneRef.cpp:220-260); layouts without tangents get
+    // them from the triangles, which may split vertices
     const uint32_t vbase = (uint32_t)s->vertices.size();
     s->vertices.resize(vbase + d->vtx_attrs_count);
     for (uint64_t i = 0; i < d->vtx_attrs_count; i++) {
@@ -501,10 +480,14 @@ int ray_scene_add_mesh(ray_scene *s, const ray_mesh_desc *d, uint32_t *out_index
             memcpy(v.t[1], a + 11, 8);
         }
     }
-    for (uint64_t j = 0; j < d->vtx_indices_count; j++) s->vtx_indices.push_back((uint32_t)(d->vtx_indices[j] + d->base_vertex) + vbase);
+    std::vector<uint32_t> ni(d->vtx_indices_count);
+    for (uint64_t j = 0; j < d->vtx_indices_count; j++) ni[j] = (uint32_t)(d->vtx_indices[j] + d->base_vertex) + vbase;
+    if (d->layout == RAY_LAYOUT_PNT || d->layout == RAY_LAYOUT_PNTT) compute_tangent_basis(s->vertices, ni, vbase);
+    s->vtx_indices.insert(s->vtx_indices.end(), ni.begin(), ni.end());
     s->meshes.push_back(std::move(m));
     s->total_tris += (uint32_t)ntris;
     s->geom_dirty = true;
+    s->shade_dirty = true;
     *out_index = (uint32_t)(s->meshes.size() - 1);
     return RAY_OK;
     RG_GUARD_END
@@ -535,6 +518,7 @@ int ray_scene_remove_mesh(ray_scene *s, uint32_t i) {
     s->vtx_indices.erase(s->vtx_indices.begin() + 3ull * tris_index, s->vtx_indices.begin() + 3ull * (tris_index + tris_count));
     s->total_tris -= tris_count;
     s->geom_dirty = true;
+    s->shade_dirty = true;
     return RAY_OK;
     RG_GUARD_END
 }
@@ -568,6 +552,7 @@ int ray_scene_add_light(ray_scene *s, const ray_light_desc *d, uint32_t *out_ind
     }
     l.brightness = std::max(l.col[0], std::max(l.col[1], l.col[2]));
     s->lights.push_back(l);
+    s->shade_dirty = true;
     *out_index = (uint32_t)(s->lights.size() - 1);
     return RAY_OK;
     RG_GUARD_END
@@ -832,23 +817,4 @@ int ray_scene_debug_read(ray_scene *s, int what, void *dst, uint64_t bytes, uint
 }
 
 // ---- renderer entry points that do not need the render loop
-int ray_resize(ray_renderer *r, int w, int h) {
-    RG_CHECK(r && w > 0 && h > 0 && w <= 32768 && h <= 32768, "invalid size");
-    r->w = w;
-    r->h = h;
-    return RAY_OK;
-}
-
-int ray_get_stats(ray_renderer *r, ray_stats *out) {
-    RG_CHECK(r && out, "null argument");
-    *out = r->stats;
-    return RAY_OK;
-}
-
-int ray_reset_stats(ray_renderer *r) {
-    RG_CHECK(r, "null argument");
-    r->stats = ray_stats{};
-    return RAY_OK;
-}
-
 } // extern "C"

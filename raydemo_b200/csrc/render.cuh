@@ -1,0 +1,135 @@
+// Device-side data of the renderer (the Ref backend's render loop,
+// src/Ray/internal/RendererRef.cpp:19-325) and its kernel launchers.
+#pragma once
+
+#include "../../include/raygpu.h"
+#include "common.cuh"
+#include "trace.cuh"
+
+namespace rg {
+
+// material_t (src/Ray/internal/Core.h:121-131): textures[] = normal map,
+// main texture, and for mix materials the two mixed materials.
+struct MaterialRec {
+    uint32_t textures[4];
+    float main_color[3], pad;
+    uint32_t type;
+    float roughness_or_strength;
+    float int_ior, ext_ior;
+};
+static_assert(sizeof(MaterialRec) == 48, "MaterialRec must stay 48 bytes");
+
+// light_t (Core.h:133-138)
+struct LightRec {
+    float pos[3], radius;
+    float col[3], brightness;
+    float dir[3], spot;
+};
+static_assert(sizeof(LightRec) == 48, "LightRec must stay 48 bytes");
+
+// vertex_t (Core.h:259-262)
+struct VertexRec {
+    float p[3], n[3], b[3], t[2][2];
+};
+static_assert(sizeof(VertexRec) == 52, "VertexRec must stay 52 bytes");
+
+constexpr int NUM_MIP_LEVELS = 14;
+
+// One mip level as stored on the device: a (w + 2) x (h + 2) block of RGBA8
+// texels (with the wrap border) at texel offset `off`; (px, py) is where the
+// reference's atlas places the level, which fixes the rounding of its
+// sampling coordinates.
+struct TexLevel {
+    uint32_t off;
+    uint16_t px, py;
+    uint16_t pitch, rows;
+};
+static_assert(sizeof(TexLevel) == 12, "TexLevel must stay 12 bytes");
+
+// texture_t (Core.h:103-108) as the device samples it. Levels past the last
+// generated one repeat it, as in the reference (SceneRef.cpp:104-109).
+struct TexDev {
+    uint32_t width; // bit 15: sRGB
+    uint32_t height;
+    TexLevel lv[NUM_MIP_LEVELS];
+};
+
+// Everything a shading kernel reads of the scene.
+struct RenderScene {
+    SceneView sv;                  // BVH, leaf triangles and instances (shadow rays)
+    const TriRec *tris;            // triangles in insertion order (materials, plane normal)
+    const uint32_t *vtx_indices;   // 3 per triangle
+    const VertexRec *vertices;
+    const MaterialRec *materials;
+    const TexDev *textures;
+    const uint32_t *texels;
+    const LightRec *lights;
+    uint32_t n_tris, n_materials, n_textures, n_lights;
+    float env_col[3], env_clamp;
+    uint32_t env_map;
+};
+
+// pass_settings_t flags (src/Ray/Types.h:39-45)
+enum : uint32_t {
+    PASS_SKIP_DIRECT = 1u << 0,
+    PASS_SKIP_INDIRECT = 1u << 1,
+    PASS_LIGHTING_ONLY = 1u << 2,
+    PASS_NO_BACKGROUND = 1u << 3,
+    PASS_CLAMP = 1u << 4,
+    PASS_OUTPUT_SH = 1u << 5,
+    PASS_COHERENT = 1u << 6,
+};
+
+// pass_info_t (Core.h:269-292) minus the per-ray index
+struct PassInfo {
+    int iteration, bounce;
+    uint32_t flags;
+    int max_diff_depth, max_glossy_depth, max_refr_depth, max_transp_depth, max_total_depth, termination_start_depth;
+    int w; // framebuffer width (pixel index = y * w + x)
+};
+
+// camera_t (Types.h:59-71) fields ray generation needs
+struct CameraDev {
+    int filter; // 0 box, 1 tent
+    float fov, focus_distance, focus_factor;
+    float origin[3], fwd[3], side[3], up[3];
+};
+
+// Ray payload beside the 32-byte trace record (o, tmax | d, xy): the rest of
+// ray_packet_t (CoreRef.h:34-45), 80 bytes.
+struct alignas(16) RayPayload {
+    float c[3], ior;
+    float do_dx[3], dd_dx[3], do_dy[3], dd_dy[3];
+    int32_t ray_depth;
+    uint32_t pad[3];
+};
+static_assert(sizeof(RayPayload) == 80, "RayPayload must stay 80 bytes");
+
+// shl1_data_t (Types.h:25-28)
+struct SHData {
+    float coeff_r[4], coeff_g[4], coeff_b[4];
+};
+
+constexpr int HALTON_COUNT = 24;
+constexpr int HALTON_SEQ_LEN = 256;
+// table entries plus a guard band: the reference's deepest bounce reads two
+// entries past row 255 (RendererRef.cpp:327-358 with MAX_BOUNCES 10)
+constexpr int HALTON_TABLE_FLOATS = HALTON_COUNT * HALTON_SEQ_LEN + 64;
+
+// Launchers (render_kernels.cu). All stream-ordered; counts live on the device.
+cudaError_t launch_halton_table(const uint16_t *perms, int base_iteration, float *table, cudaStream_t st);
+cudaError_t launch_raygen(const CameraDev &cam, float k, float fov_k, int iteration, int rx, int ry, int rw, int rh, int w, int h, const float *halton,
+                          float4 *rays, RayPayload *pay, uint32_t *count, cudaStream_t st);
+// Shades the hits of *in_count rays; appends continuation rays to out (count
+// *out_count). primary: SetPixel into temp, else AddPixel with alpha 0.
+cudaError_t launch_shade(const RenderScene &sc, const PassInfo &pi, const float *halton, const float4 *rays, const RayPayload *pay,
+                         const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays, float4 *out_rays,
+                         RayPayload *out_pay, uint32_t *out_count, float4 *temp, SHData *temp_sh, bool primary, uint32_t *err,
+                         cudaStream_t st);
+// clean += (temp - clean) * k over the rect, then final = tone(clean)
+cudaError_t launch_resolve(const float4 *temp, float4 *clean, float4 *fin, SHData *temp_sh, SHData *clean_sh, int rx, int ry, int rw,
+                           int rh, int w, float k, int srgb, float gamma, bool clamp, bool sh, cudaStream_t st);
+cudaError_t launch_fill(float4 *buf, size_t n, float4 v, cudaStream_t st);
+cudaError_t launch_fill_sh(SHData *buf, size_t n, cudaStream_t st);
+
+} // namespace rg

@@ -1,0 +1,755 @@
+// Kernels of the renderer: sample table, primary rays, shading (with shadow
+// rays traced in the kernel), and the accumulate/tone pass. One thread per
+// ray or pixel; ray counts live on the device so a frame's bounces run back
+// to back without a host round trip.
+#include "render.cuh"
+#include "shade.cuh"
+#include "traverse.cuh"
+
+namespace rg {
+
+using namespace shade;
+using trav::Best;
+using trav::Stack;
+
+namespace {
+
+constexpr int SHADE_BLOCK = 128;
+constexpr float PI_F = 3.141592653589793238463f;
+constexpr float HIT_BIAS = 0.001f;
+constexpr float LIGHT_ATTEN_CUTOFF = 0.001f;
+
+__constant__ int c_primes[HALTON_COUNT] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53, 59, 61, 67, 71, 73, 79, 83, 89};
+// sampling_pattern (src/Ray/internal/Core.cpp:152-160): the 8x8 pixel pattern
+// of UseCoherentSampling
+__constant__ int c_sampling_pattern[64] = {0, 1, 2, 3, 1, 2, 3, 0, 2, 3, 0, 1, 3, 0, 1, 2, 1, 2, 3, 0, 2, 1, 0, 3,
+                                           3, 0, 1, 2, 0, 3, 2, 1, 2, 3, 0, 1, 1, 0, 3, 2, 0, 1, 2, 3, 0, 3, 2, 1,
+                                           3, 2, 1, 0, 3, 2, 1, 0, 1, 0, 3, 2, 2, 1, 0, 3};
+
+// ScrambledRadicalInverse (src/Ray/internal/Halton.h:61-74) for row i, dim k
+// of UpdateHaltonSequence (RendererRef.cpp:327-358).
+__global__ void k_halton_table(const uint16_t *__restrict__ perms, int base_iteration, float *__restrict__ table) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= HALTON_COUNT * HALTON_SEQ_LEN) return;
+    const int i = idx / HALTON_COUNT, k = idx % HALTON_COUNT;
+    int off = 0;
+    for (int j = 0; j < k; j++) off += c_primes[j];
+    const int base = c_primes[k];
+    const uint16_t *perm = perms + off;
+    const float inv_base = __fdiv_rn(1.0f, (float)base);
+    uint64_t a = (uint64_t)(int64_t)(base_iteration + i);
+    uint64_t reversed = 0;
+    float inv_base_n = 1.0f;
+    while (a) {
+        const uint64_t next = a / (uint64_t)base;
+        const uint64_t digit = a - next * (uint64_t)base;
+        reversed = reversed * (uint64_t)base + perm[digit];
+        inv_base_n = __fmul_rn(inv_base_n, inv_base);
+        a = next;
+    }
+    const float v = __fmul_rn(inv_base_n, __fadd_rn(__ull2float_rn(reversed), __fdiv_rn(__fmul_rn(inv_base, (float)perm[0]),
+                                                                                          __fsub_rn(1.0f, inv_base))));
+    const float lim = 1.0f - 1.1920928955078125e-07f;
+    table[idx] = (lim < v) ? lim : v;
+}
+
+// get_pix_dir of GeneratePrimaryRays (CoreRef.cpp:434-438)
+__device__ __forceinline__ V3 pix_dir(const CameraDev &cam, float k, float fov_k, int w, int h, float x, float y, V3 origin) {
+    const float px = 2 * fov_k * x / (float)w - fov_k, py = 2 * fov_k * (-y) / (float)h + fov_k, pz = cam.focus_distance;
+    const V3 p = v3(cam.origin) + (k * px) * v3(cam.side) + py * v3(cam.up) + pz * v3(cam.fwd);
+    return normalize(p - origin);
+}
+
+// GeneratePrimaryRays, CoreRef.cpp:427-505: one thread per pixel of the rect.
+__global__ void k_raygen(CameraDev cam, float k, float fov_k, int iteration, int rx, int ry, int rw, int rh, int w, int h,
+                         const float *__restrict__ halton, float4 *__restrict__ rays, RayPayload *__restrict__ pay,
+                         uint32_t *__restrict__ count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = (uint32_t)rw * (uint32_t)rh;
+    if (i == 0) *count = n;
+    if (i >= n) return;
+    const int x = rx + (int)(i % (uint32_t)rw), y = ry + (int)(i / (uint32_t)rw);
+    const int index = y * w + x;
+    const int hi = (iteration & (HALTON_SEQ_LEN - 1)) * HALTON_COUNT;
+    float fx = (float)x, fy = (float)y;
+    const int hash_val = hash_i(index);
+    const float o1 = construct_float((uint32_t)hash_val), o2 = construct_float((uint32_t)hash_i(hash_val));
+    if (cam.filter == 1) {
+        float tx = frac_modf(halton[hi + 0] + o1);
+        if (tx < 0.5f) tx = sqrtf(2.0f * tx) - 1.0f;
+        else tx = 1.0f - sqrtf(2.0f - 2 * tx);
+        float ty = frac_modf(halton[hi + 1] + o2);
+        if (ty < 0.5f) ty = sqrtf(2.0f * ty) - 1.0f;
+        else ty = 1.0f - sqrtf(2.0f - 2.0f * ty);
+        fx += 0.5f + tx;
+        fy += 0.5f + ty;
+    } else {
+        fx += frac_modf(halton[hi + 0] + o1);
+        fy += frac_modf(halton[hi + 1] + o2);
+    }
+    const float ff1 = cam.focus_factor * (-0.5f + frac_modf(halton[hi + 2 + 0] + o1));
+    const float ff2 = cam.focus_factor * (-0.5f + frac_modf(halton[hi + 2 + 1] + o2));
+    const V3 origin = v3(cam.origin) + v3(cam.side) * ff1 + v3(cam.up) * ff2;
+    const V3 d = pix_dir(cam, k, fov_k, w, h, fx, fy, origin);
+    const V3 dx = pix_dir(cam, k, fov_k, w, h, fx + 1, fy, origin);
+    const V3 dy = pix_dir(cam, k, fov_k, w, h, fx, fy + 1, origin);
+    rays[2ull * i] = make_float4(origin.x, origin.y, origin.z, MAX_DIST);
+    rays[2ull * i + 1] = make_float4(d.x, d.y, d.z, __int_as_float((x << 16) | y));
+    RayPayload p;
+    p.c[0] = p.c[1] = p.c[2] = 1.0f;
+    p.ior = 1.0f;
+    const V3 ddx = dx - d, ddy = dy - d;
+    p.do_dx[0] = p.do_dx[1] = p.do_dx[2] = 0.0f;
+    p.do_dy[0] = p.do_dy[1] = p.do_dy[2] = 0.0f;
+    p.dd_dx[0] = ddx.x; p.dd_dx[1] = ddx.y; p.dd_dx[2] = ddx.z;
+    p.dd_dy[0] = ddy.x; p.dd_dy[1] = ddy.y; p.dd_dy[2] = ddy.z;
+    p.ray_depth = 0;
+    p.pad[0] = p.pad[1] = p.pad[2] = 0;
+    pay[i] = p;
+}
+
+// Shadow ray against the whole scene: the instance loop of
+// Traverse_MacroTree_WithStack_AnyHit (CoreRef.cpp:1224-1368).
+__device__ __forceinline__ Best trace_any(const SceneView &sv, V3 o, V3 d, float tmax, Stack<true> &st, uint32_t &err) {
+    Best best;
+    best.t = tmax;
+    best.u = best.v = 0.0f;
+    best.prim = best.obj = -1;
+    const float sx = trav::safe_inv(d.x), sy = trav::safe_inv(d.y), sz = trav::safe_inv(d.z);
+    const float4 r0 = make_float4(o.x, o.y, o.z, tmax), r1 = make_float4(d.x, d.y, d.z, 0.0f);
+    for (uint32_t m = 0; m < sv.n_inst; m++) {
+        const InstanceRec *ir = sv.inst + m;
+        float bmin[3], bmax[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            bmin[q] = __ldg(&ir->bbox_min[q]);
+            bmax[q] = __ldg(&ir->bbox_max[q]);
+        }
+        if (!trav::ref_bbox_test(o.x, o.y, o.z, sx, sy, sz, best.t, bmin, bmax)) continue;
+        if (trav::trace_mesh_any<true>(trav::mesh_of(sv, ir, (int)m), trav::transform_ray(ir, r0, r1), best, st, err)) break;
+    }
+    return best;
+}
+
+__device__ __forceinline__ void load_vertex(const RenderScene &sc, uint32_t vi, VertexRec &v) {
+    const float *src = reinterpret_cast<const float *>(sc.vertices + vi);
+    float *dst = reinterpret_cast<float *>(&v);
+#pragma unroll
+    for (int q = 0; q < 13; q++) dst[q] = __ldg(src + q);
+}
+
+__device__ __forceinline__ TriRec load_tri(const RenderScene &sc, uint32_t prim) {
+    const float4 *tp = reinterpret_cast<const float4 *>(sc.tris + prim);
+    const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+    TriRec t;
+    t.nu = a.x; t.nv = a.y; t.np = a.z; t.pu = a.w;
+    t.pv = b.x; t.ci = __float_as_int(b.y); t.e0u = b.z; t.e0v = b.w;
+    t.e1u = c.x; t.e1v = c.y; t.mi = __float_as_uint(c.z); t.back_mi = __float_as_uint(c.w);
+    return t;
+}
+
+constexpr uint32_t SHADE_ERR_BAD_INDEX = 8u;   // a material/texture/instance index out of range
+constexpr uint32_t SHADE_ERR_MIX_LOOP = 16u;    // mix materials nested beyond the bound
+constexpr uint32_t SHADE_ERR_SHADOW_LOOP = 32u; // more transparent layers than the bound
+constexpr int MAX_MIX_NESTING = 32;
+constexpr int MAX_SHADOW_LAYERS = 256;
+
+// ComputeVisibility, CoreRef.cpp:1800-1896
+__device__ float compute_visibility(const RenderScene &sc, V3 p1, V3 p2, const float *halton, int hi, int rand_hash2, Stack<true> &st,
+                                    uint32_t &err) {
+    V3 dir = p2 - p1;
+    float dist = length(dir);
+    dir = dir / dist;
+    V3 o = p1;
+    float visibility = 1.0f;
+    int layers = 0;
+    while (dist > HIT_EPS) {
+        if (++layers > MAX_SHADOW_LAYERS) {
+            err |= SHADE_ERR_SHADOW_LOOP;
+            break;
+        }
+        const Best sh = trace_any(sc.sv, o, dir, dist, st, err);
+        if (sh.prim < 0) break;
+        if ((uint32_t)sh.prim >= sc.n_tris || (uint32_t)sh.obj >= sc.sv.n_inst) {
+            err |= SHADE_ERR_BAD_INDEX;
+            break;
+        }
+        const TriRec tri = load_tri(sc, (uint32_t)sh.prim);
+        if (tri.ci & TRI_SOLID_BIT) {
+            visibility = 0;
+            break;
+        }
+        uint32_t mi = tri.mi;
+        const float *inv = sc.sv.inst[sh.obj].inv_xform;
+        VertexRec v1, v2, v3v;
+        load_vertex(sc, sc.vtx_indices[(uint32_t)sh.prim * 3 + 0], v1);
+        load_vertex(sc, sc.vtx_indices[(uint32_t)sh.prim * 3 + 1], v2);
+        load_vertex(sc, sc.vtx_indices[(uint32_t)sh.prim * 3 + 2], v3v);
+        const V3 I = dir;
+        const float w = 1.0f - sh.u - sh.v;
+        const float uvx = v1.t[0][0] * w + v2.t[0][0] * sh.u + v3v.t[0][0] * sh.v;
+        const float uvy = v1.t[0][1] * w + v2.t[0][1] * sh.u + v3v.t[0][1] * sh.v;
+        V3 pn = transform_normal(plane_normal(tri), inv);
+        bool skip = false;
+        const bool is_backfacing = dot(pn, I) < 0.0f;
+        if (is_backfacing) {
+            if (tri.back_mi == RAY_INVALID_INDEX) skip = true;
+            else {
+                mi = tri.back_mi;
+                pn = -pn;
+            }
+        }
+        if (!skip) {
+            const int sh_rand_hash = hash_i(rand_hash2);
+            const float sh_rand_offset = construct_float((uint32_t)sh_rand_hash);
+            float sh_r = frac_modf(halton[hi] + sh_rand_offset);
+            int nest = 0;
+            bool bad = false;
+            while (true) {
+                if (mi >= sc.n_materials) {
+                    bad = true;
+                    err |= SHADE_ERR_BAD_INDEX;
+                    break;
+                }
+                const MaterialRec &mat = sc.materials[mi];
+                if (mat.type != (uint32_t)RAY_MAT_MIX) break;
+                if (++nest > MAX_MIX_NESTING) {
+                    bad = true;
+                    err |= SHADE_ERR_MIX_LOOP;
+                    break;
+                }
+                const float mix_val = sample_bilinear(sc, mat.textures[1], uvx, uvy, 0).x * mat.roughness_or_strength;
+                if (sh_r > mix_val) {
+                    mi = mat.textures[2];
+                    sh_r = (sh_r - mix_val) / (1.0f - mix_val);
+                } else {
+                    mi = mat.textures[3];
+                    sh_r = sh_r / mix_val;
+                }
+            }
+            if (bad || sc.materials[mi].type != (uint32_t)RAY_MAT_TRANSPARENT) {
+                visibility = 0;
+                break;
+            }
+        }
+        const float t = sh.t + HIT_BIAS;
+        o.x += dir.x * t;
+        o.y += dir.y * t;
+        o.z += dir.z * t;
+        dist -= t;
+    }
+    return visibility;
+}
+
+// AcumulateLightContribution, CoreRef.cpp:1898-1933
+__device__ __forceinline__ void accumulate_light(const RenderScene &sc, const LightRec &l, V3 I, V3 P, V3 N, V3 B, V3 plane_N, float sigma,
+                                                 const float *halton, int hi, int rand_hash2, float rand_offset, float rand_offset2, V3 &col,
+                                                 Stack<true> &st, uint32_t &err) {
+    const V3 lpos = v3(l.pos);
+    V3 L = P - lpos;
+    const float distance = length(L);
+    const float d = fmax_std(distance - l.radius, 0.0f);
+    L = L / distance;
+    const float z = frac_modf(halton[hi + 0] + rand_offset);
+    const float dir = sqrtf(z);
+    const float phi = 2 * PI_F * frac_modf(halton[hi + 1] + rand_offset2);
+    const float cos_phi = cr_cos(phi), sin_phi = cr_sin(phi);
+    const V3 TT = cross(L, B);
+    const V3 BB = cross(L, TT);
+    const V3 V = (dir * sin_phi) * BB + sqrtf(1.0f - dir) * L + (dir * cos_phi) * TT;
+    L = normalize(lpos + V * l.radius - P);
+    const float denom = d / l.radius + 1.0f;
+    float atten = 1.0f / (denom * denom);
+    atten = (atten - LIGHT_ATTEN_CUTOFF / l.brightness) / (1.0f - LIGHT_ATTEN_CUTOFF);
+    atten = fmax_std(atten, 0.0f);
+    const float dot1 = fmax_std(dot(L, N), 0.0f);
+    const float dot2 = dot(L, v3(l.dir));
+    if (dot1 > FLT_EPS_ && dot2 > l.spot && (l.brightness * atten) > FLT_EPS_) {
+        const float visibility = compute_visibility(sc, P + HIT_BIAS * plane_N, lpos, halton, hi, rand_hash2, st, err);
+        col = col + v3(l.col) * dot1 * visibility * atten * brdf_oren_nayar(L, I, N, B, sigma);
+    }
+}
+
+struct NewRay {
+    float4 r0, r1;
+    RayPayload p;
+};
+
+// Russian roulette and emission of a continuation ray (CoreRef.cpp:2246-2256)
+__device__ __forceinline__ bool roulette(NewRay &r, bool cant_terminate, float p) {
+    const float lum = fmax_std(r.p.c[0], fmax_std(r.p.c[1], r.p.c[2]));
+    const float q = cant_terminate ? 0.0f : fmax_std(0.05f, 1.0f - lum);
+    if (p >= q) {
+        r.p.c[0] /= 1.0f - q;
+        r.p.c[1] /= 1.0f - q;
+        r.p.c[2] /= 1.0f - q;
+        return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void set3(float *dst, V3 v) {
+    dst[0] = v.x;
+    dst[1] = v.y;
+    dst[2] = v.z;
+}
+
+// ShadeSurface, CoreRef.cpp:2055-2391. Returns the pixel contribution;
+// fills nr and sets emit when the path continues.
+__device__ F4 shade_surface(const RenderScene &sc, const PassInfo &pi, int rand_index, const float *halton, float4 hit, int obj,
+                            float4 r0, float4 r1, const RayPayload &ray, NewRay &nr, bool &emit, Stack<true> &st, uint32_t &err) {
+    emit = false;
+    const int prim = __float_as_int(hit.x);
+    const V3 I = v3(r1.x, r1.y, r1.z);
+    const uint32_t xy = __float_as_uint(r1.w);
+    if (prim < 0) {
+        F4 env = {0.0f, 0.0f, 0.0f, 0.0f};
+        if (!(pi.flags & PASS_NO_BACKGROUND) || pi.bounce > 2) {
+            env = sample_latlong_rgbe(sc, sc.env_map, I);
+            if (sc.env_clamp > FLT_EPS_) {
+                const float c = sc.env_clamp;
+                env.x = env.x < c ? env.x : c;
+                env.y = env.y < c ? env.y : c;
+                env.z = env.z < c ? env.z : c;
+                env.w = env.w < c ? env.w : c;
+            }
+            env.w = 1.0f;
+        }
+        return F4{ray.c[0] * env.x * sc.env_col[0], ray.c[1] * env.y * sc.env_col[1], ray.c[2] * env.z * sc.env_col[2], env.w};
+    }
+    if ((uint32_t)prim >= sc.n_tris || (uint32_t)obj >= sc.sv.n_inst) {
+        err |= SHADE_ERR_BAD_INDEX;
+        return F4{0.0f, 0.0f, 0.0f, 0.0f};
+    }
+    const float t = hit.y, hu = hit.z, hv = hit.w;
+    const V3 P = v3(r0.x, r0.y, r0.z) + t * I;
+    const TriRec tri = load_tri(sc, (uint32_t)prim);
+    uint32_t mi = tri.mi;
+    const float *inv = sc.sv.inst[obj].inv_xform;
+    VertexRec v1, v2, v3v;
+    load_vertex(sc, sc.vtx_indices[(uint32_t)prim * 3 + 0], v1);
+    load_vertex(sc, sc.vtx_indices[(uint32_t)prim * 3 + 1], v2);
+    load_vertex(sc, sc.vtx_indices[(uint32_t)prim * 3 + 2], v3v);
+
+    const float w = 1.0f - hu - hv;
+    V3 N = v3(v1.n) * w + v3(v2.n) * hu + v3(v3v.n) * hv;
+    const float uvx = v1.t[0][0] * w + v2.t[0][0] * hu + v3v.t[0][0] * hv;
+    const float uvy = v1.t[0][1] * w + v2.t[0][1] * hu + v3v.t[0][1] * hv;
+
+    V3 plane_N = transform_normal(plane_normal(tri), inv);
+    const bool is_backfacing = dot(plane_N, I) > 0.0f;
+    if (is_backfacing) {
+        if (tri.back_mi == RAY_INVALID_INDEX) return F4{0.0f, 0.0f, 0.0f, 0.0f};
+        mi = tri.back_mi;
+        plane_N = -plane_N;
+        N = -N;
+    }
+
+    Derivs der;
+    compute_derivatives(I, t, v3(ray.do_dx), v3(ray.do_dy), v3(ray.dd_dx), v3(ray.dd_dy), v1, v2, v3v, plane_N, der);
+
+    const int rand_hash = hash_i(rand_index), rand_hash2 = hash_i(rand_hash), rand_hash3 = hash_i(rand_hash2);
+    const float rand_offset = construct_float((uint32_t)rand_hash), rand_offset2 = construct_float((uint32_t)rand_hash2),
+                rand_offset3 = construct_float((uint32_t)rand_hash3);
+    const int hi = (pi.iteration & (HALTON_SEQ_LEN - 1)) * HALTON_COUNT + pi.bounce * 2;
+
+    float mix_rand = frac_modf(halton[hi] + rand_offset);
+    int nest = 0;
+    while (true) {
+        if (mi >= sc.n_materials) {
+            err |= SHADE_ERR_BAD_INDEX;
+            return F4{0.0f, 0.0f, 0.0f, 0.0f};
+        }
+        const MaterialRec &mat = sc.materials[mi];
+        if (mat.type != (uint32_t)RAY_MAT_MIX) break;
+        if (++nest > MAX_MIX_NESTING) {
+            err |= SHADE_ERR_MIX_LOOP;
+            return F4{0.0f, 0.0f, 0.0f, 0.0f};
+        }
+        float mix_val = sample_bilinear(sc, mat.textures[1], uvx, uvy, 0).x * mat.roughness_or_strength;
+        const float mix_ior = is_backfacing ? mat.ext_ior : mat.int_ior;
+        float R0 = (ray.ior - mix_ior) / (ray.ior + mix_ior);
+        R0 *= R0;
+        float RR;
+        if (ray.ior > mix_ior) {
+            const float eta = ray.ior / mix_ior;
+            const float cosi = -dot(I, N);
+            const float cost2 = 1.0f - eta * eta * (1.0f - cosi * cosi);
+            if (cost2 >= 0.0f) {
+                const float m = eta * cosi - sqrtf(cost2);
+                const V3 V = eta * I + m * N;
+                RR = R0 + (1.0f - R0) * pow5(1.0f + dot(V, N));
+            } else {
+                RR = 1.0f;
+            }
+        } else {
+            RR = R0 + (1.0f - R0) * pow5(1.0f + dot(I, N));
+        }
+        mix_val *= clampf_ref(RR, 0.0f, 1.0f);
+        if (mix_rand > mix_val) {
+            mi = mat.textures[2];
+            mix_rand = (mix_rand - mix_val) / (1.0f - mix_val);
+        } else {
+            mi = mat.textures[3];
+            mix_rand = mix_rand / mix_val;
+        }
+    }
+    const MaterialRec &mat = sc.materials[mi];
+
+    // normal map
+    V3 B = v3(v1.b) * w + v3(v2.b) * hu + v3(v3v.b) * hv;
+    V3 T = cross(B, N);
+    F4 nm = sample_bilinear(sc, mat.textures[0], uvx, uvy, 0);
+    nm.x = nm.x * 2.0f - 1.0f;
+    nm.y = nm.y * 2.0f - 1.0f;
+    nm.z = nm.z * 2.0f - 1.0f;
+    N = nm.x * B + nm.z * N + nm.y * T;
+    N = transform_normal(N, inv);
+    B = transform_normal(B, inv);
+    T = transform_normal(T, inv);
+
+    // main texture
+    const uint32_t main_tex = mat.textures[1];
+    const float albedo_lod = texture_lod(sc, main_tex, der.duv_dx[0], der.duv_dx[1], der.duv_dy[0], der.duv_dy[1]);
+    F4 albedo = sample_bilinear(sc, main_tex, uvx, uvy, f2i_x86(albedo_lod));
+    if (main_tex < sc.n_textures && (sc.textures[main_tex].width & 0x8000u)) albedo = srgb_to_rgb(albedo);
+    albedo.x *= mat.main_color[0];
+    albedo.y *= mat.main_color[1];
+    albedo.z *= mat.main_color[2];
+    const V3 alb = v3(albedo.x, albedo.y, albedo.z);
+
+    V3 col = v3(0.0f, 0.0f, 0.0f);
+    const int diff_depth = ray.ray_depth & 0xff, gloss_depth = (ray.ray_depth >> 8) & 0xff, refr_depth = (ray.ray_depth >> 16) & 0xff,
+              transp_depth = (ray.ray_depth >> 24) & 0xff;
+    const int total_depth = diff_depth + gloss_depth + refr_depth + transp_depth;
+    const bool cant_terminate = total_depth < pi.termination_start_depth;
+    const bool consider_albedo = !(pi.flags & PASS_LIGHTING_ONLY) || pi.bounce > 2;
+
+    nr.r1.w = __uint_as_float(xy);
+    nr.p.ior = ray.ior;
+    nr.p.pad[0] = nr.p.pad[1] = nr.p.pad[2] = 0;
+    const float dot_I_pN = dot(I, plane_N);
+
+    if (mat.type == (uint32_t)RAY_MAT_DIFFUSE) {
+        if (!(pi.flags & PASS_SKIP_DIRECT) || pi.bounce > 2) {
+            for (uint32_t li = 0; li < sc.n_lights; li++)
+                accumulate_light(sc, sc.lights[li], I, P, N, B, plane_N, mat.roughness_or_strength, halton, hi, rand_hash2, rand_offset,
+                                 rand_offset2, col, st, err);
+            if (consider_albedo) col = col * alb;
+        }
+        if (diff_depth < pi.max_diff_depth && total_depth < pi.max_total_depth) {
+            const float u1 = frac_modf(halton[hi + 0] + rand_offset);
+            const float u2 = frac_modf(halton[hi + 1] + rand_offset2);
+            const float phi = 2 * PI_F * u2;
+            const float cos_phi = cr_cos(phi), sin_phi = cr_sin(phi);
+            V3 V;
+            float weight = 1.0f;
+            if ((pi.flags & PASS_OUTPUT_SH) && pi.bounce <= 2) {
+                const float dir = sqrtf(1.0f - u1 * u1);
+                V = (dir * sin_phi) * B + u1 * N + (dir * cos_phi) * T;
+                weight = 2 * u1;
+            } else {
+                const float dir = sqrtf(u1);
+                V = (dir * sin_phi) * B + sqrtf(1.0f - u1) * N + (dir * cos_phi) * T;
+            }
+            weight *= brdf_oren_nayar(V, I, N, B, mat.roughness_or_strength);
+            nr.p.ray_depth = ray.ray_depth + 0x00000001;
+            const V3 o = P + HIT_BIAS * plane_N;
+            nr.r0 = make_float4(o.x, o.y, o.z, MAX_DIST);
+            nr.r1.x = V.x; nr.r1.y = V.y; nr.r1.z = V.z;
+            nr.p.c[0] = ray.c[0] * weight;
+            nr.p.c[1] = ray.c[1] * weight;
+            nr.p.c[2] = ray.c[2] * weight;
+            if (consider_albedo) {
+                nr.p.c[0] *= albedo.x;
+                nr.p.c[1] *= albedo.y;
+                nr.p.c[2] *= albedo.z;
+            }
+            set3(nr.p.do_dx, der.do_dx);
+            set3(nr.p.do_dy, der.do_dy);
+            set3(nr.p.dd_dx, der.dd_dx - 2 * (dot_I_pN * der.dndx + der.ddn_dx * plane_N));
+            set3(nr.p.dd_dy, der.dd_dy - 2 * (dot_I_pN * der.dndy + der.ddn_dy * plane_N));
+            emit = roulette(nr, cant_terminate, frac_modf(halton[hi + 0] + rand_offset3));
+        }
+    } else if (mat.type == (uint32_t)RAY_MAT_GLOSSY) {
+        if (gloss_depth < pi.max_glossy_depth && total_depth < pi.max_total_depth) {
+            V3 V = reflect(I, N);
+            const float rough = mat.roughness_or_strength;
+            const float h = 1.0f - cr_cos(0.5f * PI_F * rough * rough);
+            const float z = h * frac_modf(halton[hi + 0] + rand_offset);
+            const float dir = sqrtf(z);
+            const float phi = 2 * PI_F * frac_modf(halton[hi + 1] + rand_offset2);
+            const float cos_phi = cr_cos(phi), sin_phi = cr_sin(phi);
+            const V3 TT = cross(V, B);
+            const V3 BB = cross(V, TT);
+            if (dot(V, plane_N) > 0) {
+                V = (dir * sin_phi) * BB + sqrtf(1.0f - dir) * V + (dir * cos_phi) * TT;
+            } else {
+                V = (-dir * sin_phi) * BB + sqrtf(1.0f - dir) * V - (dir * cos_phi) * TT;
+            }
+            nr.p.ray_depth = ray.ray_depth + 0x00000100;
+            const V3 o = P + HIT_BIAS * plane_N;
+            nr.r0 = make_float4(o.x, o.y, o.z, MAX_DIST);
+            nr.r1.x = V.x; nr.r1.y = V.y; nr.r1.z = V.z;
+            nr.p.c[0] = ray.c[0];
+            nr.p.c[1] = ray.c[1];
+            nr.p.c[2] = ray.c[2];
+            if (consider_albedo) {
+                nr.p.c[0] *= albedo.x;
+                nr.p.c[1] *= albedo.y;
+                nr.p.c[2] *= albedo.z;
+            }
+            set3(nr.p.do_dx, der.do_dx);
+            set3(nr.p.do_dy, der.do_dy);
+            set3(nr.p.dd_dx, der.dd_dx - 2 * (dot_I_pN * der.dndx + der.ddn_dx * plane_N));
+            set3(nr.p.dd_dy, der.dd_dy - 2 * (dot_I_pN * der.dndy + der.ddn_dy * plane_N));
+            emit = roulette(nr, cant_terminate, frac_modf(halton[hi + 0] + rand_offset3));
+        }
+    } else if (mat.type == (uint32_t)RAY_MAT_REFRACTIVE) {
+        if (refr_depth < pi.max_refr_depth && total_depth < pi.max_total_depth) {
+            const float ior = is_backfacing ? mat.ext_ior : mat.int_ior;
+            const float eta = ray.ior / ior;
+            const float cosi = -dot(I, N);
+            const float cost2 = 1.0f - eta * eta * (1.0f - cosi * cosi);
+            if (cost2 < 0) return F4{0.0f, 0.0f, 0.0f, 1.0f};
+            const float m = eta * cosi - sqrtf(cost2);
+            V3 V = eta * I + m * N;
+            const float z = 1.0f - halton[hi + 0] * mat.roughness_or_strength;
+            const float temp = sqrtf(1.0f - z * z);
+            const int hj = (int)(((uint32_t)(hash_i(hi) + pi.iteration) & (HALTON_SEQ_LEN - 1)) * HALTON_COUNT) + pi.bounce * 2;
+            const float phi = halton[hj + 0] * 2 * PI_F;
+            const float cos_phi = cr_cos(phi), sin_phi = cr_sin(phi);
+            const V3 TT = normalize(cross(V, B));
+            const V3 BB = normalize(cross(V, TT));
+            V = (temp * sin_phi) * BB + z * V + (temp * cos_phi) * TT;
+            const float kk = (eta - eta * eta * dot(I, plane_N) / dot(V, plane_N));
+            const float dmdx = kk * der.ddn_dx, dmdy = kk * der.ddn_dy;
+            nr.p.ior = ior;
+            nr.p.ray_depth = ray.ray_depth + 0x00010000;
+            const V3 o = P + HIT_BIAS * I;
+            nr.r0 = make_float4(o.x, o.y, o.z, MAX_DIST);
+            nr.r1.x = V.x; nr.r1.y = V.y; nr.r1.z = V.z;
+            nr.p.c[0] = ray.c[0] * z;
+            nr.p.c[1] = ray.c[1] * z;
+            nr.p.c[2] = ray.c[2] * z;
+            set3(nr.p.do_dx, der.do_dx);
+            set3(nr.p.do_dy, der.do_dy);
+            set3(nr.p.dd_dx, eta * der.dd_dx - (m * der.dndx + dmdx * plane_N));
+            set3(nr.p.dd_dy, eta * der.dd_dy - (m * der.dndy + dmdy * plane_N));
+            emit = roulette(nr, cant_terminate, frac_modf(halton[hi + 0] + rand_offset3));
+        }
+    } else if (mat.type == (uint32_t)RAY_MAT_EMISSIVE) {
+        col = mat.roughness_or_strength * alb;
+    } else if (mat.type == (uint32_t)RAY_MAT_TRANSPARENT) {
+        if (transp_depth < pi.max_transp_depth && total_depth < pi.max_total_depth) {
+            nr.p.ray_depth = ray.ray_depth + 0x01000000;
+            const V3 o = P + HIT_BIAS * I;
+            nr.r0 = make_float4(o.x, o.y, o.z, MAX_DIST);
+            nr.r1.x = I.x; nr.r1.y = I.y; nr.r1.z = I.z;
+            for (int q = 0; q < 3; q++) {
+                nr.p.c[q] = ray.c[q];
+                nr.p.do_dx[q] = ray.do_dx[q];
+                nr.p.do_dy[q] = ray.do_dy[q];
+                nr.p.dd_dx[q] = ray.dd_dx[q];
+                nr.p.dd_dy[q] = ray.dd_dy[q];
+            }
+            emit = roulette(nr, cant_terminate, frac_modf(halton[hi + 0] + rand_offset3));
+        }
+    }
+    return F4{ray.c[0] * col.x, ray.c[1] * col.y, ray.c[2] * col.z, 1.0f};
+}
+
+template <bool PRIMARY>
+__global__ void __launch_bounds__(SHADE_BLOCK) k_shade(RenderScene sc, PassInfo pi, const float *__restrict__ halton,
+                                                       const float4 *__restrict__ rays, const RayPayload *__restrict__ pay,
+                                                       const float4 *__restrict__ hits, const int32_t *__restrict__ obj,
+                                                       const uint32_t *__restrict__ in_count, uint32_t max_rays, float4 *__restrict__ out_rays,
+                                                       RayPayload *__restrict__ out_pay, uint32_t *__restrict__ out_count,
+                                                       float4 *__restrict__ temp, SHData *__restrict__ temp_sh, uint32_t *__restrict__ err_out) {
+    __shared__ uint2 s_stack[trav::SMEM_STACK * SHADE_BLOCK];
+    Stack<true> st;
+    st.smem = s_stack + threadIdx.x;
+    st.sp = 0;
+    uint32_t err = 0;
+    const uint32_t n = min(*in_count, max_rays);
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * SHADE_BLOCK; base < n; base += gridDim.x * SHADE_BLOCK) {
+        const uint32_t i = base + threadIdx.x;
+        bool emit = false;
+        NewRay nr;
+        if (i < n) {
+            const float4 r0 = rays[2ull * i], r1 = rays[2ull * i + 1];
+            const RayPayload p = pay[i];
+            const uint32_t xy = __float_as_uint(r1.w);
+            const int x = (int)(xy >> 16), y = (int)(xy & 0xffffu);
+            const int index = y * pi.w + x;
+            const int rand_index = (pi.flags & PASS_COHERENT) ? c_sampling_pattern[(y % 8) * 8 + (x % 8)] : index;
+            const F4 c = shade_surface(sc, pi, rand_index, halton, hits[i], obj[i], r0, r1, p, nr, emit, st, err);
+            if (PRIMARY) {
+                temp[index] = make_float4(c.x, c.y, c.z, c.w);
+                if (temp_sh) {
+                    // ResetSampleData + SetSampleDir/SetSampleWeight (FramebufferRef.h:69-88)
+                    SHData &s = temp_sh[index];
+                    s.coeff_g[0] = 0.0f;
+                    if (emit) {
+                        const float SH_Y0 = 0.282094806f, SH_Y1 = 0.488602519f;
+                        s.coeff_r[0] = SH_Y0;
+                        s.coeff_r[1] = SH_Y1 * nr.r1.y;
+                        s.coeff_r[2] = SH_Y1 * nr.r1.z;
+                        s.coeff_r[3] = SH_Y1 * nr.r1.x;
+                        s.coeff_g[0] = nr.p.c[0];
+                    }
+                }
+            } else {
+                float4 acc = temp[index];
+                acc.x += c.x;
+                acc.y += c.y;
+                acc.z += c.z;
+                acc.w += 0.0f;
+                temp[index] = acc;
+            }
+        }
+        // warp-aggregated append of the continuation rays
+        const uint32_t m = __ballot_sync(0xffffffffu, emit);
+        if (m) {
+            uint32_t slot = 0;
+            const uint32_t leader = __ffs(m) - 1;
+            if (lane == leader) slot = atomicAdd(out_count, (uint32_t)__popc(m));
+            slot = __shfl_sync(0xffffffffu, slot, leader) + __popc(m & ((1u << lane) - 1u));
+            if (emit && slot < max_rays) {
+                out_rays[2ull * slot] = nr.r0;
+                out_rays[2ull * slot + 1] = nr.r1;
+                out_pay[slot] = nr.p;
+            }
+        }
+    }
+    if (err) atomicOr(err_out, err);
+}
+
+// Framebuffer::MixWith, ComputeSHData, MixWith_SH (FramebufferRef.cpp:57-101)
+// and the tone step of RenderScene (RendererRef.cpp:301-324).
+__global__ void k_resolve(const float4 *__restrict__ temp, float4 *__restrict__ clean, float4 *__restrict__ fin, SHData *__restrict__ temp_sh,
+                          SHData *__restrict__ clean_sh, int rx, int ry, int rw, int rh, int w, float k, int srgb, float gamma, int clamp,
+                          int sh) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint32_t)rw * (uint32_t)rh) return;
+    const int x = rx + (int)(i % (uint32_t)rw), y = ry + (int)(i / (uint32_t)rw);
+    const size_t idx = (size_t)y * w + x;
+    const float4 p = temp[idx];
+    float4 c = clean[idx];
+    c.x += (p.x - c.x) * k;
+    c.y += (p.y - c.y) * k;
+    c.z += (p.z - c.z) * k;
+    c.w += (p.w - c.w) * k;
+    clean[idx] = c;
+    if (sh) {
+        SHData s = temp_sh[idx];
+        const float inv_weight = s.coeff_g[0] > FLT_EPS_ ? (2.0f * PI_F / s.coeff_g[0]) : 0.0f;
+        const float pr = p.x * inv_weight, pg = p.y * inv_weight, pb = p.z * inv_weight;
+        for (int j = 0; j < 4; j++) {
+            s.coeff_g[j] = s.coeff_r[j] * pg;
+            s.coeff_b[j] = s.coeff_r[j] * pb;
+            s.coeff_r[j] = s.coeff_r[j] * pr;
+        }
+        temp_sh[idx] = s;
+        SHData o = clean_sh[idx];
+        for (int j = 0; j < 4; j++) {
+            o.coeff_r[j] += (s.coeff_r[j] - o.coeff_r[j]) * k;
+            o.coeff_g[j] += (s.coeff_g[j] - o.coeff_g[j]) * k;
+            o.coeff_b[j] += (s.coeff_b[j] - o.coeff_b[j]) * k;
+        }
+        clean_sh[idx] = o;
+    }
+    float v[4] = {c.x, c.y, c.z, c.w};
+    if (srgb) {
+        for (int q = 0; q < 3; q++) {
+            if (v[q] > 0.0031308f) v[q] = cr_pow(1.055f * v[q], (1.0f / 2.4f)) - 0.055f;
+            else v[q] = 12.92f * v[q];
+        }
+    }
+    if (gamma != 1.0f) {
+        const float g = 1.0f / gamma;
+        for (int q = 0; q < 4; q++) v[q] = cr_pow(v[q], g);
+    }
+    if (clamp) {
+        for (int q = 0; q < 4; q++) {
+            const float t = v[q] < 1.0f ? v[q] : 1.0f; // minps(v, 1)
+            v[q] = 0.0f > t ? 0.0f : t;               // maxps(0, t)
+        }
+    }
+    fin[idx] = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+__global__ void k_fill(float4 *buf, size_t n, float4 v) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) buf[i] = v;
+}
+
+__global__ void k_fill_sh(SHData *buf, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        SHData z;
+        for (int j = 0; j < 4; j++) z.coeff_r[j] = z.coeff_g[j] = z.coeff_b[j] = 0.0f;
+        buf[i] = z;
+    }
+}
+
+int g_shade_blocks = 0;
+
+} // namespace
+
+cudaError_t launch_halton_table(const uint16_t *perms, int base_iteration, float *table, cudaStream_t st) {
+    k_halton_table<<<(HALTON_COUNT * HALTON_SEQ_LEN + 255) / 256, 256, 0, st>>>(perms, base_iteration, table);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_raygen(const CameraDev &cam, float k, float fov_k, int iteration, int rx, int ry, int rw, int rh, int w, int h,
+                          const float *halton, float4 *rays, RayPayload *pay, uint32_t *count, cudaStream_t st) {
+    const uint32_t n = (uint32_t)rw * (uint32_t)rh;
+    k_raygen<<<(n + 255) / 256, 256, 0, st>>>(cam, k, fov_k, iteration, rx, ry, rw, rh, w, h, halton, rays, pay, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shade(const RenderScene &sc, const PassInfo &pi, const float *halton, const float4 *rays, const RayPayload *pay,
+                         const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays, float4 *out_rays,
+                         RayPayload *out_pay, uint32_t *out_count, float4 *temp, SHData *temp_sh, bool primary, uint32_t *err,
+                         cudaStream_t st) {
+    if (g_shade_blocks == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_shade<false>, SHADE_BLOCK, 0);
+        g_shade_blocks = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 4);
+    }
+    const uint32_t need = (max_rays + SHADE_BLOCK - 1) / SHADE_BLOCK;
+    const uint32_t blocks = need < (uint32_t)g_shade_blocks ? (need > 0 ? need : 1) : (uint32_t)g_shade_blocks;
+    if (primary)
+        k_shade<true><<<blocks, SHADE_BLOCK, 0, st>>>(sc, pi, halton, rays, pay, hits, obj, in_count, max_rays, out_rays, out_pay, out_count, temp,
+                                                      temp_sh, err);
+    else
+        k_shade<false><<<blocks, SHADE_BLOCK, 0, st>>>(sc, pi, halton, rays, pay, hits, obj, in_count, max_rays, out_rays, out_pay, out_count,
+                                                       temp, temp_sh, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_resolve(const float4 *temp, float4 *clean, float4 *fin, SHData *temp_sh, SHData *clean_sh, int rx, int ry, int rw, int rh,
+                           int w, float k, int srgb, float gamma, bool clamp, bool sh, cudaStream_t st) {
+    const uint32_t n = (uint32_t)rw * (uint32_t)rh;
+    k_resolve<<<(n + 255) / 256, 256, 0, st>>>(temp, clean, fin, temp_sh, clean_sh, rx, ry, rw, rh, w, k, srgb, gamma, clamp ? 1 : 0,
+                                               sh ? 1 : 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill(float4 *buf, size_t n, float4 v, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_fill<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(buf, n, v);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_sh(SHData *buf, size_t n, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_fill_sh<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(buf, n);
+    return cudaGetLastError();
+}
+
+} // namespace rg

@@ -10,40 +10,28 @@
 #include "../../include/raygpu.h"
 #include "bvh.cuh"
 #include "common.cuh"
+#include "render.cuh"
 
 namespace rg {
 
-// material_t (src/Ray/internal/Core.h:121-131): textures[] holds the normal
-// map, the main texture and, for mix materials, the two mixed materials.
-struct MaterialRec {
-    uint32_t textures[4];
-    float main_color[3], pad;
-    uint32_t type;
-    float roughness_or_strength;
-    float int_ior, ext_ior;
-};
-static_assert(sizeof(MaterialRec) == 48, "MaterialRec must stay 48 bytes");
-
-// light_t (Core.h:133-138)
-struct LightRec {
-    float pos[3], radius;
-    float col[3], brightness;
-    float dir[3], spot;
-};
-static_assert(sizeof(LightRec) == 48, "LightRec must stay 48 bytes");
-
-// vertex_t (Core.h:259-262)
-struct VertexRec {
-    float p[3], n[3], b[3], t[2][2];
-};
-static_assert(sizeof(VertexRec) == 52, "VertexRec must stay 52 bytes");
-
+// A texture with its mip chain (RGBA8, one uint32 per texel) and the atlas
+// position the reference's splitter gives each level (texture_t, Core.h:103-108).
 struct TextureRec {
     int w = 0, h = 0;
-    bool srgb = true, mips = false;
-    std::vector<uint8_t> rgba; // level 0 followed by the mip chain when mips
-    std::vector<uint32_t> level_offset, level_w, level_h;
-    bool alive = true;
+    bool srgb = true;
+    std::vector<std::vector<uint32_t>> levels;
+    std::vector<int> lw, lh;
+    uint16_t pos[NUM_MIP_LEVELS][2] = {};
+    uint8_t page[NUM_MIP_LEVELS] = {};
+};
+
+// Node of the guillotine splitter that places textures in the reference's
+// atlas pages (TextureSplitter, src/Ray/internal/TextureSplitter.cpp).
+struct SplitNode {
+    int parent = -1;
+    int child[2] = {-1, -1};
+    int pos[2] = {0, 0}, size[2] = {0, 0};
+    bool is_free = true;
 };
 
 struct MeshRec {
@@ -77,6 +65,15 @@ struct DeviceBuf {
     ~DeviceBuf() { release(); }
 };
 
+// api.cu: builds pending BVHs and uploads pending scene data
+int commit(ray_scene *s);
+
+// scene_shading.cu
+int add_texture(ray_scene *s, const uint8_t *data, int w, int h, bool srgb, bool mips, uint32_t *out);
+void compute_tangent_basis(std::vector<VertexRec> &vertices, std::vector<uint32_t> &indices, size_t vtx_start);
+int upload_shading(ray_scene *s); // device copies of vertices, materials, textures and lights
+RenderScene render_scene_view(const ray_scene *s);
+
 } // namespace rg
 
 struct ray_scene {
@@ -86,6 +83,7 @@ struct ray_scene {
     std::vector<rg::InstanceRecHost> instances;
     std::vector<rg::MaterialRec> materials;
     std::vector<rg::TextureRec> textures;
+    std::vector<std::vector<rg::SplitNode>> atlas_pages;
     std::vector<rg::LightRec> lights;
     std::vector<rg::CameraRec> cameras;
     uint32_t cam_first_free = RAY_INVALID_INDEX, current_cam = RAY_INVALID_INDEX;
@@ -96,12 +94,13 @@ struct ray_scene {
     std::vector<rg::VertexRec> vertices;
     std::vector<uint32_t> vtx_indices;
 
-    bool geom_dirty = true;
-    uint32_t total_tris = 0, total_nodes = 0;
+    bool geom_dirty = true, shade_dirty = true;
+    uint32_t total_tris = 0, total_nodes = 0, max_depth = 0;
 
     // device arrays assembled at commit
     rg::DeviceBuf d_nodes, d_leaf, d_inst, d_tris_ref;
     uint32_t n_inst_dev = 0;
+    rg::DeviceBuf d_vertices, d_vtx_indices, d_materials, d_textures, d_texels, d_lights;
 
     // batch-trace staging and diagnostics
     rg::DeviceBuf d_rays, d_hits, d_obj, d_err, d_counters, d_next_ray;
@@ -120,6 +119,24 @@ struct ray_renderer {
     cudaStream_t stream = nullptr;
     ray_stats stats{};
     std::vector<ray_pixel> host_pixels;
+    std::vector<ray_shl1> host_sh;
     rg::DeviceBuf d_sort_scratch;
+
+    // framebuffers (w * h): the sample being accumulated, the running mean,
+    // the toned output; spherical-harmonics data when a camera asks for it
+    rg::DeviceBuf d_temp, d_clean, d_final, d_temp_sh, d_clean_sh;
+    // wavefront: two ray buffers (trace record + payload), hits, instance ids,
+    // counters [0..1] ray counts, [2] persistent-trace work counter, [3] errors
+    rg::DeviceBuf d_rays[2], d_pay[2], d_hits, d_obj, d_counters;
+    rg::DeviceBuf d_halton, d_perms;
+    int halton_base = -1; // base iteration of the table in d_halton
+    bool pixels_on_host = false, sh_on_host = false;
+    // phase events of the last two frames (stats): start, after ray generation,
+    // primary trace and shade, two per bounce, and the frame's end
+    static constexpr int N_EVENTS = 25;
+    cudaEvent_t ev_sets[2][N_EVENTS] = {};
+    bool ev_frame_pending[2] = {false, false};
+    int ev_bounces[2] = {0, 0};
+    uint64_t frame = 0;
     ~ray_renderer();
 };

@@ -48,11 +48,12 @@ __device__ __forceinline__ void flush_counters(uint32_t err, uint32_t nvis, uint
 template <bool COUNT, bool DEEP>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, const float4 *__restrict__ rays, uint32_t n, float4 *__restrict__ hits,
                                                                int32_t *__restrict__ obj_out, uint32_t *__restrict__ err_out,
-                                                               unsigned long long *__restrict__ counters) {
+                                                               unsigned long long *__restrict__ counters, const uint32_t *__restrict__ n_dev) {
     __shared__ uint2 s_stack[SMEM_STACK * TRACE_BLOCK];
     Stack<DEEP> st;
     st.smem = s_stack + threadIdx.x;
     st.sp = 0;
+    if (n_dev) n = min(n, *n_dev);
     const uint32_t i = blockIdx.x * TRACE_BLOCK + threadIdx.x;
     uint32_t err = 0, nvis = 0, ntri = 0;
     if (i < n) {
@@ -89,7 +90,9 @@ template <bool COUNT, bool DEEP>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, const float4 *__restrict__ rays, uint32_t n,
                                                                   float4 *__restrict__ hits, int32_t *__restrict__ obj_out,
                                                                   uint32_t *__restrict__ err_out, unsigned long long *__restrict__ counters,
-                                                                  uint32_t *__restrict__ next_ray, int refill_min) {
+                                                                  uint32_t *__restrict__ next_ray, int refill_min,
+                                                                  const uint32_t *__restrict__ n_dev) {
+    if (n_dev) n = min(n, *n_dev);
     __shared__ uint2 s_stack[SMEM_STACK * TRACE_BLOCK];
     Stack<DEEP> st;
     st.smem = s_stack + threadIdx.x;
@@ -207,9 +210,9 @@ cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, flo
     if (!tp.persistent) {
         const uint32_t grid = (n + TRACE_BLOCK - 1) / TRACE_BLOCK;
         if (count)
-            k_trace_closest<true, DEEP><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters);
+            k_trace_closest<true, DEEP><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.count);
         else
-            k_trace_closest<false, DEEP><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters);
+            k_trace_closest<false, DEEP><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.count);
         return cudaGetLastError();
     }
     if (!tp.next_ray) return cudaErrorInvalidValue;
@@ -225,9 +228,11 @@ cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, flo
     cudaError_t e = cudaMemsetAsync(tp.next_ray, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     if (count)
-        k_trace_persistent<true, DEEP><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min);
+        k_trace_persistent<true, DEEP><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min,
+                                                                        tp.count);
     else
-        k_trace_persistent<false, DEEP><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min);
+        k_trace_persistent<false, DEEP><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min,
+                                                                         tp.count);
     return cudaGetLastError();
 }
 

@@ -24,6 +24,7 @@ struct TraceParams {
     int refill_min = 8;     // refill a warp's idle lanes once at least this many are idle
     uint32_t max_depth = 0; // deepest wide BVH among the traced meshes (sizes the stack)
     uint32_t *next_ray = nullptr; // device work counter for the persistent kernel
+    const uint32_t *count = nullptr; // device ray count: when set, min(n, *count) rays are traced
 };
 
 // rays: n x 8 floats (ox, oy, oz, tmax, dx, dy, dz, unused).

@@ -215,12 +215,14 @@ __device__ __forceinline__ bool node_step(const MeshRef &mr, const LocalRay &r, 
     return true;
 }
 
-// One triangle test; updates best when it is the closer hit.
-template <bool COUNT>
-__device__ __forceinline__ void tri_test(const MeshRef &mr, const LocalRay &r, uint32_t li, Best &best, uint32_t &err, uint32_t &ntri) {
+// One triangle test; updates best when it is the closer hit. With SOLID,
+// returns whether that hit is on a solid triangle (TRI_SOLID_BIT), which ends
+// a shadow ray's search (IntersectTris_AnyHit, CoreRef.cpp:804-829).
+template <bool COUNT, bool SOLID = false>
+__device__ __forceinline__ bool tri_test(const MeshRef &mr, const LocalRay &r, uint32_t li, Best &best, uint32_t &err, uint32_t &ntri) {
     if (li >= mr.tri_count) {
         err |= TRACE_ERR_BOUNDS;
-        return;
+        return false;
     }
     const float4 *tp = reinterpret_cast<const float4 *>(mr.tris + li);
     const float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
@@ -247,8 +249,10 @@ __device__ __forceinline__ void tri_test(const MeshRef &mr, const LocalRay &r, u
             best.v = __fmul_rn(detv, rdet);
             best.prim = gp;
             best.obj = mr.obj;
+            if (SOLID) return (__float_as_int(t1.y) & TRI_SOLID_BIT) != 0;
         }
     }
+    return false;
 }
 
 // Whole traversal of one mesh for one ray (the one-thread-per-ray kernel).
@@ -269,6 +273,30 @@ __device__ __forceinline__ void trace_mesh(const MeshRef &mr, const LocalRay &r,
         }
         if (ng_bits <= 0x00FFFFFFu) {
             if (st.sp == 0) return;
+            const uint2 e = st.pop();
+            ng_base = e.x;
+            ng_bits = e.y;
+        }
+    }
+}
+
+// Shadow-ray traversal of one mesh (Traverse_MicroTree_WithStack_AnyHit,
+// CoreRef.cpp:1470-1577): closest-hit order, stopping at the first accepted
+// hit on a solid triangle. Returns true when it stopped there.
+template <bool DEEP>
+__device__ __forceinline__ bool trace_mesh_any(const MeshRef &mr, const LocalRay &r, Best &best, Stack<DEEP> &st, uint32_t &err) {
+    uint32_t ng_base = 0, ng_bits = (1u << (24 + r.oct)) | 1u;
+    uint32_t tg_base = 0, tg_bits = 0, visits = 0, nvis = 0, ntri = 0;
+    st.sp = 0;
+    while (true) {
+        if (!node_step<false>(mr, r, best.t, ng_base, ng_bits, tg_base, tg_bits, st, visits, err, nvis)) return false;
+        while (tg_bits) {
+            const uint32_t k = __ffs(tg_bits) - 1;
+            tg_bits &= tg_bits - 1;
+            if (tri_test<false, true>(mr, r, tg_base + k, best, err, ntri)) return true;
+        }
+        if (ng_bits <= 0x00FFFFFFu) {
+            if (st.sp == 0) return false;
             const uint2 e = st.pop();
             ng_base = e.x;
             ng_bits = e.y;

@@ -68,3 +68,138 @@ def triangle_soup_mesh(tris: np.ndarray):
 
 def tri_aabbs(tris: np.ndarray) -> np.ndarray:
     return np.concatenate([tris.min(axis=1), tris.max(axis=1)], axis=1).astype(np.float32)
+
+
+# ---------------------------------------------------------------- render scenes
+#
+# A scene spec is a plain dict that both this library's API and the reference
+# build from the same calls, in the same order (so every index matches):
+#   textures:  [(rgba (h, w, 4) uint8, is_srgb, generate_mipmaps)]
+#   materials: [dict of AddMaterial keyword arguments]
+#   meshes:    [(attrs (n, stride) float32, indices uint32, shapes [(mat, back_mat, start, count)], layout)]
+#   instances: [(mesh, xform (16,) float32 column-major)]
+#   lights:    [dict of AddLight keyword arguments]
+#   env:       dict of SetEnvironment keyword arguments
+#   camera:    dict of camera_desc_t fields
+# Texture indices count from 2: the scene's first two textures are its default
+# environment and normal maps.
+
+def icosphere(subdiv: int, radius: float = 1.0):
+    """Icosahedron subdivided `subdiv` times (20 * 4^subdiv triangles),
+    projected to the sphere. Returns (positions (v, 3), indices (t, 3))."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t), (t, 0, -1), (t, 0, 1),
+         (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6), (7, 1, 8),
+         (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    verts = [np.array(p, np.float64) / np.linalg.norm(p) for p in v]
+    faces = list(f)
+    for _ in range(subdiv):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    return (np.array(verts) * radius).astype(np.float32), np.array(faces, np.uint32)
+
+
+def _quad(p0, p1, p2, p3, n):
+    """Two triangles (p0 p1 p2, p0 p2 p3) as PxyzNxyzTuv rows."""
+    uv = [(0, 0), (1, 0), (1, 1), (0, 1)]
+    rows = [list(p) + list(n) + list(t) for p, t in zip((p0, p1, p2, p3), uv)]
+    return np.array(rows, np.float32), np.array([0, 1, 2, 0, 2, 3], np.uint32)
+
+
+def _box(size, yaw, center):
+    """12-triangle box (flat normals) of the given size, rotated by yaw about y."""
+    sx, sy, sz = (s / 2.0 for s in size)
+    c, s = np.cos(yaw), np.sin(yaw)
+    R = np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]])
+    faces = [((1, 0, 0), [(1, -1, -1), (1, 1, -1), (1, 1, 1), (1, -1, 1)]), ((-1, 0, 0), [(-1, -1, 1), (-1, 1, 1), (-1, 1, -1), (-1, -1, -1)]),
+             ((0, 1, 0), [(-1, 1, -1), (-1, 1, 1), (1, 1, 1), (1, 1, -1)]), ((0, -1, 0), [(-1, -1, 1), (-1, -1, -1), (1, -1, -1), (1, -1, 1)]),
+             ((0, 0, 1), [(1, -1, 1), (1, 1, 1), (-1, 1, 1), (-1, -1, 1)]), ((0, 0, -1), [(-1, -1, -1), (-1, 1, -1), (1, 1, -1), (1, -1, -1)])]
+    rows, idx = [], []
+    for n, corners in faces:
+        pts = [R @ np.array([cx * sx, cy * sy, cz * sz]) + np.array(center) for cx, cy, cz in corners]
+        a, i = _quad(*pts, R @ np.array(n, np.float64))
+        idx.append(i + 4 * len(rows))
+        rows.append(a)
+    return np.concatenate(rows), np.concatenate(idx)
+
+
+def _concat(parts):
+    """[(attrs, idx, material)] -> one mesh with one two-sided shape per part."""
+    attrs, idx, shapes, base = [], [], [], 0
+    for a, i, m in parts:
+        shapes.append((m, m, sum(len(x) for x in idx), len(i)))
+        idx.append(i + base)
+        attrs.append(a)
+        base += len(a)
+    return np.concatenate(attrs).astype(np.float32), np.concatenate(idx).astype(np.uint32), shapes
+
+
+def cornell_box(seed: int = 0, w: int = 256, h: int = 256, max_bounces: int = 4) -> dict:
+    """The small render configuration: a Cornell-style box from `seed` --
+    five axis-aligned wall quads (10 triangles), two boxes (24 triangles)
+    rotated U[0, 45 deg] about y, an icosphere of subdivision 3 (1,280
+    triangles, radius 0.2) and a 0.3 x 0.3 quad light of strength 15 (2
+    triangles); 1,316 triangles in all. Lambertian materials (Oren-Nayar with roughness 0) with
+    albedo U[0.2, 0.8] per channel."""
+    rng = np.random.default_rng(seed)
+    white = np.full((1, 1, 4), 255, np.uint8)
+    spec = {"textures": [(white, False, False)], "materials": [], "meshes": [], "instances": [], "lights": [],
+            "env": {"env_col": (0.0, 0.0, 0.0)}}
+    tex = 2
+
+    def diffuse():
+        spec["materials"].append({"type": 0, "main_color": tuple(float(x) for x in rng.uniform(0.2, 0.8, 3)), "main_texture": tex,
+                                  "roughness": 0.0})
+        return len(spec["materials"]) - 1
+
+    parts = []
+    walls = [((0, 0, 0), (1, 0, 0), (1, 0, 1), (0, 0, 1), (0, 1, 0)), ((0, 1, 0), (0, 1, 1), (1, 1, 1), (1, 1, 0), (0, -1, 0)),
+             ((0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1), (0, 0, -1)), ((0, 0, 0), (0, 0, 1), (0, 1, 1), (0, 1, 0), (1, 0, 0)),
+             ((1, 0, 0), (1, 1, 0), (1, 1, 1), (1, 0, 1), (-1, 0, 0))]
+    for p0, p1, p2, p3, n in walls:
+        a, i = _quad(p0, p1, p2, p3, n)
+        parts.append((a, i, diffuse()))
+    for size, center in (((0.25, 0.5, 0.25), (0.68, 0.25, 0.68)), ((0.25, 0.25, 0.25), (0.3, 0.125, 0.35))):
+        yaw = np.deg2rad(rng.uniform(0.0, 45.0))
+        a, i = _box(size, yaw, center)
+        parts.append((a, i, diffuse()))
+    spec["materials"].append({"type": 3, "main_color": (1.0, 1.0, 1.0), "main_texture": tex, "strength": 15.0})
+    light = len(spec["materials"]) - 1
+    a, i = _quad((0.35, 0.999, 0.35), (0.35, 0.999, 0.65), (0.65, 0.999, 0.65), (0.65, 0.999, 0.35), (0, -1, 0))
+    parts.append((a, i, light))
+    attrs, idx, shapes = _concat(parts)
+    spec["meshes"].append((attrs, idx, shapes, 0))
+    spec["instances"].append((0, np.eye(4, dtype=np.float32).reshape(-1)))
+    # the icosphere: its own mesh, placed by its instance transform
+    pos, faces = icosphere(3, 0.2)
+    nrm = pos / np.linalg.norm(pos, axis=1, keepdims=True)
+    uv = np.stack([0.5 + np.arctan2(nrm[:, 2], nrm[:, 0]) / (2 * np.pi), 0.5 - np.arcsin(nrm[:, 1]) / np.pi], axis=1)
+    sphere_mat = diffuse()
+    sattrs = np.concatenate([pos, nrm, uv], axis=1).astype(np.float32)
+    spec["meshes"].append((sattrs, faces.reshape(-1), [(sphere_mat, sphere_mat, 0, faces.size)], 0))
+    xf = np.eye(4, dtype=np.float32)
+    xf[3, 0:3] = (0.62, 0.7, 0.3)  # floating in front of the tall box
+    spec["instances"].append((1, xf.reshape(-1)))
+    spec["camera"] = {"type": 0, "filter": 1, "dtype": 0, "origin": (0.5, 0.5, -1.0), "fwd": (0.0, 0.0, 1.0), "up": (0.0, 1.0, 0.0),
+                      "fov": 45.0, "gamma": 1.0, "max_total_depth": max_bounces, "max_diff_depth": max_bounces,
+                      "termination_start_depth": max_bounces}
+    spec["size"] = (w, h)
+    return spec
+
+
+def spec_triangles(spec: dict) -> int:
+    return int(sum(len(m[1]) // 3 for m in spec["meshes"]))
