@@ -138,6 +138,104 @@ def cpu_reference(tris, rays, sample: int, steps: int, warmup: int):
     return vals, threads, build_s
 
 
+RENDER_WORKLOAD = "Cornell box (seed 0): 1,316 tris, 256x256, 1 sample per frame, 4 bounces, ray sorting off"
+
+
+def render_frames(args, dev, stream, rank: int, world: int) -> dict:
+    """The render loop on the small render configuration: frames of the
+    Cornell box through RenderScene, timed with CUDA events on the renderer's
+    stream; rays per frame from the renderer's counters; the image compared
+    with the reference's Ref renderer on the same sample sequence."""
+    import torch
+    import torch.distributed as dist
+
+    from raydemo_b200 import api, scenes
+
+    spec = scenes.cornell_box(0)
+    w, h = spec["size"]
+    r = api.Renderer(w, h, device=dev.index)
+    r.set_stream(stream.cuda_stream)
+    sc = r.CreateScene()
+    sc.SetEnvironment(**spec["env"])
+    for rgba, srgb, mips in spec["textures"]:
+        sc.AddTexture(rgba, is_srgb=srgb, generate_mipmaps=mips)
+    for m in spec["materials"]:
+        sc.AddMaterial(**m)
+    for attrs, idx, shapes, layout in spec["meshes"]:
+        sc.AddMesh(attrs, idx, shapes, layout=layout)
+    for mesh, xf in spec["instances"]:
+        sc.AddMeshInstance(mesh, xf)
+    sc.set_current_cam(sc.AddCamera(api.CameraDesc(**spec["camera"])))
+    sc.Commit()
+    # first frame: the image compared with the reference
+    r.Clear()
+    reg = api.RegionContext()
+    r.RenderScene(sc, reg)
+    first = r.get_pixels_ref()
+    info = r.frame_info()
+    if info.error_flags:
+        raise RuntimeError(f"render reported error flags {info.error_flags}")
+    rays_per_frame = info.rays + info.shadow_rays
+    frames = max(10, args.steps * 10)
+    for _ in range(max(3, args.warmup)):
+        r.RenderScene(sc, reg)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(frames):
+        r.RenderScene(sc, reg)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    t = torch.tensor([ev0.elapsed_time(ev1) / frames], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_frame = float(t.item())
+    # end to end through the public API: RenderScene, then the pixels read back to the host
+    e_frames = max(5, min(frames, 50))
+    ev0.record(stream)
+    for _ in range(e_frames):
+        r.RenderScene(sc, reg)
+        r.get_pixels_ref()
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_e2e = ev0.elapsed_time(ev1) / e_frames
+    out = {"workload": RENDER_WORKLOAD, "ms_per_frame": round(ms_frame, 4), "frames": frames,
+           "mrays_per_s": round(world * rays_per_frame / (ms_frame * 1e-3) / 1e6, 2), "rays_per_frame": int(rays_per_frame),
+           "closest_hit_rays_per_frame": int(info.rays), "shadow_rays_per_frame": int(info.shadow_rays),
+           "e2e_ms_per_frame": round(ms_e2e, 4), "e2e_d2h_bytes_per_frame": w * h * 16}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle.oracle import RefLib, RefRenderer
+            from tests.render_scenes import build_ref
+
+            ref = RefLib()
+            rsc = build_ref(ref, spec)
+            rr = RefRenderer(ref, w, h, RefRenderer.REF, True)
+            t0 = time.perf_counter()
+            rr.render(rsc, 1, reset=True, nthreads=1)
+            ref_ms = (time.perf_counter() - t0) * 1e3
+            img = rr.pixels()
+            d = img.astype(np.float64) - first.astype(np.float64)
+            out["rmse_vs_ref"] = float(np.sqrt(np.mean(d[..., :3] ** 2)))
+            out["identical_px_vs_ref"] = float(np.mean(np.all(img == first, axis=-1)))
+            threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+            ra = RefRenderer(ref, w, h, RefRenderer.AVX2, True)
+            ra.render(rsc, 1, reset=True, nthreads=threads)  # warm-up
+            t0 = time.perf_counter()
+            n_cpu = 5
+            ra.render(rsc, n_cpu, reset=False, nthreads=threads)
+            avx_ms = (time.perf_counter() - t0) * 1e3 / n_cpu
+            out["cpu_baseline"] = {"ms_per_frame": round(avx_ms, 3), "cores": threads, "kind": "reference",
+                                   "sample": f"{n_cpu} frames, AVX2 renderer, 64-px buckets on {threads} threads",
+                                   "ref_1core_ms_per_frame": round(ref_ms, 2)}
+        except FileNotFoundError as e:
+            out["cpu_baseline"] = {"ms_per_frame": None, "kind": "reference", "sample": f"unavailable: {e}"}
+    r.set_stream(0)
+    return out
+
+
 def run_reference_arm(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -172,6 +270,17 @@ def run_gpu_arm(args) -> None:
 
     from raydemo_b200.api import Renderer
     from raydemo_b200 import scenes
+
+    if args.render_only:  # the render frames alone (for profiling the render loop)
+        stream = torch.cuda.Stream(dev)
+        torch.cuda.set_stream(stream)
+        args.no_cpu_baseline = True
+        out = render_frames(args, dev, stream, rank, world)
+        if rank == 0:
+            print(json.dumps({"render": out}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     tris, rays = make_workload(rank)
     r = Renderer(64, 64, device=local)
@@ -276,6 +385,8 @@ def run_gpu_arm(args) -> None:
         except FileNotFoundError as e:
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
 
+    render = None if args.no_render else render_frames(args, dev, stream, rank, world)
+
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -285,7 +396,7 @@ def run_gpu_arm(args) -> None:
                            "bvh_nodes": info.nodes, "bvh_depth": info.depth, "parallelism": f"replicas x{world}"},
                 "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": N_RAYS * 32, "d2h_bytes_per_step": N_RAYS * 16,
                         "matches_device_path": bool(ok)},
-                "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary()}
+                "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "render": render}
         print(json.dumps(line), flush=True)
     del sc, r
     if world > 1:
@@ -300,6 +411,8 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=262144)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-render", action="store_true", help="skip the render-loop frames")
+    ap.add_argument("--render-only", action="store_true", help="only the render-loop frames (no microbench, no CPU baseline)")
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes per launch of the traversal kernel from an ncu capture (reported as roofline.traffic)")
     args = ap.parse_args()

@@ -274,6 +274,25 @@ int ray_scene_debug_read(ray_scene *s, int what, void *dst, uint64_t bytes, uint
  * `bytes` bytes; *out_bytes receives the array size. */
 int ray_renderer_debug_read(ray_renderer *r, int what, void *dst, uint64_t bytes, uint64_t *out_bytes);
 
+/* Counts of the last ray_render (no counterpart in the reference): rays traced
+ * for closest hits (primary and continuation rays), shadow-ray segments traced
+ * (one per surface a light's visibility ray passes), and error flags OR-ed over
+ * the frame's kernels (1 traversal stack overflow, 2 corrupt BVH index,
+ * 4 traversal step limit, 8 a material/texture/instance index out of range,
+ * 16 mix materials nested deeper than 32, 32 more than 256 transparent layers
+ * on a shadow ray). Waits for the frame to finish. */
+typedef struct ray_frame_info {
+    uint32_t error_flags;
+    uint64_t rays, shadow_rays;
+} ray_frame_info;
+int ray_renderer_frame_info(ray_renderer *r, ray_frame_info *out);
+
+/* The CUDA stream the renderer enqueues its work on from now on (a
+ * cudaStream_t; NULL: the renderer's own stream). No counterpart in the
+ * reference, whose renderers run on the calling thread. Waits for the work
+ * already enqueued on the previous stream. */
+int ray_renderer_set_stream(ray_renderer *r, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

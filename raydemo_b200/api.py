@@ -337,6 +337,16 @@ class Renderer:
             return buf.reshape(h, w, 4)
         return buf
 
+    def set_stream(self, stream: int = 0) -> None:
+        """Enqueue the renderer's work on this cudaStream_t (0: its own stream)."""
+        check(lib().ray_renderer_set_stream(self._h, stream or None))
+
+    def frame_info(self) -> capi.FrameInfo:
+        """Ray counts and error flags of the last RenderScene (waits for it)."""
+        out = capi.FrameInfo()
+        check(lib().ray_renderer_frame_info(self._h, C.byref(out)))
+        return out
+
     def GetStats(self) -> dict:
         st = capi.Stats()
         check(lib().ray_get_stats(self._h, C.byref(st)))

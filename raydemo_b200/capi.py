@@ -91,6 +91,10 @@ class TraceInfo(C.Structure):
     _fields_ = [("error_flags", C.c_uint32), ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64)]
 
 
+class FrameInfo(C.Structure):
+    _fields_ = [("error_flags", C.c_uint32), ("rays", C.c_uint64), ("shadow_rays", C.c_uint64)]
+
+
 class TraceTuning(C.Structure):
     _fields_ = [("kernel", C.c_int), ("refill_min", C.c_int), ("deep_stack", C.c_int)]
 
@@ -155,6 +159,8 @@ _SIGS = {
     "ray_scene_mesh_bvh_info": ([_P, C.c_uint32, C.POINTER(BvhInfo)], C.c_int),
     "ray_scene_debug_read": ([_P, C.c_int, _P, C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
     "ray_renderer_debug_read": ([_P, C.c_int, _P, C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
+    "ray_renderer_frame_info": ([_P, C.POINTER(FrameInfo)], C.c_int),
+    "ray_renderer_set_stream": ([_P, _P], C.c_int),
     "ray_sort_rays": ([_P, _P, C.c_uint64, C.POINTER(C.c_float), C.POINTER(C.c_float), _P, _P, _P, _P], C.c_int),
     "ray_sort_rays_noalloc": ([_P, C.c_uint64, C.POINTER(C.c_float), C.POINTER(C.c_float), _P, _P, _P, _P], C.c_int),
     "ray_scene_set_trace_tuning": ([_P, C.POINTER(TraceTuning)], C.c_int),

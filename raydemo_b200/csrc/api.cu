@@ -278,12 +278,13 @@ int ray_create_renderer(const ray_settings *s, ray_renderer **out) {
     r->device = s->device;
     r->w = s->w;
     r->h = s->h;
-    cudaError_t e = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking);
+    cudaError_t e = cudaStreamCreateWithFlags(&r->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete r;
         set_error(cudaGetErrorString(e));
         return RAY_ERR_CUDA;
     }
+    r->stream = r->own_stream;
     *out = r;
     return RAY_OK;
     RG_GUARD_END

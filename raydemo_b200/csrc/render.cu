@@ -119,7 +119,7 @@ ray_renderer::~ray_renderer() {
     for (int s = 0; s < 2; s++)
         for (int e = 0; e < N_EVENTS; e++)
             if (ev_sets[s][e]) cudaEventDestroy(ev_sets[s][e]);
-    if (stream) cudaStreamDestroy(stream);
+    if (own_stream) cudaStreamDestroy(own_stream);
 }
 
 extern "C" {
@@ -275,7 +275,10 @@ int ray_render(ray_renderer *r, ray_scene *s, ray_region *region) {
         const float kx = float(w) / h;
         const float fov_k = std::tan(0.5f * cd.fov * PI / 180.0f) * cd.focus_distance;
         uint32_t *cnt = static_cast<uint32_t *>(r->d_counters.p);
+        // [0], [1] ray counts of the two buffers, [2] trace work counter,
+        // [3] error flags, [4..7] two uint64: rays traced, shadow segments
         RG_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8 * sizeof(uint32_t), st));
+        unsigned long long *ray_stats = reinterpret_cast<unsigned long long *>(cnt + 4);
         float4 *rays[2] = {static_cast<float4 *>(r->d_rays[0].p), static_cast<float4 *>(r->d_rays[1].p)};
         RayPayload *pay[2] = {static_cast<RayPayload *>(r->d_pay[0].p), static_cast<RayPayload *>(r->d_pay[1].p)};
         RG_CUDA_TRY(launch_raygen(cdev, kx, fov_k, it, rect.x, rect.y, rect.w, rect.h, w, h, halton, rays[0], pay[0], cnt + 0, st));
@@ -296,7 +299,8 @@ int ray_render(ray_renderer *r, ray_scene *s, ray_region *region) {
         RG_CUDA_TRY(launch_trace_closest(sc.sv, rays[0], max_rays, hits, obj, err, nullptr, false, st, tp));
         RG_CUDA_TRY(cudaEventRecord(ev[2], st));
         RG_CUDA_TRY(launch_shade(sc, pi, halton, rays[0], pay[0], hits, obj, cnt + 0, max_rays, rays[1], pay[1], cnt + 1,
-                                 static_cast<float4 *>(r->d_temp.p), sh ? static_cast<SHData *>(r->d_temp_sh.p) : nullptr, true, err, st));
+                                 static_cast<float4 *>(r->d_temp.p), sh ? static_cast<SHData *>(r->d_temp_sh.p) : nullptr, true, err,
+                                 ray_stats, st));
         RG_CUDA_TRY(cudaEventRecord(ev[3], st));
 
         // bounces (RendererRef.cpp:183-278); ray counts stay on the device
@@ -311,7 +315,7 @@ int ray_render(ray_renderer *r, ray_scene *s, ray_region *region) {
                 RG_CUDA_TRY(cudaEventRecord(ev[4 + 2 * bounce], st));
                 pi.bounce = bounce + 3;
                 RG_CUDA_TRY(launch_shade(sc, pi, halton, rays[cur], pay[cur], hits, obj, cnt + cur, max_rays, rays[nxt], pay[nxt],
-                                         cnt + nxt, static_cast<float4 *>(r->d_temp.p), nullptr, false, err, st));
+                                         cnt + nxt, static_cast<float4 *>(r->d_temp.p), nullptr, false, err, ray_stats, st));
                 RG_CUDA_TRY(cudaEventRecord(ev[5 + 2 * bounce], st));
                 cur = nxt;
                 nb++;
@@ -392,6 +396,34 @@ int ray_renderer_debug_read(ray_renderer *r, int what, void *dst, uint64_t bytes
     *out_bytes = size;
     const uint64_t n = std::min<uint64_t>(bytes, size);
     if (n) RG_CUDA_TRY(cudaMemcpy(dst, b->p, n, cudaMemcpyDeviceToHost));
+    return RAY_OK;
+}
+
+int ray_renderer_set_stream(ray_renderer *r, void *stream) {
+    if (!r) {
+        set_error("null renderer");
+        return RAY_ERR_INVALID_ARG;
+    }
+    RG_CUDA_TRY(cudaSetDevice(r->device));
+    RG_CUDA_TRY(cudaStreamSynchronize(r->stream)); // work on the old stream finishes first
+    r->stream = stream ? static_cast<cudaStream_t>(stream) : r->own_stream;
+    return RAY_OK;
+}
+
+int ray_renderer_frame_info(ray_renderer *r, ray_frame_info *out) {
+    if (!r || !out) {
+        set_error("null argument");
+        return RAY_ERR_INVALID_ARG;
+    }
+    *out = ray_frame_info{};
+    if (!r->d_counters.p) return RAY_OK;
+    RG_CUDA_TRY(cudaSetDevice(r->device));
+    RG_CUDA_TRY(cudaStreamSynchronize(r->stream));
+    uint32_t c[8];
+    RG_CUDA_TRY(cudaMemcpy(c, r->d_counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+    out->error_flags = c[3];
+    memcpy(&out->rays, c + 4, 8);
+    memcpy(&out->shadow_rays, c + 6, 8);
     return RAY_OK;
 }
 

@@ -125,7 +125,7 @@ cudaError_t launch_raygen(const CameraDev &cam, float k, float fov_k, int iterat
 cudaError_t launch_shade(const RenderScene &sc, const PassInfo &pi, const float *halton, const float4 *rays, const RayPayload *pay,
                          const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays, float4 *out_rays,
                          RayPayload *out_pay, uint32_t *out_count, float4 *temp, SHData *temp_sh, bool primary, uint32_t *err,
-                         cudaStream_t st);
+                         unsigned long long *ray_stats, cudaStream_t st);
 // clean += (temp - clean) * k over the rect, then final = tone(clean)
 cudaError_t launch_resolve(const float4 *temp, float4 *clean, float4 *fin, SHData *temp_sh, SHData *clean_sh, int rx, int ry, int rw,
                            int rh, int w, float k, int srgb, float gamma, bool clamp, bool sh, cudaStream_t st);

@@ -156,7 +156,7 @@ constexpr int MAX_SHADOW_LAYERS = 256;
 
 // ComputeVisibility, CoreRef.cpp:1800-1896
 __device__ float compute_visibility(const RenderScene &sc, V3 p1, V3 p2, const float *halton, int hi, int rand_hash2, Stack<true> &st,
-                                    uint32_t &err) {
+                                    uint32_t &err, uint32_t &nshadow) {
     V3 dir = p2 - p1;
     float dist = length(dir);
     dir = dir / dist;
@@ -169,6 +169,7 @@ __device__ float compute_visibility(const RenderScene &sc, V3 p1, V3 p2, const f
             break;
         }
         const Best sh = trace_any(sc.sv, o, dir, dist, st, err);
+        nshadow++;
         if (sh.prim < 0) break;
         if ((uint32_t)sh.prim >= sc.n_tris || (uint32_t)sh.obj >= sc.sv.n_inst) {
             err |= SHADE_ERR_BAD_INDEX;
@@ -244,7 +245,7 @@ __device__ float compute_visibility(const RenderScene &sc, V3 p1, V3 p2, const f
 // AcumulateLightContribution, CoreRef.cpp:1898-1933
 __device__ __forceinline__ void accumulate_light(const RenderScene &sc, const LightRec &l, V3 I, V3 P, V3 N, V3 B, V3 plane_N, float sigma,
                                                  const float *halton, int hi, int rand_hash2, float rand_offset, float rand_offset2, V3 &col,
-                                                 Stack<true> &st, uint32_t &err) {
+                                                 Stack<true> &st, uint32_t &err, uint32_t &nshadow) {
     const V3 lpos = v3(l.pos);
     V3 L = P - lpos;
     const float distance = length(L);
@@ -265,7 +266,7 @@ __device__ __forceinline__ void accumulate_light(const RenderScene &sc, const Li
     const float dot1 = fmax_std(dot(L, N), 0.0f);
     const float dot2 = dot(L, v3(l.dir));
     if (dot1 > FLT_EPS_ && dot2 > l.spot && (l.brightness * atten) > FLT_EPS_) {
-        const float visibility = compute_visibility(sc, P + HIT_BIAS * plane_N, lpos, halton, hi, rand_hash2, st, err);
+        const float visibility = compute_visibility(sc, P + HIT_BIAS * plane_N, lpos, halton, hi, rand_hash2, st, err, nshadow);
         col = col + v3(l.col) * dot1 * visibility * atten * brdf_oren_nayar(L, I, N, B, sigma);
     }
 }
@@ -297,7 +298,8 @@ __device__ __forceinline__ void set3(float *dst, V3 v) {
 // ShadeSurface, CoreRef.cpp:2055-2391. Returns the pixel contribution;
 // fills nr and sets emit when the path continues.
 __device__ F4 shade_surface(const RenderScene &sc, const PassInfo &pi, int rand_index, const float *halton, float4 hit, int obj,
-                            float4 r0, float4 r1, const RayPayload &ray, NewRay &nr, bool &emit, Stack<true> &st, uint32_t &err) {
+                            float4 r0, float4 r1, const RayPayload &ray, NewRay &nr, bool &emit, Stack<true> &st, uint32_t &err,
+                            uint32_t &nshadow) {
     emit = false;
     const int prim = __float_as_int(hit.x);
     const V3 I = v3(r1.x, r1.y, r1.z);
@@ -434,7 +436,7 @@ __device__ F4 shade_surface(const RenderScene &sc, const PassInfo &pi, int rand_
         if (!(pi.flags & PASS_SKIP_DIRECT) || pi.bounce > 2) {
             for (uint32_t li = 0; li < sc.n_lights; li++)
                 accumulate_light(sc, sc.lights[li], I, P, N, B, plane_N, mat.roughness_or_strength, halton, hi, rand_hash2, rand_offset,
-                                 rand_offset2, col, st, err);
+                                 rand_offset2, col, st, err, nshadow);
             if (consider_albedo) col = col * alb;
         }
         if (diff_depth < pi.max_diff_depth && total_depth < pi.max_total_depth) {
@@ -565,12 +567,13 @@ __global__ void __launch_bounds__(SHADE_BLOCK) k_shade(RenderScene sc, PassInfo 
                                                        const float4 *__restrict__ hits, const int32_t *__restrict__ obj,
                                                        const uint32_t *__restrict__ in_count, uint32_t max_rays, float4 *__restrict__ out_rays,
                                                        RayPayload *__restrict__ out_pay, uint32_t *__restrict__ out_count,
-                                                       float4 *__restrict__ temp, SHData *__restrict__ temp_sh, uint32_t *__restrict__ err_out) {
+                                                       float4 *__restrict__ temp, SHData *__restrict__ temp_sh, uint32_t *__restrict__ err_out,
+                                                       unsigned long long *__restrict__ ray_stats) {
     __shared__ uint2 s_stack[trav::SMEM_STACK * SHADE_BLOCK];
     Stack<true> st;
     st.smem = s_stack + threadIdx.x;
     st.sp = 0;
-    uint32_t err = 0;
+    uint32_t err = 0, nshadow = 0;
     const uint32_t n = min(*in_count, max_rays);
     const uint32_t lane = threadIdx.x & 31u;
     for (uint32_t base = blockIdx.x * SHADE_BLOCK; base < n; base += gridDim.x * SHADE_BLOCK) {
@@ -584,7 +587,7 @@ __global__ void __launch_bounds__(SHADE_BLOCK) k_shade(RenderScene sc, PassInfo 
             const int x = (int)(xy >> 16), y = (int)(xy & 0xffffu);
             const int index = y * pi.w + x;
             const int rand_index = (pi.flags & PASS_COHERENT) ? c_sampling_pattern[(y % 8) * 8 + (x % 8)] : index;
-            const F4 c = shade_surface(sc, pi, rand_index, halton, hits[i], obj[i], r0, r1, p, nr, emit, st, err);
+            const F4 c = shade_surface(sc, pi, rand_index, halton, hits[i], obj[i], r0, r1, p, nr, emit, st, err, nshadow);
             if (PRIMARY) {
                 temp[index] = make_float4(c.x, c.y, c.z, c.w);
                 if (temp_sh) {
@@ -624,6 +627,12 @@ __global__ void __launch_bounds__(SHADE_BLOCK) k_shade(RenderScene sc, PassInfo 
         }
     }
     if (err) atomicOr(err_out, err);
+    // rays shaded (each was traced once) and shadow-ray segments traced
+    if (ray_stats) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&ray_stats[0], (unsigned long long)n);
+        const uint32_t ws = __reduce_add_sync(0xffffffffu, nshadow);
+        if (lane == 0 && ws) atomicAdd(&ray_stats[1], (unsigned long long)ws);
+    }
 }
 
 // Framebuffer::MixWith, ComputeSHData, MixWith_SH (FramebufferRef.cpp:57-101)
@@ -713,7 +722,7 @@ cudaError_t launch_raygen(const CameraDev &cam, float k, float fov_k, int iterat
 cudaError_t launch_shade(const RenderScene &sc, const PassInfo &pi, const float *halton, const float4 *rays, const RayPayload *pay,
                          const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays, float4 *out_rays,
                          RayPayload *out_pay, uint32_t *out_count, float4 *temp, SHData *temp_sh, bool primary, uint32_t *err,
-                         cudaStream_t st) {
+                         unsigned long long *ray_stats, cudaStream_t st) {
     if (g_shade_blocks == 0) {
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
@@ -725,10 +734,10 @@ cudaError_t launch_shade(const RenderScene &sc, const PassInfo &pi, const float 
     const uint32_t blocks = need < (uint32_t)g_shade_blocks ? (need > 0 ? need : 1) : (uint32_t)g_shade_blocks;
     if (primary)
         k_shade<true><<<blocks, SHADE_BLOCK, 0, st>>>(sc, pi, halton, rays, pay, hits, obj, in_count, max_rays, out_rays, out_pay, out_count, temp,
-                                                      temp_sh, err);
+                                                      temp_sh, err, ray_stats);
     else
         k_shade<false><<<blocks, SHADE_BLOCK, 0, st>>>(sc, pi, halton, rays, pay, hits, obj, in_count, max_rays, out_rays, out_pay, out_count,
-                                                       temp, temp_sh, err);
+                                                       temp, temp_sh, err, ray_stats);
     return cudaGetLastError();
 }
 

@@ -116,7 +116,8 @@ struct ray_scene {
 struct ray_renderer {
     int device = 0;
     int w = 0, h = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;     // where the renderer's work goes: own_stream or the caller's
+    cudaStream_t own_stream = nullptr;
     ray_stats stats{};
     std::vector<ray_pixel> host_pixels;
     std::vector<ray_shl1> host_sh;
