@@ -177,21 +177,29 @@ def render_frames(args, dev, stream, rank: int, world: int) -> dict:
         raise RuntimeError(f"render reported error flags {info.error_flags}")
     rays_per_frame = info.rays + info.shadow_rays
     frames = max(10, args.steps * 10)
-    for _ in range(max(3, args.warmup)):
-        r.RenderScene(sc, reg)
-    torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(frames):
-        r.RenderScene(sc, reg)
-    ev1.record(stream)
-    torch.cuda.synchronize(dev)
-    t = torch.tensor([ev0.elapsed_time(ev1) / frames], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_frame = float(t.item())
+
+    def timed(kernel: int) -> float:
+        """ms per frame with the given kernel choice (0: the renderer's own choice by timing)."""
+        r.set_kernel(kernel)
+        for _ in range(max(8, args.warmup)):  # covers the timing frames of the kernel choice
+            r.RenderScene(sc, reg)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        ev0.record(stream)
+        for _ in range(frames):
+            r.RenderScene(sc, reg)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        t = torch.tensor([ev0.elapsed_time(ev1) / frames], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    by_kernel = {"wavefront": round(timed(1), 4), "path": round(timed(2), 4)}
+    ms_frame = timed(0)
+    chosen = {1: "wavefront", 2: "path"}.get(r.frame_info().kernel, "?")
     # end to end through the public API: RenderScene, then the pixels read back to the host
     e_frames = max(5, min(frames, 50))
     ev0.record(stream)
@@ -204,7 +212,8 @@ def render_frames(args, dev, stream, rank: int, world: int) -> dict:
     out = {"workload": RENDER_WORKLOAD, "ms_per_frame": round(ms_frame, 4), "frames": frames,
            "mrays_per_s": round(world * rays_per_frame / (ms_frame * 1e-3) / 1e6, 2), "rays_per_frame": int(rays_per_frame),
            "closest_hit_rays_per_frame": int(info.rays), "shadow_rays_per_frame": int(info.shadow_rays),
-           "e2e_ms_per_frame": round(ms_e2e, 4), "e2e_d2h_bytes_per_frame": w * h * 16}
+           "e2e_ms_per_frame": round(ms_e2e, 4), "e2e_d2h_bytes_per_frame": w * h * 16, "kernel": chosen,
+           "ms_per_frame_by_kernel": by_kernel}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             from oracle.oracle import RefLib, RefRenderer
@@ -234,6 +243,101 @@ def render_frames(args, dev, stream, rank: int, world: int) -> dict:
             out["cpu_baseline"] = {"ms_per_frame": None, "kind": "reference", "sample": f"unavailable: {e}"}
     r.set_stream(0)
     return out
+
+
+BATCH_WORKLOAD = ("batched form: 64 scenes (ground plane + displaced icospheres, 962..491,522 tris, log-uniform target "
+                  "[1e3, 5e5]), resolutions from {64..1024}^2 (19.9 Mpixel), 4 samples, max 6 bounces, sun + sky")
+
+
+def batch_frames(args, dev, stream, n_scenes: int = 64, samples: int = 4) -> dict:
+    """The batched configuration: `samples` samples of every scene as ONE
+    ray_render_batch call, against the plain loop of RenderScene per scene
+    and sample (each renderer with its own kernel choice), on one stream.
+    Both loops render the same images (compared bit for bit)."""
+    import torch
+
+    from raydemo_b200 import api, scenes
+
+    specs = [scenes.batch_scene(i) for i in range(n_scenes)]
+    rs, scs = [], []
+    for sp in specs:
+        w, h = sp["size"]
+        r = api.Renderer(w, h, device=dev.index)
+        r.set_stream(stream.cuda_stream)
+        sc = r.CreateScene()
+        sc.SetEnvironment(**sp["env"])
+        for rgba, srgb, mips in sp["textures"]:
+            sc.AddTexture(rgba, is_srgb=srgb, generate_mipmaps=mips)
+        for m in sp["materials"]:
+            sc.AddMaterial(**m)
+        for attrs, idx, shapes, layout in sp["meshes"]:
+            sc.AddMesh(attrs, idx, shapes, layout=layout)
+        for mesh, xf in sp["instances"]:
+            sc.AddMeshInstance(mesh, xf)
+        for l in sp["lights"]:
+            sc.AddLight(**l)
+        sc.set_current_cam(sc.AddCamera(api.CameraDesc(**sp["camera"])))
+        sc.Commit()
+        rs.append(r)
+        scs.append(sc)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def plain_pass() -> list:
+        regs = [api.RegionContext() for _ in rs]
+        for r, sc, g in zip(rs, scs, regs):
+            r.Clear()
+            for _ in range(samples):
+                r.RenderScene(sc, g)
+        return regs
+
+    def batch_pass() -> list:
+        regs = [api.RegionContext() for _ in rs]
+        for r in rs:
+            r.Clear()
+        api.render_batch(rs, scs, regs, samples)
+        return regs
+
+    # warm-up: the plain loop twice (each renderer times both kernels on its first frames), the batch once
+    plain_pass()
+    plain_pass()
+    torch.cuda.synchronize(dev)
+    ev0.record(stream)
+    plain_pass()
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    plain_ms = ev0.elapsed_time(ev1)
+    plain_imgs = [r.get_pixels_ref() for r in rs]
+    kernels = [r.frame_info().kernel for r in rs]
+
+    def timed_batch(kernel: int, warm: int) -> float:
+        rs[0].set_kernel(kernel)  # the batch follows the first renderer's setting
+        for _ in range(warm):
+            batch_pass()
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        batch_pass()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        return ev0.elapsed_time(ev1)
+
+    by_kernel = {"wavefront": round(timed_batch(1, 1), 3), "path": round(timed_batch(2, 1), 3)}
+    batch_ms = timed_batch(0, 4)  # the default: the faster of the two, timed on the first calls
+    info = rs[0].frame_info()
+    if info.error_flags:
+        raise RuntimeError(f"batch reported error flags {info.error_flags}")
+    identical, worst = 0, 0.0
+    for r, a in zip(rs, plain_imgs):
+        b = r.get_pixels_ref()
+        identical += int(np.array_equal(a.view(np.uint32), b.view(np.uint32)))
+        worst = max(worst, float(np.sqrt(np.mean((a[..., :3].astype(np.float64) - b[..., :3]) ** 2))))
+    rays = info.rays + info.shadow_rays
+    return {"workload": BATCH_WORKLOAD, "scenes": n_scenes, "samples": samples, "tris_total": int(sum(s["tris"] for s in specs)),
+            "pixels_per_sample": int(sum(s["size"][0] * s["size"][1] for s in specs)), "batch_ms": round(batch_ms, 3),
+            "plain_loop_ms": round(plain_ms, 3), "speedup_vs_plain": round(plain_ms / batch_ms, 3),
+            "batch_mrays_per_s": round(rays / (batch_ms * 1e-3) / 1e6, 1), "rays": int(rays),
+            "plain_kernels": {"wavefront": kernels.count(1), "path": kernels.count(2)},
+            "batch_kernel": {1: "wavefront", 2: "path"}.get(info.kernel, "?"), "batch_ms_by_kernel": by_kernel,
+            "images_identical_to_plain": f"{identical}/{n_scenes}", "max_rmse_vs_plain": worst}
 
 
 def run_reference_arm(args) -> None:
@@ -271,13 +375,16 @@ def run_gpu_arm(args) -> None:
     from raydemo_b200.api import Renderer
     from raydemo_b200 import scenes
 
-    if args.render_only:  # the render frames alone (for profiling the render loop)
+    if args.render_only or args.batch_only:  # one part alone (for profiling)
         stream = torch.cuda.Stream(dev)
         torch.cuda.set_stream(stream)
         args.no_cpu_baseline = True
-        out = render_frames(args, dev, stream, rank, world)
+        if args.render_only:
+            out = {"render": render_frames(args, dev, stream, rank, world)}
+        else:
+            out = {"batch": batch_frames(args, dev, stream)}
         if rank == 0:
-            print(json.dumps({"render": out}), flush=True)
+            print(json.dumps(out), flush=True)
         if world > 1:
             dist.destroy_process_group()
         return
@@ -386,6 +493,7 @@ def run_gpu_arm(args) -> None:
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
 
     render = None if args.no_render else render_frames(args, dev, stream, rank, world)
+    batch = None if args.no_batch else batch_frames(args, dev, stream)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -396,7 +504,7 @@ def run_gpu_arm(args) -> None:
                            "bvh_nodes": info.nodes, "bvh_depth": info.depth, "parallelism": f"replicas x{world}"},
                 "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": N_RAYS * 32, "d2h_bytes_per_step": N_RAYS * 16,
                         "matches_device_path": bool(ok)},
-                "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "render": render}
+                "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "render": render, "batch": batch}
         print(json.dumps(line), flush=True)
     del sc, r
     if world > 1:
@@ -413,6 +521,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-render", action="store_true", help="skip the render-loop frames")
     ap.add_argument("--render-only", action="store_true", help="only the render-loop frames (no microbench, no CPU baseline)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-form measurement")
+    ap.add_argument("--batch-only", action="store_true", help="only the batched-form measurement")
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes per launch of the traversal kernel from an ncu capture (reported as roofline.traffic)")
     args = ap.parse_args()

@@ -283,9 +283,35 @@ int ray_renderer_debug_read(ray_renderer *r, int what, void *dst, uint64_t bytes
  * on a shadow ray). Waits for the frame to finish. */
 typedef struct ray_frame_info {
     uint32_t error_flags;
+    int32_t kernel; /* the kernel that rendered it: 1 wavefront, 2 path kernel */
     uint64_t rays, shadow_rays;
 } ray_frame_info;
 int ray_renderer_frame_info(ray_renderer *r, ray_frame_info *out);
+
+/* Kernel choice for ray_render (no counterpart in the reference, whose CPU
+ * renderers have one loop): 1 = wavefront (a launch per bounce for ray
+ * generation, closest hit and shading; ray counts on the device), 2 = path
+ * kernel (one launch per frame, one thread per pixel through all bounces),
+ * 0 = chosen per frame configuration (scene, rect size, bounces) by timing
+ * both on its first frames. Both give the same image. Default 0. */
+int ray_renderer_set_kernel(ray_renderer *r, int kernel);
+
+/* Batched form (no counterpart in the reference): `samples` samples over each
+ * region of `count` (renderer, scene, region) triples, as if ray_render were
+ * called `samples` times for each in turn, with the scenes rendered together:
+ * the path kernel renders every region's samples in one launch; the wavefront
+ * runs each phase (ray generation, closest hit, shading, accumulation) as one
+ * launch over the rays of all scenes. The first renderer's kernel setting
+ * (ray_renderer_set_kernel) picks one; by default both are timed on the first
+ * calls of a batch configuration and the faster is kept. A region's samples
+ * are split where its iterations cross a multiple of 256 (its sample table
+ * changes there). Renderers may repeat: regions of one framebuffer must not
+ * overlap and must be at the same iteration. All renderers must be on one
+ * device. The work goes on the first renderer's stream, ordered after the work
+ * already on every renderer's stream and before the work enqueued there later;
+ * the first renderer's ray_renderer_frame_info reports the last sample's
+ * launches. Batched frames are not timed into the stats. */
+int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, ray_region *const *regions, int count, int samples);
 
 /* The CUDA stream the renderer enqueues its work on from now on (a
  * cudaStream_t; NULL: the renderer's own stream). No counterpart in the

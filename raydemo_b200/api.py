@@ -337,6 +337,10 @@ class Renderer:
             return buf.reshape(h, w, 4)
         return buf
 
+    def set_kernel(self, kernel: int = 0) -> None:
+        """1 wavefront, 2 path kernel, 0 chosen by timing (ray_renderer_set_kernel)."""
+        check(lib().ray_renderer_set_kernel(self._h, kernel))
+
     def set_stream(self, stream: int = 0) -> None:
         """Enqueue the renderer's work on this cudaStream_t (0: its own stream)."""
         check(lib().ray_renderer_set_stream(self._h, stream or None))
@@ -359,6 +363,17 @@ class Renderer:
 def RegionContext(x: int = 0, y: int = 0, w: int = 0, h: int = 0) -> capi.Region:
     """RegionContext (RendererBase.h:35-51): a rect plus the iteration counter."""
     return capi.Region(capi.Rect(x, y, w, h), 0)
+
+
+def render_batch(renderers, scenes, regions, samples: int = 1) -> None:
+    """`samples` samples of every (renderer, scene, region) in one launch (ray_render_batch)."""
+    n = len(renderers)
+    if not (len(scenes) == n == len(regions)):
+        raise ValueError("renderers, scenes and regions must have the same length")
+    rs = (C.c_void_p * max(n, 1))(*[r.handle.value for r in renderers])
+    ss = (C.c_void_p * max(n, 1))(*[s.handle.value for s in scenes])
+    gs = (C.POINTER(capi.Region) * max(n, 1))(*[C.pointer(g) for g in regions])
+    check(lib().ray_render_batch(rs, ss, gs, n, samples))
 
 
 def create_renderer(w: int, h: int, device: int = 0) -> Renderer:

@@ -4,6 +4,7 @@
 // framebuffer accessors, Resize/Clear and the stats.
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <functional>
 #include <random>
@@ -17,6 +18,7 @@ using namespace rg;
 namespace {
 
 constexpr int MAX_BOUNCES = 10; // Core.h:53
+constexpr int TUNE_SAMPLES = 2; // timed frames per kernel before the choice
 constexpr int N_EVENTS = ray_renderer::N_EVENTS; // 4 + 2 * MAX_BOUNCES + 1
 static_assert(N_EVENTS == 5 + 2 * MAX_BOUNCES, "one event per phase");
 
@@ -67,6 +69,7 @@ int ensure_frame_buffers(ray_renderer *r, bool sh) {
     return RAY_OK;
 }
 
+// The wavefront's ray buffers: two generations of n rays, their hits and instance ids.
 int ensure_ray_buffers(ray_renderer *r, size_t n) {
     for (int k = 0; k < 2; k++) {
         RG_CUDA_TRY(r->d_rays[k].ensure(n * 2 * sizeof(float4)));
@@ -74,6 +77,11 @@ int ensure_ray_buffers(ray_renderer *r, size_t n) {
     }
     RG_CUDA_TRY(r->d_hits.ensure(n * sizeof(float4)));
     RG_CUDA_TRY(r->d_obj.ensure(n * sizeof(int32_t)));
+    return RAY_OK;
+}
+
+// Counters, the sample table and its permutations, the stats events.
+int ensure_frame_state(ray_renderer *r) {
     RG_CUDA_TRY(r->d_counters.ensure(8 * sizeof(uint32_t)));
     if (!r->d_perms.p) {
         const std::vector<uint16_t> perms = halton_permutations();
@@ -85,6 +93,8 @@ int ensure_ray_buffers(ray_renderer *r, size_t n) {
     if (!r->ev_sets[0][0]) {
         for (int s = 0; s < 2; s++)
             for (int e = 0; e < N_EVENTS; e++) RG_CUDA_TRY(cudaEventCreate(&r->ev_sets[s][e]));
+        RG_CUDA_TRY(cudaEventCreateWithFlags(&r->ev_sync, cudaEventDisableTiming));
+        for (int e = 0; e < 2; e++) RG_CUDA_TRY(cudaEventCreate(&r->ev_batch[e]));
     }
     return RAY_OK;
 }
@@ -107,7 +117,220 @@ int resolve_stats(ray_renderer *r, int set) {
         r->stats.time_secondary_trace_us += us(3 + 2 * b, 4 + 2 * b);
         r->stats.time_secondary_shade_us += us(4 + 2 * b, 5 + 2 * b);
     }
+    // a frame the kernel choice is timing
+    const int ti = r->ev_tune[set];
+    if (ti >= 0 && ti < (int)r->tune.size()) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e[0], e[N_EVENTS - 1]);
+        ray_renderer::TuneEntry &t = r->tune[ti];
+        const int k = r->ev_kernel[set] - 1;
+        t.best[k] = std::min(t.best[k], ms);
+        t.n[k]++;
+        if (t.pending[k] > 0) t.pending[k]--;
+        if (t.n[0] >= TUNE_SAMPLES && t.n[1] >= TUNE_SAMPLES) t.choice = t.best[1] < t.best[0] ? 2 : 1;
+    }
+    r->ev_tune[set] = -1;
     r->ev_frame_pending[set] = false;
+    return RAY_OK;
+}
+
+// Kernel for this frame: the caller's choice, or per frame configuration
+// (scene, its triangle and light counts, rect size, bounces) the faster of
+// the two as timed on its first frames (TUNE_SAMPLES each, the best kept; both
+// give the same image). Returns the kernel and, for a timed frame, the entry.
+int choose_kernel(ray_renderer *r, const ray_scene *s, uint32_t pixels, int bounces, int &tune_entry) {
+    tune_entry = -1;
+    if (r->kernel == 1 || r->kernel == 2) return r->kernel;
+    for (size_t i = 0; i < r->tune.size(); i++) {
+        ray_renderer::TuneEntry &t = r->tune[i];
+        if (t.scene == s && t.tris == s->total_tris && t.lights == (uint32_t)s->lights.size() && t.pixels == pixels && t.bounces == bounces) {
+            if (t.choice) return t.choice;
+            tune_entry = (int)i;
+            return t.n[0] + t.pending[0] <= t.n[1] + t.pending[1] ? 1 : 2;
+        }
+    }
+    if (r->tune.size() >= 64) { // forget them all (the frames in flight lose their timing)
+        r->tune.clear();
+        r->ev_tune[0] = r->ev_tune[1] = -1;
+    }
+    ray_renderer::TuneEntry t;
+    t.scene = s;
+    t.tris = s->total_tris;
+    t.lights = (uint32_t)s->lights.size();
+    t.pixels = pixels;
+    t.bounces = bounces;
+    r->tune.push_back(t);
+    tune_entry = (int)r->tune.size() - 1;
+    return 1;
+}
+
+// RegionContext's sample table (RendererRef.cpp:85-89): regenerated on the
+// first call and every 256 iterations. For a region that starts at
+// iteration 0 its base is 1 until iteration 255, then the iteration rounded
+// down to a multiple of 256.
+int table_base(int iteration) { return iteration < HALTON_SEQ_LEN ? 1 : (iteration & ~(HALTON_SEQ_LEN - 1)); }
+
+constexpr int PREPARE_NOTHING = 1; // the call renders nothing (a scene of another device)
+
+// One RenderScene call up to its kernels: checks, the scene's device data,
+// frame buffers, the region's iteration and sample table (on the renderer's
+// stream), and the job both kernels read.
+int prepare_job(ray_renderer *r, ray_scene *s, ray_region *region, FrameJob &J, ray_rect &rect, int samples = 1) {
+    if (!r || !s || !region) {
+        set_error("null argument");
+        return RAY_ERR_INVALID_ARG;
+    }
+    if (s->device != r->device) return PREPARE_NOTHING; // as the reference's failed scene cast: a no-op
+    if (s->current_cam >= s->cameras.size() || !s->cameras[s->current_cam].alive) {
+        set_error("the scene has no current camera");
+        return RAY_ERR_INVALID_ARG;
+    }
+    const CameraRec &cam = s->cameras[s->current_cam];
+    const ray_camera_desc &cd = cam.desc;
+    if (cd.type != 0) {
+        set_error("only perspective cameras are rendered");
+        return RAY_ERR_UNSUPPORTED;
+    }
+    RG_CUDA_TRY(cudaSetDevice(r->device));
+    int rc = commit(s);
+    if (rc != RAY_OK) return rc;
+    const int w = r->w, h = r->h;
+    rect = region->rect;
+    if (rect.w == 0 || rect.h == 0) rect = ray_rect{0, 0, w, h};
+    if (rect.x < 0 || rect.y < 0 || rect.w < 0 || rect.h < 0 || rect.x + rect.w > w || rect.y + rect.h > h) {
+        set_error("region outside the framebuffer");
+        return RAY_ERR_INVALID_ARG;
+    }
+    const bool sh = cd.output_sh != 0;
+    rc = ensure_frame_buffers(r, sh);
+    if (rc != RAY_OK) return rc;
+    rc = ensure_frame_state(r);
+    if (rc != RAY_OK) return rc;
+
+    // `samples` consecutive iterations, all in one block of the sample table
+    const int it = region->iteration + 1;
+    region->iteration += samples;
+    const int base = table_base(it);
+    if (base != r->halton_base) {
+        RG_CUDA_TRY(launch_halton_table(static_cast<const uint16_t *>(r->d_perms.p), base, static_cast<float *>(r->d_halton.p), r->stream));
+        r->halton_base = base;
+    }
+
+    J = FrameJob{};
+    J.sc = render_scene_view(s);
+    PassInfo &pi = J.pi;
+    pi.iteration = it;
+    pi.bounce = 2;
+    pi.flags = (cd.lighting_only ? PASS_LIGHTING_ONLY : 0u) | (cd.skip_direct_lighting ? PASS_SKIP_DIRECT : 0u) |
+               (cd.skip_indirect_lighting ? PASS_SKIP_INDIRECT : 0u) | (cd.no_background ? PASS_NO_BACKGROUND : 0u) |
+               (cd.clamp ? PASS_CLAMP : 0u) | (cd.output_sh ? PASS_OUTPUT_SH : 0u) | (cd.use_coherent_sampling ? PASS_COHERENT : 0u);
+    // pass_settings_t holds uint8 depths (Types.h:47-55); the total is capped at MAX_BOUNCES (RendererRef.cpp:111)
+    pi.max_diff_depth = (uint8_t)cd.max_diff_depth;
+    pi.max_glossy_depth = (uint8_t)cd.max_glossy_depth;
+    pi.max_refr_depth = (uint8_t)cd.max_refr_depth;
+    pi.max_transp_depth = (uint8_t)cd.max_transp_depth;
+    pi.max_total_depth = std::min((int)(uint8_t)cd.max_total_depth, MAX_BOUNCES);
+    pi.termination_start_depth = (uint8_t)cd.termination_start_depth;
+    pi.w = w;
+    // camera constants of GeneratePrimaryRays (CoreRef.cpp:430-432), computed on the host as on the CPU
+    J.cam.filter = cd.filter;
+    J.cam.fov = cd.fov;
+    J.cam.focus_distance = cd.focus_distance;
+    J.cam.focus_factor = cd.focus_factor;
+    for (int k = 0; k < 3; k++) {
+        J.cam.origin[k] = cam.origin[k];
+        J.cam.fwd[k] = cam.fwd[k];
+        J.cam.side[k] = cam.side[k];
+        J.cam.up[k] = cam.up[k];
+    }
+    const float PI = 3.141592653589793238463f;
+    J.k = float(w) / h;
+    J.fov_k = std::tan(0.5f * cd.fov * PI / 180.0f) * cd.focus_distance;
+    J.rx = rect.x;
+    J.ry = rect.y;
+    J.rw = rect.w;
+    J.rh = rect.h;
+    J.w = w;
+    J.h = h;
+    J.halton = static_cast<const float *>(r->d_halton.p);
+    J.temp = static_cast<float4 *>(r->d_temp.p);
+    J.clean = static_cast<float4 *>(r->d_clean.p);
+    J.fin = static_cast<float4 *>(r->d_final.p);
+    J.temp_sh = sh ? static_cast<SHData *>(r->d_temp_sh.p) : nullptr;
+    J.clean_sh = sh ? static_cast<SHData *>(r->d_clean_sh.p) : nullptr;
+    // accumulation and tone (RendererRef.cpp:292-324)
+    J.mix_k = 1.0f / it;
+    J.gamma = cd.gamma;
+    J.srgb = cd.dtype == 1 ? 1 : 0;
+    J.clamp = cd.clamp != 0 ? 1 : 0;
+    J.bounces = (pi.flags & PASS_SKIP_INDIRECT) ? 0 : pi.max_total_depth;
+    J.samples = samples;
+    J.pixel_base = 0;
+    r->pixels_on_host = r->sh_on_host = false;
+    return RAY_OK;
+}
+
+// The wavefront over the jobs in d_jobs (host copies in jobs): ray generation,
+// per bounce a closest-hit trace and a shading launch over the rays of all
+// jobs, then the accumulation. Buffers and counters are rb's. sample: offset
+// from each job's first iteration. ev (may be null): stats events.
+int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<FrameJob> &jobs, const std::vector<const ray_scene *> &scn,
+                  uint32_t total, int sample, cudaStream_t st, cudaEvent_t *ev, int &nb) {
+    nb = 0;
+    int rc = ensure_ray_buffers(rb, std::max<size_t>(total, 1));
+    if (rc != RAY_OK) return rc;
+    for (int k = 0; k < 2; k++) RG_CUDA_TRY(rb->d_job[k].ensure(std::max<size_t>(total, 1) * sizeof(uint32_t)));
+    uint32_t *cnt = static_cast<uint32_t *>(rb->d_counters.p);
+    unsigned long long *ray_stats = reinterpret_cast<unsigned long long *>(cnt + 4);
+    uint32_t *err = cnt + 3;
+    float4 *rays[2] = {static_cast<float4 *>(rb->d_rays[0].p), static_cast<float4 *>(rb->d_rays[1].p)};
+    RayPayload *pay[2] = {static_cast<RayPayload *>(rb->d_pay[0].p), static_cast<RayPayload *>(rb->d_pay[1].p)};
+    uint32_t *job[2] = {static_cast<uint32_t *>(rb->d_job[0].p), static_cast<uint32_t *>(rb->d_job[1].p)};
+    float4 *hits = static_cast<float4 *>(rb->d_hits.p);
+    int32_t *obj = static_cast<int32_t *>(rb->d_obj.p);
+    const int n_jobs = (int)jobs.size();
+    int bounces = 0;
+    TraceParams tp;
+    tp.persistent = scn[0]->tuning.kernel == 2;
+    tp.refill_min = scn[0]->tuning.refill_min;
+    for (int j = 0; j < n_jobs; j++) {
+        bounces = std::max(bounces, jobs[j].bounces);
+        tp.max_depth = std::max(tp.max_depth, scn[j]->tuning.deep_stack ? 0xffffffffu : scn[j]->max_depth);
+    }
+    tp.next_ray = cnt + 2;
+    if (n_jobs > 1) { // each ray traced in its job's scene
+        tp.views = reinterpret_cast<const uint8_t *>(d_jobs) + offsetof(FrameJob, sc) + offsetof(RenderScene, sv);
+        tp.view_stride = (uint32_t)sizeof(FrameJob);
+    }
+    const SceneView &sv = jobs[0].sc.sv;
+    // primary rays (GeneratePrimaryRays, CoreRef.cpp:427-505)
+    RG_CUDA_TRY(cudaMemsetAsync(cnt, 0, 2 * sizeof(uint32_t), st));
+    RG_CUDA_TRY(launch_raygen_jobs(d_jobs, n_jobs, total, sample, rays[0], pay[0], job[0], cnt + 0, st));
+    if (ev) RG_CUDA_TRY(cudaEventRecord(ev[1], st));
+    tp.count = cnt + 0;
+    tp.ray_job = job[0];
+    RG_CUDA_TRY(launch_trace_closest(sv, rays[0], total, hits, obj, err, nullptr, false, st, tp));
+    if (ev) RG_CUDA_TRY(cudaEventRecord(ev[2], st));
+    RG_CUDA_TRY(launch_shade_jobs(d_jobs, sample, 2, rays[0], pay[0], job[0], hits, obj, cnt + 0, total, rays[1], pay[1], job[1], cnt + 1,
+                                  err, ray_stats, st));
+    if (ev) RG_CUDA_TRY(cudaEventRecord(ev[3], st));
+    // bounces (RendererRef.cpp:183-278); ray counts stay on the device
+    int cur = 1;
+    for (int bounce = 0; bounce < bounces; bounce++) {
+        const int nxt = cur ^ 1;
+        RG_CUDA_TRY(cudaMemsetAsync(cnt + nxt, 0, sizeof(uint32_t), st));
+        tp.count = cnt + cur;
+        tp.ray_job = job[cur];
+        RG_CUDA_TRY(launch_trace_closest(sv, rays[cur], total, hits, obj, err, nullptr, false, st, tp));
+        if (ev) RG_CUDA_TRY(cudaEventRecord(ev[4 + 2 * bounce], st));
+        RG_CUDA_TRY(launch_shade_jobs(d_jobs, sample, bounce + 3, rays[cur], pay[cur], job[cur], hits, obj, cnt + cur, total, rays[nxt],
+                                      pay[nxt], job[nxt], cnt + nxt, err, ray_stats, st));
+        if (ev) RG_CUDA_TRY(cudaEventRecord(ev[5 + 2 * bounce], st));
+        cur = nxt;
+        nb++;
+    }
+    // accumulate and tone (RendererRef.cpp:292-324)
+    RG_CUDA_TRY(launch_resolve_jobs(d_jobs, n_jobs, total, sample, st));
     return RAY_OK;
 }
 
@@ -119,6 +342,9 @@ ray_renderer::~ray_renderer() {
     for (int s = 0; s < 2; s++)
         for (int e = 0; e < N_EVENTS; e++)
             if (ev_sets[s][e]) cudaEventDestroy(ev_sets[s][e]);
+    if (ev_sync) cudaEventDestroy(ev_sync);
+    for (int e = 0; e < 2; e++)
+        if (ev_batch[e]) cudaEventDestroy(ev_batch[e]);
     if (own_stream) cudaStreamDestroy(own_stream);
 }
 
@@ -188,156 +414,211 @@ int ray_clear(ray_renderer *r, const ray_pixel *c) {
 }
 
 int ray_render(ray_renderer *r, ray_scene *s, ray_region *region) {
-    if (!r || !s || !region) {
-        set_error("null argument");
-        return RAY_ERR_INVALID_ARG;
-    }
-    if (s->device != r->device) return RAY_OK; // a scene of another renderer: a no-op, as the reference's failed cast
-    if (s->current_cam >= s->cameras.size() || !s->cameras[s->current_cam].alive) {
-        set_error("the scene has no current camera");
-        return RAY_ERR_INVALID_ARG;
-    }
-    const CameraRec &cam = s->cameras[s->current_cam];
-    const ray_camera_desc &cd = cam.desc;
-    if (cd.type != 0) {
-        set_error("only perspective cameras are rendered");
-        return RAY_ERR_UNSUPPORTED;
-    }
     try {
-        RG_CUDA_TRY(cudaSetDevice(r->device));
-        int rc = commit(s);
-        if (rc != RAY_OK) return rc;
-        const int w = r->w, h = r->h;
-        ray_rect rect = region->rect;
-        if (rect.w == 0 || rect.h == 0) rect = ray_rect{0, 0, w, h};
-        if (rect.x < 0 || rect.y < 0 || rect.w < 0 || rect.h < 0 || rect.x + rect.w > w || rect.y + rect.h > h) {
-            set_error("region outside the framebuffer");
-            return RAY_ERR_INVALID_ARG;
-        }
-        const bool sh = cd.output_sh != 0;
-        rc = ensure_frame_buffers(r, sh);
-        if (rc != RAY_OK) return rc;
-        const size_t n_pix = (size_t)rect.w * rect.h;
-        rc = ensure_ray_buffers(r, std::max<size_t>(n_pix, 1));
+        FrameJob J;
+        ray_rect rect;
+        int rc = prepare_job(r, s, region, J, rect);
+        if (rc == PREPARE_NOTHING) return RAY_OK;
         if (rc != RAY_OK) return rc;
         cudaStream_t st = r->stream;
+        const size_t n_pix = (size_t)rect.w * rect.h;
 
         // stats of the frame two calls back are complete by now or soon
         const int set = (int)(r->frame & 1);
         rc = resolve_stats(r, set);
         if (rc != RAY_OK) return rc;
         cudaEvent_t *ev = r->ev_sets[set];
+        int tune_entry = -1;
+        const int kern = choose_kernel(r, s, (uint32_t)n_pix, J.bounces, tune_entry);
 
-        // RegionContext: iteration++, and the sample table regenerated every
-        // 256 iterations (RendererRef.cpp:85-89). For a region that starts at
-        // iteration 0 the table's base is 1 until iteration 255, then the
-        // iteration rounded down to a multiple of 256.
-        region->iteration++;
-        const int it = region->iteration;
-        const int base = it < HALTON_SEQ_LEN ? 1 : (it & ~(HALTON_SEQ_LEN - 1));
-        RG_CUDA_TRY(cudaEventRecord(ev[0], st));
-        if (base != r->halton_base) {
-            RG_CUDA_TRY(launch_halton_table(static_cast<const uint16_t *>(r->d_perms.p), base, static_cast<float *>(r->d_halton.p), st));
-            r->halton_base = base;
-        }
-        const float *halton = static_cast<const float *>(r->d_halton.p);
-
-        PassInfo pi{};
-        pi.iteration = it;
-        pi.bounce = 2;
-        pi.flags = (cd.lighting_only ? PASS_LIGHTING_ONLY : 0u) | (cd.skip_direct_lighting ? PASS_SKIP_DIRECT : 0u) |
-                   (cd.skip_indirect_lighting ? PASS_SKIP_INDIRECT : 0u) | (cd.no_background ? PASS_NO_BACKGROUND : 0u) |
-                   (cd.clamp ? PASS_CLAMP : 0u) | (cd.output_sh ? PASS_OUTPUT_SH : 0u) |
-                   (cd.use_coherent_sampling ? PASS_COHERENT : 0u);
-        // pass_settings_t holds uint8 depths (Types.h:47-55)
-        pi.max_diff_depth = (uint8_t)cd.max_diff_depth;
-        pi.max_glossy_depth = (uint8_t)cd.max_glossy_depth;
-        pi.max_refr_depth = (uint8_t)cd.max_refr_depth;
-        pi.max_transp_depth = (uint8_t)cd.max_transp_depth;
-        pi.max_total_depth = std::min((int)(uint8_t)cd.max_total_depth, MAX_BOUNCES);
-        pi.termination_start_depth = (uint8_t)cd.termination_start_depth;
-        pi.w = w;
-
-        // primary rays (GeneratePrimaryRays, CoreRef.cpp:427-505); the camera
-        // constants are computed here as on the CPU
-        CameraDev cdev{};
-        cdev.filter = cd.filter;
-        cdev.fov = cd.fov;
-        cdev.focus_distance = cd.focus_distance;
-        cdev.focus_factor = cd.focus_factor;
-        for (int k = 0; k < 3; k++) {
-            cdev.origin[k] = cam.origin[k];
-            cdev.fwd[k] = cam.fwd[k];
-            cdev.side[k] = cam.side[k];
-            cdev.up[k] = cam.up[k];
-        }
-        const float PI = 3.141592653589793238463f;
-        const float kx = float(w) / h;
-        const float fov_k = std::tan(0.5f * cd.fov * PI / 180.0f) * cd.focus_distance;
         uint32_t *cnt = static_cast<uint32_t *>(r->d_counters.p);
-        // [0], [1] ray counts of the two buffers, [2] trace work counter,
+        // [0], [1] ray counts of the two buffers, [2] trace / path work counter,
         // [3] error flags, [4..7] two uint64: rays traced, shadow segments
         RG_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8 * sizeof(uint32_t), st));
         unsigned long long *ray_stats = reinterpret_cast<unsigned long long *>(cnt + 4);
-        float4 *rays[2] = {static_cast<float4 *>(r->d_rays[0].p), static_cast<float4 *>(r->d_rays[1].p)};
-        RayPayload *pay[2] = {static_cast<RayPayload *>(r->d_pay[0].p), static_cast<RayPayload *>(r->d_pay[1].p)};
-        RG_CUDA_TRY(launch_raygen(cdev, kx, fov_k, it, rect.x, rect.y, rect.w, rect.h, w, h, halton, rays[0], pay[0], cnt + 0, st));
-        RG_CUDA_TRY(cudaEventRecord(ev[1], st));
-
-        const RenderScene sc = render_scene_view(s);
-        TraceParams tp;
-        tp.persistent = s->tuning.kernel == 2;
-        tp.refill_min = s->tuning.refill_min;
-        tp.max_depth = s->tuning.deep_stack ? 0xffffffffu : s->max_depth;
-        tp.next_ray = cnt + 2;
-        float4 *hits = static_cast<float4 *>(r->d_hits.p);
-        int32_t *obj = static_cast<int32_t *>(r->d_obj.p);
         uint32_t *err = cnt + 3;
-        const uint32_t max_rays = (uint32_t)n_pix;
-
-        tp.count = cnt + 0;
-        RG_CUDA_TRY(launch_trace_closest(sc.sv, rays[0], max_rays, hits, obj, err, nullptr, false, st, tp));
-        RG_CUDA_TRY(cudaEventRecord(ev[2], st));
-        RG_CUDA_TRY(launch_shade(sc, pi, halton, rays[0], pay[0], hits, obj, cnt + 0, max_rays, rays[1], pay[1], cnt + 1,
-                                 static_cast<float4 *>(r->d_temp.p), sh ? static_cast<SHData *>(r->d_temp_sh.p) : nullptr, true, err,
-                                 ray_stats, st));
-        RG_CUDA_TRY(cudaEventRecord(ev[3], st));
-
-        // bounces (RendererRef.cpp:183-278); ray counts stay on the device
+        RG_CUDA_TRY(cudaEventRecord(ev[0], st));
         int nb = 0;
-        if (!(pi.flags & PASS_SKIP_INDIRECT)) {
-            int cur = 1;
-            for (int bounce = 0; bounce < pi.max_total_depth; bounce++) {
-                const int nxt = cur ^ 1;
-                RG_CUDA_TRY(cudaMemsetAsync(cnt + nxt, 0, sizeof(uint32_t), st));
-                tp.count = cnt + cur;
-                RG_CUDA_TRY(launch_trace_closest(sc.sv, rays[cur], max_rays, hits, obj, err, nullptr, false, st, tp));
-                RG_CUDA_TRY(cudaEventRecord(ev[4 + 2 * bounce], st));
-                pi.bounce = bounce + 3;
-                RG_CUDA_TRY(launch_shade(sc, pi, halton, rays[cur], pay[cur], hits, obj, cnt + cur, max_rays, rays[nxt], pay[nxt],
-                                         cnt + nxt, static_cast<float4 *>(r->d_temp.p), nullptr, false, err, ray_stats, st));
-                RG_CUDA_TRY(cudaEventRecord(ev[5 + 2 * bounce], st));
-                cur = nxt;
-                nb++;
-            }
+        RG_CUDA_TRY(r->d_jobs.ensure(sizeof(FrameJob)));
+        RG_CUDA_TRY(cudaMemcpyAsync(r->d_jobs.p, &J, sizeof(FrameJob), cudaMemcpyHostToDevice, st));
+        const FrameJob *d_jobs = static_cast<const FrameJob *>(r->d_jobs.p);
+        if (kern == 2) {
+            // the whole frame in one launch; its time counts as primary trace in the stats
+            RG_CUDA_TRY(cudaEventRecord(ev[1], st));
+            RG_CUDA_TRY(launch_render_paths(d_jobs, 1, (uint32_t)n_pix, cnt + 2, err, ray_stats, st));
+            RG_CUDA_TRY(cudaEventRecord(ev[2], st));
+            RG_CUDA_TRY(cudaEventRecord(ev[3], st));
+        } else {
+            rc = run_wavefront(r, d_jobs, std::vector<FrameJob>{J}, std::vector<const ray_scene *>{s}, (uint32_t)n_pix, 0, st, ev, nb);
+            if (rc != RAY_OK) return rc;
         }
-
-        // accumulate and tone (RendererRef.cpp:292-324)
-        const float mix_factor = 1.0f / it;
-        RG_CUDA_TRY(launch_resolve(static_cast<const float4 *>(r->d_temp.p), static_cast<float4 *>(r->d_clean.p),
-                                   static_cast<float4 *>(r->d_final.p), sh ? static_cast<SHData *>(r->d_temp_sh.p) : nullptr,
-                                   sh ? static_cast<SHData *>(r->d_clean_sh.p) : nullptr, rect.x, rect.y, rect.w, rect.h, w, mix_factor,
-                                   cd.dtype == 1 ? 1 : 0, cd.gamma, cd.clamp != 0, sh, st));
         RG_CUDA_TRY(cudaEventRecord(ev[N_EVENTS - 1], st));
         r->ev_bounces[set] = nb;
+        r->ev_tune[set] = tune_entry;
+        r->ev_kernel[set] = kern;
+        if (tune_entry >= 0) r->tune[tune_entry].pending[kern - 1]++;
         r->ev_frame_pending[set] = true;
+        r->last_kernel = kern;
         r->frame++;
-        r->pixels_on_host = r->sh_on_host = false;
         return RAY_OK;
     } catch (const std::bad_alloc &) {
         set_error("host allocation failed");
         return RAY_ERR_OUT_OF_MEMORY;
     }
+}
+
+int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, ray_region *const *regions, int count, int samples) {
+    if (count < 0 || samples < 1 || (count > 0 && (!renderers || !scenes || !regions))) {
+        set_error("null argument");
+        return RAY_ERR_INVALID_ARG;
+    }
+    if (count == 0) return RAY_OK;
+    try {
+        ray_renderer *r0 = renderers[0];
+        for (int i = 0; i < count; i++) {
+            if (!renderers[i] || !scenes[i] || !regions[i]) {
+                set_error("null argument");
+                return RAY_ERR_INVALID_ARG;
+            }
+            if (renderers[i]->device != r0->device) {
+                set_error("a batch runs on one device: all renderers must share it");
+                return RAY_ERR_INVALID_ARG;
+            }
+            for (int j = 0; j < i; j++) {
+                if (regions[j] == regions[i]) {
+                    set_error("a region appears twice in the batch");
+                    return RAY_ERR_INVALID_ARG;
+                }
+                // one sample table per renderer and launch: its regions advance in step
+                if (renderers[j] == renderers[i] && regions[j]->iteration != regions[i]->iteration) {
+                    set_error("regions of one renderer in one batch must be at the same iteration");
+                    return RAY_ERR_INVALID_ARG;
+                }
+            }
+        }
+        RG_CUDA_TRY(cudaSetDevice(r0->device));
+        int rc = ensure_frame_state(r0);
+        if (rc != RAY_OK) return rc;
+        cudaStream_t st = r0->stream;
+        // kernel: the first renderer's setting; by default per batch configuration the
+        // faster of the two, timed (blocking) on the configuration's first calls
+        uint64_t px_all = 0, tris_all = 0;
+        for (int i = 0; i < count; i++) {
+            const ray_rect &q = regions[i]->rect;
+            px_all += (q.w == 0 || q.h == 0) ? (uint64_t)renderers[i]->w * renderers[i]->h : (uint64_t)q.w * q.h;
+            tris_all += scenes[i]->total_tris;
+        }
+        int kern = r0->kernel, tune_entry = -1;
+        if (kern == 0) {
+            for (size_t t = 0; t < r0->tune.size() && tune_entry < 0; t++) {
+                ray_renderer::TuneEntry &e = r0->tune[t];
+                if (e.scene == scenes[0] && e.bounces == -samples && e.lights == (uint32_t)count && e.pixels == (uint32_t)px_all &&
+                    e.tris == (uint32_t)tris_all)
+                    tune_entry = (int)t;
+            }
+            if (tune_entry < 0) {
+                if (r0->tune.size() >= 64) {
+                    r0->tune.clear();
+                    r0->ev_tune[0] = r0->ev_tune[1] = -1;
+                }
+                ray_renderer::TuneEntry e;
+                e.scene = scenes[0];
+                e.bounces = -samples; // a batch entry
+                e.lights = (uint32_t)count;
+                e.pixels = (uint32_t)px_all;
+                e.tris = (uint32_t)tris_all;
+                r0->tune.push_back(e);
+                tune_entry = (int)r0->tune.size() - 1;
+            }
+            const ray_renderer::TuneEntry &e = r0->tune[tune_entry];
+            if (e.choice) {
+                kern = e.choice;
+                tune_entry = -1;
+            } else {
+                kern = e.n[0] <= e.n[1] ? 1 : 2;
+            }
+        }
+        if (tune_entry >= 0) RG_CUDA_TRY(cudaEventRecord(r0->ev_batch[0], st));
+        for (int done = 0; done < samples;) {
+            // a run of iterations that keeps every region within one block of 256 (one sample table each)
+            int run = samples - done;
+            for (int i = 0; i < count; i++) run = std::min(run, HALTON_SEQ_LEN - ((regions[i]->iteration + 1) & (HALTON_SEQ_LEN - 1)));
+            std::vector<FrameJob> jobs;
+            std::vector<const ray_scene *> jscn;
+            jobs.reserve(count);
+            uint64_t total = 0;
+            for (int i = 0; i < count; i++) {
+                FrameJob J;
+                ray_rect rect;
+                rc = prepare_job(renderers[i], scenes[i], regions[i], J, rect, run);
+                if (rc == PREPARE_NOTHING) continue;
+                if (rc != RAY_OK) return rc;
+                J.pixel_base = (uint32_t)total;
+                total += (uint64_t)rect.w * rect.h;
+                if (total > 0xffffffffull) {
+                    set_error("too many pixels in one batch");
+                    return RAY_ERR_INVALID_ARG;
+                }
+                jobs.push_back(J);
+                jscn.push_back(scenes[i]);
+            }
+            // the batch runs on the first renderer's stream, after each renderer's own work
+            for (int i = 0; i < count; i++) {
+                ray_renderer *r = renderers[i];
+                if (r->stream == st) continue;
+                RG_CUDA_TRY(cudaEventRecord(r->ev_sync, r->stream));
+                RG_CUDA_TRY(cudaStreamWaitEvent(st, r->ev_sync, 0));
+            }
+            uint32_t *cnt = static_cast<uint32_t *>(r0->d_counters.p);
+            RG_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8 * sizeof(uint32_t), st));
+            if (!jobs.empty()) {
+                RG_CUDA_TRY(r0->d_jobs.ensure(jobs.size() * sizeof(FrameJob)));
+                RG_CUDA_TRY(cudaMemcpyAsync(r0->d_jobs.p, jobs.data(), jobs.size() * sizeof(FrameJob), cudaMemcpyHostToDevice, st));
+                const FrameJob *d_jobs = static_cast<const FrameJob *>(r0->d_jobs.p);
+                if (kern == 2) {
+                    RG_CUDA_TRY(launch_render_paths(d_jobs, (int)jobs.size(), (uint32_t)total, cnt + 2, cnt + 3,
+                                                    reinterpret_cast<unsigned long long *>(cnt + 4), st));
+                } else {
+                    for (int k = 0; k < run; k++) { // one wavefront per sample over the rays of all jobs
+                        int nb = 0;
+                        rc = run_wavefront(r0, d_jobs, jobs, jscn, (uint32_t)total, k, st, nullptr, nb);
+                        if (rc != RAY_OK) return rc;
+                    }
+                }
+            }
+            // and each renderer's later work (reads of its pixels, its next frames) after the batch
+            RG_CUDA_TRY(cudaEventRecord(r0->ev_sync, st));
+            for (int i = 0; i < count; i++) {
+                ray_renderer *r = renderers[i];
+                if (r->stream != st) RG_CUDA_TRY(cudaStreamWaitEvent(r->stream, r0->ev_sync, 0));
+                r->last_kernel = kern;
+            }
+            done += run;
+        }
+        if (tune_entry >= 0) { // a timed call of the kernel choice
+            RG_CUDA_TRY(cudaEventRecord(r0->ev_batch[1], st));
+            RG_CUDA_TRY(cudaEventSynchronize(r0->ev_batch[1]));
+            float ms = 0.0f;
+            RG_CUDA_TRY(cudaEventElapsedTime(&ms, r0->ev_batch[0], r0->ev_batch[1]));
+            ray_renderer::TuneEntry &e = r0->tune[tune_entry];
+            e.best[kern - 1] = std::min(e.best[kern - 1], ms);
+            e.n[kern - 1]++;
+            if (e.n[0] >= TUNE_SAMPLES && e.n[1] >= TUNE_SAMPLES) e.choice = e.best[1] < e.best[0] ? 2 : 1;
+        }
+        return RAY_OK;
+    } catch (const std::bad_alloc &) {
+        set_error("host allocation failed");
+        return RAY_ERR_OUT_OF_MEMORY;
+    }
+}
+
+int ray_renderer_set_kernel(ray_renderer *r, int kernel) {
+    if (!r || kernel < 0 || kernel > 2) {
+        set_error("kernel must be 0 (chosen by timing), 1 (wavefront) or 2 (path kernel)");
+        return RAY_ERR_INVALID_ARG;
+    }
+    r->kernel = kernel;
+    return RAY_OK;
 }
 
 int ray_get_pixels(ray_renderer *r, const ray_pixel **out, int on_device) {
@@ -422,6 +703,7 @@ int ray_renderer_frame_info(ray_renderer *r, ray_frame_info *out) {
     uint32_t c[8];
     RG_CUDA_TRY(cudaMemcpy(c, r->d_counters.p, sizeof(c), cudaMemcpyDeviceToHost));
     out->error_flags = c[3];
+    out->kernel = r->last_kernel;
     memcpy(&out->rays, c + 4, 8);
     memcpy(&out->shadow_rays, c + 6, 8);
     return RAY_OK;

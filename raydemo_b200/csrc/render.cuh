@@ -116,19 +116,46 @@ constexpr int HALTON_SEQ_LEN = 256;
 // entries past row 255 (RendererRef.cpp:327-358 with MAX_BOUNCES 10)
 constexpr int HALTON_TABLE_FLOATS = HALTON_COUNT * HALTON_SEQ_LEN + 64;
 
+// One (renderer, scene, region) of a frame, read by both kernels: the
+// wavefront (a launch per phase over the rays of all jobs) and the path
+// kernel (one thread follows one pixel's path through all its bounces). The
+// jobs of a launch cover consecutive global pixel ranges from pixel_base.
+struct FrameJob {
+    RenderScene sc;
+    PassInfo pi;       // bounce is set per bounce
+    CameraDev cam;
+    float k, fov_k;    // aspect ratio and tan(fov / 2) * focus distance
+    int rx, ry, rw, rh, w, h;
+    const float *halton;
+    float4 *temp, *clean, *fin;
+    SHData *temp_sh, *clean_sh; // null unless the camera outputs SH data
+    float mix_k, gamma;
+    int srgb, clamp;
+    int bounces;       // continuation rays traced: max_total_depth, or 0 with skip_indirect_lighting
+    int samples;       // consecutive iterations pi.iteration .. + samples - 1, one after another per pixel
+    uint32_t pixel_base;
+};
+
 // Launchers (render_kernels.cu). All stream-ordered; counts live on the device.
 cudaError_t launch_halton_table(const uint16_t *perms, int base_iteration, float *table, cudaStream_t st);
-cudaError_t launch_raygen(const CameraDev &cam, float k, float fov_k, int iteration, int rx, int ry, int rw, int rh, int w, int h, const float *halton,
-                          float4 *rays, RayPayload *pay, uint32_t *count, cudaStream_t st);
-// Shades the hits of *in_count rays; appends continuation rays to out (count
-// *out_count). primary: SetPixel into temp, else AddPixel with alpha 0.
-cudaError_t launch_shade(const RenderScene &sc, const PassInfo &pi, const float *halton, const float4 *rays, const RayPayload *pay,
-                         const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays, float4 *out_rays,
-                         RayPayload *out_pay, uint32_t *out_count, float4 *temp, SHData *temp_sh, bool primary, uint32_t *err,
-                         unsigned long long *ray_stats, cudaStream_t st);
-// clean += (temp - clean) * k over the rect, then final = tone(clean)
-cudaError_t launch_resolve(const float4 *temp, float4 *clean, float4 *fin, SHData *temp_sh, SHData *clean_sh, int rx, int ry, int rw,
-                           int rh, int w, float k, int srgb, float gamma, bool clamp, bool sh, cudaStream_t st);
+// The wavefront over the jobs of a launch (rays of several scenes together).
+// Ray generation: one ray per pixel of every job, ray_job[i] = job of ray i,
+// *count = total. Iterations are pi.iteration + sample.
+cudaError_t launch_raygen_jobs(const FrameJob *jobs, int n_jobs, uint32_t total, int sample, float4 *rays, RayPayload *pay,
+                               uint32_t *ray_job, uint32_t *count, cudaStream_t st);
+// Shades the hits of *in_count rays (bounce: pass_info_t::bounce, 2 for the
+// primary rays: SetPixel, else AddPixel with alpha 0) and appends the rays
+// that go on to out (count *out_count).
+cudaError_t launch_shade_jobs(const FrameJob *jobs, int sample, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
+                              const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays, float4 *out_rays,
+                              RayPayload *out_pay, uint32_t *out_job, uint32_t *out_count, uint32_t *err, unsigned long long *ray_stats,
+                              cudaStream_t st);
+// clean += (temp - clean) / iteration over every job's rect, then final = tone(clean)
+cudaError_t launch_resolve_jobs(const FrameJob *jobs, int n_jobs, uint32_t total, int sample, cudaStream_t st);
+// The whole frame of every job in one launch (ray generation, all bounces,
+// accumulation and tone): jobs in device memory, *work zeroed beforehand.
+cudaError_t launch_render_paths(const FrameJob *jobs, int n_jobs, uint32_t total_pixels, uint32_t *work, uint32_t *err,
+                                unsigned long long *ray_stats, cudaStream_t st);
 cudaError_t launch_fill(float4 *buf, size_t n, float4 v, cudaStream_t st);
 cudaError_t launch_fill_sh(SHData *buf, size_t n, cudaStream_t st);
 

@@ -60,15 +60,9 @@ __device__ __forceinline__ V3 pix_dir(const CameraDev &cam, float k, float fov_k
     return normalize(p - origin);
 }
 
-// GeneratePrimaryRays, CoreRef.cpp:427-505: one thread per pixel of the rect.
-__global__ void k_raygen(CameraDev cam, float k, float fov_k, int iteration, int rx, int ry, int rw, int rh, int w, int h,
-                         const float *__restrict__ halton, float4 *__restrict__ rays, RayPayload *__restrict__ pay,
-                         uint32_t *__restrict__ count) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t n = (uint32_t)rw * (uint32_t)rh;
-    if (i == 0) *count = n;
-    if (i >= n) return;
-    const int x = rx + (int)(i % (uint32_t)rw), y = ry + (int)(i / (uint32_t)rw);
+// GeneratePrimaryRays, CoreRef.cpp:427-505, for the pixel (x, y).
+__device__ __forceinline__ void gen_primary(const CameraDev &cam, float k, float fov_k, int iteration, int x, int y, int w, int h,
+                                            const float *__restrict__ halton, float4 &r0, float4 &r1, RayPayload &p) {
     const int index = y * w + x;
     const int hi = (iteration & (HALTON_SEQ_LEN - 1)) * HALTON_COUNT;
     float fx = (float)x, fy = (float)y;
@@ -93,9 +87,8 @@ __global__ void k_raygen(CameraDev cam, float k, float fov_k, int iteration, int
     const V3 d = pix_dir(cam, k, fov_k, w, h, fx, fy, origin);
     const V3 dx = pix_dir(cam, k, fov_k, w, h, fx + 1, fy, origin);
     const V3 dy = pix_dir(cam, k, fov_k, w, h, fx, fy + 1, origin);
-    rays[2ull * i] = make_float4(origin.x, origin.y, origin.z, MAX_DIST);
-    rays[2ull * i + 1] = make_float4(d.x, d.y, d.z, __int_as_float((x << 16) | y));
-    RayPayload p;
+    r0 = make_float4(origin.x, origin.y, origin.z, MAX_DIST);
+    r1 = make_float4(d.x, d.y, d.z, __int_as_float((x << 16) | y));
     p.c[0] = p.c[1] = p.c[2] = 1.0f;
     p.ior = 1.0f;
     const V3 ddx = dx - d, ddy = dy - d;
@@ -105,7 +98,30 @@ __global__ void k_raygen(CameraDev cam, float k, float fov_k, int iteration, int
     p.dd_dy[0] = ddy.x; p.dd_dy[1] = ddy.y; p.dd_dy[2] = ddy.z;
     p.ray_depth = 0;
     p.pad[0] = p.pad[1] = p.pad[2] = 0;
-    pay[i] = p;
+}
+
+// Closest hit of one ray against the whole scene: the instance loop of
+// Traverse_MacroTree_WithStack_ClosestHit (CoreRef.cpp:1133-1222), as the
+// trace kernels run it.
+__device__ __forceinline__ Best trace_closest_scene(const SceneView &sv, float4 r0, float4 r1, Stack<true> &st, uint32_t &err) {
+    Best best;
+    best.t = r0.w;
+    best.u = best.v = 0.0f;
+    best.prim = best.obj = -1;
+    const float sx = trav::safe_inv(r1.x), sy = trav::safe_inv(r1.y), sz = trav::safe_inv(r1.z);
+    uint32_t nvis = 0, ntri = 0;
+    for (uint32_t m = 0; m < sv.n_inst; m++) {
+        const InstanceRec *ir = sv.inst + m;
+        float bmin[3], bmax[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            bmin[q] = __ldg(&ir->bbox_min[q]);
+            bmax[q] = __ldg(&ir->bbox_max[q]);
+        }
+        if (!trav::ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
+        trav::trace_mesh<false, true>(trav::mesh_of(sv, ir, (int)m), trav::transform_ray(ir, r0, r1), best, st, err, nvis, ntri);
+    }
+    return best;
 }
 
 // Shadow ray against the whole scene: the instance loop of
@@ -561,111 +577,30 @@ __device__ F4 shade_surface(const RenderScene &sc, const PassInfo &pi, int rand_
     return F4{ray.c[0] * col.x, ray.c[1] * col.y, ray.c[2] * col.z, 1.0f};
 }
 
-template <bool PRIMARY>
-__global__ void __launch_bounds__(SHADE_BLOCK) k_shade(RenderScene sc, PassInfo pi, const float *__restrict__ halton,
-                                                       const float4 *__restrict__ rays, const RayPayload *__restrict__ pay,
-                                                       const float4 *__restrict__ hits, const int32_t *__restrict__ obj,
-                                                       const uint32_t *__restrict__ in_count, uint32_t max_rays, float4 *__restrict__ out_rays,
-                                                       RayPayload *__restrict__ out_pay, uint32_t *__restrict__ out_count,
-                                                       float4 *__restrict__ temp, SHData *__restrict__ temp_sh, uint32_t *__restrict__ err_out,
-                                                       unsigned long long *__restrict__ ray_stats) {
-    __shared__ uint2 s_stack[trav::SMEM_STACK * SHADE_BLOCK];
-    Stack<true> st;
-    st.smem = s_stack + threadIdx.x;
-    st.sp = 0;
-    uint32_t err = 0, nshadow = 0;
-    const uint32_t n = min(*in_count, max_rays);
-    const uint32_t lane = threadIdx.x & 31u;
-    for (uint32_t base = blockIdx.x * SHADE_BLOCK; base < n; base += gridDim.x * SHADE_BLOCK) {
-        const uint32_t i = base + threadIdx.x;
-        bool emit = false;
-        NewRay nr;
-        if (i < n) {
-            const float4 r0 = rays[2ull * i], r1 = rays[2ull * i + 1];
-            const RayPayload p = pay[i];
-            const uint32_t xy = __float_as_uint(r1.w);
-            const int x = (int)(xy >> 16), y = (int)(xy & 0xffffu);
-            const int index = y * pi.w + x;
-            const int rand_index = (pi.flags & PASS_COHERENT) ? c_sampling_pattern[(y % 8) * 8 + (x % 8)] : index;
-            const F4 c = shade_surface(sc, pi, rand_index, halton, hits[i], obj[i], r0, r1, p, nr, emit, st, err, nshadow);
-            if (PRIMARY) {
-                temp[index] = make_float4(c.x, c.y, c.z, c.w);
-                if (temp_sh) {
-                    // ResetSampleData + SetSampleDir/SetSampleWeight (FramebufferRef.h:69-88)
-                    SHData &s = temp_sh[index];
-                    s.coeff_g[0] = 0.0f;
-                    if (emit) {
-                        const float SH_Y0 = 0.282094806f, SH_Y1 = 0.488602519f;
-                        s.coeff_r[0] = SH_Y0;
-                        s.coeff_r[1] = SH_Y1 * nr.r1.y;
-                        s.coeff_r[2] = SH_Y1 * nr.r1.z;
-                        s.coeff_r[3] = SH_Y1 * nr.r1.x;
-                        s.coeff_g[0] = nr.p.c[0];
-                    }
-                }
-            } else {
-                float4 acc = temp[index];
-                acc.x += c.x;
-                acc.y += c.y;
-                acc.z += c.z;
-                acc.w += 0.0f;
-                temp[index] = acc;
-            }
-        }
-        // warp-aggregated append of the continuation rays
-        const uint32_t m = __ballot_sync(0xffffffffu, emit);
-        if (m) {
-            uint32_t slot = 0;
-            const uint32_t leader = __ffs(m) - 1;
-            if (lane == leader) slot = atomicAdd(out_count, (uint32_t)__popc(m));
-            slot = __shfl_sync(0xffffffffu, slot, leader) + __popc(m & ((1u << lane) - 1u));
-            if (emit && slot < max_rays) {
-                out_rays[2ull * slot] = nr.r0;
-                out_rays[2ull * slot + 1] = nr.r1;
-                out_pay[slot] = nr.p;
-            }
-        }
-    }
-    if (err) atomicOr(err_out, err);
-    // rays shaded (each was traced once) and shadow-ray segments traced
-    if (ray_stats) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&ray_stats[0], (unsigned long long)n);
-        const uint32_t ws = __reduce_add_sync(0xffffffffu, nshadow);
-        if (lane == 0 && ws) atomicAdd(&ray_stats[1], (unsigned long long)ws);
-    }
-}
-
 // Framebuffer::MixWith, ComputeSHData, MixWith_SH (FramebufferRef.cpp:57-101)
 // and the tone step of RenderScene (RendererRef.cpp:301-324).
-__global__ void k_resolve(const float4 *__restrict__ temp, float4 *__restrict__ clean, float4 *__restrict__ fin, SHData *__restrict__ temp_sh,
-                          SHData *__restrict__ clean_sh, int rx, int ry, int rw, int rh, int w, float k, int srgb, float gamma, int clamp,
-                          int sh) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (uint32_t)rw * (uint32_t)rh) return;
-    const int x = rx + (int)(i % (uint32_t)rw), y = ry + (int)(i / (uint32_t)rw);
-    const size_t idx = (size_t)y * w + x;
-    const float4 p = temp[idx];
+// p: the pixel's sample; s (may be null): its SH sample data, rewritten in place.
+__device__ __forceinline__ void resolve_pixel(float4 p, float4 *__restrict__ clean, float4 *__restrict__ fin, SHData *s,
+                                              SHData *__restrict__ clean_sh, size_t idx, float k, int srgb, float gamma, int clamp) {
     float4 c = clean[idx];
     c.x += (p.x - c.x) * k;
     c.y += (p.y - c.y) * k;
     c.z += (p.z - c.z) * k;
     c.w += (p.w - c.w) * k;
     clean[idx] = c;
-    if (sh) {
-        SHData s = temp_sh[idx];
-        const float inv_weight = s.coeff_g[0] > FLT_EPS_ ? (2.0f * PI_F / s.coeff_g[0]) : 0.0f;
+    if (s) {
+        const float inv_weight = s->coeff_g[0] > FLT_EPS_ ? (2.0f * PI_F / s->coeff_g[0]) : 0.0f;
         const float pr = p.x * inv_weight, pg = p.y * inv_weight, pb = p.z * inv_weight;
         for (int j = 0; j < 4; j++) {
-            s.coeff_g[j] = s.coeff_r[j] * pg;
-            s.coeff_b[j] = s.coeff_r[j] * pb;
-            s.coeff_r[j] = s.coeff_r[j] * pr;
+            s->coeff_g[j] = s->coeff_r[j] * pg;
+            s->coeff_b[j] = s->coeff_r[j] * pb;
+            s->coeff_r[j] = s->coeff_r[j] * pr;
         }
-        temp_sh[idx] = s;
         SHData o = clean_sh[idx];
         for (int j = 0; j < 4; j++) {
-            o.coeff_r[j] += (s.coeff_r[j] - o.coeff_r[j]) * k;
-            o.coeff_g[j] += (s.coeff_g[j] - o.coeff_g[j]) * k;
-            o.coeff_b[j] += (s.coeff_b[j] - o.coeff_b[j]) * k;
+            o.coeff_r[j] += (s->coeff_r[j] - o.coeff_r[j]) * k;
+            o.coeff_g[j] += (s->coeff_g[j] - o.coeff_g[j]) * k;
+            o.coeff_b[j] += (s->coeff_b[j] - o.coeff_b[j]) * k;
         }
         clean_sh[idx] = o;
     }
@@ -687,6 +622,239 @@ __global__ void k_resolve(const float4 *__restrict__ temp, float4 *__restrict__ 
         }
     }
     fin[idx] = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// Job of a global ray or pixel index: the jobs cover consecutive ranges from pixel_base.
+__device__ __forceinline__ int job_of(const FrameJob *__restrict__ jobs, int n_jobs, uint32_t p) {
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].pixel_base <= p) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Primary rays of every job, one thread per pixel: job-major, row-major in
+// each job's rect. ray_job[i] records the job of ray i.
+__global__ void k_raygen_jobs(const FrameJob *__restrict__ jobs, int n_jobs, uint32_t total, int sample, float4 *__restrict__ rays,
+                              RayPayload *__restrict__ pay, uint32_t *__restrict__ ray_job, uint32_t *__restrict__ count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *count = total;
+    if (i >= total) return;
+    const int j = job_of(jobs, n_jobs, i);
+    const FrameJob &J = jobs[j];
+    const uint32_t li = i - J.pixel_base;
+    const int x = J.rx + (int)(li % (uint32_t)J.rw), y = J.ry + (int)(li / (uint32_t)J.rw);
+    float4 r0, r1;
+    RayPayload p;
+    gen_primary(J.cam, J.k, J.fov_k, J.pi.iteration + sample, x, y, J.w, J.h, J.halton, r0, r1, p);
+    rays[2ull * i] = r0;
+    rays[2ull * i + 1] = r1;
+    pay[i] = p;
+    ray_job[i] = (uint32_t)j;
+}
+
+// Shading of *in_count rays of any jobs (bounce: pass_info_t::bounce, 2 for
+// primary rays). PRIMARY: SetPixel into the job's sample buffer, else AddPixel
+// with alpha 0. A continuation ray is appended where the path goes on and its
+// job traces another bounce.
+template <bool PRIMARY>
+__global__ void __launch_bounds__(SHADE_BLOCK) k_shade_jobs(const FrameJob *__restrict__ jobs, int sample, int bounce,
+                                                            const float4 *__restrict__ rays, const RayPayload *__restrict__ pay,
+                                                            const uint32_t *__restrict__ ray_job, const float4 *__restrict__ hits,
+                                                            const int32_t *__restrict__ obj, const uint32_t *__restrict__ in_count,
+                                                            uint32_t max_rays, float4 *__restrict__ out_rays, RayPayload *__restrict__ out_pay,
+                                                            uint32_t *__restrict__ out_job, uint32_t *__restrict__ out_count,
+                                                            uint32_t *__restrict__ err_out, unsigned long long *__restrict__ ray_stats) {
+    __shared__ uint2 s_stack[trav::SMEM_STACK * SHADE_BLOCK];
+    Stack<true> st;
+    st.smem = s_stack + threadIdx.x;
+    st.sp = 0;
+    uint32_t err = 0, nshadow = 0;
+    const uint32_t n = min(*in_count, max_rays);
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * SHADE_BLOCK; base < n; base += gridDim.x * SHADE_BLOCK) {
+        const uint32_t i = base + threadIdx.x;
+        bool append = false;
+        uint32_t j = 0;
+        NewRay nr;
+        if (i < n) {
+            j = ray_job[i];
+            const FrameJob &J = jobs[j];
+            const float4 r0 = rays[2ull * i], r1 = rays[2ull * i + 1];
+            const RayPayload p = pay[i];
+            const uint32_t xy = __float_as_uint(r1.w);
+            const int x = (int)(xy >> 16), y = (int)(xy & 0xffffu);
+            const int index = y * J.w + x;
+            PassInfo pi = J.pi;
+            pi.iteration += sample;
+            pi.bounce = bounce;
+            const int rand_index = (pi.flags & PASS_COHERENT) ? c_sampling_pattern[(y % 8) * 8 + (x % 8)] : index;
+            bool emit = false;
+            const F4 c = shade_surface(J.sc, pi, rand_index, J.halton, hits[i], obj[i], r0, r1, p, nr, emit, st, err, nshadow);
+            append = emit && bounce - 2 < J.bounces;
+            if (PRIMARY) {
+                J.temp[index] = make_float4(c.x, c.y, c.z, c.w);
+                if (J.temp_sh) {
+                    // ResetSampleData + SetSampleDir/SetSampleWeight (FramebufferRef.h:69-88)
+                    SHData &s = J.temp_sh[index];
+                    s.coeff_g[0] = 0.0f;
+                    if (emit) {
+                        const float SH_Y0 = 0.282094806f, SH_Y1 = 0.488602519f;
+                        s.coeff_r[0] = SH_Y0;
+                        s.coeff_r[1] = SH_Y1 * nr.r1.y;
+                        s.coeff_r[2] = SH_Y1 * nr.r1.z;
+                        s.coeff_r[3] = SH_Y1 * nr.r1.x;
+                        s.coeff_g[0] = nr.p.c[0];
+                    }
+                }
+            } else {
+                float4 acc = J.temp[index];
+                acc.x += c.x;
+                acc.y += c.y;
+                acc.z += c.z;
+                acc.w += 0.0f;
+                J.temp[index] = acc;
+            }
+        }
+        // warp-aggregated append of the continuation rays
+        const uint32_t m = __ballot_sync(0xffffffffu, append);
+        if (m) {
+            uint32_t slot = 0;
+            const uint32_t leader = __ffs(m) - 1;
+            if (lane == leader) slot = atomicAdd(out_count, (uint32_t)__popc(m));
+            slot = __shfl_sync(0xffffffffu, slot, leader) + __popc(m & ((1u << lane) - 1u));
+            if (append && slot < max_rays) {
+                out_rays[2ull * slot] = nr.r0;
+                out_rays[2ull * slot + 1] = nr.r1;
+                out_pay[slot] = nr.p;
+                out_job[slot] = j;
+            }
+        }
+    }
+    if (err) atomicOr(err_out, err);
+    // rays shaded (each was traced once) and shadow-ray segments traced
+    if (ray_stats) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&ray_stats[0], (unsigned long long)n);
+        const uint32_t ws = __reduce_add_sync(0xffffffffu, nshadow);
+        if (lane == 0 && ws) atomicAdd(&ray_stats[1], (unsigned long long)ws);
+    }
+}
+
+// Accumulation and tone of every job's rect, one thread per pixel.
+__global__ void k_resolve_jobs(const FrameJob *__restrict__ jobs, int n_jobs, uint32_t total, int sample) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const FrameJob &J = jobs[job_of(jobs, n_jobs, i)];
+    const uint32_t li = i - J.pixel_base;
+    const int x = J.rx + (int)(li % (uint32_t)J.rw), y = J.ry + (int)(li / (uint32_t)J.rw);
+    const size_t idx = (size_t)y * J.w + x;
+    const float mix_k = 1.0f / (J.pi.iteration + sample); // RendererRef.cpp:293
+    if (J.temp_sh) {
+        SHData s = J.temp_sh[idx];
+        resolve_pixel(J.temp[idx], J.clean, J.fin, &s, J.clean_sh, idx, mix_k, J.srgb, J.gamma, J.clamp);
+        J.temp_sh[idx] = s;
+    } else {
+        resolve_pixel(J.temp[idx], J.clean, J.fin, nullptr, nullptr, idx, mix_k, J.srgb, J.gamma, J.clamp);
+    }
+}
+
+// The path kernel: one thread follows one pixel's path through ray
+// generation, every bounce (closest hit, shading, shadow rays) and the
+// accumulation, with the same arithmetic as the wavefront kernels, so both
+// give the same image. Warps take 32 pixels at a time from *work across all
+// jobs of the launch.
+__device__ __forceinline__ void render_path(const FrameJob &J, uint32_t i, int iteration, Stack<true> &st, uint32_t &err,
+                                            uint32_t &nshadow, uint32_t &nrays) {
+    const int x = J.rx + (int)(i % (uint32_t)J.rw), y = J.ry + (int)(i / (uint32_t)J.rw);
+    const int index = y * J.w + x;
+    float4 r0, r1;
+    RayPayload pay;
+    gen_primary(J.cam, J.k, J.fov_k, iteration, x, y, J.w, J.h, J.halton, r0, r1, pay);
+    const int rand_index = (J.pi.flags & PASS_COHERENT) ? c_sampling_pattern[(y % 8) * 8 + (x % 8)] : index;
+    PassInfo pi = J.pi;
+    pi.iteration = iteration;
+    pi.bounce = 2;
+    Best b = trace_closest_scene(J.sc.sv, r0, r1, st, err);
+    nrays++;
+    NewRay nr;
+    bool emit = false;
+    F4 c = shade_surface(J.sc, pi, rand_index, J.halton,
+                         make_float4(__int_as_float(b.prim), b.t, b.prim >= 0 ? b.u : 0.0f, b.prim >= 0 ? b.v : 0.0f), b.obj, r0, r1, pay, nr,
+                         emit, st, err, nshadow);
+    float4 acc = make_float4(c.x, c.y, c.z, c.w);
+    SHData s;
+    if (J.temp_sh) {
+        // ResetSampleData + SetSampleDir/SetSampleWeight (FramebufferRef.h:69-88)
+        s = J.temp_sh[index];
+        s.coeff_g[0] = 0.0f;
+        if (emit) {
+            const float SH_Y0 = 0.282094806f, SH_Y1 = 0.488602519f;
+            s.coeff_r[0] = SH_Y0;
+            s.coeff_r[1] = SH_Y1 * nr.r1.y;
+            s.coeff_r[2] = SH_Y1 * nr.r1.z;
+            s.coeff_r[3] = SH_Y1 * nr.r1.x;
+            s.coeff_g[0] = nr.p.c[0];
+        }
+    }
+    for (int bounce = 0; bounce < J.bounces && emit; bounce++) {
+        r0 = nr.r0;
+        r1 = nr.r1;
+        pay = nr.p;
+        b = trace_closest_scene(J.sc.sv, r0, r1, st, err);
+        nrays++;
+        pi.bounce = bounce + 3;
+        c = shade_surface(J.sc, pi, rand_index, J.halton,
+                          make_float4(__int_as_float(b.prim), b.t, b.prim >= 0 ? b.u : 0.0f, b.prim >= 0 ? b.v : 0.0f), b.obj, r0, r1, pay,
+                          nr, emit, st, err, nshadow);
+        acc.x += c.x;
+        acc.y += c.y;
+        acc.z += c.z;
+        acc.w += 0.0f;
+    }
+    J.temp[index] = acc;
+    const float mix_k = 1.0f / iteration; // RendererRef.cpp:293
+    if (J.temp_sh) {
+        resolve_pixel(acc, J.clean, J.fin, &s, J.clean_sh, (size_t)index, mix_k, J.srgb, J.gamma, J.clamp);
+        J.temp_sh[index] = s;
+    } else {
+        resolve_pixel(acc, J.clean, J.fin, nullptr, nullptr, (size_t)index, mix_k, J.srgb, J.gamma, J.clamp);
+    }
+}
+
+__global__ void __launch_bounds__(SHADE_BLOCK) k_render_paths(const FrameJob *__restrict__ jobs, int n_jobs, uint32_t total,
+                                                              uint32_t *__restrict__ work, uint32_t *__restrict__ err_out,
+                                                              unsigned long long *__restrict__ ray_stats) {
+    __shared__ uint2 s_stack[trav::SMEM_STACK * SHADE_BLOCK];
+    Stack<true> st;
+    st.smem = s_stack + threadIdx.x;
+    st.sp = 0;
+    uint32_t err = 0, nshadow = 0, nrays = 0;
+    const uint32_t lane = threadIdx.x & 31u;
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(work, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) break;
+        const uint32_t p = base + lane;
+        if (p < total) {
+            int lo = 0, hi = n_jobs - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (jobs[mid].pixel_base <= p) lo = mid;
+                else hi = mid - 1;
+            }
+            const FrameJob &J = jobs[lo];
+            for (int k = 0; k < J.samples; k++) render_path(J, p - J.pixel_base, J.pi.iteration + k, st, err, nshadow, nrays);
+        }
+    }
+    if (err) atomicOr(err_out, err);
+    if (ray_stats) {
+        const uint32_t wr = __reduce_add_sync(0xffffffffu, nrays), ws = __reduce_add_sync(0xffffffffu, nshadow);
+        if (lane == 0 && wr) atomicAdd(&ray_stats[0], (unsigned long long)wr);
+        if (lane == 0 && ws) atomicAdd(&ray_stats[1], (unsigned long long)ws);
+    }
 }
 
 __global__ void k_fill(float4 *buf, size_t n, float4 v) {
@@ -712,40 +880,55 @@ cudaError_t launch_halton_table(const uint16_t *perms, int base_iteration, float
     return cudaGetLastError();
 }
 
-cudaError_t launch_raygen(const CameraDev &cam, float k, float fov_k, int iteration, int rx, int ry, int rw, int rh, int w, int h,
-                          const float *halton, float4 *rays, RayPayload *pay, uint32_t *count, cudaStream_t st) {
-    const uint32_t n = (uint32_t)rw * (uint32_t)rh;
-    k_raygen<<<(n + 255) / 256, 256, 0, st>>>(cam, k, fov_k, iteration, rx, ry, rw, rh, w, h, halton, rays, pay, count);
+cudaError_t launch_raygen_jobs(const FrameJob *jobs, int n_jobs, uint32_t total, int sample, float4 *rays, RayPayload *pay,
+                               uint32_t *ray_job, uint32_t *count, cudaStream_t st) {
+    if (total == 0) return cudaSuccess;
+    k_raygen_jobs<<<(total + 255) / 256, 256, 0, st>>>(jobs, n_jobs, total, sample, rays, pay, ray_job, count);
     return cudaGetLastError();
 }
 
-cudaError_t launch_shade(const RenderScene &sc, const PassInfo &pi, const float *halton, const float4 *rays, const RayPayload *pay,
-                         const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays, float4 *out_rays,
-                         RayPayload *out_pay, uint32_t *out_count, float4 *temp, SHData *temp_sh, bool primary, uint32_t *err,
-                         unsigned long long *ray_stats, cudaStream_t st) {
+cudaError_t launch_shade_jobs(const FrameJob *jobs, int sample, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
+                              const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays, float4 *out_rays,
+                              RayPayload *out_pay, uint32_t *out_job, uint32_t *out_count, uint32_t *err, unsigned long long *ray_stats,
+                              cudaStream_t st) {
     if (g_shade_blocks == 0) {
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_shade<false>, SHADE_BLOCK, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_shade_jobs<false>, SHADE_BLOCK, 0);
         g_shade_blocks = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 4);
     }
     const uint32_t need = (max_rays + SHADE_BLOCK - 1) / SHADE_BLOCK;
     const uint32_t blocks = need < (uint32_t)g_shade_blocks ? (need > 0 ? need : 1) : (uint32_t)g_shade_blocks;
-    if (primary)
-        k_shade<true><<<blocks, SHADE_BLOCK, 0, st>>>(sc, pi, halton, rays, pay, hits, obj, in_count, max_rays, out_rays, out_pay, out_count, temp,
-                                                      temp_sh, err, ray_stats);
+    if (bounce == 2)
+        k_shade_jobs<true><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, sample, bounce, rays, pay, ray_job, hits, obj, in_count, max_rays, out_rays,
+                                                           out_pay, out_job, out_count, err, ray_stats);
     else
-        k_shade<false><<<blocks, SHADE_BLOCK, 0, st>>>(sc, pi, halton, rays, pay, hits, obj, in_count, max_rays, out_rays, out_pay, out_count,
-                                                       temp, temp_sh, err, ray_stats);
+        k_shade_jobs<false><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, sample, bounce, rays, pay, ray_job, hits, obj, in_count, max_rays, out_rays,
+                                                            out_pay, out_job, out_count, err, ray_stats);
     return cudaGetLastError();
 }
 
-cudaError_t launch_resolve(const float4 *temp, float4 *clean, float4 *fin, SHData *temp_sh, SHData *clean_sh, int rx, int ry, int rw, int rh,
-                           int w, float k, int srgb, float gamma, bool clamp, bool sh, cudaStream_t st) {
-    const uint32_t n = (uint32_t)rw * (uint32_t)rh;
-    k_resolve<<<(n + 255) / 256, 256, 0, st>>>(temp, clean, fin, temp_sh, clean_sh, rx, ry, rw, rh, w, k, srgb, gamma, clamp ? 1 : 0,
-                                               sh ? 1 : 0);
+cudaError_t launch_resolve_jobs(const FrameJob *jobs, int n_jobs, uint32_t total, int sample, cudaStream_t st) {
+    if (total == 0) return cudaSuccess;
+    k_resolve_jobs<<<(total + 255) / 256, 256, 0, st>>>(jobs, n_jobs, total, sample);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_render_paths(const FrameJob *jobs, int n_jobs, uint32_t total_pixels, uint32_t *work, uint32_t *err,
+                                unsigned long long *ray_stats, cudaStream_t st) {
+    static int blocks = 0;
+    if (blocks == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_paths, SHADE_BLOCK, 0);
+        blocks = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 2);
+    }
+    if (total_pixels == 0 || n_jobs <= 0) return cudaSuccess;
+    const uint32_t need = (total_pixels + SHADE_BLOCK - 1) / SHADE_BLOCK;
+    const uint32_t grid = need < (uint32_t)blocks ? need : (uint32_t)blocks;
+    k_render_paths<<<grid, SHADE_BLOCK, 0, st>>>(jobs, n_jobs, total_pixels, work, err, ray_stats);
     return cudaGetLastError();
 }
 

@@ -128,7 +128,7 @@ struct ray_renderer {
     rg::DeviceBuf d_temp, d_clean, d_final, d_temp_sh, d_clean_sh;
     // wavefront: two ray buffers (trace record + payload), hits, instance ids,
     // counters [0..1] ray counts, [2] persistent-trace work counter, [3] errors
-    rg::DeviceBuf d_rays[2], d_pay[2], d_hits, d_obj, d_counters;
+    rg::DeviceBuf d_rays[2], d_pay[2], d_job[2], d_hits, d_obj, d_counters;
     rg::DeviceBuf d_halton, d_perms;
     int halton_base = -1; // base iteration of the table in d_halton
     bool pixels_on_host = false, sh_on_host = false;
@@ -139,5 +139,22 @@ struct ray_renderer {
     bool ev_frame_pending[2] = {false, false};
     int ev_bounces[2] = {0, 0};
     uint64_t frame = 0;
+    cudaEvent_t ev_sync = nullptr;        // orders this renderer's stream against a batch
+    cudaEvent_t ev_batch[2] = {};         // times the batches of the kernel choice
+
+    // kernel choice: 0 by timing per frame configuration, 1 wavefront, 2 path kernel
+    int kernel = 0, last_kernel = 0;
+    struct TuneEntry {
+        const void *scene = nullptr;
+        uint32_t tris = 0, lights = 0, pixels = 0;
+        int bounces = 0;
+        int choice = 0;                 // 0 while timing
+        float best[2] = {1e30f, 1e30f}; // best frame time (ms) of each kernel
+        int n[2] = {0, 0}, pending[2] = {0, 0};
+    };
+    std::vector<TuneEntry> tune;
+    int ev_tune[2] = {-1, -1}; // tune entry timed by the frame in each event set
+    int ev_kernel[2] = {0, 0};
+    rg::DeviceBuf d_jobs;      // FrameJob array of the path kernel
     ~ray_renderer();
 };

@@ -86,12 +86,15 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
 // state. Each loop iteration of a warp: refill lanes without a ray when
 // enough of them are idle, advance lanes to their next instance (or finish
 // their ray), then one node step plus the triangles it hit.
-template <bool COUNT, bool DEEP>
+// MULTI: rays of several scenes in one launch; ray i belongs to the scene
+// whose SceneView is at views + ray_job[i] * view_stride.
+template <bool COUNT, bool DEEP, bool MULTI = false>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, const float4 *__restrict__ rays, uint32_t n,
                                                                   float4 *__restrict__ hits, int32_t *__restrict__ obj_out,
                                                                   uint32_t *__restrict__ err_out, unsigned long long *__restrict__ counters,
                                                                   uint32_t *__restrict__ next_ray, int refill_min,
-                                                                  const uint32_t *__restrict__ n_dev) {
+                                                                  const uint32_t *__restrict__ n_dev, const uint8_t *__restrict__ views = nullptr,
+                                                                  uint32_t view_stride = 0, const uint32_t *__restrict__ ray_job = nullptr) {
     if (n_dev) n = min(n, *n_dev);
     __shared__ uint2 s_stack[SMEM_STACK * TRACE_BLOCK];
     Stack<DEEP> st;
@@ -136,8 +139,11 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
         if (!in_mesh) {
             const float4 r0 = __ldg(rays + 2ull * ri), r1 = __ldg(rays + 2ull * ri + 1);
             const float sx = safe_inv(r1.x), sy = safe_inv(r1.y), sz = safe_inv(r1.z);
-            while (mi < sv.n_inst) {
-                const InstanceRec *ir = sv.inst + mi;
+            SceneView job_sv;
+            if (MULTI) job_sv = *reinterpret_cast<const SceneView *>(views + (size_t)__ldg(ray_job + ri) * view_stride);
+            const SceneView &lsv = MULTI ? job_sv : sv;
+            while (mi < lsv.n_inst) {
+                const InstanceRec *ir = lsv.inst + mi;
                 float bmin[3], bmax[3];
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
@@ -146,7 +152,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
                 }
                 mi++;
                 if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
-                mr = mesh_of(sv, ir, (int)mi - 1);
+                mr = mesh_of(lsv, ir, (int)mi - 1);
                 r = transform_ray(ir, r0, r1);
                 ng_base = 0;
                 ng_bits = (1u << (24 + r.oct)) | 1u;
@@ -207,7 +213,7 @@ int g_persistent_blocks[2] = {0, 0};
 template <bool DEEP>
 cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
                         unsigned long long *counters, bool count, cudaStream_t st, const TraceParams &tp) {
-    if (!tp.persistent) {
+    if (!tp.persistent && !tp.views) {
         const uint32_t grid = (n + TRACE_BLOCK - 1) / TRACE_BLOCK;
         if (count)
             k_trace_closest<true, DEEP><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.count);
@@ -227,6 +233,11 @@ cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, flo
     }
     cudaError_t e = cudaMemsetAsync(tp.next_ray, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
+    if (tp.views) { // rays of several scenes (no counting variant)
+        k_trace_persistent<false, DEEP, true><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray,
+                                                                               tp.refill_min, tp.count, tp.views, tp.view_stride, tp.ray_job);
+        return cudaGetLastError();
+    }
     if (count)
         k_trace_persistent<true, DEEP><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min,
                                                                         tp.count);

@@ -25,6 +25,11 @@ struct TraceParams {
     uint32_t max_depth = 0; // deepest wide BVH among the traced meshes (sizes the stack)
     uint32_t *next_ray = nullptr; // device work counter for the persistent kernel
     const uint32_t *count = nullptr; // device ray count: when set, min(n, *count) rays are traced
+    // rays of several scenes (persistent kernel only): ray i is traced in the
+    // SceneView at views + ray_job[i] * view_stride, and the sv argument is unused
+    const uint8_t *views = nullptr;
+    uint32_t view_stride = 0;
+    const uint32_t *ray_job = nullptr;
 };
 
 // rays: n x 8 floats (ox, oy, oz, tmax, dx, dy, dz, unused).

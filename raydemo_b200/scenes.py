@@ -203,3 +203,131 @@ def cornell_box(seed: int = 0, w: int = 256, h: int = 256, max_bounces: int = 4)
 
 def spec_triangles(spec: dict) -> int:
     return int(sum(len(m[1]) // 3 for m in spec["meshes"]))
+
+
+# ---------------------------------------------------------------- batched form
+
+_ICO_V = np.array([(-1, 1.618033988749895, 0), (1, 1.618033988749895, 0), (-1, -1.618033988749895, 0), (1, -1.618033988749895, 0),
+                   (0, -1, 1.618033988749895), (0, 1, 1.618033988749895), (0, -1, -1.618033988749895), (0, 1, -1.618033988749895),
+                   (1.618033988749895, 0, -1), (1.618033988749895, 0, 1), (-1.618033988749895, 0, -1), (-1.618033988749895, 0, 1)])
+_ICO_F = np.array([(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6), (7, 1, 8),
+                   (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)])
+
+
+def grid_sphere(level: int):
+    """Icosphere with 20 * 4^level triangles: each icosahedron face split into
+    an n x n triangle grid (n = 2^level) and projected to the unit sphere.
+    Vertices on shared edges are repeated per face. Returns (positions (v, 3)
+    float64, indices (t, 3) uint32)."""
+    n = 1 << level
+    ii, jj = np.meshgrid(np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    keep = ii + jj <= n
+    I, J = ii[keep], jj[keep]                       # barycentric grid of one face
+    vid = -np.ones((n + 1, n + 1), np.int64)
+    vid[I, J] = np.arange(len(I))
+    a, b = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    up = a + b <= n - 1
+    t_up = np.stack([vid[a[up], b[up]], vid[a[up] + 1, b[up]], vid[a[up], b[up] + 1]], 1)
+    dn = a + b <= n - 2
+    t_dn = np.stack([vid[a[dn] + 1, b[dn]], vid[a[dn] + 1, b[dn] + 1], vid[a[dn], b[dn] + 1]], 1)
+    tri1 = np.concatenate([t_up, t_dn])
+    V = _ICO_V / np.linalg.norm(_ICO_V, axis=1, keepdims=True)
+    p0, p1, p2 = V[_ICO_F[:, 0]], V[_ICO_F[:, 1]], V[_ICO_F[:, 2]]
+    w1, w2 = I / n, J / n
+    pts = p0[:, None, :] + (p1 - p0)[:, None, :] * w1[None, :, None] + (p2 - p0)[:, None, :] * w2[None, :, None]
+    pts = pts.reshape(-1, 3)
+    pts /= np.linalg.norm(pts, axis=1, keepdims=True)
+    faces = (tri1[None, :, :] + (np.arange(20) * len(I))[:, None, None]).reshape(-1, 3)
+    return pts, faces.astype(np.uint32)
+
+
+def value_noise(p: np.ndarray, seed: int) -> np.ndarray:
+    """3D value noise in [-1, 1]: hashed lattice values, smooth trilinear blend."""
+    q = np.floor(p).astype(np.int64)
+    f = p - q
+    f = f * f * (3 - 2 * f)
+
+    def h(x, y, z):
+        v = (x * 73856093) ^ (y * 19349663) ^ (z * 83492791) ^ (seed * 2654435761)
+        v = (v ^ (v >> 13)) * 1274126177
+        v = v ^ (v >> 16)
+        return (v & 0xFFFF) / 32767.5 - 1.0
+
+    x, y, z = q[:, 0], q[:, 1], q[:, 2]
+    c = [[[h(x + i, y + j, z + k) for k in (0, 1)] for j in (0, 1)] for i in (0, 1)]
+    fx, fy, fz = f[:, 0], f[:, 1], f[:, 2]
+    lerp = lambda a, b, t: a + (b - a) * t
+    return lerp(lerp(lerp(c[0][0][0], c[0][0][1], fz), lerp(c[0][1][0], c[0][1][1], fz), fy),
+                lerp(lerp(c[1][0][0], c[1][0][1], fz), lerp(c[1][1][0], c[1][1][1], fz), fy), fx)
+
+
+def displaced_sphere(level: int, seed: int, amplitude: float = 0.05, freq: float = 4.0):
+    """Icosphere of 20 * 4^level triangles with value-noise displacement of
+    the radius; PxyzNxyzTuv attributes (normals from the displaced faces)."""
+    pos, faces = grid_sphere(level)
+    pos = pos * (1.0 + amplitude * value_noise(pos * freq, seed))[:, None]
+    e1 = pos[faces[:, 1]] - pos[faces[:, 0]]
+    e2 = pos[faces[:, 2]] - pos[faces[:, 0]]
+    fn = np.cross(e1, e2)
+    nrm = np.zeros_like(pos)
+    for k in range(3):
+        np.add.at(nrm, faces[:, k], fn)
+    nrm /= np.maximum(np.linalg.norm(nrm, axis=1, keepdims=True), 1e-20)
+    uv = np.stack([0.5 + np.arctan2(pos[:, 2], pos[:, 0]) / (2 * np.pi), 0.5 - np.arcsin(np.clip(pos[:, 1], -1, 1)) / np.pi], 1)
+    return np.concatenate([pos, nrm, uv], 1).astype(np.float32), faces.reshape(-1)
+
+
+def _trs(rng, scale_range=(0.5, 2.0), spread=6.0):
+    s = rng.uniform(*scale_range)
+    a = rng.uniform(0, 2 * np.pi)
+    c, si = np.cos(a), np.sin(a)
+    m = np.eye(4, dtype=np.float32)
+    m[0, 0], m[0, 2], m[2, 0], m[2, 2] = c * s, -si * s, si * s, c * s
+    m[1, 1] = s
+    m[3, 0:3] = (rng.uniform(-spread, spread), s, rng.uniform(-spread, spread))
+    return m.reshape(-1)
+
+
+def batch_scene(seed: int, max_bounces: int = 6) -> dict:
+    """One scene of the batched configuration: a ground plane and displaced
+    icospheres (instanced, random TRS with scale U[0.5, 2]) with a total
+    triangle count log-uniform in [1,000, 500,000], a resolution drawn from
+    {64, 128, 256, 512, 1024} squared, Ref materials (Oren-Nayar diffuse and
+    glossy), a sun (directional light) and a sky colour."""
+    rng = np.random.default_rng(1000 + seed)
+    target = float(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
+    res = int(rng.choice([64, 128, 256, 512, 1024]))
+    level = int(np.clip(np.floor(np.log(target / 20.0) / np.log(4.0)), 1, 6))
+    per = 20 * 4 ** level
+    count = int(np.clip(round(target / per), 1, 24))
+    white = np.full((1, 1, 4), 255, np.uint8)
+    spec = {"textures": [(white, False, False)], "materials": [], "meshes": [], "instances": [], "size": (res, res),
+            "env": {"env_col": (0.35, 0.45, 0.6)}}
+    mats = spec["materials"]
+    mats.append({"type": 0, "main_color": (0.5, 0.5, 0.45), "main_texture": 2, "roughness": 0.5})  # ground
+    for _ in range(4):
+        if rng.uniform() < 0.3:
+            mats.append({"type": 1, "main_color": tuple(float(x) for x in rng.uniform(0.5, 0.95, 3)), "main_texture": 2,
+                         "roughness": float(rng.uniform(0.05, 0.6))})
+        else:
+            mats.append({"type": 0, "main_color": tuple(float(x) for x in rng.uniform(0.2, 0.8, 3)), "main_texture": 2,
+                         "roughness": float(rng.uniform(0.0, 1.0))})
+    g, gi = _quad((-40, 0, -40), (-40, 0, 40), (40, 0, 40), (40, 0, -40), (0, 1, 0))
+    spec["meshes"].append((g, gi, [(0, 0, 0, 6)], 0))
+    spec["instances"].append((0, np.eye(4, dtype=np.float32).reshape(-1)))
+    n_meshes = min(count, 3)
+    for m in range(n_meshes):
+        a, i = displaced_sphere(level, seed * 7 + m)
+        mat = 1 + m % 4
+        spec["meshes"].append((a, i, [(mat, mat, 0, len(i))], 0))
+    for k in range(count):
+        spec["instances"].append((1 + k % n_meshes, _trs(rng)))
+    sun = rng.normal(size=3)
+    sun[1] = -abs(sun[1]) - 1.0
+    spec["lights"] = [{"type": 2, "position": (0.0, 0.0, 0.0), "radius": 0.0, "color": (2.5, 2.4, 2.2),
+                       "direction": tuple(float(x) for x in sun / np.linalg.norm(sun)), "angle": 1.0}]
+    spec["camera"] = {"type": 0, "filter": 1, "dtype": 0, "origin": (0.0, 9.0, -16.0), "fwd": (0.0, -0.45, 0.9), "up": (0.0, 1.0, 0.0),
+                      "fov": 55.0, "gamma": 1.0, "max_total_depth": max_bounces, "max_diff_depth": max_bounces,
+                      "max_glossy_depth": max_bounces, "termination_start_depth": 3}
+    spec["tris"] = 2 + count * per
+    return spec

@@ -52,9 +52,10 @@ def build_ref(ref, spec: dict):
     return sc
 
 
-def render_gpu(spec: dict, iterations: int, rect=(0, 0, 0, 0)):
+def render_gpu(spec: dict, iterations: int, rect=(0, 0, 0, 0), kernel: int = 0):
     w, h = spec["size"]
     r = api.Renderer(w, h)
+    r.set_kernel(kernel)
     sc = build_gpu(r, spec)
     r.Clear()
     reg = api.RegionContext(*rect)

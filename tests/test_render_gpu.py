@@ -68,6 +68,7 @@ def test_sample_table_and_primary_rays_bit_exact(reflib, cuda_device, ref_tests)
     spec = _mesh_lights_spec(ref_tests, 48, 40)
     spec["camera"].update(filter=api.Tent, focus_factor=0.3, focus_distance=1.7, skip_indirect_lighting=True)
     r = api.Renderer(48, 40)
+    r.set_kernel(1)  # the wavefront keeps the primary rays in its first buffer
     sc = build_gpu(r, spec)
     rect = (5, 3, 30, 29)
     reg = api.RegionContext(*rect)
@@ -112,9 +113,10 @@ def test_mesh_lights_golden(ref_tests, cuda_device):
     assert diff <= 1.0, diff
 
 
-def test_mesh_lights_matches_ref_renderer(reflib, ref_tests, cuda_device):
+@pytest.mark.parametrize("kernel", [1, 2], ids=["wavefront", "path"])
+def test_mesh_lights_matches_ref_renderer(reflib, ref_tests, cuda_device, kernel):
     spec = _mesh_lights_spec(ref_tests)
-    gpu, _, _ = render_gpu(spec, 16)
+    gpu, _, _ = render_gpu(spec, 16, kernel=kernel)
     cpu = render_ref(reflib, spec, 16)
     d = image_diff(gpu, cpu)
     assert d["rmse"] <= 1e-3, d
@@ -129,24 +131,26 @@ def test_texture_scene(ref_tests, cuda_device):
     assert d <= 0.0015, d
 
 
-def test_texture_matches_ref_renderer(reflib, ref_tests, cuda_device):
+@pytest.mark.parametrize("kernel", [1, 2], ids=["wavefront", "path"])
+def test_texture_matches_ref_renderer(reflib, ref_tests, cuda_device, kernel):
     spec = _texture_spec(ref_tests)
-    gpu, _, _ = render_gpu(spec, 4)
+    gpu, _, _ = render_gpu(spec, 4, kernel=kernel)
     cpu = render_ref(reflib, spec, 4)
     d = image_diff(gpu, cpu)
     assert d["rmse"] <= 1e-3, d
 
 
-def test_cornell_matches_ref_renderer(reflib, cuda_device):
+@pytest.mark.parametrize("kernel", [1, 2], ids=["wavefront", "path"])
+def test_cornell_matches_ref_renderer(reflib, cuda_device, kernel):
     """The small render configuration (Cornell box, 256x256, 1 sample, 4
     bounces) against the reference's Ref renderer."""
     spec = scenes.cornell_box(0)
-    gpu, _, _ = render_gpu(spec, 1)
+    gpu, _, _ = render_gpu(spec, 1, kernel=kernel)
     cpu = render_ref(reflib, spec, 1)
     d = image_diff(gpu, cpu)
     print("cornell 1 spp", d)
     assert d["identical_px"] >= 0.95, d
-    gpu8, _, _ = render_gpu(spec, 8)
+    gpu8, _, _ = render_gpu(spec, 8, kernel=kernel)
     cpu8 = render_ref(reflib, spec, 8)
     d8 = image_diff(gpu8, cpu8)
     print("cornell 8 spp", d8)
@@ -186,9 +190,10 @@ def _lights_spec():
     return spec
 
 
-def test_lights_and_materials_match_ref_renderer(reflib, cuda_device):
+@pytest.mark.parametrize("kernel", [1, 2], ids=["wavefront", "path"])
+def test_lights_and_materials_match_ref_renderer(reflib, cuda_device, kernel):
     spec = _lights_spec()
-    gpu, _, _ = render_gpu(spec, 4)
+    gpu, _, _ = render_gpu(spec, 4, kernel=kernel)
     cpu = render_ref(reflib, spec, 4)
     d = image_diff(gpu, cpu)
     print("lights/materials 4 spp", d)
@@ -196,13 +201,14 @@ def test_lights_and_materials_match_ref_renderer(reflib, cuda_device):
     assert d["rmse"] <= 2e-2, d
 
 
-def test_region_and_sh_match_ref_renderer(reflib, ref_tests, cuda_device):
+@pytest.mark.parametrize("kernel", [1, 2], ids=["wavefront", "path"])
+def test_region_and_sh_match_ref_renderer(reflib, ref_tests, cuda_device, kernel):
     """A sub-rectangle region, coherent sampling and spherical-harmonics output
     (test_mesh_lights mode 1)."""
     spec = _mesh_lights_spec(ref_tests)
     spec["camera"].update(output_sh=True, use_coherent_sampling=True)
     rect = (8, 4, 40, 52)
-    gpu, r, _ = render_gpu(spec, 8, rect=rect)
+    gpu, r, _ = render_gpu(spec, 8, rect=rect, kernel=kernel)
     cpu = render_ref(reflib, spec, 8, rect=rect)
     d = image_diff(gpu, cpu)
     assert d["identical_px"] >= 0.95, d
@@ -230,3 +236,48 @@ def test_clear_resize_stats(ref_tests, cuda_device):
     assert r.get_pixels_ref().shape == (24, 40, 4)
     with pytest.raises(api.capi.RayError):
         r.RenderScene(sc, api.RegionContext(30, 0, 20, 10))  # outside the framebuffer
+
+
+@pytest.mark.parametrize("kernel", [1, 2], ids=["wavefront", "path"])
+def test_batch_matches_single_renders(reflib, ref_tests, cuda_device, kernel):
+    """The batched form: four scenes of different sizes (the mesh-lights
+    scene, the texture scene, the Cornell box and the lights/materials scene,
+    one of them as two regions of one framebuffer) rendered together, 3
+    samples in two calls: the images equal each scene rendered alone, and the
+    Cornell box equals the Ref renderer's."""
+    specs = [_mesh_lights_spec(ref_tests), _texture_spec(ref_tests), scenes.cornell_box(0), _lights_spec()]
+    rs, scs = [], []
+    for sp in specs:
+        w, h = sp["size"]
+        r = api.Renderer(w, h)
+        rs.append(r)
+        scs.append(build_gpu(r, sp))
+        r.Clear()
+    rs[0].set_kernel(kernel)
+    w3, h3 = specs[3]["size"]
+    regions = [api.RegionContext(), api.RegionContext(), api.RegionContext(), api.RegionContext(0, 0, w3, h3 // 2),
+               api.RegionContext(0, h3 // 2, w3, h3 - h3 // 2)]
+    rr = rs + [rs[3]]
+    ss = scs + [scs[3]]
+    api.render_batch(rr, ss, regions)       # one sample
+    api.render_batch(rr, ss, regions, 2)    # two more in one call
+    info = rs[0].frame_info()
+    assert info.kernel == kernel and info.error_flags == 0
+    for sp, r in zip(specs, rs):
+        alone, _, _ = render_gpu(sp, 3, kernel=1)
+        batch = r.get_pixels_ref()
+        np.testing.assert_array_equal(batch.view(np.uint32), alone.view(np.uint32))
+    cpu = render_ref(reflib, specs[2], 3)
+    d = image_diff(rs[2].get_pixels_ref(), cpu)
+    assert d["rmse"] <= 2e-2 and d["identical_px"] >= 0.95, d
+
+
+def test_kernel_choice_by_timing(ref_tests, cuda_device):
+    """Default kernel choice: both kernels are timed on the first frames of a
+    configuration, then one is kept; the image is the same either way."""
+    spec = _mesh_lights_spec(ref_tests, 32, 32)
+    img_auto, r, _ = render_gpu(spec, 12)
+    kinds = {r.frame_info().kernel}
+    img_wave, _, _ = render_gpu(spec, 12, kernel=1)
+    np.testing.assert_array_equal(img_auto.view(np.uint32), img_wave.view(np.uint32))
+    assert kinds <= {1, 2}
