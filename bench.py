@@ -297,17 +297,25 @@ def batch_frames(args, dev, stream, n_scenes: int = 64, samples: int = 4) -> dic
         api.render_batch(rs, scs, regs, samples)
         return regs
 
-    # warm-up: the plain loop twice (each renderer times both kernels on its first frames), the batch once
-    plain_pass()
-    plain_pass()
-    torch.cuda.synchronize(dev)
-    ev0.record(stream)
-    plain_pass()
-    ev1.record(stream)
-    torch.cuda.synchronize(dev)
-    plain_ms = ev0.elapsed_time(ev1)
-    plain_imgs = [r.get_pixels_ref() for r in rs]
-    kernels = [r.frame_info().kernel for r in rs]
+    plain_ms, plain_imgs, kernels = None, None, []
+    if not args.batch_no_plain:
+        # warm-up: the plain loop twice (each renderer times both kernels on its first frames)
+        plain_pass()
+        plain_pass()
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        plain_pass()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        plain_ms = ev0.elapsed_time(ev1)
+        plain_imgs = [r.get_pixels_ref() for r in rs]
+        kernels = [r.frame_info().kernel for r in rs]
+    if args.batch_no_plain:  # profiling: the batch alone, wavefront
+        rs[0].set_kernel(1)
+        batch_pass()
+        batch_pass()
+        torch.cuda.synchronize(dev)
+        return {"workload": BATCH_WORKLOAD, "profiling_run": True}
 
     def timed_batch(kernel: int, warm: int) -> float:
         rs[0].set_kernel(kernel)  # the batch follows the first renderer's setting
@@ -382,7 +390,7 @@ def run_gpu_arm(args) -> None:
         if args.render_only:
             out = {"render": render_frames(args, dev, stream, rank, world)}
         else:
-            out = {"batch": batch_frames(args, dev, stream)}
+            out = {"batch": batch_frames(args, dev, stream, n_scenes=args.batch_scenes)}
         if rank == 0:
             print(json.dumps(out), flush=True)
         if world > 1:
@@ -523,6 +531,8 @@ def main() -> None:
     ap.add_argument("--render-only", action="store_true", help="only the render-loop frames (no microbench, no CPU baseline)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-form measurement")
     ap.add_argument("--batch-only", action="store_true", help="only the batched-form measurement")
+    ap.add_argument("--batch-no-plain", action="store_true", help="with --batch-only: two wavefront batches, nothing timed (profiling)")
+    ap.add_argument("--batch-scenes", type=int, default=64, help="with --batch-only: the first N scenes of the batch")
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes per launch of the traversal kernel from an ncu capture (reported as roofline.traffic)")
     args = ap.parse_args()
