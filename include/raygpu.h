@@ -69,10 +69,32 @@ typedef struct ray_stats {
 
 /* eMaterialType (SceneBase.h:45-52) */
 enum { RAY_MAT_DIFFUSE = 0, RAY_MAT_GLOSSY, RAY_MAT_REFRACTIVE, RAY_MAT_EMISSIVE, RAY_MAT_MIX, RAY_MAT_TRANSPARENT };
+/* Extension with no counterpart in the reference: a metallic-roughness
+ * material (Lambert diffuse + GGX microfacet specular, Smith height-correlated
+ * shadowing, Schlick Fresnel with F0 = 0.04 for the dielectric part). Base
+ * colour = main_color x main_texture (bilinear, level 0; RAY_INVALID_INDEX:
+ * white; the normal map is not used), roughness (alpha =
+ * roughness^2), metallic in ray_mat_desc::metallic. It takes direct light by
+ * next-event estimation from RAY_LIGHT_QUAD and RAY_LIGHT_SUN lights (quad
+ * lights also by its sampled rays, combined by multiple importance sampling),
+ * and indirect light from emissive surfaces and the environment; the
+ * reference's point, spot and directional lights light only the reference's
+ * materials. Its random numbers come from a padded 2D Sobol sequence with
+ * hash-based Owen scrambling per pixel (the reference's materials keep the
+ * reference's Halton table). */
+#define RAY_MAT_PRINCIPLED 6
 /* eVertexLayout (SceneBase.h:27-32) */
 enum { RAY_LAYOUT_PNT = 0, RAY_LAYOUT_PNTT, RAY_LAYOUT_PNBT, RAY_LAYOUT_PNBTT };
 /* eLightType (SceneBase.h:108-112) */
 enum { RAY_LIGHT_POINT = 0, RAY_LIGHT_SPOT, RAY_LIGHT_DIRECTIONAL };
+/* Extensions with no counterpart in the reference, used by RAY_MAT_PRINCIPLED:
+ * QUAD: a one-sided rectangle p = position + s * edge_u + t * edge_v
+ * (s, t in [0, 1], edges perpendicular) emitting radiance `color` towards
+ * edge_u x edge_v; not part of the geometry (rays pass through it). SUN: light
+ * arriving from -direction within a cone of `angle` degrees (full angle),
+ * irradiance `color` on a surface facing it. */
+#define RAY_LIGHT_QUAD 3
+#define RAY_LIGHT_SUN 4
 
 /* mat_desc_t (SceneBase.h:55-67) */
 typedef struct ray_mat_desc {
@@ -80,6 +102,7 @@ typedef struct ray_mat_desc {
     float main_color[3];
     uint32_t main_texture, normal_map, mix_materials[2];
     float roughness, strength, fresnel, int_ior, ext_ior;
+    float metallic; /* RAY_MAT_PRINCIPLED only (not in the reference's mat_desc_t) */
 } ray_mat_desc;
 
 /* shape_desc_t (SceneBase.h:70-81) */
@@ -115,6 +138,7 @@ typedef struct ray_light_desc {
     float position[3], radius;
     float color[3];
     float direction[3], angle;
+    float edge_u[3], edge_v[3]; /* RAY_LIGHT_QUAD only (not in the reference's light_desc_t) */
 } ray_light_desc;
 
 /* camera_desc_t (SceneBase.h:122-145) */

@@ -69,6 +69,9 @@ class Oracle:
         L.orc_hash.restype = C.c_int32
         L.orc_construct_float.argtypes = [C.c_uint32]
         L.orc_construct_float.restype = C.c_float
+        L.orc_render_principled.argtypes = [C.POINTER(OrcPrincipledScene), C.POINTER(OrcCamera), i32, i32, i32, i32, i32, i32, vp, i32]
+        L.orc_area_light.argtypes = [i32, vp, vp, vp, C.c_float, vp, vp, vp]
+        L.orc_area_light.restype = i32
 
     # -- triangles / hits
     def preprocess_tris(self, pos: np.ndarray, idx: np.ndarray, stride: int = 3) -> np.ndarray:
@@ -143,6 +146,132 @@ class Oracle:
         out = np.zeros(24 * 256, np.float32)
         self.lib.orc_halton_table(iteration, _p(perms), _p(out))
         return out
+
+    # -- metallic-roughness scenes
+    def area_light(self, type: int, position=(0.0, 0.0, 0.0), color=(1.0, 1.0, 1.0), direction=(0.0, -1.0, 0.0), angle=0.0,
+                   edge_u=(0.0, 0.0, 0.0), edge_v=(0.0, 0.0, 0.0), **_) -> np.ndarray:
+        out = np.zeros(20, np.float32)
+        args = [np.asarray(v, np.float32) for v in (position, color, direction)]
+        eu, ev = np.asarray(edge_u, np.float32), np.asarray(edge_v, np.float32)
+        if self.lib.orc_area_light(type, _p(args[0]), _p(args[1]), _p(args[2]), C.c_float(angle), _p(eu), _p(ev), _p(out)) != 0:
+            raise ValueError("invalid quad or sun light")
+        return out
+
+    def principled_scene(self, spec: dict) -> "PrincipledScene":
+        """Flattens a scene spec (the format of raydemo_b200.scenes) whose
+        materials are all RAY_MAT_PRINCIPLED and whose lights are quad or sun
+        lights into the arrays orc_render_principled reads."""
+        return PrincipledScene(self, spec)
+
+    def render_principled(self, spec: dict, spp: int, nthreads: int = 8, scene: "PrincipledScene" = None) -> np.ndarray:
+        """The renderer's clean buffer (mean of iterations 1..spp), (h, w, 4)."""
+        ps = scene if scene is not None else self.principled_scene(spec)
+        w, h = spec["size"]
+        cam = spec["camera"]
+        c = self.construct_camera(cam["origin"], cam["fwd"], cam["up"], cam.get("fov", 45.0), filter=cam.get("filter", 1),
+                                  gamma=cam.get("gamma", 1.0), focus_distance=cam.get("focus_distance", 1.0),
+                                  focus_factor=cam.get("focus_factor", 0.0))
+        out = np.zeros((h, w, 4), np.float32)
+        self.lib.orc_render_principled(C.byref(ps.c), C.byref(c), w, h, spp, cam.get("max_diff_depth", 4), cam.get("max_total_depth", 4),
+                                       cam.get("termination_start_depth", 3), _p(out), nthreads)
+        return out
+
+
+class OrcPrincipledScene(C.Structure):
+    _fields_ = [("tris", C.c_void_p), ("aabbs", C.c_void_p), ("normals", C.c_void_p), ("uvs", C.c_void_p), ("mat", C.c_void_p),
+                ("mesh_tris", C.c_void_p), ("inst_mesh", C.c_void_p), ("inst_xform", C.c_void_p), ("mats", C.c_void_p),
+                ("texels", C.c_void_p), ("tex_info", C.c_void_p), ("lights", C.c_void_p), ("ntris", C.c_int64), ("nmeshes", C.c_int),
+                ("ninst", C.c_int), ("nmats", C.c_int), ("ntex", C.c_int), ("nlights", C.c_int), ("env_col", C.c_float * 3)]
+
+
+class PrincipledScene:
+    """The arrays of one scene spec for orc_render_principled (kept alive with
+    the structure that points at them)."""
+
+    INVALID = 0xFFFFFFFF
+    FIRST_TEXTURE = 2  # a scene's textures 0 and 1 are its default environment and normal map
+
+    def __init__(self, orc: Oracle, spec: dict):
+        texels, tex_info, off = [], [], 0
+        for rgba, srgb, _mips in spec.get("textures", []):
+            a = np.ascontiguousarray(rgba, np.uint8)
+            th, tw = a.shape[:2]
+            texels.append(a.view(np.uint32).reshape(-1))
+            tex_info += [off, tw, th, int(bool(srgb))]
+            off += tw * th
+        ntex = len(tex_info) // 4
+        mats = []
+        for m in spec.get("materials", []):
+            if m.get("type") != 6:
+                raise ValueError("only metallic-roughness materials")
+            t = m.get("main_texture", self.INVALID)
+            if t == self.INVALID:
+                ti = -1
+            elif self.FIRST_TEXTURE <= t < self.FIRST_TEXTURE + ntex:
+                ti = t - self.FIRST_TEXTURE
+            else:
+                raise ValueError("main texture must be one of the spec's textures")
+            mats += [*map(float, m.get("main_color", (1.0, 1.0, 1.0))), float(m.get("roughness", 0.0)), float(m.get("metallic", 0.0)),
+                     float(ti), 0.0, 0.0]
+        tris, aabbs, normals, uvs, mat, mesh_tris = [], [], [], [], [], []
+        first = 0
+        for attrs, idx, shapes, layout in spec.get("meshes", []):
+            stride = (8, 10, 11, 13)[layout]
+            A = np.ascontiguousarray(attrs, np.float32).reshape(-1, stride)
+            I = np.ascontiguousarray(idx, np.uint32).reshape(-1, 3)
+            n = len(I)
+            uv_off = 6 if layout in (0, 1) else 9
+            V = A[I.astype(np.int64)]  # (n, 3, stride)
+            tris.append(orc.preprocess_tris(np.ascontiguousarray(A[:, :3]), I))
+            aabbs.append(np.concatenate([V[:, :, :3].min(axis=1), V[:, :, :3].max(axis=1)], axis=1))
+            normals.append(V[:, :, 3:6].reshape(n, 9))
+            uvs.append(V[:, :, uv_off:uv_off + 2].reshape(n, 6))
+            mt = np.zeros((n, 2), np.int32)  # triangles no shape covers: material 0 on both sides
+            for s in shapes:
+                if len(s) == 3:
+                    s = (s[0], self.INVALID, s[1], s[2])
+                mi, back, start, count = (int(x) for x in s)
+                for i in range(start, start + count, 3):
+                    if i // 3 < n:
+                        mt[i // 3] = (mi, -1 if back == self.INVALID else back)
+            mat.append(mt)
+            mesh_tris += [first, n]
+            first += n
+        inst_mesh, inst_xform = [], []
+        for mesh, xf in spec.get("instances", []):
+            inst_mesh.append(int(mesh))
+            inst_xform.append(np.eye(4, dtype=np.float32).reshape(-1) if xf is None else np.asarray(xf, np.float32).reshape(-1))
+        lights = [orc.area_light(**l) for l in spec.get("lights", [])]
+        env = spec.get("env", {})
+        if env.get("env_map", self.INVALID) != self.INVALID:
+            raise ValueError("only the default environment map")
+        self.arrays = {
+            "tris": np.concatenate(tris) if tris else np.zeros(0, TRI_DTYPE),
+            "aabbs": np.ascontiguousarray(np.concatenate(aabbs) if aabbs else np.zeros((0, 6)), np.float32),
+            "normals": np.ascontiguousarray(np.concatenate(normals) if normals else np.zeros((0, 9)), np.float32),
+            "uvs": np.ascontiguousarray(np.concatenate(uvs) if uvs else np.zeros((0, 6)), np.float32),
+            "mat": np.ascontiguousarray(np.concatenate(mat) if mat else np.zeros((0, 2)), np.int32),
+            "mesh_tris": np.asarray(mesh_tris, np.int64),
+            "inst_mesh": np.asarray(inst_mesh, np.int32),
+            "inst_xform": np.ascontiguousarray(np.concatenate(inst_xform) if inst_xform else np.zeros(0), np.float32),
+            "mats": np.asarray(mats, np.float32),
+            "texels": np.concatenate(texels) if texels else np.zeros(1, np.uint32),
+            "tex_info": np.asarray(tex_info, np.int32),
+            "lights": np.ascontiguousarray(np.concatenate(lights) if lights else np.zeros(0), np.float32),
+        }
+        a = self.arrays
+        c = OrcPrincipledScene()
+        for k in ("tris", "aabbs", "normals", "uvs", "mat", "mesh_tris", "inst_mesh", "inst_xform", "mats", "texels", "tex_info", "lights"):
+            setattr(c, k, a[k].ctypes.data if a[k].size else None)
+        c.ntris = len(a["tris"])
+        c.nmeshes = len(mesh_tris) // 2
+        c.ninst = len(inst_mesh)
+        c.nmats = len(mats) // 8
+        c.ntex = ntex
+        c.nlights = len(lights)
+        for k, v in enumerate(env.get("env_col", (0.0, 0.0, 0.0))):
+            c.env_col[k] = float(v)
+        self.c = c
 
 
 # ----------------------------------------------------------------- reference

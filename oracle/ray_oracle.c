@@ -610,3 +610,624 @@ void orc_halton_table(int iteration, const uint16_t *perms, float *out) {
         for (int k = 0; k < 24; k++)
             out[i * 24 + k] = scrambled_radical_inverse(g_primes[k], perms + offs[k], (uint64_t)(int64_t)(iteration + i));
 }
+
+/* ------------------------------------------------ metallic-roughness material
+ * CPU restatement of the library's RAY_MAT_PRINCIPLED path (no counterpart in
+ * the reference): raydemo_b200/csrc/ggx.cuh and the RAY_MAT_PRINCIPLED branch
+ * of shade_hit / shade_surface in raydemo_b200/csrc/render_kernels.cu, written
+ * again from the same formulas in the same operation order. cos, sin, acos and
+ * pow are evaluated in double and rounded once to float, as on the GPU. */
+
+typedef struct { float x, y, z; } pv3;
+static pv3 P3(float x, float y, float z) { pv3 r = {x, y, z}; return r; }
+static pv3 padd(pv3 a, pv3 b) { return P3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static pv3 psub(pv3 a, pv3 b) { return P3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static pv3 pmul(pv3 a, pv3 b) { return P3(a.x * b.x, a.y * b.y, a.z * b.z); }
+static pv3 pscale(pv3 a, float s) { return P3(a.x * s, a.y * s, a.z * s); }
+static pv3 pdiv(pv3 a, float s) { return P3(a.x / s, a.y / s, a.z / s); }
+static float pdot(pv3 a, pv3 b) {
+    float r = 0.0f;
+    r += a.x * b.x;
+    r += a.y * b.y;
+    r += a.z * b.z;
+    return r;
+}
+static pv3 pnorm(pv3 a) { return pdiv(a, sqrtf(pdot(a, a))); }
+static pv3 pcross(pv3 a, pv3 b) { return P3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+static float fmax_s(float a, float b) { return (a < b) ? b : a; }
+static float clamp_s(float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); }
+static float cr_cosf(float x) { return (float)cos((double)x); }
+static float cr_sinf(float x) { return (float)sin((double)x); }
+static float cr_acosf(float x) { return (float)acos((double)x); }
+static float cr_powf(float x, float y) { return (float)pow((double)x, (double)y); }
+static float pow5f(float v) { return (v * v) * (v * v) * v; }
+static float simd_floorf(float v) { return (float)(int32_t)((uint32_t)f2i_x86(v) - (v < 0.0f ? 1u : 0u)); }
+
+static uint32_t brev32(uint32_t x) {
+    uint32_t r = 0;
+    for (int i = 0; i < 32; i++) r |= ((x >> i) & 1u) << (31 - i);
+    return r;
+}
+static uint32_t mix32(uint32_t x) { return (uint32_t)orc_hash((int32_t)x); }
+static uint32_t nested_scramble(uint32_t x, uint32_t seed) {
+    x = brev32(x);
+    x += seed;
+    x ^= x * 0x9E3779B8u;
+    x ^= x * 0x7F4A7C16u;
+    x ^= x * 0x94D049BAu;
+    x ^= x * 0x2C1B3C6Eu;
+    return brev32(x);
+}
+static uint32_t sobol_dim1(uint32_t i) {
+    uint32_t r = 0, v = 0x80000000u;
+    for (; i; i >>= 1, v ^= v >> 1)
+        if (i & 1u) r ^= v;
+    return r;
+}
+static void sobol2(uint32_t index, uint32_t seed, float *x, float *y) {
+    const uint32_t i = nested_scramble(index, seed);
+    const uint32_t sx = nested_scramble(brev32(i), mix32(seed ^ 0x5bd1e995u));
+    const uint32_t sy = nested_scramble(sobol_dim1(i), mix32(seed ^ 0x1b873593u));
+    *x = (float)(sx >> 8) * (1.0f / 16777216.0f);
+    *y = (float)(sy >> 8) * (1.0f / 16777216.0f);
+}
+static uint32_t dim_seed(uint32_t pixel, int bounce, int pair) {
+    return mix32(mix32(pixel * 0x2545F491u + 0x68E31DA4u) ^ (uint32_t)(bounce * 8 + pair) * 0x9E3779B1u);
+}
+
+typedef struct { pv3 t, b, n; } pframe;
+static pframe make_frame(pv3 n) {
+    const float sign = n.z >= 0.0f ? 1.0f : -1.0f;
+    const float a = -1.0f / (sign + n.z);
+    const float b = n.x * n.y * a;
+    pframe f;
+    f.t = P3(1.0f + sign * n.x * n.x * a, sign * b, -sign * n.x);
+    f.b = P3(b, sign + n.y * n.y * a, -n.y);
+    f.n = n;
+    return f;
+}
+static pv3 to_local(const pframe *f, pv3 v) { return P3(pdot(v, f->t), pdot(v, f->b), pdot(v, f->n)); }
+static pv3 to_world(const pframe *f, pv3 v) { return padd(padd(pscale(f->t, v.x), pscale(f->b, v.y)), pscale(f->n, v.z)); }
+
+typedef struct { pv3 f0, diffuse; float alpha, p_spec; } pparams;
+static pparams make_params(pv3 base, float roughness, float metallic) {
+    pparams p;
+    p.f0 = P3(0.04f + (base.x - 0.04f) * metallic, 0.04f + (base.y - 0.04f) * metallic, 0.04f + (base.z - 0.04f) * metallic);
+    p.diffuse = pscale(base, 1.0f - metallic);
+    p.alpha = fmax_s(roughness * roughness, 1.0e-4f);
+    p.p_spec = 0.5f + 0.5f * metallic;
+    return p;
+}
+static float smith_lambda(pv3 v, float a) {
+    const float t2 = (v.x * v.x + v.y * v.y) / (v.z * v.z);
+    return 0.5f * (sqrtf(1.0f + a * a * t2) - 1.0f);
+}
+static float ggx_d(pv3 h, float a) {
+    const float a2 = a * a;
+    const float k = h.z * h.z * (a2 - 1.0f) + 1.0f;
+    return a2 / (ORC_PI * k * k);
+}
+#define ORC_INV_PI 0.318309886183790671538f
+static void ggx_eval(const pparams *p, pv3 wo, pv3 wi, pv3 *f_cos, float *pdf) {
+    *f_cos = P3(0.0f, 0.0f, 0.0f);
+    *pdf = 0.0f;
+    if (wo.z <= 0.0f || wi.z <= 0.0f) return;
+    const pv3 h = pnorm(padd(wo, wi));
+    const float d = ggx_d(h, p->alpha);
+    const float lo = smith_lambda(wo, p->alpha), li = smith_lambda(wi, p->alpha);
+    const float g2 = 1.0f / (1.0f + lo + li);
+    const float g1 = 1.0f / (1.0f + lo);
+    const float c = 1.0f - fmax_s(pdot(wo, h), 0.0f);
+    const float c5 = pow5f(c);
+    const pv3 F = P3(p->f0.x + (1.0f - p->f0.x) * c5, p->f0.y + (1.0f - p->f0.y) * c5, p->f0.z + (1.0f - p->f0.z) * c5);
+    const float spec = d * g2 / (4.0f * wo.z * wi.z);
+    *f_cos = pscale(padd(pscale(F, spec), pscale(p->diffuse, ORC_INV_PI)), wi.z);
+    const float pdf_spec = g1 * d / (4.0f * wo.z);
+    const float pdf_diff = wi.z * ORC_INV_PI;
+    *pdf = p->p_spec * pdf_spec + (1.0f - p->p_spec) * pdf_diff;
+}
+static int ggx_sample(const pparams *p, pv3 wo, float u1, float u2, float ulobe, pv3 *wi) {
+    if (ulobe < p->p_spec) {
+        const float a = p->alpha;
+        const pv3 vh = pnorm(P3(a * wo.x, a * wo.y, wo.z));
+        const float lensq = vh.x * vh.x + vh.y * vh.y;
+        const pv3 t1 = lensq > 0.0f ? pdiv(P3(-vh.y, vh.x, 0.0f), sqrtf(lensq)) : P3(1.0f, 0.0f, 0.0f);
+        const pv3 t2 = pcross(vh, t1);
+        const float r = sqrtf(u1);
+        const float phi = 2.0f * ORC_PI * u2;
+        const float q1 = r * cr_cosf(phi);
+        float q2 = r * cr_sinf(phi);
+        const float s = 0.5f * (1.0f + vh.z);
+        q2 = (1.0f - s) * sqrtf(1.0f - q1 * q1) + s * q2;
+        const pv3 nh = padd(padd(pscale(t1, q1), pscale(t2, q2)), pscale(vh, sqrtf(fmax_s(0.0f, 1.0f - q1 * q1 - q2 * q2))));
+        const pv3 h = pnorm(P3(a * nh.x, a * nh.y, fmax_s(0.0f, nh.z)));
+        *wi = psub(pscale(h, 2.0f * pdot(wo, h)), wo);
+    } else {
+        const float r = sqrtf(u1);
+        const float phi = 2.0f * ORC_PI * u2;
+        *wi = P3(r * cr_cosf(phi), r * cr_sinf(phi), sqrtf(fmax_s(0.0f, 1.0f - u1)));
+    }
+    return wi->z > 0.0f;
+}
+static float power_heuristic(float a, float b) { return (a * a) / (a * a + b * b); }
+
+/* the AreaLight record (20 floats) */
+typedef struct { float p0[3]; uint32_t type; float u[3], area; float v[3], cos_max; float n[3], pad0; float L[3], pad1; } plight;
+#define ORC_LIGHT_QUAD 3u
+static int hit_quad(const plight *l, pv3 o, pv3 d, float tmax, float *t) {
+    const pv3 n = P3(l->n[0], l->n[1], l->n[2]);
+    const float dn = pdot(d, n);
+    if (!(dn < 0.0f)) return 0;
+    const pv3 p0 = P3(l->p0[0], l->p0[1], l->p0[2]);
+    *t = pdot(psub(p0, o), n) / dn;
+    if (!(*t > 0.0f && *t < tmax)) return 0;
+    const pv3 q = psub(padd(o, pscale(d, *t)), p0);
+    const pv3 u = P3(l->u[0], l->u[1], l->u[2]), v = P3(l->v[0], l->v[1], l->v[2]);
+    const float s = pdot(q, u) / pdot(u, u), r = pdot(q, v) / pdot(v, v);
+    return s >= 0.0f && s <= 1.0f && r >= 0.0f && r <= 1.0f;
+}
+
+/* InverseMatrix (src/Ray/internal/Core.cpp:909-949): the cofactor inverse of
+ * a column-major 4x4 matrix, every product and difference in the order the
+ * reference evaluates them. */
+static float mdet2(const float *m, int a, int b, int c, int d) { return m[a] * m[b] - m[c] * m[d]; }
+static void inverse4(const float m[16], float o[16]) {
+    const float A2323 = mdet2(m, 10, 15, 11, 14), A1323 = mdet2(m, 9, 15, 11, 13), A1223 = mdet2(m, 9, 14, 10, 13);
+    const float A0323 = mdet2(m, 8, 15, 11, 12), A0223 = mdet2(m, 8, 14, 10, 12), A0123 = mdet2(m, 8, 13, 9, 12);
+    const float A2313 = mdet2(m, 6, 15, 7, 14), A1313 = mdet2(m, 5, 15, 7, 13), A1213 = mdet2(m, 5, 14, 6, 13);
+    const float A2312 = mdet2(m, 6, 11, 7, 10), A1312 = mdet2(m, 5, 11, 7, 9), A1212 = mdet2(m, 5, 10, 6, 9);
+    const float A0313 = mdet2(m, 4, 15, 7, 12), A0213 = mdet2(m, 4, 14, 6, 12), A0312 = mdet2(m, 4, 11, 7, 8);
+    const float A0212 = mdet2(m, 4, 10, 6, 8), A0113 = mdet2(m, 4, 13, 5, 12), A0112 = mdet2(m, 4, 9, 5, 8);
+    /* c(a, b, c, p, q, r) = a * p - b * q + c * r */
+#define C3(a, b, c, p, q, r) (m[a] * (p) - m[b] * (q) + m[c] * (r))
+    const float det = m[0] * C3(5, 6, 7, A2323, A1323, A1223) - m[1] * C3(4, 6, 7, A2323, A0323, A0223) +
+                      m[2] * C3(4, 5, 7, A1323, A0323, A0123) - m[3] * C3(4, 5, 6, A1223, A0223, A0123);
+    const float k = 1.0f / det;
+    o[0] = k * C3(5, 6, 7, A2323, A1323, A1223);
+    o[1] = k * -C3(1, 2, 3, A2323, A1323, A1223);
+    o[2] = k * C3(1, 2, 3, A2313, A1313, A1213);
+    o[3] = k * -C3(1, 2, 3, A2312, A1312, A1212);
+    o[4] = k * -C3(4, 6, 7, A2323, A0323, A0223);
+    o[5] = k * C3(0, 2, 3, A2323, A0323, A0223);
+    o[6] = k * -C3(0, 2, 3, A2313, A0313, A0213);
+    o[7] = k * C3(0, 2, 3, A2312, A0312, A0212);
+    o[8] = k * C3(4, 5, 7, A1323, A0323, A0123);
+    o[9] = k * -C3(0, 1, 3, A1323, A0323, A0123);
+    o[10] = k * C3(0, 1, 3, A1313, A0313, A0113);
+    o[11] = k * -C3(0, 1, 3, A1312, A0312, A0112);
+    o[12] = k * -C3(4, 5, 6, A1223, A0223, A0123);
+    o[13] = k * C3(0, 1, 2, A1223, A0223, A0123);
+    o[14] = k * -C3(0, 1, 2, A1213, A0213, A0113);
+    o[15] = k * C3(0, 1, 2, A1212, A0212, A0112);
+#undef C3
+}
+
+/* TransformBoundingBox (src/Ray/internal/Core.cpp:888-907): the box of the
+ * transformed corners, per output axis from the translation plus the smaller
+ * and larger of each input axis' two products. */
+static void transform_box(const float bmin[3], const float bmax[3], const float x[16], float out[6]) {
+    for (int j = 0; j < 3; j++) {
+        float lo = x[12 + j], hi = x[12 + j];
+        for (int i = 0; i < 3; i++) {
+            const float a = x[4 * i + j] * bmin[i], b = x[4 * i + j] * bmax[i];
+            lo += a < b ? a : b;
+            hi += a < b ? b : a;
+        }
+        out[j] = lo;
+        out[3 + j] = hi;
+    }
+}
+
+/* TransformNormal (CoreRef.cpp:1625-1629) with the inverse transform */
+static pv3 xform_normal(const float *inv, pv3 n) {
+    return P3(inv[0] * n.x + inv[1] * n.y + inv[2] * n.z, inv[4] * n.x + inv[5] * n.y + inv[6] * n.z,
+              inv[8] * n.x + inv[9] * n.y + inv[10] * n.z);
+}
+
+/* ExtractPlaneNormal (src/Ray/internal/Core.cpp:216-228): the stored plane
+ * coefficients scaled by their length (the reference's own scaling) */
+static pv3 plane_normal(const orc_tri *tri) {
+    float n[3];
+    const int iw = tri->ci & 3;
+    const int iu = iw == 0 ? 1 : 0, iv = iw == 2 ? 1 : 2;
+    n[iw] = 1.0f;
+    n[iu] = tri->nu;
+    n[iv] = tri->nv;
+    float l = sqrtf(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    if (tri->ci & 8) l = -l;
+    return P3(n[0] * l, n[1] * l, n[2] * l);
+}
+
+typedef struct {
+    const orc_principled_scene *sc;
+    orc_bvh **bvh; /* per mesh */
+    float *inv;    /* 16 floats per instance */
+    float *wbox;   /* 6 floats per instance */
+} pscene;
+
+/* Closest hit over the instances in order (Traverse_MacroTree_WithStack_ClosestHit,
+ * CoreRef.cpp:1133-1222): the instance box test with the current t, the ray
+ * taken to object space by TransformRay (CoreRef.cpp:1605-1617), then the
+ * mesh's triangles; hit.prim is the global triangle index, *obj the instance. */
+static orc_hit trace_scene(const pscene *ps, pv3 po, pv3 pd, float tmax, int *obj) {
+    const orc_principled_scene *sc = ps->sc;
+    const float o[3] = {po.x, po.y, po.z}, d[3] = {pd.x, pd.y, pd.z};
+    orc_hit h = {-1, tmax, 0.0f, 0.0f};
+    *obj = -1;
+    int32_t stack[512];
+    for (int m = 0; m < sc->ninst; m++) {
+        const int mesh = sc->inst_mesh[m];
+        const int64_t first = sc->mesh_tris[2 * mesh], cnt = sc->mesh_tris[2 * mesh + 1];
+        if (cnt == 0 || !ref_bbox_test(o, d, h.t, ps->wbox + 6 * m)) continue;
+        const float *x = ps->inv + 16 * m;
+        const float lo[3] = {x[0] * o[0] + x[4] * o[1] + x[8] * o[2] + x[12], x[1] * o[0] + x[5] * o[1] + x[9] * o[2] + x[13],
+                             x[2] * o[0] + x[6] * o[1] + x[10] * o[2] + x[14]};
+        const float ld[3] = {x[0] * d[0] + x[4] * d[1] + x[8] * d[2], x[1] * d[0] + x[5] * d[1] + x[9] * d[2],
+                             x[2] * d[0] + x[6] * d[1] + x[10] * d[2]};
+        const float inv_d[3] = {1.0f / ld[0], 1.0f / ld[1], 1.0f / ld[2]};
+        const orc_bvh *b = ps->bvh[mesh];
+        const int32_t before = h.prim;
+        int sp = 0;
+        if (b->nnodes > 0 && b->nodes[0].right != 0) stack[sp++] = 0;
+        while (sp) {
+            const onode *nd = &b->nodes[stack[--sp]];
+            if (!box_hit(nd, lo, inv_d, h.t)) continue;
+            if (nd->right <= 0) {
+                for (int32_t i = 0; i < -nd->right; i++) {
+                    const int64_t p = first + b->prims[nd->left + i];
+                    intersect_tri(lo, ld, &sc->tris[p], (int32_t)p, &h);
+                }
+            } else if (sp < 510) {
+                stack[sp++] = nd->right;
+                stack[sp++] = nd->left;
+            }
+        }
+        if (h.prim != before) *obj = m;
+    }
+    return h;
+}
+
+/* ComputeVisibility (CoreRef.cpp:1813-1896) for scenes whose surfaces are
+ * all solid: blocked by any hit closer than p2. */
+static float visibility(const pscene *ps, pv3 p1, pv3 p2) {
+    pv3 dir = psub(p2, p1);
+    const float dist = sqrtf(pdot(dir, dir));
+    dir = pdiv(dir, dist);
+    if (!(dist > ORC_HIT_EPS)) return 1.0f;
+    int obj;
+    return trace_scene(ps, p1, dir, dist, &obj).prim >= 0 ? 0.0f : 1.0f;
+}
+
+static pv3 sample_plain(const orc_principled_scene *sc, int tex, float u, float v) {
+    if (tex < 0 || tex >= sc->ntex) return P3(1.0f, 1.0f, 1.0f);
+    const int32_t *ti = sc->tex_info + 4 * tex;
+    const uint32_t *px = sc->texels + ti[0];
+    const int w = ti[1], h = ti[2];
+    float fu = u - floorf(u), fv = v - floorf(v);
+    if (!(fu >= 0.0f && fu < 1.0f)) fu = 0.0f;
+    if (!(fv >= 0.0f && fv < 1.0f)) fv = 0.0f;
+    const float x = fu * (float)w - 0.5f, y = fv * (float)h - 0.5f;
+    const float x0 = floorf(x), y0 = floorf(y);
+    const float kx = x - x0, ky = y - y0;
+    const int ix = (int)x0, iy = (int)y0;
+    const int xa = (ix + w) % w, xb = (ix + 1) % w, ya = (iy + h) % h, yb = (iy + 1) % h;
+    const uint32_t p00 = px[ya * w + xa], p01 = px[ya * w + xb], p10 = px[yb * w + xa], p11 = px[yb * w + xb];
+    float c[3];
+    for (int k = 0; k < 3; k++) {
+        const float a00 = (float)((p00 >> (8 * k)) & 0xFFu), a01 = (float)((p01 >> (8 * k)) & 0xFFu);
+        const float a10 = (float)((p10 >> (8 * k)) & 0xFFu), a11 = (float)((p11 >> (8 * k)) & 0xFFu);
+        const float top = a00 * (1.0f - kx) + a01 * kx, bot = a10 * (1.0f - kx) + a11 * kx;
+        c[k] = (top * (1.0f - ky) + bot * ky) * (1.0f / 255.0f);
+    }
+    if (ti[3]) { /* srgb_to_rgb, CoreRef.cpp:377-389 */
+        for (int k = 0; k < 3; k++) c[k] = c[k] > 0.04045f ? cr_powf((c[k] + 0.055f) / 1.055f, 2.4f) : c[k] / 12.92f;
+    }
+    return P3(c[0], c[1], c[2]);
+}
+
+/* the default environment map, one white RGBE texel (exponent 128) at the
+ * atlas origin, read by SampleLatlong_RGBE (CoreRef.cpp:1772-1798) */
+static float env_white(pv3 dir) {
+    const float theta = cr_acosf(clamp_s(dir.y, -1.0f, 1.0f)) / ORC_PI;
+    const float r = sqrtf(dir.x * dir.x + dir.z * dir.z);
+    float u = 0.5f * cr_acosf(r > ORC_FLT_EPS ? clamp_s(dir.x / r, -1.0f, 1.0f) : 0.0f) / ORC_PI;
+    if (dir.z < 0.0f) u = 1.0f - u;
+    const float ux = 0.0f + u * 1.0f + 1.0f, uy = 0.0f + theta * 1.0f + 1.0f;
+    const float kx = ux - simd_floorf(ux), ky = uy - simd_floorf(uy);
+    return (1.0f * kx + 1.0f * (1 - kx)) * ky + (1.0f * kx + 1.0f * (1 - kx)) * (1 - ky);
+}
+
+typedef struct {
+    pv3 o, d, c;
+    float prev_pdf;
+    int depth;
+} ppath;
+
+#define ORC_HIT_BIAS 0.001f
+#define ORC_MAX_DIST 3.402823466e+38F
+
+/* One shading step of the GPU renderer for a path segment: returns its
+ * colour in col_out; *emit is set, with the continuation in *next, when the
+ * path goes on. */
+static void shade_principled(const pscene *ps, const ppath *ray, int pixel, int iteration, int bounce, int max_diff, int max_total,
+                             int term_start, float col_out[4], ppath *next, int *emit) {
+    const orc_principled_scene *sc = ps->sc;
+    *emit = 0;
+    int obj;
+    const orc_hit hit = trace_scene(ps, ray->o, ray->d, ORC_MAX_DIST, &obj);
+    const pv3 I = ray->d;
+    float cr = 0.0f, cg = 0.0f, cb = 0.0f, ca = 1.0f;
+    if (hit.prim < 0) {
+        const float e = env_white(I);
+        cr = ray->c.x * e * sc->env_col[0];
+        cg = ray->c.y * e * sc->env_col[1];
+        cb = ray->c.z * e * sc->env_col[2];
+    } else {
+        const orc_tri *tri = &sc->tris[hit.prim];
+        const float *inv = ps->inv + 16 * obj;
+        const float t = hit.t, hu = hit.u, hv = hit.v;
+        const pv3 P = padd(ray->o, pscale(I, t));
+        const float w = 1.0f - hu - hv;
+        const float *nn = sc->normals + 9 * (int64_t)hit.prim, *uv = sc->uvs + 6 * (int64_t)hit.prim;
+        pv3 N = padd(padd(pscale(P3(nn[0], nn[1], nn[2]), w), pscale(P3(nn[3], nn[4], nn[5]), hu)), pscale(P3(nn[6], nn[7], nn[8]), hv));
+        const float uvx = uv[0] * w + uv[2] * hu + uv[4] * hv;
+        const float uvy = uv[1] * w + uv[3] * hu + uv[5] * hv;
+        pv3 plane_N = xform_normal(inv, plane_normal(tri));
+        int mi = sc->mat[2 * (int64_t)hit.prim];
+        if (pdot(plane_N, I) > 0.0f) {
+            mi = sc->mat[2 * (int64_t)hit.prim + 1];
+            plane_N = P3(-plane_N.x, -plane_N.y, -plane_N.z);
+            N = P3(-N.x, -N.y, -N.z);
+        }
+        if (mi < 0 || mi >= sc->nmats) {
+            ca = 0.0f;
+        } else {
+            const float *m = sc->mats + 8 * mi;
+            const int diff_depth = ray->depth & 0xff;
+            const int total_depth = diff_depth;
+            const int cant_terminate = total_depth < term_start;
+            const pv3 wo = pnorm(P3(-I.x, -I.y, -I.z));
+            pv3 Ns = pnorm(xform_normal(inv, N));
+            if (!(pdot(Ns, wo) > 0.0f)) Ns = pnorm(plane_N);
+            const pframe fr = make_frame(Ns);
+            const pv3 wo_l = to_local(&fr, wo);
+            const pv3 base = pmul(sample_plain(sc, (int)m[5], uvx, uvy), P3(m[0], m[1], m[2]));
+            const pparams prm = make_params(base, m[3], m[4]);
+            const uint32_t sidx = (uint32_t)(iteration - 1);
+            const pv3 P_off = padd(P, pscale(plane_N, ORC_HIT_BIAS));
+            pv3 col = P3(0.0f, 0.0f, 0.0f);
+            if (sc->nlights > 0) { /* next-event estimation from one light picked uniformly */
+                float ul, ua, ub, uc;
+                sobol2(sidx, dim_seed((uint32_t)pixel, bounce, 2), &ul, &ua);
+                sobol2(sidx, dim_seed((uint32_t)pixel, bounce, 3), &ub, &uc);
+                const uint32_t nl = (uint32_t)sc->nlights;
+                uint32_t k = (uint32_t)(ul * (float)nl);
+                if (k >= nl) k = nl - 1;
+                const plight *L = (const plight *)(sc->lights + 20 * k);
+                const pv3 Lc = P3(L->L[0], L->L[1], L->L[2]);
+                if (L->type == ORC_LIGHT_QUAD) {
+                    const pv3 p = padd(padd(P3(L->p0[0], L->p0[1], L->p0[2]), pscale(P3(L->u[0], L->u[1], L->u[2]), ub)),
+                                       pscale(P3(L->v[0], L->v[1], L->v[2]), uc));
+                    const pv3 dv = psub(p, P_off);
+                    const float dist2 = pdot(dv, dv);
+                    const float dist = sqrtf(dist2);
+                    const pv3 wi = pdiv(dv, dist);
+                    const float cos_l = -pdot(wi, P3(L->n[0], L->n[1], L->n[2]));
+                    if (cos_l > 0.0f) {
+                        const float pdf_l = dist2 / (L->area * cos_l) / (float)nl;
+                        pv3 f_cos;
+                        float pdf_b;
+                        ggx_eval(&prm, wo_l, to_local(&fr, wi), &f_cos, &pdf_b);
+                        if (f_cos.x > 0.0f || f_cos.y > 0.0f || f_cos.z > 0.0f) {
+                            const float vis = visibility(ps, P_off, p);
+                            col = padd(col, pscale(pmul(Lc, f_cos), power_heuristic(pdf_l, pdf_b) * vis / pdf_l));
+                        }
+                    }
+                } else {
+                    const float cos_t = 1.0f - ub * (1.0f - L->cos_max);
+                    const float sin_t = sqrtf(fmax_s(0.0f, 1.0f - cos_t * cos_t));
+                    const float phi = 2.0f * ORC_PI * uc;
+                    const pframe fs = make_frame(P3(L->n[0], L->n[1], L->n[2]));
+                    const pv3 wi = to_world(&fs, P3(sin_t * cr_cosf(phi), sin_t * cr_sinf(phi), cos_t));
+                    pv3 f_cos;
+                    float pdf_b;
+                    ggx_eval(&prm, wo_l, to_local(&fr, wi), &f_cos, &pdf_b);
+                    if (f_cos.x > 0.0f || f_cos.y > 0.0f || f_cos.z > 0.0f) {
+                        const float vis = visibility(ps, P_off, padd(P_off, pscale(wi, 1.0e5f)));
+                        col = padd(col, pscale(pmul(Lc, f_cos), vis * (float)nl));
+                    }
+                }
+            }
+            if (diff_depth < max_diff && total_depth < max_total) {
+                float u1, u2, ulobe, urr;
+                sobol2(sidx, dim_seed((uint32_t)pixel, bounce, 0), &u1, &u2);
+                sobol2(sidx, dim_seed((uint32_t)pixel, bounce, 1), &ulobe, &urr);
+                pv3 wi_l;
+                if (ggx_sample(&prm, wo_l, u1, u2, ulobe, &wi_l)) {
+                    pv3 f_cos;
+                    float pdf;
+                    ggx_eval(&prm, wo_l, wi_l, &f_cos, &pdf);
+                    if (pdf > 0.0f) {
+                        const pv3 wi = to_world(&fr, wi_l);
+                        next->o = padd(P, pscale(plane_N, pdot(wi, plane_N) > 0.0f ? ORC_HIT_BIAS : -ORC_HIT_BIAS));
+                        next->d = wi;
+                        next->c = pmul(ray->c, pdiv(f_cos, pdf));
+                        next->prev_pdf = pdf;
+                        next->depth = ray->depth + 1;
+                        /* Russian roulette, CoreRef.cpp:2246-2256 */
+                        const float lum = fmax_s(next->c.x, fmax_s(next->c.y, next->c.z));
+                        const float q = cant_terminate ? 0.0f : fmax_s(0.05f, 1.0f - lum);
+                        if (urr >= q) {
+                            next->c = P3(next->c.x / (1.0f - q), next->c.y / (1.0f - q), next->c.z / (1.0f - q));
+                            *emit = 1;
+                        }
+                    }
+                }
+            }
+            cr = ray->c.x * col.x;
+            cg = ray->c.y * col.y;
+            cb = ray->c.z * col.z;
+        }
+    }
+    /* quad lights the segment passes before its hit, weighted against the
+     * light pdf of the vertex that sampled it */
+    const float tmax = hit.prim >= 0 ? hit.t : ORC_MAX_DIST;
+    for (int k = 0; k < sc->nlights; k++) {
+        const plight *L = (const plight *)(sc->lights + 20 * k);
+        float tq;
+        if (L->type != ORC_LIGHT_QUAD || !hit_quad(L, ray->o, ray->d, tmax, &tq)) continue;
+        float wgt = 1.0f;
+        if (ray->prev_pdf > 0.0f) {
+            const float cos_l = -pdot(ray->d, P3(L->n[0], L->n[1], L->n[2]));
+            const float pdf_l = tq * tq / (L->area * cos_l) / (float)sc->nlights;
+            wgt = power_heuristic(ray->prev_pdf, pdf_l);
+        }
+        cr += ray->c.x * L->L[0] * wgt;
+        cg += ray->c.y * L->L[1] * wgt;
+        cb += ray->c.z * L->L[2] * wgt;
+    }
+    col_out[0] = cr;
+    col_out[1] = cg;
+    col_out[2] = cb;
+    col_out[3] = ca;
+}
+
+typedef struct {
+    const pscene *ps;
+    const orc_camera *cam;
+    const float *halton;
+    int w, h, iteration, max_diff, max_total, term_start;
+    float *temp;
+    int row0, row1;
+} prender_work;
+
+static void *prender_worker(void *arg) {
+    prender_work *pw = (prender_work *)arg;
+    for (int y = pw->row0; y < pw->row1; y++) {
+        for (int x = 0; x < pw->w; x++) {
+            orc_ray_packet pk;
+            orc_generate_primary_rays(pw->cam, pw->iteration, x, y, 1, 1, pw->w, pw->h, pw->halton, &pk);
+            ppath ray = {P3(pk.o[0], pk.o[1], pk.o[2]), P3(pk.d[0], pk.d[1], pk.d[2]), P3(pk.c[0], pk.c[1], pk.c[2]), 0.0f, 0};
+            const int pixel = y * pw->w + x;
+            float c[4], acc[4];
+            ppath next;
+            int emit;
+            /* bounce numbering as the renderer's: 2 for camera rays, 3.. after */
+            shade_principled(pw->ps, &ray, pixel, pw->iteration, 2, pw->max_diff, pw->max_total, pw->term_start, acc, &next, &emit);
+            for (int b = 0; b < pw->max_total && emit; b++) {
+                ray = next;
+                shade_principled(pw->ps, &ray, pixel, pw->iteration, b + 3, pw->max_diff, pw->max_total, pw->term_start, c, &next, &emit);
+                acc[0] += c[0];
+                acc[1] += c[1];
+                acc[2] += c[2];
+            }
+            memcpy(pw->temp + 4 * (size_t)pixel, acc, sizeof(acc));
+        }
+    }
+    return NULL;
+}
+
+void orc_render_principled(const orc_principled_scene *sc, const orc_camera *cam, int w, int h, int spp, int max_diff_depth,
+                           int max_total_depth, int termination_start_depth, float *out, int nthreads) {
+    pscene ps;
+    ps.sc = sc;
+    ps.bvh = (orc_bvh **)calloc((size_t)(sc->nmeshes > 0 ? sc->nmeshes : 1), sizeof(orc_bvh *));
+    ps.inv = (float *)malloc(sizeof(float) * 16 * (size_t)(sc->ninst > 0 ? sc->ninst : 1));
+    ps.wbox = (float *)malloc(sizeof(float) * 6 * (size_t)(sc->ninst > 0 ? sc->ninst : 1));
+    float *mbox = (float *)malloc(sizeof(float) * 6 * (size_t)(sc->nmeshes > 0 ? sc->nmeshes : 1));
+    for (int m = 0; m < sc->nmeshes; m++) {
+        const int64_t first = sc->mesh_tris[2 * m], cnt = sc->mesh_tris[2 * m + 1];
+        ps.bvh[m] = orc_bvh_build(sc->aabbs + 6 * first, cnt);
+        /* the mesh box: the union of its triangles' boxes */
+        for (int k = 0; k < 3; k++) {
+            mbox[6 * m + k] = INFINITY;
+            mbox[6 * m + 3 + k] = -INFINITY;
+        }
+        for (int64_t i = first; i < first + cnt; i++)
+            for (int k = 0; k < 3; k++) {
+                mbox[6 * m + k] = fminf(mbox[6 * m + k], sc->aabbs[6 * i + k]);
+                mbox[6 * m + 3 + k] = fmaxf(mbox[6 * m + 3 + k], sc->aabbs[6 * i + 3 + k]);
+            }
+    }
+    for (int i = 0; i < sc->ninst; i++) {
+        inverse4(sc->inst_xform + 16 * i, ps.inv + 16 * i);
+        const float *mb = mbox + 6 * sc->inst_mesh[i];
+        transform_box(mb, mb + 3, sc->inst_xform + 16 * i, ps.wbox + 6 * i);
+    }
+    uint16_t perms[1002];
+    orc_halton_perms(perms);
+    float *table = (float *)malloc(sizeof(float) * (24 * 256 + 64));
+    float *temp = (float *)malloc(sizeof(float) * 4 * (size_t)w * h);
+    memset(out, 0, sizeof(float) * 4 * (size_t)w * h);
+    if (nthreads < 1) nthreads = 1;
+    if (max_total_depth > 10) max_total_depth = 10; /* MAX_BOUNCES, src/Ray/internal/Core.h:53 */
+    int base = -1;
+    for (int it = 1; it <= spp; it++) {
+        /* the sample table of iteration it: from 1 below 256, else from it & ~255 */
+        const int b = it < 256 ? 1 : (it & ~255);
+        if (b != base) {
+            memset(table, 0, sizeof(float) * (24 * 256 + 64));
+            orc_halton_table(b, perms, table);
+            base = b;
+        }
+        pthread_t th[64];
+        prender_work pw[64];
+        const int nt = nthreads > 64 ? 64 : nthreads;
+        for (int t = 0; t < nt; t++) {
+            pw[t] = (prender_work){&ps,
+                                   cam,
+                                   table,
+                                   w,
+                                   h,
+                                   it,
+                                   max_diff_depth,
+                                   max_total_depth,
+                                   termination_start_depth,
+                                   temp,
+                                   (int)((int64_t)h * t / nt),
+                                   (int)((int64_t)h * (t + 1) / nt)};
+            pthread_create(&th[t], NULL, prender_worker, &pw[t]);
+        }
+        for (int t = 0; t < nt; t++) pthread_join(th[t], NULL);
+        /* Framebuffer::MixWith (FramebufferRef.cpp:57-68) */
+        const float k = 1.0f / (float)it;
+        for (size_t i = 0; i < 4 * (size_t)w * h; i++) out[i] += (temp[i] - out[i]) * k;
+    }
+    free(temp);
+    free(table);
+    for (int m = 0; m < sc->nmeshes; m++) orc_bvh_free(ps.bvh[m]);
+    free(mbox);
+    free(ps.bvh);
+    free(ps.inv);
+    free(ps.wbox);
+}
+
+int orc_area_light(int type, const float position[3], const float color[3], const float direction[3], float angle,
+                   const float edge_u[3], const float edge_v[3], float out[20]) {
+    plight a;
+    memset(&a, 0, sizeof(a));
+    a.type = (uint32_t)type;
+    for (int k = 0; k < 3; k++) a.L[k] = color[k];
+    if (type == 3) {
+        const float *u = edge_u, *v = edge_v;
+        const float c[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+        const float area = sqrtf(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+        if (!(area > 0.0f)) return -1;
+        for (int k = 0; k < 3; k++) {
+            a.p0[k] = position[k];
+            a.u[k] = u[k];
+            a.v[k] = v[k];
+            a.n[k] = c[k] / area;
+        }
+        a.area = area;
+    } else if (type == 4) {
+        const float l = sqrtf(direction[0] * direction[0] + direction[1] * direction[1] + direction[2] * direction[2]);
+        if (!(l > 0.0f) || !(angle > 0.0f && angle < 180.0f)) return -1;
+        for (int k = 0; k < 3; k++) a.n[k] = -direction[k] / l;
+        a.cos_max = cosf(0.5f * angle * ORC_PI / 180.0f);
+    } else {
+        return -1;
+    }
+    memcpy(out, &a, sizeof(a));
+    return 0;
+}

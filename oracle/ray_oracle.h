@@ -91,6 +91,52 @@ void orc_halton_table(int iteration, const uint16_t *perms, float *out);
 int32_t orc_hash(int32_t x);
 float orc_construct_float(uint32_t m);
 
+/* ---- the metallic-roughness material (RAY_MAT_PRINCIPLED of the library's
+ * C ABI; no counterpart in the reference): a CPU path tracer restating the
+ * GPU renderer's frames for scenes of such materials lit by quad and sun
+ * lights and the default (white) environment map times env_col. Meshes are
+ * given in object space and placed by instances, intersected as the
+ * reference's macro traversal does (instance box test, TransformRay), so the
+ * hits are the GPU's bit for bit.
+ *   tris       ntris records (orc_preprocess_tris of each mesh's positions),
+ *              mesh after mesh
+ *   aabbs      6 floats per triangle (for the oracle BVH of each mesh)
+ *   normals    9 floats per triangle: the vertex normals
+ *   uvs        6 floats per triangle
+ *   mat        per triangle: front material index, back material index
+ *              (-1: a back face is black)
+ *   mesh_tris  2 per mesh: first triangle, triangle count
+ *   inst_mesh  per instance: its mesh; inst_xform: 16 floats, column-major
+ *   mats       8 floats per material: base rgb, roughness, metallic, texture
+ *              index (-1: white), unused x2
+ *   texels     RGBA8 of every texture, one after another
+ *   tex_info   4 ints per texture: texel offset, w, h, sRGB
+ *   lights     20 floats per light, from orc_area_light
+ * Renders `spp` iterations (1 .. spp) of the full w x h frame and returns the
+ * accumulated mean (the renderer's clean buffer) in out (w * h * 4). */
+typedef struct orc_principled_scene {
+    const orc_tri *tris;
+    const float *aabbs, *normals, *uvs;
+    const int32_t *mat;
+    const int64_t *mesh_tris;
+    const int32_t *inst_mesh;
+    const float *inst_xform;
+    const float *mats;
+    const uint32_t *texels;
+    const int32_t *tex_info;
+    const float *lights;
+    int64_t ntris;
+    int nmeshes, ninst, nmats, ntex, nlights;
+    float env_col[3];
+} orc_principled_scene;
+void orc_render_principled(const orc_principled_scene *sc, const orc_camera *cam, int w, int h, int spp, int max_diff_depth,
+                           int max_total_depth, int termination_start_depth, float *out, int nthreads);
+/* The 20-float light record of a quad (type 3: position, edge_u, edge_v,
+ * radiance) or sun (type 4: direction, full cone angle in degrees,
+ * irradiance) light. Returns 0, or -1 for an invalid light. */
+int orc_area_light(int type, const float position[3], const float color[3], const float direction[3], float angle,
+                   const float edge_u[3], const float edge_v[3], float out[20]);
+
 #ifdef __cplusplus
 }
 #endif

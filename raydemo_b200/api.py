@@ -17,8 +17,10 @@ from .capi import check, lib
 
 # eMaterialType (SceneBase.h:45-52)
 DiffuseMaterial, GlossyMaterial, RefractiveMaterial, EmissiveMaterial, MixMaterial, TransparentMaterial = range(6)
-# eLightType (SceneBase.h:108-112)
-PointLight, SpotLight, DirectionalLight = range(3)
+# eLightType (SceneBase.h:108-112), then this library's quad and sun lights
+PointLight, SpotLight, DirectionalLight, QuadLight, SunLight = range(5)
+# this library's metallic-roughness material (include/raygpu.h RAY_MAT_PRINCIPLED)
+PrincipledMaterial = 6
 # eCamType / eFilterType / eDeviceType (Types.h:33-37)
 Persp, Ortho, Geo = range(3)
 Box, Tent = range(2)
@@ -125,9 +127,9 @@ class Scene:
 
     def AddMaterial(self, type=DiffuseMaterial, main_color=(1.0, 1.0, 1.0), main_texture=0, normal_map=capi.RAY_INVALID_INDEX,
                     mix_materials=(capi.RAY_INVALID_INDEX, capi.RAY_INVALID_INDEX), roughness=0.0, strength=1.0, fresnel=1.0,
-                    int_ior=1.0, ext_ior=1.0) -> int:
+                    int_ior=1.0, ext_ior=1.0, metallic=0.0) -> int:
         d = capi.MatDesc(type, capi.f3(*main_color), main_texture, normal_map, (C.c_uint32 * 2)(*mix_materials), roughness, strength,
-                         fresnel, int_ior, ext_ior)
+                         fresnel, int_ior, ext_ior, metallic)
         out = C.c_uint32()
         check(lib().ray_scene_add_material(self._h, C.byref(d), C.byref(out)))
         return out.value
@@ -154,8 +156,9 @@ class Scene:
         check(lib().ray_scene_remove_mesh(self._h, i))
 
     def AddLight(self, type=PointLight, position=(0.0, 0.0, 0.0), radius=1.0, color=(1.0, 1.0, 1.0), direction=(0.0, -1.0, 0.0),
-                 angle=0.0) -> int:
-        d = capi.LightDesc(type, capi.f3(*position), radius, capi.f3(*color), capi.f3(*direction), angle)
+                 angle=0.0, edge_u=(0.0, 0.0, 0.0), edge_v=(0.0, 0.0, 0.0)) -> int:
+        d = capi.LightDesc(type, capi.f3(*position), radius, capi.f3(*color), capi.f3(*direction), angle, capi.f3(*edge_u),
+                           capi.f3(*edge_v))
         out = C.c_uint32()
         check(lib().ray_scene_add_light(self._h, C.byref(d), C.byref(out)))
         return out.value

@@ -24,6 +24,9 @@ RAY_ERR_UNSUPPORTED = -7
 RAY_INVALID_INDEX = 0xFFFFFFFF
 RAY_MEM_HOST = 0
 RAY_MEM_DEVICE = 1
+RAY_MAT_PRINCIPLED = 6
+RAY_LIGHT_QUAD = 3
+RAY_LIGHT_SUN = 4
 
 f3 = C.c_float * 3
 
@@ -52,7 +55,7 @@ class Stats(C.Structure):
 class MatDesc(C.Structure):
     _fields_ = [("type", C.c_int), ("main_color", f3), ("main_texture", C.c_uint32), ("normal_map", C.c_uint32),
                 ("mix_materials", C.c_uint32 * 2), ("roughness", C.c_float), ("strength", C.c_float), ("fresnel", C.c_float),
-                ("int_ior", C.c_float), ("ext_ior", C.c_float)]
+                ("int_ior", C.c_float), ("ext_ior", C.c_float), ("metallic", C.c_float)]
 
 
 class ShapeDesc(C.Structure):
@@ -71,7 +74,8 @@ class TexDesc(C.Structure):
 
 
 class LightDesc(C.Structure):
-    _fields_ = [("type", C.c_int), ("position", f3), ("radius", C.c_float), ("color", f3), ("direction", f3), ("angle", C.c_float)]
+    _fields_ = [("type", C.c_int), ("position", f3), ("radius", C.c_float), ("color", f3), ("direction", f3), ("angle", C.c_float),
+                ("edge_u", f3), ("edge_v", f3)]
 
 
 class CameraDesc(C.Structure):

@@ -367,7 +367,11 @@ int ray_scene_remove_texture(ray_scene *s, uint32_t i) {
 
 int ray_scene_add_material(ray_scene *s, const ray_mat_desc *m, uint32_t *out_index) {
     RG_CHECK(s && m && out_index, "null argument");
-    RG_CHECK(m->type >= RAY_MAT_DIFFUSE && m->type <= RAY_MAT_TRANSPARENT, "invalid material type");
+    RG_CHECK((m->type >= RAY_MAT_DIFFUSE && m->type <= RAY_MAT_TRANSPARENT) || m->type == RAY_MAT_PRINCIPLED, "invalid material type");
+    RG_CHECK(m->type != RAY_MAT_PRINCIPLED || (m->roughness >= 0.0f && m->roughness <= 1.0f && m->metallic >= 0.0f && m->metallic <= 1.0f),
+             "roughness and metallic must lie in [0, 1]");
+    RG_CHECK(m->type != RAY_MAT_PRINCIPLED || m->main_texture == RAY_INVALID_INDEX || m->main_texture < s->textures.size(),
+             "main texture out of range");
     RG_GUARD_BEGIN
     // AddMaterial, SceneRef.cpp:118-150
     MaterialRec r{};
@@ -379,6 +383,9 @@ int ray_scene_add_material(ray_scene *s, const ray_mat_desc *m, uint32_t *out_in
     r.ext_ior = m->ext_ior;
     if (m->type == RAY_MAT_DIFFUSE || m->type == RAY_MAT_GLOSSY || m->type == RAY_MAT_REFRACTIVE) {
         r.roughness_or_strength = m->roughness;
+    } else if (m->type == RAY_MAT_PRINCIPLED) {
+        r.roughness_or_strength = m->roughness;
+        r.metallic = m->metallic;
     } else if (m->type == RAY_MAT_EMISSIVE) {
         r.roughness_or_strength = m->strength;
     } else if (m->type == RAY_MAT_MIX) {
@@ -526,10 +533,40 @@ int ray_scene_remove_mesh(ray_scene *s, uint32_t i) {
 
 int ray_scene_add_light(ray_scene *s, const ray_light_desc *d, uint32_t *out_index) {
     RG_CHECK(s && d && out_index, "null argument");
-    RG_CHECK(d->type >= RAY_LIGHT_POINT && d->type <= RAY_LIGHT_DIRECTIONAL, "invalid light type");
+    RG_CHECK(d->type >= RAY_LIGHT_POINT && d->type <= RAY_LIGHT_SUN, "invalid light type");
     RG_GUARD_BEGIN
-    // AddLight, SceneRef.cpp:305-349
     const float PI = 3.141592653589793238463f;
+    if (d->type == RAY_LIGHT_QUAD || d->type == RAY_LIGHT_SUN) {
+        AreaLight a{};
+        a.type = (uint32_t)d->type;
+        for (int k = 0; k < 3; k++) a.L[k] = d->color[k];
+        if (d->type == RAY_LIGHT_QUAD) {
+            const float *u = d->edge_u, *v = d->edge_v;
+            const float c[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+            const float area = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+            const float uv = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+            const float lu = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]), lv = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            RG_CHECK(area > 0.0f && std::abs(uv) <= 1e-4f * lu * lv, "a quad light needs two non-zero perpendicular edges");
+            for (int k = 0; k < 3; k++) {
+                a.p0[k] = d->position[k];
+                a.u[k] = u[k];
+                a.v[k] = v[k];
+                a.n[k] = c[k] / area;
+            }
+            a.area = area;
+        } else {
+            const float *w = d->direction;
+            const float l = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+            RG_CHECK(l > 0.0f && d->angle > 0.0f && d->angle < 180.0f, "a sun light needs a direction and an angle in (0, 180)");
+            for (int k = 0; k < 3; k++) a.n[k] = -w[k] / l;
+            a.cos_max = std::cos(0.5f * d->angle * PI / 180.0f);
+        }
+        s->area_lights.push_back(a);
+        s->shade_dirty = true;
+        *out_index = (uint32_t)(s->lights.size() + s->area_lights.size() - 1);
+        return RAY_OK;
+    }
+    // AddLight, SceneRef.cpp:305-349
     LightRec l{};
     memcpy(l.pos, d->position, 12);
     l.radius = d->radius;
@@ -554,7 +591,7 @@ int ray_scene_add_light(ray_scene *s, const ray_light_desc *d, uint32_t *out_ind
     l.brightness = std::max(l.col[0], std::max(l.col[1], l.col[2]));
     s->lights.push_back(l);
     s->shade_dirty = true;
-    *out_index = (uint32_t)(s->lights.size() - 1);
+    *out_index = (uint32_t)(s->lights.size() + s->area_lights.size() - 1);
     return RAY_OK;
     RG_GUARD_END
 }

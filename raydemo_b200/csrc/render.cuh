@@ -9,10 +9,11 @@
 namespace rg {
 
 // material_t (src/Ray/internal/Core.h:121-131): textures[] = normal map,
-// main texture, and for mix materials the two mixed materials.
+// main texture, and for mix materials the two mixed materials. The padding
+// word holds the metallic parameter of RAY_MAT_PRINCIPLED.
 struct MaterialRec {
     uint32_t textures[4];
-    float main_color[3], pad;
+    float main_color[3], metallic;
     uint32_t type;
     float roughness_or_strength;
     float int_ior, ext_ior;
@@ -54,6 +55,20 @@ struct TexDev {
     TexLevel lv[NUM_MIP_LEVELS];
 };
 
+// A quad or sun light of RAY_MAT_PRINCIPLED's next-event estimation (80 bytes).
+// Quad: p0 + s u + t v, unit normal n = u x v / |u x v|, area, radiance L.
+// Sun: n = unit direction towards the sun, cos_max = cosine of the cone's
+// half angle, L = irradiance.
+struct AreaLight {
+    float p0[3];
+    uint32_t type; // RAY_LIGHT_QUAD or RAY_LIGHT_SUN
+    float u[3], area;
+    float v[3], cos_max;
+    float n[3], pad0;
+    float L[3], pad1;
+};
+static_assert(sizeof(AreaLight) == 80, "AreaLight must stay 80 bytes");
+
 // Everything a shading kernel reads of the scene.
 struct RenderScene {
     SceneView sv;                  // BVH, leaf triangles and instances (shadow rays)
@@ -64,7 +79,8 @@ struct RenderScene {
     const TexDev *textures;
     const uint32_t *texels;
     const LightRec *lights;
-    uint32_t n_tris, n_materials, n_textures, n_lights;
+    const AreaLight *area_lights;
+    uint32_t n_tris, n_materials, n_textures, n_lights, n_area_lights;
     float env_col[3], env_clamp;
     uint32_t env_map;
 };

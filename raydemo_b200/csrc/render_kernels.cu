@@ -2,6 +2,7 @@
 // rays traced in the kernel), and the accumulate/tone pass. One thread per
 // ray or pixel; ray counts live on the device so a frame's bounces run back
 // to back without a host round trip.
+#include "ggx.cuh"
 #include "render.cuh"
 #include "shade.cuh"
 #include "traverse.cuh"
@@ -313,9 +314,9 @@ __device__ __forceinline__ void set3(float *dst, V3 v) {
 
 // ShadeSurface, CoreRef.cpp:2055-2391. Returns the pixel contribution;
 // fills nr and sets emit when the path continues.
-__device__ F4 shade_surface(const RenderScene &sc, const PassInfo &pi, int rand_index, const float *halton, float4 hit, int obj,
-                            float4 r0, float4 r1, const RayPayload &ray, NewRay &nr, bool &emit, Stack<true> &st, uint32_t &err,
-                            uint32_t &nshadow) {
+__device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_index, const float *halton, float4 hit, int obj,
+                        float4 r0, float4 r1, const RayPayload &ray, NewRay &nr, bool &emit, Stack<true> &st, uint32_t &err,
+                        uint32_t &nshadow) {
     emit = false;
     const int prim = __float_as_int(hit.x);
     const V3 I = v3(r1.x, r1.y, r1.z);
@@ -413,6 +414,7 @@ __device__ F4 shade_surface(const RenderScene &sc, const PassInfo &pi, int rand_
         }
     }
     const MaterialRec &mat = sc.materials[mi];
+    const V3 N_vertex = N; // interpolated vertex normal (flipped on a back face), before the normal map
 
     // normal map
     V3 B = v3(v1.b) * w + v3(v2.b) * hu + v3(v3v.b) * hv;
@@ -556,6 +558,85 @@ __device__ F4 shade_surface(const RenderScene &sc, const PassInfo &pi, int rand_
             set3(nr.p.dd_dy, eta * der.dd_dy - (m * der.dndy + dmdy * plane_N));
             emit = roulette(nr, cant_terminate, frac_modf(halton[hi + 0] + rand_offset3));
         }
+    } else if (mat.type == (uint32_t)RAY_MAT_PRINCIPLED) {
+        // metallic-roughness material: next-event estimation + a sampled continuation ray
+        const V3 wo = normalize(-I);
+        V3 Ns = normalize(transform_normal(N_vertex, inv));
+        if (!(dot(Ns, wo) > 0.0f)) Ns = normalize(plane_N); // shading normal facing away: the face normal
+        const ggx::Frame fr = ggx::make_frame(Ns);
+        const V3 wo_l = ggx::to_local(fr, wo);
+        const V3 base = ggx::sample_plain(sc, mat.textures[1], uvx, uvy) * v3(mat.main_color);
+        const ggx::Params prm = ggx::make_params(base, mat.roughness_or_strength, mat.metallic);
+        const uint32_t sidx = (uint32_t)(pi.iteration - 1);
+        const V3 P_off = P + HIT_BIAS * plane_N;
+        if ((!(pi.flags & PASS_SKIP_DIRECT) || pi.bounce > 2) && sc.n_area_lights > 0) {
+            float ul, ua, ub, uc;
+            ggx::sobol2(sidx, ggx::dim_seed((uint32_t)rand_index, pi.bounce, 2), ul, ua);
+            ggx::sobol2(sidx, ggx::dim_seed((uint32_t)rand_index, pi.bounce, 3), ub, uc);
+            const uint32_t nl = sc.n_area_lights;
+            uint32_t k = (uint32_t)(ul * (float)nl);
+            if (k >= nl) k = nl - 1;
+            const AreaLight L = sc.area_lights[k];
+            if (L.type == (uint32_t)RAY_LIGHT_QUAD) {
+                const V3 p = v3(L.p0) + v3(L.u) * ub + v3(L.v) * uc;
+                const V3 dv = p - P_off;
+                const float dist2 = dot(dv, dv);
+                const float dist = sqrtf(dist2);
+                const V3 wi = dv / dist;
+                const float cos_l = -dot(wi, v3(L.n));
+                if (cos_l > 0.0f) {
+                    const float pdf_l = dist2 / (L.area * cos_l) / (float)nl;
+                    V3 f_cos;
+                    float pdf_b;
+                    ggx::eval(prm, wo_l, ggx::to_local(fr, wi), f_cos, pdf_b);
+                    if (f_cos.x > 0.0f || f_cos.y > 0.0f || f_cos.z > 0.0f) {
+                        const float vis = compute_visibility(sc, P_off, p, halton, hi, rand_hash2, st, err, nshadow);
+                        col = col + v3(L.L) * f_cos * (ggx::power_heuristic(pdf_l, pdf_b) * vis / pdf_l);
+                    }
+                }
+            } else {
+                const float cos_t = 1.0f - ub * (1.0f - L.cos_max);
+                const float sin_t = sqrtf(fmax_std(0.0f, 1.0f - cos_t * cos_t));
+                const float phi = 2.0f * PI_F * uc;
+                const ggx::Frame fs = ggx::make_frame(v3(L.n));
+                const V3 wi = ggx::to_world(fs, v3(sin_t * cr_cos(phi), sin_t * cr_sin(phi), cos_t));
+                V3 f_cos;
+                float pdf_b;
+                ggx::eval(prm, wo_l, ggx::to_local(fr, wi), f_cos, pdf_b);
+                if (f_cos.x > 0.0f || f_cos.y > 0.0f || f_cos.z > 0.0f) {
+                    const float vis = compute_visibility(sc, P_off, P_off + wi * 1.0e5f, halton, hi, rand_hash2, st, err, nshadow);
+                    col = col + v3(L.L) * f_cos * (vis * (float)nl);
+                }
+            }
+        }
+        if (diff_depth < pi.max_diff_depth && total_depth < pi.max_total_depth) {
+            float u1, u2, ulobe, urr;
+            ggx::sobol2(sidx, ggx::dim_seed((uint32_t)rand_index, pi.bounce, 0), u1, u2);
+            ggx::sobol2(sidx, ggx::dim_seed((uint32_t)rand_index, pi.bounce, 1), ulobe, urr);
+            V3 wi_l;
+            if (ggx::sample(prm, wo_l, u1, u2, ulobe, wi_l)) {
+                V3 f_cos;
+                float pdf;
+                ggx::eval(prm, wo_l, wi_l, f_cos, pdf);
+                if (pdf > 0.0f) {
+                    const V3 wi = ggx::to_world(fr, wi_l);
+                    const V3 o = P + (dot(wi, plane_N) > 0.0f ? HIT_BIAS : -HIT_BIAS) * plane_N;
+                    nr.p.ray_depth = ray.ray_depth + 0x00000001;
+                    nr.r0 = make_float4(o.x, o.y, o.z, MAX_DIST);
+                    nr.r1.x = wi.x; nr.r1.y = wi.y; nr.r1.z = wi.z;
+                    const V3 wgt = f_cos / pdf;
+                    nr.p.c[0] = ray.c[0] * wgt.x;
+                    nr.p.c[1] = ray.c[1] * wgt.y;
+                    nr.p.c[2] = ray.c[2] * wgt.z;
+                    set3(nr.p.do_dx, der.do_dx);
+                    set3(nr.p.do_dy, der.do_dy);
+                    set3(nr.p.dd_dx, der.dd_dx - 2 * (dot_I_pN * der.dndx + der.ddn_dx * plane_N));
+                    set3(nr.p.dd_dy, der.dd_dy - 2 * (dot_I_pN * der.dndy + der.ddn_dy * plane_N));
+                    nr.p.pad[0] = __float_as_uint(pdf); // for the MIS weight where this ray meets a quad light
+                    emit = roulette(nr, cant_terminate, urr);
+                }
+            }
+        }
     } else if (mat.type == (uint32_t)RAY_MAT_EMISSIVE) {
         col = mat.roughness_or_strength * alb;
     } else if (mat.type == (uint32_t)RAY_MAT_TRANSPARENT) {
@@ -575,6 +656,35 @@ __device__ F4 shade_surface(const RenderScene &sc, const PassInfo &pi, int rand_
         }
     }
     return F4{ray.c[0] * col.x, ray.c[1] * col.y, ray.c[2] * col.z, 1.0f};
+}
+
+// shade_hit plus the emission of the quad lights the ray passes on its way to
+// the hit: weight 1 for rays whose last vertex did not sample quad lights
+// (pdf 0 in the payload), else the power heuristic against the light pdf that
+// next-event estimation at that vertex used.
+__device__ __forceinline__ F4 shade_surface(const RenderScene &sc, const PassInfo &pi, int rand_index, const float *halton, float4 hit,
+                                            int obj, float4 r0, float4 r1, const RayPayload &ray, NewRay &nr, bool &emit, Stack<true> &st,
+                                            uint32_t &err, uint32_t &nshadow) {
+    F4 c = shade_hit(sc, pi, rand_index, halton, hit, obj, r0, r1, ray, nr, emit, st, err, nshadow);
+    if (sc.n_area_lights == 0) return c;
+    const V3 o = v3(r0.x, r0.y, r0.z), d = v3(r1.x, r1.y, r1.z);
+    const float tmax = __float_as_int(hit.x) >= 0 ? hit.y : MAX_DIST;
+    const float prev_pdf = __uint_as_float(ray.pad[0]);
+    for (uint32_t k = 0; k < sc.n_area_lights; k++) {
+        const AreaLight &L = sc.area_lights[k];
+        float tq;
+        if (L.type != (uint32_t)RAY_LIGHT_QUAD || !ggx::hit_quad(L, o, d, tmax, tq)) continue;
+        float w = 1.0f;
+        if (prev_pdf > 0.0f) { // a unit direction sampled by RAY_MAT_PRINCIPLED
+            const float cos_l = -dot(d, v3(L.n));
+            const float pdf_l = tq * tq / (L.area * cos_l) / (float)sc.n_area_lights;
+            w = ggx::power_heuristic(prev_pdf, pdf_l);
+        }
+        c.x += ray.c[0] * L.L[0] * w;
+        c.y += ray.c[1] * L.L[1] * w;
+        c.z += ray.c[2] * L.L[2] * w;
+    }
+    return c;
 }
 
 // Framebuffer::MixWith, ComputeSHData, MixWith_SH (FramebufferRef.cpp:57-101)

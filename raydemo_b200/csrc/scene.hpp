@@ -85,6 +85,7 @@ struct ray_scene {
     std::vector<rg::TextureRec> textures;
     std::vector<std::vector<rg::SplitNode>> atlas_pages;
     std::vector<rg::LightRec> lights;
+    std::vector<rg::AreaLight> area_lights; // RAY_LIGHT_QUAD / RAY_LIGHT_SUN
     std::vector<rg::CameraRec> cameras;
     uint32_t cam_first_free = RAY_INVALID_INDEX, current_cam = RAY_INVALID_INDEX;
     ray_environment_desc env{};
@@ -100,7 +101,7 @@ struct ray_scene {
     // device arrays assembled at commit
     rg::DeviceBuf d_nodes, d_leaf, d_inst, d_tris_ref;
     uint32_t n_inst_dev = 0;
-    rg::DeviceBuf d_vertices, d_vtx_indices, d_materials, d_textures, d_texels, d_lights;
+    rg::DeviceBuf d_vertices, d_vtx_indices, d_materials, d_textures, d_texels, d_lights, d_area_lights;
 
     // batch-trace staging and diagnostics
     rg::DeviceBuf d_rays, d_hits, d_obj, d_err, d_counters, d_next_ray;

@@ -284,6 +284,10 @@ int upload_shading(ray_scene *s) {
     RG_CUDA_TRY(s->d_lights.ensure(std::max<size_t>(s->lights.size(), 1) * sizeof(LightRec)));
     if (!s->lights.empty())
         RG_CUDA_TRY(cudaMemcpyAsync(s->d_lights.p, s->lights.data(), s->lights.size() * sizeof(LightRec), cudaMemcpyHostToDevice, st));
+    RG_CUDA_TRY(s->d_area_lights.ensure(std::max<size_t>(s->area_lights.size(), 1) * sizeof(AreaLight)));
+    if (!s->area_lights.empty())
+        RG_CUDA_TRY(cudaMemcpyAsync(s->d_area_lights.p, s->area_lights.data(), s->area_lights.size() * sizeof(AreaLight),
+                                    cudaMemcpyHostToDevice, st));
     // textures: one bordered block per stored level (TextureAtlasTiled::Allocate,
     // TextureAtlasRef.cpp:138-163: top border = last row, bottom border = first
     // row, left column = last column, right column = first column, corners wrapped)
@@ -347,6 +351,8 @@ RenderScene render_scene_view(const ray_scene *s) {
     r.textures = static_cast<const TexDev *>(s->d_textures.p);
     r.texels = static_cast<const uint32_t *>(s->d_texels.p);
     r.lights = static_cast<const LightRec *>(s->d_lights.p);
+    r.area_lights = static_cast<const AreaLight *>(s->d_area_lights.p);
+    r.n_area_lights = (uint32_t)s->area_lights.size();
     r.n_tris = s->total_tris;
     r.n_materials = (uint32_t)s->materials.size();
     r.n_textures = (uint32_t)s->textures.size();

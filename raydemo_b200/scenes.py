@@ -331,3 +331,93 @@ def batch_scene(seed: int, max_bounces: int = 6) -> dict:
                       "max_glossy_depth": max_bounces, "termination_start_depth": 3}
     spec["tris"] = 2 + count * per
     return spec
+
+
+# ------------------------------------------------ metallic-roughness atrium
+
+def _wall(corners, n, uv_scale):
+    """A quad with normal n (winding fixed to agree with it) and UVs tiled uv_scale times."""
+    p = [np.asarray(c, np.float64) for c in corners]
+    if np.dot(np.cross(p[1] - p[0], p[2] - p[0]), n) < 0:
+        p = p[::-1]
+    a, i = _quad(*p, n)
+    a[:, 6:8] *= np.asarray(uv_scale, np.float32)
+    return a, i
+
+
+def noise_texture(res: int, seed: int) -> np.ndarray:
+    """res x res RGBA8 albedo from two octaves of value noise (tileable only
+    in the sense that sampling wraps)."""
+    y, x = np.meshgrid(np.arange(res), np.arange(res), indexing="ij")
+    p = np.stack([x.reshape(-1) / res, y.reshape(-1) / res, np.zeros(res * res)], 1)
+    n = 0.65 * value_noise(p * 12.0, seed) + 0.35 * value_noise(p * 48.0 + 7.0, seed + 1)
+    rgb = np.stack([0.55 + 0.30 * n, 0.50 + 0.25 * n, 0.42 + 0.20 * n], 1)
+    img = np.empty((res * res, 4), np.uint8)
+    img[:, :3] = np.clip(np.round(rgb * 255.0), 0, 255).astype(np.uint8)
+    img[:, 3] = 255
+    return img.reshape(res, res, 4)
+
+
+def atrium(seed: int = 0, w: int = 1280, h: int = 720, max_bounces: int = 8, level: int = 5, n_spheres: int = 16,
+           tex_res: int = 1024, room=(20.0, 4.0, 60.0)) -> dict:
+    """The metallic-roughness render configuration: a closed box room of
+    room[0] x room[1] x room[2] (12 triangles, seen from inside) and
+    n_spheres displaced icospheres of 20 * 4^level triangles each (value-noise
+    displacement of amplitude 0.05), each its own mesh placed by one instance
+    with a random TRS (scale U[0.5, 2], rotation about y). Every material is
+    RAY_MAT_PRINCIPLED with roughness U[0.05, 1], metallic Bernoulli(0.3) and
+    its albedo from one tex_res^2 RGBA8 value-noise texture (tinted per
+    material). Lights: a sun of irradiance 5 (outside the closed room, so its
+    shadow rays are all blocked) and 4 quad lights under the ceiling. All
+    surfaces are two-sided."""
+    rng = np.random.default_rng(2000 + seed)
+    X, Y, Z = (float(v) for v in room)
+    spec = {"textures": [(noise_texture(tex_res, seed), True, False)], "materials": [], "meshes": [], "instances": [], "lights": [],
+            "env": {"env_col": (0.0, 0.0, 0.0)}}
+    mats = spec["materials"]
+
+    def material(tint):
+        mats.append({"type": 6, "main_color": tuple(float(c) for c in tint), "main_texture": 2, "roughness": float(rng.uniform(0.05, 1.0)),
+                     "metallic": float(rng.uniform() < 0.3)})
+        return len(mats) - 1
+
+    # the room: floor, ceiling and four walls, normals pointing inwards
+    m_room = material((1.0, 1.0, 1.0))
+    hx, hz = X / 2.0, Z / 2.0
+    walls = [
+        ([(-hx, 0, -hz), (hx, 0, -hz), (hx, 0, hz), (-hx, 0, hz)], (0, 1, 0), (X / 4, Z / 4)),
+        ([(-hx, Y, -hz), (-hx, Y, hz), (hx, Y, hz), (hx, Y, -hz)], (0, -1, 0), (X / 4, Z / 4)),
+        ([(-hx, 0, -hz), (-hx, 0, hz), (-hx, Y, hz), (-hx, Y, -hz)], (1, 0, 0), (Z / 4, Y / 4)),
+        ([(hx, 0, -hz), (hx, Y, -hz), (hx, Y, hz), (hx, 0, hz)], (-1, 0, 0), (Z / 4, Y / 4)),
+        ([(-hx, 0, -hz), (-hx, Y, -hz), (hx, Y, -hz), (hx, 0, -hz)], (0, 0, 1), (X / 4, Y / 4)),
+        ([(-hx, 0, hz), (hx, 0, hz), (hx, Y, hz), (-hx, Y, hz)], (0, 0, -1), (X / 4, Y / 4)),
+    ]
+    parts = [(*_wall(c, np.asarray(n, np.float64), s), m_room) for c, n, s in walls]
+    a, i, shapes = _concat(parts)
+    spec["meshes"].append((a, i, shapes, 0))
+    spec["instances"].append((0, np.eye(4, dtype=np.float32).reshape(-1)))
+    for k in range(n_spheres):
+        m = material(rng.uniform(0.5, 1.0, 3))
+        a, i = displaced_sphere(level, seed * 101 + k, amplitude=0.05)
+        spec["meshes"].append((a, i, [(m, m, 0, len(i))], 0))
+        s = rng.uniform(0.5, 2.0)
+        ang = rng.uniform(0, 2 * np.pi)
+        c, si = np.cos(ang), np.sin(ang)
+        xf = np.eye(4, dtype=np.float32)
+        xf[0, 0], xf[0, 2], xf[2, 0], xf[2, 2] = c * s, -si * s, si * s, c * s
+        xf[1, 1] = s
+        xf[3, 0:3] = (rng.uniform(-hx + 1.5, hx - 1.5), min(s, Y / 2), rng.uniform(-hz + 3.0, hz - 3.0))
+        spec["instances"].append((k + 1, xf.reshape(-1)))
+    sun = np.array([0.35, -1.0, 0.25])
+    spec["lights"].append({"type": 4, "color": (5.0, 5.0, 5.0), "direction": tuple(float(v) for v in sun / np.linalg.norm(sun)),
+                           "angle": 0.53})
+    for k in range(4):
+        z = -hz + Z * (k + 0.5) / 4.0
+        spec["lights"].append({"type": 3, "position": (-1.5, Y - 0.01, z - 1.5), "color": (30.0, 28.5, 26.0), "edge_u": (3.0, 0.0, 0.0),
+                               "edge_v": (0.0, 0.0, 3.0)})
+    spec["camera"] = {"type": 0, "filter": 1, "dtype": 0, "origin": (0.0, Y * 0.5, -hz + 1.0), "fwd": (0.0, -0.04, 1.0),
+                      "up": (0.0, 1.0, 0.0), "fov": 60.0, "gamma": 1.0, "max_total_depth": max_bounces, "max_diff_depth": max_bounces,
+                      "max_glossy_depth": max_bounces, "termination_start_depth": 3}
+    spec["size"] = (w, h)
+    spec["tris"] = 12 + n_spheres * 20 * 4 ** level
+    return spec
