@@ -141,6 +141,26 @@ def cpu_reference(tris, rays, sample: int, steps: int, warmup: int):
 RENDER_WORKLOAD = "Cornell box (seed 0): 1,316 tris, 256x256, 1 sample per frame, 4 bounces, ray sorting off"
 
 
+def build_scene(api, r, spec: dict):
+    """A scene spec (raydemo_b200.scenes) through the public API, committed."""
+    sc = r.CreateScene()
+    if "env" in spec:
+        sc.SetEnvironment(**spec["env"])
+    for rgba, srgb, mips in spec.get("textures", []):
+        sc.AddTexture(rgba, is_srgb=srgb, generate_mipmaps=mips)
+    for m in spec.get("materials", []):
+        sc.AddMaterial(**m)
+    for attrs, idx, shapes, layout in spec.get("meshes", []):
+        sc.AddMesh(attrs, idx, shapes, layout=layout)
+    for mesh, xf in spec.get("instances", []):
+        sc.AddMeshInstance(mesh, xf)
+    for l in spec.get("lights", []):
+        sc.AddLight(**l)
+    sc.set_current_cam(sc.AddCamera(api.CameraDesc(**spec["camera"])))
+    sc.Commit()
+    return sc
+
+
 def render_frames(args, dev, stream, rank: int, world: int) -> dict:
     """The render loop on the small render configuration: frames of the
     Cornell box through RenderScene, timed with CUDA events on the renderer's
@@ -155,18 +175,7 @@ def render_frames(args, dev, stream, rank: int, world: int) -> dict:
     w, h = spec["size"]
     r = api.Renderer(w, h, device=dev.index)
     r.set_stream(stream.cuda_stream)
-    sc = r.CreateScene()
-    sc.SetEnvironment(**spec["env"])
-    for rgba, srgb, mips in spec["textures"]:
-        sc.AddTexture(rgba, is_srgb=srgb, generate_mipmaps=mips)
-    for m in spec["materials"]:
-        sc.AddMaterial(**m)
-    for attrs, idx, shapes, layout in spec["meshes"]:
-        sc.AddMesh(attrs, idx, shapes, layout=layout)
-    for mesh, xf in spec["instances"]:
-        sc.AddMeshInstance(mesh, xf)
-    sc.set_current_cam(sc.AddCamera(api.CameraDesc(**spec["camera"])))
-    sc.Commit()
+    sc = build_scene(api, r, spec)
     # first frame: the image compared with the reference
     r.Clear()
     reg = api.RegionContext()
@@ -264,20 +273,7 @@ def batch_frames(args, dev, stream, n_scenes: int = 64, samples: int = 4) -> dic
         w, h = sp["size"]
         r = api.Renderer(w, h, device=dev.index)
         r.set_stream(stream.cuda_stream)
-        sc = r.CreateScene()
-        sc.SetEnvironment(**sp["env"])
-        for rgba, srgb, mips in sp["textures"]:
-            sc.AddTexture(rgba, is_srgb=srgb, generate_mipmaps=mips)
-        for m in sp["materials"]:
-            sc.AddMaterial(**m)
-        for attrs, idx, shapes, layout in sp["meshes"]:
-            sc.AddMesh(attrs, idx, shapes, layout=layout)
-        for mesh, xf in sp["instances"]:
-            sc.AddMeshInstance(mesh, xf)
-        for l in sp["lights"]:
-            sc.AddLight(**l)
-        sc.set_current_cam(sc.AddCamera(api.CameraDesc(**sp["camera"])))
-        sc.Commit()
+        sc = build_scene(api, r, sp)
         rs.append(r)
         scs.append(sc)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -329,7 +325,7 @@ def batch_frames(args, dev, stream, n_scenes: int = 64, samples: int = 4) -> dic
         return ev0.elapsed_time(ev1)
 
     by_kernel = {"wavefront": round(timed_batch(1, 1), 3), "path": round(timed_batch(2, 1), 3)}
-    batch_ms = timed_batch(0, 4)  # the default: the faster of the two, timed on the first calls
+    batch_ms = timed_batch(0, 7)  # the default: kernel and sort chosen by timing the first calls (2 per variant)
     info = rs[0].frame_info()
     if info.error_flags:
         raise RuntimeError(f"batch reported error flags {info.error_flags}")
@@ -346,6 +342,118 @@ def batch_frames(args, dev, stream, n_scenes: int = 64, samples: int = 4) -> dic
             "plain_kernels": {"wavefront": kernels.count(1), "path": kernels.count(2)},
             "batch_kernel": {1: "wavefront", 2: "path"}.get(info.kernel, "?"), "batch_ms_by_kernel": by_kernel,
             "images_identical_to_plain": f"{identical}/{n_scenes}", "max_rmse_vs_plain": worst}
+
+
+ATRIUM_WORKLOAD = ("metallic-roughness atrium (seed 0): 20x4x60 room (12 tris) + 16 displaced icospheres of subdivision 5 "
+                   "(327,680 tris), GGX roughness U[0.05,1], metallic Bernoulli(0.3), 1024^2 value-noise albedo, sun 5 + 4 quad "
+                   "lights; 1280x720, 16 samples per frame, max 8 bounces")
+
+
+def atrium_frames(args, dev, stream, rank: int, world: int) -> dict:
+    """The metallic-roughness configuration: 16-sample frames of the atrium
+    through RenderScene (16 calls), timed with CUDA events per variant (the
+    wavefront without ray sorting, sorting before every bounce, the mask the
+    timing chooses; the path kernel) and with the renderer's own choice; the
+    image compared with the oracle's CPU restatement on the same sample
+    sequence, whose time is the CPU baseline."""
+    import torch
+    import torch.distributed as dist
+
+    from raydemo_b200 import api, scenes
+
+    spp = 16
+    spec = scenes.atrium(0)
+    w, h = spec["size"]
+    r = api.Renderer(w, h, device=dev.index)
+    r.set_stream(stream.cuda_stream)
+    sc = build_scene(api, r, spec)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def frame(reg):
+        for _ in range(spp):
+            r.RenderScene(sc, reg)
+
+    # the 16-sample image (wavefront, no sorting) and its ray counts
+    r.set_kernel(1)
+    r.set_ray_sort(0)
+    r.Clear()
+    reg = api.RegionContext()
+    rays = shadow = 0
+    for _ in range(spp):
+        r.RenderScene(sc, reg)
+        info = r.frame_info()
+        if info.error_flags:
+            raise RuntimeError(f"render reported error flags {info.error_flags}")
+        rays += info.rays
+        shadow += info.shadow_rays
+    image = r.get_pixels_ref()
+    frames = max(2, min(args.steps // 10, 5))
+
+    def timed(kernel: int, sort: int) -> float:
+        r.set_kernel(kernel)
+        r.set_ray_sort(sort)
+        g = api.RegionContext()
+        for _ in range(max(1, args.warmup // 3)):  # 16 RenderScene calls each: covers the timing of the choice
+            frame(g)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        ev0.record(stream)
+        for _ in range(frames):
+            frame(g)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        t = torch.tensor([ev0.elapsed_time(ev1) / frames], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    variants = {"wavefront_sort_off": timed(1, 0), "wavefront_sort_all": timed(1, 0x3FF), "wavefront_sort_auto": timed(1, -1)}
+    auto_mask = r.frame_info().sort_mask
+    variants["path"] = timed(2, 0)
+    r.ResetStats()
+    ms_frame = timed(0, -1)
+    chosen = r.frame_info()
+    stats = r.GetStats()
+    # end to end: the 16 RenderScene calls and the pixels read back to the host
+    g = api.RegionContext()
+    ev0.record(stream)
+    frame(g)
+    img_h = r.get_pixels_ref()
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_e2e = ev0.elapsed_time(ev1)
+    all_rays = rays + shadow
+    out = {"workload": ATRIUM_WORKLOAD, "tris": int(spec["tris"]), "samples_per_frame": spp, "ms_per_frame": round(ms_frame, 3),
+           "frames": frames, "mrays_per_s": round(world * all_rays / (ms_frame * 1e-3) / 1e6, 1), "rays_per_frame": int(all_rays),
+           "closest_hit_rays_per_frame": int(rays), "shadow_rays_per_frame": int(shadow),
+           "ms_per_frame_by_variant": {k: round(v, 3) for k, v in variants.items()},
+           "auto_sort_mask": f"0x{auto_mask:03x}", "chosen": {"kernel": {1: "wavefront", 2: "path"}.get(chosen.kernel, "?"),
+                                                              "sort_mask": f"0x{chosen.sort_mask:03x}"},
+           "e2e_ms_per_frame": round(ms_e2e, 3), "e2e_d2h_bytes_per_frame": w * h * 16, "data": "synthetic (seeded procedural scene)",
+           "stats_us": {k: int(v) for k, v in stats.items()}}
+    del img_h
+    if rank == 0 and world == 1 and args.atrium_oracle_spp > 0:
+        from oracle.oracle import Oracle
+
+        threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+        n = min(spp, args.atrium_oracle_spp)
+        orc = Oracle()
+        ps = orc.principled_scene(spec)
+        t0 = time.perf_counter()
+        ref = orc.render_principled(spec, n, nthreads=threads, scene=ps)
+        cpu_s = time.perf_counter() - t0
+        if n == spp:
+            d = ref[..., :3].astype(np.float64) - image[..., :3]
+            out["rmse_vs_oracle"] = float(np.sqrt(np.mean(d ** 2)))
+            out["identical_px_vs_oracle"] = float(np.mean(np.all(ref == image, axis=-1)))
+            out["max_abs_vs_oracle"] = float(np.max(np.abs(d)))
+        out["cpu_baseline"] = {"ms_per_frame": round(cpu_s * 1e3 * spp / n, 1), "mrays_per_s": round(all_rays * n / spp / cpu_s / 1e6, 2),
+                               "cores": threads, "kind": "port",
+                               "sample": f"{n} of the frame's {spp} samples by the oracle's CPU restatement (single-ray BVH "
+                                         f"traversal, {threads} threads); rays counted by the GPU renderer on the same paths"}
+    r.set_stream(0)
+    return out
 
 
 def run_reference_arm(args) -> None:
@@ -383,14 +491,16 @@ def run_gpu_arm(args) -> None:
     from raydemo_b200.api import Renderer
     from raydemo_b200 import scenes
 
-    if args.render_only or args.batch_only:  # one part alone (for profiling)
+    if args.render_only or args.batch_only or args.atrium_only:  # one part alone (for profiling)
         stream = torch.cuda.Stream(dev)
         torch.cuda.set_stream(stream)
         args.no_cpu_baseline = True
         if args.render_only:
             out = {"render": render_frames(args, dev, stream, rank, world)}
-        else:
+        elif args.batch_only:
             out = {"batch": batch_frames(args, dev, stream, n_scenes=args.batch_scenes)}
+        else:
+            out = {"atrium": atrium_frames(args, dev, stream, rank, world)}
         if rank == 0:
             print(json.dumps(out), flush=True)
         if world > 1:
@@ -502,6 +612,7 @@ def run_gpu_arm(args) -> None:
 
     render = None if args.no_render else render_frames(args, dev, stream, rank, world)
     batch = None if args.no_batch else batch_frames(args, dev, stream)
+    atrium = None if args.no_atrium else atrium_frames(args, dev, stream, rank, world)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -512,7 +623,8 @@ def run_gpu_arm(args) -> None:
                            "bvh_nodes": info.nodes, "bvh_depth": info.depth, "parallelism": f"replicas x{world}"},
                 "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": N_RAYS * 32, "d2h_bytes_per_step": N_RAYS * 16,
                         "matches_device_path": bool(ok)},
-                "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "render": render, "batch": batch}
+                "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "render": render, "batch": batch,
+                "atrium": atrium}
         print(json.dumps(line), flush=True)
     del sc, r
     if world > 1:
@@ -533,6 +645,10 @@ def main() -> None:
     ap.add_argument("--batch-only", action="store_true", help="only the batched-form measurement")
     ap.add_argument("--batch-no-plain", action="store_true", help="with --batch-only: two wavefront batches, nothing timed (profiling)")
     ap.add_argument("--batch-scenes", type=int, default=64, help="with --batch-only: the first N scenes of the batch")
+    ap.add_argument("--no-atrium", action="store_true", help="skip the metallic-roughness atrium frames")
+    ap.add_argument("--atrium-only", action="store_true", help="only the atrium frames")
+    ap.add_argument("--atrium-oracle-spp", type=int, default=16,
+                    help="samples the oracle renders for the atrium's image check and CPU time (16: the whole frame; 0: none)")
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes per launch of the traversal kernel from an ncu capture (reported as roofline.traffic)")
     args = ap.parse_args()

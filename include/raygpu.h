@@ -309,8 +309,22 @@ typedef struct ray_frame_info {
     uint32_t error_flags;
     int32_t kernel; /* the kernel that rendered it: 1 wavefront, 2 path kernel */
     uint64_t rays, shadow_rays;
+    uint32_t sort_mask; /* wavefront: bounces whose rays were sorted first (bit b: secondary bounce b) */
+    uint32_t reserved;
 } ray_frame_info;
 int ray_renderer_frame_info(ray_renderer *r, ray_frame_info *out);
+
+/* Ray sorting in the wavefront (the reference's Ref renderer sorts the
+ * continuation rays before every bounce by get_ray_hash, RendererRef.cpp:
+ * 200-203; the image does not depend on it). policy: RAY_SORT_AUTO (the
+ * default) sorts per bounce where timing the configuration's first frames
+ * showed it faster (chosen together with the kernel), 0 never, else a mask of
+ * the bounces to sort before (bit b: secondary bounce b; RAY_SORT_ALL every
+ * bounce). The sort is stable on the key (job, hash): rays of one scene of a
+ * batch stay together. */
+#define RAY_SORT_AUTO (-1)
+#define RAY_SORT_ALL 0x3FF
+int ray_renderer_set_ray_sort(ray_renderer *r, int policy);
 
 /* Kernel choice for ray_render (no counterpart in the reference, whose CPU
  * renderers have one loop): 1 = wavefront (a launch per bounce for ray

@@ -948,11 +948,13 @@ typedef struct {
 
 /* One shading step of the GPU renderer for a path segment: returns its
  * colour in col_out; *emit is set, with the continuation in *next, when the
- * path goes on. */
+ * path goes on. The vertex's light sample comes back apart (nee, *nee_valid):
+ * the pixel adds it after col_out when its shadow ray is unblocked. */
 static void shade_principled(const pscene *ps, const ppath *ray, int pixel, int iteration, int bounce, int max_diff, int max_total,
-                             int term_start, float col_out[4], ppath *next, int *emit) {
+                             int term_start, float col_out[4], ppath *next, int *emit, float nee[3], int *nee_valid) {
     const orc_principled_scene *sc = ps->sc;
     *emit = 0;
+    *nee_valid = 0;
     int obj;
     const orc_hit hit = trace_scene(ps, ray->o, ray->d, ORC_MAX_DIST, &obj);
     const pv3 I = ray->d;
@@ -1019,8 +1021,13 @@ static void shade_principled(const pscene *ps, const ppath *ray, int pixel, int 
                         float pdf_b;
                         ggx_eval(&prm, wo_l, to_local(&fr, wi), &f_cos, &pdf_b);
                         if (f_cos.x > 0.0f || f_cos.y > 0.0f || f_cos.z > 0.0f) {
-                            const float vis = visibility(ps, P_off, p);
-                            col = padd(col, pscale(pmul(Lc, f_cos), power_heuristic(pdf_l, pdf_b) * vis / pdf_l));
+                            const pv3 e = pscale(pmul(Lc, f_cos), power_heuristic(pdf_l, pdf_b) / pdf_l);
+                            if (visibility(ps, P_off, p) > 0.0f) {
+                                nee[0] = ray->c.x * e.x;
+                                nee[1] = ray->c.y * e.y;
+                                nee[2] = ray->c.z * e.z;
+                                *nee_valid = 1;
+                            }
                         }
                     }
                 } else {
@@ -1033,8 +1040,13 @@ static void shade_principled(const pscene *ps, const ppath *ray, int pixel, int 
                     float pdf_b;
                     ggx_eval(&prm, wo_l, to_local(&fr, wi), &f_cos, &pdf_b);
                     if (f_cos.x > 0.0f || f_cos.y > 0.0f || f_cos.z > 0.0f) {
-                        const float vis = visibility(ps, P_off, padd(P_off, pscale(wi, 1.0e5f)));
-                        col = padd(col, pscale(pmul(Lc, f_cos), vis * (float)nl));
+                        const pv3 e = pscale(pmul(Lc, f_cos), (float)nl);
+                        if (visibility(ps, P_off, padd(P_off, pscale(wi, 1.0e5f))) > 0.0f) {
+                            nee[0] = ray->c.x * e.x;
+                            nee[1] = ray->c.y * e.y;
+                            nee[2] = ray->c.z * e.z;
+                            *nee_valid = 1;
+                        }
                     }
                 }
             }
@@ -1109,17 +1121,24 @@ static void *prender_worker(void *arg) {
             orc_generate_primary_rays(pw->cam, pw->iteration, x, y, 1, 1, pw->w, pw->h, pw->halton, &pk);
             ppath ray = {P3(pk.o[0], pk.o[1], pk.o[2]), P3(pk.d[0], pk.d[1], pk.d[2]), P3(pk.c[0], pk.c[1], pk.c[2]), 0.0f, 0};
             const int pixel = y * pw->w + x;
-            float c[4], acc[4];
+            float c[4], acc[4], nee[3];
             ppath next;
-            int emit;
-            /* bounce numbering as the renderer's: 2 for camera rays, 3.. after */
-            shade_principled(pw->ps, &ray, pixel, pw->iteration, 2, pw->max_diff, pw->max_total, pw->term_start, acc, &next, &emit);
+            int emit, nee_valid;
+            /* bounce numbering as the renderer's: 2 for camera rays, 3.. after;
+             * each vertex adds its colour, then its unblocked light sample */
+            shade_principled(pw->ps, &ray, pixel, pw->iteration, 2, pw->max_diff, pw->max_total, pw->term_start, acc, &next, &emit, nee,
+                             &nee_valid);
+            if (nee_valid)
+                for (int k = 0; k < 3; k++) acc[k] += nee[k];
             for (int b = 0; b < pw->max_total && emit; b++) {
                 ray = next;
-                shade_principled(pw->ps, &ray, pixel, pw->iteration, b + 3, pw->max_diff, pw->max_total, pw->term_start, c, &next, &emit);
+                shade_principled(pw->ps, &ray, pixel, pw->iteration, b + 3, pw->max_diff, pw->max_total, pw->term_start, c, &next, &emit,
+                                 nee, &nee_valid);
                 acc[0] += c[0];
                 acc[1] += c[1];
                 acc[2] += c[2];
+                if (nee_valid)
+                    for (int k = 0; k < 3; k++) acc[k] += nee[k];
             }
             memcpy(pw->temp + 4 * (size_t)pixel, acc, sizeof(acc));
         }

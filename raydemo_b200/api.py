@@ -344,6 +344,11 @@ class Renderer:
         """1 wavefront, 2 path kernel, 0 chosen by timing (ray_renderer_set_kernel)."""
         check(lib().ray_renderer_set_kernel(self._h, kernel))
 
+    def set_ray_sort(self, policy: int = -1) -> None:
+        """Ray sorting before the wavefront's bounces (ray_renderer_set_ray_sort):
+        -1 chosen per bounce by timing, 0 never, else a mask of bounces (0x3FF all)."""
+        check(lib().ray_renderer_set_ray_sort(self._h, policy))
+
     def set_stream(self, stream: int = 0) -> None:
         """Enqueue the renderer's work on this cudaStream_t (0: its own stream)."""
         check(lib().ray_renderer_set_stream(self._h, stream or None))

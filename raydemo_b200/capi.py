@@ -96,7 +96,8 @@ class TraceInfo(C.Structure):
 
 
 class FrameInfo(C.Structure):
-    _fields_ = [("error_flags", C.c_uint32), ("kernel", C.c_int32), ("rays", C.c_uint64), ("shadow_rays", C.c_uint64)]
+    _fields_ = [("error_flags", C.c_uint32), ("kernel", C.c_int32), ("rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("sort_mask", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class TraceTuning(C.Structure):
@@ -166,6 +167,7 @@ _SIGS = {
     "ray_renderer_frame_info": ([_P, C.POINTER(FrameInfo)], C.c_int),
     "ray_renderer_set_stream": ([_P, _P], C.c_int),
     "ray_renderer_set_kernel": ([_P, C.c_int], C.c_int),
+    "ray_renderer_set_ray_sort": ([_P, C.c_int], C.c_int),
     "ray_render_batch": ([C.POINTER(_P), C.POINTER(_P), C.POINTER(C.POINTER(Region)), C.c_int, C.c_int], C.c_int),
     "ray_sort_rays": ([_P, _P, C.c_uint64, C.POINTER(C.c_float), C.POINTER(C.c_float), _P, _P, _P, _P], C.c_int),
     "ray_sort_rays_noalloc": ([_P, C.c_uint64, C.POINTER(C.c_float), C.POINTER(C.c_float), _P, _P, _P, _P], C.c_int),

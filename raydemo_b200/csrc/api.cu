@@ -220,6 +220,16 @@ int commit(ray_scene *s) {
     if (!inst.empty())
         RG_CUDA_TRY(cudaMemcpyAsync(s->d_inst.p, inst.data(), inst.size() * sizeof(InstanceRec), cudaMemcpyHostToDevice, st));
     s->n_inst_dev = (uint32_t)inst.size();
+    // the scene's box: the union of the instance boxes (the ray hash grid of the render loop's sort)
+    for (int k = 0; k < 3; k++) {
+        s->world_min[k] = inst.empty() ? 0.0f : inst[0].bbox_min[k];
+        s->world_max[k] = inst.empty() ? 0.0f : inst[0].bbox_max[k];
+    }
+    for (const InstanceRec &q : inst)
+        for (int k = 0; k < 3; k++) {
+            s->world_min[k] = std::min(s->world_min[k], q.bbox_min[k]);
+            s->world_max[k] = std::max(s->world_max[k], q.bbox_max[k]);
+        }
     RG_CUDA_TRY(cudaStreamSynchronize(st));
     s->total_nodes = (uint32_t)nodes;
     s->max_depth = 0;

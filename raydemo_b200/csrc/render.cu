@@ -19,8 +19,13 @@ namespace {
 
 constexpr int MAX_BOUNCES = 10; // Core.h:53
 constexpr int TUNE_SAMPLES = 2; // timed frames per kernel before the choice
-constexpr int N_EVENTS = ray_renderer::N_EVENTS; // 4 + 2 * MAX_BOUNCES + 1
-static_assert(N_EVENTS == 5 + 2 * MAX_BOUNCES, "one event per phase");
+constexpr int N_EVENTS = ray_renderer::N_EVENTS; // 4 + 3 * MAX_BOUNCES + 1
+static_assert(N_EVENTS == 5 + 3 * MAX_BOUNCES, "one event per phase");
+constexpr uint32_t SORT_ALL = (1u << MAX_BOUNCES) - 1u;
+// events of bounce b: it starts at ev[3 + 3b] (the end of the previous shade)
+constexpr int ev_sorted(int b) { return 4 + 3 * b; }
+constexpr int ev_traced(int b) { return 5 + 3 * b; }
+constexpr int ev_shaded(int b) { return 6 + 3 * b; }
 
 // ComputeRadicalInversePermutations + Shuffle (src/Ray/internal/Halton.h:7-43)
 // fed as RendererRef.cpp:10-13 does: uniform_int_distribution<int> over mt19937(0).
@@ -82,7 +87,7 @@ int ensure_ray_buffers(ray_renderer *r, size_t n) {
 
 // Counters, the sample table and its permutations, the stats events.
 int ensure_frame_state(ray_renderer *r) {
-    RG_CUDA_TRY(r->d_counters.ensure(8 * sizeof(uint32_t)));
+    RG_CUDA_TRY(r->d_counters.ensure(16 * sizeof(uint32_t)));
     if (!r->d_perms.p) {
         const std::vector<uint16_t> perms = halton_permutations();
         RG_CUDA_TRY(r->d_perms.ensure(perms.size() * sizeof(uint16_t)));
@@ -99,54 +104,125 @@ int ensure_frame_state(ray_renderer *r) {
     return RAY_OK;
 }
 
+// Finishes the timing of a tune entry once every variant it times has its
+// samples: the sort mask (per bounce, sorting where its timed bounce was
+// faster) and the kernel (the path kernel against the wavefront's time with
+// that mask, estimated from the per-bounce times).
+void finish_tune(ray_renderer::TuneEntry &t) {
+    const bool tune_kernel = t.kernel_setting == 0, tune_sort = t.sort_setting < 0;
+    if (t.n[0] < TUNE_SAMPLES || (tune_kernel && t.n[1] < TUNE_SAMPLES) || (tune_sort && t.n[2] < TUNE_SAMPLES)) return;
+    float wave = t.best[0];
+    uint32_t mask = tune_sort ? 0u : (uint32_t)t.sort_setting & SORT_ALL;
+    if (tune_sort) {
+        for (int b = 0; b < t.bounces && b < MAX_BOUNCES; b++) {
+            if (t.bounce_ms[1][b] < t.bounce_ms[0][b]) {
+                mask |= 1u << b;
+                wave -= t.bounce_ms[0][b] - t.bounce_ms[1][b];
+            }
+        }
+        wave = std::min(wave, t.best[2]);
+        if (t.best[2] < t.best[0] && mask == 0) mask = SORT_ALL; // per-bounce noise hid the gain
+    }
+    t.mask = mask;
+    t.choice = (tune_kernel && t.best[1] < wave) ? 2 : 1;
+}
+
 // Adds the phase times of a finished frame to the stats (stats_t, RendererBase.h:93-100).
 int resolve_stats(ray_renderer *r, int set) {
     if (!r->ev_frame_pending[set]) return RAY_OK;
     cudaEvent_t *e = r->ev_sets[set];
     const int nb = r->ev_bounces[set];
     RG_CUDA_TRY(cudaEventSynchronize(e[N_EVENTS - 1]));
-    auto us = [&](int a, int b) -> unsigned long long {
+    auto ms_between = [&](int a, int b) -> float {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, e[a], e[b]);
-        return (unsigned long long)(ms * 1000.0f);
+        return ms;
     };
+    auto us = [&](int a, int b) -> unsigned long long { return (unsigned long long)(ms_between(a, b) * 1000.0f); };
     r->stats.time_primary_ray_gen_us += us(0, 1);
     r->stats.time_primary_trace_us += us(1, 2);
     r->stats.time_primary_shade_us += us(2, 3);
     for (int b = 0; b < nb; b++) {
-        r->stats.time_secondary_trace_us += us(3 + 2 * b, 4 + 2 * b);
-        r->stats.time_secondary_shade_us += us(4 + 2 * b, 5 + 2 * b);
+        r->stats.time_secondary_sort_us += us(3 + 3 * b, ev_sorted(b));
+        r->stats.time_secondary_trace_us += us(ev_sorted(b), ev_traced(b));
+        r->stats.time_secondary_shade_us += us(ev_traced(b), ev_shaded(b));
     }
-    // a frame the kernel choice is timing
+    // a frame the kernel and sort choice is timing
     const int ti = r->ev_tune[set];
     if (ti >= 0 && ti < (int)r->tune.size()) {
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, e[0], e[N_EVENTS - 1]);
         ray_renderer::TuneEntry &t = r->tune[ti];
-        const int k = r->ev_kernel[set] - 1;
-        t.best[k] = std::min(t.best[k], ms);
-        t.n[k]++;
-        if (t.pending[k] > 0) t.pending[k]--;
-        if (t.n[0] >= TUNE_SAMPLES && t.n[1] >= TUNE_SAMPLES) t.choice = t.best[1] < t.best[0] ? 2 : 1;
+        const int v = r->ev_variant[set];
+        t.best[v] = std::min(t.best[v], ms_between(0, N_EVENTS - 1));
+        if (v != 1)
+            for (int b = 0; b < nb && b < MAX_BOUNCES; b++) {
+                float &slot = t.bounce_ms[v == 2 ? 1 : 0][b];
+                const float ms = ms_between(3 + 3 * b, ev_shaded(b));
+                slot = (slot == 0.0f) ? ms : std::min(slot, ms);
+            }
+        t.n[v]++;
+        if (t.pending[v] > 0) t.pending[v]--;
+        finish_tune(t);
     }
     r->ev_tune[set] = -1;
     r->ev_frame_pending[set] = false;
     return RAY_OK;
 }
 
-// Kernel for this frame: the caller's choice, or per frame configuration
-// (scene, its triangle and light counts, rect size, bounces) the faster of
-// the two as timed on its first frames (TUNE_SAMPLES each, the best kept; both
-// give the same image). Returns the kernel and, for a timed frame, the entry.
-int choose_kernel(ray_renderer *r, const ray_scene *s, uint32_t pixels, int bounces, int &tune_entry) {
-    tune_entry = -1;
-    if (r->kernel == 1 || r->kernel == 2) return r->kernel;
+// How a frame runs: the kernel, the sort mask of the wavefront, and, for a
+// frame that times a variant of its configuration, the tune entry and variant.
+struct FramePlan {
+    int kernel = 1;
+    uint32_t sort_mask = 0;
+    int tune_entry = -1, variant = 0;
+};
+
+// The variant of an untimed-enough entry to run next: the one with the
+// fewest timed plus in-flight frames among those the settings leave open.
+int next_variant(const ray_renderer::TuneEntry &t) {
+    int best = 0;
+    for (int v = 1; v < 3; v++) {
+        if (v == 1 && t.kernel_setting != 0) continue;
+        if (v == 2 && t.sort_setting >= 0) continue;
+        if (t.n[v] + t.pending[v] < t.n[best] + t.pending[best]) best = v;
+    }
+    return best;
+}
+
+FramePlan plan_of_variant(const ray_renderer::TuneEntry &t, int v) {
+    FramePlan p;
+    p.variant = v;
+    p.kernel = v == 1 ? 2 : 1;
+    p.sort_mask = v == 2 ? SORT_ALL : (t.sort_setting >= 0 ? (uint32_t)t.sort_setting & SORT_ALL : 0u);
+    return p;
+}
+
+// Per frame configuration (scene, its triangle and light counts, rect size,
+// bounces, the renderer's settings), the kernel and the sort mask: the
+// caller's fixed settings, else timed on the configuration's first frames
+// (TUNE_SAMPLES per variant, the best kept; every variant gives the same image).
+// bounces < 0 marks a batch configuration (-samples; lights then holds the count).
+FramePlan plan_frame(ray_renderer *r, const void *s, uint32_t tris, uint32_t lights, uint32_t pixels, int bounces) {
+    FramePlan p;
+    if (r->kernel == 2) {
+        p.kernel = 2;
+        return p;
+    }
+    if (r->kernel == 1 && r->sort_policy >= 0) {
+        p.sort_mask = (uint32_t)r->sort_policy & SORT_ALL;
+        return p;
+    }
     for (size_t i = 0; i < r->tune.size(); i++) {
         ray_renderer::TuneEntry &t = r->tune[i];
-        if (t.scene == s && t.tris == s->total_tris && t.lights == (uint32_t)s->lights.size() && t.pixels == pixels && t.bounces == bounces) {
-            if (t.choice) return t.choice;
-            tune_entry = (int)i;
-            return t.n[0] + t.pending[0] <= t.n[1] + t.pending[1] ? 1 : 2;
+        if (t.scene == s && t.tris == tris && t.lights == lights && t.pixels == pixels && t.bounces == bounces &&
+            t.kernel_setting == r->kernel && t.sort_setting == r->sort_policy) {
+            if (t.choice) {
+                p.kernel = t.choice;
+                p.sort_mask = t.choice == 1 ? t.mask : 0u;
+                return p;
+            }
+            p = plan_of_variant(t, next_variant(t));
+            p.tune_entry = (int)i;
+            return p;
         }
     }
     if (r->tune.size() >= 64) { // forget them all (the frames in flight lose their timing)
@@ -155,13 +231,16 @@ int choose_kernel(ray_renderer *r, const ray_scene *s, uint32_t pixels, int boun
     }
     ray_renderer::TuneEntry t;
     t.scene = s;
-    t.tris = s->total_tris;
-    t.lights = (uint32_t)s->lights.size();
+    t.tris = tris;
+    t.lights = lights;
     t.pixels = pixels;
     t.bounces = bounces;
+    t.kernel_setting = r->kernel;
+    t.sort_setting = r->sort_policy;
     r->tune.push_back(t);
-    tune_entry = (int)r->tune.size() - 1;
-    return 1;
+    p = plan_of_variant(t, 0);
+    p.tune_entry = (int)r->tune.size() - 1;
+    return p;
 }
 
 // RegionContext's sample table (RendererRef.cpp:85-89): regenerated on the
@@ -266,6 +345,11 @@ int prepare_job(ray_renderer *r, ray_scene *s, ray_region *region, FrameJob &J, 
     J.bounces = (pi.flags & PASS_SKIP_INDIRECT) ? 0 : pi.max_total_depth;
     J.samples = samples;
     J.pixel_base = 0;
+    // the ray hash grid (RendererRef.cpp:48-77): the scene's box in 255 cells per axis
+    for (int k = 0; k < 3; k++) {
+        J.root_min[k] = s->world_min[k];
+        J.cell[k] = (s->world_max[k] - s->world_min[k]) / 255;
+    }
     r->pixels_on_host = r->sh_on_host = false;
     return RAY_OK;
 }
@@ -275,14 +359,25 @@ int prepare_job(ray_renderer *r, ray_scene *s, ray_region *region, FrameJob &J, 
 // jobs, then the accumulation. Buffers and counters are rb's. sample: offset
 // from each job's first iteration. ev (may be null): stats events.
 int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<FrameJob> &jobs, const std::vector<const ray_scene *> &scn,
-                  uint32_t total, int sample, cudaStream_t st, cudaEvent_t *ev, int &nb) {
+                  uint32_t total, int sample, uint32_t sort_mask, cudaStream_t st, cudaEvent_t *ev, int &nb) {
     nb = 0;
     int rc = ensure_ray_buffers(rb, std::max<size_t>(total, 1));
     if (rc != RAY_OK) return rc;
+    if (sort_mask) RG_CUDA_TRY(rb->d_loop_sort.ensure(loop_sort_scratch_bytes(std::max<size_t>(total, 1), (int)jobs.size())));
+    // light samples of RAY_MAT_PRINCIPLED vertices wait in d_shadow (count in counter [8])
+    // for their shadow rays; the reference's own lights are traced inside the shading
+    bool ref_lights = false, nee = false;
+    for (const FrameJob &J : jobs) {
+        ref_lights = ref_lights || J.sc.n_lights > 0;
+        nee = nee || J.sc.n_area_lights > 0;
+    }
+    if (nee) RG_CUDA_TRY(rb->d_shadow.ensure(std::max<size_t>(total, 1) * sizeof(ShadowRec)));
+    ShadowRec *shadow = nee ? static_cast<ShadowRec *>(rb->d_shadow.p) : nullptr;
     for (int k = 0; k < 2; k++) RG_CUDA_TRY(rb->d_job[k].ensure(std::max<size_t>(total, 1) * sizeof(uint32_t)));
     uint32_t *cnt = static_cast<uint32_t *>(rb->d_counters.p);
     unsigned long long *ray_stats = reinterpret_cast<unsigned long long *>(cnt + 4);
     uint32_t *err = cnt + 3;
+    uint32_t *shadow_cnt = cnt + 8;
     float4 *rays[2] = {static_cast<float4 *>(rb->d_rays[0].p), static_cast<float4 *>(rb->d_rays[1].p)};
     RayPayload *pay[2] = {static_cast<RayPayload *>(rb->d_pay[0].p), static_cast<RayPayload *>(rb->d_pay[1].p)};
     uint32_t *job[2] = {static_cast<uint32_t *>(rb->d_job[0].p), static_cast<uint32_t *>(rb->d_job[1].p)};
@@ -311,21 +406,33 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
     tp.ray_job = job[0];
     RG_CUDA_TRY(launch_trace_closest(sv, rays[0], total, hits, obj, err, nullptr, false, st, tp));
     if (ev) RG_CUDA_TRY(cudaEventRecord(ev[2], st));
+    if (nee) RG_CUDA_TRY(cudaMemsetAsync(shadow_cnt, 0, sizeof(uint32_t), st));
     RG_CUDA_TRY(launch_shade_jobs(d_jobs, sample, 2, rays[0], pay[0], job[0], hits, obj, cnt + 0, total, rays[1], pay[1], job[1], cnt + 1,
-                                  err, ray_stats, st));
+                                  shadow, shadow_cnt, ref_lights, err, ray_stats, st));
+    if (nee) RG_CUDA_TRY(launch_shadow_jobs(d_jobs, sample, 2, shadow, shadow_cnt, total, err, ray_stats, st));
     if (ev) RG_CUDA_TRY(cudaEventRecord(ev[3], st));
     // bounces (RendererRef.cpp:183-278); ray counts stay on the device
     int cur = 1;
     for (int bounce = 0; bounce < bounces; bounce++) {
+        if ((sort_mask >> bounce) & 1u) {
+            // SortRays_CPU before each bounce (RendererRef.cpp:200-203): the rays move to the other buffer in hash order
+            const int dst = cur ^ 1;
+            RG_CUDA_TRY(launch_loop_sort(d_jobs, (int)jobs.size(), rays[cur], pay[cur], job[cur], cnt + cur, total, rays[dst], pay[dst], job[dst],
+                                         cnt + dst, rb->d_loop_sort.p, st));
+            cur = dst;
+        }
+        if (ev) RG_CUDA_TRY(cudaEventRecord(ev[ev_sorted(bounce)], st));
         const int nxt = cur ^ 1;
         RG_CUDA_TRY(cudaMemsetAsync(cnt + nxt, 0, sizeof(uint32_t), st));
         tp.count = cnt + cur;
         tp.ray_job = job[cur];
         RG_CUDA_TRY(launch_trace_closest(sv, rays[cur], total, hits, obj, err, nullptr, false, st, tp));
-        if (ev) RG_CUDA_TRY(cudaEventRecord(ev[4 + 2 * bounce], st));
+        if (ev) RG_CUDA_TRY(cudaEventRecord(ev[ev_traced(bounce)], st));
+        if (nee) RG_CUDA_TRY(cudaMemsetAsync(shadow_cnt, 0, sizeof(uint32_t), st));
         RG_CUDA_TRY(launch_shade_jobs(d_jobs, sample, bounce + 3, rays[cur], pay[cur], job[cur], hits, obj, cnt + cur, total, rays[nxt],
-                                      pay[nxt], job[nxt], cnt + nxt, err, ray_stats, st));
-        if (ev) RG_CUDA_TRY(cudaEventRecord(ev[5 + 2 * bounce], st));
+                                      pay[nxt], job[nxt], cnt + nxt, shadow, shadow_cnt, ref_lights, err, ray_stats, st));
+        if (nee) RG_CUDA_TRY(launch_shadow_jobs(d_jobs, sample, bounce + 3, shadow, shadow_cnt, total, err, ray_stats, st));
+        if (ev) RG_CUDA_TRY(cudaEventRecord(ev[ev_shaded(bounce)], st));
         cur = nxt;
         nb++;
     }
@@ -428,8 +535,8 @@ int ray_render(ray_renderer *r, ray_scene *s, ray_region *region) {
         rc = resolve_stats(r, set);
         if (rc != RAY_OK) return rc;
         cudaEvent_t *ev = r->ev_sets[set];
-        int tune_entry = -1;
-        const int kern = choose_kernel(r, s, (uint32_t)n_pix, J.bounces, tune_entry);
+        const FramePlan plan = plan_frame(r, s, s->total_tris, (uint32_t)(s->lights.size() + s->area_lights.size()), (uint32_t)n_pix, J.bounces);
+        const int kern = plan.kernel;
 
         uint32_t *cnt = static_cast<uint32_t *>(r->d_counters.p);
         // [0], [1] ray counts of the two buffers, [2] trace / path work counter,
@@ -449,16 +556,19 @@ int ray_render(ray_renderer *r, ray_scene *s, ray_region *region) {
             RG_CUDA_TRY(cudaEventRecord(ev[2], st));
             RG_CUDA_TRY(cudaEventRecord(ev[3], st));
         } else {
-            rc = run_wavefront(r, d_jobs, std::vector<FrameJob>{J}, std::vector<const ray_scene *>{s}, (uint32_t)n_pix, 0, st, ev, nb);
+            rc = run_wavefront(r, d_jobs, std::vector<FrameJob>{J}, std::vector<const ray_scene *>{s}, (uint32_t)n_pix, 0, plan.sort_mask, st,
+                               ev, nb);
             if (rc != RAY_OK) return rc;
         }
         RG_CUDA_TRY(cudaEventRecord(ev[N_EVENTS - 1], st));
         r->ev_bounces[set] = nb;
-        r->ev_tune[set] = tune_entry;
+        r->ev_tune[set] = plan.tune_entry;
         r->ev_kernel[set] = kern;
-        if (tune_entry >= 0) r->tune[tune_entry].pending[kern - 1]++;
+        r->ev_variant[set] = plan.variant;
+        if (plan.tune_entry >= 0) r->tune[plan.tune_entry].pending[plan.variant]++;
         r->ev_frame_pending[set] = true;
         r->last_kernel = kern;
+        r->last_sort_mask = kern == 1 ? plan.sort_mask : 0u;
         r->frame++;
         return RAY_OK;
     } catch (const std::bad_alloc &) {
@@ -508,36 +618,10 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
             px_all += (q.w == 0 || q.h == 0) ? (uint64_t)renderers[i]->w * renderers[i]->h : (uint64_t)q.w * q.h;
             tris_all += scenes[i]->total_tris;
         }
-        int kern = r0->kernel, tune_entry = -1;
-        if (kern == 0) {
-            for (size_t t = 0; t < r0->tune.size() && tune_entry < 0; t++) {
-                ray_renderer::TuneEntry &e = r0->tune[t];
-                if (e.scene == scenes[0] && e.bounces == -samples && e.lights == (uint32_t)count && e.pixels == (uint32_t)px_all &&
-                    e.tris == (uint32_t)tris_all)
-                    tune_entry = (int)t;
-            }
-            if (tune_entry < 0) {
-                if (r0->tune.size() >= 64) {
-                    r0->tune.clear();
-                    r0->ev_tune[0] = r0->ev_tune[1] = -1;
-                }
-                ray_renderer::TuneEntry e;
-                e.scene = scenes[0];
-                e.bounces = -samples; // a batch entry
-                e.lights = (uint32_t)count;
-                e.pixels = (uint32_t)px_all;
-                e.tris = (uint32_t)tris_all;
-                r0->tune.push_back(e);
-                tune_entry = (int)r0->tune.size() - 1;
-            }
-            const ray_renderer::TuneEntry &e = r0->tune[tune_entry];
-            if (e.choice) {
-                kern = e.choice;
-                tune_entry = -1;
-            } else {
-                kern = e.n[0] <= e.n[1] ? 1 : 2;
-            }
-        }
+        // kernel and sort: the first renderer's settings; what they leave open is
+        // chosen per batch configuration by timing (blocking) its first calls
+        const FramePlan plan = plan_frame(r0, scenes[0], (uint32_t)tris_all, (uint32_t)count, (uint32_t)px_all, -samples);
+        const int kern = plan.kernel, tune_entry = plan.tune_entry;
         if (tune_entry >= 0) RG_CUDA_TRY(cudaEventRecord(r0->ev_batch[0], st));
         for (int done = 0; done < samples;) {
             // a run of iterations that keeps every region within one block of 256 (one sample table each)
@@ -581,7 +665,7 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
                 } else {
                     for (int k = 0; k < run; k++) { // one wavefront per sample over the rays of all jobs
                         int nb = 0;
-                        rc = run_wavefront(r0, d_jobs, jobs, jscn, (uint32_t)total, k, st, nullptr, nb);
+                        rc = run_wavefront(r0, d_jobs, jobs, jscn, (uint32_t)total, k, plan.sort_mask, st, nullptr, nb);
                         if (rc != RAY_OK) return rc;
                     }
                 }
@@ -592,6 +676,7 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
                 ray_renderer *r = renderers[i];
                 if (r->stream != st) RG_CUDA_TRY(cudaStreamWaitEvent(r->stream, r0->ev_sync, 0));
                 r->last_kernel = kern;
+                r->last_sort_mask = kern == 1 ? plan.sort_mask : 0u;
             }
             done += run;
         }
@@ -601,9 +686,9 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
             float ms = 0.0f;
             RG_CUDA_TRY(cudaEventElapsedTime(&ms, r0->ev_batch[0], r0->ev_batch[1]));
             ray_renderer::TuneEntry &e = r0->tune[tune_entry];
-            e.best[kern - 1] = std::min(e.best[kern - 1], ms);
-            e.n[kern - 1]++;
-            if (e.n[0] >= TUNE_SAMPLES && e.n[1] >= TUNE_SAMPLES) e.choice = e.best[1] < e.best[0] ? 2 : 1;
+            e.best[plan.variant] = std::min(e.best[plan.variant], ms);
+            e.n[plan.variant]++;
+            finish_tune(e); // no per-bounce times here: the sort runs before every bounce or none
         }
         return RAY_OK;
     } catch (const std::bad_alloc &) {
@@ -618,6 +703,15 @@ int ray_renderer_set_kernel(ray_renderer *r, int kernel) {
         return RAY_ERR_INVALID_ARG;
     }
     r->kernel = kernel;
+    return RAY_OK;
+}
+
+int ray_renderer_set_ray_sort(ray_renderer *r, int policy) {
+    if (!r || policy < -1 || policy > (int)SORT_ALL) {
+        set_error("ray sort policy must be RAY_SORT_AUTO (-1), 0 or a mask of bounces within RAY_SORT_ALL");
+        return RAY_ERR_INVALID_ARG;
+    }
+    r->sort_policy = policy;
     return RAY_OK;
 }
 
@@ -704,6 +798,7 @@ int ray_renderer_frame_info(ray_renderer *r, ray_frame_info *out) {
     RG_CUDA_TRY(cudaMemcpy(c, r->d_counters.p, sizeof(c), cudaMemcpyDeviceToHost));
     out->error_flags = c[3];
     out->kernel = r->last_kernel;
+    out->sort_mask = r->last_sort_mask;
     memcpy(&out->rays, c + 4, 8);
     memcpy(&out->shadow_rays, c + 6, 8);
     return RAY_OK;

@@ -150,7 +150,17 @@ struct FrameJob {
     int bounces;       // continuation rays traced: max_total_depth, or 0 with skip_indirect_lighting
     int samples;       // consecutive iterations pi.iteration .. + samples - 1, one after another per pixel
     uint32_t pixel_base;
+    float root_min[3], cell[3]; // the ray hash grid: the scene's box split into 255 cells per axis
 };
+
+// A RAY_MAT_PRINCIPLED light sample waiting for its shadow ray (48 bytes):
+// the segment o -> p2, the colour it adds to temp[index] of job `job` when
+// unblocked, and the pixel's sampling index.
+struct ShadowRec {
+    float o[3], p2[3], c[3];
+    uint32_t index, job, rand_index;
+};
+static_assert(sizeof(ShadowRec) == 48, "shadow record layout");
 
 // Launchers (render_kernels.cu). All stream-ordered; counts live on the device.
 cudaError_t launch_halton_table(const uint16_t *perms, int base_iteration, float *table, cudaStream_t st);
@@ -160,18 +170,33 @@ cudaError_t launch_halton_table(const uint16_t *perms, int base_iteration, float
 cudaError_t launch_raygen_jobs(const FrameJob *jobs, int n_jobs, uint32_t total, int sample, float4 *rays, RayPayload *pay,
                                uint32_t *ray_job, uint32_t *count, cudaStream_t st);
 // Shades the hits of *in_count rays (bounce: pass_info_t::bounce, 2 for the
-// primary rays: SetPixel, else AddPixel with alpha 0) and appends the rays
-// that go on to out (count *out_count).
+// primary rays: SetPixel, else AddPixel with alpha 0), appends the rays that
+// go on to out (count *out_count) and the light samples of RAY_MAT_PRINCIPLED
+// vertices to shadow (count *shadow_count, zeroed beforehand). ref_lights:
+// some job's scene has the reference's lights (traced inside the shading).
 cudaError_t launch_shade_jobs(const FrameJob *jobs, int sample, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
                               const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays, float4 *out_rays,
-                              RayPayload *out_pay, uint32_t *out_job, uint32_t *out_count, uint32_t *err, unsigned long long *ray_stats,
-                              cudaStream_t st);
+                              RayPayload *out_pay, uint32_t *out_job, uint32_t *out_count, ShadowRec *shadow, uint32_t *shadow_count,
+                              bool ref_lights, uint32_t *err, unsigned long long *ray_stats, cudaStream_t st);
+// Traces the *count shadow records of a shading launch and adds the colour
+// of each unblocked one to its pixel.
+cudaError_t launch_shadow_jobs(const FrameJob *jobs, int sample, int bounce, const ShadowRec *recs, const uint32_t *count, uint32_t max_recs,
+                               uint32_t *err, unsigned long long *ray_stats, cudaStream_t st);
 // clean += (temp - clean) / iteration over every job's rect, then final = tone(clean)
 cudaError_t launch_resolve_jobs(const FrameJob *jobs, int n_jobs, uint32_t total, int sample, cudaStream_t st);
 // The whole frame of every job in one launch (ray generation, all bounces,
 // accumulation and tone): jobs in device memory, *work zeroed beforehand.
 cudaError_t launch_render_paths(const FrameJob *jobs, int n_jobs, uint32_t total_pixels, uint32_t *work, uint32_t *err,
                                 unsigned long long *ray_stats, cudaStream_t st);
+// Ray sorting between bounces (sort.cu): the *count rays of a wavefront
+// buffer in the order of a stable sort on (job, get_ray_hash of the ray in
+// its job's grid), written to the other buffer with *count_out = *count.
+// capacity: the buffers' size (the sort covers it; entries past *count sort
+// last and are not copied).
+size_t loop_sort_scratch_bytes(uint64_t capacity, int n_jobs);
+cudaError_t launch_loop_sort(const FrameJob *jobs, int n_jobs, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
+                             const uint32_t *count, uint32_t capacity, float4 *rays_out, RayPayload *pay_out, uint32_t *job_out,
+                             uint32_t *count_out, void *scratch, cudaStream_t st);
 cudaError_t launch_fill(float4 *buf, size_t n, float4 v, cudaStream_t st);
 cudaError_t launch_fill_sh(SHData *buf, size_t n, cudaStream_t st);
 

@@ -293,6 +293,15 @@ struct NewRay {
     RayPayload p;
 };
 
+// A RAY_MAT_PRINCIPLED vertex's light sample, traced after the shading: the
+// segment o -> p2 and the colour it adds to the pixel when nothing blocks it
+// (the path weight times the estimator). The pixel's sum takes the shading's
+// colour first and this one after it, in every kernel and in the oracle.
+struct ShadowReq {
+    V3 o, p2, contrib;
+    bool valid;
+};
+
 // Russian roulette and emission of a continuation ray (CoreRef.cpp:2246-2256)
 __device__ __forceinline__ bool roulette(NewRay &r, bool cant_terminate, float p) {
     const float lum = fmax_std(r.p.c[0], fmax_std(r.p.c[1], r.p.c[2]));
@@ -313,11 +322,16 @@ __device__ __forceinline__ void set3(float *dst, V3 v) {
 }
 
 // ShadeSurface, CoreRef.cpp:2055-2391. Returns the pixel contribution;
-// fills nr and sets emit when the path continues.
+// fills nr and sets emit when the path continues, and sr with a
+// RAY_MAT_PRINCIPLED vertex's light sample. REF_LIGHTS: the scene may have
+// the reference's point/spot/directional lights (their shadow rays are traced
+// here); without, the kernel carries no traversal code.
+template <bool REF_LIGHTS>
 __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_index, const float *halton, float4 hit, int obj,
-                        float4 r0, float4 r1, const RayPayload &ray, NewRay &nr, bool &emit, Stack<true> &st, uint32_t &err,
-                        uint32_t &nshadow) {
+                        float4 r0, float4 r1, const RayPayload &ray, NewRay &nr, bool &emit, ShadowReq &sr, Stack<true> &st,
+                        uint32_t &err, uint32_t &nshadow) {
     emit = false;
+    sr.valid = false;
     const int prim = __float_as_int(hit.x);
     const V3 I = v3(r1.x, r1.y, r1.z);
     const uint32_t xy = __float_as_uint(r1.w);
@@ -452,9 +466,10 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
 
     if (mat.type == (uint32_t)RAY_MAT_DIFFUSE) {
         if (!(pi.flags & PASS_SKIP_DIRECT) || pi.bounce > 2) {
-            for (uint32_t li = 0; li < sc.n_lights; li++)
-                accumulate_light(sc, sc.lights[li], I, P, N, B, plane_N, mat.roughness_or_strength, halton, hi, rand_hash2, rand_offset,
-                                 rand_offset2, col, st, err, nshadow);
+            if (REF_LIGHTS)
+                for (uint32_t li = 0; li < sc.n_lights; li++)
+                    accumulate_light(sc, sc.lights[li], I, P, N, B, plane_N, mat.roughness_or_strength, halton, hi, rand_hash2, rand_offset,
+                                     rand_offset2, col, st, err, nshadow);
             if (consider_albedo) col = col * alb;
         }
         if (diff_depth < pi.max_diff_depth && total_depth < pi.max_total_depth) {
@@ -590,8 +605,11 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
                     float pdf_b;
                     ggx::eval(prm, wo_l, ggx::to_local(fr, wi), f_cos, pdf_b);
                     if (f_cos.x > 0.0f || f_cos.y > 0.0f || f_cos.z > 0.0f) {
-                        const float vis = compute_visibility(sc, P_off, p, halton, hi, rand_hash2, st, err, nshadow);
-                        col = col + v3(L.L) * f_cos * (ggx::power_heuristic(pdf_l, pdf_b) * vis / pdf_l);
+                        const V3 e = v3(L.L) * f_cos * (ggx::power_heuristic(pdf_l, pdf_b) / pdf_l);
+                        sr.o = P_off;
+                        sr.p2 = p;
+                        sr.contrib = v3(ray.c[0] * e.x, ray.c[1] * e.y, ray.c[2] * e.z);
+                        sr.valid = true;
                     }
                 }
             } else {
@@ -604,8 +622,11 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
                 float pdf_b;
                 ggx::eval(prm, wo_l, ggx::to_local(fr, wi), f_cos, pdf_b);
                 if (f_cos.x > 0.0f || f_cos.y > 0.0f || f_cos.z > 0.0f) {
-                    const float vis = compute_visibility(sc, P_off, P_off + wi * 1.0e5f, halton, hi, rand_hash2, st, err, nshadow);
-                    col = col + v3(L.L) * f_cos * (vis * (float)nl);
+                    const V3 e = v3(L.L) * f_cos * (float)nl;
+                    sr.o = P_off;
+                    sr.p2 = P_off + wi * 1.0e5f;
+                    sr.contrib = v3(ray.c[0] * e.x, ray.c[1] * e.y, ray.c[2] * e.z);
+                    sr.valid = true;
                 }
             }
         }
@@ -662,10 +683,11 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
 // the hit: weight 1 for rays whose last vertex did not sample quad lights
 // (pdf 0 in the payload), else the power heuristic against the light pdf that
 // next-event estimation at that vertex used.
+template <bool REF_LIGHTS>
 __device__ __forceinline__ F4 shade_surface(const RenderScene &sc, const PassInfo &pi, int rand_index, const float *halton, float4 hit,
-                                            int obj, float4 r0, float4 r1, const RayPayload &ray, NewRay &nr, bool &emit, Stack<true> &st,
-                                            uint32_t &err, uint32_t &nshadow) {
-    F4 c = shade_hit(sc, pi, rand_index, halton, hit, obj, r0, r1, ray, nr, emit, st, err, nshadow);
+                                            int obj, float4 r0, float4 r1, const RayPayload &ray, NewRay &nr, bool &emit, ShadowReq &sr,
+                                            Stack<true> &st, uint32_t &err, uint32_t &nshadow) {
+    F4 c = shade_hit<REF_LIGHTS>(sc, pi, rand_index, halton, hit, obj, r0, r1, ray, nr, emit, sr, st, err, nshadow);
     if (sc.n_area_lights == 0) return c;
     const V3 o = v3(r0.x, r0.y, r0.z), d = v3(r1.x, r1.y, r1.z);
     const float tmax = __float_as_int(hit.x) >= 0 ? hit.y : MAX_DIST;
@@ -769,15 +791,16 @@ __global__ void k_raygen_jobs(const FrameJob *__restrict__ jobs, int n_jobs, uin
 // primary rays). PRIMARY: SetPixel into the job's sample buffer, else AddPixel
 // with alpha 0. A continuation ray is appended where the path goes on and its
 // job traces another bounce.
-template <bool PRIMARY>
-__global__ void __launch_bounds__(SHADE_BLOCK) k_shade_jobs(const FrameJob *__restrict__ jobs, int sample, int bounce,
+template <bool PRIMARY, bool REF_LIGHTS>
+__global__ void __launch_bounds__(SHADE_BLOCK, REF_LIGHTS ? 3 : 4) k_shade_jobs(const FrameJob *__restrict__ jobs, int sample, int bounce,
                                                             const float4 *__restrict__ rays, const RayPayload *__restrict__ pay,
                                                             const uint32_t *__restrict__ ray_job, const float4 *__restrict__ hits,
                                                             const int32_t *__restrict__ obj, const uint32_t *__restrict__ in_count,
                                                             uint32_t max_rays, float4 *__restrict__ out_rays, RayPayload *__restrict__ out_pay,
                                                             uint32_t *__restrict__ out_job, uint32_t *__restrict__ out_count,
+                                                            ShadowRec *__restrict__ shadow, uint32_t *__restrict__ shadow_count,
                                                             uint32_t *__restrict__ err_out, unsigned long long *__restrict__ ray_stats) {
-    __shared__ uint2 s_stack[trav::SMEM_STACK * SHADE_BLOCK];
+    __shared__ uint2 s_stack[REF_LIGHTS ? trav::SMEM_STACK * SHADE_BLOCK : 1];
     Stack<true> st;
     st.smem = s_stack + threadIdx.x;
     st.sp = 0;
@@ -789,6 +812,9 @@ __global__ void __launch_bounds__(SHADE_BLOCK) k_shade_jobs(const FrameJob *__re
         bool append = false;
         uint32_t j = 0;
         NewRay nr;
+        ShadowReq sr;
+        sr.valid = false;
+        uint32_t sr_index = 0, sr_rand = 0;
         if (i < n) {
             j = ray_job[i];
             const FrameJob &J = jobs[j];
@@ -802,7 +828,9 @@ __global__ void __launch_bounds__(SHADE_BLOCK) k_shade_jobs(const FrameJob *__re
             pi.bounce = bounce;
             const int rand_index = (pi.flags & PASS_COHERENT) ? c_sampling_pattern[(y % 8) * 8 + (x % 8)] : index;
             bool emit = false;
-            const F4 c = shade_surface(J.sc, pi, rand_index, J.halton, hits[i], obj[i], r0, r1, p, nr, emit, st, err, nshadow);
+            const F4 c = shade_surface<REF_LIGHTS>(J.sc, pi, rand_index, J.halton, hits[i], obj[i], r0, r1, p, nr, emit, sr, st, err, nshadow);
+            sr_index = (uint32_t)index;
+            sr_rand = (uint32_t)rand_index;
             append = emit && bounce - 2 < J.bounces;
             if (PRIMARY) {
                 J.temp[index] = make_float4(c.x, c.y, c.z, c.w);
@@ -828,6 +856,24 @@ __global__ void __launch_bounds__(SHADE_BLOCK) k_shade_jobs(const FrameJob *__re
                 J.temp[index] = acc;
             }
         }
+        // warp-aggregated append of the light samples
+        const uint32_t ms = __ballot_sync(0xffffffffu, sr.valid);
+        if (ms) {
+            uint32_t slot = 0;
+            const uint32_t leader = __ffs(ms) - 1;
+            if (lane == leader) slot = atomicAdd(shadow_count, (uint32_t)__popc(ms));
+            slot = __shfl_sync(0xffffffffu, slot, leader) + __popc(ms & ((1u << lane) - 1u));
+            if (sr.valid && slot < max_rays) {
+                ShadowRec rec;
+                rec.o[0] = sr.o.x; rec.o[1] = sr.o.y; rec.o[2] = sr.o.z;
+                rec.p2[0] = sr.p2.x; rec.p2[1] = sr.p2.y; rec.p2[2] = sr.p2.z;
+                rec.c[0] = sr.contrib.x; rec.c[1] = sr.contrib.y; rec.c[2] = sr.contrib.z;
+                rec.index = sr_index;
+                rec.job = j;
+                rec.rand_index = sr_rand;
+                shadow[slot] = rec;
+            }
+        }
         // warp-aggregated append of the continuation rays
         const uint32_t m = __ballot_sync(0xffffffffu, append);
         if (m) {
@@ -849,6 +895,41 @@ __global__ void __launch_bounds__(SHADE_BLOCK) k_shade_jobs(const FrameJob *__re
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&ray_stats[0], (unsigned long long)n);
         const uint32_t ws = __reduce_add_sync(0xffffffffu, nshadow);
         if (lane == 0 && ws) atomicAdd(&ray_stats[1], (unsigned long long)ws);
+    }
+}
+
+// The shadow rays of a shading launch's light samples (ComputeVisibility,
+// CoreRef.cpp:1813-1896), a grid over the records; an unblocked one adds its
+// colour to the pixel, after the colour the shading added.
+__global__ void __launch_bounds__(SHADE_BLOCK) k_shadow_jobs(const FrameJob *__restrict__ jobs, int sample, int bounce,
+                                                             const ShadowRec *__restrict__ recs, const uint32_t *__restrict__ count,
+                                                             uint32_t max_recs, uint32_t *__restrict__ err_out,
+                                                             unsigned long long *__restrict__ ray_stats) {
+    __shared__ uint2 s_stack[trav::SMEM_STACK * SHADE_BLOCK];
+    Stack<true> st;
+    st.smem = s_stack + threadIdx.x;
+    st.sp = 0;
+    uint32_t err = 0, nshadow = 0;
+    const uint32_t n = min(*count, max_recs);
+    for (uint32_t i = blockIdx.x * SHADE_BLOCK + threadIdx.x; i < n; i += gridDim.x * SHADE_BLOCK) {
+        const ShadowRec rec = recs[i];
+        const FrameJob &J = jobs[rec.job];
+        const int iteration = J.pi.iteration + sample;
+        const int hi = (iteration & (HALTON_SEQ_LEN - 1)) * HALTON_COUNT + bounce * 2;
+        const int rand_hash2 = hash_i(hash_i((int)rec.rand_index));
+        const float vis = compute_visibility(J.sc, v3(rec.o), v3(rec.p2), J.halton, hi, rand_hash2, st, err, nshadow);
+        if (vis > 0.0f) {
+            float4 acc = J.temp[rec.index];
+            acc.x += rec.c[0];
+            acc.y += rec.c[1];
+            acc.z += rec.c[2];
+            J.temp[rec.index] = acc;
+        }
+    }
+    if (err) atomicOr(err_out, err);
+    if (ray_stats) {
+        const uint32_t ws = __reduce_add_sync(0xffffffffu, nshadow);
+        if ((threadIdx.x & 31u) == 0 && ws) atomicAdd(&ray_stats[1], (unsigned long long)ws);
     }
 }
 
@@ -890,10 +971,19 @@ __device__ __forceinline__ void render_path(const FrameJob &J, uint32_t i, int i
     nrays++;
     NewRay nr;
     bool emit = false;
-    F4 c = shade_surface(J.sc, pi, rand_index, J.halton,
-                         make_float4(__int_as_float(b.prim), b.t, b.prim >= 0 ? b.u : 0.0f, b.prim >= 0 ? b.v : 0.0f), b.obj, r0, r1, pay, nr,
-                         emit, st, err, nshadow);
+    ShadowReq sr;
+    const int rand_hash2 = hash_i(hash_i(rand_index));
+    F4 c = shade_surface<true>(J.sc, pi, rand_index, J.halton,
+                               make_float4(__int_as_float(b.prim), b.t, b.prim >= 0 ? b.u : 0.0f, b.prim >= 0 ? b.v : 0.0f), b.obj, r0, r1, pay,
+                               nr, emit, sr, st, err, nshadow);
     float4 acc = make_float4(c.x, c.y, c.z, c.w);
+    // a light sample adds after the shading's colour, as k_shadow_jobs does
+    if (sr.valid && compute_visibility(J.sc, sr.o, sr.p2, J.halton, (iteration & (HALTON_SEQ_LEN - 1)) * HALTON_COUNT + pi.bounce * 2,
+                                       rand_hash2, st, err, nshadow) > 0.0f) {
+        acc.x += sr.contrib.x;
+        acc.y += sr.contrib.y;
+        acc.z += sr.contrib.z;
+    }
     SHData s;
     if (J.temp_sh) {
         // ResetSampleData + SetSampleDir/SetSampleWeight (FramebufferRef.h:69-88)
@@ -915,13 +1005,19 @@ __device__ __forceinline__ void render_path(const FrameJob &J, uint32_t i, int i
         b = trace_closest_scene(J.sc.sv, r0, r1, st, err);
         nrays++;
         pi.bounce = bounce + 3;
-        c = shade_surface(J.sc, pi, rand_index, J.halton,
-                          make_float4(__int_as_float(b.prim), b.t, b.prim >= 0 ? b.u : 0.0f, b.prim >= 0 ? b.v : 0.0f), b.obj, r0, r1, pay,
-                          nr, emit, st, err, nshadow);
+        c = shade_surface<true>(J.sc, pi, rand_index, J.halton,
+                                make_float4(__int_as_float(b.prim), b.t, b.prim >= 0 ? b.u : 0.0f, b.prim >= 0 ? b.v : 0.0f), b.obj, r0, r1,
+                                pay, nr, emit, sr, st, err, nshadow);
         acc.x += c.x;
         acc.y += c.y;
         acc.z += c.z;
         acc.w += 0.0f;
+        if (sr.valid && compute_visibility(J.sc, sr.o, sr.p2, J.halton, (iteration & (HALTON_SEQ_LEN - 1)) * HALTON_COUNT + pi.bounce * 2,
+                                           rand_hash2, st, err, nshadow) > 0.0f) {
+            acc.x += sr.contrib.x;
+            acc.y += sr.contrib.y;
+            acc.z += sr.contrib.z;
+        }
     }
     J.temp[index] = acc;
     const float mix_k = 1.0f / iteration; // RendererRef.cpp:293
@@ -981,8 +1077,6 @@ __global__ void k_fill_sh(SHData *buf, size_t n) {
     }
 }
 
-int g_shade_blocks = 0;
-
 } // namespace
 
 cudaError_t launch_halton_table(const uint16_t *perms, int base_iteration, float *table, cudaStream_t st) {
@@ -997,25 +1091,47 @@ cudaError_t launch_raygen_jobs(const FrameJob *jobs, int n_jobs, uint32_t total,
     return cudaGetLastError();
 }
 
+// Resident blocks of a kernel on this device (one multiple of the SM count).
+template <typename K>
+static int resident_blocks(K kernel, int fallback_per_sm) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, SHADE_BLOCK, 0);
+    return (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : fallback_per_sm);
+}
+
 cudaError_t launch_shade_jobs(const FrameJob *jobs, int sample, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
                               const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays, float4 *out_rays,
-                              RayPayload *out_pay, uint32_t *out_job, uint32_t *out_count, uint32_t *err, unsigned long long *ray_stats,
-                              cudaStream_t st) {
-    if (g_shade_blocks == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_shade_jobs<false>, SHADE_BLOCK, 0);
-        g_shade_blocks = (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 4);
-    }
+                              RayPayload *out_pay, uint32_t *out_job, uint32_t *out_count, ShadowRec *shadow, uint32_t *shadow_count,
+                              bool ref_lights, uint32_t *err, unsigned long long *ray_stats, cudaStream_t st) {
+    static int resident[2] = {0, 0};
+    int &res = resident[ref_lights ? 1 : 0];
+    if (res == 0) res = ref_lights ? resident_blocks(k_shade_jobs<false, true>, 4) : resident_blocks(k_shade_jobs<false, false>, 4);
     const uint32_t need = (max_rays + SHADE_BLOCK - 1) / SHADE_BLOCK;
-    const uint32_t blocks = need < (uint32_t)g_shade_blocks ? (need > 0 ? need : 1) : (uint32_t)g_shade_blocks;
-    if (bounce == 2)
-        k_shade_jobs<true><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, sample, bounce, rays, pay, ray_job, hits, obj, in_count, max_rays, out_rays,
-                                                           out_pay, out_job, out_count, err, ray_stats);
-    else
-        k_shade_jobs<false><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, sample, bounce, rays, pay, ray_job, hits, obj, in_count, max_rays, out_rays,
-                                                            out_pay, out_job, out_count, err, ray_stats);
+    const uint32_t blocks = need < (uint32_t)res ? (need > 0 ? need : 1) : (uint32_t)res;
+#define RG_SHADE(P, R)                                                                                                                     \
+    k_shade_jobs<P, R><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, sample, bounce, rays, pay, ray_job, hits, obj, in_count, max_rays, out_rays, \
+                                                       out_pay, out_job, out_count, shadow, shadow_count, err, ray_stats)
+    if (bounce == 2) {
+        if (ref_lights) RG_SHADE(true, true);
+        else RG_SHADE(true, false);
+    } else {
+        if (ref_lights) RG_SHADE(false, true);
+        else RG_SHADE(false, false);
+    }
+#undef RG_SHADE
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shadow_jobs(const FrameJob *jobs, int sample, int bounce, const ShadowRec *recs, const uint32_t *count, uint32_t max_recs,
+                               uint32_t *err, unsigned long long *ray_stats, cudaStream_t st) {
+    static int resident = 0;
+    if (resident == 0) resident = resident_blocks(k_shadow_jobs, 4);
+    if (max_recs == 0) return cudaSuccess;
+    const uint32_t need = (max_recs + SHADE_BLOCK - 1) / SHADE_BLOCK;
+    const uint32_t blocks = need < (uint32_t)resident ? need : (uint32_t)resident;
+    k_shadow_jobs<<<blocks, SHADE_BLOCK, 0, st>>>(jobs, sample, bounce, recs, count, max_recs, err, ray_stats);
     return cudaGetLastError();
 }
 

@@ -97,6 +97,7 @@ struct ray_scene {
 
     bool geom_dirty = true, shade_dirty = true;
     uint32_t total_tris = 0, total_nodes = 0, max_depth = 0;
+    float world_min[3] = {0.0f, 0.0f, 0.0f}, world_max[3] = {0.0f, 0.0f, 0.0f}; // union of the instance boxes
 
     // device arrays assembled at commit
     rg::DeviceBuf d_nodes, d_leaf, d_inst, d_tris_ref;
@@ -122,20 +123,23 @@ struct ray_renderer {
     ray_stats stats{};
     std::vector<ray_pixel> host_pixels;
     std::vector<ray_shl1> host_sh;
-    rg::DeviceBuf d_sort_scratch;
+    rg::DeviceBuf d_sort_scratch, d_loop_sort;
 
     // framebuffers (w * h): the sample being accumulated, the running mean,
     // the toned output; spherical-harmonics data when a camera asks for it
     rg::DeviceBuf d_temp, d_clean, d_final, d_temp_sh, d_clean_sh;
-    // wavefront: two ray buffers (trace record + payload), hits, instance ids,
-    // counters [0..1] ray counts, [2] persistent-trace work counter, [3] errors
-    rg::DeviceBuf d_rays[2], d_pay[2], d_job[2], d_hits, d_obj, d_counters;
+    // wavefront: two ray buffers (trace record + payload, job ids), hits,
+    // instance ids, light samples waiting for their shadow rays; counters
+    // [0..1] ray counts, [2] persistent-trace work counter, [3] errors,
+    // [4..7] rays and shadow segments traced (two uint64), [8] light samples
+    rg::DeviceBuf d_rays[2], d_pay[2], d_job[2], d_hits, d_obj, d_counters, d_shadow;
     rg::DeviceBuf d_halton, d_perms;
     int halton_base = -1; // base iteration of the table in d_halton
     bool pixels_on_host = false, sh_on_host = false;
     // phase events of the last two frames (stats): start, after ray generation,
-    // primary trace and shade, two per bounce, and the frame's end
-    static constexpr int N_EVENTS = 25;
+    // primary trace and shade, three per bounce (after its sort, trace and
+    // shade), and the frame's end
+    static constexpr int N_EVENTS = 35;
     cudaEvent_t ev_sets[2][N_EVENTS] = {};
     bool ev_frame_pending[2] = {false, false};
     int ev_bounces[2] = {0, 0};
@@ -145,17 +149,28 @@ struct ray_renderer {
 
     // kernel choice: 0 by timing per frame configuration, 1 wavefront, 2 path kernel
     int kernel = 0, last_kernel = 0;
+    // ray sorting before the wavefront's bounces: -1 chosen per bounce by
+    // timing, else a mask (bit b: sort before secondary bounce b)
+    int sort_policy = -1;
+    uint32_t last_sort_mask = 0;
+    // A frame configuration being timed. Variants: 0 wavefront without
+    // sorting (or with the fixed mask), 1 path kernel, 2 wavefront sorting
+    // before every bounce.
     struct TuneEntry {
         const void *scene = nullptr;
         uint32_t tris = 0, lights = 0, pixels = 0;
         int bounces = 0;
-        int choice = 0;                 // 0 while timing
-        float best[2] = {1e30f, 1e30f}; // best frame time (ms) of each kernel
-        int n[2] = {0, 0}, pending[2] = {0, 0};
+        int kernel_setting = 0, sort_setting = -1;
+        int choice = 0;                        // 0 while timing, else the kernel
+        uint32_t mask = 0;                     // the sort mask chosen with kernel 1
+        float best[3] = {1e30f, 1e30f, 1e30f}; // best frame time (ms) of each variant
+        float bounce_ms[2][10] = {};           // variants 0 and 2: best time of each bounce (sort + trace + shade)
+        int n[3] = {0, 0, 0}, pending[3] = {0, 0, 0};
     };
     std::vector<TuneEntry> tune;
     int ev_tune[2] = {-1, -1}; // tune entry timed by the frame in each event set
     int ev_kernel[2] = {0, 0};
+    int ev_variant[2] = {0, 0};
     rg::DeviceBuf d_jobs;      // FrameJob array of the path kernel
     ~ray_renderer();
 };

@@ -5,6 +5,7 @@
 // adjacent keys into chunks, radix-sorts the chunks stably and expands them
 // again, so equal keys keep their input order.
 #include "radix_sort.cuh"
+#include "render.cuh"
 #include "sort.cuh"
 
 namespace rg {
@@ -60,12 +61,9 @@ __device__ __forceinline__ uint32_t spread2(uint32_t v) {
     return v;
 }
 
-__global__ void k_ray_hash(const float4 *__restrict__ rays, uint32_t n, float3 root_min, float3 cell, uint32_t *__restrict__ keys_out,
-                           uint32_t *__restrict__ sort_keys, uint32_t *__restrict__ perm) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float4 o = rays[2ull * i], d = rays[2ull * i + 1];
-    // get_ray_hash, CoreRef.cpp:316-333
+// get_ray_hash, CoreRef.cpp:316-333: the origin's cell as a 24-bit Morton
+// code under 8 bits of direction sector.
+__device__ __forceinline__ uint32_t ray_hash(float4 o, float4 d, float3 root_min, float3 cell) {
     const int x = clampi(f2i_x86(__fdiv_rn(__fsub_rn(o.x, root_min.x), cell.x)), 0, 255);
     const int y = clampi(f2i_x86(__fdiv_rn(__fsub_rn(o.y, root_min.y), cell.y)), 0, 255);
     const int z = clampi(f2i_x86(__fdiv_rn(__fsub_rn(o.z, root_min.z), cell.z)), 0, 255);
@@ -74,7 +72,14 @@ __global__ void k_ray_hash(const float4 *__restrict__ rays, uint32_t n, float3 r
     const int px = clampi(f2i_x86(__fdiv_rn(__fadd_rn(1.0f, d.x), 0.125f)), 0, 16);
     const uint32_t om = spread2(c_omega[oi]);
     const uint32_t pm = spread2(c_phi[py][px]);
-    const uint32_t key = (om << 25) | (pm << 24) | (spread3((uint32_t)y) << 2) | (spread3((uint32_t)z) << 1) | spread3((uint32_t)x);
+    return (om << 25) | (pm << 24) | (spread3((uint32_t)y) << 2) | (spread3((uint32_t)z) << 1) | spread3((uint32_t)x);
+}
+
+__global__ void k_ray_hash(const float4 *__restrict__ rays, uint32_t n, float3 root_min, float3 cell, uint32_t *__restrict__ keys_out,
+                           uint32_t *__restrict__ sort_keys, uint32_t *__restrict__ perm) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t key = ray_hash(rays[2ull * i], rays[2ull * i + 1], root_min, cell);
     if (keys_out) keys_out[i] = key;
     sort_keys[i] = key;
     perm[i] = i;
@@ -88,7 +93,80 @@ __global__ void k_gather_rays(const float4 *__restrict__ rays, const uint32_t *_
     out[2ull * i + 1] = rays[2ull * s + 1];
 }
 
+// Keys of the render loop's sort: for i < *count the ray's hash in its job's
+// grid (with the job above it when there are several), all ones past *count
+// (sorted last: the sort is stable and they come last in the input).
+template <typename Key>
+__global__ void k_loop_keys(const FrameJob *__restrict__ jobs, const float4 *__restrict__ rays, const uint32_t *__restrict__ ray_job,
+                            const uint32_t *__restrict__ count, uint32_t capacity, Key *__restrict__ keys, uint32_t *__restrict__ perm) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= capacity) return;
+    Key key = ~(Key)0;
+    if (i < min(*count, capacity)) {
+        const uint32_t j = ray_job[i];
+        const FrameJob &J = jobs[j];
+        const uint32_t h = ray_hash(rays[2ull * i], rays[2ull * i + 1], make_float3(J.root_min[0], J.root_min[1], J.root_min[2]),
+                                    make_float3(J.cell[0], J.cell[1], J.cell[2]));
+        key = sizeof(Key) == 8 ? (Key)(((uint64_t)j << 32) | h) : (Key)h;
+    }
+    keys[i] = key;
+    perm[i] = i;
+}
+
+__global__ void k_loop_gather(const float4 *__restrict__ rays, const RayPayload *__restrict__ pay, const uint32_t *__restrict__ ray_job,
+                              const uint32_t *__restrict__ perm, const uint32_t *__restrict__ count, uint32_t capacity,
+                              float4 *__restrict__ rays_out, RayPayload *__restrict__ pay_out, uint32_t *__restrict__ job_out,
+                              uint32_t *__restrict__ count_out) {
+    const uint32_t n = min(*count, capacity);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *count_out = n;
+    if (i >= n) return;
+    const uint32_t s = perm[i];
+    if (s >= n) return; // cannot happen: the first n positions hold the n valid rays
+    rays_out[2ull * i] = rays[2ull * s];
+    rays_out[2ull * i + 1] = rays[2ull * s + 1];
+    static_assert(sizeof(RayPayload) % 16 == 0, "payload copied as uint4");
+    const uint4 *src = reinterpret_cast<const uint4 *>(pay + s);
+    uint4 *dst = reinterpret_cast<uint4 *>(pay_out + i);
+#pragma unroll
+    for (int k = 0; k < (int)(sizeof(RayPayload) / 16); k++) dst[k] = src[k];
+    job_out[i] = ray_job[s];
+}
+
+int job_bits(int n_jobs) {
+    int b = 0;
+    while ((1 << b) < n_jobs) b++;
+    return b;
+}
+
 } // namespace
+
+size_t loop_sort_scratch_bytes(uint64_t capacity, int n_jobs) {
+    const int kb = n_jobs > 1 ? 8 : 4;
+    return ((capacity * kb + 255) / 256) * 256 + ((capacity * 4 + 255) / 256) * 256 + radix_sort_scratch_bytes(capacity, kb);
+}
+
+cudaError_t launch_loop_sort(const FrameJob *jobs, int n_jobs, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
+                             const uint32_t *count, uint32_t capacity, float4 *rays_out, RayPayload *pay_out, uint32_t *job_out,
+                             uint32_t *count_out, void *scratch, cudaStream_t st) {
+    if (capacity == 0) return cudaSuccess;
+    const int kb = n_jobs > 1 ? 8 : 4;
+    char *p = static_cast<char *>(scratch);
+    void *keys = p;
+    uint32_t *perm = reinterpret_cast<uint32_t *>(p + ((uint64_t(capacity) * kb + 255) / 256) * 256);
+    void *rs_scratch = reinterpret_cast<char *>(perm) + ((uint64_t(capacity) * 4 + 255) / 256) * 256;
+    const uint32_t blocks = (capacity + 255) / 256;
+    if (kb == 8)
+        k_loop_keys<uint64_t><<<blocks, 256, 0, st>>>(jobs, rays, ray_job, count, capacity, static_cast<uint64_t *>(keys), perm);
+    else
+        k_loop_keys<uint32_t><<<blocks, 256, 0, st>>>(jobs, rays, ray_job, count, capacity, static_cast<uint32_t *>(keys), perm);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = radix_sort_pairs(keys, perm, capacity, kb, 0, kb == 8 ? 32 + job_bits(n_jobs) : 32, rs_scratch, st);
+    if (e != cudaSuccess) return e;
+    k_loop_gather<<<blocks, 256, 0, st>>>(rays, pay, ray_job, perm, count, capacity, rays_out, pay_out, job_out, count_out);
+    return cudaGetLastError();
+}
 
 size_t sort_rays_scratch_bytes(uint64_t n) { return ((n * 4 + 255) / 256) * 256 + radix_sort_scratch_bytes(n, 4); }
 
