@@ -351,6 +351,45 @@ int ray_renderer_set_kernel(ray_renderer *r, int kernel);
  * launches. Batched frames are not timed into the stats. */
 int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, ray_region *const *regions, int count, int samples);
 
+/* ---- differentiable rendering (no counterpart in the reference).
+ * Parameters of RAY_MAT_PRINCIPLED materials held in caller-owned device
+ * memory: a float RGB albedo texture (albedo_h x albedo_w x 3, linear, read
+ * bilinearly with wrap-around, texel centres at (i + 0.5) / w) and roughness
+ * slots. material_slot (host, one entry per material of the scene, or NULL
+ * for none) gives each material's slot, or -1: a material with a slot takes
+ * its base colour from the texture (times main_color) and its roughness from
+ * the slot. The arrays are read by every later render; NULL p detaches them.
+ * At most 64 slots. roughness_sampling (device, n_roughness; may be NULL):
+ * the roughness that direction sampling, pdfs and MIS weights take instead
+ * of `roughness` -- frozen sampling, under which the rendered estimator is a
+ * smooth function of the roughness and its derivative is exactly what the
+ * adjoint computes (for checking it by finite differences). */
+typedef struct ray_diff_params {
+    const float *albedo;
+    int albedo_w, albedo_h;
+    const float *roughness;
+    int n_roughness;
+    const int32_t *material_slot;
+    int n_materials;
+    const float *roughness_sampling;
+} ray_diff_params;
+int ray_scene_set_diff_params(ray_scene *s, const ray_diff_params *p);
+/* Forward pass: samples iterations first_iteration .. first_iteration +
+ * samples - 1 (from 1, within one block of 256) of the whole frame through
+ * the current camera, without touching the renderer's accumulation.
+ * image_rgb (device, h x w x 3) = mean of the samples; sample_rgb (device,
+ * samples x h x w x 3) = each sample's radiance, which the adjoint needs. */
+int ray_render_diff(ray_renderer *r, ray_scene *s, int first_iteration, int samples, float *image_rgb, float *sample_rgb);
+/* Adjoint pass (path replay backpropagation): replays the paths of the
+ * ray_render_diff call with the same first_iteration and samples and adds
+ * dLoss/dalbedo to grad_albedo (device, albedo_h x albedo_w x 3) and
+ * dLoss/droughness to grad_roughness (device, n_roughness), given d_image
+ * (device, h x w x 3) = dLoss/dimage_rgb. Sampling is detached (pdfs and MIS
+ * weights held constant). Scenes: RAY_MAT_PRINCIPLED materials, quad and sun
+ * lights only (RAY_ERR_UNSUPPORTED otherwise). */
+int ray_render_adjoint(ray_renderer *r, ray_scene *s, int first_iteration, int samples, const float *sample_rgb, const float *d_image,
+                       float *grad_albedo, float *grad_roughness);
+
 /* The CUDA stream the renderer enqueues its work on from now on (a
  * cudaStream_t; NULL: the renderer's own stream). No counterpart in the
  * reference, whose renderers run on the calling thread. Waits for the work

@@ -69,7 +69,7 @@ class Oracle:
         L.orc_hash.restype = C.c_int32
         L.orc_construct_float.argtypes = [C.c_uint32]
         L.orc_construct_float.restype = C.c_float
-        L.orc_render_principled.argtypes = [C.POINTER(OrcPrincipledScene), C.POINTER(OrcCamera), i32, i32, i32, i32, i32, i32, vp, i32]
+        L.orc_render_principled.argtypes = [C.POINTER(OrcPrincipledScene), C.POINTER(OrcCamera), i32, i32, i32, i32, i32, i32, vp, i32, i32]
         L.orc_area_light.argtypes = [i32, vp, vp, vp, C.c_float, vp, vp, vp]
         L.orc_area_light.restype = i32
 
@@ -157,14 +157,19 @@ class Oracle:
             raise ValueError("invalid quad or sun light")
         return out
 
-    def principled_scene(self, spec: dict) -> "PrincipledScene":
+    def principled_scene(self, spec: dict, albedo=None, roughness=None, material_slot=None,
+                         roughness_sampling=None) -> "PrincipledScene":
         """Flattens a scene spec (the format of raydemo_b200.scenes) whose
         materials are all RAY_MAT_PRINCIPLED and whose lights are quad or sun
-        lights into the arrays orc_render_principled reads."""
-        return PrincipledScene(self, spec)
+        lights into the arrays orc_render_principled reads; albedo (h, w, 3),
+        roughness (n,), material_slot: the differentiable parameters;
+        roughness_sampling: frozen roughness for sampling and pdfs."""
+        return PrincipledScene(self, spec, albedo, roughness, material_slot, roughness_sampling)
 
-    def render_principled(self, spec: dict, spp: int, nthreads: int = 8, scene: "PrincipledScene" = None) -> np.ndarray:
-        """The renderer's clean buffer (mean of iterations 1..spp), (h, w, 4)."""
+    def render_principled(self, spec: dict, spp: int, nthreads: int = 8, scene: "PrincipledScene" = None,
+                          plain_mean: bool = False) -> np.ndarray:
+        """The mean of iterations 1..spp, (h, w, 4): the renderer's clean buffer,
+        or with plain_mean the differentiable forward pass's sum / spp."""
         ps = scene if scene is not None else self.principled_scene(spec)
         w, h = spec["size"]
         cam = spec["camera"]
@@ -173,15 +178,17 @@ class Oracle:
                                   focus_factor=cam.get("focus_factor", 0.0))
         out = np.zeros((h, w, 4), np.float32)
         self.lib.orc_render_principled(C.byref(ps.c), C.byref(c), w, h, spp, cam.get("max_diff_depth", 4), cam.get("max_total_depth", 4),
-                                       cam.get("termination_start_depth", 3), _p(out), nthreads)
+                                       cam.get("termination_start_depth", 3), _p(out), nthreads, int(plain_mean))
         return out
 
 
 class OrcPrincipledScene(C.Structure):
     _fields_ = [("tris", C.c_void_p), ("aabbs", C.c_void_p), ("normals", C.c_void_p), ("uvs", C.c_void_p), ("mat", C.c_void_p),
                 ("mesh_tris", C.c_void_p), ("inst_mesh", C.c_void_p), ("inst_xform", C.c_void_p), ("mats", C.c_void_p),
-                ("texels", C.c_void_p), ("tex_info", C.c_void_p), ("lights", C.c_void_p), ("ntris", C.c_int64), ("nmeshes", C.c_int),
-                ("ninst", C.c_int), ("nmats", C.c_int), ("ntex", C.c_int), ("nlights", C.c_int), ("env_col", C.c_float * 3)]
+                ("texels", C.c_void_p), ("tex_info", C.c_void_p), ("lights", C.c_void_p), ("diff_albedo", C.c_void_p),
+                ("diff_rough", C.c_void_p), ("diff_rough_sampling", C.c_void_p), ("ntris", C.c_int64), ("nmeshes", C.c_int), ("ninst", C.c_int), ("nmats", C.c_int),
+                ("ntex", C.c_int), ("nlights", C.c_int), ("diff_aw", C.c_int), ("diff_ah", C.c_int), ("n_diff_rough", C.c_int),
+                ("env_col", C.c_float * 3)]
 
 
 class PrincipledScene:
@@ -191,7 +198,7 @@ class PrincipledScene:
     INVALID = 0xFFFFFFFF
     FIRST_TEXTURE = 2  # a scene's textures 0 and 1 are its default environment and normal map
 
-    def __init__(self, orc: Oracle, spec: dict):
+    def __init__(self, orc: Oracle, spec: dict, albedo=None, roughness=None, material_slot=None, roughness_sampling=None):
         texels, tex_info, off = [], [], 0
         for rgba, srgb, _mips in spec.get("textures", []):
             a = np.ascontiguousarray(rgba, np.uint8)
@@ -201,7 +208,8 @@ class PrincipledScene:
             off += tw * th
         ntex = len(tex_info) // 4
         mats = []
-        for m in spec.get("materials", []):
+        slots = list(material_slot) if material_slot is not None else []
+        for mi, m in enumerate(spec.get("materials", [])):
             if m.get("type") != 6:
                 raise ValueError("only metallic-roughness materials")
             t = m.get("main_texture", self.INVALID)
@@ -211,8 +219,9 @@ class PrincipledScene:
                 ti = t - self.FIRST_TEXTURE
             else:
                 raise ValueError("main texture must be one of the spec's textures")
+            slot = slots[mi] if mi < len(slots) else -1
             mats += [*map(float, m.get("main_color", (1.0, 1.0, 1.0))), float(m.get("roughness", 0.0)), float(m.get("metallic", 0.0)),
-                     float(ti), 0.0, 0.0]
+                     float(ti), float(slot), 0.0]
         tris, aabbs, normals, uvs, mat, mesh_tris = [], [], [], [], [], []
         first = 0
         for attrs, idx, shapes, layout in spec.get("meshes", []):
@@ -258,11 +267,19 @@ class PrincipledScene:
             "texels": np.concatenate(texels) if texels else np.zeros(1, np.uint32),
             "tex_info": np.asarray(tex_info, np.int32),
             "lights": np.ascontiguousarray(np.concatenate(lights) if lights else np.zeros(0), np.float32),
+            "diff_albedo": np.ascontiguousarray(albedo, np.float32) if albedo is not None else np.zeros(0, np.float32),
+            "diff_rough": np.ascontiguousarray(roughness, np.float32).reshape(-1) if roughness is not None else np.zeros(0, np.float32),
+            "diff_rough_sampling": (np.ascontiguousarray(roughness_sampling, np.float32).reshape(-1) if roughness_sampling is not None
+                                    else np.zeros(0, np.float32)),
         }
         a = self.arrays
         c = OrcPrincipledScene()
-        for k in ("tris", "aabbs", "normals", "uvs", "mat", "mesh_tris", "inst_mesh", "inst_xform", "mats", "texels", "tex_info", "lights"):
+        for k in ("tris", "aabbs", "normals", "uvs", "mat", "mesh_tris", "inst_mesh", "inst_xform", "mats", "texels", "tex_info", "lights",
+                  "diff_albedo", "diff_rough", "diff_rough_sampling"):
             setattr(c, k, a[k].ctypes.data if a[k].size else None)
+        if albedo is not None:
+            c.diff_ah, c.diff_aw = a["diff_albedo"].shape[:2]
+            c.n_diff_rough = a["diff_rough"].size
         c.ntris = len(a["tris"])
         c.nmeshes = len(mesh_tris) // 2
         c.ninst = len(inst_mesh)

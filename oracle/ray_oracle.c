@@ -925,6 +925,27 @@ static pv3 sample_plain(const orc_principled_scene *sc, int tex, float u, float 
     return P3(c[0], c[1], c[2]);
 }
 
+/* the differentiable albedo at (u, v): bilinear, wrap-around, texel centres at (i + 0.5) / w */
+static pv3 sample_param(const orc_principled_scene *sc, float u, float v) {
+    const int w = sc->diff_aw, h = sc->diff_ah;
+    float fu = u - floorf(u), fv = v - floorf(v);
+    if (!(fu >= 0.0f && fu < 1.0f)) fu = 0.0f;
+    if (!(fv >= 0.0f && fv < 1.0f)) fv = 0.0f;
+    const float x = fu * (float)w - 0.5f, y = fv * (float)h - 0.5f;
+    const float x0 = floorf(x), y0 = floorf(y);
+    const float kx = x - x0, ky = y - y0;
+    const int ix = (int)x0, iy = (int)y0;
+    const int xa = (ix + w) % w, xb = (ix + 1) % w, ya = (iy + h) % h, yb = (iy + 1) % h;
+    const float *t = sc->diff_albedo;
+    float c[3];
+    for (int k = 0; k < 3; k++) {
+        const float top = t[((size_t)ya * w + xa) * 3 + k] * (1.0f - kx) + t[((size_t)ya * w + xb) * 3 + k] * kx;
+        const float bot = t[((size_t)yb * w + xa) * 3 + k] * (1.0f - kx) + t[((size_t)yb * w + xb) * 3 + k] * kx;
+        c[k] = top * (1.0f - ky) + bot * ky;
+    }
+    return P3(c[0], c[1], c[2]);
+}
+
 /* the default environment map, one white RGBE texel (exponent 128) at the
  * atlas origin, read by SampleLatlong_RGBE (CoreRef.cpp:1772-1798) */
 static float env_white(pv3 dir) {
@@ -993,8 +1014,12 @@ static void shade_principled(const pscene *ps, const ppath *ray, int pixel, int 
             if (!(pdot(Ns, wo) > 0.0f)) Ns = pnorm(plane_N);
             const pframe fr = make_frame(Ns);
             const pv3 wo_l = to_local(&fr, wo);
-            const pv3 base = pmul(sample_plain(sc, (int)m[5], uvx, uvy), P3(m[0], m[1], m[2]));
-            const pparams prm = make_params(base, m[3], m[4]);
+            const int slot = (int)m[6];
+            const int dparam = slot >= 0 && slot < sc->n_diff_rough && sc->diff_albedo != NULL;
+            const pv3 base = pmul(dparam ? sample_param(sc, uvx, uvy) : sample_plain(sc, (int)m[5], uvx, uvy), P3(m[0], m[1], m[2]));
+            const pparams prm = make_params(base, dparam ? sc->diff_rough[slot] : m[3], m[4]);
+            const int frozen = dparam && sc->diff_rough_sampling != NULL;
+            const pparams prm_s = frozen ? make_params(base, sc->diff_rough_sampling[slot], m[4]) : prm;
             const uint32_t sidx = (uint32_t)(iteration - 1);
             const pv3 P_off = padd(P, pscale(plane_N, ORC_HIT_BIAS));
             pv3 col = P3(0.0f, 0.0f, 0.0f);
@@ -1017,9 +1042,10 @@ static void shade_principled(const pscene *ps, const ppath *ray, int pixel, int 
                     const float cos_l = -pdot(wi, P3(L->n[0], L->n[1], L->n[2]));
                     if (cos_l > 0.0f) {
                         const float pdf_l = dist2 / (L->area * cos_l) / (float)nl;
-                        pv3 f_cos;
+                        pv3 f_cos, unused;
                         float pdf_b;
                         ggx_eval(&prm, wo_l, to_local(&fr, wi), &f_cos, &pdf_b);
+                        if (frozen) ggx_eval(&prm_s, wo_l, to_local(&fr, wi), &unused, &pdf_b);
                         if (f_cos.x > 0.0f || f_cos.y > 0.0f || f_cos.z > 0.0f) {
                             const pv3 e = pscale(pmul(Lc, f_cos), power_heuristic(pdf_l, pdf_b) / pdf_l);
                             if (visibility(ps, P_off, p) > 0.0f) {
@@ -1055,10 +1081,11 @@ static void shade_principled(const pscene *ps, const ppath *ray, int pixel, int 
                 sobol2(sidx, dim_seed((uint32_t)pixel, bounce, 0), &u1, &u2);
                 sobol2(sidx, dim_seed((uint32_t)pixel, bounce, 1), &ulobe, &urr);
                 pv3 wi_l;
-                if (ggx_sample(&prm, wo_l, u1, u2, ulobe, &wi_l)) {
-                    pv3 f_cos;
+                if (ggx_sample(&prm_s, wo_l, u1, u2, ulobe, &wi_l)) {
+                    pv3 f_cos, unused;
                     float pdf;
                     ggx_eval(&prm, wo_l, wi_l, &f_cos, &pdf);
+                    if (frozen) ggx_eval(&prm_s, wo_l, wi_l, &unused, &pdf);
                     if (pdf > 0.0f) {
                         const pv3 wi = to_world(&fr, wi_l);
                         next->o = padd(P, pscale(plane_N, pdot(wi, plane_N) > 0.0f ? ORC_HIT_BIAS : -ORC_HIT_BIAS));
@@ -1147,7 +1174,7 @@ static void *prender_worker(void *arg) {
 }
 
 void orc_render_principled(const orc_principled_scene *sc, const orc_camera *cam, int w, int h, int spp, int max_diff_depth,
-                           int max_total_depth, int termination_start_depth, float *out, int nthreads) {
+                           int max_total_depth, int termination_start_depth, float *out, int nthreads, int plain_mean) {
     pscene ps;
     ps.sc = sc;
     ps.bvh = (orc_bvh **)calloc((size_t)(sc->nmeshes > 0 ? sc->nmeshes : 1), sizeof(orc_bvh *));
@@ -1208,9 +1235,16 @@ void orc_render_principled(const orc_principled_scene *sc, const orc_camera *cam
             pthread_create(&th[t], NULL, prender_worker, &pw[t]);
         }
         for (int t = 0; t < nt; t++) pthread_join(th[t], NULL);
-        /* Framebuffer::MixWith (FramebufferRef.cpp:57-68) */
-        const float k = 1.0f / (float)it;
-        for (size_t i = 0; i < 4 * (size_t)w * h; i++) out[i] += (temp[i] - out[i]) * k;
+        if (plain_mean) { /* the differentiable forward pass: a sum, scaled at the end */
+            for (size_t i = 0; i < 4 * (size_t)w * h; i++) out[i] = it == 1 ? temp[i] : out[i] + temp[i];
+        } else { /* Framebuffer::MixWith (FramebufferRef.cpp:57-68) */
+            const float k = 1.0f / (float)it;
+            for (size_t i = 0; i < 4 * (size_t)w * h; i++) out[i] += (temp[i] - out[i]) * k;
+        }
+    }
+    if (plain_mean) {
+        const float inv = 1.0f / (float)spp;
+        for (size_t i = 0; i < 4 * (size_t)w * h; i++) out[i] = out[i] * inv;
     }
     free(temp);
     free(table);

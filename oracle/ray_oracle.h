@@ -108,12 +108,19 @@ float orc_construct_float(uint32_t m);
  *   mesh_tris  2 per mesh: first triangle, triangle count
  *   inst_mesh  per instance: its mesh; inst_xform: 16 floats, column-major
  *   mats       8 floats per material: base rgb, roughness, metallic, texture
- *              index (-1: white), unused x2
+ *              index (-1: white), differentiable slot (-1: none), unused
+ *   diff_*     the differentiable parameters (may be NULL): a float RGB
+ *              albedo (diff_ah x diff_aw x 3) and roughness slots; a material
+ *              with a slot takes base = rgb x albedo(uv), roughness = slot's;
+ *              diff_rough_sampling (may be NULL): frozen roughness for
+ *              sampling, pdfs and MIS weights
  *   texels     RGBA8 of every texture, one after another
  *   tex_info   4 ints per texture: texel offset, w, h, sRGB
  *   lights     20 floats per light, from orc_area_light
  * Renders `spp` iterations (1 .. spp) of the full w x h frame and returns the
- * accumulated mean (the renderer's clean buffer) in out (w * h * 4). */
+ * accumulated mean in out (w * h * 4): the renderer's clean buffer
+ * (clean += (sample - clean) / iteration), or with plain_mean the
+ * differentiable forward pass's (sum of the samples) * (1 / spp). */
 typedef struct orc_principled_scene {
     const orc_tri *tris;
     const float *aabbs, *normals, *uvs;
@@ -125,12 +132,14 @@ typedef struct orc_principled_scene {
     const uint32_t *texels;
     const int32_t *tex_info;
     const float *lights;
+    const float *diff_albedo, *diff_rough, *diff_rough_sampling;
     int64_t ntris;
     int nmeshes, ninst, nmats, ntex, nlights;
+    int diff_aw, diff_ah, n_diff_rough;
     float env_col[3];
 } orc_principled_scene;
 void orc_render_principled(const orc_principled_scene *sc, const orc_camera *cam, int w, int h, int spp, int max_diff_depth,
-                           int max_total_depth, int termination_start_depth, float *out, int nthreads);
+                           int max_total_depth, int termination_start_depth, float *out, int nthreads, int plain_mean);
 /* The 20-float light record of a quad (type 3: position, edge_u, edge_v,
  * radiance) or sun (type 4: direction, full cone angle in degrees,
  * irradiance) light. Returns 0, or -1 for an invalid light. */

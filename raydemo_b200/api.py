@@ -203,6 +203,24 @@ class Scene:
     def set_current_cam(self, i: int) -> None:
         check(lib().ray_scene_set_current_cam(self._h, i))
 
+    def set_diff_params(self, albedo_ptr: int, albedo_w: int, albedo_h: int, roughness_ptr: int, n_roughness: int,
+                        material_slot=None, roughness_sampling_ptr: int = 0) -> None:
+        """Differentiable parameters (ray_scene_set_diff_params): device pointers
+        to a float RGB albedo texture (albedo_h x albedo_w x 3) and n_roughness
+        slots; material_slot: per material its slot or -1 (None: no slots);
+        roughness_sampling_ptr: frozen roughness for sampling (0: none)."""
+        if albedo_ptr is None:
+            check(lib().ray_scene_set_diff_params(self._h, None))
+            return
+        slots = None
+        n = 0
+        if material_slot is not None:
+            n = len(material_slot)
+            slots = (C.c_int32 * max(n, 1))(*[int(k) for k in material_slot])
+        p = capi.DiffParams(albedo_ptr, albedo_w, albedo_h, roughness_ptr, n_roughness,
+                            C.cast(slots, C.POINTER(C.c_int32)) if slots is not None else None, n, roughness_sampling_ptr or None)
+        check(lib().ray_scene_set_diff_params(self._h, C.byref(p)))
+
     def triangle_count(self) -> int:
         out = C.c_uint32()
         check(lib().ray_scene_triangle_count(self._h, C.byref(out)))
@@ -296,6 +314,17 @@ class Renderer:
         out = C.c_void_p()
         check(lib().ray_create_scene(self._h, C.byref(out)))
         return Scene(out.value, self)
+
+    def render_diff(self, scene: Scene, first_iteration: int, samples: int, image_ptr: int, sample_ptr: int) -> None:
+        """Differentiable forward pass (ray_render_diff): device pointers to the
+        mean image (h x w x 3) and the per-sample radiance (samples x h x w x 3)."""
+        check(lib().ray_render_diff(self._h, scene.handle, first_iteration, samples, image_ptr, sample_ptr))
+
+    def render_adjoint(self, scene: Scene, first_iteration: int, samples: int, sample_ptr: int, d_image_ptr: int, grad_albedo_ptr: int,
+                       grad_rough_ptr: int) -> None:
+        """Path-replay adjoint (ray_render_adjoint): accumulates the gradients."""
+        check(lib().ray_render_adjoint(self._h, scene.handle, first_iteration, samples, sample_ptr, d_image_ptr, grad_albedo_ptr,
+                                       grad_rough_ptr))
 
     def RenderScene(self, scene: Scene, region: capi.Region) -> None:
         check(lib().ray_render(self._h, scene.handle, C.byref(region)))

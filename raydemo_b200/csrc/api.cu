@@ -411,6 +411,40 @@ int ray_scene_add_material(ray_scene *s, const ray_mat_desc *m, uint32_t *out_in
     RG_GUARD_END
 }
 
+int ray_scene_set_diff_params(ray_scene *s, const ray_diff_params *p) {
+    RG_CHECK(s, "null scene");
+    if (!p) {
+        for (MaterialRec &m : s->materials)
+            if (m.type == (uint32_t)RAY_MAT_PRINCIPLED) m.textures[2] = RAY_INVALID_INDEX;
+        s->diff_albedo = s->diff_rough = s->diff_rough_sampling = nullptr;
+        s->diff_aw = s->diff_ah = s->n_diff_rough = 0;
+        s->shade_dirty = true;
+        return RAY_OK;
+    }
+    RG_CHECK(p->albedo && p->roughness && p->albedo_w > 0 && p->albedo_h > 0, "albedo and roughness arrays are required");
+    RG_CHECK(p->n_roughness > 0 && p->n_roughness <= 64, "1 to 64 roughness slots");
+    RG_CHECK(!p->material_slot || p->n_materials == (int)s->materials.size(), "one slot entry per material of the scene");
+    if (p->material_slot)
+        for (size_t m = 0; m < s->materials.size(); m++) {
+            const int32_t k = p->material_slot[m];
+            RG_CHECK(k >= -1 && k < p->n_roughness, "material slot out of range");
+            RG_CHECK(k < 0 || s->materials[m].type == (uint32_t)RAY_MAT_PRINCIPLED, "slots are for RAY_MAT_PRINCIPLED materials");
+        }
+    for (size_t m = 0; m < s->materials.size(); m++) {
+        if (s->materials[m].type != (uint32_t)RAY_MAT_PRINCIPLED) continue;
+        const int32_t k = p->material_slot ? p->material_slot[m] : -1;
+        s->materials[m].textures[2] = k >= 0 ? (uint32_t)k : RAY_INVALID_INDEX;
+    }
+    s->diff_albedo = p->albedo;
+    s->diff_rough = p->roughness;
+    s->diff_rough_sampling = p->roughness_sampling;
+    s->diff_aw = p->albedo_w;
+    s->diff_ah = p->albedo_h;
+    s->n_diff_rough = p->n_roughness;
+    s->shade_dirty = true;
+    return RAY_OK;
+}
+
 int ray_scene_remove_material(ray_scene *s, uint32_t i) {
     RG_CHECK(s, "null argument");
     (void)i; // no-op in the reference too (SceneRef.h:87)

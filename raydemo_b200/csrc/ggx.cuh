@@ -191,6 +191,78 @@ __device__ __forceinline__ V3 sample_plain(const RenderScene &sc, uint32_t tex, 
     return r;
 }
 
+// The four texels and bilinear weights of a wrap-around read of a w x h
+// texture at (u, v), texel centres at (i + 0.5) / w: texel k = iy[k >> 1] * w
+// + ix[k & 1], weight wt[k].
+struct Bilinear {
+    uint32_t ix[2], iy[2];
+    float kx, ky;
+};
+__device__ __forceinline__ Bilinear bilinear_at(uint32_t w, uint32_t h, float u, float v) {
+    float fu = u - floorf(u), fv = v - floorf(v);
+    if (!(fu >= 0.0f && fu < 1.0f)) fu = 0.0f;
+    if (!(fv >= 0.0f && fv < 1.0f)) fv = 0.0f;
+    const float x = fu * (float)w - 0.5f, y = fv * (float)h - 0.5f;
+    const float x0 = floorf(x), y0 = floorf(y);
+    Bilinear b;
+    b.kx = x - x0;
+    b.ky = y - y0;
+    const int ix = (int)x0, iy = (int)y0; // -1 .. w - 1
+    b.ix[0] = (uint32_t)((ix + (int)w) % (int)w);
+    b.ix[1] = (uint32_t)((ix + 1) % (int)w);
+    b.iy[0] = (uint32_t)((iy + (int)h) % (int)h);
+    b.iy[1] = (uint32_t)((iy + 1) % (int)h);
+    return b;
+}
+
+// The differentiable albedo (float RGB, h x w x 3) at (u, v).
+__device__ __forceinline__ V3 sample_param(const RenderScene &sc, float u, float v) {
+    const Bilinear b = bilinear_at(sc.diff_aw, sc.diff_ah, u, v);
+    const float *t = sc.diff_albedo;
+    const size_t i00 = ((size_t)b.iy[0] * sc.diff_aw + b.ix[0]) * 3, i01 = ((size_t)b.iy[0] * sc.diff_aw + b.ix[1]) * 3;
+    const size_t i10 = ((size_t)b.iy[1] * sc.diff_aw + b.ix[0]) * 3, i11 = ((size_t)b.iy[1] * sc.diff_aw + b.ix[1]) * 3;
+    float c[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float top = __ldg(t + i00 + k) * (1.0f - b.kx) + __ldg(t + i01 + k) * b.kx;
+        const float bot = __ldg(t + i10 + k) * (1.0f - b.kx) + __ldg(t + i11 + k) * b.kx;
+        c[k] = top * (1.0f - b.ky) + bot * b.ky;
+    }
+    return v3(c[0], c[1], c[2]);
+}
+
+// f * cos of eval() with its derivatives: per channel with respect to the
+// base colour (the same channel) and with respect to alpha. Zero where eval
+// is zero.
+__device__ __forceinline__ void eval_grad(const Params &p, float metallic, V3 wo, V3 wi, V3 &f_cos, V3 &df_dbase, V3 &df_dalpha) {
+    f_cos = df_dbase = df_dalpha = v3(0.0f, 0.0f, 0.0f);
+    if (wo.z <= 0.0f || wi.z <= 0.0f) return;
+    const V3 h = normalize(wo + wi);
+    const float a = p.alpha, a2 = a * a;
+    const float k = h.z * h.z * (a2 - 1.0f) + 1.0f;
+    const float d = a2 / (PI_G * k * k);
+    const float dd_da = 2.0f * a * (k - 2.0f * a2 * h.z * h.z) / (PI_G * k * k * k);
+    const float to = (wo.x * wo.x + wo.y * wo.y) / (wo.z * wo.z), ti = (wi.x * wi.x + wi.y * wi.y) / (wi.z * wi.z);
+    const float so = sqrtf(1.0f + a2 * to), si = sqrtf(1.0f + a2 * ti);
+    const float g2 = 1.0f / (1.0f + 0.5f * (so - 1.0f) + 0.5f * (si - 1.0f));
+    const float dg2_da = -g2 * g2 * (0.5f * a * to / so + 0.5f * a * ti / si);
+    const float c5 = pow5(1.0f - fmax_std(dot(wo, h), 0.0f));
+    const float spec = d * g2 / (4.0f * wo.z * wi.z);
+    const float dspec = (dd_da * g2 + d * dg2_da) / (4.0f * wo.z * wi.z);
+    const float fb = (metallic * (1.0f - c5) * spec + (1.0f - metallic) * INV_PI_G) * wi.z;
+    const float f0[3] = {p.f0.x, p.f0.y, p.f0.z}, dif[3] = {p.diffuse.x, p.diffuse.y, p.diffuse.z};
+    float fc[3], fa[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const float F = f0[c] + (1.0f - f0[c]) * c5;
+        fc[c] = (F * spec + dif[c] * INV_PI_G) * wi.z;
+        fa[c] = F * dspec * wi.z;
+    }
+    f_cos = v3(fc[0], fc[1], fc[2]);
+    df_dbase = v3(fb, fb, fb);
+    df_dalpha = v3(fa[0], fa[1], fa[2]);
+}
+
 // Ray against a quad light (front side only); t in (0, tmax) on a hit.
 __device__ __forceinline__ bool hit_quad(const AreaLight &l, V3 o, V3 d, float tmax, float &t) {
     const V3 n = v3(l.n);

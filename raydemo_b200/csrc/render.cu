@@ -358,9 +358,18 @@ int prepare_job(ray_renderer *r, ray_scene *s, ray_region *region, FrameJob &J, 
 // per bounce a closest-hit trace and a shading launch over the rays of all
 // jobs, then the accumulation. Buffers and counters are rb's. sample: offset
 // from each job's first iteration. ev (may be null): stats events.
+// The adjoint's replay (adj in run_wavefront): its arguments and per-ray state buffers.
+struct AdjointRun {
+    AdjArgs args;
+    AdjState *state[2];
+    AdjShadowRec *recs;
+};
+
 int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<FrameJob> &jobs, const std::vector<const ray_scene *> &scn,
-                  uint32_t total, int sample, uint32_t sort_mask, cudaStream_t st, cudaEvent_t *ev, int &nb) {
+                  uint32_t total, int sample, uint32_t sort_mask, cudaStream_t st, cudaEvent_t *ev, int &nb, bool resolve = true,
+                  const AdjointRun *adj = nullptr) {
     nb = 0;
+    if (adj) sort_mask = 0; // the replay keeps the forward pass's order
     int rc = ensure_ray_buffers(rb, std::max<size_t>(total, 1));
     if (rc != RAY_OK) return rc;
     if (sort_mask) RG_CUDA_TRY(rb->d_loop_sort.ensure(loop_sort_scratch_bytes(std::max<size_t>(total, 1), (int)jobs.size())));
@@ -406,10 +415,23 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
     tp.ray_job = job[0];
     RG_CUDA_TRY(launch_trace_closest(sv, rays[0], total, hits, obj, err, nullptr, false, st, tp));
     if (ev) RG_CUDA_TRY(cudaEventRecord(ev[2], st));
-    if (nee) RG_CUDA_TRY(cudaMemsetAsync(shadow_cnt, 0, sizeof(uint32_t), st));
-    RG_CUDA_TRY(launch_shade_jobs(d_jobs, sample, 2, rays[0], pay[0], job[0], hits, obj, cnt + 0, total, rays[1], pay[1], job[1], cnt + 1,
-                                  shadow, shadow_cnt, ref_lights, err, ray_stats, st));
-    if (nee) RG_CUDA_TRY(launch_shadow_jobs(d_jobs, sample, 2, shadow, shadow_cnt, total, err, ray_stats, st));
+    // shading of the rays in buffer `in` (bounce b), continuation rays to `out`, then the light samples' shadow rays
+    auto shade = [&](int b, int in, int out) -> cudaError_t {
+        cudaError_t e = cudaSuccess;
+        if (nee || adj) e = cudaMemsetAsync(shadow_cnt, 0, sizeof(uint32_t), st);
+        if (e != cudaSuccess) return e;
+        if (adj) {
+            e = launch_adjoint_shade(d_jobs, b, rays[in], pay[in], job[in], adj->state[in], hits, obj, cnt + in, total, rays[out], pay[out],
+                                     job[out], adj->state[out], cnt + out, adj->recs, shadow_cnt, adj->args, err, st);
+            if (e != cudaSuccess) return e;
+            return launch_adjoint_shadow(d_jobs, b, adj->recs, shadow_cnt, total, adj->state[out], adj->args, err, st);
+        }
+        e = launch_shade_jobs(d_jobs, sample, b, rays[in], pay[in], job[in], hits, obj, cnt + in, total, rays[out], pay[out], job[out],
+                              cnt + out, shadow, shadow_cnt, ref_lights, err, ray_stats, st);
+        if (e != cudaSuccess || !nee) return e;
+        return launch_shadow_jobs(d_jobs, sample, b, shadow, shadow_cnt, total, err, ray_stats, st);
+    };
+    RG_CUDA_TRY(shade(2, 0, 1));
     if (ev) RG_CUDA_TRY(cudaEventRecord(ev[3], st));
     // bounces (RendererRef.cpp:183-278); ray counts stay on the device
     int cur = 1;
@@ -428,16 +450,53 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
         tp.ray_job = job[cur];
         RG_CUDA_TRY(launch_trace_closest(sv, rays[cur], total, hits, obj, err, nullptr, false, st, tp));
         if (ev) RG_CUDA_TRY(cudaEventRecord(ev[ev_traced(bounce)], st));
-        if (nee) RG_CUDA_TRY(cudaMemsetAsync(shadow_cnt, 0, sizeof(uint32_t), st));
-        RG_CUDA_TRY(launch_shade_jobs(d_jobs, sample, bounce + 3, rays[cur], pay[cur], job[cur], hits, obj, cnt + cur, total, rays[nxt],
-                                      pay[nxt], job[nxt], cnt + nxt, shadow, shadow_cnt, ref_lights, err, ray_stats, st));
-        if (nee) RG_CUDA_TRY(launch_shadow_jobs(d_jobs, sample, bounce + 3, shadow, shadow_cnt, total, err, ray_stats, st));
+        RG_CUDA_TRY(shade(bounce + 3, cur, nxt));
         if (ev) RG_CUDA_TRY(cudaEventRecord(ev[ev_shaded(bounce)], st));
         cur = nxt;
         nb++;
     }
     // accumulate and tone (RendererRef.cpp:292-324)
-    RG_CUDA_TRY(launch_resolve_jobs(d_jobs, n_jobs, total, sample, st));
+    if (resolve) RG_CUDA_TRY(launch_resolve_jobs(d_jobs, n_jobs, total, sample, st));
+    return RAY_OK;
+}
+
+// The jobs of a differentiable render: sample k (iteration first + k) as job k,
+// each summing into its own w x h slice of d_diff_temp; the whole frame.
+int diff_jobs(ray_renderer *r, ray_scene *s, int first_iteration, int samples, std::vector<FrameJob> &jobs, uint32_t &n_pix) {
+    if (!r || !s) {
+        set_error("null argument");
+        return RAY_ERR_INVALID_ARG;
+    }
+    if (first_iteration < 1 || samples < 1 || samples > HALTON_SEQ_LEN ||
+        table_base(first_iteration) != table_base(first_iteration + samples - 1)) {
+        set_error("the samples' iterations (from 1) must lie in one block of 256");
+        return RAY_ERR_INVALID_ARG;
+    }
+    ray_region reg{{0, 0, 0, 0}, first_iteration - 1};
+    FrameJob J;
+    ray_rect rect;
+    int rc = prepare_job(r, s, &reg, J, rect, 1);
+    if (rc == PREPARE_NOTHING) {
+        set_error("the scene belongs to another device");
+        return RAY_ERR_INVALID_ARG;
+    }
+    if (rc != RAY_OK) return rc;
+    n_pix = (uint32_t)r->w * (uint32_t)r->h;
+    if ((uint64_t)n_pix * samples > 0xffffffffull) {
+        set_error("too many pixels x samples");
+        return RAY_ERR_INVALID_ARG;
+    }
+    RG_CUDA_TRY(r->d_diff_temp.ensure((size_t)n_pix * samples * sizeof(float4)));
+    jobs.assign(samples, J);
+    for (int k = 0; k < samples; k++) {
+        FrameJob &Jk = jobs[k];
+        Jk.pi.iteration = first_iteration + k;
+        Jk.temp = static_cast<float4 *>(r->d_diff_temp.p) + (size_t)k * n_pix;
+        Jk.temp_sh = Jk.clean_sh = nullptr;
+        Jk.pixel_base = (uint32_t)k * n_pix;
+    }
+    RG_CUDA_TRY(r->d_jobs.ensure(jobs.size() * sizeof(FrameJob)));
+    RG_CUDA_TRY(cudaMemcpyAsync(r->d_jobs.p, jobs.data(), jobs.size() * sizeof(FrameJob), cudaMemcpyHostToDevice, r->stream));
     return RAY_OK;
 }
 
@@ -704,6 +763,82 @@ int ray_renderer_set_kernel(ray_renderer *r, int kernel) {
     }
     r->kernel = kernel;
     return RAY_OK;
+}
+
+int ray_render_diff(ray_renderer *r, ray_scene *s, int first_iteration, int samples, float *image_rgb, float *sample_rgb) {
+    try {
+        if (!image_rgb || !sample_rgb) {
+            set_error("null output buffer");
+            return RAY_ERR_INVALID_ARG;
+        }
+        std::vector<FrameJob> jobs;
+        uint32_t n_pix = 0;
+        int rc = diff_jobs(r, s, first_iteration, samples, jobs, n_pix);
+        if (rc != RAY_OK) return rc;
+        cudaStream_t st = r->stream;
+        uint32_t *cnt = static_cast<uint32_t *>(r->d_counters.p);
+        RG_CUDA_TRY(cudaMemsetAsync(cnt, 0, 16 * sizeof(uint32_t), st));
+        const FrameJob *d_jobs = static_cast<const FrameJob *>(r->d_jobs.p);
+        int nb = 0;
+        rc = run_wavefront(r, d_jobs, jobs, std::vector<const ray_scene *>(jobs.size(), s), n_pix * (uint32_t)samples, 0, 0u, st, nullptr, nb,
+                           false);
+        if (rc != RAY_OK) return rc;
+        RG_CUDA_TRY(launch_diff_collect(d_jobs, samples, n_pix, image_rgb, sample_rgb, st));
+        r->last_kernel = 1;
+        r->last_sort_mask = 0;
+        return RAY_OK;
+    } catch (const std::bad_alloc &) {
+        set_error("host allocation failed");
+        return RAY_ERR_OUT_OF_MEMORY;
+    }
+}
+
+int ray_render_adjoint(ray_renderer *r, ray_scene *s, int first_iteration, int samples, const float *sample_rgb, const float *d_image,
+                       float *grad_albedo, float *grad_roughness) {
+    try {
+        if (!r || !s || !sample_rgb || !d_image || !grad_albedo || !grad_roughness) {
+            set_error("null argument");
+            return RAY_ERR_INVALID_ARG;
+        }
+        if (!s->diff_albedo || !s->diff_rough) {
+            set_error("the scene has no differentiable parameters (ray_scene_set_diff_params)");
+            return RAY_ERR_INVALID_ARG;
+        }
+        if (!s->lights.empty()) {
+            set_error("the adjoint takes scenes lit by quad and sun lights only");
+            return RAY_ERR_UNSUPPORTED;
+        }
+        for (const MaterialRec &m : s->materials)
+            if (m.type != (uint32_t)RAY_MAT_PRINCIPLED) {
+                set_error("the adjoint takes scenes of RAY_MAT_PRINCIPLED materials only");
+                return RAY_ERR_UNSUPPORTED;
+            }
+        std::vector<FrameJob> jobs;
+        uint32_t n_pix = 0;
+        int rc = diff_jobs(r, s, first_iteration, samples, jobs, n_pix);
+        if (rc != RAY_OK) return rc;
+        const uint32_t total = n_pix * (uint32_t)samples;
+        for (int k = 0; k < 2; k++) RG_CUDA_TRY(r->d_adj[k].ensure(std::max<size_t>(total, 1) * sizeof(AdjState)));
+        RG_CUDA_TRY(r->d_adj_shadow.ensure(std::max<size_t>(total, 1) * sizeof(AdjShadowRec)));
+        AdjointRun adj;
+        adj.args.sample_rgb = sample_rgb;
+        adj.args.d_image = d_image;
+        adj.args.grad_albedo = grad_albedo;
+        adj.args.grad_rough = grad_roughness;
+        adj.args.inv_spp = 1.0f / (float)samples;
+        adj.state[0] = static_cast<AdjState *>(r->d_adj[0].p);
+        adj.state[1] = static_cast<AdjState *>(r->d_adj[1].p);
+        adj.recs = static_cast<AdjShadowRec *>(r->d_adj_shadow.p);
+        cudaStream_t st = r->stream;
+        uint32_t *cnt = static_cast<uint32_t *>(r->d_counters.p);
+        RG_CUDA_TRY(cudaMemsetAsync(cnt, 0, 16 * sizeof(uint32_t), st));
+        int nb = 0;
+        return run_wavefront(r, static_cast<const FrameJob *>(r->d_jobs.p), jobs, std::vector<const ray_scene *>(jobs.size(), s), total, 0, 0u,
+                             st, nullptr, nb, false, &adj);
+    } catch (const std::bad_alloc &) {
+        set_error("host allocation failed");
+        return RAY_ERR_OUT_OF_MEMORY;
+    }
 }
 
 int ray_renderer_set_ray_sort(ray_renderer *r, int policy) {

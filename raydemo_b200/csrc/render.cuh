@@ -83,6 +83,14 @@ struct RenderScene {
     uint32_t n_tris, n_materials, n_textures, n_lights, n_area_lights;
     float env_col[3], env_clamp;
     uint32_t env_map;
+    // differentiable parameters (ray_scene_set_diff_params): a float RGB
+    // albedo texture (h x w x 3) and roughness slots; a RAY_MAT_PRINCIPLED
+    // material whose textures[2] holds a slot takes its base colour from the
+    // texture (times main_color) and its roughness from the slot
+    const float *diff_albedo;
+    const float *diff_rough;
+    const float *diff_rough_sampling; // null: sampling and pdfs take diff_rough too
+    uint32_t diff_aw, diff_ah, n_diff_rough;
 };
 
 // pass_settings_t flags (src/Ray/Types.h:39-45)
@@ -162,6 +170,42 @@ struct ShadowRec {
 };
 static_assert(sizeof(ShadowRec) == 48, "shadow record layout");
 
+// ---- the path-replay adjoint (differentiable parameters of RAY_MAT_PRINCIPLED)
+constexpr int ADJ_MAX_SLOTS = 64; // roughness slots
+
+// Per ray of the adjoint wavefront (48 bytes): the path's colour summed
+// through its previous vertex (in the order the sample buffer sums it) and
+// what the previous vertex's continuation contributes to the gradient:
+// per channel d(f cos)/d(albedo) / (f cos) times main_color, and
+// d(f cos)/d(roughness) / (f cos), at its texture coordinates and slot.
+struct AdjState {
+    float a[3];
+    float u, v;
+    uint32_t slot; // RAY_INVALID_INDEX: no differentiable previous vertex
+    float ga[3], gr[3];
+};
+static_assert(sizeof(AdjState) == 48, "AdjState layout");
+
+// A light sample of the adjoint wavefront (80 bytes): the segment, its colour
+// (added to the continuation's sum when unblocked), its gradient factors
+// (albedo per channel with d_image folded in, roughness) and where they go.
+struct AdjShadowRec {
+    float o[3], p2[3], nee[3], ga[3];
+    float gr, u, v;
+    uint32_t slot, cont, job, rand_index, index;
+};
+static_assert(sizeof(AdjShadowRec) == 80, "AdjShadowRec layout");
+
+// The adjoint's inputs and outputs. Job k of the launch is sample k: its
+// radiance per pixel at sample_rgb[(k * w * h + pixel) * 3]; d_image: dLoss /
+// d(mean image) per pixel (RGB); gradients accumulate into grad_albedo
+// (diff_ah x diff_aw x 3) and grad_rough (n_diff_rough).
+struct AdjArgs {
+    const float *sample_rgb, *d_image;
+    float *grad_albedo, *grad_rough;
+    float inv_spp;
+};
+
 // Launchers (render_kernels.cu). All stream-ordered; counts live on the device.
 cudaError_t launch_halton_table(const uint16_t *perms, int base_iteration, float *table, cudaStream_t st);
 // The wavefront over the jobs of a launch (rays of several scenes together).
@@ -197,6 +241,17 @@ size_t loop_sort_scratch_bytes(uint64_t capacity, int n_jobs);
 cudaError_t launch_loop_sort(const FrameJob *jobs, int n_jobs, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
                              const uint32_t *count, uint32_t capacity, float4 *rays_out, RayPayload *pay_out, uint32_t *job_out,
                              uint32_t *count_out, void *scratch, cudaStream_t st);
+// Differentiable forward: per pixel, image = (sum over the jobs k of temp_k) / n_jobs
+// and sample_rgb[k] = temp_k (RGB); temp_k = jobs[k].temp, all w x h.
+cudaError_t launch_diff_collect(const FrameJob *jobs, int n_jobs, uint32_t n_pix, float *image, float *sample_rgb, cudaStream_t st);
+// The adjoint's shading (replays the forward shading of each ray and adds the
+// gradient of its previous vertex's continuation) and its light samples.
+cudaError_t launch_adjoint_shade(const FrameJob *jobs, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
+                                 const AdjState *adj_in, const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays,
+                                 float4 *out_rays, RayPayload *out_pay, uint32_t *out_job, AdjState *adj_out, uint32_t *out_count,
+                                 AdjShadowRec *shadow, uint32_t *shadow_count, const AdjArgs &args, uint32_t *err, cudaStream_t st);
+cudaError_t launch_adjoint_shadow(const FrameJob *jobs, int bounce, const AdjShadowRec *recs, const uint32_t *count, uint32_t max_recs,
+                                  AdjState *adj_cont, const AdjArgs &args, uint32_t *err, cudaStream_t st);
 cudaError_t launch_fill(float4 *buf, size_t n, float4 v, cudaStream_t st);
 cudaError_t launch_fill_sh(SHData *buf, size_t n, cudaStream_t st);
 

@@ -302,6 +302,19 @@ struct ShadowReq {
     bool valid;
 };
 
+// What the adjoint needs of a RAY_MAT_PRINCIPLED vertex whose parameters are
+// differentiable: the parameters as read, the local outgoing direction, the
+// light sample's local direction and Le times its estimator scale, and the
+// continuation's local direction.
+struct VertexGrad {
+    bool valid, light, cont;
+    uint32_t slot;
+    float u, v, rough;
+    V3 main_color, wo_l, wl_l, le_s, wi_l;
+    ggx::Params prm;
+    float metallic;
+};
+
 // Russian roulette and emission of a continuation ray (CoreRef.cpp:2246-2256)
 __device__ __forceinline__ bool roulette(NewRay &r, bool cant_terminate, float p) {
     const float lum = fmax_std(r.p.c[0], fmax_std(r.p.c[1], r.p.c[2]));
@@ -329,9 +342,10 @@ __device__ __forceinline__ void set3(float *dst, V3 v) {
 template <bool REF_LIGHTS>
 __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_index, const float *halton, float4 hit, int obj,
                         float4 r0, float4 r1, const RayPayload &ray, NewRay &nr, bool &emit, ShadowReq &sr, Stack<true> &st,
-                        uint32_t &err, uint32_t &nshadow) {
+                        uint32_t &err, uint32_t &nshadow, VertexGrad *vg = nullptr) {
     emit = false;
     sr.valid = false;
+    if (vg) vg->valid = false;
     const int prim = __float_as_int(hit.x);
     const V3 I = v3(r1.x, r1.y, r1.z);
     const uint32_t xy = __float_as_uint(r1.w);
@@ -580,8 +594,27 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
         if (!(dot(Ns, wo) > 0.0f)) Ns = normalize(plane_N); // shading normal facing away: the face normal
         const ggx::Frame fr = ggx::make_frame(Ns);
         const V3 wo_l = ggx::to_local(fr, wo);
-        const V3 base = ggx::sample_plain(sc, mat.textures[1], uvx, uvy) * v3(mat.main_color);
-        const ggx::Params prm = ggx::make_params(base, mat.roughness_or_strength, mat.metallic);
+        // the differentiable parameters where the material has a slot
+        const uint32_t slot = mat.textures[2];
+        const bool dparam = slot < sc.n_diff_rough && sc.diff_albedo != nullptr;
+        const V3 base = (dparam ? ggx::sample_param(sc, uvx, uvy) : ggx::sample_plain(sc, mat.textures[1], uvx, uvy)) * v3(mat.main_color);
+        const float rough = dparam ? __ldg(sc.diff_rough + slot) : mat.roughness_or_strength;
+        const ggx::Params prm = ggx::make_params(base, rough, mat.metallic);
+        // sampling, pdfs and MIS weights: the same parameters unless frozen ones are given
+        const bool frozen = dparam && sc.diff_rough_sampling != nullptr;
+        const ggx::Params prm_s = frozen ? ggx::make_params(base, __ldg(sc.diff_rough_sampling + slot), mat.metallic) : prm;
+        if (vg && dparam) {
+            vg->valid = true;
+            vg->light = vg->cont = false;
+            vg->slot = slot;
+            vg->u = uvx;
+            vg->v = uvy;
+            vg->rough = rough;
+            vg->main_color = v3(mat.main_color);
+            vg->wo_l = wo_l;
+            vg->prm = prm;
+            vg->metallic = mat.metallic;
+        }
         const uint32_t sidx = (uint32_t)(pi.iteration - 1);
         const V3 P_off = P + HIT_BIAS * plane_N;
         if ((!(pi.flags & PASS_SKIP_DIRECT) || pi.bounce > 2) && sc.n_area_lights > 0) {
@@ -604,12 +637,22 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
                     V3 f_cos;
                     float pdf_b;
                     ggx::eval(prm, wo_l, ggx::to_local(fr, wi), f_cos, pdf_b);
+                    if (frozen) {
+                        V3 unused;
+                        ggx::eval(prm_s, wo_l, ggx::to_local(fr, wi), unused, pdf_b);
+                    }
                     if (f_cos.x > 0.0f || f_cos.y > 0.0f || f_cos.z > 0.0f) {
-                        const V3 e = v3(L.L) * f_cos * (ggx::power_heuristic(pdf_l, pdf_b) / pdf_l);
+                        const float scale = ggx::power_heuristic(pdf_l, pdf_b) / pdf_l;
+                        const V3 e = v3(L.L) * f_cos * scale;
                         sr.o = P_off;
                         sr.p2 = p;
                         sr.contrib = v3(ray.c[0] * e.x, ray.c[1] * e.y, ray.c[2] * e.z);
                         sr.valid = true;
+                        if (vg && vg->valid) {
+                            vg->light = true;
+                            vg->wl_l = ggx::to_local(fr, wi);
+                            vg->le_s = v3(L.L) * scale;
+                        }
                     }
                 }
             } else {
@@ -627,6 +670,11 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
                     sr.p2 = P_off + wi * 1.0e5f;
                     sr.contrib = v3(ray.c[0] * e.x, ray.c[1] * e.y, ray.c[2] * e.z);
                     sr.valid = true;
+                    if (vg && vg->valid) {
+                        vg->light = true;
+                        vg->wl_l = ggx::to_local(fr, wi);
+                        vg->le_s = v3(L.L) * (float)nl;
+                    }
                 }
             }
         }
@@ -635,10 +683,14 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
             ggx::sobol2(sidx, ggx::dim_seed((uint32_t)rand_index, pi.bounce, 0), u1, u2);
             ggx::sobol2(sidx, ggx::dim_seed((uint32_t)rand_index, pi.bounce, 1), ulobe, urr);
             V3 wi_l;
-            if (ggx::sample(prm, wo_l, u1, u2, ulobe, wi_l)) {
+            if (ggx::sample(prm_s, wo_l, u1, u2, ulobe, wi_l)) {
                 V3 f_cos;
                 float pdf;
                 ggx::eval(prm, wo_l, wi_l, f_cos, pdf);
+                if (frozen) {
+                    V3 unused;
+                    ggx::eval(prm_s, wo_l, wi_l, unused, pdf);
+                }
                 if (pdf > 0.0f) {
                     const V3 wi = ggx::to_world(fr, wi_l);
                     const V3 o = P + (dot(wi, plane_N) > 0.0f ? HIT_BIAS : -HIT_BIAS) * plane_N;
@@ -655,6 +707,10 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
                     set3(nr.p.dd_dy, der.dd_dy - 2 * (dot_I_pN * der.dndy + der.ddn_dy * plane_N));
                     nr.p.pad[0] = __float_as_uint(pdf); // for the MIS weight where this ray meets a quad light
                     emit = roulette(nr, cant_terminate, urr);
+                    if (vg && vg->valid) {
+                        vg->cont = emit;
+                        vg->wi_l = wi_l;
+                    }
                 }
             }
         }
@@ -686,8 +742,8 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
 template <bool REF_LIGHTS>
 __device__ __forceinline__ F4 shade_surface(const RenderScene &sc, const PassInfo &pi, int rand_index, const float *halton, float4 hit,
                                             int obj, float4 r0, float4 r1, const RayPayload &ray, NewRay &nr, bool &emit, ShadowReq &sr,
-                                            Stack<true> &st, uint32_t &err, uint32_t &nshadow) {
-    F4 c = shade_hit<REF_LIGHTS>(sc, pi, rand_index, halton, hit, obj, r0, r1, ray, nr, emit, sr, st, err, nshadow);
+                                            Stack<true> &st, uint32_t &err, uint32_t &nshadow, VertexGrad *vg = nullptr) {
+    F4 c = shade_hit<REF_LIGHTS>(sc, pi, rand_index, halton, hit, obj, r0, r1, ray, nr, emit, sr, st, err, nshadow, vg);
     if (sc.n_area_lights == 0) return c;
     const V3 o = v3(r0.x, r0.y, r0.z), d = v3(r1.x, r1.y, r1.z);
     const float tmax = __float_as_int(hit.x) >= 0 ? hit.y : MAX_DIST;
@@ -1077,6 +1133,265 @@ __global__ void k_fill_sh(SHData *buf, size_t n) {
     }
 }
 
+// ---- the path-replay adjoint
+//
+// Path replay backpropagation (Vicini, Speierer and Jakob 2021) with detached
+// sampling: each sample's path is traced again with the same random numbers
+// and shaded by the same code as the forward pass; at a vertex with
+// differentiable parameters the gradient of the pixel's loss takes
+//   * the light sample: d_image . beta . Le . s . d(f cos)/dp, when its shadow
+//     ray is unblocked (beta: the path weight, s: its estimator scale);
+//   * the continuation: d_image . R . (d(f cos)/dp) / (f cos) per channel,
+//     with R = (the sample's radiance) - (what the path summed through this
+//     vertex), the radiance that arrived through the continuation. The sum is
+//     kept in the order the forward pass summed it, so R is exact up to the
+//     one subtraction. It is settled when the continuation ray is shaded (or,
+//     the path having ended, never: R = 0).
+// Sampling pdfs and MIS weights are held constant (detached), which keeps the
+// estimator of the gradient of the expected image unbiased.
+
+// d alpha / d roughness of make_params (alpha = max(r^2, 1e-4)).
+__device__ __forceinline__ float dalpha_drough(float r) { return r * r > 1.0e-4f ? 2.0f * r : 0.0f; }
+
+__device__ __forceinline__ void scatter_albedo(const RenderScene &sc, float *grad, float u, float v, float g0, float g1, float g2) {
+    if (g0 == 0.0f && g1 == 0.0f && g2 == 0.0f) return;
+    const ggx::Bilinear b = ggx::bilinear_at(sc.diff_aw, sc.diff_ah, u, v);
+    const float w[4] = {(1.0f - b.kx) * (1.0f - b.ky), b.kx * (1.0f - b.ky), (1.0f - b.kx) * b.ky, b.kx * b.ky};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if (w[k] == 0.0f) continue;
+        float *t = grad + ((size_t)b.iy[k >> 1] * sc.diff_aw + b.ix[k & 1]) * 3;
+        atomicAdd(t + 0, g0 * w[k]);
+        atomicAdd(t + 1, g1 * w[k]);
+        atomicAdd(t + 2, g2 * w[k]);
+    }
+}
+
+__device__ __forceinline__ float safe_ratio(float a, float b) { return b != 0.0f ? a / b : 0.0f; }
+
+__device__ __forceinline__ void flush_slots(float *s_gr, float *grad_rough, uint32_t n_slots) {
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < n_slots; k += blockDim.x)
+        if (s_gr[k] != 0.0f) atomicAdd(grad_rough + k, s_gr[k]);
+}
+
+template <bool PRIMARY>
+__global__ void __launch_bounds__(SHADE_BLOCK, 3) k_adjoint_shade(const FrameJob *__restrict__ jobs, int bounce,
+                                                                  const float4 *__restrict__ rays, const RayPayload *__restrict__ pay,
+                                                                  const uint32_t *__restrict__ ray_job, const AdjState *__restrict__ adj_in,
+                                                                  const float4 *__restrict__ hits, const int32_t *__restrict__ obj,
+                                                                  const uint32_t *__restrict__ in_count, uint32_t max_rays,
+                                                                  float4 *__restrict__ out_rays, RayPayload *__restrict__ out_pay,
+                                                                  uint32_t *__restrict__ out_job, AdjState *__restrict__ adj_out,
+                                                                  uint32_t *__restrict__ out_count, AdjShadowRec *__restrict__ shadow,
+                                                                  uint32_t *__restrict__ shadow_count, AdjArgs args,
+                                                                  uint32_t *__restrict__ err_out) {
+    __shared__ float s_gr[ADJ_MAX_SLOTS];
+    __shared__ uint2 s_stack[1];
+    for (int k = threadIdx.x; k < ADJ_MAX_SLOTS; k += blockDim.x) s_gr[k] = 0.0f;
+    __syncthreads();
+    Stack<true> st;
+    st.smem = s_stack;
+    st.sp = 0;
+    uint32_t err = 0, nshadow = 0;
+    const uint32_t n = min(*in_count, max_rays);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t n_slots = jobs[0].sc.n_diff_rough < (uint32_t)ADJ_MAX_SLOTS ? jobs[0].sc.n_diff_rough : (uint32_t)ADJ_MAX_SLOTS;
+    for (uint32_t base = blockIdx.x * SHADE_BLOCK; base < n; base += gridDim.x * SHADE_BLOCK) {
+        const uint32_t i = base + threadIdx.x;
+        bool append = false, light = false;
+        uint32_t j = 0;
+        NewRay nr;
+        ShadowReq sr;
+        sr.valid = false;
+        AdjState out;
+        AdjShadowRec rec;
+        if (i < n) {
+            j = ray_job[i];
+            const FrameJob &J = jobs[j];
+            const RenderScene &sc = J.sc;
+            const float4 r0 = rays[2ull * i], r1 = rays[2ull * i + 1];
+            const RayPayload p = pay[i];
+            const uint32_t xy = __float_as_uint(r1.w);
+            const int x = (int)(xy >> 16), y = (int)(xy & 0xffffu);
+            const int index = y * J.w + x;
+            const size_t px = (size_t)j * ((size_t)J.w * J.h) + (size_t)index;
+            const float d0 = args.d_image[3ull * index + 0] * args.inv_spp, d1 = args.d_image[3ull * index + 1] * args.inv_spp,
+                        d2 = args.d_image[3ull * index + 2] * args.inv_spp;
+            float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+            if (!PRIMARY) {
+                const AdjState in = adj_in[i];
+                a0 = in.a[0];
+                a1 = in.a[1];
+                a2 = in.a[2];
+                if (in.slot < n_slots) { // the previous vertex's continuation: R = radiance - sum so far
+                    const float R0 = args.sample_rgb[3 * px + 0] - a0, R1 = args.sample_rgb[3 * px + 1] - a1,
+                                R2 = args.sample_rgb[3 * px + 2] - a2;
+                    scatter_albedo(sc, args.grad_albedo, in.u, in.v, d0 * R0 * in.ga[0], d1 * R1 * in.ga[1], d2 * R2 * in.ga[2]);
+                    const float g = d0 * R0 * in.gr[0] + d1 * R1 * in.gr[1] + d2 * R2 * in.gr[2];
+                    if (g != 0.0f) atomicAdd(&s_gr[in.slot], g);
+                }
+            }
+            PassInfo pi = J.pi;
+            pi.bounce = bounce;
+            const int rand_index = (pi.flags & PASS_COHERENT) ? c_sampling_pattern[(y % 8) * 8 + (x % 8)] : index;
+            bool emit = false;
+            VertexGrad vg;
+            const F4 c = shade_surface<false>(sc, pi, rand_index, J.halton, hits[i], obj[i], r0, r1, p, nr, emit, sr, st, err, nshadow, &vg);
+            // the sum as the sample buffer takes it (SetPixel on camera rays, AddPixel after)
+            if (PRIMARY) {
+                a0 = c.x;
+                a1 = c.y;
+                a2 = c.z;
+            } else {
+                a0 += c.x;
+                a1 += c.y;
+                a2 += c.z;
+            }
+            append = emit && bounce - 2 < J.bounces;
+            out.a[0] = a0;
+            out.a[1] = a1;
+            out.a[2] = a2;
+            out.slot = RAY_INVALID_INDEX;
+            out.u = out.v = 0.0f;
+            out.ga[0] = out.ga[1] = out.ga[2] = out.gr[0] = out.gr[1] = out.gr[2] = 0.0f;
+            const bool dv = vg.valid && vg.slot < n_slots;
+            const float dadr = dv ? dalpha_drough(vg.rough) : 0.0f;
+            if (append && dv && vg.cont) {
+                V3 f, dfb, dfa;
+                ggx::eval_grad(vg.prm, vg.metallic, vg.wo_l, vg.wi_l, f, dfb, dfa);
+                out.slot = vg.slot;
+                out.u = vg.u;
+                out.v = vg.v;
+                out.ga[0] = safe_ratio(dfb.x, f.x) * vg.main_color.x;
+                out.ga[1] = safe_ratio(dfb.y, f.y) * vg.main_color.y;
+                out.ga[2] = safe_ratio(dfb.z, f.z) * vg.main_color.z;
+                out.gr[0] = safe_ratio(dfa.x, f.x) * dadr;
+                out.gr[1] = safe_ratio(dfa.y, f.y) * dadr;
+                out.gr[2] = safe_ratio(dfa.z, f.z) * dadr;
+            }
+            if (sr.valid) {
+                light = true;
+                rec.o[0] = sr.o.x; rec.o[1] = sr.o.y; rec.o[2] = sr.o.z;
+                rec.p2[0] = sr.p2.x; rec.p2[1] = sr.p2.y; rec.p2[2] = sr.p2.z;
+                rec.nee[0] = sr.contrib.x; rec.nee[1] = sr.contrib.y; rec.nee[2] = sr.contrib.z;
+                rec.ga[0] = rec.ga[1] = rec.ga[2] = rec.gr = 0.0f;
+                rec.u = vg.u;
+                rec.v = vg.v;
+                rec.slot = RAY_INVALID_INDEX;
+                if (dv && vg.light) {
+                    V3 f, dfb, dfa;
+                    ggx::eval_grad(vg.prm, vg.metallic, vg.wo_l, vg.wl_l, f, dfb, dfa);
+                    // d(beta . Le . s . f cos) with d_image folded in
+                    const float k0 = d0 * p.c[0] * vg.le_s.x, k1 = d1 * p.c[1] * vg.le_s.y, k2 = d2 * p.c[2] * vg.le_s.z;
+                    rec.ga[0] = k0 * dfb.x * vg.main_color.x;
+                    rec.ga[1] = k1 * dfb.y * vg.main_color.y;
+                    rec.ga[2] = k2 * dfb.z * vg.main_color.z;
+                    rec.gr = (k0 * dfa.x + k1 * dfa.y + k2 * dfa.z) * dadr;
+                    rec.slot = vg.slot;
+                }
+                rec.job = j;
+                rec.rand_index = (uint32_t)rand_index;
+                rec.index = (uint32_t)index;
+            }
+        }
+        // continuation rays first (their slots go into the light samples)
+        uint32_t cont = RAY_INVALID_INDEX;
+        const uint32_t m = __ballot_sync(0xffffffffu, append);
+        if (m) {
+            uint32_t slot = 0;
+            const uint32_t leader = __ffs(m) - 1;
+            if (lane == leader) slot = atomicAdd(out_count, (uint32_t)__popc(m));
+            slot = __shfl_sync(0xffffffffu, slot, leader) + __popc(m & ((1u << lane) - 1u));
+            if (append && slot < max_rays) {
+                out_rays[2ull * slot] = nr.r0;
+                out_rays[2ull * slot + 1] = nr.r1;
+                out_pay[slot] = nr.p;
+                out_job[slot] = j;
+                adj_out[slot] = out;
+                cont = slot;
+            }
+        }
+        const uint32_t ml = __ballot_sync(0xffffffffu, light);
+        if (ml) {
+            uint32_t slot = 0;
+            const uint32_t leader = __ffs(ml) - 1;
+            if (lane == leader) slot = atomicAdd(shadow_count, (uint32_t)__popc(ml));
+            slot = __shfl_sync(0xffffffffu, slot, leader) + __popc(ml & ((1u << lane) - 1u));
+            if (light && slot < max_rays) {
+                rec.cont = cont;
+                shadow[slot] = rec;
+            }
+        }
+    }
+    if (err) atomicOr(err_out, err);
+    flush_slots(s_gr, args.grad_rough, n_slots);
+}
+
+__global__ void __launch_bounds__(SHADE_BLOCK) k_adjoint_shadow(const FrameJob *__restrict__ jobs, int bounce,
+                                                                const AdjShadowRec *__restrict__ recs, const uint32_t *__restrict__ count,
+                                                                uint32_t max_recs, AdjState *__restrict__ adj_cont, AdjArgs args,
+                                                                uint32_t *__restrict__ err_out) {
+    __shared__ float s_gr[ADJ_MAX_SLOTS];
+    __shared__ uint2 s_stack[trav::SMEM_STACK * SHADE_BLOCK];
+    for (int k = threadIdx.x; k < ADJ_MAX_SLOTS; k += blockDim.x) s_gr[k] = 0.0f;
+    __syncthreads();
+    Stack<true> st;
+    st.smem = s_stack + threadIdx.x;
+    st.sp = 0;
+    uint32_t err = 0, nshadow = 0;
+    const uint32_t n = min(*count, max_recs);
+    const uint32_t n_slots = jobs[0].sc.n_diff_rough < (uint32_t)ADJ_MAX_SLOTS ? jobs[0].sc.n_diff_rough : (uint32_t)ADJ_MAX_SLOTS;
+    for (uint32_t i = blockIdx.x * SHADE_BLOCK + threadIdx.x; i < n; i += gridDim.x * SHADE_BLOCK) {
+        const AdjShadowRec rec = recs[i];
+        const FrameJob &J = jobs[rec.job];
+        const int hi = (J.pi.iteration & (HALTON_SEQ_LEN - 1)) * HALTON_COUNT + bounce * 2;
+        const int rand_hash2 = hash_i(hash_i((int)rec.rand_index));
+        if (compute_visibility(J.sc, v3(rec.o), v3(rec.p2), J.halton, hi, rand_hash2, st, err, nshadow) > 0.0f) {
+            if (rec.slot < n_slots) {
+                scatter_albedo(J.sc, args.grad_albedo, rec.u, rec.v, rec.ga[0], rec.ga[1], rec.ga[2]);
+                if (rec.gr != 0.0f) atomicAdd(&s_gr[rec.slot], rec.gr);
+            }
+            if (rec.cont != RAY_INVALID_INDEX) { // the sum goes on with the light sample, as in the forward pass
+                AdjState &a = adj_cont[rec.cont];
+                a.a[0] += rec.nee[0];
+                a.a[1] += rec.nee[1];
+                a.a[2] += rec.nee[2];
+            }
+        }
+    }
+    if (err) atomicOr(err_out, err);
+    flush_slots(s_gr, args.grad_rough, n_slots);
+}
+
+// image = (sum over samples of the sample buffers) / n, and each sample's RGB.
+__global__ void k_diff_collect(const FrameJob *__restrict__ jobs, int n_jobs, uint32_t n_pix, float *__restrict__ image,
+                               float *__restrict__ sample_rgb) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_pix) return;
+    float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+    for (int k = 0; k < n_jobs; k++) {
+        const float4 t = jobs[k].temp[i];
+        float *o = sample_rgb + 3 * ((size_t)k * n_pix + i);
+        o[0] = t.x;
+        o[1] = t.y;
+        o[2] = t.z;
+        if (k == 0) {
+            s0 = t.x;
+            s1 = t.y;
+            s2 = t.z;
+        } else {
+            s0 += t.x;
+            s1 += t.y;
+            s2 += t.z;
+        }
+    }
+    const float inv = 1.0f / (float)n_jobs;
+    image[3ull * i + 0] = s0 * inv;
+    image[3ull * i + 1] = s1 * inv;
+    image[3ull * i + 2] = s2 * inv;
+}
+
 } // namespace
 
 cudaError_t launch_halton_table(const uint16_t *perms, int base_iteration, float *table, cudaStream_t st) {
@@ -1155,6 +1470,40 @@ cudaError_t launch_render_paths(const FrameJob *jobs, int n_jobs, uint32_t total
     const uint32_t need = (total_pixels + SHADE_BLOCK - 1) / SHADE_BLOCK;
     const uint32_t grid = need < (uint32_t)blocks ? need : (uint32_t)blocks;
     k_render_paths<<<grid, SHADE_BLOCK, 0, st>>>(jobs, n_jobs, total_pixels, work, err, ray_stats);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diff_collect(const FrameJob *jobs, int n_jobs, uint32_t n_pix, float *image, float *sample_rgb, cudaStream_t st) {
+    if (n_pix == 0 || n_jobs <= 0) return cudaSuccess;
+    k_diff_collect<<<(n_pix + 255) / 256, 256, 0, st>>>(jobs, n_jobs, n_pix, image, sample_rgb);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_shade(const FrameJob *jobs, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
+                                 const AdjState *adj_in, const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays,
+                                 float4 *out_rays, RayPayload *out_pay, uint32_t *out_job, AdjState *adj_out, uint32_t *out_count,
+                                 AdjShadowRec *shadow, uint32_t *shadow_count, const AdjArgs &args, uint32_t *err, cudaStream_t st) {
+    static int resident = 0;
+    if (resident == 0) resident = resident_blocks(k_adjoint_shade<false>, 3);
+    const uint32_t need = (max_rays + SHADE_BLOCK - 1) / SHADE_BLOCK;
+    const uint32_t blocks = need < (uint32_t)resident ? (need > 0 ? need : 1) : (uint32_t)resident;
+    if (bounce == 2)
+        k_adjoint_shade<true><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, bounce, rays, pay, ray_job, adj_in, hits, obj, in_count, max_rays, out_rays,
+                                                              out_pay, out_job, adj_out, out_count, shadow, shadow_count, args, err);
+    else
+        k_adjoint_shade<false><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, bounce, rays, pay, ray_job, adj_in, hits, obj, in_count, max_rays,
+                                                               out_rays, out_pay, out_job, adj_out, out_count, shadow, shadow_count, args, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_shadow(const FrameJob *jobs, int bounce, const AdjShadowRec *recs, const uint32_t *count, uint32_t max_recs,
+                                  AdjState *adj_cont, const AdjArgs &args, uint32_t *err, cudaStream_t st) {
+    static int resident = 0;
+    if (resident == 0) resident = resident_blocks(k_adjoint_shadow, 3);
+    if (max_recs == 0) return cudaSuccess;
+    const uint32_t need = (max_recs + SHADE_BLOCK - 1) / SHADE_BLOCK;
+    const uint32_t blocks = need < (uint32_t)resident ? need : (uint32_t)resident;
+    k_adjoint_shadow<<<blocks, SHADE_BLOCK, 0, st>>>(jobs, bounce, recs, count, max_recs, adj_cont, args, err);
     return cudaGetLastError();
 }
 

@@ -98,6 +98,9 @@ struct ray_scene {
     bool geom_dirty = true, shade_dirty = true;
     uint32_t total_tris = 0, total_nodes = 0, max_depth = 0;
     float world_min[3] = {0.0f, 0.0f, 0.0f}, world_max[3] = {0.0f, 0.0f, 0.0f}; // union of the instance boxes
+    // differentiable parameters (caller-owned device arrays, ray_scene_set_diff_params)
+    const float *diff_albedo = nullptr, *diff_rough = nullptr, *diff_rough_sampling = nullptr;
+    int diff_aw = 0, diff_ah = 0, n_diff_rough = 0;
 
     // device arrays assembled at commit
     rg::DeviceBuf d_nodes, d_leaf, d_inst, d_tris_ref;
@@ -133,6 +136,8 @@ struct ray_renderer {
     // [0..1] ray counts, [2] persistent-trace work counter, [3] errors,
     // [4..7] rays and shadow segments traced (two uint64), [8] light samples
     rg::DeviceBuf d_rays[2], d_pay[2], d_job[2], d_hits, d_obj, d_counters, d_shadow;
+    // differentiable form: the samples' sample buffers, the adjoint's per-ray state and light samples
+    rg::DeviceBuf d_diff_temp, d_adj[2], d_adj_shadow;
     rg::DeviceBuf d_halton, d_perms;
     int halton_base = -1; // base iteration of the table in d_halton
     bool pixels_on_host = false, sh_on_host = false;

@@ -360,6 +360,12 @@ RenderScene render_scene_view(const ray_scene *s) {
     for (int k = 0; k < 3; k++) r.env_col[k] = s->env.env_col[k];
     r.env_clamp = s->env.env_clamp;
     r.env_map = s->env.env_map;
+    r.diff_albedo = s->diff_albedo;
+    r.diff_rough = s->diff_rough;
+    r.diff_rough_sampling = s->diff_rough_sampling;
+    r.diff_aw = (uint32_t)s->diff_aw;
+    r.diff_ah = (uint32_t)s->diff_ah;
+    r.n_diff_rough = (uint32_t)s->n_diff_rough;
     return r;
 }
 

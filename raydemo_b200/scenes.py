@@ -359,7 +359,7 @@ def noise_texture(res: int, seed: int) -> np.ndarray:
 
 
 def atrium(seed: int = 0, w: int = 1280, h: int = 720, max_bounces: int = 8, level: int = 5, n_spheres: int = 16,
-           tex_res: int = 1024, room=(20.0, 4.0, 60.0)) -> dict:
+           tex_res: int = 1024, room=(20.0, 4.0, 60.0), n_materials: int | None = None) -> dict:
     """The metallic-roughness render configuration: a closed box room of
     room[0] x room[1] x room[2] (12 triangles, seen from inside) and
     n_spheres displaced icospheres of 20 * 4^level triangles each (value-noise
@@ -369,7 +369,8 @@ def atrium(seed: int = 0, w: int = 1280, h: int = 720, max_bounces: int = 8, lev
     its albedo from one tex_res^2 RGBA8 value-noise texture (tinted per
     material). Lights: a sun of irradiance 5 (outside the closed room, so its
     shadow rays are all blocked) and 4 quad lights under the ceiling. All
-    surfaces are two-sided."""
+    surfaces are two-sided. n_materials (optional): that many materials in
+    all, the room taking the first and the spheres the others in turn."""
     rng = np.random.default_rng(2000 + seed)
     X, Y, Z = (float(v) for v in room)
     spec = {"textures": [(noise_texture(tex_res, seed), True, False)], "materials": [], "meshes": [], "instances": [], "lights": [],
@@ -396,8 +397,11 @@ def atrium(seed: int = 0, w: int = 1280, h: int = 720, max_bounces: int = 8, lev
     a, i, shapes = _concat(parts)
     spec["meshes"].append((a, i, shapes, 0))
     spec["instances"].append((0, np.eye(4, dtype=np.float32).reshape(-1)))
+    sphere_mats = None
+    if n_materials is not None:
+        sphere_mats = [material(rng.uniform(0.5, 1.0, 3)) for _ in range(max(1, n_materials - 1))]
     for k in range(n_spheres):
-        m = material(rng.uniform(0.5, 1.0, 3))
+        m = material(rng.uniform(0.5, 1.0, 3)) if sphere_mats is None else sphere_mats[k % len(sphere_mats)]
         a, i = displaced_sphere(level, seed * 101 + k, amplitude=0.05)
         spec["meshes"].append((a, i, [(m, m, 0, len(i))], 0))
         s = rng.uniform(0.5, 2.0)
@@ -420,4 +424,33 @@ def atrium(seed: int = 0, w: int = 1280, h: int = 720, max_bounces: int = 8, lev
                       "max_glossy_depth": max_bounces, "termination_start_depth": 3}
     spec["size"] = (w, h)
     spec["tris"] = 12 + n_spheres * 20 * 4 ** level
+    return spec
+
+
+def float_noise_texture(res: int, seed: int) -> np.ndarray:
+    """res x res x 3 float32 albedo in [0.15, 0.85] from two octaves of value noise."""
+    y, x = np.meshgrid(np.arange(res), np.arange(res), indexing="ij")
+    p = np.stack([x.reshape(-1) / res, y.reshape(-1) / res, np.zeros(res * res)], 1)
+    chans = []
+    for c in range(3):
+        n = 0.65 * value_noise(p * 10.0 + 3.0 * c, seed + 11 * c) + 0.35 * value_noise(p * 40.0 + 5.0 * c, seed + 11 * c + 1)
+        chans.append(0.5 + 0.35 * n)
+    return np.clip(np.stack(chans, 1), 0.0, 1.0).astype(np.float32).reshape(res, res, 3)
+
+
+def diff_atrium(seed: int = 0, w: int = 256, h: int = 256, max_bounces: int = 4, level: int = 5, n_spheres: int = 16,
+                tex_res: int = 512, n_materials: int = 8) -> dict:
+    """The differentiable configuration: the atrium with n_materials materials
+    (every one differentiable, material k in roughness slot k) seen at w x h,
+    max_bounces bounces and no Russian roulette (termination starts at the
+    last bounce). Hidden parameters: a tex_res^2 RGB value-noise albedo and
+    roughness U[0.1, 0.9] per material. Returns the scene spec with the keys
+    'albedo_target' (tex_res, tex_res, 3), 'rough_target' (n_materials,) and
+    'material_slot'."""
+    spec = atrium(seed, w, h, max_bounces, level=level, n_spheres=n_spheres, tex_res=64, n_materials=n_materials)
+    rng = np.random.default_rng(3000 + seed)
+    spec["camera"] = dict(spec["camera"], termination_start_depth=max_bounces)
+    spec["albedo_target"] = float_noise_texture(tex_res, seed + 17)
+    spec["rough_target"] = rng.uniform(0.1, 0.9, len(spec["materials"])).astype(np.float32)
+    spec["material_slot"] = list(range(len(spec["materials"])))
     return spec
