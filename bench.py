@@ -456,6 +456,173 @@ def atrium_frames(args, dev, stream, rank: int, world: int) -> dict:
     return out
 
 
+DIFF_WORKLOAD = ("differentiable form: the atrium (16 displaced icospheres of subdivision 5, 8 materials) at 256x256, 8 samples, max 4 "
+                 "bounces; parameters: 512x512 RGB albedo, 8 roughness slots; L2 image loss; path-replay adjoint")
+
+
+def diff_frames(args, dev, stream, rank: int, world: int) -> dict:
+    """The differentiable configuration: forward (ray_render_diff) and adjoint
+    (ray_render_adjoint) times through the torch harness, the adjoint's
+    gradients against central differences (h = 1e-3) of this renderer and of
+    the oracle, and 200 Adam steps of inverse rendering from albedo 0.5 and
+    roughness 0.5 towards the hidden parameters."""
+    import torch
+
+    from raydemo_b200 import api, diff, scenes
+
+    spp, h_fd = 8, 1e-3
+    spec = scenes.diff_atrium(0)
+    w, h = spec["size"]
+    r = api.Renderer(w, h, device=dev.index)
+    sc = build_scene(api, r, spec)
+    slots = spec["material_slot"]
+    tgt_a = torch.tensor(spec["albedo_target"], device=dev)
+    tgt_r = torch.tensor(spec["rough_target"], device=dev)
+
+    def render(a, g, frozen=None):
+        return diff.render(a, g, r, sc, slots, 1, spp, frozen)
+
+    with torch.no_grad():
+        target = render(tgt_a, tgt_r).clone()
+    albedo = torch.full_like(tgt_a, 0.5).requires_grad_(True)
+    rough = torch.full_like(tgt_r, 0.5).requires_grad_(True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    n_t = max(5, min(args.steps, 20))
+    # forward alone, then forward + loss + adjoint (the gradient step)
+    for _ in range(3):
+        with torch.no_grad():
+            render(albedo, rough)
+    torch.cuda.synchronize(dev)
+    ev[0].record()
+    for _ in range(n_t):
+        with torch.no_grad():
+            render(albedo, rough)
+    ev[1].record()
+    for _ in range(n_t):
+        albedo.grad = rough.grad = None
+        loss = ((render(albedo, rough) - target) ** 2).sum()
+        loss.backward()
+    ev[2].record()
+    torch.cuda.synchronize(dev)
+    fwd_ms = ev[0].elapsed_time(ev[1]) / n_t
+    step_ms = ev[1].elapsed_time(ev[2]) / n_t
+    ga = albedo.grad.detach().cpu().numpy().reshape(-1)
+    gr = rough.grad.detach().cpu().numpy()
+
+    def loss_of(a, g, frozen=None):
+        with torch.no_grad():
+            return float(((render(a, g, frozen).double() - target.double()) ** 2).sum())
+
+    # gradient checks: 64 texels drawn at random from those the view sees well (the top fifth by gradient
+    # magnitude: elsewhere the differences of a float32 image drown in its rounding), every roughness slot
+    rng = np.random.default_rng(0)
+    seen = np.flatnonzero(ga != 0.0)
+    well = seen[np.argsort(-np.abs(ga[seen]))][: max(64, len(seen) // 5)]
+    texels = rng.choice(well, size=min(64, len(well)), replace=False)
+    a0, r0 = albedo.detach(), rough.detach()
+    errs_a = []
+    for i in texels:
+        ap, am = a0.clone(), a0.clone()
+        ap.view(-1)[int(i)] += h_fd
+        am.view(-1)[int(i)] -= h_fd
+        fd = (loss_of(ap, r0) - loss_of(am, r0)) / (2 * h_fd)
+        errs_a.append(abs(ga[i] - fd) / max(abs(fd), 1e-12))
+    errs_r, fd_r, fd_r_attached = [], [], []
+    for k in range(len(gr)):
+        gp, gm = r0.clone(), r0.clone()
+        gp[k] += h_fd
+        gm[k] -= h_fd
+        fd = (loss_of(a0, gp, r0) - loss_of(a0, gm, r0)) / (2 * h_fd)
+        fd_r.append(fd)
+        errs_r.append(abs(gr[k] - fd) / max(abs(fd), 1e-12))
+        fd_r_attached.append((loss_of(a0, gp) - loss_of(a0, gm)) / (2 * h_fd))
+    out = {"workload": DIFF_WORKLOAD, "samples": spp, "forward_ms": round(fwd_ms, 3), "grad_step_ms": round(step_ms, 3),
+           "adjoint_ms": round(step_ms - fwd_ms, 3), "grad_step_over_forward": round(step_ms / fwd_ms, 3),
+           "fd_h": h_fd, "albedo_texels_checked": len(texels), "albedo_max_rel_err_vs_fd": round(float(max(errs_a)), 5),
+           "albedo_within_2pct": f"{sum(e <= 0.02 for e in errs_a)}/{len(errs_a)}",
+           "roughness_grad": [round(float(x), 4) for x in gr], "roughness_fd_frozen_sampling": [round(float(x), 4) for x in fd_r],
+           "roughness_max_rel_err_vs_fd": round(float(max(errs_r)), 5),
+           "roughness_within_2pct": f"{sum(e <= 0.02 for e in errs_r)}/{len(errs_r)}",
+           "roughness_fd_same_samples_unfrozen": [round(float(x), 2) for x in fd_r_attached]}
+    if rank == 0 and world == 1 and args.diff_oracle_fd:
+        from oracle.oracle import Oracle
+
+        orc = Oracle()
+        threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+        tnp = target.cpu().numpy().astype(np.float64)
+        a_np, r_np = a0.cpu().numpy(), r0.cpu().numpy()
+
+        def oloss(a, g):
+            ps = orc.principled_scene(spec, a, g, slots, roughness_sampling=r_np)
+            img = orc.render_principled(spec, spp, nthreads=threads, scene=ps, plain_mean=True)[..., :3].astype(np.float64)
+            return float(((img - tnp) ** 2).sum())
+
+        t0 = time.perf_counter()
+        oerr_r = []
+        for k in range(len(gr)):
+            gp, gm = r_np.copy(), r_np.copy()
+            gp[k] += h_fd
+            gm[k] -= h_fd
+            fd = (oloss(a_np, gp) - oloss(a_np, gm)) / (2 * h_fd)
+            oerr_r.append(abs(gr[k] - fd) / max(abs(fd), 1e-12))
+        oerr_a = []
+        for i in texels[:8]:
+            ap, am = a_np.copy().reshape(-1), a_np.copy().reshape(-1)
+            ap[i] += h_fd
+            am[i] -= h_fd
+            fd = (oloss(ap.reshape(a_np.shape), r_np) - oloss(am.reshape(a_np.shape), r_np)) / (2 * h_fd)
+            oerr_a.append(abs(ga[i] - fd) / max(abs(fd), 1e-12))
+        out["oracle_fd"] = {"roughness_max_rel_err": round(float(max(oerr_r)), 5), "albedo_texels": len(oerr_a),
+                            "albedo_max_rel_err": round(float(max(oerr_a)), 5), "seconds": round(time.perf_counter() - t0, 1),
+                            "threads": threads}
+    # inverse rendering: 200 Adam steps towards a 64-sample target. Each step takes the residual from one
+    # render and the adjoint from an independent one (other samples): with the same samples for both, the
+    # gradient would also follow the estimator's variance, which pulls the parameters away from the truth.
+    with torch.no_grad():
+        target = diff.render(tgt_a, tgt_r, r, sc, slots, 1, 64).clone()
+    albedo = torch.full_like(tgt_a, 0.5).requires_grad_(True)
+    rough = torch.full_like(tgt_r, 0.5).requires_grad_(True)
+    opt = torch.optim.Adam([{"params": [albedo], "lr": args.diff_lr_albedo}, {"params": [rough], "lr": args.diff_lr_rough}])
+
+    def loss64():  # the image loss at 64 samples (its noise floor far below the 8-sample loss's)
+        with torch.no_grad():
+            return float(((diff.render(albedo, rough, r, sc, slots, 129, 64) - target) ** 2).sum())
+
+    with torch.no_grad():  # the floor: another 64-sample render at the hidden parameters
+        loss64_truth = float(((diff.render(tgt_a, tgt_r, r, sc, slots, 129, 64) - target) ** 2).sum())
+    loss64_start = loss64()
+    losses = []
+    t0 = time.perf_counter()
+    for step in range(args.diff_steps):
+        opt.zero_grad()
+        first = 1 + (2 * spp * step) % (256 - 2 * spp)
+        with torch.no_grad():
+            resid = diff.render(albedo, rough, r, sc, slots, first, spp) - target
+        img = diff.render(albedo, rough, r, sc, slots, first + spp, spp)
+        (2.0 * resid * img).sum().backward()  # gradient 2 (I_a - T) dI_b
+        opt.step()
+        with torch.no_grad():
+            albedo.clamp_(0.0, 1.0)
+            rough.clamp_(0.05, 1.0)
+        losses.append(float((resid ** 2).sum()))
+    torch.cuda.synchronize(dev)
+    seen_mask = torch.zeros(tgt_a.numel(), dtype=torch.bool, device=dev)
+    seen_mask[torch.as_tensor(seen, device=dev)] = True
+    a_err0 = float(((0.5 - tgt_a.reshape(-1)[seen_mask]) ** 2).mean().sqrt())
+    a_err = float(((albedo.detach().reshape(-1) - tgt_a.reshape(-1))[seen_mask] ** 2).mean().sqrt())
+    secs = time.perf_counter() - t0
+    loss64_end = loss64()
+    out["inverse"] = {"steps": args.diff_steps, "seconds": round(secs, 2), "lr": [args.diff_lr_albedo, args.diff_lr_rough],
+                      "loss8_first": round(losses[0], 3), "loss8_last": round(losses[-1], 3),
+                      "loss64_start": round(loss64_start, 3), "loss64_end": round(loss64_end, 3),
+                      "loss64_ratio": round(loss64_end / loss64_start, 5), "loss64_at_hidden_parameters": round(loss64_truth, 3),
+                      "roughness_mae_start": round(float((0.5 - tgt_r).abs().mean()), 4),
+                      "roughness_mae_end": round(float((rough.detach() - tgt_r).abs().mean()), 4),
+                      "albedo_rmse_seen_start": round(a_err0, 4), "albedo_rmse_seen_end": round(a_err, 4)}
+    r.set_stream(0)
+    return out
+
+
 def run_reference_arm(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -491,7 +658,7 @@ def run_gpu_arm(args) -> None:
     from raydemo_b200.api import Renderer
     from raydemo_b200 import scenes
 
-    if args.render_only or args.batch_only or args.atrium_only:  # one part alone (for profiling)
+    if args.render_only or args.batch_only or args.atrium_only or args.diff_only:  # one part alone (for profiling)
         stream = torch.cuda.Stream(dev)
         torch.cuda.set_stream(stream)
         args.no_cpu_baseline = True
@@ -499,8 +666,10 @@ def run_gpu_arm(args) -> None:
             out = {"render": render_frames(args, dev, stream, rank, world)}
         elif args.batch_only:
             out = {"batch": batch_frames(args, dev, stream, n_scenes=args.batch_scenes)}
-        else:
+        elif args.atrium_only:
             out = {"atrium": atrium_frames(args, dev, stream, rank, world)}
+        else:
+            out = {"diff": diff_frames(args, dev, stream, rank, world)}
         if rank == 0:
             print(json.dumps(out), flush=True)
         if world > 1:
@@ -613,6 +782,7 @@ def run_gpu_arm(args) -> None:
     render = None if args.no_render else render_frames(args, dev, stream, rank, world)
     batch = None if args.no_batch else batch_frames(args, dev, stream)
     atrium = None if args.no_atrium else atrium_frames(args, dev, stream, rank, world)
+    diffr = None if args.no_diff else diff_frames(args, dev, stream, rank, world)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -624,7 +794,7 @@ def run_gpu_arm(args) -> None:
                 "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": N_RAYS * 32, "d2h_bytes_per_step": N_RAYS * 16,
                         "matches_device_path": bool(ok)},
                 "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "render": render, "batch": batch,
-                "atrium": atrium}
+                "atrium": atrium, "diff": diffr}
         print(json.dumps(line), flush=True)
     del sc, r
     if world > 1:
@@ -649,6 +819,13 @@ def main() -> None:
     ap.add_argument("--atrium-only", action="store_true", help="only the atrium frames")
     ap.add_argument("--atrium-oracle-spp", type=int, default=16,
                     help="samples the oracle renders for the atrium's image check and CPU time (16: the whole frame; 0: none)")
+    ap.add_argument("--no-diff", action="store_true", help="skip the differentiable form")
+    ap.add_argument("--diff-only", action="store_true", help="only the differentiable form")
+    ap.add_argument("--diff-steps", type=int, default=200, help="Adam steps of the inverse-rendering run")
+    ap.add_argument("--diff-lr-albedo", type=float, default=2e-3)
+    ap.add_argument("--diff-lr-rough", type=float, default=1e-2)
+    ap.add_argument("--no-diff-oracle-fd", dest="diff_oracle_fd", action="store_false",
+                    help="skip the oracle's finite differences in the differentiable form")
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes per launch of the traversal kernel from an ncu capture (reported as roofline.traffic)")
     args = ap.parse_args()

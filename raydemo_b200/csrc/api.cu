@@ -430,10 +430,16 @@ int ray_scene_set_diff_params(ray_scene *s, const ray_diff_params *p) {
             RG_CHECK(k >= -1 && k < p->n_roughness, "material slot out of range");
             RG_CHECK(k < 0 || s->materials[m].type == (uint32_t)RAY_MAT_PRINCIPLED, "slots are for RAY_MAT_PRINCIPLED materials");
         }
+    // the slots live in the device material records: upload only when one changes
+    // (the parameter arrays themselves are read through the pointers at each render)
     for (size_t m = 0; m < s->materials.size(); m++) {
         if (s->materials[m].type != (uint32_t)RAY_MAT_PRINCIPLED) continue;
         const int32_t k = p->material_slot ? p->material_slot[m] : -1;
-        s->materials[m].textures[2] = k >= 0 ? (uint32_t)k : RAY_INVALID_INDEX;
+        const uint32_t v = k >= 0 ? (uint32_t)k : RAY_INVALID_INDEX;
+        if (s->materials[m].textures[2] != v) {
+            s->materials[m].textures[2] = v;
+            s->shade_dirty = true;
+        }
     }
     s->diff_albedo = p->albedo;
     s->diff_rough = p->roughness;
@@ -441,7 +447,6 @@ int ray_scene_set_diff_params(ray_scene *s, const ray_diff_params *p) {
     s->diff_aw = p->albedo_w;
     s->diff_ah = p->albedo_h;
     s->n_diff_rough = p->n_roughness;
-    s->shade_dirty = true;
     return RAY_OK;
 }
 

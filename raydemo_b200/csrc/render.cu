@@ -914,9 +914,11 @@ int ray_renderer_set_stream(ray_renderer *r, void *stream) {
         set_error("null renderer");
         return RAY_ERR_INVALID_ARG;
     }
+    cudaStream_t next = stream ? static_cast<cudaStream_t>(stream) : r->own_stream;
+    if (next == r->stream) return RAY_OK;
     RG_CUDA_TRY(cudaSetDevice(r->device));
     RG_CUDA_TRY(cudaStreamSynchronize(r->stream)); // work on the old stream finishes first
-    r->stream = stream ? static_cast<cudaStream_t>(stream) : r->own_stream;
+    r->stream = next;
     return RAY_OK;
 }
 
