@@ -313,8 +313,9 @@ def batch_frames(args, dev, stream, n_scenes: int = 64, samples: int = 4) -> dic
         torch.cuda.synchronize(dev)
         return {"workload": BATCH_WORKLOAD, "profiling_run": True}
 
-    def timed_batch(kernel: int, warm: int) -> float:
-        rs[0].set_kernel(kernel)  # the batch follows the first renderer's setting
+    def timed_batch(kernel: int, warm: int, sort: int = -1) -> float:
+        rs[0].set_kernel(kernel)  # the batch follows the first renderer's settings
+        rs[0].set_ray_sort(sort)
         for _ in range(warm):
             batch_pass()
         torch.cuda.synchronize(dev)
@@ -324,7 +325,8 @@ def batch_frames(args, dev, stream, n_scenes: int = 64, samples: int = 4) -> dic
         torch.cuda.synchronize(dev)
         return ev0.elapsed_time(ev1)
 
-    by_kernel = {"wavefront": round(timed_batch(1, 1), 3), "path": round(timed_batch(2, 1), 3)}
+    by_kernel = {"wavefront": round(timed_batch(1, 1, 0), 3), "wavefront_sorted": round(timed_batch(1, 1, 0x3FF), 3),
+                 "path": round(timed_batch(2, 1, 0), 3)}
     batch_ms = timed_batch(0, 7)  # the default: kernel and sort chosen by timing the first calls (2 per variant)
     info = rs[0].frame_info()
     if info.error_flags:
