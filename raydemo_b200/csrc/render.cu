@@ -380,13 +380,21 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
         ref_lights = ref_lights || J.sc.n_lights > 0;
         nee = nee || J.sc.n_area_lights > 0;
     }
-    if (nee) RG_CUDA_TRY(rb->d_shadow.ensure(std::max<size_t>(total, 1) * sizeof(ShadowRec)));
-    ShadowRec *shadow = nee ? static_cast<ShadowRec *>(rb->d_shadow.p) : nullptr;
+    ShadowQueue shadow{nullptr, nullptr, nullptr, nullptr};
+    if (nee || adj) {
+        if (!adj) RG_CUDA_TRY(rb->d_shadow.ensure(std::max<size_t>(total, 1) * sizeof(ShadowRec)));
+        RG_CUDA_TRY(rb->d_shadow_rays.ensure(std::max<size_t>(total, 1) * 2 * sizeof(float4)));
+        RG_CUDA_TRY(rb->d_shadow_job.ensure(std::max<size_t>(total, 1) * sizeof(uint32_t)));
+        shadow.recs = adj ? static_cast<void *>(adj->recs) : rb->d_shadow.p;
+        shadow.rays = static_cast<float4 *>(rb->d_shadow_rays.p);
+        shadow.job = static_cast<uint32_t *>(rb->d_shadow_job.p);
+    }
     for (int k = 0; k < 2; k++) RG_CUDA_TRY(rb->d_job[k].ensure(std::max<size_t>(total, 1) * sizeof(uint32_t)));
     uint32_t *cnt = static_cast<uint32_t *>(rb->d_counters.p);
     unsigned long long *ray_stats = reinterpret_cast<unsigned long long *>(cnt + 4);
     uint32_t *err = cnt + 3;
     uint32_t *shadow_cnt = cnt + 8;
+    shadow.count = shadow_cnt;
     float4 *rays[2] = {static_cast<float4 *>(rb->d_rays[0].p), static_cast<float4 *>(rb->d_rays[1].p)};
     RayPayload *pay[2] = {static_cast<RayPayload *>(rb->d_pay[0].p), static_cast<RayPayload *>(rb->d_pay[1].p)};
     uint32_t *job[2] = {static_cast<uint32_t *>(rb->d_job[0].p), static_cast<uint32_t *>(rb->d_job[1].p)};
@@ -415,21 +423,28 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
     tp.ray_job = job[0];
     RG_CUDA_TRY(launch_trace_closest(sv, rays[0], total, hits, obj, err, nullptr, false, st, tp));
     if (ev) RG_CUDA_TRY(cudaEventRecord(ev[2], st));
-    // shading of the rays in buffer `in` (bounce b), continuation rays to `out`, then the light samples' shadow rays
+    // shadow rays of the light samples: the persistent kernel in any-hit mode (the hits buffer is free again)
+    TraceParams tps = tp;
+    tps.any = true;
+    tps.count = shadow_cnt;
+    tps.ray_job = shadow.job;
+    // shading of the rays in buffer `in` (bounce b), continuation rays to `out`, then the light samples'
+    // shadow rays and the colour of the unblocked ones
     auto shade = [&](int b, int in, int out) -> cudaError_t {
         cudaError_t e = cudaSuccess;
         if (nee || adj) e = cudaMemsetAsync(shadow_cnt, 0, sizeof(uint32_t), st);
         if (e != cudaSuccess) return e;
-        if (adj) {
+        if (adj)
             e = launch_adjoint_shade(d_jobs, b, rays[in], pay[in], job[in], adj->state[in], hits, obj, cnt + in, total, rays[out], pay[out],
-                                     job[out], adj->state[out], cnt + out, adj->recs, shadow_cnt, adj->args, err, st);
-            if (e != cudaSuccess) return e;
-            return launch_adjoint_shadow(d_jobs, b, adj->recs, shadow_cnt, total, adj->state[out], adj->args, err, st);
-        }
-        e = launch_shade_jobs(d_jobs, sample, b, rays[in], pay[in], job[in], hits, obj, cnt + in, total, rays[out], pay[out], job[out],
-                              cnt + out, shadow, shadow_cnt, ref_lights, err, ray_stats, st);
-        if (e != cudaSuccess || !nee) return e;
-        return launch_shadow_jobs(d_jobs, sample, b, shadow, shadow_cnt, total, err, ray_stats, st);
+                                     job[out], adj->state[out], cnt + out, shadow, adj->args, err, st);
+        else
+            e = launch_shade_jobs(d_jobs, sample, b, rays[in], pay[in], job[in], hits, obj, cnt + in, total, rays[out], pay[out], job[out],
+                                  cnt + out, shadow, ref_lights, err, ray_stats, st);
+        if (e != cudaSuccess || !(nee || adj)) return e;
+        e = launch_trace_closest(sv, shadow.rays, total, hits, nullptr, err, nullptr, false, st, tps);
+        if (e != cudaSuccess) return e;
+        if (adj) return launch_adjoint_shadow_apply(d_jobs, b, shadow, hits, total, adj->state[out], adj->args, err, st);
+        return launch_shadow_apply(d_jobs, sample, b, shadow, hits, total, err, ray_stats, st);
     };
     RG_CUDA_TRY(shade(2, 0, 1));
     if (ev) RG_CUDA_TRY(cudaEventRecord(ev[3], st));

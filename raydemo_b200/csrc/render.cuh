@@ -170,6 +170,16 @@ struct ShadowRec {
 };
 static_assert(sizeof(ShadowRec) == 48, "shadow record layout");
 
+// Where a shading launch appends its light samples: the records (ShadowRec
+// or AdjShadowRec), their shadow rays (o, tmax = segment length; d) for the
+// any-hit trace, the rays' jobs, and the device count.
+struct ShadowQueue {
+    void *recs;
+    float4 *rays;
+    uint32_t *job;
+    uint32_t *count;
+};
+
 // ---- the path-replay adjoint (differentiable parameters of RAY_MAT_PRINCIPLED)
 constexpr int ADJ_MAX_SLOTS = 64; // roughness slots
 
@@ -220,12 +230,14 @@ cudaError_t launch_raygen_jobs(const FrameJob *jobs, int n_jobs, uint32_t total,
 // some job's scene has the reference's lights (traced inside the shading).
 cudaError_t launch_shade_jobs(const FrameJob *jobs, int sample, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
                               const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays, float4 *out_rays,
-                              RayPayload *out_pay, uint32_t *out_job, uint32_t *out_count, ShadowRec *shadow, uint32_t *shadow_count,
-                              bool ref_lights, uint32_t *err, unsigned long long *ray_stats, cudaStream_t st);
-// Traces the *count shadow records of a shading launch and adds the colour
-// of each unblocked one to its pixel.
-cudaError_t launch_shadow_jobs(const FrameJob *jobs, int sample, int bounce, const ShadowRec *recs, const uint32_t *count, uint32_t max_recs,
-                               uint32_t *err, unsigned long long *ray_stats, cudaStream_t st);
+                              RayPayload *out_pay, uint32_t *out_job, uint32_t *out_count, const ShadowQueue &shadow, bool ref_lights,
+                              uint32_t *err, unsigned long long *ray_stats, cudaStream_t st);
+// After the any-hit trace of a shading launch's shadow rays (hits): adds the
+// colour of each unblocked light sample to its pixel. A ray whose first hit
+// is on a non-solid triangle takes the full visibility walk through the
+// transparent layers (ComputeVisibility) instead.
+cudaError_t launch_shadow_apply(const FrameJob *jobs, int sample, int bounce, const ShadowQueue &shadow, const float4 *hits, uint32_t max_recs,
+                                uint32_t *err, unsigned long long *ray_stats, cudaStream_t st);
 // clean += (temp - clean) / iteration over every job's rect, then final = tone(clean)
 cudaError_t launch_resolve_jobs(const FrameJob *jobs, int n_jobs, uint32_t total, int sample, cudaStream_t st);
 // The whole frame of every job in one launch (ray generation, all bounces,
@@ -249,9 +261,9 @@ cudaError_t launch_diff_collect(const FrameJob *jobs, int n_jobs, uint32_t n_pix
 cudaError_t launch_adjoint_shade(const FrameJob *jobs, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
                                  const AdjState *adj_in, const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays,
                                  float4 *out_rays, RayPayload *out_pay, uint32_t *out_job, AdjState *adj_out, uint32_t *out_count,
-                                 AdjShadowRec *shadow, uint32_t *shadow_count, const AdjArgs &args, uint32_t *err, cudaStream_t st);
-cudaError_t launch_adjoint_shadow(const FrameJob *jobs, int bounce, const AdjShadowRec *recs, const uint32_t *count, uint32_t max_recs,
-                                  AdjState *adj_cont, const AdjArgs &args, uint32_t *err, cudaStream_t st);
+                                 const ShadowQueue &shadow, const AdjArgs &args, uint32_t *err, cudaStream_t st);
+cudaError_t launch_adjoint_shadow_apply(const FrameJob *jobs, int bounce, const ShadowQueue &shadow, const float4 *hits, uint32_t max_recs,
+                                        AdjState *adj_cont, const AdjArgs &args, uint32_t *err, cudaStream_t st);
 cudaError_t launch_fill(float4 *buf, size_t n, float4 v, cudaStream_t st);
 cudaError_t launch_fill_sh(SHData *buf, size_t n, cudaStream_t st);
 

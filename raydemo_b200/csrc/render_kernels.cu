@@ -293,6 +293,22 @@ struct NewRay {
     RayPayload p;
 };
 
+// The shadow ray of the segment p1 -> p2 as ComputeVisibility forms it
+// (direction p2 - p1 over its length, tmax the length); a segment of length
+// HIT_EPS or less (which is visible without a trace) gets tmax 0.
+__device__ __forceinline__ void shadow_ray(V3 p1, V3 p2, float4 &r0, float4 &r1) {
+    V3 dir = p2 - p1;
+    const float dist = length(dir);
+    dir = dir / dist;
+    if (dist > HIT_EPS) {
+        r0 = make_float4(p1.x, p1.y, p1.z, dist);
+        r1 = make_float4(dir.x, dir.y, dir.z, 0.0f);
+    } else {
+        r0 = make_float4(p1.x, p1.y, p1.z, 0.0f);
+        r1 = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+    }
+}
+
 // A RAY_MAT_PRINCIPLED vertex's light sample, traced after the shading: the
 // segment o -> p2 and the colour it adds to the pixel when nothing blocks it
 // (the path weight times the estimator). The pixel's sum takes the shading's
@@ -854,8 +870,8 @@ __global__ void __launch_bounds__(SHADE_BLOCK, REF_LIGHTS ? 3 : 4) k_shade_jobs(
                                                             const int32_t *__restrict__ obj, const uint32_t *__restrict__ in_count,
                                                             uint32_t max_rays, float4 *__restrict__ out_rays, RayPayload *__restrict__ out_pay,
                                                             uint32_t *__restrict__ out_job, uint32_t *__restrict__ out_count,
-                                                            ShadowRec *__restrict__ shadow, uint32_t *__restrict__ shadow_count,
-                                                            uint32_t *__restrict__ err_out, unsigned long long *__restrict__ ray_stats) {
+                                                            ShadowQueue shadow, uint32_t *__restrict__ err_out,
+                                                            unsigned long long *__restrict__ ray_stats) {
     __shared__ uint2 s_stack[REF_LIGHTS ? trav::SMEM_STACK * SHADE_BLOCK : 1];
     Stack<true> st;
     st.smem = s_stack + threadIdx.x;
@@ -917,7 +933,7 @@ __global__ void __launch_bounds__(SHADE_BLOCK, REF_LIGHTS ? 3 : 4) k_shade_jobs(
         if (ms) {
             uint32_t slot = 0;
             const uint32_t leader = __ffs(ms) - 1;
-            if (lane == leader) slot = atomicAdd(shadow_count, (uint32_t)__popc(ms));
+            if (lane == leader) slot = atomicAdd(shadow.count, (uint32_t)__popc(ms));
             slot = __shfl_sync(0xffffffffu, slot, leader) + __popc(ms & ((1u << lane) - 1u));
             if (sr.valid && slot < max_rays) {
                 ShadowRec rec;
@@ -927,7 +943,12 @@ __global__ void __launch_bounds__(SHADE_BLOCK, REF_LIGHTS ? 3 : 4) k_shade_jobs(
                 rec.index = sr_index;
                 rec.job = j;
                 rec.rand_index = sr_rand;
-                shadow[slot] = rec;
+                static_cast<ShadowRec *>(shadow.recs)[slot] = rec;
+                float4 q0, q1;
+                shadow_ray(sr.o, sr.p2, q0, q1);
+                shadow.rays[2ull * slot] = q0;
+                shadow.rays[2ull * slot + 1] = q1;
+                shadow.job[slot] = j;
             }
         }
         // warp-aggregated append of the continuation rays
@@ -954,27 +975,41 @@ __global__ void __launch_bounds__(SHADE_BLOCK, REF_LIGHTS ? 3 : 4) k_shade_jobs(
     }
 }
 
-// The shadow rays of a shading launch's light samples (ComputeVisibility,
-// CoreRef.cpp:1813-1896), a grid over the records; an unblocked one adds its
-// colour to the pixel, after the colour the shading added.
-__global__ void __launch_bounds__(SHADE_BLOCK) k_shadow_jobs(const FrameJob *__restrict__ jobs, int sample, int bounce,
-                                                             const ShadowRec *__restrict__ recs, const uint32_t *__restrict__ count,
-                                                             uint32_t max_recs, uint32_t *__restrict__ err_out,
-                                                             unsigned long long *__restrict__ ray_stats) {
+// Whether the light sample of record i is unblocked, from its shadow ray's
+// any-hit result: a miss is; a solid first hit is not; a first hit on a
+// non-solid triangle takes ComputeVisibility's walk through the transparent
+// layers (CoreRef.cpp:1813-1896), which decides it as the reference does.
+__device__ __forceinline__ bool sample_visible(const FrameJob &J, int iteration, int bounce, const float *o, const float *p2,
+                                               uint32_t rand_index, float4 hit, Stack<true> &st, uint32_t &err, uint32_t &nshadow) {
+    nshadow++;
+    const int prim = __float_as_int(hit.x);
+    if (prim < 0) return true;
+    if ((uint32_t)prim >= J.sc.n_tris) {
+        err |= SHADE_ERR_BAD_INDEX;
+        return false;
+    }
+    if (load_tri(J.sc, (uint32_t)prim).ci & TRI_SOLID_BIT) return false;
+    const int hi = (iteration & (HALTON_SEQ_LEN - 1)) * HALTON_COUNT + bounce * 2;
+    const int rand_hash2 = hash_i(hash_i((int)rand_index));
+    return compute_visibility(J.sc, v3(o), v3(p2), J.halton, hi, rand_hash2, st, err, nshadow) > 0.0f;
+}
+
+// Adds the colour of each unblocked light sample to its pixel, after the
+// colour the shading added (the order the path kernel and the oracle keep).
+__global__ void __launch_bounds__(SHADE_BLOCK) k_shadow_apply(const FrameJob *__restrict__ jobs, int sample, int bounce, ShadowQueue q,
+                                                              const float4 *__restrict__ hits, uint32_t max_recs,
+                                                              uint32_t *__restrict__ err_out, unsigned long long *__restrict__ ray_stats) {
     __shared__ uint2 s_stack[trav::SMEM_STACK * SHADE_BLOCK];
     Stack<true> st;
     st.smem = s_stack + threadIdx.x;
     st.sp = 0;
     uint32_t err = 0, nshadow = 0;
-    const uint32_t n = min(*count, max_recs);
+    const uint32_t n = min(*q.count, max_recs);
+    const ShadowRec *recs = static_cast<const ShadowRec *>(q.recs);
     for (uint32_t i = blockIdx.x * SHADE_BLOCK + threadIdx.x; i < n; i += gridDim.x * SHADE_BLOCK) {
         const ShadowRec rec = recs[i];
         const FrameJob &J = jobs[rec.job];
-        const int iteration = J.pi.iteration + sample;
-        const int hi = (iteration & (HALTON_SEQ_LEN - 1)) * HALTON_COUNT + bounce * 2;
-        const int rand_hash2 = hash_i(hash_i((int)rec.rand_index));
-        const float vis = compute_visibility(J.sc, v3(rec.o), v3(rec.p2), J.halton, hi, rand_hash2, st, err, nshadow);
-        if (vis > 0.0f) {
+        if (sample_visible(J, J.pi.iteration + sample, bounce, rec.o, rec.p2, rec.rand_index, hits[i], st, err, nshadow)) {
             float4 acc = J.temp[rec.index];
             acc.x += rec.c[0];
             acc.y += rec.c[1];
@@ -1033,7 +1068,7 @@ __device__ __forceinline__ void render_path(const FrameJob &J, uint32_t i, int i
                                make_float4(__int_as_float(b.prim), b.t, b.prim >= 0 ? b.u : 0.0f, b.prim >= 0 ? b.v : 0.0f), b.obj, r0, r1, pay,
                                nr, emit, sr, st, err, nshadow);
     float4 acc = make_float4(c.x, c.y, c.z, c.w);
-    // a light sample adds after the shading's colour, as k_shadow_jobs does
+    // a light sample adds after the shading's colour, as k_shadow_apply does
     if (sr.valid && compute_visibility(J.sc, sr.o, sr.p2, J.halton, (iteration & (HALTON_SEQ_LEN - 1)) * HALTON_COUNT + pi.bounce * 2,
                                        rand_hash2, st, err, nshadow) > 0.0f) {
         acc.x += sr.contrib.x;
@@ -1183,8 +1218,7 @@ __global__ void __launch_bounds__(SHADE_BLOCK, 3) k_adjoint_shade(const FrameJob
                                                                   const uint32_t *__restrict__ in_count, uint32_t max_rays,
                                                                   float4 *__restrict__ out_rays, RayPayload *__restrict__ out_pay,
                                                                   uint32_t *__restrict__ out_job, AdjState *__restrict__ adj_out,
-                                                                  uint32_t *__restrict__ out_count, AdjShadowRec *__restrict__ shadow,
-                                                                  uint32_t *__restrict__ shadow_count, AdjArgs args,
+                                                                  uint32_t *__restrict__ out_count, ShadowQueue shadow, AdjArgs args,
                                                                   uint32_t *__restrict__ err_out) {
     __shared__ float s_gr[ADJ_MAX_SLOTS];
     __shared__ uint2 s_stack[1];
@@ -1316,11 +1350,16 @@ __global__ void __launch_bounds__(SHADE_BLOCK, 3) k_adjoint_shade(const FrameJob
         if (ml) {
             uint32_t slot = 0;
             const uint32_t leader = __ffs(ml) - 1;
-            if (lane == leader) slot = atomicAdd(shadow_count, (uint32_t)__popc(ml));
+            if (lane == leader) slot = atomicAdd(shadow.count, (uint32_t)__popc(ml));
             slot = __shfl_sync(0xffffffffu, slot, leader) + __popc(ml & ((1u << lane) - 1u));
             if (light && slot < max_rays) {
                 rec.cont = cont;
-                shadow[slot] = rec;
+                static_cast<AdjShadowRec *>(shadow.recs)[slot] = rec;
+                float4 q0, q1;
+                shadow_ray(v3(rec.o), v3(rec.p2), q0, q1);
+                shadow.rays[2ull * slot] = q0;
+                shadow.rays[2ull * slot + 1] = q1;
+                shadow.job[slot] = j;
             }
         }
     }
@@ -1328,10 +1367,10 @@ __global__ void __launch_bounds__(SHADE_BLOCK, 3) k_adjoint_shade(const FrameJob
     flush_slots(s_gr, args.grad_rough, n_slots);
 }
 
-__global__ void __launch_bounds__(SHADE_BLOCK) k_adjoint_shadow(const FrameJob *__restrict__ jobs, int bounce,
-                                                                const AdjShadowRec *__restrict__ recs, const uint32_t *__restrict__ count,
-                                                                uint32_t max_recs, AdjState *__restrict__ adj_cont, AdjArgs args,
-                                                                uint32_t *__restrict__ err_out) {
+__global__ void __launch_bounds__(SHADE_BLOCK) k_adjoint_shadow_apply(const FrameJob *__restrict__ jobs, int bounce, ShadowQueue q,
+                                                                      const float4 *__restrict__ hits, uint32_t max_recs,
+                                                                      AdjState *__restrict__ adj_cont, AdjArgs args,
+                                                                      uint32_t *__restrict__ err_out) {
     __shared__ float s_gr[ADJ_MAX_SLOTS];
     __shared__ uint2 s_stack[trav::SMEM_STACK * SHADE_BLOCK];
     for (int k = threadIdx.x; k < ADJ_MAX_SLOTS; k += blockDim.x) s_gr[k] = 0.0f;
@@ -1340,14 +1379,13 @@ __global__ void __launch_bounds__(SHADE_BLOCK) k_adjoint_shadow(const FrameJob *
     st.smem = s_stack + threadIdx.x;
     st.sp = 0;
     uint32_t err = 0, nshadow = 0;
-    const uint32_t n = min(*count, max_recs);
+    const uint32_t n = min(*q.count, max_recs);
     const uint32_t n_slots = jobs[0].sc.n_diff_rough < (uint32_t)ADJ_MAX_SLOTS ? jobs[0].sc.n_diff_rough : (uint32_t)ADJ_MAX_SLOTS;
+    const AdjShadowRec *recs = static_cast<const AdjShadowRec *>(q.recs);
     for (uint32_t i = blockIdx.x * SHADE_BLOCK + threadIdx.x; i < n; i += gridDim.x * SHADE_BLOCK) {
         const AdjShadowRec rec = recs[i];
         const FrameJob &J = jobs[rec.job];
-        const int hi = (J.pi.iteration & (HALTON_SEQ_LEN - 1)) * HALTON_COUNT + bounce * 2;
-        const int rand_hash2 = hash_i(hash_i((int)rec.rand_index));
-        if (compute_visibility(J.sc, v3(rec.o), v3(rec.p2), J.halton, hi, rand_hash2, st, err, nshadow) > 0.0f) {
+        if (sample_visible(J, J.pi.iteration, bounce, rec.o, rec.p2, rec.rand_index, hits[i], st, err, nshadow)) {
             if (rec.slot < n_slots) {
                 scatter_albedo(J.sc, args.grad_albedo, rec.u, rec.v, rec.ga[0], rec.ga[1], rec.ga[2]);
                 if (rec.gr != 0.0f) atomicAdd(&s_gr[rec.slot], rec.gr);
@@ -1418,8 +1456,8 @@ static int resident_blocks(K kernel, int fallback_per_sm) {
 
 cudaError_t launch_shade_jobs(const FrameJob *jobs, int sample, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
                               const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays, float4 *out_rays,
-                              RayPayload *out_pay, uint32_t *out_job, uint32_t *out_count, ShadowRec *shadow, uint32_t *shadow_count,
-                              bool ref_lights, uint32_t *err, unsigned long long *ray_stats, cudaStream_t st) {
+                              RayPayload *out_pay, uint32_t *out_job, uint32_t *out_count, const ShadowQueue &shadow, bool ref_lights,
+                              uint32_t *err, unsigned long long *ray_stats, cudaStream_t st) {
     static int resident[2] = {0, 0};
     int &res = resident[ref_lights ? 1 : 0];
     if (res == 0) res = ref_lights ? resident_blocks(k_shade_jobs<false, true>, 4) : resident_blocks(k_shade_jobs<false, false>, 4);
@@ -1427,7 +1465,7 @@ cudaError_t launch_shade_jobs(const FrameJob *jobs, int sample, int bounce, cons
     const uint32_t blocks = need < (uint32_t)res ? (need > 0 ? need : 1) : (uint32_t)res;
 #define RG_SHADE(P, R)                                                                                                                     \
     k_shade_jobs<P, R><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, sample, bounce, rays, pay, ray_job, hits, obj, in_count, max_rays, out_rays, \
-                                                       out_pay, out_job, out_count, shadow, shadow_count, err, ray_stats)
+                                                       out_pay, out_job, out_count, shadow, err, ray_stats)
     if (bounce == 2) {
         if (ref_lights) RG_SHADE(true, true);
         else RG_SHADE(true, false);
@@ -1439,14 +1477,14 @@ cudaError_t launch_shade_jobs(const FrameJob *jobs, int sample, int bounce, cons
     return cudaGetLastError();
 }
 
-cudaError_t launch_shadow_jobs(const FrameJob *jobs, int sample, int bounce, const ShadowRec *recs, const uint32_t *count, uint32_t max_recs,
-                               uint32_t *err, unsigned long long *ray_stats, cudaStream_t st) {
+cudaError_t launch_shadow_apply(const FrameJob *jobs, int sample, int bounce, const ShadowQueue &shadow, const float4 *hits, uint32_t max_recs,
+                                uint32_t *err, unsigned long long *ray_stats, cudaStream_t st) {
     static int resident = 0;
-    if (resident == 0) resident = resident_blocks(k_shadow_jobs, 4);
+    if (resident == 0) resident = resident_blocks(k_shadow_apply, 4);
     if (max_recs == 0) return cudaSuccess;
     const uint32_t need = (max_recs + SHADE_BLOCK - 1) / SHADE_BLOCK;
     const uint32_t blocks = need < (uint32_t)resident ? need : (uint32_t)resident;
-    k_shadow_jobs<<<blocks, SHADE_BLOCK, 0, st>>>(jobs, sample, bounce, recs, count, max_recs, err, ray_stats);
+    k_shadow_apply<<<blocks, SHADE_BLOCK, 0, st>>>(jobs, sample, bounce, shadow, hits, max_recs, err, ray_stats);
     return cudaGetLastError();
 }
 
@@ -1482,28 +1520,28 @@ cudaError_t launch_diff_collect(const FrameJob *jobs, int n_jobs, uint32_t n_pix
 cudaError_t launch_adjoint_shade(const FrameJob *jobs, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
                                  const AdjState *adj_in, const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays,
                                  float4 *out_rays, RayPayload *out_pay, uint32_t *out_job, AdjState *adj_out, uint32_t *out_count,
-                                 AdjShadowRec *shadow, uint32_t *shadow_count, const AdjArgs &args, uint32_t *err, cudaStream_t st) {
+                                 const ShadowQueue &shadow, const AdjArgs &args, uint32_t *err, cudaStream_t st) {
     static int resident = 0;
     if (resident == 0) resident = resident_blocks(k_adjoint_shade<false>, 3);
     const uint32_t need = (max_rays + SHADE_BLOCK - 1) / SHADE_BLOCK;
     const uint32_t blocks = need < (uint32_t)resident ? (need > 0 ? need : 1) : (uint32_t)resident;
     if (bounce == 2)
         k_adjoint_shade<true><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, bounce, rays, pay, ray_job, adj_in, hits, obj, in_count, max_rays, out_rays,
-                                                              out_pay, out_job, adj_out, out_count, shadow, shadow_count, args, err);
+                                                              out_pay, out_job, adj_out, out_count, shadow, args, err);
     else
         k_adjoint_shade<false><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, bounce, rays, pay, ray_job, adj_in, hits, obj, in_count, max_rays,
-                                                               out_rays, out_pay, out_job, adj_out, out_count, shadow, shadow_count, args, err);
+                                                               out_rays, out_pay, out_job, adj_out, out_count, shadow, args, err);
     return cudaGetLastError();
 }
 
-cudaError_t launch_adjoint_shadow(const FrameJob *jobs, int bounce, const AdjShadowRec *recs, const uint32_t *count, uint32_t max_recs,
-                                  AdjState *adj_cont, const AdjArgs &args, uint32_t *err, cudaStream_t st) {
+cudaError_t launch_adjoint_shadow_apply(const FrameJob *jobs, int bounce, const ShadowQueue &shadow, const float4 *hits, uint32_t max_recs,
+                                        AdjState *adj_cont, const AdjArgs &args, uint32_t *err, cudaStream_t st) {
     static int resident = 0;
-    if (resident == 0) resident = resident_blocks(k_adjoint_shadow, 3);
+    if (resident == 0) resident = resident_blocks(k_adjoint_shadow_apply, 3);
     if (max_recs == 0) return cudaSuccess;
     const uint32_t need = (max_recs + SHADE_BLOCK - 1) / SHADE_BLOCK;
     const uint32_t blocks = need < (uint32_t)resident ? need : (uint32_t)resident;
-    k_adjoint_shadow<<<blocks, SHADE_BLOCK, 0, st>>>(jobs, bounce, recs, count, max_recs, adj_cont, args, err);
+    k_adjoint_shadow_apply<<<blocks, SHADE_BLOCK, 0, st>>>(jobs, bounce, shadow, hits, max_recs, adj_cont, args, err);
     return cudaGetLastError();
 }
 

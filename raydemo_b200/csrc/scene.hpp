@@ -135,7 +135,7 @@ struct ray_renderer {
     // instance ids, light samples waiting for their shadow rays; counters
     // [0..1] ray counts, [2] persistent-trace work counter, [3] errors,
     // [4..7] rays and shadow segments traced (two uint64), [8] light samples
-    rg::DeviceBuf d_rays[2], d_pay[2], d_job[2], d_hits, d_obj, d_counters, d_shadow;
+    rg::DeviceBuf d_rays[2], d_pay[2], d_job[2], d_hits, d_obj, d_counters, d_shadow, d_shadow_rays, d_shadow_job;
     // differentiable form: the samples' sample buffers, the adjoint's per-ray state and light samples
     rg::DeviceBuf d_diff_temp, d_adj[2], d_adj_shadow;
     rg::DeviceBuf d_halton, d_perms;

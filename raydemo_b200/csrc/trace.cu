@@ -88,7 +88,9 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
 // their ray), then one node step plus the triangles it hit.
 // MULTI: rays of several scenes in one launch; ray i belongs to the scene
 // whose SceneView is at views + ray_job[i] * view_stride.
-template <bool COUNT, bool DEEP, bool MULTI = false>
+// ANY: shadow rays -- a ray ends at its first accepted hit on a solid
+// triangle (Traverse_MacroTree_WithStack_AnyHit, CoreRef.cpp:1224-1368).
+template <bool COUNT, bool DEEP, bool MULTI = false, bool ANY = false>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, const float4 *__restrict__ rays, uint32_t n,
                                                                   float4 *__restrict__ hits, int32_t *__restrict__ obj_out,
                                                                   uint32_t *__restrict__ err_out, unsigned long long *__restrict__ counters,
@@ -187,13 +189,26 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
         }
         if (!ok) {
             in_mesh = false;
-            mi = sv.n_inst; // abandon the ray; the error flag reports it
+            mi = 0xffffffffu; // abandon the ray; the error flag reports it
             continue;
         }
+        bool stop = false;
         while (tg_bits) {
             const uint32_t k = __ffs(tg_bits) - 1;
             tg_bits &= tg_bits - 1;
-            tri_test<COUNT>(mr, r, tg_base + k, best, err, ntri);
+            if (ANY) {
+                if (tri_test<COUNT, true>(mr, r, tg_base + k, best, err, ntri)) {
+                    stop = true;
+                    tg_bits = 0;
+                }
+            } else {
+                tri_test<COUNT>(mr, r, tg_base + k, best, err, ntri);
+            }
+        }
+        if (ANY && stop) { // a solid triangle blocks the ray: no further instance
+            in_mesh = false;
+            mi = 0xffffffffu;
+            continue;
         }
         if (ng_bits <= 0x00FFFFFFu) {
             if (st.sp == 0) {
@@ -213,7 +228,7 @@ int g_persistent_blocks[2] = {0, 0};
 template <bool DEEP>
 cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
                         unsigned long long *counters, bool count, cudaStream_t st, const TraceParams &tp) {
-    if (!tp.persistent && !tp.views) {
+    if (!tp.persistent && !tp.views && !tp.any) {
         const uint32_t grid = (n + TRACE_BLOCK - 1) / TRACE_BLOCK;
         if (count)
             k_trace_closest<true, DEEP><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.count);
@@ -233,6 +248,15 @@ cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, flo
     }
     cudaError_t e = cudaMemsetAsync(tp.next_ray, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
+    if (tp.any) { // shadow rays (no counting variant)
+        if (tp.views)
+            k_trace_persistent<false, DEEP, true, true><<<blocks, TRACE_BLOCK, 0, st>>>(
+                sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min, tp.count, tp.views, tp.view_stride, tp.ray_job);
+        else
+            k_trace_persistent<false, DEEP, false, true><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray,
+                                                                                        tp.refill_min, tp.count);
+        return cudaGetLastError();
+    }
     if (tp.views) { // rays of several scenes (no counting variant)
         k_trace_persistent<false, DEEP, true><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray,
                                                                                tp.refill_min, tp.count, tp.views, tp.view_stride, tp.ray_job);

@@ -30,6 +30,10 @@ struct TraceParams {
     const uint8_t *views = nullptr;
     uint32_t view_stride = 0;
     const uint32_t *ray_job = nullptr;
+    // shadow rays (persistent kernel): a ray ends at its first accepted hit on
+    // a solid triangle (that hit is returned); without one, the closest hit
+    // on a non-solid triangle or a miss
+    bool any = false;
 };
 
 // rays: n x 8 floats (ox, oy, oz, tmax, dx, dy, dz, unused).
