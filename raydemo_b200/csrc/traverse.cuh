@@ -13,9 +13,21 @@ constexpr int SMEM_STACK = 24; // entries per thread in shared memory
 constexpr int LMEM_STACK = 40; // further entries in a local array (DEEP instances only)
 constexpr uint32_t NO_RAY = 0xffffffffu;
 
-__device__ __forceinline__ float byte_to_float(uint32_t word, uint32_t sel) {
-    // 0x4B0000bb is 2^23 + bb as a float; subtracting 2^23 leaves bb exactly.
-    return __fsub_rn(__uint_as_float(__byte_perm(word, 0x4B000000u, sel)), 8388608.0f);
+// Three-input max / min (sm_100). NaN inputs are dropped, as fmaxf/fminf drop them.
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// Byte k of word as the float 1 + byte * 2^-15 (0x3F80bb00): exact, one permute.
+__device__ __forceinline__ float byte_to_unit(uint32_t word, uint32_t k) {
+    return __uint_as_float(__byte_perm(word, 0x3F800000u, 0x7604u | (k << 4)));
 }
 
 // The reference's slab test, exactly (bbox_test, CoreRef.cpp:64-86).
@@ -163,11 +175,16 @@ __device__ __forceinline__ bool node_step(const MeshRef &mr, const LocalRay &r, 
     if (COUNT) nvis++;
     const uint32_t imask = w0.w >> 24;
     // Slab parameter of plane q on one axis: t(q) = q * A + B with
-    // A = 2^e * inv_d (exact: a power-of-two scaling) and B = (p - o) * inv_d,
-    // one FMA per plane. Its rounding error is below 2u(|B| + 256|A|)
-    // (u = 2^-24); the slack 2^-21 (|B| + 256|A|) moves the near planes
-    // down and the far planes up by more than that, so the test accepts
-    // every box that the exact slab test on the decoded box accepts.
+    // A = 2^e * inv_d (exact: a power-of-two scaling) and B = (p - o) * inv_d.
+    // It is evaluated as one FMA on the byte read as the float
+    // v = 1 + q * 2^-15: t = v * (2^15 A) + (B - 2^15 A), where 2^15 A is
+    // exact and v * 2^15 A = 2^15 A + q A exactly inside the FMA. Rounding
+    // B - 2^15 A, then -/+ slack, then the FMA's result errs by less than
+    // 3u(|B| + 33024|A|) (u = 2^-24); the slack 2^-21 (|B| + 33024|A|)
+    // moves the near planes down and the far planes up by more than that,
+    // so the test accepts every box that the exact slab test on the decoded
+    // box accepts. (An overflowing 2^15 A gives NaN planes: that axis is
+    // left unbounded, still conservative.)
     float A[3], Bn[3], Bf[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
@@ -175,11 +192,13 @@ __device__ __forceinline__ bool node_step(const MeshRef &mr, const LocalRay &r, 
         const float sc = __uint_as_float(((w0.w >> (8 * a)) & 0xFFu) << 23);
         const float inv = a == 0 ? r.ix : (a == 1 ? r.iy : r.iz);
         const float o = a == 0 ? r.ox : (a == 1 ? r.oy : r.oz);
-        A[a] = __fmul_rn(sc, inv);
+        const float Aa = __fmul_rn(sc, inv);
         const float B = __fmul_rn(__fsub_rn(p, o), inv);
-        const float slack = __fmul_rn(__fmaf_rn(fabsf(A[a]), 256.0f, fabsf(B)), 4.76837158203125e-07f);
-        Bn[a] = __fsub_rn(B, slack);
-        Bf[a] = __fadd_rn(B, slack);
+        const float slack = __fmul_rn(__fmaf_rn(fabsf(Aa), 33024.0f, fabsf(B)), 4.76837158203125e-07f);
+        const float B0 = __fmaf_rn(-32768.0f, Aa, B);
+        A[a] = __fmul_rn(Aa, 32768.0f);
+        Bn[a] = __fsub_rn(B0, slack);
+        Bf[a] = __fadd_rn(B0, slack);
     }
     // Near/far plane words by direction sign, so that a NaN slab value
     // (origin on a plane of a box the ray runs parallel to) leaves that axis
@@ -193,16 +212,18 @@ __device__ __forceinline__ bool node_step(const MeshRef &mr, const LocalRay &r, 
 #pragma unroll
     for (int c = 0; c < 8; c++) {
         const uint32_t meta = ((c < 4 ? w1.z : w1.w) >> (8 * (c & 3))) & 0xFFu;
-        const uint32_t sel = 0x7540u | (uint32_t)(c & 3);
-        const float tnx = __fmaf_rn(byte_to_float(c < 4 ? nxa : nxb, sel), A[0], Bn[0]);
-        const float tfx = __fmaf_rn(byte_to_float(c < 4 ? fxa : fxb, sel), A[0], Bf[0]);
-        const float tny = __fmaf_rn(byte_to_float(c < 4 ? nya : nyb, sel), A[1], Bn[1]);
-        const float tfy = __fmaf_rn(byte_to_float(c < 4 ? fya : fyb, sel), A[1], Bf[1]);
-        const float tnz = __fmaf_rn(byte_to_float(c < 4 ? nza : nzb, sel), A[2], Bn[2]);
-        const float tfz = __fmaf_rn(byte_to_float(c < 4 ? fza : fzb, sel), A[2], Bf[2]);
-        const float tmin = fmaxf(fmaxf(tnx, tny), tnz);
-        const float tmax = fminf(fminf(tfx, tfy), tfz);
-        if (meta != 0 && tmin <= tmax && tmin <= best_t && tmax >= 0.0f) {
+        const uint32_t k = (uint32_t)(c & 3);
+        const float tnx = __fmaf_rn(byte_to_unit(c < 4 ? nxa : nxb, k), A[0], Bn[0]);
+        const float tfx = __fmaf_rn(byte_to_unit(c < 4 ? fxa : fxb, k), A[0], Bf[0]);
+        const float tny = __fmaf_rn(byte_to_unit(c < 4 ? nya : nyb, k), A[1], Bn[1]);
+        const float tfy = __fmaf_rn(byte_to_unit(c < 4 ? fya : fyb, k), A[1], Bf[1]);
+        const float tnz = __fmaf_rn(byte_to_unit(c < 4 ? nza : nzb, k), A[2], Bn[2]);
+        const float tfz = __fmaf_rn(byte_to_unit(c < 4 ? fza : fzb, k), A[2], Bf[2]);
+        // [max(near planes, 0), min(far planes, best_t)] non-empty: the slab
+        // test with the ray's interval folded in (best_t >= 0)
+        const float tmin = max3f(tnx, tny, fmaxf(tnz, 0.0f));
+        const float tmax = min3f(tfx, tfy, fminf(tfz, best_t));
+        if (tmin <= tmax) { // an empty slot has meta 0 and adds nothing
             uint32_t bit = meta & 31u;
             if (bit >= 24u) bit ^= r.oct;
             hitmask |= (meta >> 5) << bit;
