@@ -208,10 +208,9 @@ __device__ __forceinline__ bool node_step(const MeshRef &mr, const LocalRay &r, 
     const uint32_t nxa = nx ? w3.z : w2.x, nxb = nx ? w3.w : w2.y, fxa = nx ? w2.x : w3.z, fxb = nx ? w2.y : w3.w;
     const uint32_t nya = ny ? w4.x : w2.z, nyb = ny ? w4.y : w2.w, fya = ny ? w2.z : w4.x, fyb = ny ? w2.w : w4.y;
     const uint32_t nza = nz ? w4.z : w3.x, nzb = nz ? w4.w : w3.y, fza = nz ? w3.x : w4.z, fzb = nz ? w3.y : w4.w;
-    uint32_t hitmask = 0;
+    uint32_t hit8 = 0; // slots whose box the ray enters
 #pragma unroll
     for (int c = 0; c < 8; c++) {
-        const uint32_t meta = ((c < 4 ? w1.z : w1.w) >> (8 * (c & 3))) & 0xFFu;
         const uint32_t k = (uint32_t)(c & 3);
         const float tnx = __fmaf_rn(byte_to_unit(c < 4 ? nxa : nxb, k), A[0], Bn[0]);
         const float tfx = __fmaf_rn(byte_to_unit(c < 4 ? fxa : fxb, k), A[0], Bf[0]);
@@ -223,11 +222,20 @@ __device__ __forceinline__ bool node_step(const MeshRef &mr, const LocalRay &r, 
         // test with the ray's interval folded in (best_t >= 0)
         const float tmin = max3f(tnx, tny, fmaxf(tnz, 0.0f));
         const float tmax = min3f(tfx, tfy, fminf(tfz, best_t));
-        if (tmin <= tmax) { // an empty slot has meta 0 and adds nothing
-            uint32_t bit = meta & 31u;
-            if (bit >= 24u) bit ^= r.oct;
-            hitmask |= (meta >> 5) << bit;
-        }
+        if (tmin <= tmax) hit8 |= 1u << c;
+    }
+    // internal children: bit 24 + (slot ^ octant), so that the node group
+    // is taken in the ray's octant order
+    uint32_t inner = hit8 & imask;
+    if (r.oct & 1u) inner = ((inner & 0x55u) << 1) | ((inner >> 1) & 0x55u);
+    if (r.oct & 2u) inner = ((inner & 0x33u) << 2) | ((inner >> 2) & 0x33u);
+    if (r.oct & 4u) inner = ((inner & 0x0Fu) << 4) | ((inner >> 4) & 0x0Fu);
+    uint32_t hitmask = inner << 24;
+    // leaf children: their triangle bits (an empty slot has meta 0 and adds nothing)
+    for (uint32_t lv = hit8 & ~imask; lv; lv &= lv - 1u) {
+        const uint32_t sl = __ffs(lv) - 1u;
+        const uint32_t meta = ((sl < 4u ? w1.z : w1.w) >> (8u * (sl & 3u))) & 0xFFu;
+        hitmask |= (meta >> 5) << (meta & 31u);
     }
     ng_base = w1.x;
     ng_bits = (hitmask & 0xFF000000u) | imask;
