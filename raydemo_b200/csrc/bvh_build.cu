@@ -10,10 +10,15 @@
 //   5. k_karras      binary radix tree over the sorted keys (Karras 2012,
 //                    duplicate keys split by index)
 //   6. k_bottom_up   node boxes, leaves to root with arrival counters
-//   7. k_collapse    level by level: each wide node greedily opens its
-//                    largest-area binary children until it has 8, children
-//                    with <= 3 triangles become leaves, the others wide nodes
-//                    of the next level; children are assigned to the 8 slots
+//   7. k_wide_cost   bottom-up SAH cost of every binary subtree written as
+//                    1..8 slots of a wide node (the dynamic programme of
+//                    Ylitie, Karras and Laine 2017): a slot is a leaf (<= 3
+//                    triangles) or a wide node, or the subtree is opened and
+//                    its two children share the slots
+//   8. k_collapse    level by level: each wide node takes the slots the
+//                    programme chose for its binary node, children with
+//                    <= 3 triangles become leaves, the others wide nodes of
+//                    the next level; children are assigned to the 8 slots
 //                    by octant so that a ray visits them roughly front to
 //                    back, and their boxes are quantised to 8 bits.
 #include <algorithm>
@@ -222,6 +227,86 @@ __global__ void k_bottom_up(const float *__restrict__ aabb, const uint32_t *__re
     }
 }
 
+// SAH weights of the cost programme: a wide node's box test and fetch, and one triangle test.
+constexpr float SAH_NODE = 1.0f, SAH_TRI = 1.2f;
+
+__device__ __forceinline__ float box_area(const float lo[3], const float hi[3]) {
+    const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// C(c, j): the cost of binary subtree c in at most j slots (a single triangle: a leaf).
+__device__ __forceinline__ float slot_cost(uint32_t c, int j, const float *__restrict__ aabb, const uint32_t *__restrict__ sorted,
+                                           const float *cost) {
+    if (c & LEAF) {
+        const float *b = aabb + 6ull * sorted[c & ~LEAF];
+        const float lo[3] = {b[0], b[1], b[2]}, hi[3] = {b[3], b[4], b[5]};
+        return box_area(lo, hi) * SAH_TRI;
+    }
+    return __ldcg(cost + 8ull * c + (j - 1));
+}
+
+// Bottom-up over the binary tree (arrival counters, after k_bottom_up): for
+// every internal node, C(node, j) for j = 1..8 and its choice: j = 1 a leaf
+// (<= LEAF_MAX_TRIS triangles) or a wide node (its box's area times
+// SAH_NODE plus the best use of 8 slots by its children); j >= 2 the better
+// of one slot and the best split of the j slots between the two children
+// (dec = the left child's share, 0 for one slot). open_k: the best split of
+// 8 slots when the node is opened as a wide node.
+__global__ void k_wide_cost(const float *__restrict__ aabb, const uint32_t *__restrict__ sorted, int n, const uint32_t *__restrict__ left,
+                            const uint32_t *__restrict__ right, const uint32_t *__restrict__ parent, const uint32_t *__restrict__ first,
+                            const uint32_t *__restrict__ last, const float *__restrict__ nb, uint32_t *flags, float *cost,
+                            uint8_t *dec, uint8_t *open_k) {
+    const int j0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j0 >= n) return;
+    uint32_t node = parent[n - 1 + j0];
+    for (int climb = 0; climb < n; climb++) {
+        __threadfence();
+        if (atomicAdd(&flags[node], 1u) == 0) return; // the sibling subtree is not done yet
+        const uint32_t l = left[node], r = right[node];
+        float cl[8], cr[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            cl[k] = slot_cost(l, k + 1, aabb, sorted, cost);
+            cr[k] = slot_cost(r, k + 1, aabb, sorted, cost);
+        }
+        float lo[3], hi[3];
+        for (int k = 0; k < 3; k++) {
+            lo[k] = __ldcg(nb + 6ull * node + k);
+            hi[k] = __ldcg(nb + 6ull * node + 3 + k);
+        }
+        const float area = box_area(lo, hi);
+        const uint32_t cnt = last[node] - first[node] + 1u;
+        float dist[9];
+        uint8_t dk[9];
+        for (int j = 2; j <= 8; j++) {
+            float best = INFINITY;
+            uint8_t bk = 1;
+            for (int k = 1; k < j; k++) {
+                const float v = cl[k - 1] + cr[j - k - 1];
+                if (v < best) {
+                    best = v;
+                    bk = (uint8_t)k;
+                }
+            }
+            dist[j] = best;
+            dk[j] = bk;
+        }
+        const bool as_leaf = cnt <= (uint32_t)LEAF_MAX_TRIS;
+        const float c1 = as_leaf ? area * (float)cnt * SAH_TRI : area * SAH_NODE + dist[8];
+        __stcg(cost + 8ull * node, c1);
+        dec[8ull * node] = as_leaf ? 0 : 1;
+        for (int j = 2; j <= 8; j++) {
+            const bool split = dist[j] < c1;
+            __stcg(cost + 8ull * node + (j - 1), split ? dist[j] : c1);
+            dec[8ull * node + (j - 1)] = split ? dk[j] : 0;
+        }
+        open_k[node] = dk[8];
+        if (node == 0) return;
+        node = parent[node];
+    }
+}
+
 struct QItem {
     uint32_t bin, wide, depth;
 };
@@ -233,8 +318,8 @@ __device__ __forceinline__ uint32_t bin_count(uint32_t c, const uint32_t *first,
 __global__ void k_collapse(const QItem *__restrict__ in, uint32_t n_in, QItem *__restrict__ out, uint32_t *__restrict__ counters,
                            const float *__restrict__ aabb, const uint32_t *__restrict__ sorted, const TriRec *__restrict__ tris_ref,
                            const uint32_t *__restrict__ left, const uint32_t *__restrict__ right, const uint32_t *__restrict__ first,
-                           const uint32_t *__restrict__ last, const float *__restrict__ nb, WideNode *__restrict__ nodes,
-                           TriRec *__restrict__ leaf_tris) {
+                           const uint32_t *__restrict__ last, const float *__restrict__ nb, const uint8_t *__restrict__ dec,
+                           const uint8_t *__restrict__ open_k, WideNode *__restrict__ nodes, TriRec *__restrict__ leaf_tris) {
     // counters: [0] wide nodes allocated, [1] leaf triangles allocated,
     //           [2] items written to `out`, [3] maximum depth
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -246,25 +331,30 @@ __global__ void k_collapse(const QItem *__restrict__ in, uint32_t n_in, QItem *_
         c[0] = it.bin;
         nc = 1;
     } else {
-        c[0] = left[it.bin];
-        c[1] = right[it.bin];
-        nc = 2;
-    }
-    while (nc < 8) {
-        int best = -1;
-        float best_area = -1.0f;
-        for (int k = 0; k < nc; k++) {
-            if (c[k] & LEAF) continue;
-            float lo[3], hi[3];
-            child_box(c[k], aabb, sorted, nb, lo, hi);
-            const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
-            const float area = dx * dy + dy * dz + dz * dx;
-            if (area > best_area) { best_area = area; best = k; }
+        // the slots the cost programme chose: open it.bin into 8 slots, then
+        // follow each subtree's choice for its share of them
+        uint32_t sn[16];
+        int sj[16], sp = 0;
+        const int k0 = min(max((int)open_k[it.bin], 1), 7);
+        sn[sp] = right[it.bin];
+        sj[sp++] = 8 - k0;
+        sn[sp] = left[it.bin];
+        sj[sp++] = k0;
+        nc = 0;
+        while (sp > 0 && nc < 8) {
+            sp--;
+            const uint32_t m = sn[sp];
+            const int j = sj[sp];
+            const int k = (m & LEAF) || j <= 1 ? 0 : (int)dec[8ull * m + (j - 1)];
+            if (k <= 0 || k >= j || sp + 2 > 16) {
+                c[nc++] = m;
+            } else {
+                sn[sp] = right[m];
+                sj[sp++] = j - k;
+                sn[sp] = left[m];
+                sj[sp++] = k;
+            }
         }
-        if (best < 0) break;
-        const uint32_t b = c[best];
-        c[best] = left[b];
-        c[nc++] = right[b];
     }
     float clo[8][3], chi[8][3];
     float nlo[3] = {INFINITY, INFINITY, INFINITY}, nhi[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -417,7 +507,8 @@ int build_mesh_bvh(const TriRec *tris_ref, const float *aabb, uint32_t n, MeshBv
     TmpAllocs tmp;
     uint64_t *keys;
     uint32_t *vals, *bounds, *left, *right, *parent, *first, *last, *flags, *counters;
-    float *nb;
+    float *nb, *cost;
+    uint8_t *dec, *open_k;
     QItem *qa, *qb;
     void *scratch;
     const size_t ni = n > 1 ? n - 1 : 1;
@@ -432,6 +523,9 @@ int build_mesh_bvh(const TriRec *tris_ref, const float *aabb, uint32_t n, MeshBv
     RG_CUDA_TRY(tmp.get(&flags, ni));
     RG_CUDA_TRY(tmp.get(&counters, 4));
     RG_CUDA_TRY(tmp.get(&nb, 6 * ni));
+    RG_CUDA_TRY(tmp.get(&cost, 8 * ni));
+    RG_CUDA_TRY(tmp.get(&dec, 8 * ni));
+    RG_CUDA_TRY(tmp.get(&open_k, ni));
     RG_CUDA_TRY(tmp.get(&qa, n));
     RG_CUDA_TRY(tmp.get(&qb, n));
     RG_CUDA_TRY(tmp.get(reinterpret_cast<char **>(&scratch), radix_sort_scratch_bytes(n, 8)));
@@ -446,6 +540,9 @@ int build_mesh_bvh(const TriRec *tris_ref, const float *aabb, uint32_t n, MeshBv
         RG_CUDA_TRY(cudaMemsetAsync(flags, 0, ni * sizeof(uint32_t), st));
         k_karras<<<(uint32_t)((ni + 255) / 256), 256, 0, st>>>(keys, (int)n, left, right, parent, first, last);
         k_bottom_up<<<(n + 255) / 256, 256, 0, st>>>(aabb, vals, (int)n, left, right, parent, nb, flags);
+        RG_CUDA_TRY(cudaGetLastError());
+        RG_CUDA_TRY(cudaMemsetAsync(flags, 0, ni * sizeof(uint32_t), st));
+        k_wide_cost<<<(n + 255) / 256, 256, 0, st>>>(aabb, vals, (int)n, left, right, parent, first, last, nb, flags, cost, dec, open_k);
         RG_CUDA_TRY(cudaGetLastError());
         root_bin = 0;
     }
@@ -463,8 +560,8 @@ int build_mesh_bvh(const TriRec *tris_ref, const float *aabb, uint32_t n, MeshBv
             return RAY_ERR_CUDA;
         }
         RG_CUDA_TRY(cudaMemsetAsync(counters + 2, 0, sizeof(uint32_t), st));
-        k_collapse<<<(n_in + 127) / 128, 128, 0, st>>>(qa, n_in, qb, counters, aabb, vals, tris_ref, left, right, first, last, nb,
-                                                      out.nodes, out.leaf_tris);
+        k_collapse<<<(n_in + 127) / 128, 128, 0, st>>>(qa, n_in, qb, counters, aabb, vals, tris_ref, left, right, first, last, nb, dec,
+                                                      open_k, out.nodes, out.leaf_tris);
         RG_CUDA_TRY(cudaGetLastError());
         RG_CUDA_TRY(cudaMemcpyAsync(&n_in, counters + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         RG_CUDA_TRY(cudaStreamSynchronize(st));
