@@ -29,10 +29,12 @@ struct LightRec {
 static_assert(sizeof(LightRec) == 48, "LightRec must stay 48 bytes");
 
 // vertex_t (Core.h:259-262)
-struct VertexRec {
+// vertex_t (src/Ray/internal/Core.h:219-222) padded to 64 bytes: four 16-byte loads.
+struct alignas(16) VertexRec {
     float p[3], n[3], b[3], t[2][2];
+    float pad[3];
 };
-static_assert(sizeof(VertexRec) == 52, "VertexRec must stay 52 bytes");
+static_assert(sizeof(VertexRec) == 64, "VertexRec must stay 64 bytes");
 
 constexpr int NUM_MIP_LEVELS = 14;
 

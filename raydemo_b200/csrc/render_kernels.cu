@@ -149,10 +149,10 @@ __device__ __forceinline__ Best trace_any(const SceneView &sv, V3 o, V3 d, float
 }
 
 __device__ __forceinline__ void load_vertex(const RenderScene &sc, uint32_t vi, VertexRec &v) {
-    const float *src = reinterpret_cast<const float *>(sc.vertices + vi);
-    float *dst = reinterpret_cast<float *>(&v);
+    const float4 *src = reinterpret_cast<const float4 *>(sc.vertices + vi);
+    float4 *dst = reinterpret_cast<float4 *>(&v);
 #pragma unroll
-    for (int q = 0; q < 13; q++) dst[q] = __ldg(src + q);
+    for (int q = 0; q < 4; q++) dst[q] = __ldg(src + q);
 }
 
 __device__ __forceinline__ TriRec load_tri(const RenderScene &sc, uint32_t prim) {
@@ -460,27 +460,29 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
     const MaterialRec &mat = sc.materials[mi];
     const V3 N_vertex = N; // interpolated vertex normal (flipped on a back face), before the normal map
 
-    // normal map
-    V3 B = v3(v1.b) * w + v3(v2.b) * hu + v3(v3v.b) * hv;
-    V3 T = cross(B, N);
-    F4 nm = sample_bilinear(sc, mat.textures[0], uvx, uvy, 0);
-    nm.x = nm.x * 2.0f - 1.0f;
-    nm.y = nm.y * 2.0f - 1.0f;
-    nm.z = nm.z * 2.0f - 1.0f;
-    N = nm.x * B + nm.z * N + nm.y * T;
-    N = transform_normal(N, inv);
-    B = transform_normal(B, inv);
-    T = transform_normal(T, inv);
+    // the reference's materials: normal map and main texture (RAY_MAT_PRINCIPLED reads neither)
+    V3 B = v3(0.0f, 0.0f, 0.0f), T = v3(0.0f, 0.0f, 0.0f), alb = v3(0.0f, 0.0f, 0.0f);
+    if (mat.type != (uint32_t)RAY_MAT_PRINCIPLED) {
+        B = v3(v1.b) * w + v3(v2.b) * hu + v3(v3v.b) * hv;
+        T = cross(B, N);
+        F4 nm = sample_bilinear(sc, mat.textures[0], uvx, uvy, 0);
+        nm.x = nm.x * 2.0f - 1.0f;
+        nm.y = nm.y * 2.0f - 1.0f;
+        nm.z = nm.z * 2.0f - 1.0f;
+        N = nm.x * B + nm.z * N + nm.y * T;
+        N = transform_normal(N, inv);
+        B = transform_normal(B, inv);
+        T = transform_normal(T, inv);
 
-    // main texture
-    const uint32_t main_tex = mat.textures[1];
-    const float albedo_lod = texture_lod(sc, main_tex, der.duv_dx[0], der.duv_dx[1], der.duv_dy[0], der.duv_dy[1]);
-    F4 albedo = sample_bilinear(sc, main_tex, uvx, uvy, f2i_x86(albedo_lod));
-    if (main_tex < sc.n_textures && (sc.textures[main_tex].width & 0x8000u)) albedo = srgb_to_rgb(albedo);
-    albedo.x *= mat.main_color[0];
-    albedo.y *= mat.main_color[1];
-    albedo.z *= mat.main_color[2];
-    const V3 alb = v3(albedo.x, albedo.y, albedo.z);
+        const uint32_t main_tex = mat.textures[1];
+        const float albedo_lod = texture_lod(sc, main_tex, der.duv_dx[0], der.duv_dx[1], der.duv_dy[0], der.duv_dy[1]);
+        F4 albedo = sample_bilinear(sc, main_tex, uvx, uvy, f2i_x86(albedo_lod));
+        if (main_tex < sc.n_textures && (sc.textures[main_tex].width & 0x8000u)) albedo = srgb_to_rgb(albedo);
+        albedo.x *= mat.main_color[0];
+        albedo.y *= mat.main_color[1];
+        albedo.z *= mat.main_color[2];
+        alb = v3(albedo.x, albedo.y, albedo.z);
+    }
 
     V3 col = v3(0.0f, 0.0f, 0.0f);
     const int diff_depth = ray.ray_depth & 0xff, gloss_depth = (ray.ray_depth >> 8) & 0xff, refr_depth = (ray.ray_depth >> 16) & 0xff,
@@ -526,9 +528,9 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
             nr.p.c[1] = ray.c[1] * weight;
             nr.p.c[2] = ray.c[2] * weight;
             if (consider_albedo) {
-                nr.p.c[0] *= albedo.x;
-                nr.p.c[1] *= albedo.y;
-                nr.p.c[2] *= albedo.z;
+                nr.p.c[0] *= alb.x;
+                nr.p.c[1] *= alb.y;
+                nr.p.c[2] *= alb.z;
             }
             set3(nr.p.do_dx, der.do_dx);
             set3(nr.p.do_dy, der.do_dy);
@@ -560,9 +562,9 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
             nr.p.c[1] = ray.c[1];
             nr.p.c[2] = ray.c[2];
             if (consider_albedo) {
-                nr.p.c[0] *= albedo.x;
-                nr.p.c[1] *= albedo.y;
-                nr.p.c[2] *= albedo.z;
+                nr.p.c[0] *= alb.x;
+                nr.p.c[1] *= alb.y;
+                nr.p.c[2] *= alb.z;
             }
             set3(nr.p.do_dx, der.do_dx);
             set3(nr.p.do_dy, der.do_dy);
