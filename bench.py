@@ -490,10 +490,12 @@ def diff_frames(args, dev, stream, rank: int, world: int) -> dict:
     rough = torch.full_like(tgt_r, 0.5).requires_grad_(True)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     n_t = max(5, min(args.steps, 20))
-    # forward alone, then forward + loss + adjoint (the gradient step)
+    # forward alone, then forward + loss + adjoint (the gradient step); both warmed up first
     for _ in range(3):
         with torch.no_grad():
             render(albedo, rough)
+        albedo.grad = rough.grad = None
+        ((render(albedo, rough) - target) ** 2).sum().backward()
     torch.cuda.synchronize(dev)
     ev[0].record()
     for _ in range(n_t):
