@@ -763,6 +763,24 @@ def run_gpu_arm(args) -> None:
     e2e_value = world * N_RAYS / (float(te.item()) * 1e-3) / 1e6
     ok = np.array_equal(hits_h.numpy().view(np.uint32), hits_d.cpu().numpy().view(np.uint32))
 
+    # the same scene and kernel on 4,194,304 coherent rays (a pinhole camera at 2048x2048 outside the cube)
+    coh = torch.from_numpy(scenes.coherent_rays(2048, 2048)).to(dev)
+    for _ in range(3):
+        sc.trace_closest_device(coh.data_ptr(), N_RAYS, hits_d.data_ptr(), 0, sptr)
+    torch.cuda.synchronize(dev)
+    ev0.record(stream)
+    c_steps = max(3, min(args.steps, 20))
+    for _ in range(c_steps):
+        sc.trace_closest_device(coh.data_ptr(), N_RAYS, hits_d.data_ptr(), 0, sptr)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    coh_ms = ev0.elapsed_time(ev1) / c_steps
+    coh_hits = hits_d[:, 0].view(torch.int32)
+    coherent = {"rays": N_RAYS, "ms_per_step": round(coh_ms, 4), "mrays_per_s": round(N_RAYS / (coh_ms * 1e-3) / 1e6, 1),
+                "hit_rate": round(float((coh_hits >= 0).float().mean()), 4),
+                "camera": "pinhole at (0.5, 0.5, -1.5), fov 45 deg, one ray per pixel centre of 2048x2048"}
+    del coh
+
     # roofline of the traversal kernel (the only kernel in the timed region)
     p = peaks()
     bytes_per_launch = N_RAYS * 44 + node_visits * 80 + tri_tests * 48
@@ -797,7 +815,8 @@ def run_gpu_arm(args) -> None:
                            "bvh_nodes": info.nodes, "bvh_depth": info.depth, "parallelism": f"replicas x{world}"},
                 "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": N_RAYS * 32, "d2h_bytes_per_step": N_RAYS * 16,
                         "matches_device_path": bool(ok)},
-                "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "render": render, "batch": batch,
+                "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "coherent": coherent,
+                "render": render, "batch": batch,
                 "atrium": atrium, "diff": diffr}
         print(json.dumps(line), flush=True)
     del sc, r

@@ -5,6 +5,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <random>
@@ -358,6 +360,64 @@ int prepare_job(ray_renderer *r, ray_scene *s, ray_region *region, FrameJob &J, 
 // per bounce a closest-hit trace and a shading launch over the rays of all
 // jobs, then the accumulation. Buffers and counters are rb's. sample: offset
 // from each job's first iteration. ev (may be null): stats events.
+// FNV-1a over the values a captured launch sequence depends on.
+struct GraphKey {
+    uint64_t h = 1469598103934665603ull;
+    template <typename T>
+    GraphKey &add(const T &v) {
+        const unsigned char *p = reinterpret_cast<const unsigned char *>(&v);
+        for (size_t i = 0; i < sizeof(T); i++) h = (h ^ p[i]) * 1099511628211ull;
+        return *this;
+    }
+};
+
+// Enqueues a launch sequence through a cached CUDA graph: the first call with
+// a new key runs it directly (its buffers get allocated then), the second
+// captures and instantiates it, later ones replay it. A capture that fails
+// falls back to running the sequence directly.
+// RAY_GRAPHS=0 in the environment turns graph replay off (every call enqueues directly).
+bool graphs_enabled() {
+    static const int on = [] {
+        const char *v = std::getenv("RAY_GRAPHS");
+        return (v && v[0] == '0') ? 0 : 1;
+    }();
+    return on != 0;
+}
+
+template <typename F>
+int graph_run(GraphSlot &g, uint64_t key, cudaStream_t st, F &&enqueue) {
+    if (!graphs_enabled()) return enqueue();
+    if (g.key != key) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+        g.key = key;
+        g.runs = 0;
+    }
+    if (g.exec) {
+        RG_CUDA_TRY(cudaGraphLaunch(g.exec, st));
+        return RAY_OK;
+    }
+    if (g.runs++ == 0 || g.failed) return enqueue();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t eb = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    const int rc = eb == cudaSuccess ? enqueue() : RAY_ERR_CUDA;
+    const cudaError_t ee = eb == cudaSuccess ? cudaStreamEndCapture(st, &graph) : eb;
+    cudaError_t ei = cudaErrorUnknown;
+    if (rc == RAY_OK && ee == cudaSuccess && graph) ei = cudaGraphInstantiate(&g.exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (ei == cudaSuccess) {
+        RG_CUDA_TRY(cudaGraphLaunch(g.exec, st));
+        return RAY_OK;
+    }
+    if (std::getenv("RAY_GRAPH_DEBUG"))
+        fprintf(stderr, "graph capture failed: begin %d, enqueue %d (%s), end %d, instantiate %d\n", (int)eb, rc, ray_last_error(), (int)ee,
+                (int)ei);
+    g.exec = nullptr;
+    g.failed = true;
+    cudaGetLastError(); // the capture's error, if any, is not the caller's
+    return enqueue();
+}
+
 // The adjoint's replay (adj in run_wavefront): its arguments and per-ray state buffers.
 struct AdjointRun {
     AdjArgs args;
@@ -366,8 +426,8 @@ struct AdjointRun {
 };
 
 int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<FrameJob> &jobs, const std::vector<const ray_scene *> &scn,
-                  uint32_t total, int sample, uint32_t sort_mask, cudaStream_t st, cudaEvent_t *ev, int &nb, bool resolve = true,
-                  const AdjointRun *adj = nullptr) {
+                  uint32_t total, int sample0, uint32_t sort_mask, cudaStream_t st, cudaEvent_t *ev, int &nb, bool resolve = true,
+                  const AdjointRun *adj = nullptr, int samples = 1, GraphSlot *gs = nullptr) {
     nb = 0;
     if (adj) sort_mask = 0; // the replay keeps the forward pass's order
     int rc = ensure_ray_buffers(rb, std::max<size_t>(total, 1));
@@ -415,64 +475,83 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
         tp.view_stride = (uint32_t)sizeof(FrameJob);
     }
     const SceneView &sv = jobs[0].sc.sv;
-    // primary rays (GeneratePrimaryRays, CoreRef.cpp:427-505)
-    RG_CUDA_TRY(cudaMemsetAsync(cnt, 0, 2 * sizeof(uint32_t), st));
-    RG_CUDA_TRY(launch_raygen_jobs(d_jobs, n_jobs, total, sample, rays[0], pay[0], job[0], cnt + 0, st));
-    if (ev) RG_CUDA_TRY(cudaEventRecord(ev[1], st));
-    tp.count = cnt + 0;
-    tp.ray_job = job[0];
-    RG_CUDA_TRY(launch_trace_closest(sv, rays[0], total, hits, obj, err, nullptr, false, st, tp));
-    if (ev) RG_CUDA_TRY(cudaEventRecord(ev[2], st));
-    // shadow rays of the light samples: the persistent kernel in any-hit mode (the hits buffer is free again)
-    TraceParams tps = tp;
-    tps.any = true;
-    tps.count = shadow_cnt;
-    tps.ray_job = shadow.job;
-    // shading of the rays in buffer `in` (bounce b), continuation rays to `out`, then the light samples'
-    // shadow rays and the colour of the unblocked ones
-    auto shade = [&](int b, int in, int out) -> cudaError_t {
-        cudaError_t e = cudaSuccess;
-        if (nee || adj) e = cudaMemsetAsync(shadow_cnt, 0, sizeof(uint32_t), st);
-        if (e != cudaSuccess) return e;
-        if (adj)
-            e = launch_adjoint_shade(d_jobs, b, rays[in], pay[in], job[in], adj->state[in], hits, obj, cnt + in, total, rays[out], pay[out],
-                                     job[out], adj->state[out], cnt + out, shadow, adj->args, err, st);
-        else
-            e = launch_shade_jobs(d_jobs, sample, b, rays[in], pay[in], job[in], hits, obj, cnt + in, total, rays[out], pay[out], job[out],
-                                  cnt + out, shadow, ref_lights, err, ray_stats, st);
-        if (e != cudaSuccess || !(nee || adj)) return e;
-        e = launch_trace_closest(sv, shadow.rays, total, hits, nullptr, err, nullptr, false, st, tps);
-        if (e != cudaSuccess) return e;
-        if (adj) return launch_adjoint_shadow_apply(d_jobs, b, shadow, hits, total, adj->state[out], adj->args, err, st);
-        return launch_shadow_apply(d_jobs, sample, b, shadow, hits, total, err, ray_stats, st);
-    };
-    RG_CUDA_TRY(shade(2, 0, 1));
-    if (ev) RG_CUDA_TRY(cudaEventRecord(ev[3], st));
-    // bounces (RendererRef.cpp:183-278); ray counts stay on the device
-    int cur = 1;
-    for (int bounce = 0; bounce < bounces; bounce++) {
-        if ((sort_mask >> bounce) & 1u) {
-            // SortRays_CPU before each bounce (RendererRef.cpp:200-203): the rays move to the other buffer in hash order
-            const int dst = cur ^ 1;
-            RG_CUDA_TRY(launch_loop_sort(d_jobs, (int)jobs.size(), rays[cur], pay[cur], job[cur], cnt + cur, total, rays[dst], pay[dst], job[dst],
-                                         cnt + dst, rb->d_loop_sort.p, st));
-            cur = dst;
+    auto enqueue_sample = [&](int sample) -> int {
+        // primary rays (GeneratePrimaryRays, CoreRef.cpp:427-505)
+        RG_CUDA_TRY(cudaMemsetAsync(cnt, 0, 2 * sizeof(uint32_t), st));
+        RG_CUDA_TRY(launch_raygen_jobs(d_jobs, n_jobs, total, sample, rays[0], pay[0], job[0], cnt + 0, st));
+        if (ev) RG_CUDA_TRY(cudaEventRecord(ev[1], st));
+        tp.count = cnt + 0;
+        tp.ray_job = job[0];
+        RG_CUDA_TRY(launch_trace_closest(sv, rays[0], total, hits, obj, err, nullptr, false, st, tp));
+        if (ev) RG_CUDA_TRY(cudaEventRecord(ev[2], st));
+        // shadow rays of the light samples: the persistent kernel in any-hit mode (the hits buffer is free again)
+        TraceParams tps = tp;
+        tps.any = true;
+        tps.count = shadow_cnt;
+        tps.ray_job = shadow.job;
+        // shading of the rays in buffer `in` (bounce b), continuation rays to `out`, then the light samples'
+        // shadow rays and the colour of the unblocked ones
+        auto shade = [&](int b, int in, int out) -> cudaError_t {
+            cudaError_t e = cudaSuccess;
+            if (nee || adj) e = cudaMemsetAsync(shadow_cnt, 0, sizeof(uint32_t), st);
+            if (e != cudaSuccess) return e;
+            if (adj)
+                e = launch_adjoint_shade(d_jobs, b, rays[in], pay[in], job[in], adj->state[in], hits, obj, cnt + in, total, rays[out], pay[out],
+                                         job[out], adj->state[out], cnt + out, shadow, adj->args, err, st);
+            else
+                e = launch_shade_jobs(d_jobs, sample, b, rays[in], pay[in], job[in], hits, obj, cnt + in, total, rays[out], pay[out], job[out],
+                                      cnt + out, shadow, ref_lights, err, ray_stats, st);
+            if (e != cudaSuccess || !(nee || adj)) return e;
+            e = launch_trace_closest(sv, shadow.rays, total, hits, nullptr, err, nullptr, false, st, tps);
+            if (e != cudaSuccess) return e;
+            if (adj) return launch_adjoint_shadow_apply(d_jobs, b, shadow, hits, total, adj->state[out], adj->args, err, st);
+            return launch_shadow_apply(d_jobs, sample, b, shadow, hits, total, err, ray_stats, st);
+        };
+        RG_CUDA_TRY(shade(2, 0, 1));
+        if (ev) RG_CUDA_TRY(cudaEventRecord(ev[3], st));
+        // bounces (RendererRef.cpp:183-278); ray counts stay on the device
+        int cur = 1;
+        for (int bounce = 0; bounce < bounces; bounce++) {
+            if ((sort_mask >> bounce) & 1u) {
+                // SortRays_CPU before each bounce (RendererRef.cpp:200-203): the rays move to the other buffer in hash order
+                const int dst = cur ^ 1;
+                RG_CUDA_TRY(launch_loop_sort(d_jobs, (int)jobs.size(), rays[cur], pay[cur], job[cur], cnt + cur, total, rays[dst], pay[dst], job[dst],
+                                             cnt + dst, rb->d_loop_sort.p, st));
+                cur = dst;
+            }
+            if (ev) RG_CUDA_TRY(cudaEventRecord(ev[ev_sorted(bounce)], st));
+            const int nxt = cur ^ 1;
+            RG_CUDA_TRY(cudaMemsetAsync(cnt + nxt, 0, sizeof(uint32_t), st));
+            tp.count = cnt + cur;
+            tp.ray_job = job[cur];
+            RG_CUDA_TRY(launch_trace_closest(sv, rays[cur], total, hits, obj, err, nullptr, false, st, tp));
+            if (ev) RG_CUDA_TRY(cudaEventRecord(ev[ev_traced(bounce)], st));
+            RG_CUDA_TRY(shade(bounce + 3, cur, nxt));
+            if (ev) RG_CUDA_TRY(cudaEventRecord(ev[ev_shaded(bounce)], st));
+            cur = nxt;
         }
-        if (ev) RG_CUDA_TRY(cudaEventRecord(ev[ev_sorted(bounce)], st));
-        const int nxt = cur ^ 1;
-        RG_CUDA_TRY(cudaMemsetAsync(cnt + nxt, 0, sizeof(uint32_t), st));
-        tp.count = cnt + cur;
-        tp.ray_job = job[cur];
-        RG_CUDA_TRY(launch_trace_closest(sv, rays[cur], total, hits, obj, err, nullptr, false, st, tp));
-        if (ev) RG_CUDA_TRY(cudaEventRecord(ev[ev_traced(bounce)], st));
-        RG_CUDA_TRY(shade(bounce + 3, cur, nxt));
-        if (ev) RG_CUDA_TRY(cudaEventRecord(ev[ev_shaded(bounce)], st));
-        cur = nxt;
-        nb++;
-    }
-    // accumulate and tone (RendererRef.cpp:292-324)
-    if (resolve) RG_CUDA_TRY(launch_resolve_jobs(d_jobs, n_jobs, total, sample, st));
-    return RAY_OK;
+        // accumulate and tone (RendererRef.cpp:292-324)
+        if (resolve) RG_CUDA_TRY(launch_resolve_jobs(d_jobs, n_jobs, total, sample, st));
+        return RAY_OK;
+    };
+    // the samples one after another (each a whole wavefront)
+    auto enqueue = [&]() -> int {
+        for (int k = 0; k < samples; k++) {
+            const int rc2 = enqueue_sample(sample0 + k);
+            if (rc2 != RAY_OK) return rc2;
+        }
+        return RAY_OK;
+    };
+    nb = bounces;
+    if (!gs) return enqueue();
+    // everything the launches take by value or point at: the graph is replayed while all of it is unchanged
+    GraphKey key;
+    key.add(d_jobs).add(n_jobs).add(total).add(sample0).add(samples).add(sort_mask).add(bounces).add(resolve).add(adj).add(st);
+    for (int q = 0; q < 2; q++) key.add(rays[q]).add(pay[q]).add(job[q]);
+    key.add(hits).add(obj).add(cnt).add(shadow.recs).add(shadow.rays).add(shadow.job).add(rb->d_loop_sort.p).add(nee).add(ref_lights);
+    key.add(sv.nodes).add(sv.leaf_tris).add(sv.inst).add(sv.n_inst).add(tp.persistent).add(tp.refill_min).add(tp.max_depth).add(tp.views);
+    key.add(ev);
+    return graph_run(*gs, key.h, st, enqueue);
 }
 
 // The jobs of a differentiable render: sample k (iteration first + k) as job k,
@@ -526,6 +605,7 @@ ray_renderer::~ray_renderer() {
     if (ev_sync) cudaEventDestroy(ev_sync);
     for (int e = 0; e < 2; e++)
         if (ev_batch[e]) cudaEventDestroy(ev_batch[e]);
+    if (batch_graph.exec) cudaGraphExecDestroy(batch_graph.exec);
     if (own_stream) cudaStreamDestroy(own_stream);
 }
 
@@ -630,6 +710,7 @@ int ray_render(ray_renderer *r, ray_scene *s, ray_region *region) {
             RG_CUDA_TRY(cudaEventRecord(ev[2], st));
             RG_CUDA_TRY(cudaEventRecord(ev[3], st));
         } else {
+            // launched directly: its phase events feed the stats and the kernel and sort choice
             rc = run_wavefront(r, d_jobs, std::vector<FrameJob>{J}, std::vector<const ray_scene *>{s}, (uint32_t)n_pix, 0, plan.sort_mask, st,
                                ev, nb);
             if (rc != RAY_OK) return rc;
@@ -737,11 +818,11 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
                     RG_CUDA_TRY(launch_render_paths(d_jobs, (int)jobs.size(), (uint32_t)total, cnt + 2, cnt + 3,
                                                     reinterpret_cast<unsigned long long *>(cnt + 4), st));
                 } else {
-                    for (int k = 0; k < run; k++) { // one wavefront per sample over the rays of all jobs
-                        int nb = 0;
-                        rc = run_wavefront(r0, d_jobs, jobs, jscn, (uint32_t)total, k, plan.sort_mask, st, nullptr, nb);
-                        if (rc != RAY_OK) return rc;
-                    }
+                    // one wavefront per sample over the rays of all jobs, the run as one CUDA graph
+                    int nb = 0;
+                    rc = run_wavefront(r0, d_jobs, jobs, jscn, (uint32_t)total, 0, plan.sort_mask, st, nullptr, nb, true, nullptr, run,
+                                       &r0->batch_graph);
+                    if (rc != RAY_OK) return rc;
                 }
             }
             // and each renderer's later work (reads of its pixels, its next frames) after the batch

@@ -74,6 +74,14 @@ void compute_tangent_basis(std::vector<VertexRec> &vertices, std::vector<uint32_
 int upload_shading(ray_scene *s); // device copies of vertices, materials, textures and lights
 RenderScene render_scene_view(const ray_scene *s);
 
+// A cached CUDA graph of a launch sequence (render.cu: graph_run).
+struct GraphSlot {
+    uint64_t key = 0;
+    int runs = 0;
+    bool failed = false;
+    cudaGraphExec_t exec = nullptr;
+};
+
 } // namespace rg
 
 struct ray_scene {
@@ -177,5 +185,7 @@ struct ray_renderer {
     int ev_kernel[2] = {0, 0};
     int ev_variant[2] = {0, 0};
     rg::DeviceBuf d_jobs;      // FrameJob array of the path kernel
+    // a batch's launch sequence as a CUDA graph (render.cu: graph_run)
+    rg::GraphSlot batch_graph;
     ~ray_renderer();
 };
