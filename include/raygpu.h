@@ -85,6 +85,12 @@ enum { RAY_MAT_DIFFUSE = 0, RAY_MAT_GLOSSY, RAY_MAT_REFRACTIVE, RAY_MAT_EMISSIVE
 #define RAY_MAT_PRINCIPLED 6
 /* eVertexLayout (SceneBase.h:27-32) */
 enum { RAY_LAYOUT_PNT = 0, RAY_LAYOUT_PNTT, RAY_LAYOUT_PNBT, RAY_LAYOUT_PNBTT };
+/* eCamType (Types.h:34). GEO: a lightmap camera -- the framebuffer is the
+ * UV layer uv_index of instance mi_index's mesh, each texel's surface point
+ * shaded as a camera-ray hit (RendererRef.cpp:142-149). ORTHO is not rendered
+ * (RAY_ERR_UNSUPPORTED): the reference constructs no orthographic camera
+ * (Core.cpp:883-885). */
+enum { RAY_CAM_PERSP = 0, RAY_CAM_ORTHO, RAY_CAM_GEO };
 /* eLightType (SceneBase.h:108-112) */
 enum { RAY_LIGHT_POINT = 0, RAY_LIGHT_SPOT, RAY_LIGHT_DIRECTIONAL };
 /* Extensions with no counterpart in the reference, used by RAY_MAT_PRINCIPLED:

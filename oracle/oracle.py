@@ -358,6 +358,8 @@ class RefLib:
         L.rb_renderer_type.restype = i32
         L.rb_render.argtypes = [vp, vp, i32, i32, i32, i32, i32, i32, i32]
         L.rb_get_pixels.argtypes = [vp, vp]
+        L.rb_get_sh.argtypes = [vp, vp]
+        L.rb_get_sh.restype = C.c_int
         L.rb_get_stats.argtypes = [vp, vp]
         L.rb_clear.argtypes = [vp]
 
@@ -474,6 +476,11 @@ class RefRenderer:
         out = np.zeros((self.h, self.w, 4), np.float32)
         self.ref.lib.rb_get_pixels(self.r, _p(out))
         return out
+
+    def sh_data(self):
+        """get_sh_data_ref: (h, w, 12) float32, or None."""
+        out = np.zeros((self.h, self.w, 12), np.float32)
+        return out if self.ref.lib.rb_get_sh(self.r, _p(out)) else None
 
     def stats(self) -> np.ndarray:
         out = np.zeros(6, np.uint64)

@@ -394,6 +394,15 @@ void rb_get_pixels(void *r, float *out) {
     memcpy(out, rh->r->get_pixels_ref(), sizeof(float) * 4 * rh->w * rh->h);
 }
 
+// get_sh_data_ref: w * h shl1_data_t (12 floats each); 0 when the renderer holds none.
+int rb_get_sh(void *r, float *out) {
+    auto *rh = static_cast<RendererHandle *>(r);
+    const Ray::shl1_data_t *sh = rh->r->get_sh_data_ref();
+    if (!sh) return 0;
+    memcpy(out, sh, sizeof(Ray::shl1_data_t) * rh->w * rh->h);
+    return 1;
+}
+
 void rb_get_stats(void *r, unsigned long long *out6) {
     Ray::RendererBase::stats_t st;
     static_cast<RendererHandle *>(r)->r->GetStats(st);

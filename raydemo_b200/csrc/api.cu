@@ -134,6 +134,44 @@ static void construct_camera(CameraRec &c) {
     }
 }
 
+// SceneBase::SetCamera, SceneBase.cpp:56-84. A Geo camera takes its kind,
+// gamma, instance and UV layer and leaves the perspective fields (filter,
+// dtype, origin, axes, fov, focus) as the slot held them: zero for a new
+// slot, a previous camera's where one is replaced. A perspective camera
+// leaves mi_index / uv_index as they were.
+static void set_camera(CameraRec &rec, const ray_camera_desc &c) {
+    ray_camera_desc &d = rec.desc;
+    d.type = c.type;
+    d.gamma = c.gamma;
+    if (c.type != RAY_CAM_GEO) {
+        d.filter = c.filter;
+        d.dtype = c.dtype;
+        memcpy(d.origin, c.origin, sizeof(d.origin));
+        memcpy(d.fwd, c.fwd, sizeof(d.fwd));
+        memcpy(d.up, c.up, sizeof(d.up));
+        d.fov = c.fov;
+        d.focus_distance = c.focus_distance;
+        d.focus_factor = c.focus_factor;
+        construct_camera(rec);
+    } else {
+        d.mi_index = c.mi_index;
+        d.uv_index = c.uv_index;
+    }
+    d.lighting_only = c.lighting_only;
+    d.skip_direct_lighting = c.skip_direct_lighting;
+    d.skip_indirect_lighting = c.skip_indirect_lighting;
+    d.no_background = c.no_background;
+    d.clamp = c.clamp;
+    d.output_sh = c.output_sh;
+    d.use_coherent_sampling = c.use_coherent_sampling;
+    d.max_diff_depth = c.max_diff_depth;
+    d.max_glossy_depth = c.max_glossy_depth;
+    d.max_refr_depth = c.max_refr_depth;
+    d.max_transp_depth = c.max_transp_depth;
+    d.max_total_depth = c.max_total_depth;
+    d.termination_start_depth = c.termination_start_depth;
+}
+
 int commit(ray_scene *s) {
     if (!s->geom_dirty) return upload_shading(s);
     RG_CUDA_TRY(cudaSetDevice(s->device));
@@ -693,9 +731,8 @@ int ray_scene_add_camera(ray_scene *s, const ray_camera_desc *c, uint32_t *out_i
         i = s->cam_first_free;
         s->cam_first_free = s->cameras[i].next_free;
     }
-    s->cameras[i].desc = *c;
     s->cameras[i].alive = true;
-    construct_camera(s->cameras[i]);
+    set_camera(s->cameras[i], *c);
     if (s->current_cam == RAY_INVALID_INDEX) s->current_cam = i;
     *out_index = i;
     return RAY_OK;
@@ -704,14 +741,42 @@ int ray_scene_add_camera(ray_scene *s, const ray_camera_desc *c, uint32_t *out_i
 
 int ray_scene_get_camera(ray_scene *s, uint32_t i, ray_camera_desc *out) {
     RG_CHECK(s && out && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");
-    *out = s->cameras[i].desc;
+    // SceneBase::GetCamera, SceneBase.cpp:22-54: the fields of the camera's kind only
+    const ray_camera_desc &d = s->cameras[i].desc;
+    out->type = d.type;
+    out->dtype = d.dtype;
+    out->gamma = d.gamma;
+    if (d.type != RAY_CAM_GEO) {
+        out->filter = d.filter;
+        memcpy(out->origin, d.origin, sizeof(out->origin));
+        memcpy(out->fwd, d.fwd, sizeof(out->fwd));
+        memcpy(out->up, d.up, sizeof(out->up));
+        out->fov = d.fov;
+        out->focus_distance = d.focus_distance;
+        out->focus_factor = d.focus_factor;
+    } else {
+        out->mi_index = d.mi_index;
+        out->uv_index = d.uv_index;
+    }
+    out->lighting_only = d.lighting_only;
+    out->skip_direct_lighting = d.skip_direct_lighting;
+    out->skip_indirect_lighting = d.skip_indirect_lighting;
+    out->no_background = d.no_background;
+    out->clamp = d.clamp;
+    out->output_sh = d.output_sh;
+    out->use_coherent_sampling = d.use_coherent_sampling;
+    out->max_diff_depth = d.max_diff_depth;
+    out->max_glossy_depth = d.max_glossy_depth;
+    out->max_refr_depth = d.max_refr_depth;
+    out->max_transp_depth = d.max_transp_depth;
+    out->max_total_depth = d.max_total_depth;
+    out->termination_start_depth = d.termination_start_depth;
     return RAY_OK;
 }
 
 int ray_scene_set_camera(ray_scene *s, uint32_t i, const ray_camera_desc *c) {
     RG_CHECK(s && c && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");
-    s->cameras[i].desc = *c;
-    construct_camera(s->cameras[i]);
+    set_camera(s->cameras[i], *c);
     return RAY_OK;
 }
 

@@ -203,8 +203,12 @@ FramePlan plan_of_variant(const ray_renderer::TuneEntry &t, int v) {
 // caller's fixed settings, else timed on the configuration's first frames
 // (TUNE_SAMPLES per variant, the best kept; every variant gives the same image).
 // bounces < 0 marks a batch configuration (-samples; lights then holds the count).
-FramePlan plan_frame(ray_renderer *r, const void *s, uint32_t tris, uint32_t lights, uint32_t pixels, int bounces) {
+FramePlan plan_frame(ray_renderer *r, const void *s, uint32_t tris, uint32_t lights, uint32_t pixels, int bounces, bool geo = false) {
     FramePlan p;
+    if (geo) { // the path kernel generates camera rays only: Geo cameras run on the wavefront
+        p.sort_mask = r->sort_policy >= 0 ? (uint32_t)r->sort_policy & SORT_ALL : 0u;
+        return p;
+    }
     if (r->kernel == 2) {
         p.kernel = 2;
         return p;
@@ -268,9 +272,13 @@ int prepare_job(ray_renderer *r, ray_scene *s, ray_region *region, FrameJob &J, 
     }
     const CameraRec &cam = s->cameras[s->current_cam];
     const ray_camera_desc &cd = cam.desc;
-    if (cd.type != 0) {
-        set_error("only perspective cameras are rendered");
+    if (cd.type != RAY_CAM_PERSP && cd.type != RAY_CAM_GEO) {
+        set_error("only perspective and Geo cameras are rendered");
         return RAY_ERR_UNSUPPORTED;
+    }
+    if (cd.type == RAY_CAM_GEO && (cd.mi_index >= s->instances.size() || cd.uv_index > 1)) {
+        set_error("Geo camera: mi_index must name an instance and uv_index be 0 or 1");
+        return RAY_ERR_INVALID_ARG;
     }
     RG_CUDA_TRY(cudaSetDevice(r->device));
     int rc = commit(s);
@@ -333,6 +341,23 @@ int prepare_job(ray_renderer *r, ray_scene *s, ray_region *region, FrameJob &J, 
     J.rh = rect.h;
     J.w = w;
     J.h = h;
+    if (cd.type == RAY_CAM_GEO) {
+        // the instance's mesh, its transform, and its index among the device's
+        // instances (the hit's obj; instances of empty meshes have none)
+        const InstanceRecHost &ih = s->instances[cd.mi_index];
+        const MeshRec &m = s->meshes[ih.mesh];
+        GeoCam &g = J.geo;
+        g.on = 1;
+        g.tri0 = m.tris_index;
+        g.ntri = m.tris_count;
+        g.uv = cd.uv_index;
+        g.obj = 0;
+        for (uint32_t q = 0; q < cd.mi_index; q++) g.obj += s->meshes[s->instances[q].mesh].tris_count ? 1u : 0u;
+        for (int row = 0; row < 3; row++)
+            for (int col = 0; col < 4; col++) g.xf[row * 4 + col] = ih.xform[col * 4 + row];
+        for (int row = 0; row < 3; row++)
+            for (int col = 0; col < 3; col++) g.inv[row * 3 + col] = ih.inv_xform[row * 4 + col];
+    }
     J.halton = static_cast<const float *>(r->d_halton.p);
     J.temp = static_cast<float4 *>(r->d_temp.p);
     J.clean = static_cast<float4 *>(r->d_clean.p);
@@ -474,6 +499,18 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
         tp.views = reinterpret_cast<const uint8_t *>(d_jobs) + offsetof(FrameJob, sc) + offsetof(RenderScene, sv);
         tp.view_stride = (uint32_t)sizeof(FrameJob);
     }
+    // Geo (lightmap) jobs take their primary hits from the UV-space sampling
+    bool persp = false;
+    uint32_t geo_tris = 0;
+    for (const FrameJob &J : jobs) {
+        if (J.geo.on) geo_tris = std::max(geo_tris, std::max(J.geo.ntri, 1u));
+        else persp = true;
+    }
+    uint32_t *geo_best = nullptr;
+    if (geo_tris) {
+        RG_CUDA_TRY(rb->d_geo_best.ensure(std::max<size_t>(total, 1) * sizeof(uint32_t)));
+        geo_best = static_cast<uint32_t *>(rb->d_geo_best.p);
+    }
     const SceneView &sv = jobs[0].sc.sv;
     auto enqueue_sample = [&](int sample) -> int {
         // primary rays (GeneratePrimaryRays, CoreRef.cpp:427-505)
@@ -482,7 +519,13 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
         if (ev) RG_CUDA_TRY(cudaEventRecord(ev[1], st));
         tp.count = cnt + 0;
         tp.ray_job = job[0];
-        RG_CUDA_TRY(launch_trace_closest(sv, rays[0], total, hits, obj, err, nullptr, false, st, tp));
+        if (persp) RG_CUDA_TRY(launch_trace_closest(sv, rays[0], total, hits, obj, err, nullptr, false, st, tp));
+        if (geo_tris) {
+            // SampleMeshInTextureSpace (RendererRef.cpp:142-146): rays and hits of the Geo jobs' texels
+            RG_CUDA_TRY(cudaMemsetAsync(geo_best, 0xff, (size_t)total * sizeof(uint32_t), st));
+            RG_CUDA_TRY(launch_geo_cover(d_jobs, n_jobs, geo_tris, sample, geo_best, st));
+            RG_CUDA_TRY(launch_geo_rays(d_jobs, n_jobs, total, sample, geo_best, rays[0], pay[0], hits, obj, st));
+        }
         if (ev) RG_CUDA_TRY(cudaEventRecord(ev[2], st));
         // shadow rays of the light samples: the persistent kernel in any-hit mode (the hits buffer is free again)
         TraceParams tps = tp;
@@ -550,7 +593,7 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
     for (int q = 0; q < 2; q++) key.add(rays[q]).add(pay[q]).add(job[q]);
     key.add(hits).add(obj).add(cnt).add(shadow.recs).add(shadow.rays).add(shadow.job).add(rb->d_loop_sort.p).add(nee).add(ref_lights);
     key.add(sv.nodes).add(sv.leaf_tris).add(sv.inst).add(sv.n_inst).add(tp.persistent).add(tp.refill_min).add(tp.max_depth).add(tp.views);
-    key.add(ev);
+    key.add(ev).add(geo_best).add(geo_tris).add(persp);
     return graph_run(*gs, key.h, st, enqueue);
 }
 
@@ -689,7 +732,8 @@ int ray_render(ray_renderer *r, ray_scene *s, ray_region *region) {
         rc = resolve_stats(r, set);
         if (rc != RAY_OK) return rc;
         cudaEvent_t *ev = r->ev_sets[set];
-        const FramePlan plan = plan_frame(r, s, s->total_tris, (uint32_t)(s->lights.size() + s->area_lights.size()), (uint32_t)n_pix, J.bounces);
+        const FramePlan plan =
+            plan_frame(r, s, s->total_tris, (uint32_t)(s->lights.size() + s->area_lights.size()), (uint32_t)n_pix, J.bounces, J.geo.on != 0);
         const int kern = plan.kernel;
 
         uint32_t *cnt = static_cast<uint32_t *>(r->d_counters.p);
@@ -775,7 +819,12 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
         }
         // kernel and sort: the first renderer's settings; what they leave open is
         // chosen per batch configuration by timing (blocking) its first calls
-        const FramePlan plan = plan_frame(r0, scenes[0], (uint32_t)tris_all, (uint32_t)count, (uint32_t)px_all, -samples);
+        bool any_geo = false;
+        for (int i = 0; i < count; i++) {
+            const ray_scene *q = scenes[i];
+            any_geo = any_geo || (q->current_cam < q->cameras.size() && q->cameras[q->current_cam].desc.type == RAY_CAM_GEO);
+        }
+        const FramePlan plan = plan_frame(r0, scenes[0], (uint32_t)tris_all, (uint32_t)count, (uint32_t)px_all, -samples, any_geo);
         const int kern = plan.kernel, tune_entry = plan.tune_entry;
         if (tune_entry >= 0) RG_CUDA_TRY(cudaEventRecord(r0->ev_batch[0], st));
         for (int done = 0; done < samples;) {

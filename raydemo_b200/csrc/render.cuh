@@ -121,6 +121,18 @@ struct CameraDev {
     float origin[3], fwd[3], side[3], up[3];
 };
 
+// A Geo (lightmap) camera, camera_t::mi_index / uv_index (Types.h:69): the
+// instance's mesh sampled in its UV layer `uv` (SampleMeshInTextureSpace,
+// CoreRef.cpp:507-603). xf: the instance transform's first three rows
+// (TransformPoint's operand order), inv: its inverse's upper 3x3 in the
+// layout transform_normal reads.
+struct GeoCam {
+    int on;
+    uint32_t tri0, ntri; // the mesh's global triangle range
+    uint32_t obj, uv;
+    float xf[12], inv[9];
+};
+
 // Ray payload beside the 32-byte trace record (o, tmax | d, xy): the rest of
 // ray_packet_t (CoreRef.h:34-45), 80 bytes.
 struct alignas(16) RayPayload {
@@ -161,6 +173,7 @@ struct FrameJob {
     int samples;       // consecutive iterations pi.iteration .. + samples - 1, one after another per pixel
     uint32_t pixel_base;
     float root_min[3], cell[3]; // the ray hash grid: the scene's box split into 255 cells per axis
+    GeoCam geo;                 // geo.on: primary hits come from the UV-space sampling, not from rays
 };
 
 // A RAY_MAT_PRINCIPLED light sample waiting for its shadow ray (48 bytes):
@@ -225,6 +238,11 @@ cudaError_t launch_halton_table(const uint16_t *perms, int base_iteration, float
 // *count = total. Iterations are pi.iteration + sample.
 cudaError_t launch_raygen_jobs(const FrameJob *jobs, int n_jobs, uint32_t total, int sample, float4 *rays, RayPayload *pay,
                                uint32_t *ray_job, uint32_t *count, cudaStream_t st);
+// Geo cameras: the smallest covering triangle per texel into best (all ones
+// beforehand), then the texels' camera rays and hits into rays / pay / hits / obj.
+cudaError_t launch_geo_cover(const FrameJob *jobs, int n_jobs, uint32_t max_tris, int sample, uint32_t *best, cudaStream_t st);
+cudaError_t launch_geo_rays(const FrameJob *jobs, int n_jobs, uint32_t total, int sample, const uint32_t *best, float4 *rays, RayPayload *pay,
+                            float4 *hits, int32_t *obj, cudaStream_t st);
 // Shades the hits of *in_count rays (bounce: pass_info_t::bounce, 2 for the
 // primary rays: SetPixel, else AddPixel with alpha 0), appends the rays that
 // go on to out (count *out_count) and the light samples of RAY_MAT_PRINCIPLED

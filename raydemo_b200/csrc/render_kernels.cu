@@ -852,13 +852,177 @@ __global__ void k_raygen_jobs(const FrameJob *__restrict__ jobs, int n_jobs, uin
     const FrameJob &J = jobs[j];
     const uint32_t li = i - J.pixel_base;
     const int x = J.rx + (int)(li % (uint32_t)J.rw), y = J.ry + (int)(li / (uint32_t)J.rw);
+    ray_job[i] = (uint32_t)j;
+    if (J.geo.on) {
+        // k_geo_rays writes this pixel's ray and hit; where the trace runs for
+        // other jobs of the launch, this ray (tmax 0) hits nothing
+        rays[2ull * i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        rays[2ull * i + 1] = make_float4(0.0f, 0.0f, 1.0f, __int_as_float((x << 16) | y));
+        return;
+    }
     float4 r0, r1;
     RayPayload p;
     gen_primary(J.cam, J.k, J.fov_k, J.pi.iteration + sample, x, y, J.w, J.h, J.halton, r0, r1, p);
     rays[2ull * i] = r0;
     rays[2ull * i + 1] = r1;
     pay[i] = p;
-    ray_job[i] = (uint32_t)j;
+}
+
+// ---- Geo (lightmap) cameras: SampleMeshInTextureSpace, CoreRef.cpp:507-603.
+// The reference rasterises the mesh's triangles in order into the rect, a
+// texel taking the first triangle whose UV-space triangle holds the texel's
+// jittered sample point. Here k_geo_cover runs one warp per triangle over the
+// texels of its box and keeps the smallest covering triangle per texel
+// (atomicMin: the same winner as the first in order), then k_geo_rays
+// recomputes the winner's barycentrics per texel and writes the camera ray
+// and its hit, the arithmetic as in the reference (contraction off).
+
+// A triangle in texel space: corners t, edges d01 = t0 - t1, d12 = t1 - t2,
+// d20 = t2 - t0, signed area, and its box clipped to the rect.
+struct GeoTri {
+    float t0x, t0y, t1x, t1y, t2x, t2y;
+    float d01x, d01y, d12x, d12y, d20x, d20y;
+    float area;
+    int x0, y0, x1, y1;
+};
+
+// The per-triangle part (CoreRef.cpp:530-562); false where the triangle
+// samples no texel: its box misses the rect or its area is below FLT_EPS
+// (triangles wound clockwise in texel space included).
+__device__ __forceinline__ bool geo_setup(const FrameJob &J, uint32_t tri, GeoTri &g) {
+    const RenderScene &sc = J.sc;
+    const uint32_t uv = J.geo.uv;
+    const float sw = (float)J.w, sh = (float)J.h;
+    float tx[3], ty[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const VertexRec &v = sc.vertices[sc.vtx_indices[tri * 3u + k]];
+        tx[k] = __ldg(&v.t[uv][0]) * sw;
+        ty[k] = (1.0f - __ldg(&v.t[uv][1])) * sh;
+    }
+    g.t0x = tx[0]; g.t0y = ty[0];
+    g.t1x = tx[1]; g.t1y = ty[1];
+    g.t2x = tx[2]; g.t2y = ty[2];
+    float bminx = tx[0], bminy = ty[0], bmaxx = tx[0], bmaxy = ty[0];
+#pragma unroll
+    for (int k = 1; k < 3; k++) {
+        bminx = tx[k] < bminx ? tx[k] : bminx;
+        bminy = ty[k] < bminy ? ty[k] : bminy;
+        bmaxx = bmaxx < tx[k] ? tx[k] : bmaxx;
+        bmaxy = bmaxy < ty[k] ? ty[k] : bmaxy;
+    }
+    // the box's lower corner truncated, its upper corner rounded half away from zero
+    int x0 = (int)bminx, y0 = (int)bminy;
+    int x1 = (int)roundf(bmaxx), y1 = (int)roundf(bmaxy);
+    const int rx1 = J.rx + J.rw - 1, ry1 = J.ry + J.rh - 1;
+    if (x1 < J.rx || y1 < J.ry || x0 > rx1 || y0 > ry1) return false;
+    g.x0 = x0 > J.rx ? x0 : J.rx;
+    g.y0 = y0 > J.ry ? y0 : J.ry;
+    g.x1 = x1 < rx1 ? x1 : rx1;
+    g.y1 = y1 < ry1 ? y1 : ry1;
+    if (g.x1 < g.x0 || g.y1 < g.y0) return false;
+    g.d01x = g.t0x - g.t1x; g.d01y = g.t0y - g.t1y;
+    g.d12x = g.t1x - g.t2x; g.d12y = g.t1y - g.t2y;
+    g.d20x = g.t2x - g.t0x; g.d20y = g.t2y - g.t0y;
+    g.area = g.d01x * g.d20y - g.d20x * g.d01y;
+    return g.area >= FLT_EPS_;
+}
+
+// Texel (x, y)'s jittered sample point against the triangle (CoreRef.cpp:573-585):
+// the unnormalised barycentrics and whether all are >= -FLT_EPS.
+__device__ __forceinline__ bool geo_cover(const FrameJob &J, const GeoTri &g, int x, int y, int hi, float &u, float &v, float &w) {
+    const int index = y * J.w + x;
+    const int hash_val = hash_i(index);
+    const float sx = (float)x + frac_modf(__ldg(J.halton + hi + 0) + construct_float((uint32_t)hash_val));
+    const float sy = (float)y + frac_modf(__ldg(J.halton + hi + 1) + construct_float((uint32_t)hash_i(hash_val)));
+    u = g.d01x * (sy - g.t0y) - g.d01y * (sx - g.t0x);
+    v = g.d12x * (sy - g.t1y) - g.d12y * (sx - g.t1x);
+    w = g.d20x * (sy - g.t2y) - g.d20y * (sx - g.t2x);
+    return u >= -FLT_EPS_ && v >= -FLT_EPS_ && w >= -FLT_EPS_;
+}
+
+constexpr int GEO_BLOCK = 256;
+
+// One warp per triangle of job blockIdx.y's mesh; best (one per ray of the
+// launch, all ones beforehand) takes the smallest covering triangle.
+__global__ void __launch_bounds__(GEO_BLOCK) k_geo_cover(const FrameJob *__restrict__ jobs, int sample, uint32_t *__restrict__ best) {
+    const FrameJob &J = jobs[blockIdx.y];
+    if (!J.geo.on) return;
+    const uint32_t t = (blockIdx.x * GEO_BLOCK + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
+    if (t >= J.geo.ntri) return;
+    const uint32_t tri = J.geo.tri0 + t;
+    GeoTri g;
+    if (!geo_setup(J, tri, g)) return;
+    const int hi = ((J.pi.iteration + sample) & (HALTON_SEQ_LEN - 1)) * HALTON_COUNT;
+    const uint32_t nx = (uint32_t)(g.x1 - g.x0 + 1), n = nx * (uint32_t)(g.y1 - g.y0 + 1);
+    for (uint32_t k = lane; k < n; k += 32u) {
+        const int x = g.x0 + (int)(k % nx), y = g.y0 + (int)(k / nx);
+        float u, v, w;
+        if (geo_cover(J, g, x, y, hi, u, v, w))
+            atomicMin(best + J.pixel_base + (uint32_t)(y - J.ry) * (uint32_t)J.rw + (uint32_t)(x - J.rx), tri);
+    }
+}
+
+// The camera ray and hit of every texel of the Geo jobs (CoreRef.cpp:510-521,
+// 587-600): a covered texel's surface point p and normal n (interpolated,
+// transformed, not normalised) give the ray o = p + n, d = -n and the hit
+// (triangle, instance, t = 1, u = w, v = u); an uncovered texel is a miss
+// along d = 0. Both with colour 1 and zero differentials.
+__global__ void k_geo_rays(const FrameJob *__restrict__ jobs, int n_jobs, uint32_t total, int sample, const uint32_t *__restrict__ best,
+                           float4 *__restrict__ rays, RayPayload *__restrict__ pay, float4 *__restrict__ hits, int32_t *__restrict__ obj) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const FrameJob &J = jobs[job_of(jobs, n_jobs, i)];
+    if (!J.geo.on) return;
+    const uint32_t li = i - J.pixel_base;
+    const int x = J.rx + (int)(li % (uint32_t)J.rw), y = J.ry + (int)(li / (uint32_t)J.rw);
+    const uint32_t tri = best[i];
+    float4 r0 = make_float4(0.0f, 0.0f, 0.0f, MAX_DIST), r1 = make_float4(0.0f, 0.0f, 0.0f, __int_as_float((x << 16) | y));
+    float4 hit = make_float4(__int_as_float(-1), MAX_DIST, 0.0f, 0.0f);
+    int32_t ob = -1;
+    GeoTri g;
+    if (tri != 0xffffffffu && geo_setup(J, tri, g)) {
+        const int hi = ((J.pi.iteration + sample) & (HALTON_SEQ_LEN - 1)) * HALTON_COUNT;
+        float u, v, w;
+        geo_cover(J, g, x, y, hi, u, v, w);
+        const float inv_area = 1.0f / g.area;
+        u *= inv_area;
+        v *= inv_area;
+        w *= inv_area;
+        VertexRec a, b, c;
+        load_vertex(J.sc, J.sc.vtx_indices[tri * 3u + 0], a);
+        load_vertex(J.sc, J.sc.vtx_indices[tri * 3u + 1], b);
+        load_vertex(J.sc, J.sc.vtx_indices[tri * 3u + 2], c);
+        float pl[3], nl[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            pl[q] = a.p[q] * v + b.p[q] * w + c.p[q] * u;
+            nl[q] = a.n[q] * v + b.n[q] * w + c.n[q] * u;
+        }
+        const float *xf = J.geo.xf; // TransformPoint, CoreRef.cpp:1619-1623
+        float p[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) p[q] = xf[4 * q + 0] * pl[0] + xf[4 * q + 1] * pl[1] + xf[4 * q + 2] * pl[2] + xf[4 * q + 3];
+        const V3 n = transform_normal(V3{nl[0], nl[1], nl[2]}, J.geo.inv);
+        r0 = make_float4(p[0] + n.x, p[1] + n.y, p[2] + n.z, MAX_DIST);
+        r1.x = -n.x;
+        r1.y = -n.y;
+        r1.z = -n.z;
+        hit = make_float4(__uint_as_float(tri), 1.0f, w, u);
+        ob = (int32_t)J.geo.obj;
+    }
+    rays[2ull * i] = r0;
+    rays[2ull * i + 1] = r1;
+    RayPayload pl;
+    pl.c[0] = pl.c[1] = pl.c[2] = 1.0f;
+    pl.ior = 1.0f;
+#pragma unroll
+    for (int q = 0; q < 3; q++) pl.do_dx[q] = pl.dd_dx[q] = pl.do_dy[q] = pl.dd_dy[q] = 0.0f;
+    pl.ray_depth = 0;
+    pl.pad[0] = pl.pad[1] = pl.pad[2] = 0;
+    pay[i] = pl;
+    hits[i] = hit;
+    obj[i] = ob;
 }
 
 // Shading of *in_count rays of any jobs (bounce: pass_info_t::bounce, 2 for
@@ -1443,6 +1607,20 @@ cudaError_t launch_raygen_jobs(const FrameJob *jobs, int n_jobs, uint32_t total,
                                uint32_t *ray_job, uint32_t *count, cudaStream_t st) {
     if (total == 0) return cudaSuccess;
     k_raygen_jobs<<<(total + 255) / 256, 256, 0, st>>>(jobs, n_jobs, total, sample, rays, pay, ray_job, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_geo_cover(const FrameJob *jobs, int n_jobs, uint32_t max_tris, int sample, uint32_t *best, cudaStream_t st) {
+    if (max_tris == 0 || n_jobs == 0) return cudaSuccess;
+    const uint64_t threads = (uint64_t)max_tris * 32u;
+    k_geo_cover<<<dim3((unsigned)((threads + GEO_BLOCK - 1) / GEO_BLOCK), (unsigned)n_jobs), GEO_BLOCK, 0, st>>>(jobs, sample, best);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_geo_rays(const FrameJob *jobs, int n_jobs, uint32_t total, int sample, const uint32_t *best, float4 *rays, RayPayload *pay,
+                            float4 *hits, int32_t *obj, cudaStream_t st) {
+    if (total == 0) return cudaSuccess;
+    k_geo_rays<<<(total + 255) / 256, 256, 0, st>>>(jobs, n_jobs, total, sample, best, rays, pay, hits, obj);
     return cudaGetLastError();
 }
 

@@ -135,6 +135,7 @@ struct ray_renderer {
     std::vector<ray_pixel> host_pixels;
     std::vector<ray_shl1> host_sh;
     rg::DeviceBuf d_sort_scratch, d_loop_sort;
+    rg::DeviceBuf d_geo_best; // Geo cameras: the covering triangle per texel
 
     // framebuffers (w * h): the sample being accumulated, the running mean,
     // the toned output; spherical-harmonics data when a camera asks for it

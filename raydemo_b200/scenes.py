@@ -201,6 +201,32 @@ def cornell_box(seed: int = 0, w: int = 256, h: int = 256, max_bounces: int = 4)
     return spec
 
 
+def lightmap_box(seed: int = 0, res: int = 128, max_bounces: int = 4, overlap: bool = False) -> dict:
+    """The Cornell box of `seed` baked to a lightmap: a Geo camera on the room
+    instance (walls, boxes and light, 18 quads) whose second UV layer packs
+    each quad into its own cell of a 5 x 4 atlas over a res x res framebuffer
+    (5 % margins, so texels between cells stay uncovered and show the
+    background). overlap: the two boxes' twelve faces share one cell (the
+    first triangle in mesh order takes each texel). The environment is a dim
+    grey, the paths up to max_bounces long."""
+    spec = cornell_box(seed, res, res, max_bounces)
+    attrs, idx, shapes, _ = spec["meshes"][0]
+    n_quads = len(attrs) // 4
+    uv1 = np.zeros((len(attrs), 2), np.float32)
+    m = 0.05
+    for q in range(n_quads):
+        cell = 5 if overlap and 5 <= q < 17 else q
+        col, row = cell % 5, cell // 5
+        for k in range(4):
+            u, v = attrs[4 * q + k, 6:8]
+            uv1[4 * q + k] = ((col + m + u * (1 - 2 * m)) / 5.0, (row + m + v * (1 - 2 * m)) / 4.0)
+    spec["meshes"][0] = (np.concatenate([attrs, uv1], axis=1).astype(np.float32), idx, shapes, 1)
+    spec["env"] = {"env_col": (0.1, 0.1, 0.1)}
+    spec["camera"] = {"type": 2, "mi_index": 0, "uv_index": 1, "gamma": 1.0, "max_total_depth": max_bounces,
+                      "max_diff_depth": max_bounces, "termination_start_depth": max_bounces}
+    return spec
+
+
 def spec_triangles(spec: dict) -> int:
     return int(sum(len(m[1]) // 3 for m in spec["meshes"]))
 
