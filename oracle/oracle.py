@@ -362,6 +362,43 @@ class RefLib:
         L.rb_get_sh.restype = C.c_int
         L.rb_get_stats.argtypes = [vp, vp]
         L.rb_clear.argtypes = [vp]
+        self.has_loader = hasattr(L, "rb_load_scene")
+        if self.has_loader:  # the demo's scene loader (src/DemoLib/load/Load.cpp), when built
+            L.rb_load_scene.argtypes = [vp, C.c_char_p]
+            L.rb_load_scene.restype = vp
+            L.rb_loaded_free.argtypes = [vp]
+            L.rb_render_loaded.argtypes = [vp, vp, i32, i32]
+            L.rb_loaded_camera.argtypes = [vp, C.POINTER(RbCameraDesc)]
+            L.rb_loaded_environment.argtypes = [vp, vp, vp, vp]
+            L.rb_loaded_triangles.argtypes = [vp]
+            L.rb_loaded_triangles.restype = u32
+            L.rb_loaded_instance_xform.argtypes = [vp, u32, vp]
+            L.rb_loaded_instance_xform.restype = i32
+            L.rb_load_image.argtypes = [C.c_char_p, i32, C.POINTER(i32), C.POINTER(i32), vp, sz]
+            L.rb_load_image.restype = C.c_longlong
+            L.rb_load_mesh.argtypes = [C.c_char_p, i32, vp, sz, vp, sz, vp, sz, vp]
+            L.rb_load_mesh.restype = i32
+
+    def load_image(self, path: str, hdr: bool = False):
+        """Load_stb_image / LoadHDR of the reference: (h, w, 4) uint8, or None on error."""
+        w, h = C.c_int32(), C.c_int32()
+        n = self.lib.rb_load_image(path.encode(), int(hdr), C.byref(w), C.byref(h), None, 0)
+        if n < 0:
+            return None
+        out = np.zeros((h.value, w.value, 4), np.uint8)
+        self.lib.rb_load_image(path.encode(), int(hdr), C.byref(w), C.byref(h), _p(out), out.nbytes)
+        return out
+
+    def load_mesh(self, path: str, bin: bool = False):
+        """LoadOBJ / LoadBIN of the reference: (attrs (n, 8) float32, indices, groups), or None."""
+        sizes = np.zeros(3, np.uint64)
+        if self.lib.rb_load_mesh(path.encode(), int(bin), None, 0, None, 0, None, 0, _p(sizes)) != 0:
+            return None
+        a = np.zeros(int(sizes[0]), np.float32)
+        i = np.zeros(int(sizes[1]), np.uint32)
+        g = np.zeros(int(sizes[2]), np.uint32)
+        self.lib.rb_load_mesh(path.encode(), int(bin), _p(a), a.size, _p(i), i.size, _p(g), g.size, _p(sizes))
+        return a.reshape(-1, 8), i, g
 
     def halton_table(self, iteration: int) -> np.ndarray:
         out = np.zeros(24 * 256, np.float32)
@@ -388,6 +425,46 @@ class RefLib:
         out = np.zeros(rw * rh, PACKET_DTYPE)
         self.lib.rb_generate_primary_rays(C.byref(cam), iteration, x, y, rw, rh, w, h, _p(halton), _p(out))
         return out
+
+
+class RefLoadedScene:
+    """A scene made by the reference's LoadScene (Load.cpp:22) on a Ref renderer
+    from JSON text (paths relative to the working directory); .ok is False
+    where LoadScene returned null."""
+
+    def __init__(self, renderer: "RefRenderer", json_text: str):
+        self.ref = renderer.ref
+        self.h = self.ref.lib.rb_load_scene(renderer.r, json_text.encode())
+        self.ok = bool(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.ref.lib.rb_loaded_free(self.h)
+            self.h = None
+
+    def camera(self) -> "RbCameraDesc":
+        d = RbCameraDesc()
+        self.ref.lib.rb_loaded_camera(self.h, C.byref(d))
+        return d
+
+    def environment(self):
+        col = np.zeros(3, np.float32)
+        clamp = np.zeros(1, np.float32)
+        env_map = np.zeros(1, np.uint32)
+        self.ref.lib.rb_loaded_environment(self.h, _p(col), _p(clamp), _p(env_map))
+        return col, float(clamp[0]), int(env_map[0])
+
+    def triangle_count(self) -> int:
+        return self.ref.lib.rb_loaded_triangles(self.h)
+
+    def instance_xforms(self) -> list:
+        out, i = [], 0
+        while True:
+            x = np.zeros(16, np.float32)
+            if not self.ref.lib.rb_loaded_instance_xform(self.h, i, _p(x)):
+                return out
+            out.append(x)
+            i += 1
 
 
 class RefScene:
@@ -476,6 +553,9 @@ class RefRenderer:
         out = np.zeros((self.h, self.w, 4), np.float32)
         self.ref.lib.rb_get_pixels(self.r, _p(out))
         return out
+
+    def render_loaded(self, scene: RefLoadedScene, iterations: int, nthreads: int = 1):
+        self.ref.lib.rb_render_loaded(self.r, scene.h, iterations, nthreads)
 
     def sh_data(self):
         """get_sh_data_ref: (h, w, 12) float32, or None."""

@@ -20,6 +20,13 @@
 #include <thread>
 #include <vector>
 
+#ifdef RB_WITH_LOADER
+#include <sstream>
+#include <string>
+
+#include "load/Load.h"
+#endif
+
 #include "Ray/RendererFactory.h"
 #include "Ray/internal/Halton.h"
 #include "Ray/internal/RendererAVX2.h"
@@ -40,6 +47,7 @@ struct SceneAccess : public Ray::Ref::Scene {
     const Ray::tri_accel_t *tris() const { return tris_.empty() ? nullptr : tris_.data(); }
     const uint32_t *tri_indices() const { return tri_indices_.empty() ? nullptr : tri_indices_.data(); }
     size_t ntris() const { return tris_.size(); }
+    size_t ninst() const { return mesh_instances_.size(); }
 };
 
 struct RendererHandle {
@@ -364,11 +372,18 @@ void rb_renderer_free(void *r) { delete static_cast<RendererHandle *>(r); }
 
 int rb_renderer_type(void *r) { return (int)static_cast<RendererHandle *>(r)->r->type(); }
 
+static void render_scene(RendererHandle *rh, const std::shared_ptr<Ray::SceneBase> &sp, int iterations, int rx, int ry, int rw, int rh_,
+                         int reset, int nthreads);
+
 // Renders `iterations` samples over `rect` (w == 0 -> whole image) with one
 // RegionContext kept across calls; reset != 0 starts a new context.
 void rb_render(void *r, void *s, int iterations, int rx, int ry, int rw, int rh_, int reset, int nthreads) {
-    auto *rh = static_cast<RendererHandle *>(r);
-    std::shared_ptr<Ray::SceneBase> sp = *static_cast<std::shared_ptr<SceneAccess> *>(s);
+    render_scene(static_cast<RendererHandle *>(r), *static_cast<std::shared_ptr<SceneAccess> *>(s), iterations, rx, ry, rw, rh_, reset,
+                 nthreads);
+}
+
+static void render_scene(RendererHandle *rh, const std::shared_ptr<Ray::SceneBase> &sp, int iterations, int rx, int ry, int rw, int rh_,
+                         int reset, int nthreads) {
     if (nthreads <= 1) {
         if (reset || !rh->region) rh->region.reset(new Ray::RegionContext(Ray::rect_t{rx, ry, rw, rh_}));
         for (int i = 0; i < iterations; i++) rh->r->RenderScene(sp, *rh->region);
@@ -410,4 +425,107 @@ void rb_get_stats(void *r, unsigned long long *out6) {
 }
 
 void rb_clear(void *r) { static_cast<RendererHandle *>(r)->r->Clear({0, 0, 0, 0}); }
+
+#ifdef RB_WITH_LOADER
+// ---- the demo's scene loader (src/DemoLib/load/Load.cpp) and its file readers
+
+// LoadScene (Load.cpp:22-417) on renderer r from JSON text, file paths relative
+// to the working directory. Null where the JSON does not parse or LoadScene
+// returns null (its own parse errors).
+void *rb_load_scene(void *r, const char *json) {
+    JsObject js;
+    std::stringstream ss{std::string(json)};
+    if (!js.Read(ss)) return nullptr;
+    std::shared_ptr<Ray::SceneBase> sc;
+    try {
+        sc = LoadScene(static_cast<RendererHandle *>(r)->r.get(), js);
+    } catch (...) {
+        return nullptr;
+    }
+    return sc ? new std::shared_ptr<Ray::SceneBase>(sc) : nullptr;
+}
+
+void rb_loaded_free(void *s) { delete static_cast<std::shared_ptr<Ray::SceneBase> *>(s); }
+
+void rb_render_loaded(void *r, void *s, int iterations, int nthreads) {
+    render_scene(static_cast<RendererHandle *>(r), *static_cast<std::shared_ptr<Ray::SceneBase> *>(s), iterations, 0, 0, 0, 0, 1, nthreads);
+}
+
+static Ray::SceneBase *L(void *s) { return static_cast<std::shared_ptr<Ray::SceneBase> *>(s)->get(); }
+
+// The loaded scene's current camera (GetCamera), environment and counts.
+void rb_loaded_camera(void *s, rb_camera_desc *d) {
+    Ray::camera_desc_t c;
+    L(s)->GetCamera(L(s)->current_cam(), c);
+    d->type = c.type;
+    d->filter = c.filter;
+    d->dtype = c.dtype;
+    memcpy(d->origin, c.origin, sizeof(d->origin));
+    memcpy(d->fwd, c.fwd, sizeof(d->fwd));
+    memcpy(d->up, c.up, sizeof(d->up));
+    d->fov = c.fov;
+    d->gamma = c.gamma;
+    d->focus_distance = c.focus_distance;
+    d->focus_factor = c.focus_factor;
+    d->clamp = c.clamp;
+    d->max_diff_depth = c.max_diff_depth;
+    d->max_glossy_depth = c.max_glossy_depth;
+    d->max_refr_depth = c.max_refr_depth;
+    d->max_transp_depth = c.max_transp_depth;
+    d->max_total_depth = c.max_total_depth;
+    d->termination_start_depth = c.termination_start_depth;
+}
+
+void rb_loaded_environment(void *s, float *env_col, float *env_clamp, uint32_t *env_map) {
+    Ray::environment_desc_t e;
+    L(s)->GetEnvironment(e);
+    memcpy(env_col, e.env_col, 3 * sizeof(float));
+    *env_clamp = e.env_clamp;
+    *env_map = e.env_map;
+}
+
+uint32_t rb_loaded_triangles(void *s) { return L(s)->triangle_count(); }
+
+// The transform of mesh instance i (the Ref renderer's scene type); 0 past the last.
+int rb_loaded_instance_xform(void *s, uint32_t i, float *out16) {
+    const SceneAccess *a = static_cast<const SceneAccess *>(static_cast<const Ray::Ref::Scene *>(L(s)));
+    if (i >= a->ninst()) return 0;
+    memcpy(out16, a->transforms()[a->mesh_instances()[i].tr_index].xform, 16 * sizeof(float));
+    return 1;
+}
+
+// Load_stb_image (Load.cpp:813-831), or LoadHDR (Load.cpp:679-811) with hdr != 0:
+// w * h RGBA8 texels into out when cap allows; returns w * h, or -1 on error.
+long long rb_load_image(const char *path, int hdr, int *w, int *h, uint8_t *out, size_t cap) {
+    std::vector<Ray::pixel_color8_t> px;
+    try {
+        px = hdr ? LoadHDR(path, *w, *h) : Load_stb_image(path, *w, *h);
+    } catch (...) {
+        return -1;
+    }
+    const size_t n = (size_t)(*w) * (*h);
+    if (out && cap >= 4 * n && px.size() >= n) memcpy(out, px.data(), 4 * n);
+    return (long long)n;
+}
+
+// LoadOBJ (Load.cpp:515-634) or LoadBIN (Load.cpp:636-658): the three arrays'
+// sizes into sizes[3] and, when the capacities allow, the arrays.
+int rb_load_mesh(const char *path, int bin, float *attrs, size_t attrs_cap, uint32_t *idx, size_t idx_cap, uint32_t *groups,
+                 size_t groups_cap, size_t *sizes) {
+    std::vector<float> a;
+    std::vector<unsigned> i, g;
+    try {
+        std::tie(a, i, g) = bin ? LoadBIN(path) : LoadOBJ(path);
+    } catch (...) {
+        return -1;
+    }
+    sizes[0] = a.size();
+    sizes[1] = i.size();
+    sizes[2] = g.size();
+    if (attrs && attrs_cap >= a.size() && !a.empty()) memcpy(attrs, a.data(), a.size() * sizeof(float));
+    if (idx && idx_cap >= i.size() && !i.empty()) memcpy(idx, i.data(), i.size() * sizeof(uint32_t));
+    if (groups && groups_cap >= g.size() && !g.empty()) memcpy(groups, g.data(), g.size() * sizeof(uint32_t));
+    return 0;
+}
+#endif
 }

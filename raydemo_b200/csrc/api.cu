@@ -742,15 +742,17 @@ int ray_scene_add_camera(ray_scene *s, const ray_camera_desc *c, uint32_t *out_i
 int ray_scene_get_camera(ray_scene *s, uint32_t i, ray_camera_desc *out) {
     RG_CHECK(s && out && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");
     // SceneBase::GetCamera, SceneBase.cpp:22-54: the fields of the camera's kind only
-    const ray_camera_desc &d = s->cameras[i].desc;
+    // (origin, fwd and up of the constructed camera_t: up is the orthonormalised one)
+    const CameraRec &rec = s->cameras[i];
+    const ray_camera_desc &d = rec.desc;
     out->type = d.type;
     out->dtype = d.dtype;
     out->gamma = d.gamma;
     if (d.type != RAY_CAM_GEO) {
         out->filter = d.filter;
-        memcpy(out->origin, d.origin, sizeof(out->origin));
-        memcpy(out->fwd, d.fwd, sizeof(out->fwd));
-        memcpy(out->up, d.up, sizeof(out->up));
+        memcpy(out->origin, rec.origin, sizeof(out->origin));
+        memcpy(out->fwd, rec.fwd, sizeof(out->fwd));
+        memcpy(out->up, rec.up, sizeof(out->up));
         out->fov = d.fov;
         out->focus_distance = d.focus_distance;
         out->focus_factor = d.focus_factor;
