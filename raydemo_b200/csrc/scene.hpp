@@ -122,6 +122,10 @@ struct ray_scene {
     ray_trace_info last_info{};
     bool info_pending = false;
     cudaStream_t info_stream = nullptr;
+    // host-buffer traces: the chunk pipeline's upload, download and second trace
+    // streams and its events (created on first use)
+    cudaStream_t copy_st[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t pipe_ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
     ~ray_scene();
 };

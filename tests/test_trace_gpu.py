@@ -223,6 +223,39 @@ def test_device_path_matches_host_path(renderer):
     assert np.array_equal(hd.cpu().numpy().view(np.uint32), host.view(np.float32).reshape(-1, 4).view(np.uint32))
 
 
+@pytest.mark.parametrize("n", [262144, 1000003, 3 * 262144 + 17, 2097157])
+def test_pinned_host_pipeline_matches_device_path(renderer, n):
+    """Host buffers in page-locked memory go through the chunk pipeline (uploads,
+    traces and downloads of different chunks overlapping on three streams): the
+    hits and instance ids equal the device path's bit for bit, one chunk or many,
+    on two calls in a row."""
+    import torch
+    from raydemo_b200 import capi
+
+    tris = scenes.random_triangles(200000, seed=73, mean_edge=0.006)
+    rays = scenes.incoherent_rays(n, seed=74)
+    sc = _scene(tris, renderer, instances=2)
+    rd = torch.from_numpy(rays).cuda()
+    hd = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    od = torch.empty(n, dtype=torch.int32, device="cuda")
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        sc.trace_closest_device(rd.data_ptr(), n, hd.data_ptr(), od.data_ptr(), s.cuda_stream)
+    s.synchronize()
+    rays_h = torch.from_numpy(rays).pin_memory()
+    for with_obj in (False, True):
+        for _ in range(2):
+            hits_h = torch.full((n, 4), -7.0).pin_memory()
+            obj_h = torch.full((n,), -7, dtype=torch.int32).pin_memory()
+            capi.check(capi.lib().ray_scene_trace_closest(sc.handle, rays_h.data_ptr(), n, hits_h.data_ptr(),
+                                                          obj_h.data_ptr() if with_obj else None, capi.RAY_MEM_HOST,
+                                                          s.cuda_stream))
+            assert np.array_equal(hits_h.numpy().view(np.uint32), hd.cpu().numpy().view(np.uint32))
+            if with_obj:
+                assert np.array_equal(obj_h.numpy(), od.cpu().numpy())
+    assert sc.last_trace_info().error_flags == 0
+
+
 def test_full_size_microbench_subset(renderer, oracle):
     """The 2,097,152-triangle scene: all 4,194,304 rays traced on the GPU,
     a seeded subset checked against the oracle, plus size-independent
