@@ -173,10 +173,30 @@ static void set_camera(CameraRec &rec, const ray_camera_desc &c) {
     d.termination_start_depth = c.termination_start_depth;
 }
 
+cudaError_t note_use(ray_scene *s, cudaStream_t st) {
+    for (auto &u : s->users)
+        if (u.first == st) return cudaEventRecord(u.second, st);
+    if (s->users.size() >= 8) { // a short list: the oldest user's wait goes onto the scene's stream now
+        cudaError_t e = cudaStreamWaitEvent(s->stream, s->users.front().second, 0);
+        if (e != cudaSuccess) return e;
+        cudaEventDestroy(s->users.front().second);
+        s->users.erase(s->users.begin());
+    }
+    cudaEvent_t ev = nullptr;
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+    s->users.emplace_back(st, ev);
+    return cudaEventRecord(ev, st);
+}
+
 int commit(ray_scene *s) {
-    if (!s->geom_dirty) return upload_shading(s);
+    if (!s->geom_dirty && !s->inst_dirty && !s->shade_dirty) return RAY_OK;
     RG_CUDA_TRY(cudaSetDevice(s->device));
     cudaStream_t st = s->stream;
+    // the frames and traces in flight read the arrays about to be rewritten
+    for (auto &u : s->users) RG_CUDA_TRY(cudaStreamWaitEvent(st, u.second, 0));
+    if (!s->geom_dirty && !s->inst_dirty) return upload_shading(s);
+    if (s->geom_dirty) {
     // 1. build the meshes that have no BVH yet
     for (MeshRec &m : s->meshes) {
         if (m.built) continue;
@@ -214,7 +234,9 @@ int commit(ray_scene *s) {
     RG_CUDA_TRY(s->d_nodes.ensure(nodes * sizeof(WideNode)));
     RG_CUDA_TRY(s->d_leaf.ensure(tris * sizeof(TriRec)));
     RG_CUDA_TRY(s->d_tris_ref.ensure(tris * sizeof(TriRec)));
-    std::vector<uint32_t> node_base(s->meshes.size()), tri_base(s->meshes.size());
+    std::vector<uint32_t> &node_base = s->node_base, &tri_base = s->tri_base;
+    node_base.assign(s->meshes.size(), 0);
+    tri_base.assign(s->meshes.size(), 0);
     uint64_t nb = 0, tb = 0;
     for (size_t i = 0; i < s->meshes.size(); i++) {
         const MeshRec &m = s->meshes[i];
@@ -231,7 +253,14 @@ int commit(ray_scene *s) {
         nb += m.bvh.node_count;
         tb += m.bvh.tri_count;
     }
-    // 3. instances (SetMeshInstanceTransform, SceneRef.cpp:370-414)
+    s->total_nodes = (uint32_t)nodes;
+    s->max_depth = 0;
+    for (const MeshRec &m : s->meshes) s->max_depth = std::max(s->max_depth, m.bvh.depth);
+    }
+    // 3. instances (SetMeshInstanceTransform, SceneRef.cpp:370-414). The
+    // instance level is a list the traversal tests box by box, so a moved
+    // instance costs this upload of its record and no rebuild.
+    const std::vector<uint32_t> &node_base = s->node_base, &tri_base = s->tri_base;
     std::vector<InstanceRec> inst;
     for (const InstanceRecHost &ih : s->instances) {
         const MeshRec &m = s->meshes[ih.mesh];
@@ -270,10 +299,7 @@ int commit(ray_scene *s) {
             s->world_max[k] = std::max(s->world_max[k], q.bbox_max[k]);
         }
     RG_CUDA_TRY(cudaStreamSynchronize(st));
-    s->total_nodes = (uint32_t)nodes;
-    s->max_depth = 0;
-    for (const MeshRec &m : s->meshes) s->max_depth = std::max(s->max_depth, m.bvh.depth);
-    s->geom_dirty = false;
+    s->geom_dirty = s->inst_dirty = false;
     return upload_shading(s);
 }
 
@@ -312,6 +338,7 @@ ray_scene::~ray_scene() {
         if (c) cudaStreamDestroy(c);
     for (cudaEvent_t e : pipe_ev)
         if (e) cudaEventDestroy(e);
+    for (auto &u : users) cudaEventDestroy(u.second);
 }
 
 extern "C" {
@@ -703,7 +730,7 @@ int ray_scene_add_mesh_instance(ray_scene *s, uint32_t mesh_index, const float x
     memcpy(ih.xform, xform, 64);
     inverse_matrix(ih.xform, ih.inv_xform);
     s->instances.push_back(ih);
-    s->geom_dirty = true;
+    s->inst_dirty = true;
     *out_index = (uint32_t)(s->instances.size() - 1);
     return RAY_OK;
     RG_GUARD_END
@@ -713,14 +740,14 @@ int ray_scene_set_mesh_instance_transform(ray_scene *s, uint32_t mi, const float
     RG_CHECK(s && xform && mi < s->instances.size(), "invalid instance");
     memcpy(s->instances[mi].xform, xform, 64);
     inverse_matrix(s->instances[mi].xform, s->instances[mi].inv_xform);
-    s->geom_dirty = true;
+    s->inst_dirty = true;
     return RAY_OK;
 }
 
 int ray_scene_remove_mesh_instance(ray_scene *s, uint32_t mi) {
     RG_CHECK(s && mi < s->instances.size(), "invalid instance");
     s->instances.erase(s->instances.begin() + mi);
-    s->geom_dirty = true;
+    s->inst_dirty = true;
     return RAY_OK;
 }
 
@@ -1019,6 +1046,7 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
         RG_CUDA_TRY(cudaEventRecord(s->pipe_ev[3], down));
         RG_CUDA_TRY(cudaStreamWaitEvent(st, s->pipe_ev[3], 0));
     }
+    RG_CUDA_TRY(note_use(s, st));
     s->info_pending = true;
     s->info_stream = st;
     if (mem == RAY_MEM_HOST) {

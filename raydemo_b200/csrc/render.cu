@@ -760,6 +760,7 @@ int ray_render(ray_renderer *r, ray_scene *s, ray_region *region) {
             if (rc != RAY_OK) return rc;
         }
         RG_CUDA_TRY(cudaEventRecord(ev[N_EVENTS - 1], st));
+        RG_CUDA_TRY(note_use(s, st));
         r->ev_bounces[set] = nb;
         r->ev_tune[set] = plan.tune_entry;
         r->ev_kernel[set] = kern;
@@ -875,6 +876,8 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
                 }
             }
             // and each renderer's later work (reads of its pixels, its next frames) after the batch
+            for (int i = 0; i < count; i++)
+                if (scenes[i]->device == r0->device) RG_CUDA_TRY(note_use(scenes[i], st));
             RG_CUDA_TRY(cudaEventRecord(r0->ev_sync, st));
             for (int i = 0; i < count; i++) {
                 ray_renderer *r = renderers[i];
@@ -929,6 +932,7 @@ int ray_render_diff(ray_renderer *r, ray_scene *s, int first_iteration, int samp
                            false);
         if (rc != RAY_OK) return rc;
         RG_CUDA_TRY(launch_diff_collect(d_jobs, samples, n_pix, image_rgb, sample_rgb, st));
+        RG_CUDA_TRY(note_use(s, st));
         r->last_kernel = 1;
         r->last_sort_mask = 0;
         return RAY_OK;
@@ -978,8 +982,11 @@ int ray_render_adjoint(ray_renderer *r, ray_scene *s, int first_iteration, int s
         uint32_t *cnt = static_cast<uint32_t *>(r->d_counters.p);
         RG_CUDA_TRY(cudaMemsetAsync(cnt, 0, 16 * sizeof(uint32_t), st));
         int nb = 0;
-        return run_wavefront(r, static_cast<const FrameJob *>(r->d_jobs.p), jobs, std::vector<const ray_scene *>(jobs.size(), s), total, 0, 0u,
-                             st, nullptr, nb, false, &adj);
+        rc = run_wavefront(r, static_cast<const FrameJob *>(r->d_jobs.p), jobs, std::vector<const ray_scene *>(jobs.size(), s), total, 0, 0u, st,
+                           nullptr, nb, false, &adj);
+        if (rc != RAY_OK) return rc;
+        RG_CUDA_TRY(note_use(s, st));
+        return RAY_OK;
     } catch (const std::bad_alloc &) {
         set_error("host allocation failed");
         return RAY_ERR_OUT_OF_MEMORY;

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/raygpu.h"
@@ -65,8 +66,11 @@ struct DeviceBuf {
     ~DeviceBuf() { release(); }
 };
 
-// api.cu: builds pending BVHs and uploads pending scene data
+// api.cu: builds pending BVHs and uploads pending scene data, after the
+// kernels already enqueued that read the arrays it overwrites
 int commit(ray_scene *s);
+// api.cu: records that work just enqueued on st reads the scene's device arrays
+cudaError_t note_use(ray_scene *s, cudaStream_t st);
 
 // scene_shading.cu
 int add_texture(ray_scene *s, const uint8_t *data, int w, int h, bool srgb, bool mips, uint32_t *out);
@@ -104,6 +108,11 @@ struct ray_scene {
     std::vector<uint32_t> vtx_indices;
 
     bool geom_dirty = true, shade_dirty = true;
+    bool inst_dirty = false;                      // instances added, moved or removed (meshes unchanged)
+    std::vector<uint32_t> node_base, tri_base;    // each mesh's offsets in the scene arrays (commit)
+    // the streams that read this scene's device arrays and an event after each's
+    // latest use: a commit's uploads wait for them (rg::note_use)
+    std::vector<std::pair<cudaStream_t, cudaEvent_t>> users;
     uint32_t total_tris = 0, total_nodes = 0, max_depth = 0;
     float world_min[3] = {0.0f, 0.0f, 0.0f}, world_max[3] = {0.0f, 0.0f, 0.0f}; // union of the instance boxes
     // differentiable parameters (caller-owned device arrays, ray_scene_set_diff_params)
