@@ -173,6 +173,11 @@ static void set_camera(CameraRec &rec, const ray_camera_desc &c) {
     d.termination_start_depth = c.termination_start_depth;
 }
 
+std::recursive_mutex &api_mutex() {
+    static std::recursive_mutex m;
+    return m;
+}
+
 cudaError_t note_use(ray_scene *s, cudaStream_t st) {
     for (auto &u : s->users)
         if (u.first == st) return cudaEventRecord(u.second, st);
@@ -347,6 +352,7 @@ const char *ray_last_error(void) { return g_last_error.c_str(); }
 int ray_version(void) { return 1; }
 
 int ray_create_renderer(const ray_settings *s, ray_renderer **out) {
+    RG_API_LOCK;
     RG_CHECK(s && out, "null argument");
     RG_CHECK(s->w > 0 && s->h > 0 && s->w <= 32768 && s->h <= 32768, "invalid framebuffer size");
     RG_GUARD_BEGIN
@@ -371,17 +377,20 @@ int ray_create_renderer(const ray_settings *s, ray_renderer **out) {
 }
 
 int ray_destroy_renderer(ray_renderer *r) {
+    RG_API_LOCK;
     delete r;
     return RAY_OK;
 }
 
 int ray_renderer_type(const ray_renderer *r, int *out_type) {
+    RG_API_LOCK;
     RG_CHECK(r && out_type, "null argument");
     *out_type = RAY_RENDERER_CUDA_SM100;
     return RAY_OK;
 }
 
 int ray_renderer_size(const ray_renderer *r, int *w, int *h) {
+    RG_API_LOCK;
     RG_CHECK(r && w && h, "null argument");
     *w = r->w;
     *h = r->h;
@@ -389,6 +398,7 @@ int ray_renderer_size(const ray_renderer *r, int *w, int *h) {
 }
 
 int ray_create_scene(ray_renderer *r, ray_scene **out) {
+    RG_API_LOCK;
     RG_CHECK(r && out, "null argument");
     RG_GUARD_BEGIN
     RG_CUDA_TRY(cudaSetDevice(r->device));
@@ -415,17 +425,20 @@ int ray_create_scene(ray_renderer *r, ray_scene **out) {
 }
 
 int ray_destroy_scene(ray_scene *s) {
+    RG_API_LOCK;
     delete s;
     return RAY_OK;
 }
 
 int ray_scene_get_environment(ray_scene *s, ray_environment_desc *out) {
+    RG_API_LOCK;
     RG_CHECK(s && out, "null argument");
     *out = s->env;
     return RAY_OK;
 }
 
 int ray_scene_set_environment(ray_scene *s, const ray_environment_desc *env) {
+    RG_API_LOCK;
     RG_CHECK(s && env, "null argument");
     s->env = *env;
     if (s->env.env_map == RAY_INVALID_INDEX) s->env.env_map = s->default_env_texture; // SceneRef.cpp:52-59
@@ -433,6 +446,7 @@ int ray_scene_set_environment(ray_scene *s, const ray_environment_desc *env) {
 }
 
 int ray_scene_add_texture(ray_scene *s, const ray_tex_desc *t, uint32_t *out_index) {
+    RG_API_LOCK;
     RG_CHECK(s && t && out_index, "null argument");
     RG_GUARD_BEGIN
     return add_texture(s, t->data, t->w, t->h, t->is_srgb != 0, t->generate_mipmaps != 0, out_index);
@@ -440,12 +454,14 @@ int ray_scene_add_texture(ray_scene *s, const ray_tex_desc *t, uint32_t *out_ind
 }
 
 int ray_scene_remove_texture(ray_scene *s, uint32_t i) {
+    RG_API_LOCK;
     RG_CHECK(s, "null argument");
     (void)i; // no-op in the reference too (SceneRef.h:84)
     return RAY_OK;
 }
 
 int ray_scene_add_material(ray_scene *s, const ray_mat_desc *m, uint32_t *out_index) {
+    RG_API_LOCK;
     RG_CHECK(s && m && out_index, "null argument");
     RG_CHECK((m->type >= RAY_MAT_DIFFUSE && m->type <= RAY_MAT_TRANSPARENT) || m->type == RAY_MAT_PRINCIPLED, "invalid material type");
     RG_CHECK(m->type != RAY_MAT_PRINCIPLED || (m->roughness >= 0.0f && m->roughness <= 1.0f && m->metallic >= 0.0f && m->metallic <= 1.0f),
@@ -482,6 +498,7 @@ int ray_scene_add_material(ray_scene *s, const ray_mat_desc *m, uint32_t *out_in
 }
 
 int ray_scene_set_diff_params(ray_scene *s, const ray_diff_params *p) {
+    RG_API_LOCK;
     RG_CHECK(s, "null scene");
     if (!p) {
         for (MaterialRec &m : s->materials)
@@ -521,12 +538,14 @@ int ray_scene_set_diff_params(ray_scene *s, const ray_diff_params *p) {
 }
 
 int ray_scene_remove_material(ray_scene *s, uint32_t i) {
+    RG_API_LOCK;
     RG_CHECK(s, "null argument");
     (void)i; // no-op in the reference too (SceneRef.h:87)
     return RAY_OK;
 }
 
 int ray_scene_add_mesh(ray_scene *s, const ray_mesh_desc *d, uint32_t *out_index) {
+    RG_API_LOCK;
     RG_CHECK(s && d && out_index, "null argument");
     RG_CHECK(d->prim_type == 0, "only indexed triangle lists are supported");
     RG_CHECK(d->layout >= RAY_LAYOUT_PNT && d->layout <= RAY_LAYOUT_PNBTT, "invalid vertex layout");
@@ -621,6 +640,7 @@ int ray_scene_add_mesh(ray_scene *s, const ray_mesh_desc *d, uint32_t *out_index
 }
 
 int ray_scene_remove_mesh(ray_scene *s, uint32_t i) {
+    RG_API_LOCK;
     RG_CHECK(s && i < s->meshes.size(), "invalid mesh index");
     RG_GUARD_BEGIN
     // RemoveMesh, SceneRef.cpp:263-303: swap with the last mesh, drop the
@@ -651,6 +671,7 @@ int ray_scene_remove_mesh(ray_scene *s, uint32_t i) {
 }
 
 int ray_scene_add_light(ray_scene *s, const ray_light_desc *d, uint32_t *out_index) {
+    RG_API_LOCK;
     RG_CHECK(s && d && out_index, "null argument");
     RG_CHECK(d->type >= RAY_LIGHT_POINT && d->type <= RAY_LIGHT_SUN, "invalid light type");
     RG_GUARD_BEGIN
@@ -716,12 +737,14 @@ int ray_scene_add_light(ray_scene *s, const ray_light_desc *d, uint32_t *out_ind
 }
 
 int ray_scene_remove_light(ray_scene *s, uint32_t i) {
+    RG_API_LOCK;
     RG_CHECK(s, "null argument");
     (void)i; // a no-op in the reference (SceneRef.cpp:351-354)
     return RAY_OK;
 }
 
 int ray_scene_add_mesh_instance(ray_scene *s, uint32_t mesh_index, const float xform[16], uint32_t *out_index) {
+    RG_API_LOCK;
     RG_CHECK(s && xform && out_index, "null argument");
     RG_CHECK(mesh_index < s->meshes.size(), "invalid mesh index");
     RG_GUARD_BEGIN
@@ -737,6 +760,7 @@ int ray_scene_add_mesh_instance(ray_scene *s, uint32_t mesh_index, const float x
 }
 
 int ray_scene_set_mesh_instance_transform(ray_scene *s, uint32_t mi, const float xform[16]) {
+    RG_API_LOCK;
     RG_CHECK(s && xform && mi < s->instances.size(), "invalid instance");
     memcpy(s->instances[mi].xform, xform, 64);
     inverse_matrix(s->instances[mi].xform, s->instances[mi].inv_xform);
@@ -745,6 +769,7 @@ int ray_scene_set_mesh_instance_transform(ray_scene *s, uint32_t mi, const float
 }
 
 int ray_scene_remove_mesh_instance(ray_scene *s, uint32_t mi) {
+    RG_API_LOCK;
     RG_CHECK(s && mi < s->instances.size(), "invalid instance");
     s->instances.erase(s->instances.begin() + mi);
     s->inst_dirty = true;
@@ -752,6 +777,7 @@ int ray_scene_remove_mesh_instance(ray_scene *s, uint32_t mi) {
 }
 
 int ray_scene_add_camera(ray_scene *s, const ray_camera_desc *c, uint32_t *out_index) {
+    RG_API_LOCK;
     RG_CHECK(s && c && out_index, "null argument");
     RG_GUARD_BEGIN
     // SceneBase::AddCamera, SceneBase.cpp:8-20
@@ -772,6 +798,7 @@ int ray_scene_add_camera(ray_scene *s, const ray_camera_desc *c, uint32_t *out_i
 }
 
 int ray_scene_get_camera(ray_scene *s, uint32_t i, ray_camera_desc *out) {
+    RG_API_LOCK;
     RG_CHECK(s && out && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");
     // SceneBase::GetCamera, SceneBase.cpp:22-54: the fields of the camera's kind only
     // (origin, fwd and up of the constructed camera_t: up is the orthonormalised one)
@@ -809,12 +836,14 @@ int ray_scene_get_camera(ray_scene *s, uint32_t i, ray_camera_desc *out) {
 }
 
 int ray_scene_set_camera(ray_scene *s, uint32_t i, const ray_camera_desc *c) {
+    RG_API_LOCK;
     RG_CHECK(s && c && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");
     set_camera(s->cameras[i], *c);
     return RAY_OK;
 }
 
 int ray_scene_remove_camera(ray_scene *s, uint32_t i) {
+    RG_API_LOCK;
     RG_CHECK(s && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");
     s->cameras[i].alive = false;
     s->cameras[i].next_free = s->cam_first_free;
@@ -823,24 +852,28 @@ int ray_scene_remove_camera(ray_scene *s, uint32_t i) {
 }
 
 int ray_scene_current_cam(ray_scene *s, uint32_t *out) {
+    RG_API_LOCK;
     RG_CHECK(s && out, "null argument");
     *out = s->current_cam;
     return RAY_OK;
 }
 
 int ray_scene_set_current_cam(ray_scene *s, uint32_t i) {
+    RG_API_LOCK;
     RG_CHECK(s, "null argument");
     s->current_cam = i;
     return RAY_OK;
 }
 
 int ray_scene_triangle_count(ray_scene *s, uint32_t *out) {
+    RG_API_LOCK;
     RG_CHECK(s && out, "null argument");
     *out = s->total_tris;
     return RAY_OK;
 }
 
 int ray_scene_node_count(ray_scene *s, uint32_t *out) {
+    RG_API_LOCK;
     RG_CHECK(s && out, "null argument");
     RG_GUARD_BEGIN
     const int rc = commit(s);
@@ -851,6 +884,7 @@ int ray_scene_node_count(ray_scene *s, uint32_t *out) {
 }
 
 int ray_scene_commit(ray_scene *s) {
+    RG_API_LOCK;
     RG_CHECK(s, "null argument");
     RG_GUARD_BEGIN
     return commit(s);
@@ -858,6 +892,7 @@ int ray_scene_commit(ray_scene *s) {
 }
 
 int ray_scene_mesh_bvh_info(ray_scene *s, uint32_t mesh, ray_bvh_info *out) {
+    RG_API_LOCK;
     RG_CHECK(s && out && mesh < s->meshes.size(), "invalid mesh");
     RG_GUARD_BEGIN
     const int rc = commit(s);
@@ -876,6 +911,7 @@ int ray_scene_mesh_bvh_info(ray_scene *s, uint32_t mesh, ray_bvh_info *out) {
 }
 
 int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t) {
+    RG_API_LOCK;
     RG_CHECK(s && t, "null argument");
     RG_CHECK(t->kernel >= 0 && t->kernel <= 2, "kernel must be 1 (per ray) or 2 (persistent)");
     RG_CHECK(t->refill_min <= 32, "refill_min is a lane count, at most 32");
@@ -887,18 +923,21 @@ int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t) {
 }
 
 int ray_scene_get_trace_tuning(ray_scene *s, ray_trace_tuning *out) {
+    RG_API_LOCK;
     RG_CHECK(s && out, "null argument");
     *out = s->tuning;
     return RAY_OK;
 }
 
 int ray_scene_set_counting(ray_scene *s, int enable) {
+    RG_API_LOCK;
     RG_CHECK(s, "null argument");
     s->counting = enable != 0;
     return RAY_OK;
 }
 
 int ray_scene_last_trace_info(ray_scene *s, ray_trace_info *out) {
+    RG_API_LOCK;
     RG_CHECK(s && out, "null argument");
     if (s->info_pending) {
         RG_CUDA_TRY(cudaSetDevice(s->device));
@@ -944,6 +983,7 @@ uint64_t host_chunk(uint64_t n) {
 } // namespace
 
 int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit *hits, int32_t *obj, int mem, void *stream) {
+    RG_API_LOCK;
     RG_CHECK(s, "null scene");
     RG_CHECK(n == 0 || (rays && hits), "null buffer");
     RG_CHECK(mem == RAY_MEM_HOST || mem == RAY_MEM_DEVICE, "invalid memory space");
@@ -1067,6 +1107,7 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
 }
 
 int ray_scene_debug_read(ray_scene *s, int what, void *dst, uint64_t bytes, uint64_t *out_bytes) {
+    RG_API_LOCK;
     RG_CHECK(s && out_bytes, "null argument");
     RG_CHECK(what >= 0 && what <= 2, "invalid array selector");
     RG_GUARD_BEGIN

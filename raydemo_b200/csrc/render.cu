@@ -656,6 +656,7 @@ extern "C" {
 
 int ray_sort_rays(ray_renderer *r, const float *rays, uint64_t n, const float root_min[3], const float cell_size[3], uint32_t *keys_out,
                   uint32_t *perm_out, float *rays_out, void *stream) {
+    RG_API_LOCK;
     if (!r || !root_min || !cell_size || (n && (!rays || !perm_out))) {
         set_error("ray_sort_rays: null argument");
         return RAY_ERR_INVALID_ARG;
@@ -674,6 +675,7 @@ int ray_sort_rays(ray_renderer *r, const float *rays, uint64_t n, const float ro
 }
 
 int ray_resize(ray_renderer *r, int w, int h) {
+    RG_API_LOCK;
     if (!r || w <= 0 || h <= 0 || w > 32768 || h > 32768) {
         set_error("invalid size");
         return RAY_ERR_INVALID_ARG;
@@ -703,6 +705,7 @@ int ray_resize(ray_renderer *r, int w, int h) {
 }
 
 int ray_clear(ray_renderer *r, const ray_pixel *c) {
+    RG_API_LOCK;
     if (!r) {
         set_error("null renderer");
         return RAY_ERR_INVALID_ARG;
@@ -718,6 +721,7 @@ int ray_clear(ray_renderer *r, const ray_pixel *c) {
 }
 
 int ray_render(ray_renderer *r, ray_scene *s, ray_region *region) {
+    RG_API_LOCK;
     try {
         FrameJob J;
         ray_rect rect;
@@ -778,6 +782,7 @@ int ray_render(ray_renderer *r, ray_scene *s, ray_region *region) {
 }
 
 int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, ray_region *const *regions, int count, int samples) {
+    RG_API_LOCK;
     if (count < 0 || samples < 1 || (count > 0 && (!renderers || !scenes || !regions))) {
         set_error("null argument");
         return RAY_ERR_INVALID_ARG;
@@ -905,6 +910,7 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
 }
 
 int ray_renderer_set_kernel(ray_renderer *r, int kernel) {
+    RG_API_LOCK;
     if (!r || kernel < 0 || kernel > 2) {
         set_error("kernel must be 0 (chosen by timing), 1 (wavefront) or 2 (path kernel)");
         return RAY_ERR_INVALID_ARG;
@@ -914,6 +920,7 @@ int ray_renderer_set_kernel(ray_renderer *r, int kernel) {
 }
 
 int ray_render_diff(ray_renderer *r, ray_scene *s, int first_iteration, int samples, float *image_rgb, float *sample_rgb) {
+    RG_API_LOCK;
     try {
         if (!image_rgb || !sample_rgb) {
             set_error("null output buffer");
@@ -944,6 +951,7 @@ int ray_render_diff(ray_renderer *r, ray_scene *s, int first_iteration, int samp
 
 int ray_render_adjoint(ray_renderer *r, ray_scene *s, int first_iteration, int samples, const float *sample_rgb, const float *d_image,
                        float *grad_albedo, float *grad_roughness) {
+    RG_API_LOCK;
     try {
         if (!r || !s || !sample_rgb || !d_image || !grad_albedo || !grad_roughness) {
             set_error("null argument");
@@ -994,6 +1002,7 @@ int ray_render_adjoint(ray_renderer *r, ray_scene *s, int first_iteration, int s
 }
 
 int ray_renderer_set_ray_sort(ray_renderer *r, int policy) {
+    RG_API_LOCK;
     if (!r || policy < -1 || policy > (int)SORT_ALL) {
         set_error("ray sort policy must be RAY_SORT_AUTO (-1), 0 or a mask of bounces within RAY_SORT_ALL");
         return RAY_ERR_INVALID_ARG;
@@ -1003,6 +1012,7 @@ int ray_renderer_set_ray_sort(ray_renderer *r, int policy) {
 }
 
 int ray_get_pixels(ray_renderer *r, const ray_pixel **out, int on_device) {
+    RG_API_LOCK;
     if (!r || !out) {
         set_error("null argument");
         return RAY_ERR_INVALID_ARG;
@@ -1026,6 +1036,7 @@ int ray_get_pixels(ray_renderer *r, const ray_pixel **out, int on_device) {
 }
 
 int ray_get_sh_data(ray_renderer *r, const ray_shl1 **out) {
+    RG_API_LOCK;
     if (!r || !out) {
         set_error("null argument");
         return RAY_ERR_INVALID_ARG;
@@ -1047,6 +1058,7 @@ int ray_get_sh_data(ray_renderer *r, const ray_shl1 **out) {
 }
 
 int ray_renderer_debug_read(ray_renderer *r, int what, void *dst, uint64_t bytes, uint64_t *out_bytes) {
+    RG_API_LOCK;
     if (!r || !out_bytes || (bytes && !dst) || what < 0 || what > 3) {
         set_error("invalid argument");
         return RAY_ERR_INVALID_ARG;
@@ -1062,6 +1074,7 @@ int ray_renderer_debug_read(ray_renderer *r, int what, void *dst, uint64_t bytes
 }
 
 int ray_renderer_set_stream(ray_renderer *r, void *stream) {
+    RG_API_LOCK;
     if (!r) {
         set_error("null renderer");
         return RAY_ERR_INVALID_ARG;
@@ -1075,6 +1088,7 @@ int ray_renderer_set_stream(ray_renderer *r, void *stream) {
 }
 
 int ray_renderer_frame_info(ray_renderer *r, ray_frame_info *out) {
+    RG_API_LOCK;
     if (!r || !out) {
         set_error("null argument");
         return RAY_ERR_INVALID_ARG;
@@ -1094,6 +1108,7 @@ int ray_renderer_frame_info(ray_renderer *r, ray_frame_info *out) {
 }
 
 int ray_get_stats(ray_renderer *r, ray_stats *out) {
+    RG_API_LOCK;
     if (!r || !out) {
         set_error("null argument");
         return RAY_ERR_INVALID_ARG;
@@ -1110,6 +1125,7 @@ int ray_get_stats(ray_renderer *r, ray_stats *out) {
 }
 
 int ray_reset_stats(ray_renderer *r) {
+    RG_API_LOCK;
     if (!r) {
         set_error("null argument");
         return RAY_ERR_INVALID_ARG;

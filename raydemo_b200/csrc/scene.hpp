@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
@@ -65,6 +66,14 @@ struct DeviceBuf {
     void release();
     ~DeviceBuf() { release(); }
 };
+
+// api.cu: the lock every C-ABI entry point holds while it runs. The entry
+// points only enqueue GPU work (and wait where the call is synchronous), so
+// concurrent calls from several threads -- the reference renders disjoint
+// regions of one renderer and scene from a thread pool -- are serialised onto
+// the renderer's stream in the order they take the lock.
+std::recursive_mutex &api_mutex();
+#define RG_API_LOCK std::lock_guard<std::recursive_mutex> rg_api_lock_(rg::api_mutex())
 
 // api.cu: builds pending BVHs and uploads pending scene data, after the
 // kernels already enqueued that read the arrays it overwrites
