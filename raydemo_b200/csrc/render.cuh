@@ -28,7 +28,6 @@ struct LightRec {
 };
 static_assert(sizeof(LightRec) == 48, "LightRec must stay 48 bytes");
 
-// vertex_t (Core.h:259-262)
 // vertex_t (src/Ray/internal/Core.h:219-222) padded to 64 bytes: four 16-byte loads.
 struct alignas(16) VertexRec {
     float p[3], n[3], b[3], t[2][2];
