@@ -104,12 +104,27 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def make_workload(rank: int):
+def make_workload(rank: int, n_tris: int = N_TRIS, n_rays: int = N_RAYS):
+    """Rank `rank`'s share of an N-GPU run: the same scene on every rank (a
+    replica) and the rank's own seeded rays (weak scaling: rays per rank fixed)."""
     from raydemo_b200 import scenes
 
-    tris = scenes.random_triangles(N_TRIS, seed=0)
-    rays = scenes.incoherent_rays(N_RAYS, seed=1 + rank)
+    tris = scenes.random_triangles(n_tris, seed=0)
+    rays = scenes.incoherent_rays(n_rays, seed=1 + rank)
     return tris, rays
+
+
+def max_over_ranks(ms: float, world: int, device) -> float:
+    """The slowest rank's time (the job ends with its last rank): an all-reduce
+    MAX over the process group; the value itself with one rank."""
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def cpu_reference(tris, rays, sample: int, steps: int, warmup: int):
@@ -201,10 +216,7 @@ def render_frames(args, dev, stream, rank: int, world: int) -> dict:
             r.RenderScene(sc, reg)
         ev1.record(stream)
         torch.cuda.synchronize(dev)
-        t = torch.tensor([ev0.elapsed_time(ev1) / frames], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(ev0.elapsed_time(ev1) / frames, world, dev)
 
     by_kernel = {"wavefront": round(timed(1), 4), "path": round(timed(2), 4)}
     ms_frame = timed(0)
@@ -405,10 +417,7 @@ def atrium_frames(args, dev, stream, rank: int, world: int) -> dict:
             frame(g)
         ev1.record(stream)
         torch.cuda.synchronize(dev)
-        t = torch.tensor([ev0.elapsed_time(ev1) / frames], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(ev0.elapsed_time(ev1) / frames, world, dev)
 
     variants = {"wavefront_sort_off": timed(1, 0), "wavefront_sort_all": timed(1, 0x3FF), "wavefront_sort_auto": timed(1, -1)}
     auto_mask = r.frame_info().sort_mask
@@ -731,10 +740,7 @@ def run_gpu_arm(args) -> None:
     ms = ev0.elapsed_time(ev1)
     if sc.last_trace_info().error_flags:
         raise RuntimeError("trace reported an error during the timed steps")
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, world, dev)
     ms_step = ms_max / args.steps
     value = world * N_RAYS / (ms_step * 1e-3) / 1e6
 
@@ -757,10 +763,8 @@ def run_gpu_arm(args) -> None:
         e2e_step()
     ev1.record(stream)
     torch.cuda.synchronize(dev)
-    te = torch.tensor([ev0.elapsed_time(ev1) / e_steps], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * N_RAYS / (float(te.item()) * 1e-3) / 1e6
+    te_max = max_over_ranks(ev0.elapsed_time(ev1) / e_steps, world, dev)
+    e2e_value = world * N_RAYS / (te_max * 1e-3) / 1e6
     ok = np.array_equal(hits_h.numpy().view(np.uint32), hits_d.cpu().numpy().view(np.uint32))
 
     # the same scene and kernel on 4,194,304 coherent rays (a pinhole camera at 2048x2048 outside the cube)
