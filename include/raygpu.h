@@ -213,6 +213,12 @@ int ray_scene_add_camera(ray_scene *s, const ray_camera_desc *c, uint32_t *out_i
 int ray_scene_get_camera(ray_scene *s, uint32_t i, ray_camera_desc *out);                 /* SceneBase::GetCamera */
 int ray_scene_set_camera(ray_scene *s, uint32_t i, const ray_camera_desc *c);             /* SceneBase::SetCamera */
 int ray_scene_remove_camera(ray_scene *s, uint32_t i);                                    /* SceneBase::RemoveCamera */
+/* No counterpart in the reference: sets camera i's constructed side and up
+ * axes (camera_t::side / up, Types.h:59-71) as given, in place of those
+ * ray_scene_add_camera / ray_scene_set_camera construct. An adapter that holds
+ * the reference's already constructed camera_t (SceneBase's camera store)
+ * hands its axes on unchanged, so the primary rays stay bit-identical. */
+int ray_scene_set_camera_axes(ray_scene *s, uint32_t i, const float side[3], const float up[3]);
 int ray_scene_current_cam(ray_scene *s, uint32_t *out);
 int ray_scene_set_current_cam(ray_scene *s, uint32_t i);
 int ray_scene_triangle_count(ray_scene *s, uint32_t *out);

@@ -179,6 +179,7 @@ _SIGS = {
     "ray_render_batch": ([C.POINTER(_P), C.POINTER(_P), C.POINTER(C.POINTER(Region)), C.c_int, C.c_int], C.c_int),
     "ray_sort_rays": ([_P, _P, C.c_uint64, C.POINTER(C.c_float), C.POINTER(C.c_float), _P, _P, _P, _P], C.c_int),
     "ray_sort_rays_noalloc": ([_P, C.c_uint64, C.POINTER(C.c_float), C.POINTER(C.c_float), _P, _P, _P, _P], C.c_int),
+    "ray_scene_set_camera_axes": ([_P, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
     "ray_scene_set_trace_tuning": ([_P, C.POINTER(TraceTuning)], C.c_int),
     "ray_scene_get_trace_tuning": ([_P, C.POINTER(TraceTuning)], C.c_int),
 }

@@ -842,6 +842,14 @@ int ray_scene_set_camera(ray_scene *s, uint32_t i, const ray_camera_desc *c) {
     return RAY_OK;
 }
 
+int ray_scene_set_camera_axes(ray_scene *s, uint32_t i, const float side[3], const float up[3]) {
+    RG_API_LOCK;
+    RG_CHECK(s && side && up && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");
+    memcpy(s->cameras[i].side, side, 3 * sizeof(float));
+    memcpy(s->cameras[i].up, up, 3 * sizeof(float));
+    return RAY_OK;
+}
+
 int ray_scene_remove_camera(ray_scene *s, uint32_t i) {
     RG_API_LOCK;
     RG_CHECK(s && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");

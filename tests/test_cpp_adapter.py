@@ -1,0 +1,51 @@
+"""The C++ adapter (include/raygpu_ray.hpp): this library behind the Ray
+library's RendererBase / SceneBase. On CPU: the header compiles against the
+reference's own headers (every override matches a virtual of theirs). On the
+GPU: oracle/_ref/adapter_check builds one scene through SceneBase calls for
+the reference's Ref renderer and for this library and compares the images."""
+import json
+import os
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_SRC = os.environ.get("RAY_REFERENCE_SRC", os.path.join(os.sep, "root", "reference", "src"))
+CHECK = os.path.join(ROOT, "oracle", "_ref", "adapter_check")
+
+
+def test_adapter_compiles_against_the_reference_headers(tmp_path):
+    if not os.path.exists(os.path.join(REF_SRC, "Ray", "RendererBase.h")):
+        pytest.skip("reference headers not present")
+    cxx = os.environ.get("CXX") or shutil.which("g++")
+    src = tmp_path / "use.cpp"
+    src.write_text('#include "raygpu_ray.hpp"\n'
+                   "std::shared_ptr<Ray::RendererBase> make(const Ray::settings_t &s) { return Ray::Gpu::CreateRenderer(s); }\n"
+                   "static_assert(sizeof(ray_pixel) == sizeof(Ray::pixel_color_t), \"pixel layout\");\n"
+                   "static_assert(sizeof(ray_shl1) == sizeof(Ray::shl1_data_t), \"SH layout\");\n")
+    for std in ("c++11", "c++17"):
+        out = subprocess.run([cxx, f"-std={std}", "-fsyntax-only", "-DDISABLE_OCL", f"-I{REF_SRC}", f"-I{ROOT}/include", str(src)],
+                             capture_output=True, text=True)
+        assert out.returncode == 0, out.stderr[-3000:]
+
+
+def _run(w, h, iterations, geo):
+    out = subprocess.run([CHECK, str(w), str(h), str(iterations), str(int(geo))], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("geo", [False, True], ids=["perspective", "lightmap"])
+def test_adapter_renders_as_the_ref_renderer(cuda_device, geo):
+    if not os.path.exists(CHECK):
+        pytest.skip("oracle/_ref/adapter_check not built")
+    d = _run(96, 80, 4, geo)
+    print("adapter", d)
+    assert d["type"] == 64 and (d["w"], d["h"]) == (96, 80)
+    assert d["tris_gpu"] == d["tris_ref"] > 0
+    assert d["mean"] > 0.005
+    assert d["identical_px"] >= 0.95, d
+    assert d["rmse"] <= 2e-2, d
+    assert d["sh"] == int(geo)
