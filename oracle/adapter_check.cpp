@@ -5,7 +5,11 @@
 // Built by oracle/Makefile from the reference's headers and objects where they
 // lie, linked with libraygpu.so.
 //
-//   adapter_check <w> <h> <iterations> <geo: 0 perspective camera, 1 lightmap camera>
+//   adapter_check <w> <h> <iterations> <mode> [scene.json]
+//   mode 0: the built-in scene, perspective camera; 1: the same, lightmap camera;
+//   2: the scene description scene.json read by the demo's own loader
+//      (LoadScene, src/DemoLib/load/Load.cpp) for each renderer (paths in it
+//      relative to the working directory)
 
 #include <cmath>
 #include <cstdio>
@@ -15,6 +19,13 @@
 
 #include "Ray/RendererFactory.h"
 #include "raygpu_ray.hpp"
+
+#ifdef RB_WITH_LOADER
+#include <fstream>
+#include <sstream>
+
+#include "load/Load.h"
+#endif
 
 namespace {
 
@@ -137,9 +148,22 @@ void build(Ray::SceneBase &s, bool geo) {
     s.set_current_cam(s.AddCamera(c));
 }
 
-std::vector<Ray::pixel_color_t> render(Ray::RendererBase &r, int w, int h, int iterations, bool geo, uint32_t &tris) {
-    auto s = r.CreateScene();
-    build(*s, geo);
+std::vector<Ray::pixel_color_t> render(Ray::RendererBase &r, int w, int h, int iterations, int mode, const char *json, uint32_t &tris) {
+    std::shared_ptr<Ray::SceneBase> s;
+    if (mode == 2) {
+#ifdef RB_WITH_LOADER
+        std::ifstream f(json, std::ios::binary);
+        std::stringstream text;
+        text << f.rdbuf();
+        JsObject js;
+        if (!js.Read(text)) return {};
+        s = LoadScene(&r, js);
+#endif
+        if (!s) return {};
+    } else {
+        s = r.CreateScene();
+        build(*s, mode == 1);
+    }
     tris = s->triangle_count();
     r.Clear();
     Ray::RegionContext reg({0, 0, w, h});
@@ -153,7 +177,8 @@ std::vector<Ray::pixel_color_t> render(Ray::RendererBase &r, int w, int h, int i
 int main(int argc, char **argv) {
     const int w = argc > 1 ? std::atoi(argv[1]) : 96, h = argc > 2 ? std::atoi(argv[2]) : 80;
     const int iterations = argc > 3 ? std::atoi(argv[3]) : 4;
-    const bool geo = argc > 4 && std::atoi(argv[4]) != 0;
+    const int mode = argc > 4 ? std::atoi(argv[4]) : 0;
+    const char *json = argc > 5 ? argv[5] : "";
     Ray::settings_t st;
     st.w = w;
     st.h = h;
@@ -167,8 +192,12 @@ int main(int argc, char **argv) {
         return 2;
     }
     uint32_t tr = 0, tg = 0;
-    const auto a = render(*ref, w, h, iterations, geo, tr);
-    const auto b = render(*gpu, w, h, iterations, geo, tg);
+    const auto a = render(*ref, w, h, iterations, mode, json, tr);
+    const auto b = render(*gpu, w, h, iterations, mode, json, tg);
+    if (a.empty() || a.size() != b.size()) {
+        std::printf("{\"error\": \"no scene\"}\n");
+        return 3;
+    }
     double se = 0.0, mean = 0.0;
     size_t same = 0;
     for (size_t i = 0; i < a.size(); i++) {

@@ -30,8 +30,9 @@ def test_adapter_compiles_against_the_reference_headers(tmp_path):
         assert out.returncode == 0, out.stderr[-3000:]
 
 
-def _run(w, h, iterations, geo):
-    out = subprocess.run([CHECK, str(w), str(h), str(iterations), str(int(geo))], capture_output=True, text=True, timeout=600)
+def _run(w, h, iterations, mode, json_path=None, cwd=None):
+    args = [CHECK, str(w), str(h), str(iterations), str(int(mode))] + ([json_path] if json_path else [])
+    out = subprocess.run(args, capture_output=True, text=True, timeout=600, cwd=cwd)
     assert out.returncode == 0, out.stdout + out.stderr
     return json.loads(out.stdout.strip().splitlines()[-1])
 
@@ -49,3 +50,21 @@ def test_adapter_renders_as_the_ref_renderer(cuda_device, geo):
     assert d["identical_px"] >= 0.95, d
     assert d["rmse"] <= 2e-2, d
     assert d["sh"] == int(geo)
+
+
+@pytest.mark.gpu
+def test_demo_loader_runs_unchanged_on_the_adapter(cuda_device, tmp_path):
+    """The demo's own LoadScene (src/DemoLib/load/Load.cpp, compiled from the
+    reference's sources) given the GPU renderer through the adapter: its scene
+    renders as the same description loaded for the Ref renderer."""
+    from scene_files import make_scene_dir
+
+    if not os.path.exists(CHECK):
+        pytest.skip("oracle/_ref/adapter_check not built")
+    make_scene_dir(str(tmp_path), 3, env_map=True)
+    d = _run(96, 72, 3, 2, "scene.json", cwd=str(tmp_path))
+    print("adapter loader", d)
+    assert d["tris_gpu"] == d["tris_ref"] > 0
+    assert d["mean"] > 0.005
+    assert d["identical_px"] >= 0.9, d
+    assert d["rmse"] <= 2e-2, d
