@@ -15,6 +15,9 @@ from raydemo_b200 import load
 from render_scenes import build_ref
 from scene_files import make_scene_dir, write_bin, write_hdr, write_obj, write_tga
 
+# the reference's source tree (its scene files are read by one test, on CPU only)
+REF_SRC_DIR = os.environ.get("RAY_REFERENCE_SRC", os.path.join(os.sep, "root", "reference", "src"))
+
 
 @pytest.fixture
 def loader_ref(reflib):
@@ -195,3 +198,52 @@ def test_loader_errors_as_reference(loader_ref, tmp_path):
     with pytest.raises(KeyError):
         load.parse_scene(j, base_dir=root)
     assert theirs(base)
+
+
+def test_reference_scene_file(loader_ref):
+    """The reference's own scene description assets/scenes/sponza_simple.json
+    (its BIN mesh and JPEG textures), read here and by LoadScene: the same
+    camera, triangle count and instance transforms; the JPEG texels (Pillow's
+    decoder, not stb_image's) within 3 units of the reference's, so the Ref
+    renderer's images of the two scenes agree to the texture differences."""
+    import time
+
+    from oracle.oracle import RefLoadedScene, RefRenderer
+
+    root = os.path.join(os.path.dirname(REF_SRC_DIR), "assets")
+    path = os.path.join(root, "scenes", "sponza_simple.json")
+    if not os.path.exists(path):
+        pytest.skip("the reference's assets are not present")
+    base = os.path.dirname(root)
+    with open(path) as f:
+        js = json.load(f)
+    spec = load.parse_scene(js, base_dir=base)
+    assert spec is not None
+    for m in js["materials"].values():
+        name = m["main_texture"]
+        ours = load.load_image(os.path.join(base, name))
+        theirs = loader_ref.load_image(os.path.join(base, name))
+        d = np.abs(ours.astype(int) - theirs.astype(int))
+        assert d.max() <= 3 and (d > 0).mean() < 0.05, name
+    w, h = 48, 36
+    spec["size"] = (w, h)
+    mine = RefRenderer(loader_ref, w, h, RefRenderer.REF, True)
+    mine.render(build_ref(loader_ref, spec), 1, nthreads=8)
+    theirs = RefRenderer(loader_ref, w, h, RefRenderer.REF, True)
+    cwd = os.getcwd()
+    os.chdir(base)
+    try:
+        loaded = RefLoadedScene(theirs, json.dumps(js))
+    finally:
+        os.chdir(cwd)
+    assert loaded.ok
+    assert loaded.triangle_count() == sum(len(m[1]) // 3 for m in spec["meshes"])
+    for (_, x), y in zip(spec["instances"], loaded.instance_xforms()):
+        np.testing.assert_array_equal(x, y)
+    cam = loaded.camera()
+    np.testing.assert_array_equal(np.float32(cam.origin[:]), np.float32(spec["camera"]["origin"]))
+    np.testing.assert_array_equal(np.float32(cam.fwd[:]), np.float32(spec["camera"]["fwd"]))
+    theirs.render_loaded(loaded, 1, 8)
+    a, b = mine.pixels()[..., :3].astype(np.float64), theirs.pixels()[..., :3]
+    assert a.mean() > 0.05
+    assert np.sqrt(np.mean((a - b) ** 2)) <= 0.02
