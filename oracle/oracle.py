@@ -337,6 +337,8 @@ class RefLib:
         L.rb_add_mesh.restype = u32
         L.rb_add_instance.argtypes = [vp, u32, vp]
         L.rb_add_instance.restype = u32
+        L.rb_remove_instance.argtypes = [vp, u32]
+        L.rb_set_instance_xform.argtypes = [vp, u32, vp]
         L.rb_add_light.argtypes = [vp, C.POINTER(RbLightDesc)]
         L.rb_add_light.restype = u32
         L.rb_set_environment.argtypes = [vp, vp, C.c_float, u32]
@@ -502,6 +504,13 @@ class RefScene:
     def add_instance(self, mesh: int, xform=None) -> int:
         x = np.eye(4, dtype=np.float32).reshape(-1) if xform is None else np.ascontiguousarray(xform, np.float32).reshape(-1)
         return self.ref.lib.rb_add_instance(self.h, mesh, _p(x))
+
+    def remove_instance(self, i: int) -> None:
+        self.ref.lib.rb_remove_instance(self.h, i)
+
+    def set_instance_xform(self, i: int, xform) -> None:
+        x = np.ascontiguousarray(xform, np.float32).reshape(-1)
+        self.ref.lib.rb_set_instance_xform(self.h, i, _p(x))
 
     def add_light(self, type, position=(0, 0, 0), radius=1.0, color=(1, 1, 1), direction=(0, -1, 0), angle=0.0) -> int:
         d = RbLightDesc(type, (C.c_float * 3)(*position), radius, (C.c_float * 3)(*color), (C.c_float * 3)(*direction), angle)

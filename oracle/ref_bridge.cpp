@@ -141,6 +141,8 @@ uint32_t rb_add_mesh(void *s, int layout, const float *attrs, size_t nvtx, const
 }
 
 uint32_t rb_add_instance(void *s, uint32_t mesh, const float *xform) { return S(s)->AddMeshInstance(mesh, xform); }
+void rb_remove_instance(void *s, uint32_t i) { S(s)->RemoveMeshInstance(i); }
+void rb_set_instance_xform(void *s, uint32_t i, const float *xform) { S(s)->SetMeshInstanceTransform(i, xform); }
 
 uint32_t rb_add_light(void *s, const rb_light_desc *d) {
     Ray::light_desc_t l;

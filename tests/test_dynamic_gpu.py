@@ -115,3 +115,40 @@ def test_instance_moves_between_frames_in_flight(cuda_device):
     assert _same(a, b)
     still, _, _ = render_gpu(spec, 7, kernel=1)
     assert not _same(a, still)  # the moves show
+
+
+def test_instance_edits_render_as_the_ref_renderer(reflib, cuda_device):
+    """The same instance edits through both libraries (add, move, remove; the
+    reference rebuilds its instance tree, SceneRef.cpp:370-420): the images agree."""
+    from oracle.oracle import RefRenderer
+
+    from render_scenes import build_ref, image_diff
+
+    spec = scenes.cornell_box(4, 96, 96)
+    w, h = spec["size"]
+    moved = np.eye(4, dtype=np.float32)
+    moved[3, 0:3] = (0.35, 0.3, 0.55)
+    extra = np.eye(4, dtype=np.float32)
+    extra[3, 0:3] = (0.7, 0.75, 0.6)
+    r = api.Renderer(w, h)
+    r.set_kernel(1)
+    sc = build_gpu(r, spec)
+    rs = build_ref(reflib, spec)
+    for edit in (lambda s: s.AddMeshInstance(1, extra.reshape(-1)), lambda s: s.SetMeshInstanceTransform(1, moved.reshape(-1)),
+                 lambda s: s.RemoveMeshInstance(2)):
+        edit(sc)
+    rs.add_instance(1, extra.reshape(-1))
+    rs.set_instance_xform(1, moved.reshape(-1))
+    rs.remove_instance(2)
+    r.Clear()
+    reg = api.RegionContext()
+    for _ in range(4):
+        r.RenderScene(sc, reg)
+    gpu = r.get_pixels_ref()
+    rr = RefRenderer(reflib, w, h, RefRenderer.REF, True)
+    rr.render(rs, 4, reset=True, nthreads=1)
+    d = image_diff(gpu, rr.pixels())
+    print("instance edits", d)
+    assert d["identical_px"] >= 0.95 and d["rmse"] <= 2e-2, d
+    still, _, _ = render_gpu(spec, 4, kernel=1)
+    assert not _same(gpu, still)
