@@ -32,3 +32,23 @@ def test_null_arguments_are_rejected():
     assert L.ray_create_renderer(None, None) == capi.RAY_ERR_INVALID_ARG
     assert b"null" in L.ray_last_error()
     assert L.ray_scene_trace_closest(None, None, 0, None, None, 0, None) == capi.RAY_ERR_INVALID_ARG
+
+
+def test_no_device_fails_loudly():
+    """Without a usable CUDA device every path fails with an error, through the
+    C ABI, the Python API and the C++ adapter alike: there is no CPU fallback."""
+    import os
+    import subprocess
+
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from raydemo_b200 import api
+
+    with pytest.raises(RuntimeError):
+        api.Renderer(8, 8)
+    check = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "adapter_check")
+    if os.path.exists(check):
+        out = subprocess.run([check, "8", "8", "1", "0"], capture_output=True, text=True, timeout=300)
+        assert out.returncode == 2 and '"error"' in out.stdout
