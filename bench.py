@@ -35,16 +35,78 @@ UNIT = "Mrays/s"
 WORKLOAD = "closest-hit BVH microbench: 2,097,152 random triangles, 4,194,304 incoherent rays"
 
 
-def profiled_traffic() -> float | None:
-    """DRAM bytes per launch of the traversal kernel, from the committed ncu
-    summary of this workload (profiles/trace_closest_microbench.txt)."""
-    p = os.path.join(ROOT, "profiles", "trace_closest_microbench.txt")
+PARITY_CHUNK = 1024
+PARITY_FIXTURE = os.path.join(ROOT, "tests", "golden", "headline_ref.npz")
+
+
+def chunk_digests(records: np.ndarray, chunk: int = PARITY_CHUNK) -> np.ndarray:
+    """8-byte BLAKE2b digest of each run of `chunk` hit records ((n, 4)
+    uint32: prim, t, u, v bits), as uint64."""
+    rec = np.ascontiguousarray(records, np.uint32).reshape(-1, 4)
+    import hashlib
+
+    n = (len(rec) + chunk - 1) // chunk
+    out = np.zeros(n, np.uint64)
+    for k in range(n):
+        out[k] = int.from_bytes(hashlib.blake2b(rec[k * chunk:(k + 1) * chunk].tobytes(), digest_size=8).digest(), "little")
+    return out
+
+
+def inputs_sha256(tris: np.ndarray, rays: np.ndarray) -> str:
+    import hashlib
+
+    h = hashlib.sha256(np.ascontiguousarray(tris, np.float32).tobytes())
+    h.update(np.ascontiguousarray(rays, np.float32).tobytes())
+    return h.hexdigest()
+
+
+def parity_vs_reference(name: str, tris: np.ndarray, rays: np.ndarray, records: np.ndarray, fixture: str = PARITY_FIXTURE) -> dict:
+    """Compares this tracer's hits on the full microbench (`records`, (n, 4)
+    uint32) with the compiled reference's Ref traversal, stored as per-chunk
+    digests in `fixture` (tests/golden/make_headline_fixture.py). Rays where
+    the fixture records that the reference deviates from the closest hit with
+    ties to the lower triangle index (an exact-t tie kept in traversal order,
+    or a box the reference culled) are mapped to the reference's answer when
+    this tracer gives the closest hit there; every other difference shows as a
+    mismatching chunk."""
+    if not os.path.exists(fixture):
+        return {"rays": int(len(rays)), "mismatch": None, "fixture": "absent"}
+    import hashlib
+
+    fx = np.load(fixture)
+    if inputs_sha256(tris, rays) != fx[f"{name}_inputs_sha256"].item().decode():
+        return {"rays": int(len(rays)), "mismatch": None, "fixture": "inputs differ from the fixture's"}
+    rec = np.array(records, np.uint32, copy=True).reshape(-1, 4)
+    idx = fx[f"{name}_dev_idx"]
+    ours_ok = np.all(rec[idx] == fx[f"{name}_dev_ours"], axis=1) if len(idx) else np.zeros(0, bool)
+    rec[idx[ours_ok]] = fx[f"{name}_dev_ref"][ours_ok]
+    dig = chunk_digests(rec, int(fx["chunk"]))
+    bad = np.nonzero(dig != fx[f"{name}_digests"])[0]
+    kinds = fx[f"{name}_dev_kind"]
+    return {"rays": int(len(rays)), "mismatch_chunks": int(len(bad)), "mismatch": int(len(bad)) if len(bad) else 0,
+            "bad_chunks": [int(b) for b in bad[:16]], "chunk": int(fx["chunk"]),
+            "explained": {"exact_t_ties": int(np.sum(kinds[ours_ok] == 0)), "ref_box_false_negatives": int(np.sum(kinds[ours_ok] == 1))},
+            "unexplained_deviation_rays": int(np.sum(~ours_ok)),
+            "hits": int(np.sum(rec[:, 0].view(np.int32) >= 0)), "ref_hits": int(fx[f"{name}_hits"]),
+            "fixture": hashlib.sha256(open(fixture, "rb").read()).hexdigest()[:16]}
+
+
+def profiled(name: str = "trace_closest_microbench.txt") -> dict:
+    """Machine-readable figures of a committed ncu summary (lines 'key: value'
+    at the start of a line): DRAM bytes per launch, L2 throughput and issue
+    activity of the traversal kernel on this workload."""
+    p = os.path.join(ROOT, "profiles", name)
+    out = {}
     if not os.path.exists(p):
-        return None
+        return out
     for line in open(p):
-        if line.strip().startswith("dram_bytes_per_launch:"):
-            return float(line.split(":", 1)[1])
-    return None
+        k, sep, v = line.strip().partition(":")
+        if sep and k in ("dram_bytes_per_launch", "l2_throughput_pct", "issue_active_pct", "profiled_launch_ms", "lanes_active"):
+            try:
+                out[k] = float(v.split()[0])
+            except (ValueError, IndexError):
+                pass
+    return out
 
 
 def peaks() -> dict:
@@ -765,10 +827,14 @@ def run_gpu_arm(args) -> None:
     torch.cuda.synchronize(dev)
     te_max = max_over_ranks(ev0.elapsed_time(ev1) / e_steps, world, dev)
     e2e_value = world * N_RAYS / (te_max * 1e-3) / 1e6
-    ok = np.array_equal(hits_h.numpy().view(np.uint32), hits_d.cpu().numpy().view(np.uint32))
+    hits_dev = hits_d.cpu().numpy().view(np.uint32)
+    ok = np.array_equal(hits_h.numpy().view(np.uint32), hits_dev)
+    # every hit of the timed workload against the compiled reference (digests of its Ref traversal)
+    parity = parity_vs_reference("inc", tris, rays, hits_dev) if world == 1 or rank == 0 else None
 
     # the same scene and kernel on 4,194,304 coherent rays (a pinhole camera at 2048x2048 outside the cube)
-    coh = torch.from_numpy(scenes.coherent_rays(2048, 2048)).to(dev)
+    coh_rays = scenes.coherent_rays(2048, 2048)
+    coh = torch.from_numpy(coh_rays).to(dev)
     for _ in range(3):
         sc.trace_closest_device(coh.data_ptr(), N_RAYS, hits_d.data_ptr(), 0, sptr)
     torch.cuda.synchronize(dev)
@@ -782,16 +848,31 @@ def run_gpu_arm(args) -> None:
     coh_hits = hits_d[:, 0].view(torch.int32)
     coherent = {"rays": N_RAYS, "ms_per_step": round(coh_ms, 4), "mrays_per_s": round(N_RAYS / (coh_ms * 1e-3) / 1e6, 1),
                 "hit_rate": round(float((coh_hits >= 0).float().mean()), 4),
-                "camera": "pinhole at (0.5, 0.5, -1.5), fov 45 deg, one ray per pixel centre of 2048x2048"}
+                "camera": "pinhole at (0.5, 0.5, -1.5), fov 45 deg, one ray per pixel centre of 2048x2048",
+                "parity": parity_vs_reference("coh", tris, coh_rays, hits_d.cpu().numpy().view(np.uint32)) if rank == 0 else None}
     del coh
 
-    # roofline of the traversal kernel (the only kernel in the timed region)
+    # roofline of the traversal kernel (the only kernel in the timed region).
+    # achieved = the algorithmic byte stream (rays, hits, nodes visited,
+    # triangles tested) per launch over the launch time: a request stream
+    # served mostly by L1/L2, stated against the HBM copy peak as the
+    # contract's frac. The kernel is bound by instruction issue (divergent
+    # traversal), not by DRAM: dram_frac (ncu DRAM bytes of one launch over
+    # the same launch time) and the profile's issue and L2 figures say so.
     p = peaks()
     bytes_per_launch = N_RAYS * 44 + node_visits * 80 + tri_tests * 48
-    achieved = bytes_per_launch / (ms / args.steps * 1e-3) / 1e9
-    traffic = args.traffic_bytes if args.traffic_bytes is not None else profiled_traffic()
-    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": p["hbm_gbs"], "unit": "GB/s",
+    launch_s = ms / args.steps * 1e-3
+    achieved = bytes_per_launch / launch_s / 1e9
+    prof = profiled()
+    traffic = args.traffic_bytes if args.traffic_bytes is not None else prof.get("dram_bytes_per_launch")
+    roofline = {"bound": "issue", "achieved": round(achieved, 1), "peak": p["hbm_gbs"], "unit": "GB/s",
                 "frac": round(achieved / p["hbm_gbs"], 4), "traffic": traffic, "peak_source": p["source"],
+                "achieved_is": "algorithmic request stream (44 B per ray + 80 B per node visit + 48 B per triangle test), served by L1/L2",
+                "dram_frac": round(traffic / launch_s / 1e9 / p["hbm_gbs"], 4) if traffic else None,
+                "l2_frac": round(prof["l2_throughput_pct"] / 100, 4) if "l2_throughput_pct" in prof else None,
+                "issue_active_frac": round(prof["issue_active_pct"] / 100, 4) if "issue_active_pct" in prof else None,
+                "lanes_active_of_32": prof.get("lanes_active"),
+                "profile": "profiles/trace_closest_microbench.txt",
                 "alg_bytes_per_launch": int(bytes_per_launch), "node_visits_per_ray": round(node_visits / N_RAYS, 3),
                 "tri_tests_per_ray": round(tri_tests / N_RAYS, 3)}
 
@@ -819,7 +900,7 @@ def run_gpu_arm(args) -> None:
                            "bvh_nodes": info.nodes, "bvh_depth": info.depth, "parallelism": f"replicas x{world}"},
                 "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": N_RAYS * 32, "d2h_bytes_per_step": N_RAYS * 16,
                         "matches_device_path": bool(ok)},
-                "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "coherent": coherent,
+                "parity": parity, "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "coherent": coherent,
                 "render": render, "batch": batch,
                 "atrium": atrium, "diff": diffr}
         print(json.dumps(line), flush=True)

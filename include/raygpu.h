@@ -243,7 +243,7 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
  * position k (a stable sort on the hash, the order SortRays_CPU produces);
  * rays_out (may be NULL): the rays in that order. Device memory only;
  * stream-ordered (stream: a cudaStream_t or NULL for the renderer's stream).
- * The sort's scratch memory belongs to the renderer. */
+ * The sort's scratch memory belongs to the renderer. At most 2^30 - 1 rays. */
 int ray_sort_rays(ray_renderer *r, const float *rays, uint64_t n, const float root_min[3], const float cell_size[3], uint32_t *keys_out,
                   uint32_t *perm_out, float *rays_out, void *stream);
 
@@ -252,13 +252,16 @@ int ray_sort_rays(ray_renderer *r, const float *rays, uint64_t n, const float ro
  * belongs to their own allocator and budget, and frame loops that must not
  * stall on cudaMalloc's implicit device-wide synchronisation. Same inputs,
  * outputs and results as ray_sort_rays, without a renderer: the scratch
- * memory is a fixed array of about 12.3 MB that every GPU loading this
- * library holds until the process exits, so n is limited to
+ * memory is a fixed array of 13,640,192 bytes (13.01 MiB) that every GPU
+ * loading this library holds until the process exits, so n is limited to
  * RAY_SORT_NOALLOC_MAX_RAYS (larger n: RAY_ERR_INVALID_ARG). The first call on
- * a device looks the array up on the current device; make that first call
- * before any stream capture begins. All calls share the array: calls that
- * overlap on the GPU (other streams, other host threads) race. stream: a
- * cudaStream_t, or NULL for the default stream. */
+ * a device looks the array up on the current device and keeps its address for
+ * the life of the process: make that first call before any stream capture
+ * begins, and do not reset the device (cudaDeviceReset) while the library is
+ * in use. All calls share the array: calls that overlap on the GPU (other
+ * streams, other host threads) race. Like every entry point, its host side
+ * takes the library's process-wide lock. stream: a cudaStream_t, or NULL for
+ * the default stream. */
 #define RAY_SORT_NOALLOC_MAX_RAYS (1u << 20)
 int ray_sort_rays_noalloc(const float *rays, uint64_t n, const float root_min[3], const float cell_size[3], uint32_t *keys_out,
                           uint32_t *perm_out, float *rays_out, void *stream);

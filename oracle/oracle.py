@@ -37,6 +37,19 @@ def _p(a):
     return a.ctypes.data_as(C.c_void_p) if a is not None else None
 
 
+def reference_src() -> str | None:
+    """The reference's `src` directory: $RAY_REFERENCE_SRC, else the one the
+    oracle Makefile built oracle/_ref from (oracle/_ref/refsrc.txt); None
+    when neither names an existing directory."""
+    d = os.environ.get("RAY_REFERENCE_SRC")
+    if d:
+        d = os.path.join(d, "src") if os.path.isdir(os.path.join(d, "src", "Ray")) else d
+    else:
+        f = os.path.join(HERE, "_ref", "refsrc.txt")
+        d = open(f).read().strip() if os.path.exists(f) else None
+    return d if d and os.path.isdir(d) else None
+
+
 def build(quiet: bool = True) -> None:
     """Build the oracle (and the reference bridge when the sources exist)."""
     out = subprocess.run(["make", "-C", HERE, "-j8"], capture_output=True, text=True)

@@ -1,138 +1,267 @@
-// Stable LSD radix sort, 8-bit digits (see radix_sort.cuh).
+// Stable one-sweep LSD radix sort, 8-bit digits (see radix_sort.cuh).
+//
+// Launches per sort: one memset of the counters, one histogram launch for
+// all digit passes, then one launch per pass (plus a copy when the number of
+// passes is odd, so that the result ends in the caller's arrays).
+//
+// A pass, per tile of RS_TILE keys (tiles are numbered in the order their
+// blocks start, through an atomic counter, so every tile's predecessors are
+// running or done):
+//   1. each warp ranks its 32 x RS_ITEMS keys stably (index order) with match
+//      masks and per-warp digit counters in shared memory;
+//   2. thread d sums digit d over the warps and publishes the tile's count of
+//      d (flag AGG; tile 0 publishes it as INC, an inclusive prefix);
+//   3. thread d walks back over the preceding tiles' status words of digit d,
+//      adding AGG counts until it meets an INC prefix, then publishes its own
+//      inclusive prefix (decoupled look-back); the wait on an unpublished
+//      word is bounded and reports SORT_ERR_LOOKBACK when it runs out;
+//   4. keys, then values, are placed in shared memory in digit order and
+//      written out by consecutive threads, so each digit's run of the tile is
+//      one contiguous stretch of the output.
+// A status word is 30 bits of count under 2 flag bits, written and read as
+// one 32-bit word, so a reader sees either nothing or a complete entry.
 #include "radix_sort.cuh"
 
 namespace rg {
 namespace {
 
-template <typename K>
-__global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const K *__restrict__ keys, uint64_t n, int shift, uint32_t num_tiles,
-                                                        uint32_t *__restrict__ hist) {
-    __shared__ uint32_t h[256];
-    h[threadIdx.x] = 0;
-    __syncthreads();
-    const uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
-#pragma unroll 4
-    for (int j = 0; j < RS_ITEMS; j++) {
-        const uint64_t i = base + (uint64_t)j * RS_THREADS + threadIdx.x;
-        if (i < n) atomicAdd(&h[(uint32_t)(keys[i] >> shift) & 0xFFu], 1u);
-    }
-    __syncthreads();
-    hist[(uint64_t)threadIdx.x * num_tiles + blockIdx.x] = h[threadIdx.x];
+constexpr uint32_t ST_AGG = 1u << 30, ST_INC = 2u << 30, ST_COUNT = (1u << 30) - 1u;
+constexpr uint32_t LOOKBACK_SPIN_LIMIT = 1u << 21; // polls of one word (with a short sleep) before giving up
+constexpr uint32_t HIST_MAX_BLOCKS = 148 * 8;
+
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(uint32_t *p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Exclusive scan of `count` entries with one block of 1024 threads.
-__global__ void __launch_bounds__(1024) k_rs_scan(uint32_t *__restrict__ data, uint32_t count) {
-    __shared__ uint32_t sums[1024];
-    const uint32_t per = (count + 1023) / 1024;
-    const uint32_t b = threadIdx.x * per, e = min(count, b + per);
-    uint32_t s = 0;
-    for (uint32_t i = b; i < e; i++) s += data[i];
-    sums[threadIdx.x] = s;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        const uint32_t v = threadIdx.x >= (uint32_t)off ? sums[threadIdx.x - off] : 0u;
-        __syncthreads();
-        sums[threadIdx.x] += v;
-        __syncthreads();
-    }
-    uint32_t run = sums[threadIdx.x] - s; // exclusive prefix of this thread's chunk
-    for (uint32_t i = b; i < e; i++) {
-        const uint32_t v = data[i];
-        data[i] = run;
-        run += v;
-    }
+__device__ __forceinline__ uint32_t item_count(uint64_t cap, const uint32_t *n_dev) {
+    return n_dev ? (uint32_t)min(cap, (uint64_t)*n_dev) : (uint32_t)cap;
 }
 
 template <typename K>
-__global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const K *__restrict__ keys, const uint32_t *__restrict__ vals, K *__restrict__ keys_out,
-                                                           uint32_t *__restrict__ vals_out, uint64_t n, int shift, uint32_t num_tiles,
-                                                           const uint32_t *__restrict__ offsets) {
-    __shared__ uint32_t run[256];
-    __shared__ uint32_t wc[RS_WARPS][256];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    run[tid] = offsets[(uint64_t)tid * num_tiles + blockIdx.x];
-    for (int w = 0; w < RS_WARPS; w++) wc[w][tid] = 0;
+__device__ __forceinline__ uint32_t digit(K k, int shift) {
+    return (uint32_t)(k >> shift) & 0xFFu;
+}
+
+// Exclusive scan of one value per thread over the block (RS_THREADS threads).
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s_warp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
     __syncthreads();
-    const uint32_t lanemask_lt = (1u << lane) - 1u;
-    const uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
+    uint32_t before = 0;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; w++)
+        if (w < warp) before += s_warp[w];
+    __syncthreads();
+    return before + x - v;
+}
+
+// Digit counts of every pass in one read of the keys.
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const K *__restrict__ keys, uint64_t cap, const uint32_t *__restrict__ n_dev,
+                                                        int begin_bit, int passes, uint32_t *__restrict__ ghist) {
+    __shared__ uint32_t h[RS_MAX_PASSES * 256];
+    for (int i = threadIdx.x; i < passes * 256; i += RS_THREADS) h[i] = 0;
+    __syncthreads();
+    const uint32_t n = item_count(cap, n_dev);
+    for (uint32_t i = blockIdx.x * RS_THREADS + threadIdx.x; i < n; i += gridDim.x * RS_THREADS) {
+        const K k = keys[i];
+        for (int p = 0; p < passes; p++) atomicAdd(&h[p * 256 + digit(k, begin_bit + 8 * p)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += RS_THREADS)
+        if (h[i]) atomicAdd(&ghist[i], h[i]);
+}
+
+// One digit pass. vals_in null: the values are the items' input indices.
+template <typename K>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_onesweep(const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+                                                            K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, uint64_t cap,
+                                                            const uint32_t *__restrict__ n_dev, int shift, const uint32_t *__restrict__ ghist,
+                                                            uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status,
+                                                            uint32_t *__restrict__ err) {
+    __shared__ uint32_t s_whist[RS_WARPS][256]; // per-warp digit counts, then the warps' exclusive offsets
+    __shared__ uint32_t s_dstart[256];          // first tile position of each digit
+    __shared__ uint32_t s_gofs[256];            // output index of tile position 0 of each digit
+    __shared__ uint32_t s_warp[RS_WARPS];
+    __shared__ uint32_t s_tile;
+    __shared__ __align__(16) K s_x[RS_TILE]; // the tile in digit order: keys, then values
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (t == 0) s_tile = atomicAdd(tile_counter, 1u);
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; w++) s_whist[w][t] = 0;
+    __syncthreads();
+    const uint32_t n = item_count(cap, n_dev);
+    const uint32_t tile = s_tile;
+    const uint64_t tile_base = (uint64_t)tile * RS_TILE;
+    if (tile_base >= n) return; // past the items (block-uniform)
+    const uint32_t tile_n = (uint32_t)min((uint64_t)RS_TILE, (uint64_t)n - tile_base);
+
+    // warp w holds tile positions [w * 32 * RS_ITEMS, (w + 1) * 32 * RS_ITEMS), lane-striped
+    const uint32_t wbase = (uint32_t)warp * 32u * RS_ITEMS;
+    K k[RS_ITEMS];
+    uint32_t v[RS_ITEMS], pos[RS_ITEMS];
+#pragma unroll
     for (int j = 0; j < RS_ITEMS; j++) {
-        const uint64_t i = base + (uint64_t)j * RS_THREADS + tid;
-        const bool valid = i < n;
-        K key = 0;
-        uint32_t val = 0;
-        if (valid) {
-            key = keys[i];
-            val = vals[i];
-        }
-        const uint32_t d = valid ? ((uint32_t)(key >> shift) & 0xFFu) : 0x100u;
+        const uint32_t li = wbase + (uint32_t)j * 32u + lane;
+        const bool ok = li < tile_n;
+        k[j] = ok ? keys_in[tile_base + li] : (K)0;
+        v[j] = ok ? (vals_in ? vals_in[tile_base + li] : (uint32_t)(tile_base + li)) : 0u;
+    }
+    // stable rank among the warp's keys of the same digit
+    const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; j++) {
+        const uint32_t li = wbase + (uint32_t)j * 32u + lane;
+        const uint32_t d = li < tile_n ? digit(k[j], shift) : 256u;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        const uint32_t rank = __popc(peers & lanemask_lt);
-        if (valid && rank == 0) wc[warp][d] = __popc(peers);
-        __syncthreads();
-        {
-            uint32_t r = run[tid];
+        const uint32_t before = d < 256u ? s_whist[warp][d] : 0u;
+        pos[j] = before + __popc(peers & lt);
+        __syncwarp();
+        if (d < 256u && (peers >> lane) == 1u) s_whist[warp][d] = before + __popc(peers); // the group's last lane
+        __syncwarp();
+    }
+    __syncthreads();
+    uint32_t cnt = 0;
 #pragma unroll
-            for (int w = 0; w < RS_WARPS; w++) {
-                const uint32_t c = wc[w][tid];
-                wc[w][tid] = r;
-                r += c;
+    for (int w = 0; w < RS_WARPS; w++) {
+        const uint32_t c = s_whist[w][t];
+        s_whist[w][t] = cnt;
+        cnt += c;
+    }
+    uint32_t *mine = status + (uint64_t)tile * 256u + (uint32_t)t;
+    st_relaxed(mine, (tile == 0 ? ST_INC : ST_AGG) | cnt);
+    const uint32_t gstart = block_exclusive_scan(ghist[t], s_warp);
+    const uint32_t dstart = block_exclusive_scan(cnt, s_warp);
+    uint32_t excl = 0;
+    if (tile > 0) {
+        uint32_t pred = tile - 1, spins = 0;
+        while (true) {
+            const uint32_t s = ld_relaxed(status + (uint64_t)pred * 256u + (uint32_t)t);
+            if ((s & ~ST_COUNT) == 0u) {
+                if (++spins > LOOKBACK_SPIN_LIMIT) {
+                    if (err) atomicOr(err, SORT_ERR_LOOKBACK);
+                    break;
+                }
+                if (spins > 8u) __nanosleep(64);
+                continue;
             }
-            run[tid] = r;
+            excl += s & ST_COUNT;
+            if ((s & ST_INC) || pred == 0u) break; // tile 0 always publishes INC
+            pred--;
         }
-        __syncthreads();
-        if (valid) {
-            const uint32_t pos = wc[warp][d] + rank;
-            keys_out[pos] = key;
-            vals_out[pos] = val;
-        }
-        __syncthreads();
+        st_relaxed(mine, ST_INC | ((excl + cnt) & ST_COUNT));
+    }
+    s_dstart[t] = dstart;
+    s_gofs[t] = gstart + excl - dstart;
+    __syncthreads();
 #pragma unroll
-        for (int w = 0; w < RS_WARPS; w++) wc[w][tid] = 0;
-        __syncthreads();
+    for (int j = 0; j < RS_ITEMS; j++) {
+        const uint32_t li = wbase + (uint32_t)j * 32u + lane;
+        if (li < tile_n) {
+            const uint32_t d = digit(k[j], shift);
+            pos[j] += s_dstart[d] + s_whist[warp][d];
+            s_x[pos[j]] = k[j];
+        }
+    }
+    __syncthreads();
+    uint32_t dst[RS_ITEMS];
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; j++) {
+        const uint32_t i = (uint32_t)j * RS_THREADS + (uint32_t)t;
+        if (i < tile_n) {
+            const K key = s_x[i];
+            dst[j] = s_gofs[digit(key, shift)] + i;
+            keys_out[dst[j]] = key;
+        }
+    }
+    __syncthreads();
+    uint32_t *s_v = reinterpret_cast<uint32_t *>(s_x);
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; j++) {
+        const uint32_t li = wbase + (uint32_t)j * 32u + lane;
+        if (li < tile_n) s_v[pos[j]] = v[j];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; j++) {
+        const uint32_t i = (uint32_t)j * RS_THREADS + (uint32_t)t;
+        if (i < tile_n) vals_out[dst[j]] = s_v[i];
     }
 }
 
 template <typename K>
-cudaError_t sort_impl(K *keys, uint32_t *vals, uint64_t n, int begin_bit, int end_bit, void *scratch, cudaStream_t st) {
-    if (n <= 1) return cudaSuccess;
+__global__ void k_rs_copy(const K *__restrict__ ks, const uint32_t *__restrict__ vs, K *__restrict__ kd, uint32_t *__restrict__ vd,
+                          uint64_t cap, const uint32_t *__restrict__ n_dev) {
+    const uint32_t n = item_count(cap, n_dev);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        kd[i] = ks[i];
+        vd[i] = vs[i];
+    }
+}
+
+constexpr uint64_t kCounterWords = RS_COUNTER_WORDS; // digit counts of every pass, then the tile counters
+
+template <typename K>
+cudaError_t sort_impl(K *keys, uint32_t *vals, uint64_t n, int begin_bit, int end_bit, void *scratch, cudaStream_t st, const uint32_t *n_dev,
+                      bool ident, uint32_t *err) {
+    const int passes = (end_bit - begin_bit + 7) / 8;
+    if (passes < 1 || passes > (int)sizeof(K) || begin_bit < 0 || end_bit > (int)(8 * sizeof(K)) || n > RS_MAX_ITEMS)
+        return cudaErrorInvalidValue;
+    if (n == 0) return cudaSuccess;
     const uint32_t num_tiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
     char *p = static_cast<char *>(scratch);
     K *keys_alt = reinterpret_cast<K *>(p);
-    p += ((n * sizeof(K) + 255) / 256) * 256;
+    p += rs_align256(n * sizeof(K));
     uint32_t *vals_alt = reinterpret_cast<uint32_t *>(p);
-    p += ((n * 4 + 255) / 256) * 256;
-    uint32_t *hist = reinterpret_cast<uint32_t *>(p);
+    p += rs_align256(n * 4);
+    uint32_t *ghist = reinterpret_cast<uint32_t *>(p);
+    uint32_t *counters = ghist + RS_MAX_PASSES * 256;
+    uint32_t *status = ghist + kCounterWords;
+    cudaError_t e = cudaMemsetAsync(ghist, 0, (kCounterWords + (uint64_t)passes * num_tiles * 256) * 4, st);
+    if (e != cudaSuccess) return e;
+    k_rs_hist<K><<<num_tiles < HIST_MAX_BLOCKS ? num_tiles : HIST_MAX_BLOCKS, RS_THREADS, 0, st>>>(keys, n, n_dev, begin_bit, passes, ghist);
     K *src_k = keys, *dst_k = keys_alt;
-    uint32_t *src_v = vals, *dst_v = vals_alt;
-    int passes = 0;
-    for (int shift = begin_bit; shift < end_bit; shift += 8) {
-        k_rs_hist<K><<<num_tiles, RS_THREADS, 0, st>>>(src_k, n, shift, num_tiles, hist);
-        k_rs_scan<<<1, 1024, 0, st>>>(hist, 256u * num_tiles);
-        k_rs_scatter<K><<<num_tiles, RS_THREADS, 0, st>>>(src_k, src_v, dst_k, dst_v, n, shift, num_tiles, hist);
-        K *tk = src_k; src_k = dst_k; dst_k = tk;
-        uint32_t *tv = src_v; src_v = dst_v; dst_v = tv;
-        passes++;
+    const uint32_t *src_v = ident ? nullptr : vals;
+    uint32_t *dst_v = vals_alt;
+    for (int q = 0; q < passes; q++) {
+        k_rs_onesweep<K><<<num_tiles, RS_THREADS, 0, st>>>(src_k, src_v, dst_k, dst_v, n, n_dev, begin_bit + 8 * q, ghist + 256 * q,
+                                                           counters + q, status + (uint64_t)q * num_tiles * 256, err);
+        K *tk = src_k;
+        src_k = dst_k;
+        dst_k = tk;
+        uint32_t *nv = dst_v;
+        dst_v = (dst_v == vals_alt) ? vals : vals_alt;
+        src_v = nv;
     }
     if (passes & 1) {
-        cudaError_t e = cudaMemcpyAsync(keys, src_k, n * sizeof(K), cudaMemcpyDeviceToDevice, st);
-        if (e != cudaSuccess) return e;
-        e = cudaMemcpyAsync(vals, src_v, n * 4, cudaMemcpyDeviceToDevice, st);
-        if (e != cudaSuccess) return e;
+        const uint64_t want = (n + 255) / 256;
+        const uint32_t blocks = (uint32_t)(want < 148 * 16 ? want : 148 * 16);
+        k_rs_copy<K><<<blocks, 256, 0, st>>>(src_k, src_v, keys, vals, n, n_dev);
     }
     return cudaGetLastError();
 }
 
 } // namespace
 
-size_t radix_sort_scratch_bytes(uint64_t n, int key_bytes) {
-    const uint64_t num_tiles = (n + RS_TILE - 1) / RS_TILE;
-    return ((n * key_bytes + 255) / 256) * 256 + ((n * 4 + 255) / 256) * 256 + 256 * num_tiles * 4 + 256;
-}
+size_t radix_sort_scratch_bytes(uint64_t n, int key_bytes) { return radix_sort_scratch_bytes_c(n, key_bytes); }
 
 cudaError_t radix_sort_pairs(void *keys, uint32_t *vals, uint64_t n, int key_bytes, int begin_bit, int end_bit, void *scratch,
-                             cudaStream_t stream) {
-    if (key_bytes == 8) return sort_impl<uint64_t>(static_cast<uint64_t *>(keys), vals, n, begin_bit, end_bit, scratch, stream);
-    if (key_bytes == 4) return sort_impl<uint32_t>(static_cast<uint32_t *>(keys), vals, n, begin_bit, end_bit, scratch, stream);
+                             cudaStream_t stream, const uint32_t *n_dev, bool vals_identity, uint32_t *err) {
+    if (key_bytes == 8)
+        return sort_impl<uint64_t>(static_cast<uint64_t *>(keys), vals, n, begin_bit, end_bit, scratch, stream, n_dev, vals_identity, err);
+    if (key_bytes == 4)
+        return sort_impl<uint32_t>(static_cast<uint32_t *>(keys), vals, n, begin_bit, end_bit, scratch, stream, n_dev, vals_identity, err);
     return cudaErrorInvalidValue;
 }
 

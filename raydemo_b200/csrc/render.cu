@@ -12,6 +12,7 @@
 #include <random>
 
 #include "../../include/raygpu.h"
+#include "radix_sort.cuh"
 #include "scene.hpp"
 #include "sort.cuh"
 
@@ -559,7 +560,7 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
                 // SortRays_CPU before each bounce (RendererRef.cpp:200-203): the rays move to the other buffer in hash order
                 const int dst = cur ^ 1;
                 RG_CUDA_TRY(launch_loop_sort(d_jobs, (int)jobs.size(), rays[cur], pay[cur], job[cur], cnt + cur, total, rays[dst], pay[dst], job[dst],
-                                             cnt + dst, rb->d_loop_sort.p, st));
+                                             cnt + dst, rb->d_loop_sort.p, st, err));
                 cur = dst;
             }
             if (ev) RG_CUDA_TRY(cudaEventRecord(ev[ev_sorted(bounce)], st));
@@ -661,8 +662,8 @@ int ray_sort_rays(ray_renderer *r, const float *rays, uint64_t n, const float ro
         set_error("ray_sort_rays: null argument");
         return RAY_ERR_INVALID_ARG;
     }
-    if (n > 0xffffffffull) {
-        set_error("ray_sort_rays: at most 2^32 - 1 rays per call");
+    if (n > RS_MAX_ITEMS) {
+        set_error("ray_sort_rays: at most 2^30 - 1 rays per call");
         return RAY_ERR_INVALID_ARG;
     }
     if (n == 0) return RAY_OK;

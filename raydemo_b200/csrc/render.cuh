@@ -266,12 +266,13 @@ cudaError_t launch_render_paths(const FrameJob *jobs, int n_jobs, uint32_t total
 // Ray sorting between bounces (sort.cu): the *count rays of a wavefront
 // buffer in the order of a stable sort on (job, get_ray_hash of the ray in
 // its job's grid), written to the other buffer with *count_out = *count.
-// capacity: the buffers' size (the sort covers it; entries past *count sort
-// last and are not copied).
+// capacity: the buffers' size; only the min(*count, capacity) live rays are
+// hashed, sorted and copied (the count is read on the device). err gets
+// SORT_ERR_LOOKBACK if the sort's bounded wait ran out.
 size_t loop_sort_scratch_bytes(uint64_t capacity, int n_jobs);
 cudaError_t launch_loop_sort(const FrameJob *jobs, int n_jobs, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
                              const uint32_t *count, uint32_t capacity, float4 *rays_out, RayPayload *pay_out, uint32_t *job_out,
-                             uint32_t *count_out, void *scratch, cudaStream_t st);
+                             uint32_t *count_out, void *scratch, cudaStream_t st, uint32_t *err);
 // Differentiable forward: per pixel, image = (sum over the jobs k of temp_k) / n_jobs
 // and sample_rgb[k] = temp_k (RGB); temp_k = jobs[k].temp, all w x h.
 cudaError_t launch_diff_collect(const FrameJob *jobs, int n_jobs, uint32_t n_pix, float *image, float *sample_rgb, cudaStream_t st);

@@ -76,13 +76,12 @@ __device__ __forceinline__ uint32_t ray_hash(float4 o, float4 d, float3 root_min
 }
 
 __global__ void k_ray_hash(const float4 *__restrict__ rays, uint32_t n, float3 root_min, float3 cell, uint32_t *__restrict__ keys_out,
-                           uint32_t *__restrict__ sort_keys, uint32_t *__restrict__ perm) {
+                           uint32_t *__restrict__ sort_keys) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t key = ray_hash(rays[2ull * i], rays[2ull * i + 1], root_min, cell);
     if (keys_out) keys_out[i] = key;
     sort_keys[i] = key;
-    perm[i] = i;
 }
 
 __global__ void k_gather_rays(const float4 *__restrict__ rays, const uint32_t *__restrict__ perm, uint32_t n, float4 *__restrict__ out) {
@@ -93,24 +92,18 @@ __global__ void k_gather_rays(const float4 *__restrict__ rays, const uint32_t *_
     out[2ull * i + 1] = rays[2ull * s + 1];
 }
 
-// Keys of the render loop's sort: for i < *count the ray's hash in its job's
-// grid (with the job above it when there are several), all ones past *count
-// (sorted last: the sort is stable and they come last in the input).
+// Keys of the render loop's sort for the live rays (i < *count): the ray's
+// hash in its job's grid, with the job above it when there are several.
 template <typename Key>
 __global__ void k_loop_keys(const FrameJob *__restrict__ jobs, const float4 *__restrict__ rays, const uint32_t *__restrict__ ray_job,
-                            const uint32_t *__restrict__ count, uint32_t capacity, Key *__restrict__ keys, uint32_t *__restrict__ perm) {
+                            const uint32_t *__restrict__ count, uint32_t capacity, Key *__restrict__ keys) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= capacity) return;
-    Key key = ~(Key)0;
-    if (i < min(*count, capacity)) {
-        const uint32_t j = ray_job[i];
-        const FrameJob &J = jobs[j];
-        const uint32_t h = ray_hash(rays[2ull * i], rays[2ull * i + 1], make_float3(J.root_min[0], J.root_min[1], J.root_min[2]),
-                                    make_float3(J.cell[0], J.cell[1], J.cell[2]));
-        key = sizeof(Key) == 8 ? (Key)(((uint64_t)j << 32) | h) : (Key)h;
-    }
-    keys[i] = key;
-    perm[i] = i;
+    if (i >= min(*count, capacity)) return;
+    const uint32_t j = ray_job[i];
+    const FrameJob &J = jobs[j];
+    const uint32_t h = ray_hash(rays[2ull * i], rays[2ull * i + 1], make_float3(J.root_min[0], J.root_min[1], J.root_min[2]),
+                                make_float3(J.cell[0], J.cell[1], J.cell[2]));
+    keys[i] = sizeof(Key) == 8 ? (Key)(((uint64_t)j << 32) | h) : (Key)h;
 }
 
 __global__ void k_loop_gather(const float4 *__restrict__ rays, const RayPayload *__restrict__ pay, const uint32_t *__restrict__ ray_job,
@@ -148,7 +141,7 @@ size_t loop_sort_scratch_bytes(uint64_t capacity, int n_jobs) {
 
 cudaError_t launch_loop_sort(const FrameJob *jobs, int n_jobs, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
                              const uint32_t *count, uint32_t capacity, float4 *rays_out, RayPayload *pay_out, uint32_t *job_out,
-                             uint32_t *count_out, void *scratch, cudaStream_t st) {
+                             uint32_t *count_out, void *scratch, cudaStream_t st, uint32_t *err) {
     if (capacity == 0) return cudaSuccess;
     const int kb = n_jobs > 1 ? 8 : 4;
     char *p = static_cast<char *>(scratch);
@@ -156,13 +149,15 @@ cudaError_t launch_loop_sort(const FrameJob *jobs, int n_jobs, const float4 *ray
     uint32_t *perm = reinterpret_cast<uint32_t *>(p + ((uint64_t(capacity) * kb + 255) / 256) * 256);
     void *rs_scratch = reinterpret_cast<char *>(perm) + ((uint64_t(capacity) * 4 + 255) / 256) * 256;
     const uint32_t blocks = (capacity + 255) / 256;
+    // only the live rays (their count is on the device): keys, sort and gather
+    // all read min(*count, capacity) there; blocks past it return at once
     if (kb == 8)
-        k_loop_keys<uint64_t><<<blocks, 256, 0, st>>>(jobs, rays, ray_job, count, capacity, static_cast<uint64_t *>(keys), perm);
+        k_loop_keys<uint64_t><<<blocks, 256, 0, st>>>(jobs, rays, ray_job, count, capacity, static_cast<uint64_t *>(keys));
     else
-        k_loop_keys<uint32_t><<<blocks, 256, 0, st>>>(jobs, rays, ray_job, count, capacity, static_cast<uint32_t *>(keys), perm);
+        k_loop_keys<uint32_t><<<blocks, 256, 0, st>>>(jobs, rays, ray_job, count, capacity, static_cast<uint32_t *>(keys));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    e = radix_sort_pairs(keys, perm, capacity, kb, 0, kb == 8 ? 32 + job_bits(n_jobs) : 32, rs_scratch, st);
+    e = radix_sort_pairs(keys, perm, capacity, kb, 0, kb == 8 ? 32 + job_bits(n_jobs) : 32, rs_scratch, st, count, true, err);
     if (e != cudaSuccess) return e;
     k_loop_gather<<<blocks, 256, 0, st>>>(rays, pay, ray_job, perm, count, capacity, rays_out, pay_out, job_out, count_out);
     return cudaGetLastError();
@@ -171,18 +166,18 @@ cudaError_t launch_loop_sort(const FrameJob *jobs, int n_jobs, const float4 *ray
 size_t sort_rays_scratch_bytes(uint64_t n) { return ((n * 4 + 255) / 256) * 256 + radix_sort_scratch_bytes(n, 4); }
 
 cudaError_t sort_rays(const float4 *rays, uint64_t n, const float root_min[3], const float cell_size[3], uint32_t *keys_out,
-                      uint32_t *perm_out, float4 *rays_out, void *scratch, cudaStream_t st) {
+                      uint32_t *perm_out, float4 *rays_out, void *scratch, cudaStream_t st, uint32_t *err) {
     if (n == 0) return cudaSuccess;
-    if (n > 0xffffffffull) return cudaErrorInvalidValue;
+    if (n > RS_MAX_ITEMS) return cudaErrorInvalidValue;
     char *p = static_cast<char *>(scratch);
     uint32_t *sort_keys = reinterpret_cast<uint32_t *>(p);
     void *rs_scratch = p + ((n * 4 + 255) / 256) * 256;
     const uint32_t blocks = (uint32_t)((n + 255) / 256);
     k_ray_hash<<<blocks, 256, 0, st>>>(rays, (uint32_t)n, make_float3(root_min[0], root_min[1], root_min[2]),
-                                       make_float3(cell_size[0], cell_size[1], cell_size[2]), keys_out, sort_keys, perm_out);
+                                       make_float3(cell_size[0], cell_size[1], cell_size[2]), keys_out, sort_keys);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    e = radix_sort_pairs(sort_keys, perm_out, n, 4, 0, 32, rs_scratch, st);
+    e = radix_sort_pairs(sort_keys, perm_out, n, 4, 0, 32, rs_scratch, st, nullptr, true, err);
     if (e != cudaSuccess) return e;
     if (rays_out) {
         k_gather_rays<<<blocks, 256, 0, st>>>(rays, perm_out, (uint32_t)n, rays_out);

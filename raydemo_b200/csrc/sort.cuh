@@ -14,7 +14,9 @@ size_t sort_rays_scratch_bytes(uint64_t n);
 // is the input index of the ray at position k); rays_out (may be null) = the
 // rays in that order. rays / rays_out: n records of 8 floats
 // (ox, oy, oz, tmax, dx, dy, dz, unused). All pointers are device memory.
+// err (may be null): device word that gets SORT_ERR_LOOKBACK if the radix
+// sort's bounded wait ran out. At most RS_MAX_ITEMS rays.
 cudaError_t sort_rays(const float4 *rays, uint64_t n, const float root_min[3], const float cell_size[3], uint32_t *keys_out,
-                      uint32_t *perm_out, float4 *rays_out, void *scratch, cudaStream_t st);
+                      uint32_t *perm_out, float4 *rays_out, void *scratch, cudaStream_t st, uint32_t *err = nullptr);
 
 } // namespace rg

@@ -11,17 +11,20 @@
 
 #include "../../include/raygpu.h"
 #include "common.cuh"
+#include "radix_sort.cuh"
+#include "scene.hpp"
 #include "sort.cuh"
 
 namespace rg {
 namespace {
 
 // Scratch for RAY_SORT_NOALLOC_MAX_RAYS rays, laid out as sort_rays expects:
-// the keys being sorted, then the radix sort's ping-pong keys and values and
-// its per-tile histograms (4096 keys per tile, 256 digits).
+// the keys being sorted, then the radix sort's ping-pong keys and values, its
+// digit counts and tile counters, and its look-back status words
+// (13,640,192 bytes = 13.01 MiB for 1,048,576 rays).
 constexpr uint64_t kMaxRays = RAY_SORT_NOALLOC_MAX_RAYS;
-constexpr uint64_t kWords = ((kMaxRays * 4 + 255) / 256) * 256;
-constexpr uint64_t kScratchBytes = 3 * kWords + 256 * ((kMaxRays + 4095) / 4096) * 4 + 256;
+constexpr uint64_t kScratchBytes = rs_align256(kMaxRays * 4) + radix_sort_scratch_bytes_c(kMaxRays, 4);
+static_assert(kScratchBytes == 13640192ull, "the documented size of the static scratch");
 
 static __device__ __align__(256) unsigned char g_sort_scratch[kScratchBytes];
 
@@ -38,6 +41,7 @@ using namespace rg;
 
 extern "C" int ray_sort_rays_noalloc(const float *rays, uint64_t n, const float root_min[3], const float cell_size[3], uint32_t *keys_out,
                                      uint32_t *perm_out, float *rays_out, void *stream) {
+    RG_API_LOCK; // host side serialised with every other entry point, like ray_sort_rays
     if (!root_min || !cell_size || (n && (!rays || !perm_out))) {
         set_error("ray_sort_rays_noalloc: null argument");
         return RAY_ERR_INVALID_ARG;
@@ -58,6 +62,8 @@ extern "C" int ray_sort_rays_noalloc(const float *rays, uint64_t n, const float 
         // First call on this device (with the device current): look up the
         // array's device address. This may load the library's module on the
         // device, so make this first call before any stream capture begins.
+        // The address is kept for the life of the process: a device reset
+        // (cudaDeviceReset) while the library is in use invalidates it.
         std::lock_guard<std::mutex> lock(g_setup_mutex);
         if (!g_scratch_addr[dev]) {
             void *p = nullptr;

@@ -13,7 +13,8 @@ built by oracle/Makefile); the tests read the committed .npz files.
       sort_*: keys and permutation of Ref::SortRays_CPU
       cam_*:  primary rays of Ref::GeneratePrimaryRays (tent filter, DOF)
 
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py [/path/to/reference]   (default: $RAY_REFERENCE_SRC, or the
+tree oracle/_ref was built from)
 """
 from __future__ import annotations
 
@@ -95,7 +96,12 @@ def ref_outputs() -> dict:
 
 
 def main() -> None:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    from oracle.oracle import reference_src
+
+    src = sys.argv[1] if len(sys.argv) > 1 else reference_src()
+    if not src:
+        raise SystemExit("give the reference tree as the argument or in RAY_REFERENCE_SRC")
+    ref = os.path.dirname(src) if os.path.basename(os.path.normpath(src)) == "src" else src
     np.savez_compressed(os.path.join(HERE, "ref_tests.npz"), **ref_tests(ref))
     np.savez_compressed(os.path.join(HERE, "ref_outputs.npz"), **ref_outputs())
     print("written", os.listdir(HERE))

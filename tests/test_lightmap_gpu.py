@@ -34,7 +34,7 @@ def test_lightmap_matches_ref_renderer(reflib, cuda_device, overlap):
     d = image_diff(gpu, cpu)
     print("lightmap 4 spp", d)
     assert d["identical_px"] >= 0.95, d
-    assert d["rmse"] <= 2e-2, d
+    assert d["rmse"] <= 1e-3, d
     assert r.frame_info().kernel == 1 and r.frame_info().error_flags == 0
     # texels between the cells: the environment colour (0.1) with alpha 1, as in the reference
     bg = np.all(cpu == np.float32([0.1, 0.1, 0.1, 1.0]), axis=-1)
@@ -55,14 +55,14 @@ def test_lightmap_sh_region_and_path_kernel_setting(reflib, cuda_device):
     d = image_diff(gpu, cpu)
     print("lightmap sh", d)
     assert d["identical_px"] >= 0.95, d
-    assert d["rmse"] <= 2e-2, d
+    assert d["rmse"] <= 1e-3, d
     sh = r.get_sh_data_ref()
     assert sh is not None and cpu_sh is not None
     x, y, w, h = rect
     a, b = sh[y:y + h, x:x + w], cpu_sh[y:y + h, x:x + w]
     same = np.all(a == b, axis=-1).mean()
     assert same >= 0.95, same
-    assert np.sqrt(np.mean((a.astype(np.float64) - b) ** 2)) <= 2e-2
+    assert np.sqrt(np.mean((a.astype(np.float64) - b) ** 2)) <= 1e-3
 
 
 def test_lightmap_of_transformed_instance(reflib, cuda_device):
@@ -78,7 +78,7 @@ def test_lightmap_of_transformed_instance(reflib, cuda_device):
     d = image_diff(gpu, cpu)
     print("sphere lightmap", d)
     assert d["identical_px"] >= 0.95, d
-    assert d["rmse"] <= 2e-2, d
+    assert d["rmse"] <= 1e-3, d
 
 
 def test_geo_and_perspective_jobs_in_one_batch(reflib, cuda_device):
@@ -97,7 +97,7 @@ def test_geo_and_perspective_jobs_in_one_batch(reflib, cuda_device):
         np.testing.assert_array_equal(r.get_pixels_ref().view(np.uint32), alone.view(np.uint32))
     cpu = render_ref(reflib, specs[0], 3)
     d = image_diff(rs[0].get_pixels_ref(), cpu)
-    assert d["identical_px"] >= 0.95 and d["rmse"] <= 2e-2, d
+    assert d["identical_px"] >= 0.95 and d["rmse"] <= 1e-3, d
 
 
 def test_geo_camera_api(cuda_device):

@@ -10,13 +10,15 @@ import os
 import numpy as np
 import pytest
 
+from oracle.oracle import reference_src
+
 from raydemo_b200 import load
 
 from render_scenes import build_ref
 from scene_files import make_scene_dir, write_bin, write_hdr, write_obj, write_tga
 
 # the reference's source tree (its scene files are read by one test, on CPU only)
-REF_SRC_DIR = os.environ.get("RAY_REFERENCE_SRC", os.path.join(os.sep, "root", "reference", "src"))
+REF_SRC_DIR = reference_src() or ""
 
 
 @pytest.fixture

@@ -154,7 +154,7 @@ def test_cornell_matches_ref_renderer(reflib, cuda_device, kernel):
     cpu8 = render_ref(reflib, spec, 8)
     d8 = image_diff(gpu8, cpu8)
     print("cornell 8 spp", d8)
-    assert d8["rmse"] <= 2e-2, d8
+    assert d8["rmse"] <= 1e-3, d8
 
 
 def _lights_spec():
@@ -198,7 +198,7 @@ def test_lights_and_materials_match_ref_renderer(reflib, cuda_device, kernel):
     d = image_diff(gpu, cpu)
     print("lights/materials 4 spp", d)
     assert d["identical_px"] >= 0.9, d
-    assert d["rmse"] <= 2e-2, d
+    assert d["rmse"] <= 1e-3, d
 
 
 @pytest.mark.parametrize("kernel", [1, 2], ids=["wavefront", "path"])
@@ -269,7 +269,7 @@ def test_batch_matches_single_renders(reflib, ref_tests, cuda_device, kernel):
         np.testing.assert_array_equal(batch.view(np.uint32), alone.view(np.uint32))
     cpu = render_ref(reflib, specs[2], 3)
     d = image_diff(rs[2].get_pixels_ref(), cpu)
-    assert d["rmse"] <= 2e-2 and d["identical_px"] >= 0.95, d
+    assert d["rmse"] <= 1e-3 and d["identical_px"] >= 0.95, d
 
 
 def test_kernel_choice_by_timing(ref_tests, cuda_device):

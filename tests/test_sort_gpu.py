@@ -34,7 +34,7 @@ def test_golden_sort(renderer, ref_outputs):
     assert np.array_equal(out.view(np.uint32), ref_outputs["sort_rays"][perm].view(np.uint32))
 
 
-@pytest.mark.parametrize("n,seed", [(1, 1), (255, 2), (4097, 3), (1 << 20, 4), (3_000_001, 5)])
+@pytest.mark.parametrize("n,seed", [(1, 1), (2, 6), (255, 2), (4096, 7), (4097, 3), (3 * 8192, 8), (1 << 20, 4), (3_000_001, 5)])
 def test_random_sort_vs_oracle(renderer, oracle, n, seed):
     rays = scenes.incoherent_rays(n, seed=seed)
     rays[:, 0:3] = rays[:, 0:3] * 3.0 - 1.0  # a third of the origins outside the root box on each side
@@ -73,3 +73,22 @@ def test_live_reference_sort(renderer, reflib):
     keys, perm, _ = gpu_sort(renderer, rays, root_min, cell, gather=False)
     assert np.array_equal(keys, ref_keys)
     assert np.array_equal(perm, ref_perm)
+
+
+@pytest.mark.parametrize("n", [5000, 300001])
+def test_equal_keys_keep_input_order(renderer, oracle, n):
+    """Every ray in one cell with one direction (a single digit value in
+    every pass, so every tile's count sits in one digit of the look-back):
+    the sort must be stable, the permutation the identity."""
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3] = 0.25
+    rays[:, 3] = 1e30
+    rays[:, 6] = 1.0
+    rays[::3, 0] = 0.75  # two keys, interleaved
+    root_min = np.array([0.0, 0.0, 0.0], np.float32)
+    cell = np.array([1 / 255, 1 / 255, 1 / 255], np.float32)
+    keys, perm, out = gpu_sort(renderer, rays, root_min, cell)
+    exp_keys = oracle.ray_hash(rays, root_min, cell)
+    assert np.array_equal(keys, exp_keys)
+    assert np.array_equal(perm, oracle.sort_perm(exp_keys))
+    assert np.array_equal(out.view(np.uint32), rays[perm].view(np.uint32))

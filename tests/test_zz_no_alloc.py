@@ -68,3 +68,33 @@ def test_noalloc_sort_rejects_more_than_its_scratch_holds(cuda_device):
     rc = L.ray_sort_rays_noalloc(rd.data_ptr(), n, root_min, cell, None, perm.data_ptr(), None, None)
     assert rc == capi.RAY_ERR_INVALID_ARG
     assert b"RAY_SORT_NOALLOC_MAX_RAYS" in L.ray_last_error()
+
+
+def test_noalloc_sort_allocates_nothing_on_a_side_stream(cuda_device):
+    """A warmed call leaves the device's free memory unchanged (nothing is
+    allocated), and a call on a caller's stream with keys_out and rays_out
+    NULL gives the allocating sort's permutation."""
+    import torch
+
+    L = capi.lib()
+    r = Renderer(16, 16)
+    root_min = (C.c_float * 3)(0.0, 0.0, 0.0)
+    cell = (C.c_float * 3)(1 / 255, 1 / 255, 1 / 255)
+    n = 200003
+    rays = scenes.incoherent_rays(n, seed=73)
+    rd = torch.from_numpy(rays).cuda()
+    ka, pa, oa = _buffers(torch, n)
+    pb = torch.zeros(n, dtype=torch.int32, device="cuda")
+    capi.check(L.ray_sort_rays(r.handle, rd.data_ptr(), n, root_min, cell, ka.data_ptr(), pa.data_ptr(), oa.data_ptr(), None))
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    capi.check(L.ray_sort_rays_noalloc(rd.data_ptr(), n, root_min, cell, None, pb.data_ptr(), None, s.cuda_stream))  # warm
+    s.synchronize()
+    pb.zero_()
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    capi.check(L.ray_sort_rays_noalloc(rd.data_ptr(), n, root_min, cell, None, pb.data_ptr(), None, s.cuda_stream))
+    s.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
+    assert free_after == free_before
+    assert np.array_equal(_host(pb), _host(pa))
