@@ -773,6 +773,28 @@ def run_gpu_arm(args) -> None:
     def step():
         sc.trace_closest_device(rays_d.data_ptr(), N_RAYS, hits_d.data_ptr(), 0, sptr)
 
+    # the trace order, measured: input order against rays sorted by the
+    # reference's ray hash (direction sector first, or origin cell first) on
+    # 16 or 32 key bits; the timed steps use --reorder/--reorder-bits
+    variants = {}
+    if not args.no_variants:
+        for mode, bits in ((0, 32), (1, 32), (1, 16), (2, 32), (2, 24)):
+            sc.set_trace_tuning(2, 8, 0, mode, bits)
+            for _ in range(2):
+                step()
+            va, vb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            va.record(stream)
+            for _ in range(5):
+                step()
+            vb.record(stream)
+            torch.cuda.synchronize(dev)
+            variants[f"reorder{mode}_bits{bits}"] = round(va.elapsed_time(vb) / 5, 4)
+    sc.set_trace_tuning(2, 8, 0, args.reorder, args.reorder_bits)
+    # kernels per step: the trace; with a trace order also the key kernel, the
+    # sort's histogram and digit passes (and its copy when they are odd)
+    passes = (args.reorder_bits + 7) // 8
+    launches_per_step = 1 + ((2 + passes + (passes & 1)) if args.reorder else 0)
+
     # counting pass: node visits and triangle tests of this BVH (algorithmic bytes)
     sc.set_counting(True)
     step()
@@ -897,10 +919,12 @@ def run_gpu_arm(args) -> None:
                 "data": "synthetic (seeded procedural scene and rays)",
                 "config": {"workload": WORKLOAD, "rays_per_step_per_gpu": N_RAYS, "tris": N_TRIS,
                            "l2": "inputs larger than L2 (rays 128 MiB per step, hits 64 MiB)", "bvh_build_s": round(build_s, 3),
-                           "bvh_nodes": info.nodes, "bvh_depth": info.depth, "parallelism": f"replicas x{world}"},
+                           "bvh_nodes": info.nodes, "bvh_depth": info.depth, "parallelism": f"replicas x{world}",
+                           "trace_order": {"reorder": args.reorder, "bits": args.reorder_bits,
+                                           "ms_per_step_by_variant": variants}},
                 "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": N_RAYS * 32, "d2h_bytes_per_step": N_RAYS * 16,
                         "matches_device_path": bool(ok)},
-                "parity": parity, "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "coherent": coherent,
+                "parity": parity, "gpu_launches": args.steps * launches_per_step, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "coherent": coherent,
                 "render": render, "batch": batch,
                 "atrium": atrium, "diff": diffr}
         print(json.dumps(line), flush=True)
@@ -934,6 +958,10 @@ def main() -> None:
     ap.add_argument("--diff-lr-rough", type=float, default=1e-2)
     ap.add_argument("--no-diff-oracle-fd", dest="diff_oracle_fd", action="store_false",
                     help="skip the oracle's finite differences in the differentiable form")
+    ap.add_argument("--reorder", type=int, default=0, choices=[0, 1, 2],
+                    help="trace order of the timed steps: 0 input, 1 ray hash, 2 origin cell first")
+    ap.add_argument("--reorder-bits", type=int, default=32)
+    ap.add_argument("--no-variants", action="store_true", help="skip the trace-order variants")
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes per launch of the traversal kernel from an ncu capture (reported as roofline.traffic)")
     args = ap.parse_args()

@@ -282,9 +282,17 @@ int ray_scene_last_trace_info(ray_scene *s, ray_trace_info *out);
  * refill_min lanes of a warp are idle, 1..32). kernel 0 or refill_min <= 0
  * keep the current setting. deep_stack: 0 = size the traversal stack by the
  * BVH depth (shared memory only unless a tree is deeper than it holds),
- * 1 = always continue it in local memory. */
+ * 1 = always continue it in local memory. reorder: 0 = trace the rays in
+ * their input order; 1 = first sort them (stably) by the reference's ray hash
+ * (get_ray_hash, CoreRef.cpp:316-333: direction sector above the origin's
+ * Morton cell, over the scene's box in 255 cells per axis, as SortRays_CPU
+ * keys them) and trace them in that order; 2 = the same with the origin cell
+ * above the direction sector. The hits are written at each ray's input
+ * position either way, and do not depend on the order. reorder_bits: how many
+ * of the key's top bits the sort uses (8..32; 0 = 32). Calls of fewer than
+ * 65,536 rays are not reordered. */
 typedef struct ray_trace_tuning {
-    int kernel, refill_min, deep_stack;
+    int kernel, refill_min, deep_stack, reorder, reorder_bits;
 } ray_trace_tuning;
 int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t);
 int ray_scene_get_trace_tuning(ray_scene *s, ray_trace_tuning *out);

@@ -9,7 +9,9 @@
 #include <new>
 
 #include "../../include/raygpu.h"
+#include "radix_sort.cuh"
 #include "scene.hpp"
+#include "sort.cuh"
 #include "trace.cuh"
 
 namespace rg {
@@ -924,9 +926,13 @@ int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t) {
     RG_CHECK(t->kernel >= 0 && t->kernel <= 2, "kernel must be 1 (per ray) or 2 (persistent)");
     RG_CHECK(t->refill_min <= 32, "refill_min is a lane count, at most 32");
     RG_CHECK(t->deep_stack == 0 || t->deep_stack == 1, "deep_stack is 0 or 1");
+    RG_CHECK(t->reorder >= 0 && t->reorder <= 2, "reorder is 0 (input order), 1 (ray hash) or 2 (origin cell first)");
+    RG_CHECK(t->reorder_bits == 0 || (t->reorder_bits >= 8 && t->reorder_bits <= 32), "reorder_bits is 0 or 8..32");
     if (t->kernel > 0) s->tuning.kernel = t->kernel;
     if (t->refill_min > 0) s->tuning.refill_min = t->refill_min;
     s->tuning.deep_stack = t->deep_stack;
+    s->tuning.reorder = t->reorder;
+    s->tuning.reorder_bits = t->reorder_bits ? t->reorder_bits : 32;
     return RAY_OK;
 }
 
@@ -989,6 +995,10 @@ uint64_t host_chunk(uint64_t n) {
     return c >= n ? n : c;
 }
 } // namespace
+
+// Reordered traces only from this many rays: below it the sort's fixed cost
+// outweighs what the trace gains.
+constexpr uint64_t kReorderMinRays = 65536;
 
 int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit *hits, int32_t *obj, int mem, void *stream) {
     RG_API_LOCK;
@@ -1063,6 +1073,10 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
     for (const MeshRec &m : s->meshes) tp.max_depth = std::max(tp.max_depth, m.bvh.depth);
     if (s->tuning.deep_stack) tp.max_depth = 0xffffffffu;
     uint32_t *next_ray = static_cast<uint32_t *>(s->d_next_ray.p);
+    // reordered traces: the hash grid of SortRays_CPU over the scene's box (RendererRef.cpp:48-77)
+    const bool reorder = s->tuning.reorder != 0;
+    float cell[3];
+    for (int a = 0; a < 3; a++) cell[a] = (s->world_max[a] - s->world_min[a]) / 255.0f;
     int k = 0;
     for (size_t c = 0; c + 1 < cut.size(); c++, k++) {
         const uint64_t b = cut[c], m = cut[c + 1] - b;
@@ -1076,6 +1090,15 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
                 RG_CUDA_TRY(cudaEventRecord(s->pipe_ev[1], up));
                 RG_CUDA_TRY(cudaStreamWaitEvent(ts, s->pipe_ev[1], 0));
             }
+        }
+        tp.order = nullptr;
+        if (reorder && m >= kReorderMinRays && m <= RS_MAX_ITEMS) {
+            // the chunk's trace order (scratch of this chunk's parity, like the work counter)
+            RG_CUDA_TRY(s->d_order[k & 1].ensure(order_scratch_bytes(m)));
+            uint32_t *order = nullptr;
+            RG_CUDA_TRY(order_rays(d_rays + 2 * b, (uint32_t)m, s->world_min, cell, s->tuning.reorder, s->tuning.reorder_bits,
+                                   s->d_order[k & 1].p, &order, ts));
+            tp.order = order;
         }
         RG_CUDA_TRY(launch_trace_closest(sv, d_rays + 2 * b, (uint32_t)m, d_hits + b, d_obj ? d_obj + b : nullptr,
                                          static_cast<uint32_t *>(s->d_err.p), static_cast<unsigned long long *>(s->d_counters.p), s->counting,

@@ -84,6 +84,16 @@ __global__ void k_ray_hash(const float4 *__restrict__ rays, uint32_t n, float3 r
     sort_keys[i] = key;
 }
 
+// Keys of a trace order: the ray hash (mode 1) or the hash with its 8-bit
+// direction sector moved below the origin cell (mode 2).
+__global__ void k_order_keys(const float4 *__restrict__ rays, uint32_t n, float3 root_min, float3 cell, int mode,
+                             uint32_t *__restrict__ keys) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t h = ray_hash(rays[2ull * i], rays[2ull * i + 1], root_min, cell);
+    keys[i] = mode == 2 ? ((h << 8) | (h >> 24)) : h;
+}
+
 __global__ void k_gather_rays(const float4 *__restrict__ rays, const uint32_t *__restrict__ perm, uint32_t n, float4 *__restrict__ out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -184,6 +194,29 @@ cudaError_t sort_rays(const float4 *rays, uint64_t n, const float root_min[3], c
         e = cudaGetLastError();
     }
     return e;
+}
+
+} // namespace rg
+
+namespace rg {
+
+size_t order_scratch_bytes(uint64_t n) { return ((n * 4 + 255) / 256) * 256 * 2 + radix_sort_scratch_bytes(n, 4); }
+
+cudaError_t order_rays(const float4 *rays, uint32_t n, const float root_min[3], const float cell_size[3], int mode, int bits, void *scratch,
+                       uint32_t **order_out, cudaStream_t st) {
+    if (bits <= 0 || bits > 32) bits = 32;
+    if (bits < 8) bits = 8;
+    char *p = static_cast<char *>(scratch);
+    uint32_t *keys = reinterpret_cast<uint32_t *>(p);
+    uint32_t *order = reinterpret_cast<uint32_t *>(p + ((uint64_t(n) * 4 + 255) / 256) * 256);
+    void *rs_scratch = p + ((uint64_t(n) * 4 + 255) / 256) * 256 * 2;
+    *order_out = order;
+    if (n == 0) return cudaSuccess;
+    k_order_keys<<<(n + 255) / 256, 256, 0, st>>>(rays, n, make_float3(root_min[0], root_min[1], root_min[2]),
+                                                 make_float3(cell_size[0], cell_size[1], cell_size[2]), mode, keys);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return radix_sort_pairs(keys, order, n, 4, 32 - bits, 32, rs_scratch, st, nullptr, true);
 }
 
 } // namespace rg

@@ -20,3 +20,16 @@ cudaError_t sort_rays(const float4 *rays, uint64_t n, const float root_min[3], c
                       uint32_t *perm_out, float4 *rays_out, void *scratch, cudaStream_t st, uint32_t *err = nullptr);
 
 } // namespace rg
+
+namespace rg {
+
+// Trace order of n rays (n <= RS_MAX_ITEMS): a stable sort of the ray indices
+// by get_ray_hash over the grid (root_min, cell) -- mode 1 -- or by that hash
+// rotated so that the origin's 24-bit Morton cell lies above the 8-bit
+// direction sector -- mode 2 --, on the key's top `bits` bits. *order_out
+// points into scratch (order_scratch_bytes(n)) when the call returns.
+size_t order_scratch_bytes(uint64_t n);
+cudaError_t order_rays(const float4 *rays, uint32_t n, const float root_min[3], const float cell_size[3], int mode, int bits, void *scratch,
+                       uint32_t **order_out, cudaStream_t st);
+
+} // namespace rg

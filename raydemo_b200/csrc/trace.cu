@@ -48,15 +48,17 @@ __device__ __forceinline__ void flush_counters(uint32_t err, uint32_t nvis, uint
 template <bool COUNT, bool DEEP>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, const float4 *__restrict__ rays, uint32_t n, float4 *__restrict__ hits,
                                                                int32_t *__restrict__ obj_out, uint32_t *__restrict__ err_out,
-                                                               unsigned long long *__restrict__ counters, const uint32_t *__restrict__ n_dev) {
+                                                               unsigned long long *__restrict__ counters, const uint32_t *__restrict__ n_dev,
+                                                               const uint32_t *__restrict__ order) {
     __shared__ uint2 s_stack[SMEM_STACK * TRACE_BLOCK];
     Stack<DEEP> st;
     st.smem = s_stack + threadIdx.x;
     st.sp = 0;
     if (n_dev) n = min(n, *n_dev);
-    const uint32_t i = blockIdx.x * TRACE_BLOCK + threadIdx.x;
+    const uint32_t k = blockIdx.x * TRACE_BLOCK + threadIdx.x;
     uint32_t err = 0, nvis = 0, ntri = 0;
-    if (i < n) {
+    if (k < n) {
+        const uint32_t i = order ? __ldg(order + k) : k;
         const float4 r0 = __ldg(rays + 2ull * i), r1 = __ldg(rays + 2ull * i + 1);
         Best best;
         best.t = r0.w;
@@ -96,7 +98,8 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
                                                                   uint32_t *__restrict__ err_out, unsigned long long *__restrict__ counters,
                                                                   uint32_t *__restrict__ next_ray, int refill_min,
                                                                   const uint32_t *__restrict__ n_dev, const uint8_t *__restrict__ views = nullptr,
-                                                                  uint32_t view_stride = 0, const uint32_t *__restrict__ ray_job = nullptr) {
+                                                                  uint32_t view_stride = 0, const uint32_t *__restrict__ ray_job = nullptr,
+                                                                  const uint32_t *__restrict__ order = nullptr) {
     if (n_dev) n = min(n, *n_dev);
     __shared__ uint2 s_stack[SMEM_STACK * TRACE_BLOCK];
     Stack<DEEP> st;
@@ -126,7 +129,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
             if (ri == NO_RAY) {
                 const uint32_t idx = base + __popc(need & lanemask_lt);
                 if (idx < n) {
-                    ri = idx;
+                    ri = order ? __ldg(order + idx) : idx;
                     mi = 0;
                     in_mesh = false;
                     best.t = __ldg(&rays[2ull * idx].w);
@@ -231,9 +234,9 @@ cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, flo
     if (!tp.persistent && !tp.views && !tp.any) {
         const uint32_t grid = (n + TRACE_BLOCK - 1) / TRACE_BLOCK;
         if (count)
-            k_trace_closest<true, DEEP><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.count);
+            k_trace_closest<true, DEEP><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.count, tp.order);
         else
-            k_trace_closest<false, DEEP><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.count);
+            k_trace_closest<false, DEEP><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.count, tp.order);
         return cudaGetLastError();
     }
     if (!tp.next_ray) return cudaErrorInvalidValue;
@@ -264,10 +267,10 @@ cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, flo
     }
     if (count)
         k_trace_persistent<true, DEEP><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min,
-                                                                        tp.count);
+                                                                        tp.count, nullptr, 0, nullptr, tp.order);
     else
         k_trace_persistent<false, DEEP><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min,
-                                                                         tp.count);
+                                                                         tp.count, nullptr, 0, nullptr, tp.order);
     return cudaGetLastError();
 }
 

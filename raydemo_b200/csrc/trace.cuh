@@ -30,6 +30,9 @@ struct TraceParams {
     const uint8_t *views = nullptr;
     uint32_t view_stride = 0;
     const uint32_t *ray_job = nullptr;
+    // trace order: the k-th ray taken is ray order[k] (its hit is written at
+    // that index); null: input order
+    const uint32_t *order = nullptr;
     // shadow rays (persistent kernel): a ray ends at its first accepted hit on
     // a solid triangle (that hit is returned); without one, the closest hit
     // on a non-solid triangle or a miss

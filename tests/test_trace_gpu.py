@@ -195,14 +195,17 @@ def test_empty_and_degenerate(renderer, oracle):
     assert len(sc.trace_closest(np.zeros((0, 8), np.float32))) == 0
 
 
-@pytest.mark.parametrize("kernel,refill,deep", [(1, 8, 0), (1, 8, 1), (2, 1, 0), (2, 8, 0), (2, 32, 0), (2, 8, 1)])
-def test_kernel_variants_agree(renderer, oracle, kernel, refill, deep):
-    """Every traversal kernel and stack placement gives the same bytes."""
+@pytest.mark.parametrize("kernel,refill,deep,reorder,bits", [(1, 8, 0, 0, 32), (1, 8, 1, 0, 32), (2, 1, 0, 0, 32), (2, 8, 0, 0, 32),
+                                                             (2, 32, 0, 0, 32), (2, 8, 1, 0, 32), (2, 8, 0, 1, 32), (2, 8, 0, 2, 24),
+                                                             (1, 8, 0, 1, 16), (2, 4, 1, 2, 32)])
+def test_kernel_variants_agree(renderer, oracle, kernel, refill, deep, reorder, bits):
+    """Every traversal kernel, stack placement and trace order gives the
+    same bytes, each hit at its ray's input position."""
     tris = scenes.random_triangles(100000, seed=81)
-    rays = scenes.incoherent_rays(60000, seed=82)
+    rays = scenes.incoherent_rays(100000, seed=82)
     sc = _scene(tris, renderer)
-    sc.set_trace_tuning(kernel, refill, deep)
-    assert sc.get_trace_tuning() == (kernel, refill, deep)
+    sc.set_trace_tuning(kernel, refill, deep, reorder, bits)
+    assert sc.get_trace_tuning() == (kernel, refill, deep, reorder, bits)
     _assert_hits_equal(sc.trace_closest(rays), _oracle_hits(oracle, tris, rays))
 
 
