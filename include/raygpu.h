@@ -290,9 +290,12 @@ int ray_scene_last_trace_info(ray_scene *s, ray_trace_info *out);
  * above the direction sector. The hits are written at each ray's input
  * position either way, and do not depend on the order. reorder_bits: how many
  * of the key's top bits the sort uses (8..32; 0 = 32). Calls of fewer than
- * 65,536 rays are not reordered. */
+ * 65,536 rays are not reordered. block (64, 128, 256; 0 = 128) and smem_stack
+ * (16, 24, 32 entries per thread; 0 = 24; not 32 with 256 threads): threads
+ * per block of the persistent kernel and the depth of its shared-memory stack
+ * (a deeper tree continues in local memory). */
 typedef struct ray_trace_tuning {
-    int kernel, refill_min, deep_stack, reorder, reorder_bits;
+    int kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack;
 } ray_trace_tuning;
 int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t);
 int ray_scene_get_trace_tuning(ray_scene *s, ray_trace_tuning *out);

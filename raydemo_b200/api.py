@@ -254,17 +254,20 @@ class Scene:
         """Device-pointer form (stream-ordered, asynchronous)."""
         check(lib().ray_scene_trace_closest(self._h, rays_ptr, n, hits_ptr, obj_ptr or None, capi.RAY_MEM_DEVICE, stream or None))
 
-    def set_trace_tuning(self, kernel: int = 0, refill_min: int = 0, deep_stack: int = 0, reorder: int = 0, reorder_bits: int = 0) -> None:
+    def set_trace_tuning(self, kernel: int = 0, refill_min: int = 0, deep_stack: int = 0, reorder: int = 0, reorder_bits: int = 0,
+                         block: int = 0, smem_stack: int = 0) -> None:
         """ray_scene_set_trace_tuning: kernel (1 per ray, 2 persistent; 0
         keeps), refill threshold (0 keeps), deep stack, trace order (0 input,
-        1 ray hash, 2 origin cell first) and the key bits it sorts on."""
-        t = capi.TraceTuning(kernel, refill_min, deep_stack, reorder, reorder_bits)
+        1 ray hash, 2 origin cell first), the key bits it sorts on, threads
+        per block and shared stack entries (0: 128 and 24)."""
+        t = capi.TraceTuning(kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack)
         check(lib().ray_scene_set_trace_tuning(self._h, C.byref(t)))
 
     def get_trace_tuning(self) -> tuple:
+        """(kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack)"""
         t = capi.TraceTuning()
         check(lib().ray_scene_get_trace_tuning(self._h, C.byref(t)))
-        return t.kernel, t.refill_min, t.deep_stack, t.reorder, t.reorder_bits
+        return t.kernel, t.refill_min, t.deep_stack, t.reorder, t.reorder_bits, t.block, t.smem_stack
 
     def set_counting(self, enable: bool) -> None:
         check(lib().ray_scene_set_counting(self._h, int(enable)))

@@ -106,7 +106,8 @@ class DiffParams(C.Structure):
 
 
 class TraceTuning(C.Structure):
-    _fields_ = [("kernel", C.c_int), ("refill_min", C.c_int), ("deep_stack", C.c_int), ("reorder", C.c_int), ("reorder_bits", C.c_int)]
+    _fields_ = [("kernel", C.c_int), ("refill_min", C.c_int), ("deep_stack", C.c_int), ("reorder", C.c_int), ("reorder_bits", C.c_int),
+                ("block", C.c_int), ("smem_stack", C.c_int)]
 
 
 class BvhInfo(C.Structure):

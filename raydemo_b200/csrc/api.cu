@@ -928,11 +928,16 @@ int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t) {
     RG_CHECK(t->deep_stack == 0 || t->deep_stack == 1, "deep_stack is 0 or 1");
     RG_CHECK(t->reorder >= 0 && t->reorder <= 2, "reorder is 0 (input order), 1 (ray hash) or 2 (origin cell first)");
     RG_CHECK(t->reorder_bits == 0 || (t->reorder_bits >= 8 && t->reorder_bits <= 32), "reorder_bits is 0 or 8..32");
+    RG_CHECK(t->block == 0 || t->block == 64 || t->block == 128 || t->block == 256, "block is 0, 64, 128 or 256");
+    RG_CHECK(t->smem_stack == 0 || t->smem_stack == 16 || t->smem_stack == 24 || t->smem_stack == 32, "smem_stack is 0, 16, 24 or 32");
+    RG_CHECK(!((t->block == 256) && t->smem_stack == 32), "256 threads with 32 stack entries exceed the block's shared memory");
     if (t->kernel > 0) s->tuning.kernel = t->kernel;
     if (t->refill_min > 0) s->tuning.refill_min = t->refill_min;
     s->tuning.deep_stack = t->deep_stack;
     s->tuning.reorder = t->reorder;
     s->tuning.reorder_bits = t->reorder_bits ? t->reorder_bits : 32;
+    s->tuning.block = t->block ? t->block : 128;
+    s->tuning.smem_stack = t->smem_stack ? t->smem_stack : 24;
     return RAY_OK;
 }
 
@@ -1070,6 +1075,8 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
     TraceParams tp;
     tp.persistent = s->tuning.kernel == 2;
     tp.refill_min = s->tuning.refill_min;
+    tp.block = s->tuning.block;
+    tp.smem_stack = s->tuning.smem_stack;
     for (const MeshRec &m : s->meshes) tp.max_depth = std::max(tp.max_depth, m.bvh.depth);
     if (s->tuning.deep_stack) tp.max_depth = 0xffffffffu;
     uint32_t *next_ray = static_cast<uint32_t *>(s->d_next_ray.p);

@@ -120,7 +120,7 @@ __device__ __forceinline__ Best trace_closest_scene(const SceneView &sv, float4 
             bmax[q] = __ldg(&ir->bbox_max[q]);
         }
         if (!trav::ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
-        trav::trace_mesh<false, true>(trav::mesh_of(sv, ir, (int)m), trav::transform_ray(ir, r0, r1), best, st, err, nvis, ntri);
+        trav::trace_mesh<false>(trav::mesh_of(sv, ir, (int)m), trav::transform_ray(ir, r0, r1), best, st, err, nvis, ntri);
     }
     return best;
 }
@@ -143,7 +143,7 @@ __device__ __forceinline__ Best trace_any(const SceneView &sv, V3 o, V3 d, float
             bmax[q] = __ldg(&ir->bbox_max[q]);
         }
         if (!trav::ref_bbox_test(o.x, o.y, o.z, sx, sy, sz, best.t, bmin, bmax)) continue;
-        if (trav::trace_mesh_any<true>(trav::mesh_of(sv, ir, (int)m), trav::transform_ray(ir, r0, r1), best, st, err)) break;
+        if (trav::trace_mesh_any(trav::mesh_of(sv, ir, (int)m), trav::transform_ray(ir, r0, r1), best, st, err)) break;
     }
     return best;
 }

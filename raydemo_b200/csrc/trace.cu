@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
                 bmax[k] = __ldg(&ir->bbox_max[k]);
             }
             if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
-            trace_mesh<COUNT, DEEP>(mesh_of(sv, ir, (int)m), transform_ray(ir, r0, r1), best, st, err, nvis, ntri);
+            trace_mesh<COUNT>(mesh_of(sv, ir, (int)m), transform_ray(ir, r0, r1), best, st, err, nvis, ntri);
         }
         hits[i] = make_float4(__int_as_float(best.prim), best.t, best.prim >= 0 ? best.u : 0.0f, best.prim >= 0 ? best.v : 0.0f);
         if (obj_out) obj_out[i] = best.obj;
@@ -92,8 +92,8 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
 // whose SceneView is at views + ray_job[i] * view_stride.
 // ANY: shadow rays -- a ray ends at its first accepted hit on a solid
 // triangle (Traverse_MacroTree_WithStack_AnyHit, CoreRef.cpp:1224-1368).
-template <bool COUNT, bool DEEP, bool MULTI = false, bool ANY = false>
-__global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, const float4 *__restrict__ rays, uint32_t n,
+template <bool COUNT, bool DEEP, bool MULTI = false, bool ANY = false, int BLOCK = TRACE_BLOCK, int SDEPTH = SMEM_STACK>
+__global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const float4 *__restrict__ rays, uint32_t n,
                                                                   float4 *__restrict__ hits, int32_t *__restrict__ obj_out,
                                                                   uint32_t *__restrict__ err_out, unsigned long long *__restrict__ counters,
                                                                   uint32_t *__restrict__ next_ray, int refill_min,
@@ -101,8 +101,8 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
                                                                   uint32_t view_stride = 0, const uint32_t *__restrict__ ray_job = nullptr,
                                                                   const uint32_t *__restrict__ order = nullptr) {
     if (n_dev) n = min(n, *n_dev);
-    __shared__ uint2 s_stack[SMEM_STACK * TRACE_BLOCK];
-    Stack<DEEP> st;
+    __shared__ uint2 s_stack[SDEPTH * BLOCK];
+    Stack<DEEP, BLOCK, SDEPTH> st;
     st.smem = s_stack + threadIdx.x;
     st.sp = 0;
     const uint32_t lane = threadIdx.x & 31u;
@@ -228,6 +228,41 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_persistent(SceneView sv, 
 
 int g_persistent_blocks[2] = {0, 0};
 
+// The closest-hit persistent kernel with a tuned block size and shared stack
+// depth (one resident grid: the SM count times the blocks that fit per SM).
+template <bool DEEP, int BLOCK, int SDEPTH>
+cudaError_t launch_tuned(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
+                         unsigned long long *counters, cudaStream_t st, const TraceParams &tp) {
+    static_assert(SDEPTH * BLOCK * 8 <= 48 * 1024, "static shared memory limit");
+    static int blocks = 0;
+    if (blocks == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_persistent<false, DEEP, false, false, BLOCK, SDEPTH>, BLOCK, 0);
+        if (e != cudaSuccess) return e;
+        blocks = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    cudaError_t e = cudaMemsetAsync(tp.next_ray, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    k_trace_persistent<false, DEEP, false, false, BLOCK, SDEPTH><<<blocks, BLOCK, 0, st>>>(
+        sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min, tp.count, nullptr, 0, nullptr, tp.order);
+    return cudaGetLastError();
+}
+
+template <bool DEEP>
+cudaError_t launch_tuned_dispatch(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
+                                  unsigned long long *counters, cudaStream_t st, const TraceParams &tp) {
+#define RG_TUNED(B, D)                                                                                                                  \
+    if (tp.block == B && tp.smem_stack == D) return launch_tuned<DEEP, B, D>(sv, rays, n, hits, obj, err, counters, st, tp);
+    RG_TUNED(64, 16) RG_TUNED(64, 24) RG_TUNED(64, 32)
+    RG_TUNED(128, 16) RG_TUNED(128, 32)
+    RG_TUNED(256, 16) RG_TUNED(256, 24)
+#undef RG_TUNED
+    return cudaErrorInvalidValue;
+}
+
 template <bool DEEP>
 cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
                         unsigned long long *counters, bool count, cudaStream_t st, const TraceParams &tp) {
@@ -240,6 +275,8 @@ cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, flo
         return cudaGetLastError();
     }
     if (!tp.next_ray) return cudaErrorInvalidValue;
+    if (!count && !tp.views && !tp.any && !(tp.block == TRACE_BLOCK && tp.smem_stack == SMEM_STACK))
+        return launch_tuned_dispatch<DEEP>(sv, rays, n, hits, obj, err, counters, st, tp);
     int &blocks = g_persistent_blocks[DEEP ? 1 : 0];
     if (blocks == 0) {
         int dev = 0, sms = 0, per_sm = 0;
@@ -279,8 +316,11 @@ cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, flo
 cudaError_t launch_trace_closest(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
                                  unsigned long long *counters, bool count, cudaStream_t st, const TraceParams &tp) {
     if (n == 0) return cudaSuccess;
-    // one group per level at most: the shared-memory stack suffices up to SMEM_STACK levels
-    if (tp.max_depth < (uint32_t)SMEM_STACK) return launch_impl<false>(sv, rays, n, hits, obj, err, counters, count, st, tp);
+    // one group per level at most: the shared-memory stack suffices up to its
+    // depth in levels (the tuned closest-hit kernel's depth where it applies)
+    const bool tuned = tp.persistent && !count && !tp.views && !tp.any;
+    const uint32_t sdepth = tuned ? (uint32_t)tp.smem_stack : (uint32_t)SMEM_STACK;
+    if (tp.max_depth < sdepth) return launch_impl<false>(sv, rays, n, hits, obj, err, counters, count, st, tp);
     return launch_impl<true>(sv, rays, n, hits, obj, err, counters, count, st, tp);
 }
 

@@ -22,6 +22,10 @@ constexpr uint32_t TRACE_ERR_LIMIT = 4u;  // more node visits than the mesh has 
 struct TraceParams {
     bool persistent = true; // resident grid with per-lane ray refill
     int refill_min = 8;     // refill a warp's idle lanes once at least this many are idle
+    // closest-hit persistent kernel only: threads per block (64, 128, 256) and
+    // shared-memory stack entries per thread (16, 24, 32; 256 x 32 exceeds the
+    // block's static shared memory)
+    int block = 128, smem_stack = 24;
     uint32_t max_depth = 0; // deepest wide BVH among the traced meshes (sizes the stack)
     uint32_t *next_ray = nullptr; // device work counter for the persistent kernel
     const uint32_t *count = nullptr; // device ray count: when set, min(n, *count) rays are traced

@@ -74,41 +74,44 @@ struct MeshRef {
 };
 
 // Per-thread stack of node groups: entry k of this thread at
-// smem[k * TRACE_BLOCK]; the DEEP variant continues in a local array.
-template <bool DEEP>
+// smem[k * STRIDE] (STRIDE = the block's thread count), DEPTH entries in
+// shared memory; the DEEP variant continues it in a local array, to
+// SMEM_STACK + LMEM_STACK entries in all.
+template <bool DEEP, int STRIDE = TRACE_BLOCK, int DEPTH = SMEM_STACK>
 struct Stack;
 
-template <>
-struct Stack<false> {
+template <int STRIDE, int DEPTH>
+struct Stack<false, STRIDE, DEPTH> {
     uint2 *smem;
     int sp;
     __device__ __forceinline__ bool push(uint2 e) {
-        if (sp >= SMEM_STACK) return false;
-        smem[sp * TRACE_BLOCK] = e;
+        if (sp >= DEPTH) return false;
+        smem[sp * STRIDE] = e;
         sp++;
         return true;
     }
     __device__ __forceinline__ uint2 pop() {
         sp--;
-        return smem[sp * TRACE_BLOCK];
+        return smem[sp * STRIDE];
     }
 };
 
-template <>
-struct Stack<true> {
+template <int STRIDE, int DEPTH>
+struct Stack<true, STRIDE, DEPTH> {
+    static constexpr int LOCAL = SMEM_STACK + LMEM_STACK - DEPTH;
     uint2 *smem;
-    uint2 lmem[LMEM_STACK];
+    uint2 lmem[LOCAL];
     int sp;
     __device__ __forceinline__ bool push(uint2 e) {
-        if (sp >= SMEM_STACK + LMEM_STACK) return false;
-        if (sp < SMEM_STACK) smem[sp * TRACE_BLOCK] = e;
-        else lmem[sp - SMEM_STACK] = e;
+        if (sp >= DEPTH + LOCAL) return false;
+        if (sp < DEPTH) smem[sp * STRIDE] = e;
+        else lmem[sp - DEPTH] = e;
         sp++;
         return true;
     }
     __device__ __forceinline__ uint2 pop() {
         sp--;
-        return sp < SMEM_STACK ? smem[sp * TRACE_BLOCK] : lmem[sp - SMEM_STACK];
+        return sp < DEPTH ? smem[sp * STRIDE] : lmem[sp - DEPTH];
     }
 };
 
@@ -152,9 +155,9 @@ __device__ __forceinline__ MeshRef mesh_of(const SceneView &sv, const InstanceRe
 // its 8 children and returns their hits as a node group (internal children,
 // bits 24..31, with the node's imask in bits 0..7) and a triangle group
 // (bits 0..23). Returns false (and sets err) on a corrupt index.
-template <bool COUNT, bool DEEP>
+template <bool COUNT, typename ST>
 __device__ __forceinline__ bool node_step(const MeshRef &mr, const LocalRay &r, float best_t, uint32_t &ng_base, uint32_t &ng_bits,
-                                          uint32_t &tg_base, uint32_t &tg_bits, Stack<DEEP> &st, uint32_t &visits, uint32_t &err,
+                                          uint32_t &tg_base, uint32_t &tg_bits, ST &st, uint32_t &visits, uint32_t &err,
                                           uint32_t &nvis) {
     const uint32_t j = __ffs(ng_bits >> 24) - 1;
     ng_bits &= ~(1u << (24 + j));
@@ -287,8 +290,8 @@ __device__ __forceinline__ bool tri_test(const MeshRef &mr, const LocalRay &r, u
 // Whole traversal of one mesh for one ray (the one-thread-per-ray kernel).
 // The current node group always has a child left at the top of the loop: the
 // root's, then the group a node step returns or one taken from the stack.
-template <bool COUNT, bool DEEP>
-__device__ __forceinline__ void trace_mesh(const MeshRef &mr, const LocalRay &r, Best &best, Stack<DEEP> &st, uint32_t &err,
+template <bool COUNT, typename ST>
+__device__ __forceinline__ void trace_mesh(const MeshRef &mr, const LocalRay &r, Best &best, ST &st, uint32_t &err,
                                            uint32_t &nvis, uint32_t &ntri) {
     uint32_t ng_base = 0, ng_bits = (1u << (24 + r.oct)) | 1u; // the root as slot 0 of a virtual parent
     uint32_t tg_base = 0, tg_bits = 0, visits = 0;
@@ -312,8 +315,8 @@ __device__ __forceinline__ void trace_mesh(const MeshRef &mr, const LocalRay &r,
 // Shadow-ray traversal of one mesh (Traverse_MicroTree_WithStack_AnyHit,
 // CoreRef.cpp:1470-1577): closest-hit order, stopping at the first accepted
 // hit on a solid triangle. Returns true when it stopped there.
-template <bool DEEP>
-__device__ __forceinline__ bool trace_mesh_any(const MeshRef &mr, const LocalRay &r, Best &best, Stack<DEEP> &st, uint32_t &err) {
+template <typename ST>
+__device__ __forceinline__ bool trace_mesh_any(const MeshRef &mr, const LocalRay &r, Best &best, ST &st, uint32_t &err) {
     uint32_t ng_base = 0, ng_bits = (1u << (24 + r.oct)) | 1u;
     uint32_t tg_base = 0, tg_bits = 0, visits = 0, nvis = 0, ntri = 0;
     st.sp = 0;
