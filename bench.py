@@ -773,27 +773,24 @@ def run_gpu_arm(args) -> None:
     def step():
         sc.trace_closest_device(rays_d.data_ptr(), N_RAYS, hits_d.data_ptr(), 0, sptr)
 
-    # the trace order, measured: input order against rays sorted by the
-    # reference's ray hash (direction sector first, or origin cell first) on
-    # 16 or 32 key bits; the timed steps use --reorder/--reorder-bits
-    variants = {}
-    if not args.no_variants:
-        for mode, bits in ((0, 32), (1, 32), (1, 16), (2, 32), (2, 24)):
-            sc.set_trace_tuning(2, 8, 0, mode, bits)
-            for _ in range(2):
-                step()
-            va, vb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            va.record(stream)
-            for _ in range(5):
-                step()
-            vb.record(stream)
-            torch.cuda.synchronize(dev)
-            variants[f"reorder{mode}_bits{bits}"] = round(va.elapsed_time(vb) / 5, 4)
-    sc.set_trace_tuning(2, 8, 0, args.reorder, args.reorder_bits)
+    # the library's trace tuner (ray_scene_tune_trace) on this scene and these
+    # rays: kernel, L2 residency, cache hint, refill threshold, block size with
+    # stack depth and trace order, one at a time, each the best of two timed
+    # traces; the timed steps use its choice (--trace-tuning default: the
+    # library's defaults instead)
+    tune_report = {}
+    if args.trace_tuning == "auto":
+        chosen, rep = sc.tune_trace_device(rays_d.data_ptr(), N_RAYS, hits_d.data_ptr(), sptr, force=True)
+        for item in rep.split(";"):
+            k, sep, v = item.partition("=")
+            if sep:
+                tune_report[k] = v if k == "chosen" else round(float(v), 4)
+    tuning = sc.get_trace_tuning()
+    names = ("kernel", "refill_min", "deep_stack", "reorder", "reorder_bits", "block", "smem_stack", "stream_hint", "l2_persist")
     # kernels per step: the trace; with a trace order also the key kernel, the
     # sort's histogram and digit passes (and its copy when they are odd)
-    passes = (args.reorder_bits + 7) // 8
-    launches_per_step = 1 + ((2 + passes + (passes & 1)) if args.reorder else 0)
+    passes = (tuning[4] + 7) // 8
+    launches_per_step = 1 + ((2 + passes + (passes & 1)) if tuning[3] else 0)
 
     # counting pass: node visits and triangle tests of this BVH (algorithmic bytes)
     sc.set_counting(True)
@@ -920,8 +917,8 @@ def run_gpu_arm(args) -> None:
                 "config": {"workload": WORKLOAD, "rays_per_step_per_gpu": N_RAYS, "tris": N_TRIS,
                            "l2": "inputs larger than L2 (rays 128 MiB per step, hits 64 MiB)", "bvh_build_s": round(build_s, 3),
                            "bvh_nodes": info.nodes, "bvh_depth": info.depth, "parallelism": f"replicas x{world}",
-                           "trace_order": {"reorder": args.reorder, "bits": args.reorder_bits,
-                                           "ms_per_step_by_variant": variants}},
+                           "trace_tuning": {"chosen": dict(zip(names, tuning)), "tuner": args.trace_tuning,
+                                            "ms_per_trace_by_candidate": tune_report}},
                 "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": N_RAYS * 32, "d2h_bytes_per_step": N_RAYS * 16,
                         "matches_device_path": bool(ok)},
                 "parity": parity, "gpu_launches": args.steps * launches_per_step, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "coherent": coherent,
@@ -958,10 +955,8 @@ def main() -> None:
     ap.add_argument("--diff-lr-rough", type=float, default=1e-2)
     ap.add_argument("--no-diff-oracle-fd", dest="diff_oracle_fd", action="store_false",
                     help="skip the oracle's finite differences in the differentiable form")
-    ap.add_argument("--reorder", type=int, default=0, choices=[0, 1, 2],
-                    help="trace order of the timed steps: 0 input, 1 ray hash, 2 origin cell first")
-    ap.add_argument("--reorder-bits", type=int, default=32)
-    ap.add_argument("--no-variants", action="store_true", help="skip the trace-order variants")
+    ap.add_argument("--trace-tuning", default="auto", choices=["auto", "default"],
+                    help="auto: the library's trace tuner picks the settings of the timed steps; default: its defaults")
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="DRAM bytes per launch of the traversal kernel from an ncu capture (reported as roofline.traffic)")
     args = ap.parse_args()

@@ -293,9 +293,14 @@ int ray_scene_last_trace_info(ray_scene *s, ray_trace_info *out);
  * 65,536 rays are not reordered. block (64, 128, 256; 0 = 128) and smem_stack
  * (16, 24, 32 entries per thread; 0 = 24; not 32 with 256 threads): threads
  * per block of the persistent kernel and the depth of its shared-memory stack
- * (a deeper tree continues in local memory). */
+ * (a deeper tree continues in local memory). stream_hint: 1 = the persistent
+ * kernel reads rays and writes hits with the streaming (evict-first) cache
+ * hint. l2_persist: 1 = the scene's wide nodes, 2 = its leaf triangles, are
+ * marked persisting in L2 for the trace (an access-policy window on the
+ * trace's streams, removed after it; the first such call sets this CUDA
+ * context's persisting-L2 limit, which lasts as long as the context). */
 typedef struct ray_trace_tuning {
-    int kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack;
+    int kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack, stream_hint, l2_persist;
 } ray_trace_tuning;
 int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t);
 int ray_scene_get_trace_tuning(ray_scene *s, ray_trace_tuning *out);
@@ -313,6 +318,41 @@ int ray_scene_mesh_bvh_info(ray_scene *s, uint32_t mesh, ray_bvh_info *out);
  * (48 bytes each), 2 instance records (96 bytes each). Copies at most `bytes`
  * bytes; *out_bytes receives the array size. */
 int ray_scene_debug_read(ray_scene *s, int what, void *dst, uint64_t bytes, uint64_t *out_bytes);
+
+/* Failure detection (no counterpart in the reference, whose OpenCL backend
+ * returns silently on any error, RendererOCL.cpp:474-632), for tests that make
+ * failures happen on the host:
+ * ray_scene_debug_write overwrites bytes of the committed wide nodes (what 0)
+ * or leaf triangles (what 1) from host memory, as a corrupt structure would
+ * hold them; the traversal bounds-checks every node and triangle index it
+ * reads and bounds its steps, so a trace of such a scene ends every ray and
+ * reports RAY_ERR_CUDA (corrupt structure) or RAY_ERR_STACK_OVERFLOW instead
+ * of reading out of bounds. Scene edits that rebuild the BVH restore it.
+ * ray_debug_fail_device_alloc: the after-th next device allocation the
+ * library makes fails as a full device would (0: the next one; -1: none);
+ * the failing call returns RAY_ERR_OUT_OF_MEMORY and keeps nothing it had
+ * allocated for itself beyond what the handle owns (freed with the handle).
+ * ray_set_wait_timeout_ms: the bound on every host wait of the library
+ * (default 300,000 ms; <= 0 restores it): a wait that runs out returns
+ * RAY_ERR_TIMEOUT without stopping the GPU work it waited for. */
+int ray_scene_debug_write(ray_scene *s, int what, uint64_t offset, const void *src, uint64_t bytes);
+int ray_debug_fail_device_alloc(int64_t after);
+int ray_set_wait_timeout_ms(int64_t ms);
+
+/* Trace tuner (no counterpart in the reference): times the traversal
+ * settings of ray_trace_tuning on the caller's rays (n rays in device memory;
+ * hits: an n-entry device buffer the candidates write) and keeps the fastest
+ * for this scene: one setting at a time from the current ones (kernel, L2
+ * residency, cache hint, refill threshold, block size with stack depth, trace
+ * order), each candidate the best of two timed traces after one untimed.
+ * Every candidate gives the same hits. The choice is cached per scene
+ * signature (triangle, node and instance counts, BVH depth, ray count rounded
+ * to a power of two); a later call with a cached signature applies it without
+ * timing unless flags bit 0 is set. out (may be NULL): the choice. report (may
+ * be NULL): "name=ms;..." of the candidates timed, NUL-terminated within
+ * report_cap bytes. Synchronous. */
+int ray_scene_tune_trace(ray_scene *s, const float *rays, uint64_t n, ray_hit *hits, int flags, void *stream, ray_trace_tuning *out,
+                         char *report, uint64_t report_cap);
 
 /* Diagnostics: copies one of the renderer's device arrays to host memory after
  * the last ray_render. what: 0 the first ray buffer (32 bytes per ray: ox, oy,

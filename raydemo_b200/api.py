@@ -255,19 +255,36 @@ class Scene:
         check(lib().ray_scene_trace_closest(self._h, rays_ptr, n, hits_ptr, obj_ptr or None, capi.RAY_MEM_DEVICE, stream or None))
 
     def set_trace_tuning(self, kernel: int = 0, refill_min: int = 0, deep_stack: int = 0, reorder: int = 0, reorder_bits: int = 0,
-                         block: int = 0, smem_stack: int = 0) -> None:
+                         block: int = 0, smem_stack: int = 0, stream_hint: int = 0, l2_persist: int = 0) -> None:
         """ray_scene_set_trace_tuning: kernel (1 per ray, 2 persistent; 0
         keeps), refill threshold (0 keeps), deep stack, trace order (0 input,
         1 ray hash, 2 origin cell first), the key bits it sorts on, threads
-        per block and shared stack entries (0: 128 and 24)."""
-        t = capi.TraceTuning(kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack)
+        per block and shared stack entries (0: 128 and 24), streaming cache
+        hint on rays and hits, L2 residency (1 nodes, 2 leaf triangles)."""
+        t = capi.TraceTuning(kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack, stream_hint, l2_persist)
         check(lib().ray_scene_set_trace_tuning(self._h, C.byref(t)))
 
+    def tune_trace_device(self, rays_ptr: int, n: int, hits_ptr: int, stream: int = 0, force: bool = False) -> tuple:
+        """ray_scene_tune_trace on n device rays (hits_ptr: an n-entry device
+        buffer): keeps the fastest traversal settings for this scene; returns
+        (settings tuple as get_trace_tuning, report string)."""
+        t = capi.TraceTuning()
+        buf = C.create_string_buffer(4096)
+        check(lib().ray_scene_tune_trace(self._h, rays_ptr, n, hits_ptr, 1 if force else 0, stream or None, C.byref(t), buf, 4096))
+        return self.get_trace_tuning(), buf.value.decode()
+
+    def debug_write(self, what: int, offset: int, data: bytes) -> None:
+        """ray_scene_debug_write: overwrite bytes of the committed wide nodes
+        (0) or leaf triangles (1), for failure-detection tests."""
+        b = C.create_string_buffer(bytes(data), len(data))
+        check(lib().ray_scene_debug_write(self._h, what, offset, b, len(data)))
+
     def get_trace_tuning(self) -> tuple:
-        """(kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack)"""
+        """(kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack, stream_hint, l2_persist)"""
         t = capi.TraceTuning()
         check(lib().ray_scene_get_trace_tuning(self._h, C.byref(t)))
-        return t.kernel, t.refill_min, t.deep_stack, t.reorder, t.reorder_bits, t.block, t.smem_stack
+        return (t.kernel, t.refill_min, t.deep_stack, t.reorder, t.reorder_bits, t.block, t.smem_stack, t.stream_hint,
+                t.l2_persist)
 
     def set_counting(self, enable: bool) -> None:
         check(lib().ray_scene_set_counting(self._h, int(enable)))

@@ -2,11 +2,21 @@
 // Scene semantics follow the reference Ref::Scene (src/Ray/internal/SceneRef.cpp)
 // and SceneBase (src/Ray/SceneBase.cpp); file:line citations per function.
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstdlib>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <functional>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
 #include <mutex>
 #include <new>
+#include <thread>
+#include <unordered_set>
 
 #include "../../include/raygpu.h"
 #include "radix_sort.cuh"
@@ -22,11 +32,52 @@ thread_local std::string g_last_error;
 
 void set_error(const std::string &msg) { g_last_error = msg; }
 
+namespace {
+std::atomic<long long> g_wait_timeout_ms{300000};
+std::atomic<long long> g_fail_alloc_after{-1}; // >= 0: allocations to let through before one fails
+} // namespace
+
+cudaError_t device_alloc(void **p, size_t bytes) {
+    long long k = g_fail_alloc_after.load();
+    while (k >= 0) {
+        if (g_fail_alloc_after.compare_exchange_weak(k, k - 1)) {
+            if (k == 0) { // this one fails, as cudaMalloc does when the device is full
+                *p = nullptr;
+                return cudaErrorMemoryAllocation;
+            }
+            break;
+        }
+    }
+    return cudaMalloc(p, bytes);
+}
+
+namespace {
+// Polls query() until it stops returning cudaErrorNotReady: spinning for the
+// first milliseconds (short GPU work returns promptly), then sleeping 50 us
+// between polls, up to the wait bound.
+template <typename Q>
+cudaError_t bounded_wait(Q query) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const long long limit = g_wait_timeout_ms.load();
+    for (uint64_t k = 0;; k++) {
+        const cudaError_t e = query();
+        if (e != cudaErrorNotReady) return e;
+        const long long ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
+        if (ms >= limit) return cudaErrorTimeout;
+        if (ms >= 20) std::this_thread::sleep_for(std::chrono::microseconds(50));
+        else std::this_thread::yield();
+    }
+}
+} // namespace
+
+cudaError_t wait_event(cudaEvent_t e) { return bounded_wait([&] { return cudaEventQuery(e); }); }
+cudaError_t wait_stream(cudaStream_t s) { return bounded_wait([&] { return cudaStreamQuery(s); }); }
+
 cudaError_t DeviceBuf::ensure(size_t n) {
     if (n <= bytes && p) return cudaSuccess;
     release();
     const size_t want = std::max<size_t>(n, 256);
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = device_alloc(&p, want);
     if (e != cudaSuccess) {
         p = nullptr;
         bytes = 0;
@@ -180,6 +231,16 @@ std::recursive_mutex &api_mutex() {
     return m;
 }
 
+namespace {
+std::unordered_set<const void *> &live_handles() {
+    static std::unordered_set<const void *> h;
+    return h;
+}
+} // namespace
+
+bool live_scene(const ray_scene *s) { return live_handles().count(s) != 0; }
+bool live_renderer(const ray_renderer *r) { return live_handles().count(r) != 0; }
+
 cudaError_t note_use(ray_scene *s, cudaStream_t st) {
     for (auto &u : s->users)
         if (u.first == st) return cudaEventRecord(u.second, st);
@@ -217,14 +278,15 @@ int commit(ray_scene *s) {
             RG_CUDA_TRY(verts.ensure(m.verts.size() * sizeof(float)));
             RG_CUDA_TRY(mat.ensure(m.mat.size() * sizeof(uint32_t)));
             RG_CUDA_TRY(aabb.ensure((size_t)n * 6 * sizeof(float)));
-            RG_CUDA_TRY(cudaMalloc(&m.tris_ref, (size_t)n * sizeof(TriRec)));
+            RG_CUDA_TRY(device_alloc(reinterpret_cast<void **>(&m.tris_ref), (size_t)n * sizeof(TriRec)));
             RG_CUDA_TRY(cudaMemcpyAsync(verts.p, m.verts.data(), m.verts.size() * sizeof(float), cudaMemcpyHostToDevice, st));
             RG_CUDA_TRY(cudaMemcpyAsync(mat.p, m.mat.data(), m.mat.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
             RG_CUDA_TRY(launch_preprocess_tris(static_cast<const float *>(verts.p), static_cast<const uint32_t *>(mat.p), n, m.tris_ref,
                                                static_cast<float *>(aabb.p), st));
+            free_mesh_bvh(m.bvh); // what an earlier, failed build of this mesh left
             const int rc = build_mesh_bvh(m.tris_ref, static_cast<const float *>(aabb.p), n, m.bvh, st);
             if (rc != RAY_OK) return rc;
-            RG_CUDA_TRY(cudaStreamSynchronize(st));
+            RG_CUDA_TRY(wait_stream(st));
         }
         m.built = true;
     }
@@ -305,7 +367,7 @@ int commit(ray_scene *s) {
             s->world_min[k] = std::min(s->world_min[k], q.bbox_min[k]);
             s->world_max[k] = std::max(s->world_max[k], q.bbox_max[k]);
         }
-    RG_CUDA_TRY(cudaStreamSynchronize(st));
+    RG_CUDA_TRY(wait_stream(st));
     s->geom_dirty = s->inst_dirty = false;
     return upload_shading(s);
 }
@@ -373,6 +435,7 @@ int ray_create_renderer(const ray_settings *s, ray_renderer **out) {
         return RAY_ERR_CUDA;
     }
     r->stream = r->own_stream;
+    live_handles().insert(r);
     *out = r;
     return RAY_OK;
     RG_GUARD_END
@@ -380,12 +443,16 @@ int ray_create_renderer(const ray_settings *s, ray_renderer **out) {
 
 int ray_destroy_renderer(ray_renderer *r) {
     RG_API_LOCK;
+    if (!r) return RAY_OK;
+    RG_CHECK(live_renderer(r), "unknown or already destroyed renderer handle");
+    live_handles().erase(r);
     delete r;
     return RAY_OK;
 }
 
 int ray_renderer_type(const ray_renderer *r, int *out_type) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     RG_CHECK(r && out_type, "null argument");
     *out_type = RAY_RENDERER_CUDA_SM100;
     return RAY_OK;
@@ -393,6 +460,7 @@ int ray_renderer_type(const ray_renderer *r, int *out_type) {
 
 int ray_renderer_size(const ray_renderer *r, int *w, int *h) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     RG_CHECK(r && w && h, "null argument");
     *w = r->w;
     *h = r->h;
@@ -401,6 +469,7 @@ int ray_renderer_size(const ray_renderer *r, int *w, int *h) {
 
 int ray_create_scene(ray_renderer *r, ray_scene **out) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     RG_CHECK(r && out, "null argument");
     RG_GUARD_BEGIN
     RG_CUDA_TRY(cudaSetDevice(r->device));
@@ -421,6 +490,7 @@ int ray_create_scene(ray_renderer *r, ray_scene **out) {
     s->env.env_col[0] = s->env.env_col[1] = s->env.env_col[2] = 0.0f;
     s->env.env_clamp = 0.0f;
     s->env.env_map = s->default_env_texture;
+    live_handles().insert(s);
     *out = s;
     return RAY_OK;
     RG_GUARD_END
@@ -428,12 +498,16 @@ int ray_create_scene(ray_renderer *r, ray_scene **out) {
 
 int ray_destroy_scene(ray_scene *s) {
     RG_API_LOCK;
+    if (!s) return RAY_OK;
+    RG_CHECK(live_scene(s), "unknown or already destroyed scene handle");
+    live_handles().erase(s);
     delete s;
     return RAY_OK;
 }
 
 int ray_scene_get_environment(ray_scene *s, ray_environment_desc *out) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && out, "null argument");
     *out = s->env;
     return RAY_OK;
@@ -441,6 +515,7 @@ int ray_scene_get_environment(ray_scene *s, ray_environment_desc *out) {
 
 int ray_scene_set_environment(ray_scene *s, const ray_environment_desc *env) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && env, "null argument");
     s->env = *env;
     if (s->env.env_map == RAY_INVALID_INDEX) s->env.env_map = s->default_env_texture; // SceneRef.cpp:52-59
@@ -449,6 +524,7 @@ int ray_scene_set_environment(ray_scene *s, const ray_environment_desc *env) {
 
 int ray_scene_add_texture(ray_scene *s, const ray_tex_desc *t, uint32_t *out_index) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && t && out_index, "null argument");
     RG_GUARD_BEGIN
     return add_texture(s, t->data, t->w, t->h, t->is_srgb != 0, t->generate_mipmaps != 0, out_index);
@@ -457,6 +533,7 @@ int ray_scene_add_texture(ray_scene *s, const ray_tex_desc *t, uint32_t *out_ind
 
 int ray_scene_remove_texture(ray_scene *s, uint32_t i) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s, "null argument");
     (void)i; // no-op in the reference too (SceneRef.h:84)
     return RAY_OK;
@@ -464,6 +541,7 @@ int ray_scene_remove_texture(ray_scene *s, uint32_t i) {
 
 int ray_scene_add_material(ray_scene *s, const ray_mat_desc *m, uint32_t *out_index) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && m && out_index, "null argument");
     RG_CHECK((m->type >= RAY_MAT_DIFFUSE && m->type <= RAY_MAT_TRANSPARENT) || m->type == RAY_MAT_PRINCIPLED, "invalid material type");
     RG_CHECK(m->type != RAY_MAT_PRINCIPLED || (m->roughness >= 0.0f && m->roughness <= 1.0f && m->metallic >= 0.0f && m->metallic <= 1.0f),
@@ -501,6 +579,7 @@ int ray_scene_add_material(ray_scene *s, const ray_mat_desc *m, uint32_t *out_in
 
 int ray_scene_set_diff_params(ray_scene *s, const ray_diff_params *p) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s, "null scene");
     if (!p) {
         for (MaterialRec &m : s->materials)
@@ -541,6 +620,7 @@ int ray_scene_set_diff_params(ray_scene *s, const ray_diff_params *p) {
 
 int ray_scene_remove_material(ray_scene *s, uint32_t i) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s, "null argument");
     (void)i; // no-op in the reference too (SceneRef.h:87)
     return RAY_OK;
@@ -548,6 +628,7 @@ int ray_scene_remove_material(ray_scene *s, uint32_t i) {
 
 int ray_scene_add_mesh(ray_scene *s, const ray_mesh_desc *d, uint32_t *out_index) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && d && out_index, "null argument");
     RG_CHECK(d->prim_type == 0, "only indexed triangle lists are supported");
     RG_CHECK(d->layout >= RAY_LAYOUT_PNT && d->layout <= RAY_LAYOUT_PNBTT, "invalid vertex layout");
@@ -643,6 +724,7 @@ int ray_scene_add_mesh(ray_scene *s, const ray_mesh_desc *d, uint32_t *out_index
 
 int ray_scene_remove_mesh(ray_scene *s, uint32_t i) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && i < s->meshes.size(), "invalid mesh index");
     RG_GUARD_BEGIN
     // RemoveMesh, SceneRef.cpp:263-303: swap with the last mesh, drop the
@@ -674,6 +756,7 @@ int ray_scene_remove_mesh(ray_scene *s, uint32_t i) {
 
 int ray_scene_add_light(ray_scene *s, const ray_light_desc *d, uint32_t *out_index) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && d && out_index, "null argument");
     RG_CHECK(d->type >= RAY_LIGHT_POINT && d->type <= RAY_LIGHT_SUN, "invalid light type");
     RG_GUARD_BEGIN
@@ -740,6 +823,7 @@ int ray_scene_add_light(ray_scene *s, const ray_light_desc *d, uint32_t *out_ind
 
 int ray_scene_remove_light(ray_scene *s, uint32_t i) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s, "null argument");
     (void)i; // a no-op in the reference (SceneRef.cpp:351-354)
     return RAY_OK;
@@ -747,6 +831,7 @@ int ray_scene_remove_light(ray_scene *s, uint32_t i) {
 
 int ray_scene_add_mesh_instance(ray_scene *s, uint32_t mesh_index, const float xform[16], uint32_t *out_index) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && xform && out_index, "null argument");
     RG_CHECK(mesh_index < s->meshes.size(), "invalid mesh index");
     RG_GUARD_BEGIN
@@ -763,6 +848,7 @@ int ray_scene_add_mesh_instance(ray_scene *s, uint32_t mesh_index, const float x
 
 int ray_scene_set_mesh_instance_transform(ray_scene *s, uint32_t mi, const float xform[16]) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && xform && mi < s->instances.size(), "invalid instance");
     memcpy(s->instances[mi].xform, xform, 64);
     inverse_matrix(s->instances[mi].xform, s->instances[mi].inv_xform);
@@ -772,6 +858,7 @@ int ray_scene_set_mesh_instance_transform(ray_scene *s, uint32_t mi, const float
 
 int ray_scene_remove_mesh_instance(ray_scene *s, uint32_t mi) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && mi < s->instances.size(), "invalid instance");
     s->instances.erase(s->instances.begin() + mi);
     s->inst_dirty = true;
@@ -780,6 +867,7 @@ int ray_scene_remove_mesh_instance(ray_scene *s, uint32_t mi) {
 
 int ray_scene_add_camera(ray_scene *s, const ray_camera_desc *c, uint32_t *out_index) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && c && out_index, "null argument");
     RG_GUARD_BEGIN
     // SceneBase::AddCamera, SceneBase.cpp:8-20
@@ -801,6 +889,7 @@ int ray_scene_add_camera(ray_scene *s, const ray_camera_desc *c, uint32_t *out_i
 
 int ray_scene_get_camera(ray_scene *s, uint32_t i, ray_camera_desc *out) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && out && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");
     // SceneBase::GetCamera, SceneBase.cpp:22-54: the fields of the camera's kind only
     // (origin, fwd and up of the constructed camera_t: up is the orthonormalised one)
@@ -839,6 +928,7 @@ int ray_scene_get_camera(ray_scene *s, uint32_t i, ray_camera_desc *out) {
 
 int ray_scene_set_camera(ray_scene *s, uint32_t i, const ray_camera_desc *c) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && c && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");
     set_camera(s->cameras[i], *c);
     return RAY_OK;
@@ -846,6 +936,7 @@ int ray_scene_set_camera(ray_scene *s, uint32_t i, const ray_camera_desc *c) {
 
 int ray_scene_set_camera_axes(ray_scene *s, uint32_t i, const float side[3], const float up[3]) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && side && up && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");
     memcpy(s->cameras[i].side, side, 3 * sizeof(float));
     memcpy(s->cameras[i].up, up, 3 * sizeof(float));
@@ -854,6 +945,7 @@ int ray_scene_set_camera_axes(ray_scene *s, uint32_t i, const float side[3], con
 
 int ray_scene_remove_camera(ray_scene *s, uint32_t i) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && i < s->cameras.size() && s->cameras[i].alive, "invalid camera");
     s->cameras[i].alive = false;
     s->cameras[i].next_free = s->cam_first_free;
@@ -863,6 +955,7 @@ int ray_scene_remove_camera(ray_scene *s, uint32_t i) {
 
 int ray_scene_current_cam(ray_scene *s, uint32_t *out) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && out, "null argument");
     *out = s->current_cam;
     return RAY_OK;
@@ -870,6 +963,7 @@ int ray_scene_current_cam(ray_scene *s, uint32_t *out) {
 
 int ray_scene_set_current_cam(ray_scene *s, uint32_t i) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s, "null argument");
     s->current_cam = i;
     return RAY_OK;
@@ -877,6 +971,7 @@ int ray_scene_set_current_cam(ray_scene *s, uint32_t i) {
 
 int ray_scene_triangle_count(ray_scene *s, uint32_t *out) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && out, "null argument");
     *out = s->total_tris;
     return RAY_OK;
@@ -884,6 +979,7 @@ int ray_scene_triangle_count(ray_scene *s, uint32_t *out) {
 
 int ray_scene_node_count(ray_scene *s, uint32_t *out) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && out, "null argument");
     RG_GUARD_BEGIN
     const int rc = commit(s);
@@ -895,6 +991,7 @@ int ray_scene_node_count(ray_scene *s, uint32_t *out) {
 
 int ray_scene_commit(ray_scene *s) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s, "null argument");
     RG_GUARD_BEGIN
     return commit(s);
@@ -903,6 +1000,7 @@ int ray_scene_commit(ray_scene *s) {
 
 int ray_scene_mesh_bvh_info(ray_scene *s, uint32_t mesh, ray_bvh_info *out) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && out && mesh < s->meshes.size(), "invalid mesh");
     RG_GUARD_BEGIN
     const int rc = commit(s);
@@ -922,6 +1020,7 @@ int ray_scene_mesh_bvh_info(ray_scene *s, uint32_t mesh, ray_bvh_info *out) {
 
 int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && t, "null argument");
     RG_CHECK(t->kernel >= 0 && t->kernel <= 2, "kernel must be 1 (per ray) or 2 (persistent)");
     RG_CHECK(t->refill_min <= 32, "refill_min is a lane count, at most 32");
@@ -931,6 +1030,8 @@ int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t) {
     RG_CHECK(t->block == 0 || t->block == 64 || t->block == 128 || t->block == 256, "block is 0, 64, 128 or 256");
     RG_CHECK(t->smem_stack == 0 || t->smem_stack == 16 || t->smem_stack == 24 || t->smem_stack == 32, "smem_stack is 0, 16, 24 or 32");
     RG_CHECK(!((t->block == 256) && t->smem_stack == 32), "256 threads with 32 stack entries exceed the block's shared memory");
+    RG_CHECK(t->stream_hint == 0 || t->stream_hint == 1, "stream_hint is 0 or 1");
+    RG_CHECK(t->l2_persist >= 0 && t->l2_persist <= 2, "l2_persist is 0, 1 (nodes) or 2 (leaf triangles)");
     if (t->kernel > 0) s->tuning.kernel = t->kernel;
     if (t->refill_min > 0) s->tuning.refill_min = t->refill_min;
     s->tuning.deep_stack = t->deep_stack;
@@ -938,11 +1039,14 @@ int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t) {
     s->tuning.reorder_bits = t->reorder_bits ? t->reorder_bits : 32;
     s->tuning.block = t->block ? t->block : 128;
     s->tuning.smem_stack = t->smem_stack ? t->smem_stack : 24;
+    s->tuning.stream_hint = t->stream_hint;
+    s->tuning.l2_persist = t->l2_persist;
     return RAY_OK;
 }
 
 int ray_scene_get_trace_tuning(ray_scene *s, ray_trace_tuning *out) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && out, "null argument");
     *out = s->tuning;
     return RAY_OK;
@@ -950,6 +1054,7 @@ int ray_scene_get_trace_tuning(ray_scene *s, ray_trace_tuning *out) {
 
 int ray_scene_set_counting(ray_scene *s, int enable) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s, "null argument");
     s->counting = enable != 0;
     return RAY_OK;
@@ -957,10 +1062,11 @@ int ray_scene_set_counting(ray_scene *s, int enable) {
 
 int ray_scene_last_trace_info(ray_scene *s, ray_trace_info *out) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && out, "null argument");
     if (s->info_pending) {
         RG_CUDA_TRY(cudaSetDevice(s->device));
-        RG_CUDA_TRY(cudaStreamSynchronize(s->info_stream));
+        RG_CUDA_TRY(wait_stream(s->info_stream));
         uint32_t err = 0;
         unsigned long long cnt[2] = {0, 0};
         RG_CUDA_TRY(cudaMemcpy(&err, s->d_err.p, 4, cudaMemcpyDeviceToHost));
@@ -1007,6 +1113,7 @@ constexpr uint64_t kReorderMinRays = 65536;
 
 int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit *hits, int32_t *obj, int mem, void *stream) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s, "null scene");
     RG_CHECK(n == 0 || (rays && hits), "null buffer");
     RG_CHECK(mem == RAY_MEM_HOST || mem == RAY_MEM_DEVICE, "invalid memory space");
@@ -1077,6 +1184,31 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
     tp.refill_min = s->tuning.refill_min;
     tp.block = s->tuning.block;
     tp.smem_stack = s->tuning.smem_stack;
+    tp.stream_hint = s->tuning.stream_hint;
+    // L2 residency of the nodes or leaf triangles: an access-policy window on
+    // the streams the traces run on, taken off again once they are enqueued
+    cudaStreamAttrValue win{};
+    if (s->tuning.l2_persist && n) {
+        const DeviceBuf &b = s->tuning.l2_persist == 1 ? s->d_nodes : s->d_leaf;
+        const size_t bytes = s->tuning.l2_persist == 1 ? (size_t)s->total_nodes * sizeof(WideNode) : (size_t)s->total_tris * sizeof(TriRec);
+        int max_win = 0, max_persist = 0;
+        RG_CUDA_TRY(cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, s->device));
+        RG_CUDA_TRY(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, s->device));
+        if (b.p && bytes && max_win > 0 && max_persist > 0) {
+            const size_t w = std::min(bytes, (size_t)max_win);
+            size_t limit = 0;
+            RG_CUDA_TRY(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize));
+            if (limit < std::min(w, (size_t)max_persist)) {
+                RG_CUDA_TRY(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, std::min(w, (size_t)max_persist)));
+                RG_CUDA_TRY(cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize));
+            }
+            win.accessPolicyWindow.base_ptr = b.p;
+            win.accessPolicyWindow.num_bytes = w;
+            win.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)limit / (double)w);
+            win.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+            win.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        }
+    }
     for (const MeshRec &m : s->meshes) tp.max_depth = std::max(tp.max_depth, m.bvh.depth);
     if (s->tuning.deep_stack) tp.max_depth = 0xffffffffu;
     uint32_t *next_ray = static_cast<uint32_t *>(s->d_next_ray.p);
@@ -1107,9 +1239,14 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
                                    s->d_order[k & 1].p, &order, ts));
             tp.order = order;
         }
+        if (win.accessPolicyWindow.num_bytes) RG_CUDA_TRY(cudaStreamSetAttribute(ts, cudaStreamAttributeAccessPolicyWindow, &win));
         RG_CUDA_TRY(launch_trace_closest(sv, d_rays + 2 * b, (uint32_t)m, d_hits + b, d_obj ? d_obj + b : nullptr,
                                          static_cast<uint32_t *>(s->d_err.p), static_cast<unsigned long long *>(s->d_counters.p), s->counting,
                                          ts, tp));
+        if (win.accessPolicyWindow.num_bytes) {
+            cudaStreamAttrValue off{};
+            RG_CUDA_TRY(cudaStreamSetAttribute(ts, cudaStreamAttributeAccessPolicyWindow, &off));
+        }
         if (mem == RAY_MEM_HOST && m) {
             if (piped) {
                 RG_CUDA_TRY(cudaEventRecord(s->pipe_ev[2], ts));
@@ -1146,6 +1283,7 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
 
 int ray_scene_debug_read(ray_scene *s, int what, void *dst, uint64_t bytes, uint64_t *out_bytes) {
     RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && out_bytes, "null argument");
     RG_CHECK(what >= 0 && what <= 2, "invalid array selector");
     RG_GUARD_BEGIN
@@ -1167,6 +1305,155 @@ int ray_scene_debug_read(ray_scene *s, int what, void *dst, uint64_t bytes, uint
     *out_bytes = total;
     const uint64_t n = std::min(total, bytes);
     if (n && dst) RG_CUDA_TRY(cudaMemcpy(dst, src, n, cudaMemcpyDeviceToHost));
+    return RAY_OK;
+    RG_GUARD_END
+}
+
+int ray_scene_debug_write(ray_scene *s, int what, uint64_t offset, const void *src, uint64_t bytes) {
+    RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
+    RG_CHECK(s && (src || bytes == 0), "null argument");
+    RG_CHECK(what == 0 || what == 1, "invalid array selector");
+    RG_GUARD_BEGIN
+    RG_CUDA_TRY(cudaSetDevice(s->device));
+    const int rc = commit(s);
+    if (rc != RAY_OK) return rc;
+    const uint64_t total = what == 0 ? (uint64_t)s->total_nodes * sizeof(WideNode) : (uint64_t)s->total_tris * sizeof(TriRec);
+    RG_CHECK(offset <= total && bytes <= total - offset, "write outside the array");
+    char *dst = static_cast<char *>(what == 0 ? s->d_nodes.p : s->d_leaf.p);
+    // after the work in flight that reads the scene
+    for (auto &u : s->users) RG_CUDA_TRY(cudaStreamWaitEvent(s->stream, u.second, 0));
+    if (bytes) RG_CUDA_TRY(cudaMemcpyAsync(dst + offset, src, bytes, cudaMemcpyHostToDevice, s->stream));
+    RG_CUDA_TRY(wait_stream(s->stream));
+    return RAY_OK;
+    RG_GUARD_END
+}
+
+int ray_debug_fail_device_alloc(int64_t after) {
+    g_fail_alloc_after.store(after < 0 ? -1 : (long long)after);
+    return RAY_OK;
+}
+
+int ray_set_wait_timeout_ms(int64_t ms) {
+    g_wait_timeout_ms.store(ms <= 0 ? 300000 : (long long)ms);
+    return RAY_OK;
+}
+
+namespace {
+// Scene signature -> the tuner's choice (process-wide, under the API lock).
+struct TuneKey {
+    uint64_t tris, nodes, inst, depth, log2n;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(tris, nodes, inst, depth, log2n) < std::tie(o.tris, o.nodes, o.inst, o.depth, o.log2n);
+    }
+};
+std::map<TuneKey, ray_trace_tuning> &tune_cache() {
+    static std::map<TuneKey, ray_trace_tuning> c;
+    return c;
+}
+} // namespace
+
+int ray_scene_tune_trace(ray_scene *s, const float *rays, uint64_t n, ray_hit *hits, int flags, void *stream, ray_trace_tuning *out,
+                         char *report, uint64_t report_cap) {
+    RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
+    RG_CHECK(s && rays && hits && n > 0, "null argument or no rays");
+    RG_CHECK(n <= 0xffffffffull, "too many rays in one call");
+    RG_GUARD_BEGIN
+    RG_CUDA_TRY(cudaSetDevice(s->device));
+    int rc = commit(s);
+    if (rc != RAY_OK) return rc;
+    uint64_t lg = 0;
+    while ((2ull << lg) <= n) lg++;
+    const TuneKey key{s->total_tris, s->total_nodes, s->n_inst_dev, s->max_depth, lg};
+    std::string log;
+    auto finish = [&]() {
+        if (out) *out = s->tuning;
+        if (report && report_cap) {
+            const size_t m = std::min<size_t>(log.size(), report_cap - 1);
+            memcpy(report, log.data(), m);
+            report[m] = 0;
+        }
+    };
+    auto it = tune_cache().find(key);
+    if (it != tune_cache().end() && !(flags & 1)) {
+        s->tuning = it->second;
+        log = "cached";
+        finish();
+        return RAY_OK;
+    }
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    RG_CUDA_TRY(cudaEventCreate(&e0));
+    RG_CUDA_TRY(cudaEventCreate(&e1));
+    auto time_of = [&](const ray_trace_tuning &t, float &best) -> int {
+        s->tuning = t;
+        best = 1e30f;
+        for (int k = 0; k < 3; k++) {
+            RG_CUDA_TRY(cudaEventRecord(e0, st));
+            const int r2 = ray_scene_trace_closest(s, rays, n, hits, nullptr, RAY_MEM_DEVICE, st);
+            if (r2 != RAY_OK) return r2;
+            RG_CUDA_TRY(cudaEventRecord(e1, st));
+            RG_CUDA_TRY(wait_event(e1));
+            float ms = 0.0f;
+            RG_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+            if (k > 0) best = std::min(best, ms); // the first is the untimed one
+        }
+        return RAY_OK;
+    };
+    ray_trace_tuning cur = s->tuning;
+    float cur_ms = 0.0f;
+    auto name_of = [](const ray_trace_tuning &t) {
+        char b[160];
+        snprintf(b, sizeof b, "k%d_r%d_l2%d_h%d_b%d_s%d_o%d_%d", t.kernel, t.refill_min, t.l2_persist, t.stream_hint, t.block, t.smem_stack,
+                 t.reorder, t.reorder_bits);
+        return std::string(b);
+    };
+    rc = time_of(cur, cur_ms);
+    if (rc == RAY_OK) {
+        log += name_of(cur) + "=" + std::to_string(cur_ms) + ";";
+        // one setting at a time, each stage starting from the best so far
+        using Mut = std::function<void(ray_trace_tuning &)>;
+        std::vector<std::vector<Mut>> stages = {
+            {[](ray_trace_tuning &t) { t.kernel = 2; }, [](ray_trace_tuning &t) { t.kernel = 1; }},
+            {[](ray_trace_tuning &t) { t.l2_persist = 0; }, [](ray_trace_tuning &t) { t.l2_persist = 1; },
+             [](ray_trace_tuning &t) { t.l2_persist = 2; }},
+            {[](ray_trace_tuning &t) { t.stream_hint = 0; }, [](ray_trace_tuning &t) { t.stream_hint = 1; }},
+            {[](ray_trace_tuning &t) { t.refill_min = 4; }, [](ray_trace_tuning &t) { t.refill_min = 8; },
+             [](ray_trace_tuning &t) { t.refill_min = 12; }, [](ray_trace_tuning &t) { t.refill_min = 16; }},
+            {[](ray_trace_tuning &t) { t.block = 128; t.smem_stack = 24; }, [](ray_trace_tuning &t) { t.block = 64; t.smem_stack = 24; },
+             [](ray_trace_tuning &t) { t.block = 256; t.smem_stack = 24; }, [](ray_trace_tuning &t) { t.block = 128; t.smem_stack = 16; },
+             [](ray_trace_tuning &t) { t.block = 64; t.smem_stack = 32; }, [](ray_trace_tuning &t) { t.block = 256; t.smem_stack = 16; }},
+            {[](ray_trace_tuning &t) { t.reorder = 0; t.reorder_bits = 32; }, [](ray_trace_tuning &t) { t.reorder = 1; t.reorder_bits = 32; },
+             [](ray_trace_tuning &t) { t.reorder = 2; t.reorder_bits = 24; }}};
+        for (size_t si = 0; si < stages.size() && rc == RAY_OK; si++) {
+            if (si > 0 && cur.kernel == 1 && si != 5) continue; // the per-ray kernel takes only the trace order
+            ray_trace_tuning best_t = cur;
+            float best_ms = cur_ms;
+            for (const Mut &mut : stages[si]) {
+                ray_trace_tuning t = cur;
+                mut(t);
+                if (memcmp(&t, &cur, sizeof t) == 0) continue;
+                float ms = 0.0f;
+                rc = time_of(t, ms);
+                if (rc != RAY_OK) break;
+                log += name_of(t) + "=" + std::to_string(ms) + ";";
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best_t = t;
+                }
+            }
+            cur = best_t;
+            cur_ms = best_ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->tuning = cur;
+    if (rc != RAY_OK) return rc;
+    tune_cache()[key] = cur;
+    log += "chosen=" + name_of(cur);
+    finish();
     return RAY_OK;
     RG_GUARD_END
 }

@@ -463,7 +463,7 @@ __global__ void k_collapse(const QItem *__restrict__ in, uint32_t n_in, QItem *_
 
 template <typename T>
 cudaError_t dalloc(T **p, size_t count) {
-    return cudaMalloc(reinterpret_cast<void **>(p), std::max<size_t>(count, 1) * sizeof(T));
+    return device_alloc(reinterpret_cast<void **>(p), std::max<size_t>(count, 1) * sizeof(T));
 }
 
 // Scratch allocations of one build, released when the build returns.
@@ -564,7 +564,7 @@ int build_mesh_bvh(const TriRec *tris_ref, const float *aabb, uint32_t n, MeshBv
                                                       open_k, out.nodes, out.leaf_tris);
         RG_CUDA_TRY(cudaGetLastError());
         RG_CUDA_TRY(cudaMemcpyAsync(&n_in, counters + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        RG_CUDA_TRY(cudaStreamSynchronize(st));
+        RG_CUDA_TRY(wait_stream(st));
         std::swap(qa, qb);
     }
     uint32_t cnt[4];
@@ -575,7 +575,7 @@ int build_mesh_bvh(const TriRec *tris_ref, const float *aabb, uint32_t n, MeshBv
     } else {
         RG_CUDA_TRY(cudaMemcpyAsync(rootbox, aabb, sizeof(rootbox), cudaMemcpyDeviceToHost, st));
     }
-    RG_CUDA_TRY(cudaStreamSynchronize(st));
+    RG_CUDA_TRY(wait_stream(st));
     out.node_count = cnt[0];
     out.tri_count = cnt[1];
     out.depth = cnt[3];

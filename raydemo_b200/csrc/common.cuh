@@ -75,13 +75,25 @@ constexpr int LEAF_MAX_TRIS = 3;
 // Error helpers for host code.
 namespace rg {
 void set_error(const std::string &msg);
-}
+// Every device allocation of the library goes through device_alloc, so that
+// a test can make the n-th next one fail on the host (ray_debug_fail_device_alloc).
+cudaError_t device_alloc(void **p, size_t bytes);
+// Host waits with a bound (ray_set_wait_timeout_ms; default 300 s): poll the
+// event or stream until it completes, an error is reported, or the bound
+// passes (cudaErrorTimeout; the GPU work itself is not stopped).
+cudaError_t wait_event(cudaEvent_t e);
+cudaError_t wait_stream(cudaStream_t s);
+} // namespace rg
 
+// Returns from the calling entry point with the RAY_ERR_* code of a failed
+// CUDA call (a bounded wait that ran out: RAY_ERR_TIMEOUT; a failed
+// allocation: RAY_ERR_OUT_OF_MEMORY; anything else: RAY_ERR_CUDA).
 #define RG_CUDA_TRY(expr)                                                                                              \
     do {                                                                                                               \
         cudaError_t _e = (expr);                                                                                       \
         if (_e != cudaSuccess) {                                                                                       \
             ::rg::set_error(std::string(#expr " failed: ") + cudaGetErrorString(_e));                                 \
-            return RAY_ERR_CUDA;                                                                                       \
+            return _e == cudaErrorTimeout ? RAY_ERR_TIMEOUT                                                            \
+                                          : (_e == cudaErrorMemoryAllocation ? RAY_ERR_OUT_OF_MEMORY : RAY_ERR_CUDA); \
         }                                                                                                              \
     } while (0)

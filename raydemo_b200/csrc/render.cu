@@ -18,6 +18,14 @@
 
 using namespace rg;
 
+#define RG_CHECK(cond, msg)                                                                                            \
+    do {                                                                                                               \
+        if (!(cond)) {                                                                                                 \
+            set_error(msg);                                                                                            \
+            return RAY_ERR_INVALID_ARG;                                                                                \
+        }                                                                                                              \
+    } while (0)
+
 namespace {
 
 constexpr int MAX_BOUNCES = 10; // Core.h:53
@@ -135,7 +143,7 @@ int resolve_stats(ray_renderer *r, int set) {
     if (!r->ev_frame_pending[set]) return RAY_OK;
     cudaEvent_t *e = r->ev_sets[set];
     const int nb = r->ev_bounces[set];
-    RG_CUDA_TRY(cudaEventSynchronize(e[N_EVENTS - 1]));
+    RG_CUDA_TRY(wait_event(e[N_EVENTS - 1]));
     auto ms_between = [&](int a, int b) -> float {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, e[a], e[b]);
@@ -658,6 +666,7 @@ extern "C" {
 int ray_sort_rays(ray_renderer *r, const float *rays, uint64_t n, const float root_min[3], const float cell_size[3], uint32_t *keys_out,
                   uint32_t *perm_out, float *rays_out, void *stream) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     if (!r || !root_min || !cell_size || (n && (!rays || !perm_out))) {
         set_error("ray_sort_rays: null argument");
         return RAY_ERR_INVALID_ARG;
@@ -677,13 +686,14 @@ int ray_sort_rays(ray_renderer *r, const float *rays, uint64_t n, const float ro
 
 int ray_resize(ray_renderer *r, int w, int h) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     if (!r || w <= 0 || h <= 0 || w > 32768 || h > 32768) {
         set_error("invalid size");
         return RAY_ERR_INVALID_ARG;
     }
     if (w == r->w && h == r->h) return RAY_OK;
     RG_CUDA_TRY(cudaSetDevice(r->device));
-    RG_CUDA_TRY(cudaStreamSynchronize(r->stream));
+    RG_CUDA_TRY(wait_stream(r->stream));
     // Framebuffer::Resize (FramebufferRef.cpp:10-27): the pixel array keeps
     // its leading elements and the new ones are zero
     const size_t n_old = (size_t)r->w * r->h, n_new = (size_t)w * h;
@@ -707,6 +717,7 @@ int ray_resize(ray_renderer *r, int w, int h) {
 
 int ray_clear(ray_renderer *r, const ray_pixel *c) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     if (!r) {
         set_error("null renderer");
         return RAY_ERR_INVALID_ARG;
@@ -723,6 +734,8 @@ int ray_clear(ray_renderer *r, const ray_pixel *c) {
 
 int ray_render(ray_renderer *r, ray_scene *s, ray_region *region) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     try {
         FrameJob J;
         ray_rect rect;
@@ -792,6 +805,10 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
     try {
         ray_renderer *r0 = renderers[0];
         for (int i = 0; i < count; i++) {
+            if (renderers[i] && scenes[i] && (!live_renderer(renderers[i]) || !live_scene(scenes[i]))) {
+                set_error("unknown or destroyed renderer or scene handle");
+                return RAY_ERR_INVALID_ARG;
+            }
             if (!renderers[i] || !scenes[i] || !regions[i]) {
                 set_error("null argument");
                 return RAY_ERR_INVALID_ARG;
@@ -895,7 +912,7 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
         }
         if (tune_entry >= 0) { // a timed call of the kernel choice
             RG_CUDA_TRY(cudaEventRecord(r0->ev_batch[1], st));
-            RG_CUDA_TRY(cudaEventSynchronize(r0->ev_batch[1]));
+            RG_CUDA_TRY(wait_event(r0->ev_batch[1]));
             float ms = 0.0f;
             RG_CUDA_TRY(cudaEventElapsedTime(&ms, r0->ev_batch[0], r0->ev_batch[1]));
             ray_renderer::TuneEntry &e = r0->tune[tune_entry];
@@ -912,6 +929,7 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
 
 int ray_renderer_set_kernel(ray_renderer *r, int kernel) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     if (!r || kernel < 0 || kernel > 2) {
         set_error("kernel must be 0 (chosen by timing), 1 (wavefront) or 2 (path kernel)");
         return RAY_ERR_INVALID_ARG;
@@ -922,6 +940,8 @@ int ray_renderer_set_kernel(ray_renderer *r, int kernel) {
 
 int ray_render_diff(ray_renderer *r, ray_scene *s, int first_iteration, int samples, float *image_rgb, float *sample_rgb) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     try {
         if (!image_rgb || !sample_rgb) {
             set_error("null output buffer");
@@ -953,6 +973,8 @@ int ray_render_diff(ray_renderer *r, ray_scene *s, int first_iteration, int samp
 int ray_render_adjoint(ray_renderer *r, ray_scene *s, int first_iteration, int samples, const float *sample_rgb, const float *d_image,
                        float *grad_albedo, float *grad_roughness) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     try {
         if (!r || !s || !sample_rgb || !d_image || !grad_albedo || !grad_roughness) {
             set_error("null argument");
@@ -1004,6 +1026,7 @@ int ray_render_adjoint(ray_renderer *r, ray_scene *s, int first_iteration, int s
 
 int ray_renderer_set_ray_sort(ray_renderer *r, int policy) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     if (!r || policy < -1 || policy > (int)SORT_ALL) {
         set_error("ray sort policy must be RAY_SORT_AUTO (-1), 0 or a mask of bounces within RAY_SORT_ALL");
         return RAY_ERR_INVALID_ARG;
@@ -1014,6 +1037,7 @@ int ray_renderer_set_ray_sort(ray_renderer *r, int policy) {
 
 int ray_get_pixels(ray_renderer *r, const ray_pixel **out, int on_device) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     if (!r || !out) {
         set_error("null argument");
         return RAY_ERR_INVALID_ARG;
@@ -1021,7 +1045,7 @@ int ray_get_pixels(ray_renderer *r, const ray_pixel **out, int on_device) {
     RG_CUDA_TRY(cudaSetDevice(r->device));
     int rc = ensure_frame_buffers(r, false);
     if (rc != RAY_OK) return rc;
-    RG_CUDA_TRY(cudaStreamSynchronize(r->stream));
+    RG_CUDA_TRY(wait_stream(r->stream));
     if (on_device) {
         *out = static_cast<const ray_pixel *>(r->d_final.p);
         return RAY_OK;
@@ -1038,6 +1062,7 @@ int ray_get_pixels(ray_renderer *r, const ray_pixel **out, int on_device) {
 
 int ray_get_sh_data(ray_renderer *r, const ray_shl1 **out) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     if (!r || !out) {
         set_error("null argument");
         return RAY_ERR_INVALID_ARG;
@@ -1047,7 +1072,7 @@ int ray_get_sh_data(ray_renderer *r, const ray_shl1 **out) {
         return RAY_OK;
     }
     RG_CUDA_TRY(cudaSetDevice(r->device));
-    RG_CUDA_TRY(cudaStreamSynchronize(r->stream));
+    RG_CUDA_TRY(wait_stream(r->stream));
     const size_t n = (size_t)r->w * r->h;
     if (!r->sh_on_host || r->host_sh.size() != n) {
         r->host_sh.resize(n);
@@ -1060,12 +1085,13 @@ int ray_get_sh_data(ray_renderer *r, const ray_shl1 **out) {
 
 int ray_renderer_debug_read(ray_renderer *r, int what, void *dst, uint64_t bytes, uint64_t *out_bytes) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     if (!r || !out_bytes || (bytes && !dst) || what < 0 || what > 3) {
         set_error("invalid argument");
         return RAY_ERR_INVALID_ARG;
     }
     RG_CUDA_TRY(cudaSetDevice(r->device));
-    RG_CUDA_TRY(cudaStreamSynchronize(r->stream));
+    RG_CUDA_TRY(wait_stream(r->stream));
     const DeviceBuf *b = what == 0 ? &r->d_rays[0] : (what == 1 ? &r->d_pay[0] : (what == 2 ? &r->d_halton : &r->d_temp));
     const uint64_t size = what == 2 ? (b->p ? HALTON_COUNT * HALTON_SEQ_LEN * sizeof(float) : 0) : b->bytes;
     *out_bytes = size;
@@ -1076,6 +1102,7 @@ int ray_renderer_debug_read(ray_renderer *r, int what, void *dst, uint64_t bytes
 
 int ray_renderer_set_stream(ray_renderer *r, void *stream) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     if (!r) {
         set_error("null renderer");
         return RAY_ERR_INVALID_ARG;
@@ -1083,13 +1110,14 @@ int ray_renderer_set_stream(ray_renderer *r, void *stream) {
     cudaStream_t next = stream ? static_cast<cudaStream_t>(stream) : r->own_stream;
     if (next == r->stream) return RAY_OK;
     RG_CUDA_TRY(cudaSetDevice(r->device));
-    RG_CUDA_TRY(cudaStreamSynchronize(r->stream)); // work on the old stream finishes first
+    RG_CUDA_TRY(wait_stream(r->stream)); // work on the old stream finishes first
     r->stream = next;
     return RAY_OK;
 }
 
 int ray_renderer_frame_info(ray_renderer *r, ray_frame_info *out) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     if (!r || !out) {
         set_error("null argument");
         return RAY_ERR_INVALID_ARG;
@@ -1097,7 +1125,7 @@ int ray_renderer_frame_info(ray_renderer *r, ray_frame_info *out) {
     *out = ray_frame_info{};
     if (!r->d_counters.p) return RAY_OK;
     RG_CUDA_TRY(cudaSetDevice(r->device));
-    RG_CUDA_TRY(cudaStreamSynchronize(r->stream));
+    RG_CUDA_TRY(wait_stream(r->stream));
     uint32_t c[8];
     RG_CUDA_TRY(cudaMemcpy(c, r->d_counters.p, sizeof(c), cudaMemcpyDeviceToHost));
     out->error_flags = c[3];
@@ -1110,6 +1138,7 @@ int ray_renderer_frame_info(ray_renderer *r, ray_frame_info *out) {
 
 int ray_get_stats(ray_renderer *r, ray_stats *out) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     if (!r || !out) {
         set_error("null argument");
         return RAY_ERR_INVALID_ARG;
@@ -1127,6 +1156,7 @@ int ray_get_stats(ray_renderer *r, ray_stats *out) {
 
 int ray_reset_stats(ray_renderer *r) {
     RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     if (!r) {
         set_error("null argument");
         return RAY_ERR_INVALID_ARG;

@@ -73,6 +73,11 @@ struct DeviceBuf {
 // regions of one renderer and scene from a thread pool -- are serialised onto
 // the renderer's stream in the order they take the lock.
 std::recursive_mutex &api_mutex();
+// api.cu: the handles that ray_create_* returned and ray_destroy_* has not
+// destroyed (read and changed under the API lock): an entry point given any
+// other pointer returns RAY_ERR_INVALID_ARG instead of dereferencing it.
+bool live_scene(const ray_scene *s);
+bool live_renderer(const ray_renderer *r);
 #define RG_API_LOCK std::lock_guard<std::recursive_mutex> rg_api_lock_(rg::api_mutex())
 
 // api.cu: builds pending BVHs and uploads pending scene data, after the
@@ -136,7 +141,7 @@ struct ray_scene {
     // batch-trace staging and diagnostics
     rg::DeviceBuf d_rays, d_hits, d_obj, d_err, d_counters, d_next_ray;
     rg::DeviceBuf d_order[2]; // reordered traces: keys, order and sort scratch of each of two concurrent chunks
-    ray_trace_tuning tuning{2, 8, 0, 0, 32, 128, 24};
+    ray_trace_tuning tuning{2, 8, 0, 0, 32, 128, 24, 0, 0};
     bool counting = false;
     ray_trace_info last_info{};
     bool info_pending = false;

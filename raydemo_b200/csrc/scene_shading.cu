@@ -335,7 +335,7 @@ int upload_shading(ray_scene *s) {
     if (!td.empty()) RG_CUDA_TRY(cudaMemcpyAsync(s->d_textures.p, td.data(), td.size() * sizeof(TexDev), cudaMemcpyHostToDevice, st));
     if (!texels.empty())
         RG_CUDA_TRY(cudaMemcpyAsync(s->d_texels.p, texels.data(), texels.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-    RG_CUDA_TRY(cudaStreamSynchronize(st));
+    RG_CUDA_TRY(wait_stream(st));
     s->shade_dirty = false;
     return RAY_OK;
 }

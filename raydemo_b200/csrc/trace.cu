@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
                                                                   uint32_t *__restrict__ next_ray, int refill_min,
                                                                   const uint32_t *__restrict__ n_dev, const uint8_t *__restrict__ views = nullptr,
                                                                   uint32_t view_stride = 0, const uint32_t *__restrict__ ray_job = nullptr,
-                                                                  const uint32_t *__restrict__ order = nullptr) {
+                                                                  const uint32_t *__restrict__ order = nullptr, int stream_hint = 0) {
     if (n_dev) n = min(n, *n_dev);
     __shared__ uint2 s_stack[SDEPTH * BLOCK];
     Stack<DEEP, BLOCK, SDEPTH> st;
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
                     ri = order ? __ldg(order + idx) : idx;
                     mi = 0;
                     in_mesh = false;
-                    best.t = __ldg(&rays[2ull * idx].w);
+                    best.t = __ldg(&rays[2ull * ri].w);
                     best.u = best.v = 0.0f;
                     best.prim = best.obj = -1;
                 }
@@ -142,7 +142,11 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
         if (ri == NO_RAY) continue;
         // ---- next instance whose box the ray enters, or the end of the ray
         if (!in_mesh) {
-            const float4 r0 = __ldg(rays + 2ull * ri), r1 = __ldg(rays + 2ull * ri + 1);
+            // streaming hint: the ray is read once per instance pass and the
+            // hit written once, so they may leave L1/L2 first (evict-first),
+            // which keeps more of the BVH resident
+            const float4 r0 = stream_hint ? __ldcs(rays + 2ull * ri) : __ldg(rays + 2ull * ri);
+            const float4 r1 = stream_hint ? __ldcs(rays + 2ull * ri + 1) : __ldg(rays + 2ull * ri + 1);
             const float sx = safe_inv(r1.x), sy = safe_inv(r1.y), sz = safe_inv(r1.z);
             SceneView job_sv;
             if (MULTI) job_sv = *reinterpret_cast<const SceneView *>(views + (size_t)__ldg(ray_job + ri) * view_stride);
@@ -169,7 +173,9 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
                 break;
             }
             if (!in_mesh) {
-                hits[ri] = make_float4(__int_as_float(best.prim), best.t, best.prim >= 0 ? best.u : 0.0f, best.prim >= 0 ? best.v : 0.0f);
+                const float4 h = make_float4(__int_as_float(best.prim), best.t, best.prim >= 0 ? best.u : 0.0f, best.prim >= 0 ? best.v : 0.0f);
+                if (stream_hint) __stcs(hits + ri, h);
+                else hits[ri] = h;
                 if (obj_out) obj_out[ri] = best.obj;
                 ri = NO_RAY;
                 continue;
@@ -247,7 +253,7 @@ cudaError_t launch_tuned(const SceneView &sv, const float4 *rays, uint32_t n, fl
     cudaError_t e = cudaMemsetAsync(tp.next_ray, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     k_trace_persistent<false, DEEP, false, false, BLOCK, SDEPTH><<<blocks, BLOCK, 0, st>>>(
-        sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min, tp.count, nullptr, 0, nullptr, tp.order);
+        sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min, tp.count, nullptr, 0, nullptr, tp.order, tp.stream_hint);
     return cudaGetLastError();
 }
 
@@ -307,7 +313,7 @@ cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, flo
                                                                         tp.count, nullptr, 0, nullptr, tp.order);
     else
         k_trace_persistent<false, DEEP><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min,
-                                                                         tp.count, nullptr, 0, nullptr, tp.order);
+                                                                         tp.count, nullptr, 0, nullptr, tp.order, tp.stream_hint);
     return cudaGetLastError();
 }
 

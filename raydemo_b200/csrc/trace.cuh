@@ -26,6 +26,9 @@ struct TraceParams {
     // shared-memory stack entries per thread (16, 24, 32; 256 x 32 exceeds the
     // block's static shared memory)
     int block = 128, smem_stack = 24;
+    // closest-hit persistent kernel: rays read and hits written with the
+    // streaming (evict-first) cache hint
+    int stream_hint = 0;
     uint32_t max_depth = 0; // deepest wide BVH among the traced meshes (sizes the stack)
     uint32_t *next_ray = nullptr; // device work counter for the persistent kernel
     const uint32_t *count = nullptr; // device ray count: when set, min(n, *count) rays are traced

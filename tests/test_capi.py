@@ -52,3 +52,15 @@ def test_no_device_fails_loudly():
     if os.path.exists(check):
         out = subprocess.run([check, "8", "8", "1", "0"], capture_output=True, text=True, timeout=300)
         assert out.returncode == 2 and '"error"' in out.stdout
+
+
+def test_unknown_handles_are_rejected():
+    """A pointer that ray_create_* did not return is refused before anything
+    dereferences it (no device needed)."""
+    L = capi.lib()
+    bogus = C.c_void_p(0x1234560)
+    assert L.ray_scene_commit(bogus) == capi.RAY_ERR_INVALID_ARG
+    assert b"handle" in L.ray_last_error()
+    assert L.ray_destroy_scene(bogus) == capi.RAY_ERR_INVALID_ARG
+    assert L.ray_resize(bogus, 8, 8) == capi.RAY_ERR_INVALID_ARG
+    assert L.ray_destroy_scene(None) == capi.RAY_OK

@@ -195,20 +195,29 @@ def test_empty_and_degenerate(renderer, oracle):
     assert len(sc.trace_closest(np.zeros((0, 8), np.float32))) == 0
 
 
+@pytest.fixture(scope="module")
+def variants_case(renderer, oracle):
+    tris = scenes.random_triangles(100000, seed=81)
+    rays = scenes.incoherent_rays(100000, seed=82)
+    rays[::3, 3] = np.float32(0.02)
+    return tris, rays, _scene(tris, renderer), _oracle_hits(oracle, tris, rays)
+
+
 @pytest.mark.parametrize("kernel,refill,deep,reorder,bits,block,sdepth", [
     (1, 8, 0, 0, 32, 128, 24), (1, 8, 1, 0, 32, 128, 24), (2, 1, 0, 0, 32, 128, 24), (2, 8, 0, 0, 32, 128, 24),
     (2, 32, 0, 0, 32, 128, 24), (2, 8, 1, 0, 32, 128, 24), (2, 8, 0, 1, 32, 128, 24), (2, 8, 0, 2, 24, 128, 24),
     (1, 8, 0, 1, 16, 128, 24), (2, 4, 1, 2, 32, 128, 24), (2, 8, 0, 0, 32, 64, 16), (2, 8, 0, 1, 32, 64, 32),
     (2, 8, 1, 0, 32, 256, 16), (2, 16, 0, 0, 32, 256, 24), (2, 8, 0, 0, 32, 128, 16), (2, 8, 1, 0, 32, 128, 32)])
-def test_kernel_variants_agree(renderer, oracle, kernel, refill, deep, reorder, bits, block, sdepth):
-    """Every traversal kernel, block size, stack placement and depth, and
-    trace order gives the same bytes, each hit at its ray's input position."""
-    tris = scenes.random_triangles(100000, seed=81)
-    rays = scenes.incoherent_rays(100000, seed=82)
-    sc = _scene(tris, renderer)
-    sc.set_trace_tuning(kernel, refill, deep, reorder, bits, block, sdepth)
-    assert sc.get_trace_tuning() == (kernel, refill, deep, reorder, bits, block, sdepth)
-    _assert_hits_equal(sc.trace_closest(rays), _oracle_hits(oracle, tris, rays))
+@pytest.mark.parametrize("hint,persist", [(0, 0), (1, 1), (1, 2)])
+def test_kernel_variants_agree(variants_case, kernel, refill, deep, reorder, bits, block, sdepth, hint, persist):
+    """Every traversal kernel, block size, stack placement and depth, trace
+    order, cache hint and L2 residency gives the same bytes, each hit at its
+    ray's input position (rays with different tmax, so that a ray's own
+    bound is the one its traversal starts from)."""
+    tris, rays, sc, exp = variants_case
+    sc.set_trace_tuning(kernel, refill, deep, reorder, bits, block, sdepth, hint, persist)
+    assert sc.get_trace_tuning() == (kernel, refill, deep, reorder, bits, block, sdepth, hint, persist)
+    _assert_hits_equal(sc.trace_closest(rays), exp)
 
 
 def test_device_path_matches_host_path(renderer):
