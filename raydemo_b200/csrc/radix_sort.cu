@@ -12,9 +12,11 @@
 //   2. thread d sums digit d over the warps and publishes the tile's count of
 //      d (flag AGG; tile 0 publishes it as INC, an inclusive prefix);
 //   3. thread d walks back over the preceding tiles' status words of digit d,
-//      adding AGG counts until it meets an INC prefix, then publishes its own
-//      inclusive prefix (decoupled look-back); the wait on an unpublished
-//      word is bounded and reports SORT_ERR_LOOKBACK when it runs out;
+//      LOOKBACK words per round, adding AGG counts until it meets an INC
+//      prefix, then publishes its own inclusive prefix (decoupled look-back;
+//      with every tile resident at once the walks are long, so a round has
+//      its loads in flight together); the wait on an unpublished word is
+//      bounded and reports SORT_ERR_LOOKBACK when it runs out;
 //   4. keys, then values, are placed in shared memory in digit order and
 //      written out by consecutive threads, so each digit's run of the tile is
 //      one contiguous stretch of the output.
@@ -28,6 +30,7 @@ namespace {
 constexpr uint32_t ST_AGG = 1u << 30, ST_INC = 2u << 30, ST_COUNT = (1u << 30) - 1u;
 constexpr uint32_t LOOKBACK_SPIN_LIMIT = 1u << 21; // polls of one word (with a short sleep) before giving up
 constexpr uint32_t HIST_MAX_BLOCKS = 148 * 8;
+constexpr int LOOKBACK = 16; // preceding tiles read per look-back round
 
 __device__ __forceinline__ uint32_t ld_relaxed(const uint32_t *p) {
     uint32_t v;
@@ -145,20 +148,36 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_onesweep(const K *__restrict_
     const uint32_t dstart = block_exclusive_scan(cnt, s_warp);
     uint32_t excl = 0;
     if (tile > 0) {
-        uint32_t pred = tile - 1, spins = 0;
-        while (true) {
-            const uint32_t s = ld_relaxed(status + (uint64_t)pred * 256u + (uint32_t)t);
-            if ((s & ~ST_COUNT) == 0u) {
+        // walk back over the preceding tiles' words of digit t, LOOKBACK
+        // tiles per round (independent loads in flight together), adding
+        // counts until an inclusive prefix; a word not yet published is
+        // polled again from there on the next round
+        int32_t pred = (int32_t)tile - 1;
+        uint32_t spins = 0;
+        bool done = false;
+        while (!done) {
+            uint32_t w[LOOKBACK];
+#pragma unroll
+            for (int q = 0; q < LOOKBACK; q++)
+                w[q] = pred - q >= 0 ? ld_relaxed(status + (uint64_t)(pred - q) * 256u + (uint32_t)t) : ST_INC;
+            int used = 0;
+#pragma unroll
+            for (int q = 0; q < LOOKBACK; q++) {
+                if (done || used < q) continue; // stopped earlier in this round
+                const uint32_t s = w[q];
+                if ((s & ~ST_COUNT) == 0u) continue; // unpublished: the next round starts here
+                excl += s & ST_COUNT;
+                used = q + 1;
+                if (s & ST_INC) done = true; // tile 0 (and past it, the sentinel) is inclusive
+            }
+            pred -= used;
+            if (!done && used == 0) {
                 if (++spins > LOOKBACK_SPIN_LIMIT) {
                     if (err) atomicOr(err, SORT_ERR_LOOKBACK);
                     break;
                 }
                 if (spins > 8u) __nanosleep(64);
-                continue;
             }
-            excl += s & ST_COUNT;
-            if ((s & ST_INC) || pred == 0u) break; // tile 0 always publishes INC
-            pred--;
         }
         st_relaxed(mine, ST_INC | ((excl + cnt) & ST_COUNT));
     }
