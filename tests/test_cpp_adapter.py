@@ -70,3 +70,23 @@ def test_demo_loader_runs_unchanged_on_the_adapter(cuda_device, tmp_path):
     assert d["mean"] > 0.005
     assert d["identical_px"] >= 0.9, d
     assert d["rmse"] <= 1e-3, d
+
+
+REF_TESTS = os.path.join(ROOT, "oracle", "_ref", "ref_tests_gpu")
+
+
+@pytest.mark.gpu
+def test_reference_image_tests_pass_unchanged_on_the_gpu(cuda_device, tmp_path):
+    """The reference's own test_mesh_lights (64x64, 2048 samples, mean 8-bit
+    error <= 1.0 against its golden image, with and without SH output) and
+    test_texture (256x256, 256 samples, mean |p - 0.5| <= 0.0015), compiled
+    unchanged from its tree and linked with the replacement factory
+    (include/raygpu_factory.cpp): every backend they loop over is the GPU
+    renderer. They exit non-zero on a failed check and print OK at the end."""
+    if not os.path.exists(REF_TESTS):
+        pytest.skip("oracle/_ref/ref_tests_gpu not built")
+    p = subprocess.run([REF_TESTS], capture_output=True, text=True, timeout=900, cwd=str(tmp_path))
+    print(p.stdout[-3000:])
+    assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
+    assert p.stdout.strip().endswith("OK")
+    assert "CUDA sm_100a renderer" in p.stdout
