@@ -252,7 +252,7 @@ int ray_sort_rays(ray_renderer *r, const float *rays, uint64_t n, const float ro
  * belongs to their own allocator and budget, and frame loops that must not
  * stall on cudaMalloc's implicit device-wide synchronisation. Same inputs,
  * outputs and results as ray_sort_rays, without a renderer: the scratch
- * memory is a fixed array of 13,640,192 bytes (13.01 MiB) that every GPU
+ * memory is a fixed array of 14,688,768 bytes (14.01 MiB) that every GPU
  * loading this library holds until the process exits, so n is limited to
  * RAY_SORT_NOALLOC_MAX_RAYS (larger n: RAY_ERR_INVALID_ARG). The first call on
  * a device looks the array up on the current device and keeps its address for
@@ -298,9 +298,14 @@ int ray_scene_last_trace_info(ray_scene *s, ray_trace_info *out);
  * hint. l2_persist: 1 = the scene's wide nodes, 2 = its leaf triangles, are
  * marked persisting in L2 for the trace (an access-policy window on the
  * trace's streams, removed after it; the first such call sets this CUDA
- * context's persisting-L2 limit, which lasts as long as the context). */
+ * context's persisting-L2 limit, which lasts as long as the context).
+ * instance_tree: 0 = traces walk an instance tree (a BVH over the instances'
+ * world boxes, built on the GPU at commit, refitted when only transforms
+ * changed; the reference's macro tree, SceneRef.cpp:492-516) from 32
+ * instances on and test the instance boxes in turn below that; 1 = the tree
+ * from 2 instances on; -1 = never. */
 typedef struct ray_trace_tuning {
-    int kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack, stream_hint, l2_persist;
+    int kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack, stream_hint, l2_persist, instance_tree;
 } ray_trace_tuning;
 int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t);
 int ray_scene_get_trace_tuning(ray_scene *s, ray_trace_tuning *out);
@@ -312,6 +317,17 @@ typedef struct ray_bvh_info {
     float bbox_min[3], bbox_max[3];
 } ray_bvh_info;
 int ray_scene_mesh_bvh_info(ray_scene *s, uint32_t mesh, ray_bvh_info *out);
+
+/* The instance tree after the last commit: instances it covers (0: none,
+ * the traversal tests the instance boxes in turn), host milliseconds the
+ * last commit spent building or refitting it (device work included), and
+ * whether that was a refit (1) or a build (0). */
+typedef struct ray_instance_tree_info {
+    uint32_t instances;
+    int refit;
+    double ms;
+} ray_instance_tree_info;
+int ray_scene_instance_tree_info(ray_scene *s, ray_instance_tree_info *out);
 
 /* Diagnostics: copies one of the scene's device arrays to host memory (after
  * committing). what: 0 wide nodes (80 bytes each), 1 leaf-ordered triangles

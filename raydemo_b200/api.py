@@ -255,13 +255,16 @@ class Scene:
         check(lib().ray_scene_trace_closest(self._h, rays_ptr, n, hits_ptr, obj_ptr or None, capi.RAY_MEM_DEVICE, stream or None))
 
     def set_trace_tuning(self, kernel: int = 0, refill_min: int = 0, deep_stack: int = 0, reorder: int = 0, reorder_bits: int = 0,
-                         block: int = 0, smem_stack: int = 0, stream_hint: int = 0, l2_persist: int = 0) -> None:
+                         block: int = 0, smem_stack: int = 0, stream_hint: int = 0, l2_persist: int = 0,
+                         instance_tree: int = 0) -> None:
         """ray_scene_set_trace_tuning: kernel (1 per ray, 2 persistent; 0
         keeps), refill threshold (0 keeps), deep stack, trace order (0 input,
         1 ray hash, 2 origin cell first), the key bits it sorts on, threads
         per block and shared stack entries (0: 128 and 24), streaming cache
-        hint on rays and hits, L2 residency (1 nodes, 2 leaf triangles)."""
-        t = capi.TraceTuning(kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack, stream_hint, l2_persist)
+        hint on rays and hits, L2 residency (1 nodes, 2 leaf triangles),
+        instance tree (0 from 32 instances, 1 always, -1 never)."""
+        t = capi.TraceTuning(kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack, stream_hint, l2_persist,
+                             instance_tree)
         check(lib().ray_scene_set_trace_tuning(self._h, C.byref(t)))
 
     def tune_trace_device(self, rays_ptr: int, n: int, hits_ptr: int, stream: int = 0, force: bool = False) -> tuple:
@@ -280,11 +283,18 @@ class Scene:
         check(lib().ray_scene_debug_write(self._h, what, offset, b, len(data)))
 
     def get_trace_tuning(self) -> tuple:
-        """(kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack, stream_hint, l2_persist)"""
+        """(kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack, stream_hint, l2_persist, instance_tree)"""
         t = capi.TraceTuning()
         check(lib().ray_scene_get_trace_tuning(self._h, C.byref(t)))
         return (t.kernel, t.refill_min, t.deep_stack, t.reorder, t.reorder_bits, t.block, t.smem_stack, t.stream_hint,
-                t.l2_persist)
+                t.l2_persist, t.instance_tree)
+
+    def instance_tree_info(self) -> capi.InstanceTreeInfo:
+        """ray_scene_instance_tree_info: instances the tree covers (0: none),
+        whether the last commit refitted it, and its host time in ms."""
+        i = capi.InstanceTreeInfo()
+        check(lib().ray_scene_instance_tree_info(self._h, C.byref(i)))
+        return i
 
     def set_counting(self, enable: bool) -> None:
         check(lib().ray_scene_set_counting(self._h, int(enable)))

@@ -107,7 +107,12 @@ class DiffParams(C.Structure):
 
 class TraceTuning(C.Structure):
     _fields_ = [("kernel", C.c_int), ("refill_min", C.c_int), ("deep_stack", C.c_int), ("reorder", C.c_int), ("reorder_bits", C.c_int),
-                ("block", C.c_int), ("smem_stack", C.c_int), ("stream_hint", C.c_int), ("l2_persist", C.c_int)]
+                ("block", C.c_int), ("smem_stack", C.c_int), ("stream_hint", C.c_int), ("l2_persist", C.c_int),
+                ("instance_tree", C.c_int)]
+
+
+class InstanceTreeInfo(C.Structure):
+    _fields_ = [("instances", C.c_uint32), ("refit", C.c_int), ("ms", C.c_double)]
 
 
 class BvhInfo(C.Structure):
@@ -184,6 +189,7 @@ _SIGS = {
     "ray_scene_set_trace_tuning": ([_P, C.POINTER(TraceTuning)], C.c_int),
     "ray_scene_get_trace_tuning": ([_P, C.POINTER(TraceTuning)], C.c_int),
     "ray_scene_debug_write": ([_P, C.c_int, C.c_uint64, _P, C.c_uint64], C.c_int),
+    "ray_scene_instance_tree_info": ([_P, C.POINTER(InstanceTreeInfo)], C.c_int),
     "ray_debug_fail_device_alloc": ([C.c_int64], C.c_int),
     "ray_set_wait_timeout_ms": ([C.c_int64], C.c_int),
     "ray_scene_tune_trace": ([_P, _P, C.c_uint64, _P, C.c_int, _P, C.POINTER(TraceTuning), C.c_char_p, C.c_uint64], C.c_int),

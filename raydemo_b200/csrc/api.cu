@@ -259,6 +259,7 @@ cudaError_t note_use(ray_scene *s, cudaStream_t st) {
 
 int commit(ray_scene *s) {
     if (!s->geom_dirty && !s->inst_dirty && !s->shade_dirty) return RAY_OK;
+    const bool geom_changed = s->geom_dirty;
     RG_CUDA_TRY(cudaSetDevice(s->device));
     cudaStream_t st = s->stream;
     // the frames and traces in flight read the arrays about to be rewritten
@@ -357,6 +358,30 @@ int commit(ray_scene *s) {
     if (!inst.empty())
         RG_CUDA_TRY(cudaMemcpyAsync(s->d_inst.p, inst.data(), inst.size() * sizeof(InstanceRec), cudaMemcpyHostToDevice, st));
     s->n_inst_dev = (uint32_t)inst.size();
+    // the instance tree: a refit when only instances moved (same count, no
+    // mesh rebuilt), else a build; none below the tuning's instance count
+    {
+        const uint32_t ni = (uint32_t)inst.size();
+        const int mode = s->tuning.instance_tree;
+        const bool want = mode >= 0 && ni >= 2 && (mode == 1 || ni >= TLAS_MIN_INSTANCES);
+        if (!want) {
+            free_inst_tree(s->tlas);
+        } else {
+            std::vector<float> boxes(6 * (size_t)ni);
+            for (size_t i = 0; i < inst.size(); i++)
+                for (int k = 0; k < 3; k++) {
+                    boxes[6 * i + k] = inst[i].bbox_min[k];
+                    boxes[6 * i + 3 + k] = inst[i].bbox_max[k];
+                }
+            const bool refit = !geom_changed && s->tlas.n == ni;
+            const auto t0 = std::chrono::steady_clock::now();
+            const int rc = build_inst_tree(boxes.data(), ni, refit, s->tlas, st);
+            if (rc != RAY_OK) return rc;
+            RG_CUDA_TRY(wait_stream(st));
+            s->last_tlas_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            s->last_tlas_refit = refit ? 1 : 0;
+        }
+    }
     // the scene's box: the union of the instance boxes (the ray hash grid of the render loop's sort)
     for (int k = 0; k < 3; k++) {
         s->world_min[k] = inst.empty() ? 0.0f : inst[0].bbox_min[k];
@@ -398,6 +423,7 @@ using namespace rg;
 
 ray_scene::~ray_scene() {
     cudaSetDevice(device);
+    free_inst_tree(tlas);
     for (MeshRec &m : meshes) {
         free_mesh_bvh(m.bvh);
         if (m.tris_ref) cudaFree(m.tris_ref);
@@ -1018,6 +1044,20 @@ int ray_scene_mesh_bvh_info(ray_scene *s, uint32_t mesh, ray_bvh_info *out) {
     RG_GUARD_END
 }
 
+int ray_scene_instance_tree_info(ray_scene *s, ray_instance_tree_info *out) {
+    RG_API_LOCK;
+    RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
+    RG_CHECK(s && out, "null argument");
+    RG_GUARD_BEGIN
+    const int rc = commit(s);
+    if (rc != RAY_OK) return rc;
+    out->instances = s->tlas.nodes ? s->tlas.n : 0;
+    out->refit = s->last_tlas_refit;
+    out->ms = s->last_tlas_ms;
+    return RAY_OK;
+    RG_GUARD_END
+}
+
 int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t) {
     RG_API_LOCK;
     RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
@@ -1032,6 +1072,7 @@ int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t) {
     RG_CHECK(!((t->block == 256) && t->smem_stack == 32), "256 threads with 32 stack entries exceed the block's shared memory");
     RG_CHECK(t->stream_hint == 0 || t->stream_hint == 1, "stream_hint is 0 or 1");
     RG_CHECK(t->l2_persist >= 0 && t->l2_persist <= 2, "l2_persist is 0, 1 (nodes) or 2 (leaf triangles)");
+    RG_CHECK(t->instance_tree >= -1 && t->instance_tree <= 1, "instance_tree is -1, 0 or 1");
     if (t->kernel > 0) s->tuning.kernel = t->kernel;
     if (t->refill_min > 0) s->tuning.refill_min = t->refill_min;
     s->tuning.deep_stack = t->deep_stack;
@@ -1041,6 +1082,8 @@ int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t) {
     s->tuning.smem_stack = t->smem_stack ? t->smem_stack : 24;
     s->tuning.stream_hint = t->stream_hint;
     s->tuning.l2_persist = t->l2_persist;
+    if (t->instance_tree != s->tuning.instance_tree) s->inst_dirty = true; // built or dropped at the next commit
+    s->tuning.instance_tree = t->instance_tree;
     return RAY_OK;
 }
 
@@ -1177,7 +1220,7 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
         RG_CUDA_TRY(cudaStreamWaitEvent(other, s->pipe_ev[0], 0));
     }
     SceneView sv{static_cast<const WideNode *>(s->d_nodes.p), static_cast<const TriRec *>(s->d_leaf.p),
-                 static_cast<const InstanceRec *>(s->d_inst.p), s->n_inst_dev};
+                 static_cast<const InstanceRec *>(s->d_inst.p), s->n_inst_dev, s->tlas.nodes};
     RG_CUDA_TRY(s->d_next_ray.ensure(8)); // a work counter for each of two concurrent traces
     TraceParams tp;
     tp.persistent = s->tuning.kernel == 2;

@@ -28,4 +28,23 @@ cudaError_t launch_preprocess_tris(const float *verts, const uint32_t *mat, uint
 // Returns RAY_OK or a RAY_ERR_* code (message through set_error).
 int build_mesh_bvh(const TriRec *tris_ref, const float *aabb, uint32_t n, MeshBvh &out, cudaStream_t st);
 
+// The instance tree: an LBVH over the instances' world boxes (Morton codes
+// of the box centres, the same radix sort and binary radix tree as a mesh's
+// build), its node boxes computed bottom-up and packed into TlasNode
+// records. A refit keeps the topology and recomputes only the boxes (after
+// instances moved); a build is needed when the instance count changed.
+struct InstTree {
+    uint32_t n = 0;              // instances of the current topology (0: none built)
+    float *aabb = nullptr;       // 6 floats per instance: world box
+    uint32_t *sorted = nullptr;  // sorted position -> instance index
+    uint32_t *left = nullptr, *right = nullptr, *parent = nullptr, *first = nullptr, *last = nullptr;
+    float *nb = nullptr;         // node boxes (6 floats per internal node)
+    uint32_t *flags = nullptr;   // arrival counters of the bottom-up passes
+    TlasNode *nodes = nullptr;   // n - 1 packed nodes
+};
+void free_inst_tree(InstTree &t);
+// boxes: n world boxes (6 floats each) in host memory. refit: keep the
+// topology (requires t.n == n). Returns RAY_OK or a RAY_ERR_* code.
+int build_inst_tree(const float *boxes, uint32_t n, bool refit, InstTree &t, cudaStream_t st);
+
 } // namespace rg

@@ -227,6 +227,28 @@ __global__ void k_bottom_up(const float *__restrict__ aabb, const uint32_t *__re
     }
 }
 
+// Instance tree nodes from the binary radix tree and its node boxes: both
+// children's boxes (an instance's world box, or the child node's box) and
+// ids (TLAS_LEAF | instance index, or the node index).
+__global__ void k_tlas_pack(const float *__restrict__ aabb, const uint32_t *__restrict__ sorted, int n, const uint32_t *__restrict__ left,
+                            const uint32_t *__restrict__ right, const float *__restrict__ nb, TlasNode *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    TlasNode t;
+    for (int c = 0; c < 2; c++) {
+        const uint32_t id = c == 0 ? left[i] : right[i];
+        float lo[3], hi[3];
+        child_box(id, aabb, sorted, nb, lo, hi);
+        for (int k = 0; k < 3; k++) {
+            t.lo[c][k] = lo[k];
+            t.hi[c][k] = hi[k];
+        }
+        t.child[c] = (id & LEAF) ? (TLAS_LEAF | sorted[id & ~LEAF]) : id;
+    }
+    t.pad[0] = t.pad[1] = 0;
+    out[i] = t;
+}
+
 // SAH weights of the cost programme: a wide node's box test and fetch, and one triangle test.
 constexpr float SAH_NODE = 1.0f, SAH_TRI = 1.2f;
 
@@ -587,6 +609,60 @@ int build_mesh_bvh(const TriRec *tris_ref, const float *aabb, uint32_t n, MeshBv
         set_error("BVH build lost triangles");
         return RAY_ERR_CUDA;
     }
+    return RAY_OK;
+}
+
+void free_inst_tree(InstTree &t) {
+    void *ps[] = {t.aabb, t.sorted, t.left, t.right, t.parent, t.first, t.last, t.nb, t.flags, t.nodes};
+    for (void *p : ps)
+        if (p) cudaFree(p);
+    t = InstTree{};
+}
+
+int build_inst_tree(const float *boxes, uint32_t n, bool refit, InstTree &t, cudaStream_t st) {
+    if (n < 2) { // one instance or none: the traversal tests it directly
+        free_inst_tree(t);
+        return RAY_OK;
+    }
+    const uint32_t ni = n - 1;
+    if (!refit || t.n != n) {
+        free_inst_tree(t);
+        RG_CUDA_TRY(dalloc(&t.aabb, 6 * (size_t)n));
+        RG_CUDA_TRY(dalloc(&t.sorted, n));
+        RG_CUDA_TRY(dalloc(&t.left, ni));
+        RG_CUDA_TRY(dalloc(&t.right, ni));
+        RG_CUDA_TRY(dalloc(&t.parent, 2 * (size_t)n));
+        RG_CUDA_TRY(dalloc(&t.first, ni));
+        RG_CUDA_TRY(dalloc(&t.last, ni));
+        RG_CUDA_TRY(dalloc(&t.nb, 6 * (size_t)ni));
+        RG_CUDA_TRY(dalloc(&t.flags, ni));
+        RG_CUDA_TRY(dalloc(&t.nodes, ni));
+        TmpAllocs tmp;
+        uint64_t *keys = nullptr;
+        uint32_t *bounds = nullptr;
+        char *scratch = nullptr;
+        RG_CUDA_TRY(tmp.get(&keys, n));
+        RG_CUDA_TRY(tmp.get(&bounds, 6));
+        RG_CUDA_TRY(tmp.get(&scratch, radix_sort_scratch_bytes(n, 8)));
+        RG_CUDA_TRY(cudaMemcpyAsync(t.aabb, boxes, 6 * sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, st));
+        const uint32_t init_bounds[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+        RG_CUDA_TRY(cudaMemcpyAsync(bounds, init_bounds, sizeof(init_bounds), cudaMemcpyHostToDevice, st));
+        k_bounds<<<std::min<uint32_t>((n + 255) / 256, 1184), 256, 0, st>>>(t.aabb, n, bounds);
+        k_morton<<<(n + 255) / 256, 256, 0, st>>>(t.aabb, n, bounds, keys, t.sorted);
+        RG_CUDA_TRY(cudaGetLastError());
+        RG_CUDA_TRY(radix_sort_pairs(keys, t.sorted, n, 8, 0, 64, scratch, st));
+        k_karras<<<(ni + 255) / 256, 256, 0, st>>>(keys, (int)n, t.left, t.right, t.parent, t.first, t.last);
+        RG_CUDA_TRY(cudaGetLastError());
+        RG_CUDA_TRY(wait_stream(st)); // before the temporaries are freed
+        t.n = n;
+    } else {
+        RG_CUDA_TRY(cudaMemcpyAsync(t.aabb, boxes, 6 * sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, st));
+    }
+    // node boxes bottom-up (a refit: the same topology, the instances' new boxes), then the packed nodes
+    RG_CUDA_TRY(cudaMemsetAsync(t.flags, 0, ni * sizeof(uint32_t), st));
+    k_bottom_up<<<(n + 255) / 256, 256, 0, st>>>(t.aabb, t.sorted, (int)n, t.left, t.right, t.parent, t.nb, t.flags);
+    k_tlas_pack<<<(ni + 255) / 256, 256, 0, st>>>(t.aabb, t.sorted, (int)n, t.left, t.right, t.nb, t.nodes);
+    RG_CUDA_TRY(cudaGetLastError());
     return RAY_OK;
 }
 

@@ -70,6 +70,18 @@ static_assert(sizeof(InstanceRec) == 96, "InstanceRec must stay 96 bytes");
 
 constexpr int LEAF_MAX_TRIS = 3;
 
+// Instance tree node (binary, over the instances' world boxes): the boxes
+// of both children and their ids; an id with TLAS_LEAF set is an instance
+// index, else a node index (node 0 is the root).
+constexpr uint32_t TLAS_LEAF = 0x80000000u;
+struct TlasNode {
+    float lo[2][3];
+    float hi[2][3];
+    uint32_t child[2];
+    uint32_t pad[2];
+};
+static_assert(sizeof(TlasNode) == 64, "TlasNode must stay 64 bytes");
+
 } // namespace rg
 
 // Error helpers for host code.

@@ -4,10 +4,11 @@
 // all digit passes, then one launch per pass (plus a copy when the number of
 // passes is odd, so that the result ends in the caller's arrays).
 //
-// A pass, per tile of RS_TILE keys (tiles are numbered in the order their
+// A pass, per tile of 256 x ITEMS keys (ITEMS 8 up to 16M items, else 16;
+// tiles are numbered in the order their
 // blocks start, through an atomic counter, so every tile's predecessors are
 // running or done):
-//   1. each warp ranks its 32 x RS_ITEMS keys stably (index order) with match
+//   1. each warp ranks its 32 x ITEMS keys stably (index order) with match
 //      masks and per-warp digit counters in shared memory;
 //   2. thread d sums digit d over the warps and publishes the tile's count of
 //      d (flag AGG; tile 0 publishes it as INC, an inclusive prefix);
@@ -87,8 +88,8 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const K *__restrict__ ke
 }
 
 // One digit pass. vals_in null: the values are the items' input indices.
-template <typename K>
-__global__ void __launch_bounds__(RS_THREADS) k_rs_onesweep(const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+template <typename K, int ITEMS>
+__global__ void __launch_bounds__(RS_THREADS, ITEMS <= 8 ? 3 : 2) k_rs_onesweep(const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                                                             K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, uint64_t cap,
                                                             const uint32_t *__restrict__ n_dev, int shift, const uint32_t *__restrict__ ghist,
                                                             uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status,
@@ -98,7 +99,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_onesweep(const K *__restrict_
     __shared__ uint32_t s_gofs[256];            // output index of tile position 0 of each digit
     __shared__ uint32_t s_warp[RS_WARPS];
     __shared__ uint32_t s_tile;
-    __shared__ __align__(16) K s_x[RS_TILE]; // the tile in digit order: keys, then values
+    __shared__ __align__(16) K s_x[(RS_THREADS * ITEMS)]; // the tile in digit order: keys, then values
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     if (t == 0) s_tile = atomicAdd(tile_counter, 1u);
 #pragma unroll
@@ -106,33 +107,38 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_onesweep(const K *__restrict_
     __syncthreads();
     const uint32_t n = item_count(cap, n_dev);
     const uint32_t tile = s_tile;
-    const uint64_t tile_base = (uint64_t)tile * RS_TILE;
+    const uint64_t tile_base = (uint64_t)tile * (RS_THREADS * ITEMS);
     if (tile_base >= n) return; // past the items (block-uniform)
-    const uint32_t tile_n = (uint32_t)min((uint64_t)RS_TILE, (uint64_t)n - tile_base);
+    const uint32_t tile_n = (uint32_t)min((uint64_t)(RS_THREADS * ITEMS), (uint64_t)n - tile_base);
 
-    // warp w holds tile positions [w * 32 * RS_ITEMS, (w + 1) * 32 * RS_ITEMS), lane-striped
-    const uint32_t wbase = (uint32_t)warp * 32u * RS_ITEMS;
-    K k[RS_ITEMS];
-    uint32_t v[RS_ITEMS], pos[RS_ITEMS];
+    // warp w holds tile positions [w * 32 * ITEMS, (w + 1) * 32 * ITEMS), lane-striped
+    const uint32_t wbase = (uint32_t)warp * 32u * ITEMS;
+    K k[ITEMS];
+    uint32_t v[ITEMS], pos[ITEMS];
 #pragma unroll
-    for (int j = 0; j < RS_ITEMS; j++) {
+    for (int j = 0; j < ITEMS; j++) {
         const uint32_t li = wbase + (uint32_t)j * 32u + lane;
         const bool ok = li < tile_n;
         k[j] = ok ? keys_in[tile_base + li] : (K)0;
         v[j] = ok ? (vals_in ? vals_in[tile_base + li] : (uint32_t)(tile_base + li)) : 0u;
     }
-    // stable rank among the warp's keys of the same digit
+    // stable rank among the warp's keys of the same digit: the lanes of one
+    // digit (a match group) take their places in lane order after the
+    // group's earlier keys, whose count the group's lowest lane reads and
+    // advances with one shared atomic; the warp is synchronised after each
+    // key, so the counts advance in key order
     const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
-    for (int j = 0; j < RS_ITEMS; j++) {
+    for (int j = 0; j < ITEMS; j++) {
         const uint32_t li = wbase + (uint32_t)j * 32u + lane;
         const uint32_t d = li < tile_n ? digit(k[j], shift) : 256u;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        const uint32_t before = d < 256u ? s_whist[warp][d] : 0u;
+        const uint32_t leader = __ffs(peers) - 1u;
+        uint32_t before = 0;
+        if (d < 256u && lane == leader) before = atomicAdd(&s_whist[warp][d], (uint32_t)__popc(peers));
+        before = __shfl_sync(0xffffffffu, before, leader);
         pos[j] = before + __popc(peers & lt);
-        __syncwarp();
-        if (d < 256u && (peers >> lane) == 1u) s_whist[warp][d] = before + __popc(peers); // the group's last lane
-        __syncwarp();
+        __syncwarp(); // this key's atomic is done before the next key's
     }
     __syncthreads();
     uint32_t cnt = 0;
@@ -185,7 +191,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_onesweep(const K *__restrict_
     s_gofs[t] = gstart + excl - dstart;
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < RS_ITEMS; j++) {
+    for (int j = 0; j < ITEMS; j++) {
         const uint32_t li = wbase + (uint32_t)j * 32u + lane;
         if (li < tile_n) {
             const uint32_t d = digit(k[j], shift);
@@ -194,9 +200,9 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_onesweep(const K *__restrict_
         }
     }
     __syncthreads();
-    uint32_t dst[RS_ITEMS];
+    uint32_t dst[ITEMS];
 #pragma unroll
-    for (int j = 0; j < RS_ITEMS; j++) {
+    for (int j = 0; j < ITEMS; j++) {
         const uint32_t i = (uint32_t)j * RS_THREADS + (uint32_t)t;
         if (i < tile_n) {
             const K key = s_x[i];
@@ -207,13 +213,13 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_onesweep(const K *__restrict_
     __syncthreads();
     uint32_t *s_v = reinterpret_cast<uint32_t *>(s_x);
 #pragma unroll
-    for (int j = 0; j < RS_ITEMS; j++) {
+    for (int j = 0; j < ITEMS; j++) {
         const uint32_t li = wbase + (uint32_t)j * 32u + lane;
         if (li < tile_n) s_v[pos[j]] = v[j];
     }
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < RS_ITEMS; j++) {
+    for (int j = 0; j < ITEMS; j++) {
         const uint32_t i = (uint32_t)j * RS_THREADS + (uint32_t)t;
         if (i < tile_n) vals_out[dst[j]] = s_v[i];
     }
@@ -238,7 +244,12 @@ cudaError_t sort_impl(K *keys, uint32_t *vals, uint64_t n, int begin_bit, int en
     if (passes < 1 || passes > (int)sizeof(K) || begin_bit < 0 || end_bit > (int)(8 * sizeof(K)) || n > RS_MAX_ITEMS)
         return cudaErrorInvalidValue;
     if (n == 0) return cudaSuccess;
-    const uint32_t num_tiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
+    // smaller tiles below 16M items: more blocks and shorter ranking chains
+    // per block where one tile per block would leave most of the SMs' warp
+    // slots empty
+    const bool small = n <= (1ull << 24);
+    const uint32_t tile = small ? RS_THREADS * 8 : RS_TILE;
+    const uint32_t num_tiles = (uint32_t)((n + tile - 1) / tile);
     char *p = static_cast<char *>(scratch);
     K *keys_alt = reinterpret_cast<K *>(p);
     p += rs_align256(n * sizeof(K));
@@ -250,12 +261,18 @@ cudaError_t sort_impl(K *keys, uint32_t *vals, uint64_t n, int begin_bit, int en
     cudaError_t e = cudaMemsetAsync(ghist, 0, (kCounterWords + (uint64_t)passes * num_tiles * 256) * 4, st);
     if (e != cudaSuccess) return e;
     k_rs_hist<K><<<num_tiles < HIST_MAX_BLOCKS ? num_tiles : HIST_MAX_BLOCKS, RS_THREADS, 0, st>>>(keys, n, n_dev, begin_bit, passes, ghist);
+    // (the histogram grid: one block per tile up to HIST_MAX_BLOCKS, each striding over the keys)
     K *src_k = keys, *dst_k = keys_alt;
     const uint32_t *src_v = ident ? nullptr : vals;
     uint32_t *dst_v = vals_alt;
     for (int q = 0; q < passes; q++) {
-        k_rs_onesweep<K><<<num_tiles, RS_THREADS, 0, st>>>(src_k, src_v, dst_k, dst_v, n, n_dev, begin_bit + 8 * q, ghist + 256 * q,
-                                                           counters + q, status + (uint64_t)q * num_tiles * 256, err);
+        if (small)
+            k_rs_onesweep<K, 8><<<num_tiles, RS_THREADS, 0, st>>>(src_k, src_v, dst_k, dst_v, n, n_dev, begin_bit + 8 * q, ghist + 256 * q,
+                                                                 counters + q, status + (uint64_t)q * num_tiles * 256, err);
+        else
+            k_rs_onesweep<K, RS_ITEMS><<<num_tiles, RS_THREADS, 0, st>>>(src_k, src_v, dst_k, dst_v, n, n_dev, begin_bit + 8 * q,
+                                                                        ghist + 256 * q, counters + q,
+                                                                        status + (uint64_t)q * num_tiles * 256, err);
         K *tk = src_k;
         src_k = dst_k;
         dst_k = tk;

@@ -136,12 +136,15 @@ struct ray_scene {
     // device arrays assembled at commit
     rg::DeviceBuf d_nodes, d_leaf, d_inst, d_tris_ref;
     uint32_t n_inst_dev = 0;
+    rg::InstTree tlas;               // the instance tree (built at commit from TLAS_MIN_INSTANCES instances)
+    double last_tlas_ms = 0.0;       // host time of the last commit's instance-tree build or refit
+    int last_tlas_refit = 0;         // 1: it was a refit
     rg::DeviceBuf d_vertices, d_vtx_indices, d_materials, d_textures, d_texels, d_lights, d_area_lights;
 
     // batch-trace staging and diagnostics
     rg::DeviceBuf d_rays, d_hits, d_obj, d_err, d_counters, d_next_ray;
     rg::DeviceBuf d_order[2]; // reordered traces: keys, order and sort scratch of each of two concurrent chunks
-    ray_trace_tuning tuning{2, 8, 0, 0, 32, 128, 24, 0, 0};
+    ray_trace_tuning tuning{2, 8, 0, 0, 32, 128, 24, 0, 0, 0};
     bool counting = false;
     ray_trace_info last_info{};
     bool info_pending = false;

@@ -343,7 +343,7 @@ int upload_shading(ray_scene *s) {
 RenderScene render_scene_view(const ray_scene *s) {
     RenderScene r{};
     r.sv = SceneView{static_cast<const WideNode *>(s->d_nodes.p), static_cast<const TriRec *>(s->d_leaf.p),
-                     static_cast<const InstanceRec *>(s->d_inst.p), s->n_inst_dev};
+                     static_cast<const InstanceRec *>(s->d_inst.p), s->n_inst_dev, s->tlas.nodes};
     r.tris = static_cast<const TriRec *>(s->d_tris_ref.p);
     r.vtx_indices = static_cast<const uint32_t *>(s->d_vtx_indices.p);
     r.vertices = static_cast<const VertexRec *>(s->d_vertices.p);

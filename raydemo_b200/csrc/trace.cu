@@ -66,16 +66,26 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
         best.prim = -1;
         best.obj = -1;
         const float sx = safe_inv(r1.x), sy = safe_inv(r1.y), sz = safe_inv(r1.z);
-        for (uint32_t m = 0; m < sv.n_inst; m++) {
-            const InstanceRec *ir = sv.inst + m;
-            float bmin[3], bmax[3];
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                bmin[k] = __ldg(&ir->bbox_min[k]);
-                bmax[k] = __ldg(&ir->bbox_max[k]);
+        if (sv.tlas) { // the instance tree
+            uint32_t tstk[TLAS_STACK];
+            int tsp = 1;
+            tstk[0] = 0;
+            for (int m; (m = tlas_next(sv, r0, sx, sy, sz, best.t, tstk, tsp, err)) >= 0;) {
+                const InstanceRec *ir = sv.inst + m;
+                trace_mesh<COUNT>(mesh_of(sv, ir, m), transform_ray(ir, r0, r1), best, st, err, nvis, ntri);
             }
-            if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
-            trace_mesh<COUNT>(mesh_of(sv, ir, (int)m), transform_ray(ir, r0, r1), best, st, err, nvis, ntri);
+        } else {
+            for (uint32_t m = 0; m < sv.n_inst; m++) {
+                const InstanceRec *ir = sv.inst + m;
+                float bmin[3], bmax[3];
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    bmin[k] = __ldg(&ir->bbox_min[k]);
+                    bmax[k] = __ldg(&ir->bbox_max[k]);
+                }
+                if (!ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best.t, bmin, bmax)) continue;
+                trace_mesh<COUNT>(mesh_of(sv, ir, (int)m), transform_ray(ir, r0, r1), best, st, err, nvis, ntri);
+            }
         }
         hits[i] = make_float4(__int_as_float(best.prim), best.t, best.prim >= 0 ? best.u : 0.0f, best.prim >= 0 ? best.v : 0.0f);
         if (obj_out) obj_out[i] = best.obj;
@@ -109,6 +119,8 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
     const uint32_t lanemask_lt = (1u << lane) - 1u;
     uint32_t err = 0, nvis = 0, ntri = 0;
     uint32_t ri = NO_RAY, mi = 0, visits = 0, steps = 0;
+    uint32_t tstk[TLAS_STACK]; // the ray's instance-tree stack (scenes with an instance tree)
+    int tsp = 0;
     bool in_mesh = false, pool_empty = false;
     Best best;
     best.t = 0.0f;
@@ -131,6 +143,8 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
                 if (idx < n) {
                     ri = order ? __ldg(order + idx) : idx;
                     mi = 0;
+                    tstk[0] = 0; // the tree's root, for a scene that has one
+                    tsp = 1;
                     in_mesh = false;
                     best.t = __ldg(&rays[2ull * ri].w);
                     best.u = best.v = 0.0f;
@@ -151,7 +165,22 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
             SceneView job_sv;
             if (MULTI) job_sv = *reinterpret_cast<const SceneView *>(views + (size_t)__ldg(ray_job + ri) * view_stride);
             const SceneView &lsv = MULTI ? job_sv : sv;
-            while (mi < lsv.n_inst) {
+            if (lsv.tlas) {
+                const int m = tlas_next(lsv, r0, sx, sy, sz, best.t, tstk, tsp, err);
+                if (m >= 0) {
+                    const InstanceRec *ir = lsv.inst + m;
+                    mr = mesh_of(lsv, ir, m);
+                    r = transform_ray(ir, r0, r1);
+                    ng_base = 0;
+                    ng_bits = (1u << (24 + r.oct)) | 1u;
+                    tg_bits = 0;
+                    st.sp = 0;
+                    visits = 0;
+                    steps = 0;
+                    in_mesh = true;
+                }
+            }
+            while (!lsv.tlas && mi < lsv.n_inst) {
                 const InstanceRec *ir = lsv.inst + mi;
                 float bmin[3], bmax[3];
 #pragma unroll
@@ -199,6 +228,7 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
         if (!ok) {
             in_mesh = false;
             mi = 0xffffffffu; // abandon the ray; the error flag reports it
+            tsp = 0;
             continue;
         }
         bool stop = false;
@@ -217,6 +247,7 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
         if (ANY && stop) { // a solid triangle blocks the ray: no further instance
             in_mesh = false;
             mi = 0xffffffffu;
+            tsp = 0;
             continue;
         }
         if (ng_bits <= 0x00FFFFFFu) {

@@ -11,12 +11,21 @@ struct SceneView {
     const TriRec *leaf_tris;
     const InstanceRec *inst;
     uint32_t n_inst;
+    // the instance tree (n_inst - 1 nodes), or null: the traversal then tests
+    // the instances' boxes one after another
+    const TlasNode *tlas = nullptr;
 };
+
+// Instance counts from which traces walk the instance tree instead of
+// testing every instance box in turn.
+constexpr uint32_t TLAS_MIN_INSTANCES = 32;
 
 // Error bits written (OR-ed) to *err by the traversal.
 constexpr uint32_t TRACE_ERR_STACK = 1u;
 constexpr uint32_t TRACE_ERR_BOUNDS = 2u; // a node or triangle index outside the mesh's arrays
 constexpr uint32_t TRACE_ERR_LIMIT = 4u;  // more node visits than the mesh has nodes
+// (8 is the radix sort's look-back bound, SORT_ERR_LOOKBACK)
+constexpr uint32_t TRACE_ERR_TLAS = 16u;  // the instance tree's stack overflowed or an index was out of bounds
 
 // Kernel choice and its knobs (picked by the tuner).
 struct TraceParams {

@@ -47,6 +47,27 @@ __device__ __forceinline__ bool ref_bbox_test(float ox, float oy, float oz, floa
     return tmin <= tmax && tmin <= t && tmax > 0;
 }
 
+// The same slab test, also giving the entry distance (for visiting order).
+// For a box containing another, it accepts whenever the test on the inner
+// box accepts (every rounding step is monotonic), so an instance-tree node
+// is never culled where the reference's test enters one of its instances.
+__device__ __forceinline__ bool ref_bbox_entry(float ox, float oy, float oz, float ix, float iy, float iz, float t, const float *bmin,
+                                               const float *bmax, float &tmin_out) {
+    float lo_x = __fmul_rn(ix, __fsub_rn(bmin[0], ox)), hi_x = __fmul_rn(ix, __fsub_rn(bmax[0], ox));
+    if (lo_x > hi_x) { const float tmp = lo_x; lo_x = hi_x; hi_x = tmp; }
+    float lo_y = __fmul_rn(iy, __fsub_rn(bmin[1], oy)), hi_y = __fmul_rn(iy, __fsub_rn(bmax[1], oy));
+    if (lo_y > hi_y) { const float tmp = lo_y; lo_y = hi_y; hi_y = tmp; }
+    float lo_z = __fmul_rn(iz, __fsub_rn(bmin[2], oz)), hi_z = __fmul_rn(iz, __fsub_rn(bmax[2], oz));
+    if (lo_z > hi_z) { const float tmp = lo_z; lo_z = hi_z; hi_z = tmp; }
+    float tmin = lo_x > lo_y ? lo_x : lo_y;
+    if (lo_z > tmin) tmin = lo_z;
+    float tmax = hi_x < hi_y ? hi_x : hi_y;
+    if (hi_z < tmax) tmax = hi_z;
+    tmax = __fmul_rn(tmax, 1.00000024f);
+    tmin_out = tmin;
+    return tmin <= tmax && tmin <= t && tmax > 0;
+}
+
 // safe_invert, CoreRef.cpp:272-294
 __device__ __forceinline__ float safe_inv(float v) {
     float r = __frcp_rn(v);
@@ -149,6 +170,61 @@ __device__ __forceinline__ MeshRef mesh_of(const SceneView &sv, const InstanceRe
     mr.tri_count = __ldg(&ir->tri_count);
     mr.obj = m;
     return mr;
+}
+
+// Instance-tree walk, one ray: pops entries of the ray's instance stack
+// (stk, sp) until an instance whose world box the ray enters with the
+// current best t -- the reference's instance test, bbox_test with the
+// safe-inverted direction -- and returns its index; -1 when the walk is
+// done. An internal node pushes the children whose boxes the ray enters,
+// the nearer on top; an instance pushed this way is tested again when popped
+// (best t may have shrunk). Indices outside the tree and a full stack set
+// TRACE_ERR_TLAS (the walk goes on without the entry).
+constexpr int TLAS_STACK = 48;
+__device__ __forceinline__ int tlas_next(const SceneView &sv, float4 r0, float sx, float sy, float sz, float best_t, uint32_t *stk, int &sp,
+                                         uint32_t &err) {
+    while (sp > 0) {
+        const uint32_t e = stk[--sp];
+        if (e & TLAS_LEAF) {
+            const uint32_t m = e & ~TLAS_LEAF;
+            if (m >= sv.n_inst) {
+                err |= TRACE_ERR_TLAS;
+                continue;
+            }
+            const InstanceRec *ir = sv.inst + m;
+            float bmin[3], bmax[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                bmin[k] = __ldg(&ir->bbox_min[k]);
+                bmax[k] = __ldg(&ir->bbox_max[k]);
+            }
+            if (ref_bbox_test(r0.x, r0.y, r0.z, sx, sy, sz, best_t, bmin, bmax)) return (int)m;
+            continue;
+        }
+        if (e + 1 >= sv.n_inst) {
+            err |= TRACE_ERR_TLAS;
+            continue;
+        }
+        const float4 *np = reinterpret_cast<const float4 *>(sv.tlas + e);
+        const float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
+        const uint4 ids = __ldg(reinterpret_cast<const uint4 *>(np + 3));
+        const float lo0[3] = {a.x, a.y, a.z}, lo1[3] = {a.w, b.x, b.y}, hi0[3] = {b.z, b.w, c.x}, hi1[3] = {c.y, c.z, c.w};
+        float t0 = 0.0f, t1 = 0.0f;
+        const bool h0 = ref_bbox_entry(r0.x, r0.y, r0.z, sx, sy, sz, best_t, lo0, hi0, t0);
+        const bool h1 = ref_bbox_entry(r0.x, r0.y, r0.z, sx, sy, sz, best_t, lo1, hi1, t1);
+        const bool near1 = h1 && (!h0 || t1 < t0); // child 1 first when it is the nearer (or the only) one
+        const uint32_t first = near1 ? ids.y : ids.x, second = near1 ? ids.x : ids.y;
+        const bool has_second = h0 && h1;
+        if (has_second) {
+            if (sp < TLAS_STACK) stk[sp++] = second;
+            else err |= TRACE_ERR_TLAS;
+        }
+        if (h0 || h1) {
+            if (sp < TLAS_STACK) stk[sp++] = first;
+            else err |= TRACE_ERR_TLAS;
+        }
+    }
+    return -1;
 }
 
 // Node step: takes the next child of node group (ng_base, ng_bits), tests
