@@ -237,19 +237,29 @@ __global__ void k_rs_copy(const K *__restrict__ ks, const uint32_t *__restrict__
 
 constexpr uint64_t kCounterWords = RS_COUNTER_WORDS; // digit counts of every pass, then the tile counters
 
+// smaller tiles below 16M items: more blocks and shorter ranking chains per
+// block where one tile per block would leave most of the SMs' warp slots empty
+inline bool small_tiles(uint64_t n) { return n <= (1ull << 24); }
+inline uint32_t tile_count(uint64_t n) {
+    const uint32_t tile = small_tiles(n) ? RS_THREADS * 8 : RS_TILE;
+    return (uint32_t)((n + tile - 1) / tile);
+}
+inline uint32_t *counts_of(void *scratch, uint64_t n, int key_bytes) {
+    return reinterpret_cast<uint32_t *>(static_cast<char *>(scratch) + rs_align256(n * key_bytes) + rs_align256(n * 4));
+}
+inline cudaError_t zero_counters(void *scratch, uint64_t n, int key_bytes, int passes, cudaStream_t st) {
+    return cudaMemsetAsync(counts_of(scratch, n, key_bytes), 0, (kCounterWords + (uint64_t)passes * tile_count(n) * 256) * 4, st);
+}
+
 template <typename K>
 cudaError_t sort_impl(K *keys, uint32_t *vals, uint64_t n, int begin_bit, int end_bit, void *scratch, cudaStream_t st, const uint32_t *n_dev,
-                      bool ident, uint32_t *err) {
+                      bool ident, uint32_t *err, bool counted) {
     const int passes = (end_bit - begin_bit + 7) / 8;
     if (passes < 1 || passes > (int)sizeof(K) || begin_bit < 0 || end_bit > (int)(8 * sizeof(K)) || n > RS_MAX_ITEMS)
         return cudaErrorInvalidValue;
     if (n == 0) return cudaSuccess;
-    // smaller tiles below 16M items: more blocks and shorter ranking chains
-    // per block where one tile per block would leave most of the SMs' warp
-    // slots empty
-    const bool small = n <= (1ull << 24);
-    const uint32_t tile = small ? RS_THREADS * 8 : RS_TILE;
-    const uint32_t num_tiles = (uint32_t)((n + tile - 1) / tile);
+    const bool small = small_tiles(n);
+    const uint32_t num_tiles = tile_count(n);
     char *p = static_cast<char *>(scratch);
     K *keys_alt = reinterpret_cast<K *>(p);
     p += rs_align256(n * sizeof(K));
@@ -258,10 +268,13 @@ cudaError_t sort_impl(K *keys, uint32_t *vals, uint64_t n, int begin_bit, int en
     uint32_t *ghist = reinterpret_cast<uint32_t *>(p);
     uint32_t *counters = ghist + RS_MAX_PASSES * 256;
     uint32_t *status = ghist + kCounterWords;
-    cudaError_t e = cudaMemsetAsync(ghist, 0, (kCounterWords + (uint64_t)passes * num_tiles * 256) * 4, st);
-    if (e != cudaSuccess) return e;
-    k_rs_hist<K><<<num_tiles < HIST_MAX_BLOCKS ? num_tiles : HIST_MAX_BLOCKS, RS_THREADS, 0, st>>>(keys, n, n_dev, begin_bit, passes, ghist);
-    // (the histogram grid: one block per tile up to HIST_MAX_BLOCKS, each striding over the keys)
+    if (!counted) { // else radix_sort_begin zeroed them and the key kernel counted the digits
+        cudaError_t e = zero_counters(scratch, n, (int)sizeof(K), passes, st);
+        if (e != cudaSuccess) return e;
+        // one block per tile up to HIST_MAX_BLOCKS, each striding over the keys
+        k_rs_hist<K><<<num_tiles < HIST_MAX_BLOCKS ? num_tiles : HIST_MAX_BLOCKS, RS_THREADS, 0, st>>>(keys, n, n_dev, begin_bit, passes,
+                                                                                                      ghist);
+    }
     K *src_k = keys, *dst_k = keys_alt;
     const uint32_t *src_v = ident ? nullptr : vals;
     uint32_t *dst_v = vals_alt;
@@ -292,12 +305,23 @@ cudaError_t sort_impl(K *keys, uint32_t *vals, uint64_t n, int begin_bit, int en
 
 size_t radix_sort_scratch_bytes(uint64_t n, int key_bytes) { return radix_sort_scratch_bytes_c(n, key_bytes); }
 
+cudaError_t radix_sort_begin(void *scratch, uint64_t n, int key_bytes, int begin_bit, int end_bit, cudaStream_t st) {
+    const int passes = (end_bit - begin_bit + 7) / 8;
+    if (passes < 1 || passes > key_bytes || n > RS_MAX_ITEMS) return cudaErrorInvalidValue;
+    if (n == 0) return cudaSuccess;
+    return zero_counters(scratch, n, key_bytes, passes, st);
+}
+
+uint32_t *radix_sort_counts(void *scratch, uint64_t n, int key_bytes) { return counts_of(scratch, n, key_bytes); }
+
 cudaError_t radix_sort_pairs(void *keys, uint32_t *vals, uint64_t n, int key_bytes, int begin_bit, int end_bit, void *scratch,
-                             cudaStream_t stream, const uint32_t *n_dev, bool vals_identity, uint32_t *err) {
+                             cudaStream_t stream, const uint32_t *n_dev, bool vals_identity, uint32_t *err, bool counted) {
     if (key_bytes == 8)
-        return sort_impl<uint64_t>(static_cast<uint64_t *>(keys), vals, n, begin_bit, end_bit, scratch, stream, n_dev, vals_identity, err);
+        return sort_impl<uint64_t>(static_cast<uint64_t *>(keys), vals, n, begin_bit, end_bit, scratch, stream, n_dev, vals_identity, err,
+                                   counted);
     if (key_bytes == 4)
-        return sort_impl<uint32_t>(static_cast<uint32_t *>(keys), vals, n, begin_bit, end_bit, scratch, stream, n_dev, vals_identity, err);
+        return sort_impl<uint32_t>(static_cast<uint32_t *>(keys), vals, n, begin_bit, end_bit, scratch, stream, n_dev, vals_identity, err,
+                                   counted);
     return cudaErrorInvalidValue;
 }
 

@@ -39,6 +39,27 @@ constexpr uint64_t radix_sort_scratch_bytes_c(uint64_t n, int key_bytes) {
 }
 size_t radix_sort_scratch_bytes(uint64_t n, int key_bytes);
 
+// Digit counts accumulated by the caller's key kernel instead of the sort's
+// own histogram launch (one read of the keys saved): radix_sort_begin zeroes
+// the sort's counters on the stream; the key kernel counts each key's digits
+// into a block-shared array (rs_count_key; RS_MAX_PASSES x 256 words, zeroed
+// by the block) and adds the block's counts to radix_sort_counts(scratch)
+// (rs_flush_counts); radix_sort_pairs then runs with counted = true and the
+// same n, key_bytes and bit range.
+cudaError_t radix_sort_begin(void *scratch, uint64_t n, int key_bytes, int begin_bit, int end_bit, cudaStream_t st);
+uint32_t *radix_sort_counts(void *scratch, uint64_t n, int key_bytes);
+
+#ifdef __CUDACC__
+template <typename K>
+__device__ __forceinline__ void rs_count_key(uint32_t *s_counts, K key, int begin_bit, int passes) {
+    for (int p = 0; p < passes; p++) atomicAdd(&s_counts[p * 256 + ((uint32_t)(key >> (begin_bit + 8 * p)) & 0xFFu)], 1u);
+}
+__device__ __forceinline__ void rs_flush_counts(const uint32_t *s_counts, uint32_t *g_counts, int passes) {
+    for (int i = threadIdx.x; i < passes * 256; i += blockDim.x)
+        if (s_counts[i]) atomicAdd(&g_counts[i], s_counts[i]);
+}
+#endif
+
 // Sorts keys/vals in place, stably, on the digits in [begin_bit, end_bit).
 // n: the number of items, or, when n_dev is not null, the capacity of the
 // arrays, with the item count read on the device as min(n, *n_dev) (nothing
@@ -48,6 +69,6 @@ size_t radix_sort_scratch_bytes(uint64_t n, int key_bytes);
 // Returns a CUDA error code; n above RS_MAX_ITEMS is cudaErrorInvalidValue.
 cudaError_t radix_sort_pairs(void *keys, uint32_t *vals, uint64_t n, int key_bytes, int begin_bit, int end_bit, void *scratch,
                              cudaStream_t stream, const uint32_t *n_dev = nullptr, bool vals_identity = false,
-                             uint32_t *err = nullptr);
+                             uint32_t *err = nullptr, bool counted = false);
 
 } // namespace rg

@@ -75,13 +75,22 @@ __device__ __forceinline__ uint32_t ray_hash(float4 o, float4 d, float3 root_min
     return (om << 25) | (pm << 24) | (spread3((uint32_t)y) << 2) | (spread3((uint32_t)z) << 1) | spread3((uint32_t)x);
 }
 
+// Hash of every ray, also counted into the radix sort's digit histograms
+// (all four 8-bit digits).
 __global__ void k_ray_hash(const float4 *__restrict__ rays, uint32_t n, float3 root_min, float3 cell, uint32_t *__restrict__ keys_out,
-                           uint32_t *__restrict__ sort_keys) {
+                           uint32_t *__restrict__ sort_keys, uint32_t *__restrict__ counts) {
+    __shared__ uint32_t s_counts[4 * 256];
+    for (int k = threadIdx.x; k < 4 * 256; k += blockDim.x) s_counts[k] = 0;
+    __syncthreads();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t key = ray_hash(rays[2ull * i], rays[2ull * i + 1], root_min, cell);
-    if (keys_out) keys_out[i] = key;
-    sort_keys[i] = key;
+    if (i < n) {
+        const uint32_t key = ray_hash(rays[2ull * i], rays[2ull * i + 1], root_min, cell);
+        if (keys_out) keys_out[i] = key;
+        sort_keys[i] = key;
+        rs_count_key(s_counts, key, 0, 4);
+    }
+    __syncthreads();
+    rs_flush_counts(s_counts, counts, 4);
 }
 
 // Keys of a trace order: the ray hash (mode 1) or the hash with its 8-bit
@@ -106,14 +115,25 @@ __global__ void k_gather_rays(const float4 *__restrict__ rays, const uint32_t *_
 // hash in its job's grid, with the job above it when there are several.
 template <typename Key>
 __global__ void k_loop_keys(const FrameJob *__restrict__ jobs, const float4 *__restrict__ rays, const uint32_t *__restrict__ ray_job,
-                            const uint32_t *__restrict__ count, uint32_t capacity, Key *__restrict__ keys) {
+                            const uint32_t *__restrict__ count, uint32_t capacity, Key *__restrict__ keys, int begin_bit, int passes,
+                            uint32_t *__restrict__ counts) {
+    __shared__ uint32_t s_counts[RS_MAX_PASSES * 256];
+    const uint32_t n = min(*count, capacity);
+    if (blockIdx.x * blockDim.x >= n) return; // the whole block is past the live rays
+    for (int k = threadIdx.x; k < passes * 256; k += blockDim.x) s_counts[k] = 0;
+    __syncthreads();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= min(*count, capacity)) return;
-    const uint32_t j = ray_job[i];
-    const FrameJob &J = jobs[j];
-    const uint32_t h = ray_hash(rays[2ull * i], rays[2ull * i + 1], make_float3(J.root_min[0], J.root_min[1], J.root_min[2]),
-                                make_float3(J.cell[0], J.cell[1], J.cell[2]));
-    keys[i] = sizeof(Key) == 8 ? (Key)(((uint64_t)j << 32) | h) : (Key)h;
+    if (i < n) {
+        const uint32_t j = ray_job[i];
+        const FrameJob &J = jobs[j];
+        const uint32_t h = ray_hash(rays[2ull * i], rays[2ull * i + 1], make_float3(J.root_min[0], J.root_min[1], J.root_min[2]),
+                                    make_float3(J.cell[0], J.cell[1], J.cell[2]));
+        const Key key = sizeof(Key) == 8 ? (Key)(((uint64_t)j << 32) | h) : (Key)h;
+        keys[i] = key;
+        rs_count_key(s_counts, key, begin_bit, passes);
+    }
+    __syncthreads();
+    rs_flush_counts(s_counts, counts, passes);
 }
 
 __global__ void k_loop_gather(const float4 *__restrict__ rays, const RayPayload *__restrict__ pay, const uint32_t *__restrict__ ray_job,
@@ -135,6 +155,9 @@ __global__ void k_loop_gather(const float4 *__restrict__ rays, const RayPayload 
     for (int k = 0; k < (int)(sizeof(RayPayload) / 16); k++) dst[k] = src[k];
     job_out[i] = ray_job[s];
 }
+
+// The render loop's sort keys: the ray hash from this bit up (the job above).
+constexpr int LOOP_SORT_BEGIN_BIT = 16;
 
 int job_bits(int n_jobs) {
     int b = 0;
@@ -159,15 +182,23 @@ cudaError_t launch_loop_sort(const FrameJob *jobs, int n_jobs, const float4 *ray
     uint32_t *perm = reinterpret_cast<uint32_t *>(p + ((uint64_t(capacity) * kb + 255) / 256) * 256);
     void *rs_scratch = reinterpret_cast<char *>(perm) + ((uint64_t(capacity) * 4 + 255) / 256) * 256;
     const uint32_t blocks = (capacity + 255) / 256;
-    // only the live rays (their count is on the device): keys, sort and gather
-    // all read min(*count, capacity) there; blocks past it return at once
-    if (kb == 8)
-        k_loop_keys<uint64_t><<<blocks, 256, 0, st>>>(jobs, rays, ray_job, count, capacity, static_cast<uint64_t *>(keys));
-    else
-        k_loop_keys<uint32_t><<<blocks, 256, 0, st>>>(jobs, rays, ray_job, count, capacity, static_cast<uint32_t *>(keys));
-    cudaError_t e = cudaGetLastError();
+    // Only the live rays (their count is on the device): keys, sort and
+    // gather all read min(*count, capacity) there; blocks past it return at
+    // once. The sort uses the hash's top 16 bits (the direction sector and
+    // the origin's cell at 1/32 of the scene box per axis) under the job:
+    // the images do not depend on the order, and two digit passes group the
+    // rays as well for the trace as four.
+    const int begin = LOOP_SORT_BEGIN_BIT, end = kb == 8 ? 32 + job_bits(n_jobs) : 32, passes = (end - begin + 7) / 8;
+    cudaError_t e = radix_sort_begin(rs_scratch, capacity, kb, begin, end, st);
     if (e != cudaSuccess) return e;
-    e = radix_sort_pairs(keys, perm, capacity, kb, 0, kb == 8 ? 32 + job_bits(n_jobs) : 32, rs_scratch, st, count, true, err);
+    uint32_t *counts = radix_sort_counts(rs_scratch, capacity, kb);
+    if (kb == 8)
+        k_loop_keys<uint64_t><<<blocks, 256, 0, st>>>(jobs, rays, ray_job, count, capacity, static_cast<uint64_t *>(keys), begin, passes, counts);
+    else
+        k_loop_keys<uint32_t><<<blocks, 256, 0, st>>>(jobs, rays, ray_job, count, capacity, static_cast<uint32_t *>(keys), begin, passes, counts);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = radix_sort_pairs(keys, perm, capacity, kb, begin, end, rs_scratch, st, count, true, err, true);
     if (e != cudaSuccess) return e;
     k_loop_gather<<<blocks, 256, 0, st>>>(rays, pay, ray_job, perm, count, capacity, rays_out, pay_out, job_out, count_out);
     return cudaGetLastError();
@@ -183,11 +214,14 @@ cudaError_t sort_rays(const float4 *rays, uint64_t n, const float root_min[3], c
     uint32_t *sort_keys = reinterpret_cast<uint32_t *>(p);
     void *rs_scratch = p + ((n * 4 + 255) / 256) * 256;
     const uint32_t blocks = (uint32_t)((n + 255) / 256);
-    k_ray_hash<<<blocks, 256, 0, st>>>(rays, (uint32_t)n, make_float3(root_min[0], root_min[1], root_min[2]),
-                                       make_float3(cell_size[0], cell_size[1], cell_size[2]), keys_out, sort_keys);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = radix_sort_begin(rs_scratch, n, 4, 0, 32, st);
     if (e != cudaSuccess) return e;
-    e = radix_sort_pairs(sort_keys, perm_out, n, 4, 0, 32, rs_scratch, st, nullptr, true, err);
+    k_ray_hash<<<blocks, 256, 0, st>>>(rays, (uint32_t)n, make_float3(root_min[0], root_min[1], root_min[2]),
+                                       make_float3(cell_size[0], cell_size[1], cell_size[2]), keys_out, sort_keys,
+                                       radix_sort_counts(rs_scratch, n, 4));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = radix_sort_pairs(sort_keys, perm_out, n, 4, 0, 32, rs_scratch, st, nullptr, true, err, true);
     if (e != cudaSuccess) return e;
     if (rays_out) {
         k_gather_rays<<<blocks, 256, 0, st>>>(rays, perm_out, (uint32_t)n, rays_out);
