@@ -1228,6 +1228,7 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
     tp.block = s->tuning.block;
     tp.smem_stack = s->tuning.smem_stack;
     tp.stream_hint = s->tuning.stream_hint;
+    tp.tlas = s->tlas.nodes != nullptr;
     // L2 residency of the nodes or leaf triangles: an access-policy window on
     // the streams the traces run on, taken off again once they are enqueued
     cudaStreamAttrValue win{};

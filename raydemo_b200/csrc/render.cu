@@ -502,6 +502,7 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
     for (int j = 0; j < n_jobs; j++) {
         bounces = std::max(bounces, jobs[j].bounces);
         tp.max_depth = std::max(tp.max_depth, scn[j]->tuning.deep_stack ? 0xffffffffu : scn[j]->max_depth);
+        if (scn[j]->tlas.nodes) tp.tlas = true; // the kernels that can walk an instance tree
     }
     tp.next_ray = cnt + 2;
     if (n_jobs > 1) { // each ray traced in its job's scene
@@ -602,6 +603,7 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
     for (int q = 0; q < 2; q++) key.add(rays[q]).add(pay[q]).add(job[q]);
     key.add(hits).add(obj).add(cnt).add(shadow.recs).add(shadow.rays).add(shadow.job).add(rb->d_loop_sort.p).add(nee).add(ref_lights);
     key.add(sv.nodes).add(sv.leaf_tris).add(sv.inst).add(sv.n_inst).add(tp.persistent).add(tp.refill_min).add(tp.max_depth).add(tp.views);
+    key.add(sv.tlas).add(tp.tlas);
     key.add(ev).add(geo_best).add(geo_tris).add(persp);
     return graph_run(*gs, key.h, st, enqueue);
 }

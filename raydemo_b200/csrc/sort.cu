@@ -4,6 +4,8 @@
 // of the rays by that 32-bit key: the reference compresses runs of equal
 // adjacent keys into chunks, radix-sorts the chunks stably and expands them
 // again, so equal keys keep their input order.
+#include <algorithm>
+
 #include "radix_sort.cuh"
 #include "render.cuh"
 #include "sort.cuh"
@@ -76,14 +78,13 @@ __device__ __forceinline__ uint32_t ray_hash(float4 o, float4 d, float3 root_min
 }
 
 // Hash of every ray, also counted into the radix sort's digit histograms
-// (all four 8-bit digits).
+// (all four 8-bit digits); a grid-stride loop.
 __global__ void k_ray_hash(const float4 *__restrict__ rays, uint32_t n, float3 root_min, float3 cell, uint32_t *__restrict__ keys_out,
                            uint32_t *__restrict__ sort_keys, uint32_t *__restrict__ counts) {
     __shared__ uint32_t s_counts[4 * 256];
     for (int k = threadIdx.x; k < 4 * 256; k += blockDim.x) s_counts[k] = 0;
     __syncthreads();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t key = ray_hash(rays[2ull * i], rays[2ull * i + 1], root_min, cell);
         if (keys_out) keys_out[i] = key;
         sort_keys[i] = key;
@@ -92,6 +93,10 @@ __global__ void k_ray_hash(const float4 *__restrict__ rays, uint32_t n, float3 r
     __syncthreads();
     rs_flush_counts(s_counts, counts, 4);
 }
+
+// Blocks of the key kernels: a grid that strides over the rays, few enough
+// that the blocks' flushes of their digit counts stay cheap.
+constexpr uint32_t KEY_BLOCKS = 148 * 4;
 
 // Keys of a trace order: the ray hash (mode 1) or the hash with its 8-bit
 // direction sector moved below the origin cell (mode 2).
@@ -122,8 +127,7 @@ __global__ void k_loop_keys(const FrameJob *__restrict__ jobs, const float4 *__r
     if (blockIdx.x * blockDim.x >= n) return; // the whole block is past the live rays
     for (int k = threadIdx.x; k < passes * 256; k += blockDim.x) s_counts[k] = 0;
     __syncthreads();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t j = ray_job[i];
         const FrameJob &J = jobs[j];
         const uint32_t h = ray_hash(rays[2ull * i], rays[2ull * i + 1], make_float3(J.root_min[0], J.root_min[1], J.root_min[2]),
@@ -182,6 +186,7 @@ cudaError_t launch_loop_sort(const FrameJob *jobs, int n_jobs, const float4 *ray
     uint32_t *perm = reinterpret_cast<uint32_t *>(p + ((uint64_t(capacity) * kb + 255) / 256) * 256);
     void *rs_scratch = reinterpret_cast<char *>(perm) + ((uint64_t(capacity) * 4 + 255) / 256) * 256;
     const uint32_t blocks = (capacity + 255) / 256;
+    const uint32_t key_blocks = std::min(blocks, KEY_BLOCKS);
     // Only the live rays (their count is on the device): keys, sort and
     // gather all read min(*count, capacity) there; blocks past it return at
     // once. The sort uses the hash's top 16 bits (the direction sector and
@@ -193,9 +198,11 @@ cudaError_t launch_loop_sort(const FrameJob *jobs, int n_jobs, const float4 *ray
     if (e != cudaSuccess) return e;
     uint32_t *counts = radix_sort_counts(rs_scratch, capacity, kb);
     if (kb == 8)
-        k_loop_keys<uint64_t><<<blocks, 256, 0, st>>>(jobs, rays, ray_job, count, capacity, static_cast<uint64_t *>(keys), begin, passes, counts);
+        k_loop_keys<uint64_t><<<key_blocks, 256, 0, st>>>(jobs, rays, ray_job, count, capacity, static_cast<uint64_t *>(keys), begin, passes,
+                                                         counts);
     else
-        k_loop_keys<uint32_t><<<blocks, 256, 0, st>>>(jobs, rays, ray_job, count, capacity, static_cast<uint32_t *>(keys), begin, passes, counts);
+        k_loop_keys<uint32_t><<<key_blocks, 256, 0, st>>>(jobs, rays, ray_job, count, capacity, static_cast<uint32_t *>(keys), begin, passes,
+                                                         counts);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     e = radix_sort_pairs(keys, perm, capacity, kb, begin, end, rs_scratch, st, count, true, err, true);
@@ -216,7 +223,7 @@ cudaError_t sort_rays(const float4 *rays, uint64_t n, const float root_min[3], c
     const uint32_t blocks = (uint32_t)((n + 255) / 256);
     cudaError_t e = radix_sort_begin(rs_scratch, n, 4, 0, 32, st);
     if (e != cudaSuccess) return e;
-    k_ray_hash<<<blocks, 256, 0, st>>>(rays, (uint32_t)n, make_float3(root_min[0], root_min[1], root_min[2]),
+    k_ray_hash<<<std::min(blocks, KEY_BLOCKS), 256, 0, st>>>(rays, (uint32_t)n, make_float3(root_min[0], root_min[1], root_min[2]),
                                        make_float3(cell_size[0], cell_size[1], cell_size[2]), keys_out, sort_keys,
                                        radix_sort_counts(rs_scratch, n, 4));
     e = cudaGetLastError();

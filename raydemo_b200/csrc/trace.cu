@@ -45,7 +45,7 @@ __device__ __forceinline__ void flush_counters(uint32_t err, uint32_t nvis, uint
     }
 }
 
-template <bool COUNT, bool DEEP>
+template <bool COUNT, bool DEEP, bool TLAS = false>
 __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, const float4 *__restrict__ rays, uint32_t n, float4 *__restrict__ hits,
                                                                int32_t *__restrict__ obj_out, uint32_t *__restrict__ err_out,
                                                                unsigned long long *__restrict__ counters, const uint32_t *__restrict__ n_dev,
@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
         best.prim = -1;
         best.obj = -1;
         const float sx = safe_inv(r1.x), sy = safe_inv(r1.y), sz = safe_inv(r1.z);
-        if (sv.tlas) { // the instance tree
+        if (TLAS && sv.tlas) { // the instance tree
             uint32_t tstk[TLAS_STACK];
             int tsp = 1;
             tstk[0] = 0;
@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
 // whose SceneView is at views + ray_job[i] * view_stride.
 // ANY: shadow rays -- a ray ends at its first accepted hit on a solid
 // triangle (Traverse_MacroTree_WithStack_AnyHit, CoreRef.cpp:1224-1368).
-template <bool COUNT, bool DEEP, bool MULTI = false, bool ANY = false, int BLOCK = TRACE_BLOCK, int SDEPTH = SMEM_STACK>
+template <bool COUNT, bool DEEP, bool MULTI = false, bool ANY = false, int BLOCK = TRACE_BLOCK, int SDEPTH = SMEM_STACK, bool TLAS = false>
 __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const float4 *__restrict__ rays, uint32_t n,
                                                                   float4 *__restrict__ hits, int32_t *__restrict__ obj_out,
                                                                   uint32_t *__restrict__ err_out, unsigned long long *__restrict__ counters,
@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
     const uint32_t lanemask_lt = (1u << lane) - 1u;
     uint32_t err = 0, nvis = 0, ntri = 0;
     uint32_t ri = NO_RAY, mi = 0, visits = 0, steps = 0;
-    uint32_t tstk[TLAS_STACK]; // the ray's instance-tree stack (scenes with an instance tree)
+    uint32_t tstk[TLAS ? TLAS_STACK : 1]; // the ray's instance-tree stack (scenes with an instance tree)
     int tsp = 0;
     bool in_mesh = false, pool_empty = false;
     Best best;
@@ -143,8 +143,10 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
                 if (idx < n) {
                     ri = order ? __ldg(order + idx) : idx;
                     mi = 0;
-                    tstk[0] = 0; // the tree's root, for a scene that has one
-                    tsp = 1;
+                    if (TLAS) {
+                        tstk[0] = 0; // the tree's root, for a scene that has one
+                        tsp = 1;
+                    }
                     in_mesh = false;
                     best.t = __ldg(&rays[2ull * ri].w);
                     best.u = best.v = 0.0f;
@@ -165,7 +167,7 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
             SceneView job_sv;
             if (MULTI) job_sv = *reinterpret_cast<const SceneView *>(views + (size_t)__ldg(ray_job + ri) * view_stride);
             const SceneView &lsv = MULTI ? job_sv : sv;
-            if (lsv.tlas) {
+            if (TLAS && lsv.tlas) {
                 const int m = tlas_next(lsv, r0, sx, sy, sz, best.t, tstk, tsp, err);
                 if (m >= 0) {
                     const InstanceRec *ir = lsv.inst + m;
@@ -180,7 +182,7 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
                     in_mesh = true;
                 }
             }
-            while (!lsv.tlas && mi < lsv.n_inst) {
+            while ((!TLAS || !lsv.tlas) && mi < lsv.n_inst) {
                 const InstanceRec *ir = lsv.inst + mi;
                 float bmin[3], bmax[3];
 #pragma unroll
@@ -263,11 +265,11 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
     flush_counters<COUNT>(err, nvis, ntri, err_out, counters);
 }
 
-int g_persistent_blocks[2] = {0, 0};
+int g_persistent_blocks[2][2] = {{0, 0}, {0, 0}}; // [DEEP][TLAS]
 
 // The closest-hit persistent kernel with a tuned block size and shared stack
 // depth (one resident grid: the SM count times the blocks that fit per SM).
-template <bool DEEP, int BLOCK, int SDEPTH>
+template <bool DEEP, bool TLAS, int BLOCK, int SDEPTH>
 cudaError_t launch_tuned(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
                          unsigned long long *counters, cudaStream_t st, const TraceParams &tp) {
     static_assert(SDEPTH * BLOCK * 8 <= 48 * 1024, "static shared memory limit");
@@ -277,22 +279,23 @@ cudaError_t launch_tuned(const SceneView &sv, const float4 *rays, uint32_t n, fl
         cudaError_t e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_persistent<false, DEEP, false, false, BLOCK, SDEPTH>, BLOCK, 0);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_persistent<false, DEEP, false, false, BLOCK, SDEPTH, TLAS>,
+                                                              BLOCK, 0);
         if (e != cudaSuccess) return e;
         blocks = sms * (per_sm > 0 ? per_sm : 1);
     }
     cudaError_t e = cudaMemsetAsync(tp.next_ray, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
-    k_trace_persistent<false, DEEP, false, false, BLOCK, SDEPTH><<<blocks, BLOCK, 0, st>>>(
+    k_trace_persistent<false, DEEP, false, false, BLOCK, SDEPTH, TLAS><<<blocks, BLOCK, 0, st>>>(
         sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min, tp.count, nullptr, 0, nullptr, tp.order, tp.stream_hint);
     return cudaGetLastError();
 }
 
-template <bool DEEP>
+template <bool DEEP, bool TLAS>
 cudaError_t launch_tuned_dispatch(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
                                   unsigned long long *counters, cudaStream_t st, const TraceParams &tp) {
 #define RG_TUNED(B, D)                                                                                                                  \
-    if (tp.block == B && tp.smem_stack == D) return launch_tuned<DEEP, B, D>(sv, rays, n, hits, obj, err, counters, st, tp);
+    if (tp.block == B && tp.smem_stack == D) return launch_tuned<DEEP, TLAS, B, D>(sv, rays, n, hits, obj, err, counters, st, tp);
     RG_TUNED(64, 16) RG_TUNED(64, 24) RG_TUNED(64, 32)
     RG_TUNED(128, 16) RG_TUNED(128, 32)
     RG_TUNED(256, 16) RG_TUNED(256, 24)
@@ -300,26 +303,28 @@ cudaError_t launch_tuned_dispatch(const SceneView &sv, const float4 *rays, uint3
     return cudaErrorInvalidValue;
 }
 
-template <bool DEEP>
+template <bool DEEP, bool TLAS>
 cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
                         unsigned long long *counters, bool count, cudaStream_t st, const TraceParams &tp) {
+    constexpr int B = TRACE_BLOCK, D = SMEM_STACK;
     if (!tp.persistent && !tp.views && !tp.any) {
         const uint32_t grid = (n + TRACE_BLOCK - 1) / TRACE_BLOCK;
         if (count)
-            k_trace_closest<true, DEEP><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.count, tp.order);
+            k_trace_closest<true, DEEP, TLAS><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.count, tp.order);
         else
-            k_trace_closest<false, DEEP><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.count, tp.order);
+            k_trace_closest<false, DEEP, TLAS><<<grid, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.count, tp.order);
         return cudaGetLastError();
     }
     if (!tp.next_ray) return cudaErrorInvalidValue;
     if (!count && !tp.views && !tp.any && !(tp.block == TRACE_BLOCK && tp.smem_stack == SMEM_STACK))
-        return launch_tuned_dispatch<DEEP>(sv, rays, n, hits, obj, err, counters, st, tp);
-    int &blocks = g_persistent_blocks[DEEP ? 1 : 0];
+        return launch_tuned_dispatch<DEEP, TLAS>(sv, rays, n, hits, obj, err, counters, st, tp);
+    int &blocks = g_persistent_blocks[DEEP ? 1 : 0][TLAS ? 1 : 0];
     if (blocks == 0) {
         int dev = 0, sms = 0, per_sm = 0;
         cudaError_t e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_persistent<false, DEEP>, TRACE_BLOCK, 0);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_persistent<false, DEEP, false, false, B, D, TLAS>, TRACE_BLOCK, 0);
         if (e != cudaSuccess) return e;
         blocks = sms * (per_sm > 0 ? per_sm : 1);
     }
@@ -327,24 +332,24 @@ cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, flo
     if (e != cudaSuccess) return e;
     if (tp.any) { // shadow rays (no counting variant)
         if (tp.views)
-            k_trace_persistent<false, DEEP, true, true><<<blocks, TRACE_BLOCK, 0, st>>>(
+            k_trace_persistent<false, DEEP, true, true, B, D, TLAS><<<blocks, TRACE_BLOCK, 0, st>>>(
                 sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min, tp.count, tp.views, tp.view_stride, tp.ray_job);
         else
-            k_trace_persistent<false, DEEP, false, true><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray,
-                                                                                        tp.refill_min, tp.count);
+            k_trace_persistent<false, DEEP, false, true, B, D, TLAS><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters,
+                                                                                                 tp.next_ray, tp.refill_min, tp.count);
         return cudaGetLastError();
     }
     if (tp.views) { // rays of several scenes (no counting variant)
-        k_trace_persistent<false, DEEP, true><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray,
-                                                                               tp.refill_min, tp.count, tp.views, tp.view_stride, tp.ray_job);
+        k_trace_persistent<false, DEEP, true, false, B, D, TLAS><<<blocks, TRACE_BLOCK, 0, st>>>(
+            sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min, tp.count, tp.views, tp.view_stride, tp.ray_job);
         return cudaGetLastError();
     }
     if (count)
-        k_trace_persistent<true, DEEP><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min,
-                                                                        tp.count, nullptr, 0, nullptr, tp.order);
+        k_trace_persistent<true, DEEP, false, false, B, D, TLAS><<<blocks, TRACE_BLOCK, 0, st>>>(
+            sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min, tp.count, nullptr, 0, nullptr, tp.order);
     else
-        k_trace_persistent<false, DEEP><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min,
-                                                                         tp.count, nullptr, 0, nullptr, tp.order, tp.stream_hint);
+        k_trace_persistent<false, DEEP, false, false, B, D, TLAS><<<blocks, TRACE_BLOCK, 0, st>>>(
+            sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min, tp.count, nullptr, 0, nullptr, tp.order, tp.stream_hint);
     return cudaGetLastError();
 }
 
@@ -357,8 +362,12 @@ cudaError_t launch_trace_closest(const SceneView &sv, const float4 *rays, uint32
     // depth in levels (the tuned closest-hit kernel's depth where it applies)
     const bool tuned = tp.persistent && !count && !tp.views && !tp.any;
     const uint32_t sdepth = tuned ? (uint32_t)tp.smem_stack : (uint32_t)SMEM_STACK;
-    if (tp.max_depth < sdepth) return launch_impl<false>(sv, rays, n, hits, obj, err, counters, count, st, tp);
-    return launch_impl<true>(sv, rays, n, hits, obj, err, counters, count, st, tp);
+    if (tp.tlas) {
+        if (tp.max_depth < sdepth) return launch_impl<false, true>(sv, rays, n, hits, obj, err, counters, count, st, tp);
+        return launch_impl<true, true>(sv, rays, n, hits, obj, err, counters, count, st, tp);
+    }
+    if (tp.max_depth < sdepth) return launch_impl<false, false>(sv, rays, n, hits, obj, err, counters, count, st, tp);
+    return launch_impl<true, false>(sv, rays, n, hits, obj, err, counters, count, st, tp);
 }
 
 } // namespace rg

@@ -46,6 +46,9 @@ struct TraceParams {
     const uint8_t *views = nullptr;
     uint32_t view_stride = 0;
     const uint32_t *ray_job = nullptr;
+    // some scene of the launch has an instance tree: the kernels that walk it
+    // (the others test the instance boxes in turn and carry no tree stack)
+    bool tlas = false;
     // trace order: the k-th ray taken is ray order[k] (its hit is written at
     // that index); null: input order
     const uint32_t *order = nullptr;
