@@ -252,7 +252,7 @@ int ray_sort_rays(ray_renderer *r, const float *rays, uint64_t n, const float ro
  * belongs to their own allocator and budget, and frame loops that must not
  * stall on cudaMalloc's implicit device-wide synchronisation. Same inputs,
  * outputs and results as ray_sort_rays, without a renderer: the scratch
- * memory is a fixed array of 14,688,768 bytes (14.01 MiB) that every GPU
+ * memory is a fixed array of 13,640,192 bytes (13.01 MiB) that every GPU
  * loading this library holds until the process exits, so n is limited to
  * RAY_SORT_NOALLOC_MAX_RAYS (larger n: RAY_ERR_INVALID_ARG). The first call on
  * a device looks the array up on the current device and keeps its address for

@@ -4,12 +4,13 @@
 // all digit passes, then one launch per pass (plus a copy when the number of
 // passes is odd, so that the result ends in the caller's arrays).
 //
-// A pass, per tile of 256 x ITEMS keys (ITEMS 8 up to 16M items, else 16;
-// tiles are numbered in the order their
+// A pass, per tile of RS_TILE = 256 x 16 keys (tiles are numbered in the
+// order their
 // blocks start, through an atomic counter, so every tile's predecessors are
 // running or done):
-//   1. each warp ranks its 32 x ITEMS keys stably (index order) with match
-//      masks and per-warp digit counters in shared memory;
+//   1. each warp ranks its 32 x ITEMS keys stably (index order): the lanes
+//      of one digit found with one ballot per digit bit, per-warp digit
+//      counters in shared memory;
 //   2. thread d sums digit d over the warps and publishes the tile's count of
 //      d (flag AGG; tile 0 publishes it as INC, an inclusive prefix);
 //   3. thread d walks back over the preceding tiles' status words of digit d,
@@ -31,7 +32,7 @@ namespace {
 constexpr uint32_t ST_AGG = 1u << 30, ST_INC = 2u << 30, ST_COUNT = (1u << 30) - 1u;
 constexpr uint32_t LOOKBACK_SPIN_LIMIT = 1u << 21; // polls of one word (with a short sleep) before giving up
 constexpr uint32_t HIST_MAX_BLOCKS = 148 * 8;
-constexpr int LOOKBACK = 16; // preceding tiles read per look-back round
+constexpr int LOOKBACK = 24; // preceding tiles read per look-back round
 
 __device__ __forceinline__ uint32_t ld_relaxed(const uint32_t *p) {
     uint32_t v;
@@ -89,7 +90,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const K *__restrict__ ke
 
 // One digit pass. vals_in null: the values are the items' input indices.
 template <typename K, int ITEMS>
-__global__ void __launch_bounds__(RS_THREADS, ITEMS <= 8 ? 3 : 2) k_rs_onesweep(const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+__global__ void __launch_bounds__(RS_THREADS, 2) k_rs_onesweep(const K *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                                                             K *__restrict__ keys_out, uint32_t *__restrict__ vals_out, uint64_t cap,
                                                             const uint32_t *__restrict__ n_dev, int shift, const uint32_t *__restrict__ ghist,
                                                             uint32_t *__restrict__ tile_counter, uint32_t *__restrict__ status,
@@ -123,20 +124,26 @@ __global__ void __launch_bounds__(RS_THREADS, ITEMS <= 8 ? 3 : 2) k_rs_onesweep(
         v[j] = ok ? (vals_in ? vals_in[tile_base + li] : (uint32_t)(tile_base + li)) : 0u;
     }
     // stable rank among the warp's keys of the same digit: the lanes of one
-    // digit (a match group) take their places in lane order after the
-    // group's earlier keys, whose count the group's lowest lane reads and
-    // advances with one shared atomic; the warp is synchronised after each
-    // key, so the counts advance in key order
+    // digit (a group, found with one ballot per digit bit) take their places
+    // in lane order after the group's earlier keys, whose count the group's
+    // lowest lane reads and advances with one shared atomic; the warp is
+    // synchronised after each key, so the counts advance in key order
     const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
     for (int j = 0; j < ITEMS; j++) {
         const uint32_t li = wbase + (uint32_t)j * 32u + lane;
-        const uint32_t d = li < tile_n ? digit(k[j], shift) : 256u;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        const uint32_t leader = __ffs(peers) - 1u;
+        const bool ok = li < tile_n;
+        const uint32_t d = ok ? digit(k[j], shift) : 0u;
+        uint32_t peers = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const uint32_t m = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+            peers &= ((d >> b) & 1u) ? m : ~m;
+        }
+        const uint32_t leader = __ffs(peers) - 1u; // invalid lanes get a group of valid lanes or none; they use nothing
         uint32_t before = 0;
-        if (d < 256u && lane == leader) before = atomicAdd(&s_whist[warp][d], (uint32_t)__popc(peers));
-        before = __shfl_sync(0xffffffffu, before, leader);
+        if (ok && lane == leader) before = atomicAdd(&s_whist[warp][d], (uint32_t)__popc(peers));
+        before = __shfl_sync(0xffffffffu, before, ok ? leader : lane);
         pos[j] = before + __popc(peers & lt);
         __syncwarp(); // this key's atomic is done before the next key's
     }
@@ -237,13 +244,7 @@ __global__ void k_rs_copy(const K *__restrict__ ks, const uint32_t *__restrict__
 
 constexpr uint64_t kCounterWords = RS_COUNTER_WORDS; // digit counts of every pass, then the tile counters
 
-// smaller tiles below 16M items: more blocks and shorter ranking chains per
-// block where one tile per block would leave most of the SMs' warp slots empty
-inline bool small_tiles(uint64_t n) { return n <= (1ull << 24); }
-inline uint32_t tile_count(uint64_t n) {
-    const uint32_t tile = small_tiles(n) ? RS_THREADS * 8 : RS_TILE;
-    return (uint32_t)((n + tile - 1) / tile);
-}
+inline uint32_t tile_count(uint64_t n) { return (uint32_t)((n + RS_TILE - 1) / RS_TILE); }
 inline uint32_t *counts_of(void *scratch, uint64_t n, int key_bytes) {
     return reinterpret_cast<uint32_t *>(static_cast<char *>(scratch) + rs_align256(n * key_bytes) + rs_align256(n * 4));
 }
@@ -258,7 +259,6 @@ cudaError_t sort_impl(K *keys, uint32_t *vals, uint64_t n, int begin_bit, int en
     if (passes < 1 || passes > (int)sizeof(K) || begin_bit < 0 || end_bit > (int)(8 * sizeof(K)) || n > RS_MAX_ITEMS)
         return cudaErrorInvalidValue;
     if (n == 0) return cudaSuccess;
-    const bool small = small_tiles(n);
     const uint32_t num_tiles = tile_count(n);
     char *p = static_cast<char *>(scratch);
     K *keys_alt = reinterpret_cast<K *>(p);
@@ -279,13 +279,8 @@ cudaError_t sort_impl(K *keys, uint32_t *vals, uint64_t n, int begin_bit, int en
     const uint32_t *src_v = ident ? nullptr : vals;
     uint32_t *dst_v = vals_alt;
     for (int q = 0; q < passes; q++) {
-        if (small)
-            k_rs_onesweep<K, 8><<<num_tiles, RS_THREADS, 0, st>>>(src_k, src_v, dst_k, dst_v, n, n_dev, begin_bit + 8 * q, ghist + 256 * q,
-                                                                 counters + q, status + (uint64_t)q * num_tiles * 256, err);
-        else
-            k_rs_onesweep<K, RS_ITEMS><<<num_tiles, RS_THREADS, 0, st>>>(src_k, src_v, dst_k, dst_v, n, n_dev, begin_bit + 8 * q,
-                                                                        ghist + 256 * q, counters + q,
-                                                                        status + (uint64_t)q * num_tiles * 256, err);
+        k_rs_onesweep<K, RS_ITEMS><<<num_tiles, RS_THREADS, 0, st>>>(src_k, src_v, dst_k, dst_v, n, n_dev, begin_bit + 8 * q, ghist + 256 * q,
+                                                                    counters + q, status + (uint64_t)q * num_tiles * 256, err);
         K *tk = src_k;
         src_k = dst_k;
         dst_k = tk;

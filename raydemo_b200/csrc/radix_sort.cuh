@@ -16,9 +16,8 @@
 namespace rg {
 
 constexpr int RS_THREADS = 256;                // one digit per thread
-constexpr int RS_ITEMS = 16;                   // keys per thread per tile (above 16M items; 8 below)
+constexpr int RS_ITEMS = 16;                   // keys per thread per tile
 constexpr int RS_TILE = RS_THREADS * RS_ITEMS; // 4096 keys per tile
-constexpr int RS_TILE_MIN = RS_THREADS * 8;    // the smaller tile, which sizes the status words
 constexpr int RS_WARPS = RS_THREADS / 32;
 constexpr int RS_MAX_PASSES = 8;
 constexpr uint64_t RS_MAX_ITEMS = (1ull << 30) - 1; // look-back counts are 30 bits
@@ -35,7 +34,7 @@ constexpr uint64_t RS_COUNTER_WORDS = RS_MAX_PASSES * 256 + 64;
 constexpr uint64_t rs_align256(uint64_t b) { return (b + 255) / 256 * 256; }
 constexpr uint64_t radix_sort_scratch_bytes_c(uint64_t n, int key_bytes) {
     return rs_align256(n * key_bytes) + rs_align256(n * 4) +
-           (RS_COUNTER_WORDS + (uint64_t)key_bytes * ((n + RS_TILE_MIN - 1) / RS_TILE_MIN) * 256) * 4 + 256;
+           (RS_COUNTER_WORDS + (uint64_t)key_bytes * ((n + RS_TILE - 1) / RS_TILE) * 256) * 4 + 256;
 }
 size_t radix_sort_scratch_bytes(uint64_t n, int key_bytes);
 
