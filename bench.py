@@ -166,6 +166,13 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
+def tuned_tuple(info) -> dict:
+    """The frame tuner's choice as the renderer reports it after a frame."""
+    return {"kernel": {1: "wavefront", 2: "path"}.get(info.kernel, "?"), "sort_mask": f"0x{info.sort_mask:03x}",
+            "trace_variant": int(info.trace_variant), "refill": int(info.trace_refill), "block": int(info.trace_block),
+            "smem_stack": int(info.trace_stack)}
+
+
 def make_workload(rank: int, n_tris: int = N_TRIS, n_rays: int = N_RAYS):
     """Rank `rank`'s share of an N-GPU run: the same scene on every rank (a
     replica) and the rank's own seeded rays (weak scaling: rays per rank fixed)."""
@@ -282,7 +289,8 @@ def render_frames(args, dev, stream, rank: int, world: int) -> dict:
 
     by_kernel = {"wavefront": round(timed(1), 4), "path": round(timed(2), 4)}
     ms_frame = timed(0)
-    chosen = {1: "wavefront", 2: "path"}.get(r.frame_info().kernel, "?")
+    chosen_info = r.frame_info()
+    chosen = {1: "wavefront", 2: "path"}.get(chosen_info.kernel, "?")
     # end to end through the public API: RenderScene, then the pixels read back to the host
     e_frames = max(5, min(frames, 50))
     ev0.record(stream)
@@ -296,6 +304,7 @@ def render_frames(args, dev, stream, rank: int, world: int) -> dict:
            "mrays_per_s": round(world * rays_per_frame / (ms_frame * 1e-3) / 1e6, 2), "rays_per_frame": int(rays_per_frame),
            "closest_hit_rays_per_frame": int(info.rays), "shadow_rays_per_frame": int(info.shadow_rays),
            "e2e_ms_per_frame": round(ms_e2e, 4), "e2e_d2h_bytes_per_frame": w * h * 16, "kernel": chosen,
+           "tuned": tuned_tuple(chosen_info),
            "ms_per_frame_by_kernel": by_kernel}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -422,7 +431,8 @@ def batch_frames(args, dev, stream, n_scenes: int = 64, samples: int = 4) -> dic
             "plain_loop_ms": round(plain_ms, 3), "speedup_vs_plain": round(plain_ms / batch_ms, 3),
             "batch_mrays_per_s": round(rays / (batch_ms * 1e-3) / 1e6, 1), "rays": int(rays),
             "plain_kernels": {"wavefront": kernels.count(1), "path": kernels.count(2)},
-            "batch_kernel": {1: "wavefront", 2: "path"}.get(info.kernel, "?"), "batch_ms_by_kernel": by_kernel,
+            "batch_kernel": {1: "wavefront", 2: "path"}.get(info.kernel, "?"), "tuned": tuned_tuple(info),
+            "batch_ms_by_kernel": by_kernel,
             "images_identical_to_plain": f"{identical}/{n_scenes}", "max_rmse_vs_plain": worst}
 
 
@@ -471,6 +481,8 @@ def atrium_frames(args, dev, stream, rank: int, world: int) -> dict:
     image = r.get_pixels_ref()
     frames = max(2, min(args.steps // 10, 5))
 
+    phase_us = {}  # per variant: the stats' phase times per frame (us)
+
     def timed(kernel: int, sort: int) -> float:
         r.set_kernel(kernel)
         r.set_ray_sort(sort)
@@ -480,11 +492,13 @@ def atrium_frames(args, dev, stream, rank: int, world: int) -> dict:
         torch.cuda.synchronize(dev)
         if world > 1:
             dist.barrier()
+        r.ResetStats()
         ev0.record(stream)
         for _ in range(frames):
             frame(g)
         ev1.record(stream)
         torch.cuda.synchronize(dev)
+        phase_us[(kernel, sort)] = {k: int(v) // frames for k, v in r.GetStats().items()}
         return max_over_ranks(ev0.elapsed_time(ev1) / frames, world, dev)
 
     variants = {"wavefront_sort_off": timed(1, 0), "wavefront_sort_all": timed(1, 0x3FF), "wavefront_sort_auto": timed(1, -1)}
@@ -507,7 +521,9 @@ def atrium_frames(args, dev, stream, rank: int, world: int) -> dict:
            "frames": frames, "mrays_per_s": round(world * all_rays / (ms_frame * 1e-3) / 1e6, 1), "rays_per_frame": int(all_rays),
            "closest_hit_rays_per_frame": int(rays), "shadow_rays_per_frame": int(shadow),
            "ms_per_frame_by_variant": {k: round(v, 3) for k, v in variants.items()},
-           "auto_sort_mask": f"0x{auto_mask:03x}", "chosen": {"kernel": {1: "wavefront", 2: "path"}.get(chosen.kernel, "?"),
+           "auto_sort_mask": f"0x{auto_mask:03x}", "tuned": tuned_tuple(chosen),
+           "phase_us_per_frame": {"wavefront_sort_off": phase_us.get((1, 0)), "wavefront_sort_all": phase_us.get((1, 0x3FF))},
+           "chosen": {"kernel": {1: "wavefront", 2: "path"}.get(chosen.kernel, "?"),
                                                               "sort_mask": f"0x{chosen.sort_mask:03x}"},
            "e2e_ms_per_frame": round(ms_e2e, 3), "e2e_d2h_bytes_per_frame": w * h * 16, "data": "synthetic (seeded procedural scene)",
            "stats_us": {k: int(v) for k, v in stats.items()}}

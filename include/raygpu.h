@@ -393,8 +393,23 @@ typedef struct ray_frame_info {
     uint64_t rays, shadow_rays;
     uint32_t sort_mask; /* wavefront: bounces whose rays were sorted first (bit b: secondary bounce b) */
     uint32_t reserved;
+    /* wavefront: the trace settings it ran with (ray_renderer_set_trace_variant):
+     * their index, refill threshold, threads per block and shared stack entries
+     * (0 for each of the three: the scene's own settings) */
+    int32_t trace_variant, trace_refill, trace_block, trace_stack;
 } ray_frame_info;
 int ray_renderer_frame_info(ray_renderer *r, ray_frame_info *out);
+
+/* The wavefront's trace settings (no counterpart in the reference): -1 (the
+ * default) = the frame tuner times them with the kernel and the sort mask on
+ * the first frames of each frame configuration -- index 0 is the scene's own
+ * settings, 1..5 are refill threshold / threads per block / shared stack
+ * entries of (4, 128, 24), (16, 128, 24), (8, 64, 24), (8, 256, 24),
+ * (8, 128, 16) -- and keeps the fastest; the choice is also kept per frame
+ * signature (triangle and light counts, pixels, bounces, settings) for every
+ * renderer of the process; 0..5 = that setting. Every setting renders the
+ * same image. */
+int ray_renderer_set_trace_variant(ray_renderer *r, int variant);
 
 /* Ray sorting in the wavefront (the reference's Ref renderer sorts the
  * continuation rays before every bounce by get_ray_hash, RendererRef.cpp:

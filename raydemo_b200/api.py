@@ -406,6 +406,11 @@ class Renderer:
         """1 wavefront, 2 path kernel, 0 chosen by timing (ray_renderer_set_kernel)."""
         check(lib().ray_renderer_set_kernel(self._h, kernel))
 
+    def set_trace_variant(self, variant: int = -1) -> None:
+        """ray_renderer_set_trace_variant: -1 timed by the frame tuner, else
+        an index of its trace settings (0: the scene's own)."""
+        check(lib().ray_renderer_set_trace_variant(self._h, variant))
+
     def set_ray_sort(self, policy: int = -1) -> None:
         """Ray sorting before the wavefront's bounces (ray_renderer_set_ray_sort):
         -1 chosen per bounce by timing, 0 never, else a mask of bounces (0x3FF all)."""

@@ -97,7 +97,8 @@ class TraceInfo(C.Structure):
 
 class FrameInfo(C.Structure):
     _fields_ = [("error_flags", C.c_uint32), ("kernel", C.c_int32), ("rays", C.c_uint64), ("shadow_rays", C.c_uint64),
-                ("sort_mask", C.c_uint32), ("reserved", C.c_uint32)]
+                ("sort_mask", C.c_uint32), ("reserved", C.c_uint32), ("trace_variant", C.c_int32), ("trace_refill", C.c_int32),
+                ("trace_block", C.c_int32), ("trace_stack", C.c_int32)]
 
 
 class DiffParams(C.Structure):
@@ -178,6 +179,7 @@ _SIGS = {
     "ray_renderer_frame_info": ([_P, C.POINTER(FrameInfo)], C.c_int),
     "ray_renderer_set_stream": ([_P, _P], C.c_int),
     "ray_renderer_set_kernel": ([_P, C.c_int], C.c_int),
+    "ray_renderer_set_trace_variant": ([_P, C.c_int], C.c_int),
     "ray_renderer_set_ray_sort": ([_P, C.c_int], C.c_int),
     "ray_scene_set_diff_params": ([_P, C.POINTER(DiffParams)], C.c_int),
     "ray_render_diff": ([_P, _P, C.c_int, C.c_int, _P, _P], C.c_int),

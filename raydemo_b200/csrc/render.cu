@@ -9,7 +9,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <random>
+#include <tuple>
 
 #include "../../include/raygpu.h"
 #include "radix_sort.cuh"
@@ -115,14 +117,62 @@ int ensure_frame_state(ray_renderer *r) {
     return RAY_OK;
 }
 
+// Trace settings the frame tuner times for the wavefront (a refill
+// threshold, threads per block and shared stack entries of the closest-hit
+// kernel; the block and stack apply to one-scene launches): index 0 leaves
+// the scene's own settings (ray_scene_set_trace_tuning).
+struct TraceVariant {
+    int refill, block, stack;
+};
+constexpr TraceVariant TRACE_VARIANTS[] = {{0, 0, 0}, {4, 128, 24}, {16, 128, 24}, {8, 64, 24}, {8, 256, 24}, {8, 128, 16}};
+constexpr int N_TRACE_VARIANTS = (int)(sizeof(TRACE_VARIANTS) / sizeof(TRACE_VARIANTS[0]));
+static_assert(3 + N_TRACE_VARIANTS - 1 == ray_renderer::N_VARIANTS, "frame variants: 3 plus the trace variants after the first");
+
+// The tuner's choices across renderers: a frame configuration seen before
+// (triangle and light counts, pixels, bounces, the renderer's settings) takes
+// the kernel, sort mask and trace settings chosen then, with no timed frames.
+struct TuneSig {
+    uint32_t tris, lights, pixels;
+    int bounces, kernel_setting, sort_setting, trace_setting;
+    bool operator<(const TuneSig &o) const {
+        return std::tie(tris, lights, pixels, bounces, kernel_setting, sort_setting, trace_setting) <
+               std::tie(o.tris, o.lights, o.pixels, o.bounces, o.kernel_setting, o.sort_setting, o.trace_setting);
+    }
+};
+struct TuneChoice {
+    int kernel;
+    uint32_t mask;
+    int trace_var;
+};
+std::map<TuneSig, TuneChoice> &tune_cache() {
+    static std::map<TuneSig, TuneChoice> c;
+    return c;
+}
+TuneSig sig_of(const ray_renderer::TuneEntry &t) {
+    return TuneSig{t.tris, t.lights, t.pixels, t.bounces, t.kernel_setting, t.sort_setting, t.trace_setting};
+}
+
 // Finishes the timing of a tune entry once every variant it times has its
 // samples: the sort mask (per bounce, sorting where its timed bounce was
 // faster) and the kernel (the path kernel against the wavefront's time with
 // that mask, estimated from the per-bounce times).
 void finish_tune(ray_renderer::TuneEntry &t) {
-    const bool tune_kernel = t.kernel_setting == 0, tune_sort = t.sort_setting < 0;
+    const bool tune_kernel = t.kernel_setting == 0, tune_sort = t.sort_setting < 0, tune_trace = t.trace_setting < 0;
     if (t.n[0] < TUNE_SAMPLES || (tune_kernel && t.n[1] < TUNE_SAMPLES) || (tune_sort && t.n[2] < TUNE_SAMPLES)) return;
-    float wave = t.best[0];
+    if (tune_trace)
+        for (int v = 3; v < ray_renderer::N_VARIANTS; v++)
+            if (t.n[v] < TUNE_SAMPLES) return;
+    // the trace settings: the fastest unsorted wavefront frame among them
+    int tv = tune_trace ? 0 : t.trace_setting;
+    float trace_gain = 0.0f;
+    if (tune_trace)
+        for (int v = 3; v < ray_renderer::N_VARIANTS; v++)
+            if (t.best[v] < t.best[0] - trace_gain) {
+                trace_gain = t.best[0] - t.best[v];
+                tv = v - 2;
+            }
+    t.trace_var = tv;
+    float wave = t.best[0] - trace_gain;
     uint32_t mask = tune_sort ? 0u : (uint32_t)t.sort_setting & SORT_ALL;
     if (tune_sort) {
         for (int b = 0; b < t.bounces && b < MAX_BOUNCES; b++) {
@@ -136,6 +186,7 @@ void finish_tune(ray_renderer::TuneEntry &t) {
     }
     t.mask = mask;
     t.choice = (tune_kernel && t.best[1] < wave) ? 2 : 1;
+    tune_cache()[sig_of(t)] = TuneChoice{t.choice, t.mask, t.trace_var};
 }
 
 // Adds the phase times of a finished frame to the stats (stats_t, RendererBase.h:93-100).
@@ -164,7 +215,7 @@ int resolve_stats(ray_renderer *r, int set) {
         ray_renderer::TuneEntry &t = r->tune[ti];
         const int v = r->ev_variant[set];
         t.best[v] = std::min(t.best[v], ms_between(0, N_EVENTS - 1));
-        if (v != 1)
+        if (v == 0 || v == 2)
             for (int b = 0; b < nb && b < MAX_BOUNCES; b++) {
                 float &slot = t.bounce_ms[v == 2 ? 1 : 0][b];
                 const float ms = ms_between(3 + 3 * b, ev_shaded(b));
@@ -184,6 +235,7 @@ int resolve_stats(ray_renderer *r, int set) {
 struct FramePlan {
     int kernel = 1;
     uint32_t sort_mask = 0;
+    int trace_var = 0; // index of TRACE_VARIANTS
     int tune_entry = -1, variant = 0;
 };
 
@@ -191,9 +243,10 @@ struct FramePlan {
 // fewest timed plus in-flight frames among those the settings leave open.
 int next_variant(const ray_renderer::TuneEntry &t) {
     int best = 0;
-    for (int v = 1; v < 3; v++) {
+    for (int v = 1; v < ray_renderer::N_VARIANTS; v++) {
         if (v == 1 && t.kernel_setting != 0) continue;
         if (v == 2 && t.sort_setting >= 0) continue;
+        if (v >= 3 && t.trace_setting >= 0) continue;
         if (t.n[v] + t.pending[v] < t.n[best] + t.pending[best]) best = v;
     }
     return best;
@@ -204,6 +257,7 @@ FramePlan plan_of_variant(const ray_renderer::TuneEntry &t, int v) {
     p.variant = v;
     p.kernel = v == 1 ? 2 : 1;
     p.sort_mask = v == 2 ? SORT_ALL : (t.sort_setting >= 0 ? (uint32_t)t.sort_setting & SORT_ALL : 0u);
+    p.trace_var = v >= 3 ? v - 2 : (t.trace_setting >= 0 ? t.trace_setting : 0);
     return p;
 }
 
@@ -222,17 +276,19 @@ FramePlan plan_frame(ray_renderer *r, const void *s, uint32_t tris, uint32_t lig
         p.kernel = 2;
         return p;
     }
-    if (r->kernel == 1 && r->sort_policy >= 0) {
+    if (r->kernel == 1 && r->sort_policy >= 0 && r->trace_policy >= 0) {
         p.sort_mask = (uint32_t)r->sort_policy & SORT_ALL;
+        p.trace_var = r->trace_policy;
         return p;
     }
     for (size_t i = 0; i < r->tune.size(); i++) {
         ray_renderer::TuneEntry &t = r->tune[i];
         if (t.scene == s && t.tris == tris && t.lights == lights && t.pixels == pixels && t.bounces == bounces &&
-            t.kernel_setting == r->kernel && t.sort_setting == r->sort_policy) {
+            t.kernel_setting == r->kernel && t.sort_setting == r->sort_policy && t.trace_setting == r->trace_policy) {
             if (t.choice) {
                 p.kernel = t.choice;
                 p.sort_mask = t.choice == 1 ? t.mask : 0u;
+                p.trace_var = t.choice == 1 ? t.trace_var : 0;
                 return p;
             }
             p = plan_of_variant(t, next_variant(t));
@@ -252,6 +308,18 @@ FramePlan plan_frame(ray_renderer *r, const void *s, uint32_t tris, uint32_t lig
     t.bounces = bounces;
     t.kernel_setting = r->kernel;
     t.sort_setting = r->sort_policy;
+    t.trace_setting = r->trace_policy;
+    const auto cached = tune_cache().find(sig_of(t));
+    if (cached != tune_cache().end()) { // chosen before for this signature
+        t.choice = cached->second.kernel;
+        t.mask = cached->second.mask;
+        t.trace_var = cached->second.trace_var;
+        r->tune.push_back(t);
+        p.kernel = t.choice;
+        p.sort_mask = t.choice == 1 ? t.mask : 0u;
+        p.trace_var = t.choice == 1 ? t.trace_var : 0;
+        return p;
+    }
     r->tune.push_back(t);
     p = plan_of_variant(t, 0);
     p.tune_entry = (int)r->tune.size() - 1;
@@ -461,7 +529,7 @@ struct AdjointRun {
 
 int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<FrameJob> &jobs, const std::vector<const ray_scene *> &scn,
                   uint32_t total, int sample0, uint32_t sort_mask, cudaStream_t st, cudaEvent_t *ev, int &nb, bool resolve = true,
-                  const AdjointRun *adj = nullptr, int samples = 1, GraphSlot *gs = nullptr) {
+                  const AdjointRun *adj = nullptr, int samples = 1, GraphSlot *gs = nullptr, int trace_var = 0) {
     nb = 0;
     if (adj) sort_mask = 0; // the replay keeps the forward pass's order
     int rc = ensure_ray_buffers(rb, std::max<size_t>(total, 1));
@@ -503,6 +571,13 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
         bounces = std::max(bounces, jobs[j].bounces);
         tp.max_depth = std::max(tp.max_depth, scn[j]->tuning.deep_stack ? 0xffffffffu : scn[j]->max_depth);
         if (scn[j]->tlas.nodes) tp.tlas = true; // the kernels that can walk an instance tree
+    }
+    tp.block = scn[0]->tuning.block;
+    tp.smem_stack = scn[0]->tuning.smem_stack;
+    if (trace_var > 0 && trace_var < N_TRACE_VARIANTS) { // the frame tuner's trace settings
+        tp.refill_min = TRACE_VARIANTS[trace_var].refill;
+        tp.block = TRACE_VARIANTS[trace_var].block;
+        tp.smem_stack = TRACE_VARIANTS[trace_var].stack;
     }
     tp.next_ray = cnt + 2;
     if (n_jobs > 1) { // each ray traced in its job's scene
@@ -603,7 +678,7 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
     for (int q = 0; q < 2; q++) key.add(rays[q]).add(pay[q]).add(job[q]);
     key.add(hits).add(obj).add(cnt).add(shadow.recs).add(shadow.rays).add(shadow.job).add(rb->d_loop_sort.p).add(nee).add(ref_lights);
     key.add(sv.nodes).add(sv.leaf_tris).add(sv.inst).add(sv.n_inst).add(tp.persistent).add(tp.refill_min).add(tp.max_depth).add(tp.views);
-    key.add(sv.tlas).add(tp.tlas);
+    key.add(sv.tlas).add(tp.tlas).add(tp.block).add(tp.smem_stack);
     key.add(ev).add(geo_best).add(geo_tris).add(persp);
     return graph_run(*gs, key.h, st, enqueue);
 }
@@ -776,7 +851,7 @@ int ray_render(ray_renderer *r, ray_scene *s, ray_region *region) {
         } else {
             // launched directly: its phase events feed the stats and the kernel and sort choice
             rc = run_wavefront(r, d_jobs, std::vector<FrameJob>{J}, std::vector<const ray_scene *>{s}, (uint32_t)n_pix, 0, plan.sort_mask, st,
-                               ev, nb);
+                               ev, nb, true, nullptr, 1, nullptr, plan.trace_var);
             if (rc != RAY_OK) return rc;
         }
         RG_CUDA_TRY(cudaEventRecord(ev[N_EVENTS - 1], st));
@@ -789,6 +864,7 @@ int ray_render(ray_renderer *r, ray_scene *s, ray_region *region) {
         r->ev_frame_pending[set] = true;
         r->last_kernel = kern;
         r->last_sort_mask = kern == 1 ? plan.sort_mask : 0u;
+        r->last_trace_var = kern == 1 ? plan.trace_var : 0;
         r->frame++;
         return RAY_OK;
     } catch (const std::bad_alloc &) {
@@ -896,7 +972,7 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
                     // one wavefront per sample over the rays of all jobs, the run as one CUDA graph
                     int nb = 0;
                     rc = run_wavefront(r0, d_jobs, jobs, jscn, (uint32_t)total, 0, plan.sort_mask, st, nullptr, nb, true, nullptr, run,
-                                       &r0->batch_graph);
+                                       &r0->batch_graph, plan.trace_var);
                     if (rc != RAY_OK) return rc;
                 }
             }
@@ -909,6 +985,8 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
                 if (r->stream != st) RG_CUDA_TRY(cudaStreamWaitEvent(r->stream, r0->ev_sync, 0));
                 r->last_kernel = kern;
                 r->last_sort_mask = kern == 1 ? plan.sort_mask : 0u;
+                r->last_trace_var = kern == 1 ? plan.trace_var : 0;
+        r->last_trace_var = kern == 1 ? plan.trace_var : 0;
             }
             done += run;
         }
@@ -927,6 +1005,17 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
         set_error("host allocation failed");
         return RAY_ERR_OUT_OF_MEMORY;
     }
+}
+
+int ray_renderer_set_trace_variant(ray_renderer *r, int variant) {
+    RG_API_LOCK;
+    RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
+    if (!r || variant < -1 || variant >= N_TRACE_VARIANTS) {
+        set_error("trace variant must be -1 (chosen by timing) or an index of the tuner's trace settings");
+        return RAY_ERR_INVALID_ARG;
+    }
+    r->trace_policy = variant;
+    return RAY_OK;
 }
 
 int ray_renderer_set_kernel(ray_renderer *r, int kernel) {
@@ -1133,6 +1222,11 @@ int ray_renderer_frame_info(ray_renderer *r, ray_frame_info *out) {
     out->error_flags = c[3];
     out->kernel = r->last_kernel;
     out->sort_mask = r->last_sort_mask;
+    out->trace_variant = r->last_trace_var;
+    const TraceVariant &tv = TRACE_VARIANTS[r->last_trace_var];
+    out->trace_refill = tv.refill;
+    out->trace_block = tv.block;
+    out->trace_stack = tv.stack;
     memcpy(&out->rays, c + 4, 8);
     memcpy(&out->shadow_rays, c + 6, 8);
     return RAY_OK;

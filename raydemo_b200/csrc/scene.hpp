@@ -198,19 +198,28 @@ struct ray_renderer {
     // timing, else a mask (bit b: sort before secondary bounce b)
     int sort_policy = -1;
     uint32_t last_sort_mask = 0;
+    // the wavefront's trace settings: -1 chosen by timing, else an index of
+    // rg::TRACE_VARIANTS (0: the scene's own settings)
+    int trace_policy = -1;
+    int last_trace_var = 0;
     // A frame configuration being timed. Variants: 0 wavefront without
     // sorting (or with the fixed mask), 1 path kernel, 2 wavefront sorting
     // before every bounce.
+    // Variants: 0 wavefront without sorting (or with the fixed mask), 1 path
+    // kernel, 2 wavefront sorting before every bounce, 3.. the wavefront of
+    // variant 0 with trace settings rg::TRACE_VARIANTS[1..] (render.cu).
+    static constexpr int N_VARIANTS = 8;
     struct TuneEntry {
         const void *scene = nullptr;
         uint32_t tris = 0, lights = 0, pixels = 0;
         int bounces = 0;
-        int kernel_setting = 0, sort_setting = -1;
+        int kernel_setting = 0, sort_setting = -1, trace_setting = -1;
         int choice = 0;                        // 0 while timing, else the kernel
         uint32_t mask = 0;                     // the sort mask chosen with kernel 1
-        float best[3] = {1e30f, 1e30f, 1e30f}; // best frame time (ms) of each variant
+        int trace_var = 0;                     // the trace settings chosen with kernel 1
+        float best[N_VARIANTS] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f}; // best frame time (ms) of each variant
         float bounce_ms[2][10] = {};           // variants 0 and 2: best time of each bounce (sort + trace + shade)
-        int n[3] = {0, 0, 0}, pending[3] = {0, 0, 0};
+        int n[N_VARIANTS] = {}, pending[N_VARIANTS] = {};
     };
     std::vector<TuneEntry> tune;
     int ev_tune[2] = {-1, -1}; // tune entry timed by the frame in each event set
