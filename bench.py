@@ -275,7 +275,7 @@ def render_frames(args, dev, stream, rank: int, world: int) -> dict:
     def timed(kernel: int) -> float:
         """ms per frame with the given kernel choice (0: the renderer's own choice by timing)."""
         r.set_kernel(kernel)
-        for _ in range(max(8, args.warmup)):  # covers the timing frames of the kernel choice
+        for _ in range(max(24, args.warmup)):  # covers the tuner's timed frames (2 per variant, up to 8 variants)
             r.RenderScene(sc, reg)
         torch.cuda.synchronize(dev)
         if world > 1:
@@ -416,7 +416,7 @@ def batch_frames(args, dev, stream, n_scenes: int = 64, samples: int = 4) -> dic
 
     by_kernel = {"wavefront": round(timed_batch(1, 1, 0), 3), "wavefront_sorted": round(timed_batch(1, 1, 0x3FF), 3),
                  "path": round(timed_batch(2, 1, 0, reps=1), 3)}
-    batch_ms = timed_batch(0, 7)  # the default: kernel and sort chosen by timing the first calls (2 per variant)
+    batch_ms = timed_batch(0, 20)  # the default: kernel, sort and trace settings chosen by timing the first calls (2 per variant)
     info = rs[0].frame_info()
     if info.error_flags:
         raise RuntimeError(f"batch reported error flags {info.error_flags}")
@@ -487,7 +487,7 @@ def atrium_frames(args, dev, stream, rank: int, world: int) -> dict:
         r.set_kernel(kernel)
         r.set_ray_sort(sort)
         g = api.RegionContext()
-        for _ in range(max(1, args.warmup // 3)):  # 16 RenderScene calls each: covers the timing of the choice
+        for _ in range(max(2, args.warmup // 3)):  # 16 RenderScene calls each: covers the tuner's timed frames
             frame(g)
         torch.cuda.synchronize(dev)
         if world > 1:
@@ -553,6 +553,44 @@ def atrium_frames(args, dev, stream, rank: int, world: int) -> dict:
 
 DIFF_WORKLOAD = ("differentiable form: the atrium (16 displaced icospheres of subdivision 5, 8 materials) at 256x256, 8 samples, max 4 "
                  "bounces; parameters: 512x512 RGB albedo, 8 roughness slots; L2 image loss; path-replay adjoint")
+
+
+def sort_frames(args, dev, stream) -> dict:
+    """The ray sort (ray_sort_rays: get_ray_hash, then the stable one-sweep
+    radix sort of the 32-bit keys, SortRays_CPU's order) on 921,600 rays (one
+    1280x720 wavefront) and 4,194,304 rays, with and without the gather of
+    the ray records; device buffers, CUDA events on the stream."""
+    import ctypes as C
+
+    import torch
+
+    from raydemo_b200 import api, capi, scenes
+
+    r = api.Renderer(16, 16, device=dev.index)
+    L = capi.lib()
+    rm = (C.c_float * 3)(0.0, 0.0, 0.0)
+    cs = (C.c_float * 3)(1 / 255, 1 / 255, 1 / 255)
+    out = {"workload": "ray hash + stable radix sort (+ gather of the 32-byte ray records), rays uniform in the unit cube"}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = max(5, min(args.steps, 50))
+    for n in (921600, 4194304):
+        rays = torch.from_numpy(scenes.incoherent_rays(n, seed=5)).to(dev)
+        perm = torch.empty(n, dtype=torch.int32, device=dev)
+        rout = torch.empty((n, 8), dtype=torch.float32, device=dev)
+        for gather in (False, True):
+            def call():
+                capi.check(L.ray_sort_rays(r.handle, rays.data_ptr(), n, rm, cs, None, perm.data_ptr(),
+                                           rout.data_ptr() if gather else None, stream.cuda_stream))
+            for _ in range(3):
+                call()
+            torch.cuda.synchronize(dev)
+            e0.record(stream)
+            for _ in range(reps):
+                call()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            out[f"us_{n}{'_gather' if gather else ''}"] = round(e0.elapsed_time(e1) / reps * 1e3, 1)
+    return out
 
 
 def diff_frames(args, dev, stream, rank: int, world: int) -> dict:
@@ -755,11 +793,13 @@ def run_gpu_arm(args) -> None:
     from raydemo_b200.api import Renderer
     from raydemo_b200 import scenes
 
-    if args.render_only or args.batch_only or args.atrium_only or args.diff_only:  # one part alone (for profiling)
+    if args.render_only or args.batch_only or args.atrium_only or args.diff_only or args.sort_only:  # one part alone (for profiling)
         stream = torch.cuda.Stream(dev)
         torch.cuda.set_stream(stream)
         args.no_cpu_baseline = True
-        if args.render_only:
+        if args.sort_only:
+            out = {"sort": sort_frames(args, dev, stream)}
+        elif args.render_only:
             out = {"render": render_frames(args, dev, stream, rank, world)}
         elif args.batch_only:
             out = {"batch": batch_frames(args, dev, stream, n_scenes=args.batch_scenes)}
@@ -927,6 +967,7 @@ def run_gpu_arm(args) -> None:
         except FileNotFoundError as e:
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
 
+    sort = sort_frames(args, dev, stream) if rank == 0 and not args.no_sort else None
     render = None if args.no_render else render_frames(args, dev, stream, rank, world)
     batch = None if args.no_batch else batch_frames(args, dev, stream)
     atrium = None if args.no_atrium else atrium_frames(args, dev, stream, rank, world)
@@ -944,7 +985,7 @@ def run_gpu_arm(args) -> None:
                 "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": N_RAYS * 32, "d2h_bytes_per_step": N_RAYS * 16,
                         "matches_device_path": bool(ok)},
                 "parity": parity, "gpu_launches": args.steps * launches_per_step, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "coherent": coherent,
-                "render": render, "batch": batch,
+                "sort": sort, "render": render, "batch": batch,
                 "atrium": atrium, "diff": diffr}
         print(json.dumps(line), flush=True)
     del sc, r
@@ -972,6 +1013,8 @@ def main() -> None:
                     help="samples the oracle renders for the atrium's image check and CPU time (16: the whole frame; 0: none)")
     ap.add_argument("--no-diff", action="store_true", help="skip the differentiable form")
     ap.add_argument("--diff-only", action="store_true", help="only the differentiable form")
+    ap.add_argument("--sort-only", action="store_true", help="only the ray sort")
+    ap.add_argument("--no-sort", action="store_true", help="skip the ray sort measurement")
     ap.add_argument("--diff-steps", type=int, default=200, help="Adam steps of the inverse-rendering run")
     ap.add_argument("--diff-lr-albedo", type=float, default=2e-3)
     ap.add_argument("--diff-lr-rough", type=float, default=1e-2)
