@@ -379,8 +379,8 @@ def batch_frames(args, dev, stream, n_scenes: int = 64, samples: int = 4) -> dic
     plain_ms, plain_imgs, kernels = None, None, []
     if not args.batch_no_plain:
         # warm-up: the plain loop twice (each renderer times both kernels on its first frames)
-        plain_pass()
-        plain_pass()
+        for _ in range(6):  # 24 frames per renderer: past its tuner's timed frames (2 per variant)
+            plain_pass()
         plain_ms = float("inf")
         for _ in range(3):  # the best of three, as for the batch
             torch.cuda.synchronize(dev)
