@@ -460,7 +460,12 @@ int ray_render_batch(ray_renderer *const *renderers, ray_scene *const *scenes, r
  * the roughness that direction sampling, pdfs and MIS weights take instead
  * of `roughness` -- frozen sampling, under which the rendered estimator is a
  * smooth function of the roughness and its derivative is exactly what the
- * adjoint computes (for checking it by finite differences). */
+ * adjoint computes (for checking it by finite differences).
+ * The reference's RAY_MAT_DIFFUSE materials may have slots too: such a
+ * material takes its Oren-Nayar roughness (sigma) from the slot and, when
+ * color (device, n_roughness x 3; may be NULL) is given, its main colour from
+ * color[3 * slot ..] (its main texture stays as it is). With no
+ * RAY_MAT_PRINCIPLED material in a slot the albedo texture may be NULL. */
 typedef struct ray_diff_params {
     const float *albedo;
     int albedo_w, albedo_h;
@@ -469,6 +474,7 @@ typedef struct ray_diff_params {
     const int32_t *material_slot;
     int n_materials;
     const float *roughness_sampling;
+    const float *color;
 } ray_diff_params;
 int ray_scene_set_diff_params(ray_scene *s, const ray_diff_params *p);
 /* Forward pass: samples iterations first_iteration .. first_iteration +
@@ -482,10 +488,20 @@ int ray_render_diff(ray_renderer *r, ray_scene *s, int first_iteration, int samp
  * dLoss/dalbedo to grad_albedo (device, albedo_h x albedo_w x 3) and
  * dLoss/droughness to grad_roughness (device, n_roughness), given d_image
  * (device, h x w x 3) = dLoss/dimage_rgb. Sampling is detached (pdfs and MIS
- * weights held constant). Scenes: RAY_MAT_PRINCIPLED materials, quad and sun
- * lights only (RAY_ERR_UNSUPPORTED otherwise). */
+ * weights held constant). Scenes: RAY_MAT_PRINCIPLED, RAY_MAT_DIFFUSE and
+ * RAY_MAT_EMISSIVE materials; quad and sun lights, and the reference's point,
+ * spot and directional lights (their shadow rays traced again in the
+ * adjoint); RAY_ERR_UNSUPPORTED otherwise. grad_albedo may be NULL when the
+ * scene has no albedo texture. Russian roulette is not differentiated: give
+ * the camera a termination depth at or past its bounce limit for exact
+ * gradients. */
 int ray_render_adjoint(ray_renderer *r, ray_scene *s, int first_iteration, int samples, const float *sample_rgb, const float *d_image,
                        float *grad_albedo, float *grad_roughness);
+/* The same, also adding dLoss/d(main colour) of the RAY_MAT_DIFFUSE slots to
+ * grad_color (device, n_roughness x 3; may be NULL) -- the colours that
+ * ray_diff_params::color supplies. */
+int ray_render_adjoint_color(ray_renderer *r, ray_scene *s, int first_iteration, int samples, const float *sample_rgb,
+                             const float *d_image, float *grad_albedo, float *grad_roughness, float *grad_color);
 
 /* The CUDA stream the renderer enqueues its work on from now on (a
  * cudaStream_t; NULL: the renderer's own stream). No counterpart in the

@@ -204,11 +204,13 @@ class Scene:
         check(lib().ray_scene_set_current_cam(self._h, i))
 
     def set_diff_params(self, albedo_ptr: int, albedo_w: int, albedo_h: int, roughness_ptr: int, n_roughness: int,
-                        material_slot=None, roughness_sampling_ptr: int = 0) -> None:
+                        material_slot=None, roughness_sampling_ptr: int = 0, color_ptr: int = 0) -> None:
         """Differentiable parameters (ray_scene_set_diff_params): device pointers
-        to a float RGB albedo texture (albedo_h x albedo_w x 3) and n_roughness
-        slots; material_slot: per material its slot or -1 (None: no slots);
-        roughness_sampling_ptr: frozen roughness for sampling (0: none)."""
+        to a float RGB albedo texture (albedo_h x albedo_w x 3; 0 for none when
+        no RAY_MAT_PRINCIPLED material has a slot) and n_roughness slots;
+        material_slot: per material its slot or -1 (None: no slots);
+        roughness_sampling_ptr: frozen roughness for sampling (0: none);
+        color_ptr: the RAY_MAT_DIFFUSE slots' main colours (n_roughness x 3; 0: none)."""
         if albedo_ptr is None:
             check(lib().ray_scene_set_diff_params(self._h, None))
             return
@@ -217,8 +219,9 @@ class Scene:
         if material_slot is not None:
             n = len(material_slot)
             slots = (C.c_int32 * max(n, 1))(*[int(k) for k in material_slot])
-        p = capi.DiffParams(albedo_ptr, albedo_w, albedo_h, roughness_ptr, n_roughness,
-                            C.cast(slots, C.POINTER(C.c_int32)) if slots is not None else None, n, roughness_sampling_ptr or None)
+        p = capi.DiffParams(albedo_ptr or None, albedo_w, albedo_h, roughness_ptr, n_roughness,
+                            C.cast(slots, C.POINTER(C.c_int32)) if slots is not None else None, n, roughness_sampling_ptr or None,
+                            color_ptr or None)
         check(lib().ray_scene_set_diff_params(self._h, C.byref(p)))
 
     def triangle_count(self) -> int:
@@ -354,10 +357,11 @@ class Renderer:
         check(lib().ray_render_diff(self._h, scene.handle, first_iteration, samples, image_ptr, sample_ptr))
 
     def render_adjoint(self, scene: Scene, first_iteration: int, samples: int, sample_ptr: int, d_image_ptr: int, grad_albedo_ptr: int,
-                       grad_rough_ptr: int) -> None:
-        """Path-replay adjoint (ray_render_adjoint): accumulates the gradients."""
-        check(lib().ray_render_adjoint(self._h, scene.handle, first_iteration, samples, sample_ptr, d_image_ptr, grad_albedo_ptr,
-                                       grad_rough_ptr))
+                       grad_rough_ptr: int, grad_color_ptr: int = 0) -> None:
+        """Path-replay adjoint (ray_render_adjoint_color): accumulates the
+        gradients (albedo texture, roughness slots, diffuse slots' colours)."""
+        check(lib().ray_render_adjoint_color(self._h, scene.handle, first_iteration, samples, sample_ptr, d_image_ptr,
+                                             grad_albedo_ptr or None, grad_rough_ptr, grad_color_ptr or None))
 
     def RenderScene(self, scene: Scene, region: capi.Region) -> None:
         check(lib().ray_render(self._h, scene.handle, C.byref(region)))

@@ -103,7 +103,8 @@ class FrameInfo(C.Structure):
 
 class DiffParams(C.Structure):
     _fields_ = [("albedo", C.c_void_p), ("albedo_w", C.c_int), ("albedo_h", C.c_int), ("roughness", C.c_void_p), ("n_roughness", C.c_int),
-                ("material_slot", C.POINTER(C.c_int32)), ("n_materials", C.c_int), ("roughness_sampling", C.c_void_p)]
+                ("material_slot", C.POINTER(C.c_int32)), ("n_materials", C.c_int), ("roughness_sampling", C.c_void_p),
+                ("color", C.c_void_p)]
 
 
 class TraceTuning(C.Structure):
@@ -184,6 +185,7 @@ _SIGS = {
     "ray_scene_set_diff_params": ([_P, C.POINTER(DiffParams)], C.c_int),
     "ray_render_diff": ([_P, _P, C.c_int, C.c_int, _P, _P], C.c_int),
     "ray_render_adjoint": ([_P, _P, C.c_int, C.c_int, _P, _P, _P, _P], C.c_int),
+    "ray_render_adjoint_color": ([_P, _P, C.c_int, C.c_int, _P, _P, _P, _P, _P], C.c_int),
     "ray_render_batch": ([C.POINTER(_P), C.POINTER(_P), C.POINTER(C.POINTER(Region)), C.c_int, C.c_int], C.c_int),
     "ray_sort_rays": ([_P, _P, C.c_uint64, C.POINTER(C.c_float), C.POINTER(C.c_float), _P, _P, _P, _P], C.c_int),
     "ray_sort_rays_noalloc": ([_P, C.c_uint64, C.POINTER(C.c_float), C.POINTER(C.c_float), _P, _P, _P, _P], C.c_int),

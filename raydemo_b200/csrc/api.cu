@@ -607,27 +607,34 @@ int ray_scene_set_diff_params(ray_scene *s, const ray_diff_params *p) {
     RG_API_LOCK;
     RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s, "null scene");
+    auto slotted = [](const MaterialRec &m) { return m.type == (uint32_t)RAY_MAT_PRINCIPLED || m.type == (uint32_t)RAY_MAT_DIFFUSE; };
     if (!p) {
         for (MaterialRec &m : s->materials)
-            if (m.type == (uint32_t)RAY_MAT_PRINCIPLED) m.textures[2] = RAY_INVALID_INDEX;
-        s->diff_albedo = s->diff_rough = s->diff_rough_sampling = nullptr;
+            if (slotted(m) && m.textures[2] != RAY_INVALID_INDEX) {
+                m.textures[2] = RAY_INVALID_INDEX;
+                s->shade_dirty = true;
+            }
+        s->diff_albedo = s->diff_rough = s->diff_rough_sampling = s->diff_color = nullptr;
         s->diff_aw = s->diff_ah = s->n_diff_rough = 0;
         s->shade_dirty = true;
         return RAY_OK;
     }
-    RG_CHECK(p->albedo && p->roughness && p->albedo_w > 0 && p->albedo_h > 0, "albedo and roughness arrays are required");
+    RG_CHECK(p->roughness, "the roughness array is required");
+    RG_CHECK(!p->albedo || (p->albedo_w > 0 && p->albedo_h > 0), "albedo size");
     RG_CHECK(p->n_roughness > 0 && p->n_roughness <= 64, "1 to 64 roughness slots");
     RG_CHECK(!p->material_slot || p->n_materials == (int)s->materials.size(), "one slot entry per material of the scene");
     if (p->material_slot)
         for (size_t m = 0; m < s->materials.size(); m++) {
             const int32_t k = p->material_slot[m];
             RG_CHECK(k >= -1 && k < p->n_roughness, "material slot out of range");
-            RG_CHECK(k < 0 || s->materials[m].type == (uint32_t)RAY_MAT_PRINCIPLED, "slots are for RAY_MAT_PRINCIPLED materials");
+            RG_CHECK(k < 0 || slotted(s->materials[m]), "slots are for RAY_MAT_PRINCIPLED and RAY_MAT_DIFFUSE materials");
+            RG_CHECK(k < 0 || s->materials[m].type != (uint32_t)RAY_MAT_PRINCIPLED || p->albedo,
+                     "a RAY_MAT_PRINCIPLED material in a slot needs the albedo texture");
         }
     // the slots live in the device material records: upload only when one changes
     // (the parameter arrays themselves are read through the pointers at each render)
     for (size_t m = 0; m < s->materials.size(); m++) {
-        if (s->materials[m].type != (uint32_t)RAY_MAT_PRINCIPLED) continue;
+        if (!slotted(s->materials[m])) continue;
         const int32_t k = p->material_slot ? p->material_slot[m] : -1;
         const uint32_t v = k >= 0 ? (uint32_t)k : RAY_INVALID_INDEX;
         if (s->materials[m].textures[2] != v) {
@@ -638,8 +645,9 @@ int ray_scene_set_diff_params(ray_scene *s, const ray_diff_params *p) {
     s->diff_albedo = p->albedo;
     s->diff_rough = p->roughness;
     s->diff_rough_sampling = p->roughness_sampling;
-    s->diff_aw = p->albedo_w;
-    s->diff_ah = p->albedo_h;
+    s->diff_color = p->color;
+    s->diff_aw = p->albedo ? p->albedo_w : 0;
+    s->diff_ah = p->albedo ? p->albedo_h : 0;
     s->n_diff_rough = p->n_roughness;
     return RAY_OK;
 }

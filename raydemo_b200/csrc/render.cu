@@ -625,7 +625,7 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
             if (e != cudaSuccess) return e;
             if (adj)
                 e = launch_adjoint_shade(d_jobs, b, rays[in], pay[in], job[in], adj->state[in], hits, obj, cnt + in, total, rays[out], pay[out],
-                                         job[out], adj->state[out], cnt + out, shadow, adj->args, err, st);
+                                         job[out], adj->state[out], cnt + out, shadow, adj->args, err, st, ref_lights);
             else
                 e = launch_shade_jobs(d_jobs, sample, b, rays[in], pay[in], job[in], hits, obj, cnt + in, total, rays[out], pay[out], job[out],
                                       cnt + out, shadow, ref_lights, err, ray_stats, st);
@@ -1063,25 +1063,30 @@ int ray_render_diff(ray_renderer *r, ray_scene *s, int first_iteration, int samp
 
 int ray_render_adjoint(ray_renderer *r, ray_scene *s, int first_iteration, int samples, const float *sample_rgb, const float *d_image,
                        float *grad_albedo, float *grad_roughness) {
+    return ray_render_adjoint_color(r, s, first_iteration, samples, sample_rgb, d_image, grad_albedo, grad_roughness, nullptr);
+}
+
+int ray_render_adjoint_color(ray_renderer *r, ray_scene *s, int first_iteration, int samples, const float *sample_rgb,
+                             const float *d_image, float *grad_albedo, float *grad_roughness, float *grad_color) {
     RG_API_LOCK;
     RG_CHECK(!r || live_renderer(r), "unknown or destroyed renderer handle");
     RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     try {
-        if (!r || !s || !sample_rgb || !d_image || !grad_albedo || !grad_roughness) {
+        if (!r || !s || !sample_rgb || !d_image || !grad_roughness) {
             set_error("null argument");
             return RAY_ERR_INVALID_ARG;
         }
-        if (!s->diff_albedo || !s->diff_rough) {
+        if (!s->diff_rough) {
             set_error("the scene has no differentiable parameters (ray_scene_set_diff_params)");
             return RAY_ERR_INVALID_ARG;
         }
-        if (!s->lights.empty()) {
-            set_error("the adjoint takes scenes lit by quad and sun lights only");
-            return RAY_ERR_UNSUPPORTED;
+        if (s->diff_albedo && !grad_albedo) {
+            set_error("the scene has an albedo texture: grad_albedo is required");
+            return RAY_ERR_INVALID_ARG;
         }
         for (const MaterialRec &m : s->materials)
-            if (m.type != (uint32_t)RAY_MAT_PRINCIPLED) {
-                set_error("the adjoint takes scenes of RAY_MAT_PRINCIPLED materials only");
+            if (m.type != (uint32_t)RAY_MAT_PRINCIPLED && m.type != (uint32_t)RAY_MAT_DIFFUSE && m.type != (uint32_t)RAY_MAT_EMISSIVE) {
+                set_error("the adjoint takes scenes of RAY_MAT_PRINCIPLED, RAY_MAT_DIFFUSE and RAY_MAT_EMISSIVE materials only");
                 return RAY_ERR_UNSUPPORTED;
             }
         std::vector<FrameJob> jobs;
@@ -1096,6 +1101,7 @@ int ray_render_adjoint(ray_renderer *r, ray_scene *s, int first_iteration, int s
         adj.args.d_image = d_image;
         adj.args.grad_albedo = grad_albedo;
         adj.args.grad_rough = grad_roughness;
+        adj.args.grad_color = grad_color;
         adj.args.inv_spp = 1.0f / (float)samples;
         adj.state[0] = static_cast<AdjState *>(r->d_adj[0].p);
         adj.state[1] = static_cast<AdjState *>(r->d_adj[1].p);

@@ -92,6 +92,10 @@ struct RenderScene {
     const float *diff_rough;
     const float *diff_rough_sampling; // null: sampling and pdfs take diff_rough too
     uint32_t diff_aw, diff_ah, n_diff_rough;
+    // a RAY_MAT_DIFFUSE material whose textures[2] holds a slot takes its
+    // Oren-Nayar roughness from diff_rough and, when diff_color is set, its
+    // main colour from diff_color (3 floats per slot)
+    const float *diff_color;
 };
 
 // pass_settings_t flags (src/Ray/Types.h:39-45)
@@ -227,8 +231,12 @@ static_assert(sizeof(AdjShadowRec) == 80, "AdjShadowRec layout");
 struct AdjArgs {
     const float *sample_rgb, *d_image;
     float *grad_albedo, *grad_rough;
+    float *grad_color; // RAY_MAT_DIFFUSE slots' main colours (3 per slot), may be null
     float inv_spp;
 };
+// AdjState::slot / AdjShadowRec::slot: a RAY_MAT_DIFFUSE vertex's slot
+// carries this flag (its colour gradient goes to grad_color, not to texels).
+constexpr uint32_t ADJ_DIFFUSE_SLOT = 0x40000000u;
 
 // Launchers (render_kernels.cu). All stream-ordered; counts live on the device.
 cudaError_t launch_halton_table(const uint16_t *perms, int base_iteration, float *table, cudaStream_t st);
@@ -281,7 +289,7 @@ cudaError_t launch_diff_collect(const FrameJob *jobs, int n_jobs, uint32_t n_pix
 cudaError_t launch_adjoint_shade(const FrameJob *jobs, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
                                  const AdjState *adj_in, const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays,
                                  float4 *out_rays, RayPayload *out_pay, uint32_t *out_job, AdjState *adj_out, uint32_t *out_count,
-                                 const ShadowQueue &shadow, const AdjArgs &args, uint32_t *err, cudaStream_t st);
+                                 const ShadowQueue &shadow, const AdjArgs &args, uint32_t *err, cudaStream_t st, bool ref_lights);
 cudaError_t launch_adjoint_shadow_apply(const FrameJob *jobs, int bounce, const ShadowQueue &shadow, const float4 *hits, uint32_t max_recs,
                                         AdjState *adj_cont, const AdjArgs &args, uint32_t *err, cudaStream_t st);
 cudaError_t launch_fill(float4 *buf, size_t n, float4 v, cudaStream_t st);

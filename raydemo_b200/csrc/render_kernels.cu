@@ -260,9 +260,10 @@ __device__ float compute_visibility(const RenderScene &sc, V3 p1, V3 p2, const f
 }
 
 // AcumulateLightContribution, CoreRef.cpp:1898-1933
+// dcol (may be null): also adds the contribution's derivative by sigma.
 __device__ __forceinline__ void accumulate_light(const RenderScene &sc, const LightRec &l, V3 I, V3 P, V3 N, V3 B, V3 plane_N, float sigma,
                                                  const float *halton, int hi, int rand_hash2, float rand_offset, float rand_offset2, V3 &col,
-                                                 Stack<true> &st, uint32_t &err, uint32_t &nshadow) {
+                                                 Stack<true> &st, uint32_t &err, uint32_t &nshadow, V3 *dcol = nullptr) {
     const V3 lpos = v3(l.pos);
     V3 L = P - lpos;
     const float distance = length(L);
@@ -284,7 +285,14 @@ __device__ __forceinline__ void accumulate_light(const RenderScene &sc, const Li
     const float dot2 = dot(L, v3(l.dir));
     if (dot1 > FLT_EPS_ && dot2 > l.spot && (l.brightness * atten) > FLT_EPS_) {
         const float visibility = compute_visibility(sc, P + HIT_BIAS * plane_N, lpos, halton, hi, rand_hash2, st, err, nshadow);
-        col = col + v3(l.col) * dot1 * visibility * atten * brdf_oren_nayar(L, I, N, B, sigma);
+        if (dcol) {
+            float d_sigma = 0.0f;
+            const float on = brdf_oren_nayar_d(L, I, N, B, sigma, d_sigma);
+            col = col + v3(l.col) * dot1 * visibility * atten * on;
+            *dcol = *dcol + v3(l.col) * dot1 * visibility * atten * d_sigma;
+        } else {
+            col = col + v3(l.col) * dot1 * visibility * atten * brdf_oren_nayar(L, I, N, B, sigma);
+        }
     }
 }
 
@@ -329,6 +337,14 @@ struct VertexGrad {
     V3 main_color, wo_l, wl_l, le_s, wi_l;
     ggx::Params prm;
     float metallic;
+    // a RAY_MAT_DIFFUSE vertex (diffuse set): its texture colour (the albedo
+    // before main_color), the direct light it adds before the albedo and that
+    // light's derivative by the roughness, whether the albedo multiplies them
+    // (not on the camera rays of a lighting-only pass), and the continuation
+    // weight's d(Oren-Nayar)/d(roughness) over Oren-Nayar
+    bool diffuse, albedo_on;
+    V3 tex, direct, d_direct;
+    float cont_g;
 };
 
 // Russian roulette and emission of a continuation ray (CoreRef.cpp:2246-2256)
@@ -361,7 +377,7 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
                         uint32_t &err, uint32_t &nshadow, VertexGrad *vg = nullptr) {
     emit = false;
     sr.valid = false;
-    if (vg) vg->valid = false;
+    if (vg) vg->valid = vg->diffuse = false;
     const int prim = __float_as_int(hit.x);
     const V3 I = v3(r1.x, r1.y, r1.z);
     const uint32_t xy = __float_as_uint(r1.w);
@@ -462,6 +478,7 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
 
     // the reference's materials: normal map and main texture (RAY_MAT_PRINCIPLED reads neither)
     V3 B = v3(0.0f, 0.0f, 0.0f), T = v3(0.0f, 0.0f, 0.0f), alb = v3(0.0f, 0.0f, 0.0f);
+    float sigma_d = mat.roughness_or_strength; // the diffuse material's Oren-Nayar roughness
     if (mat.type != (uint32_t)RAY_MAT_PRINCIPLED) {
         B = v3(v1.b) * w + v3(v2.b) * hu + v3(v3v.b) * hv;
         T = cross(B, N);
@@ -478,9 +495,24 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
         const float albedo_lod = texture_lod(sc, main_tex, der.duv_dx[0], der.duv_dx[1], der.duv_dy[0], der.duv_dy[1]);
         F4 albedo = sample_bilinear(sc, main_tex, uvx, uvy, f2i_x86(albedo_lod));
         if (main_tex < sc.n_textures && (sc.textures[main_tex].width & 0x8000u)) albedo = srgb_to_rgb(albedo);
-        albedo.x *= mat.main_color[0];
-        albedo.y *= mat.main_color[1];
-        albedo.z *= mat.main_color[2];
+        // a differentiable diffuse material: main colour and roughness from its slot
+        const uint32_t dslot = mat.type == (uint32_t)RAY_MAT_DIFFUSE ? mat.textures[2] : RAY_INVALID_INDEX;
+        const bool dparam = dslot < sc.n_diff_rough && sc.diff_rough;
+        const V3 mc = (dparam && sc.diff_color) ? v3(sc.diff_color[3 * dslot], sc.diff_color[3 * dslot + 1], sc.diff_color[3 * dslot + 2])
+                                                : v3(mat.main_color);
+        if (dparam) sigma_d = sc.diff_rough[dslot];
+        if (vg && dparam) {
+            vg->diffuse = true;
+            vg->slot = dslot;
+            vg->tex = v3(albedo.x, albedo.y, albedo.z);
+            vg->main_color = mc;
+            vg->direct = vg->d_direct = v3(0.0f, 0.0f, 0.0f);
+            vg->cont = false;
+            vg->cont_g = 0.0f;
+        }
+        albedo.x *= mc.x;
+        albedo.y *= mc.y;
+        albedo.z *= mc.z;
         alb = v3(albedo.x, albedo.y, albedo.z);
     }
 
@@ -497,11 +529,14 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
     const float dot_I_pN = dot(I, plane_N);
 
     if (mat.type == (uint32_t)RAY_MAT_DIFFUSE) {
+        const bool dgrad = vg && vg->diffuse;
+        if (dgrad) vg->albedo_on = consider_albedo;
         if (!(pi.flags & PASS_SKIP_DIRECT) || pi.bounce > 2) {
             if (REF_LIGHTS)
                 for (uint32_t li = 0; li < sc.n_lights; li++)
-                    accumulate_light(sc, sc.lights[li], I, P, N, B, plane_N, mat.roughness_or_strength, halton, hi, rand_hash2, rand_offset,
-                                     rand_offset2, col, st, err, nshadow);
+                    accumulate_light(sc, sc.lights[li], I, P, N, B, plane_N, sigma_d, halton, hi, rand_hash2, rand_offset, rand_offset2, col, st,
+                                     err, nshadow, dgrad ? &vg->d_direct : nullptr);
+            if (dgrad) vg->direct = col;
             if (consider_albedo) col = col * alb;
         }
         if (diff_depth < pi.max_diff_depth && total_depth < pi.max_total_depth) {
@@ -519,7 +554,14 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
                 const float dir = sqrtf(u1);
                 V = (dir * sin_phi) * B + sqrtf(1.0f - u1) * N + (dir * cos_phi) * T;
             }
-            weight *= brdf_oren_nayar(V, I, N, B, mat.roughness_or_strength);
+            if (dgrad) {
+                float d_sigma = 0.0f;
+                const float on = brdf_oren_nayar_d(V, I, N, B, sigma_d, d_sigma);
+                weight *= on;
+                vg->cont_g = on > 0.0f ? d_sigma / on : 0.0f;
+            } else {
+                weight *= brdf_oren_nayar(V, I, N, B, sigma_d);
+            }
             nr.p.ray_depth = ray.ray_depth + 0x00000001;
             const V3 o = P + HIT_BIAS * plane_N;
             nr.r0 = make_float4(o.x, o.y, o.z, MAX_DIST);
@@ -537,6 +579,7 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
             set3(nr.p.dd_dx, der.dd_dx - 2 * (dot_I_pN * der.dndx + der.ddn_dx * plane_N));
             set3(nr.p.dd_dy, der.dd_dy - 2 * (dot_I_pN * der.dndy + der.ddn_dy * plane_N));
             emit = roulette(nr, cant_terminate, frac_modf(halton[hi + 0] + rand_offset3));
+            if (dgrad) vg->cont = emit;
         }
     } else if (mat.type == (uint32_t)RAY_MAT_GLOSSY) {
         if (gloss_depth < pi.max_glossy_depth && total_depth < pi.max_total_depth) {
@@ -1376,7 +1419,9 @@ __device__ __forceinline__ void flush_slots(float *s_gr, float *grad_rough, uint
         if (s_gr[k] != 0.0f) atomicAdd(grad_rough + k, s_gr[k]);
 }
 
-template <bool PRIMARY>
+// REF_LIGHTS: the scene has the reference's point/spot/directional lights
+// (the replayed shading traces their shadow rays again, as the forward did).
+template <bool PRIMARY, bool REF_LIGHTS>
 __global__ void __launch_bounds__(SHADE_BLOCK, 3) k_adjoint_shade(const FrameJob *__restrict__ jobs, int bounce,
                                                                   const float4 *__restrict__ rays, const RayPayload *__restrict__ pay,
                                                                   const uint32_t *__restrict__ ray_job, const AdjState *__restrict__ adj_in,
@@ -1387,11 +1432,13 @@ __global__ void __launch_bounds__(SHADE_BLOCK, 3) k_adjoint_shade(const FrameJob
                                                                   uint32_t *__restrict__ out_count, ShadowQueue shadow, AdjArgs args,
                                                                   uint32_t *__restrict__ err_out) {
     __shared__ float s_gr[ADJ_MAX_SLOTS];
-    __shared__ uint2 s_stack[1];
+    __shared__ float s_gc[3 * ADJ_MAX_SLOTS]; // the diffuse slots' colour gradients
+    __shared__ uint2 s_stack[REF_LIGHTS ? trav::SMEM_STACK * SHADE_BLOCK : 1];
     for (int k = threadIdx.x; k < ADJ_MAX_SLOTS; k += blockDim.x) s_gr[k] = 0.0f;
+    for (int k = threadIdx.x; k < 3 * ADJ_MAX_SLOTS; k += blockDim.x) s_gc[k] = 0.0f;
     __syncthreads();
     Stack<true> st;
-    st.smem = s_stack;
+    st.smem = s_stack + (REF_LIGHTS ? threadIdx.x : 0);
     st.sp = 0;
     uint32_t err = 0, nshadow = 0;
     const uint32_t n = min(*in_count, max_rays);
@@ -1424,12 +1471,20 @@ __global__ void __launch_bounds__(SHADE_BLOCK, 3) k_adjoint_shade(const FrameJob
                 a0 = in.a[0];
                 a1 = in.a[1];
                 a2 = in.a[2];
-                if (in.slot < n_slots) { // the previous vertex's continuation: R = radiance - sum so far
+                const uint32_t in_slot = in.slot & ~ADJ_DIFFUSE_SLOT;
+                if (in.slot != RAY_INVALID_INDEX && in_slot < n_slots) { // the previous vertex's continuation: R = radiance - sum so far
                     const float R0 = args.sample_rgb[3 * px + 0] - a0, R1 = args.sample_rgb[3 * px + 1] - a1,
                                 R2 = args.sample_rgb[3 * px + 2] - a2;
-                    scatter_albedo(sc, args.grad_albedo, in.u, in.v, d0 * R0 * in.ga[0], d1 * R1 * in.ga[1], d2 * R2 * in.ga[2]);
+                    if (in.slot & ADJ_DIFFUSE_SLOT) { // a diffuse slot's main colour
+                        const float g0 = d0 * R0 * in.ga[0], g1 = d1 * R1 * in.ga[1], g2 = d2 * R2 * in.ga[2];
+                        if (g0 != 0.0f) atomicAdd(&s_gc[3 * in_slot + 0], g0);
+                        if (g1 != 0.0f) atomicAdd(&s_gc[3 * in_slot + 1], g1);
+                        if (g2 != 0.0f) atomicAdd(&s_gc[3 * in_slot + 2], g2);
+                    } else {
+                        scatter_albedo(sc, args.grad_albedo, in.u, in.v, d0 * R0 * in.ga[0], d1 * R1 * in.ga[1], d2 * R2 * in.ga[2]);
+                    }
                     const float g = d0 * R0 * in.gr[0] + d1 * R1 * in.gr[1] + d2 * R2 * in.gr[2];
-                    if (g != 0.0f) atomicAdd(&s_gr[in.slot], g);
+                    if (g != 0.0f) atomicAdd(&s_gr[in_slot], g);
                 }
             }
             PassInfo pi = J.pi;
@@ -1437,7 +1492,8 @@ __global__ void __launch_bounds__(SHADE_BLOCK, 3) k_adjoint_shade(const FrameJob
             const int rand_index = (pi.flags & PASS_COHERENT) ? c_sampling_pattern[(y % 8) * 8 + (x % 8)] : index;
             bool emit = false;
             VertexGrad vg;
-            const F4 c = shade_surface<false>(sc, pi, rand_index, J.halton, hits[i], obj[i], r0, r1, p, nr, emit, sr, st, err, nshadow, &vg);
+            const F4 c = shade_surface<REF_LIGHTS>(sc, pi, rand_index, J.halton, hits[i], obj[i], r0, r1, p, nr, emit, sr, st, err, nshadow,
+                                                   &vg);
             // the sum as the sample buffer takes it (SetPixel on camera rays, AddPixel after)
             if (PRIMARY) {
                 a0 = c.x;
@@ -1469,6 +1525,28 @@ __global__ void __launch_bounds__(SHADE_BLOCK, 3) k_adjoint_shade(const FrameJob
                 out.gr[0] = safe_ratio(dfa.x, f.x) * dadr;
                 out.gr[1] = safe_ratio(dfa.y, f.y) * dadr;
                 out.gr[2] = safe_ratio(dfa.z, f.z) * dadr;
+            }
+            if (vg.diffuse && vg.slot < n_slots) {
+                // a diffuse vertex: the direct light it added (ray.c x direct x albedo) ...
+                const float pc0 = d0 * p.c[0], pc1 = d1 * p.c[1], pc2 = d2 * p.c[2];
+                const V3 alb = vg.albedo_on ? v3(vg.tex.x * vg.main_color.x, vg.tex.y * vg.main_color.y, vg.tex.z * vg.main_color.z)
+                                            : v3(1.0f, 1.0f, 1.0f);
+                if (vg.albedo_on) {
+                    const float g0 = pc0 * vg.direct.x * vg.tex.x, g1 = pc1 * vg.direct.y * vg.tex.y, g2 = pc2 * vg.direct.z * vg.tex.z;
+                    if (g0 != 0.0f) atomicAdd(&s_gc[3 * vg.slot + 0], g0);
+                    if (g1 != 0.0f) atomicAdd(&s_gc[3 * vg.slot + 1], g1);
+                    if (g2 != 0.0f) atomicAdd(&s_gc[3 * vg.slot + 2], g2);
+                }
+                const float gs = pc0 * vg.d_direct.x * alb.x + pc1 * vg.d_direct.y * alb.y + pc2 * vg.d_direct.z * alb.z;
+                if (gs != 0.0f) atomicAdd(&s_gr[vg.slot], gs);
+                // ... and its continuation, settled at the next vertex: weight = Oren-Nayar x albedo
+                if (append && vg.cont) {
+                    out.slot = vg.slot | ADJ_DIFFUSE_SLOT;
+                    out.ga[0] = vg.albedo_on && vg.main_color.x != 0.0f ? 1.0f / vg.main_color.x : 0.0f;
+                    out.ga[1] = vg.albedo_on && vg.main_color.y != 0.0f ? 1.0f / vg.main_color.y : 0.0f;
+                    out.ga[2] = vg.albedo_on && vg.main_color.z != 0.0f ? 1.0f / vg.main_color.z : 0.0f;
+                    out.gr[0] = out.gr[1] = out.gr[2] = vg.cont_g;
+                }
             }
             if (sr.valid) {
                 light = true;
@@ -1531,6 +1609,9 @@ __global__ void __launch_bounds__(SHADE_BLOCK, 3) k_adjoint_shade(const FrameJob
     }
     if (err) atomicOr(err_out, err);
     flush_slots(s_gr, args.grad_rough, n_slots);
+    if (args.grad_color)
+        for (uint32_t k = threadIdx.x; k < 3 * n_slots; k += blockDim.x)
+            if (s_gc[k] != 0.0f) atomicAdd(args.grad_color + k, s_gc[k]);
 }
 
 __global__ void __launch_bounds__(SHADE_BLOCK) k_adjoint_shadow_apply(const FrameJob *__restrict__ jobs, int bounce, ShadowQueue q,
@@ -1700,17 +1781,24 @@ cudaError_t launch_diff_collect(const FrameJob *jobs, int n_jobs, uint32_t n_pix
 cudaError_t launch_adjoint_shade(const FrameJob *jobs, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
                                  const AdjState *adj_in, const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays,
                                  float4 *out_rays, RayPayload *out_pay, uint32_t *out_job, AdjState *adj_out, uint32_t *out_count,
-                                 const ShadowQueue &shadow, const AdjArgs &args, uint32_t *err, cudaStream_t st) {
-    static int resident = 0;
-    if (resident == 0) resident = resident_blocks(k_adjoint_shade<false>, 3);
+                                 const ShadowQueue &shadow, const AdjArgs &args, uint32_t *err, cudaStream_t st, bool ref_lights) {
+    static int resident[2] = {0, 0};
+    if (resident[0] == 0) resident[0] = resident_blocks(k_adjoint_shade<false, false>, 3);
+    if (resident[1] == 0) resident[1] = resident_blocks(k_adjoint_shade<false, true>, 3);
+    const int res = resident[ref_lights ? 1 : 0];
     const uint32_t need = (max_rays + SHADE_BLOCK - 1) / SHADE_BLOCK;
-    const uint32_t blocks = need < (uint32_t)resident ? (need > 0 ? need : 1) : (uint32_t)resident;
-    if (bounce == 2)
-        k_adjoint_shade<true><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, bounce, rays, pay, ray_job, adj_in, hits, obj, in_count, max_rays, out_rays,
-                                                              out_pay, out_job, adj_out, out_count, shadow, args, err);
-    else
-        k_adjoint_shade<false><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, bounce, rays, pay, ray_job, adj_in, hits, obj, in_count, max_rays,
-                                                               out_rays, out_pay, out_job, adj_out, out_count, shadow, args, err);
+    const uint32_t blocks = need < (uint32_t)res ? (need > 0 ? need : 1) : (uint32_t)res;
+#define RG_ADJ(P, L)                                                                                                                    \
+    k_adjoint_shade<P, L><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, bounce, rays, pay, ray_job, adj_in, hits, obj, in_count, max_rays, out_rays, \
+                                                          out_pay, out_job, adj_out, out_count, shadow, args, err)
+    if (bounce == 2) {
+        if (ref_lights) RG_ADJ(true, true);
+        else RG_ADJ(true, false);
+    } else {
+        if (ref_lights) RG_ADJ(false, true);
+        else RG_ADJ(false, false);
+    }
+#undef RG_ADJ
     return cudaGetLastError();
 }
 

@@ -130,7 +130,7 @@ struct ray_scene {
     uint32_t total_tris = 0, total_nodes = 0, max_depth = 0;
     float world_min[3] = {0.0f, 0.0f, 0.0f}, world_max[3] = {0.0f, 0.0f, 0.0f}; // union of the instance boxes
     // differentiable parameters (caller-owned device arrays, ray_scene_set_diff_params)
-    const float *diff_albedo = nullptr, *diff_rough = nullptr, *diff_rough_sampling = nullptr;
+    const float *diff_albedo = nullptr, *diff_rough = nullptr, *diff_rough_sampling = nullptr, *diff_color = nullptr;
     int diff_aw = 0, diff_ah = 0, n_diff_rough = 0;
 
     // device arrays assembled at commit

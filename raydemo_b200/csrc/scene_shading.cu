@@ -363,6 +363,7 @@ RenderScene render_scene_view(const ray_scene *s) {
     r.diff_albedo = s->diff_albedo;
     r.diff_rough = s->diff_rough;
     r.diff_rough_sampling = s->diff_rough_sampling;
+    r.diff_color = s->diff_color;
     r.diff_aw = (uint32_t)s->diff_aw;
     r.diff_ah = (uint32_t)s->diff_ah;
     r.n_diff_rough = (uint32_t)s->n_diff_rough;

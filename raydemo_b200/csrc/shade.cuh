@@ -233,6 +233,39 @@ __device__ __forceinline__ float brdf_oren_nayar(V3 L, V3 I, V3 N, V3 T, float s
     return clampf_ref(result, 0.0f, 1.0f);
 }
 
+// The same Oren-Nayar factor and its derivative with respect to sigma:
+// A = 1 - s^2 / (2 (s^2 + 0.33)), B = 0.45 s^2 / (s^2 + 0.09), so
+// dA/ds = -0.33 s / (s^2 + 0.33)^2 and dB/ds = 0.081 s / (s^2 + 0.09)^2;
+// where the reference clamps the result to [0, 1] the derivative is 0.
+__device__ __forceinline__ float brdf_oren_nayar_d(V3 L, V3 I, V3 N, V3 T, float sigma, float &d_sigma) {
+    const float sigma_sqr = sigma * sigma;
+    const float A = 1.0f - (sigma_sqr / (2.0f * (sigma_sqr + 0.33f)));
+    const float B = (0.45f * sigma_sqr) / (sigma_sqr + 0.09f);
+    const float cos_theta_I = dot(L, N);
+    const float cos_theta_O = -dot(I, N);
+    const float sin_theta_I = sqrtf(fmax_std(0.0f, 1.0f - (cos_theta_I * cos_theta_I)));
+    const float sin_theta_O = sqrtf(fmax_std(0.0f, 1.0f - (cos_theta_O * cos_theta_O)));
+    const float cos_phi_I = dot(L, T);
+    const float cos_phi_O = -dot(I, T);
+    const float sin_phi_I = sqrtf(fmax_std(0.0f, 1.0f - (cos_phi_I * cos_phi_I)));
+    const float sin_phi_O = sqrtf(fmax_std(0.0f, 1.0f - (cos_phi_O * cos_phi_O)));
+    const float temp = fmax_std(0.0f, (cos_phi_I * cos_phi_O) + (sin_phi_I * sin_phi_O));
+    float sin_alpha, tan_beta;
+    if (cos_theta_I > cos_theta_O) {
+        sin_alpha = sin_theta_O;
+        tan_beta = (sin_theta_I / cos_theta_I);
+    } else {
+        sin_alpha = sin_theta_I;
+        tan_beta = (sin_theta_O / cos_theta_O);
+    }
+    const float g = temp * sin_alpha * tan_beta;
+    const float result = (A + (B * g));
+    const float a2 = sigma_sqr + 0.33f, b2 = sigma_sqr + 0.09f;
+    const float dA = -0.33f * sigma / (a2 * a2), dB = 0.081f * sigma / (b2 * b2);
+    d_sigma = (result > 0.0f && result < 1.0f) ? dA + dB * g : 0.0f;
+    return clampf_ref(result, 0.0f, 1.0f);
+}
+
 // ExtractPlaneNormal, Core.cpp:216-228 (the reference scales by the length,
 // not its inverse; kept as is)
 __device__ __forceinline__ V3 plane_normal(const TriRec &tri) {

@@ -1,4 +1,6 @@
-"""Differentiable rendering of RAY_MAT_PRINCIPLED scenes from PyTorch.
+"""Differentiable rendering from PyTorch (RAY_MAT_PRINCIPLED albedo texture
+and roughness; the reference's RAY_MAT_DIFFUSE main colour and Oren-Nayar
+roughness).
 
 `render` is a thin torch.autograd.Function over the C ABI: its forward is
 `ray_render_diff` (the render loop with the parameters read from the given
@@ -36,27 +38,36 @@ def _leave(side, cur):
         cur.wait_stream(side)
 
 
+def _bind(scene, albedo, roughness, slots, rs, color):
+    ah, aw = (albedo.shape[0], albedo.shape[1]) if albedo is not None else (0, 0)
+    scene.set_diff_params(albedo.data_ptr() if albedo is not None else 0, aw, ah, roughness.data_ptr(), roughness.numel(), slots,
+                          rs.data_ptr() if rs is not None else 0, color.data_ptr() if color is not None else 0)
+
+
 class _DiffRender(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, albedo, roughness, renderer, scene, material_slot, first_iteration, samples, roughness_sampling):
-        if not (albedo.is_cuda and roughness.is_cuda):
+    def forward(ctx, albedo, roughness, color, renderer, scene, material_slot, first_iteration, samples, roughness_sampling):
+        if not roughness.is_cuda or (albedo is not None and not albedo.is_cuda) or (color is not None and not color.is_cuda):
             raise ValueError("parameters must be CUDA tensors")
-        albedo = albedo.detach().contiguous().float()
+        albedo = albedo.detach().contiguous().float() if albedo is not None else None
         roughness = roughness.detach().contiguous().float()
-        ah, aw, three = albedo.shape
-        if three != 3:
+        color = color.detach().contiguous().float() if color is not None else None
+        if albedo is not None and (albedo.dim() != 3 or albedo.shape[2] != 3):
             raise ValueError("albedo must be (h, w, 3)")
+        if color is not None and color.shape != (roughness.numel(), 3):
+            raise ValueError("color must be (n_roughness, 3)")
         rs = roughness_sampling.detach().contiguous().float() if roughness_sampling is not None else None
-        scene.set_diff_params(albedo.data_ptr(), aw, ah, roughness.data_ptr(), roughness.numel(), material_slot,
-                              rs.data_ptr() if rs is not None else 0)
+        _bind(scene, albedo, roughness, material_slot, rs, color)
         w, h = renderer.size()
-        image = torch.empty((h, w, 3), dtype=torch.float32, device=albedo.device)
-        per_sample = torch.empty((samples, h, w, 3), dtype=torch.float32, device=albedo.device)
-        side, cur = _enter(albedo.device)
+        dev = roughness.device
+        image = torch.empty((h, w, 3), dtype=torch.float32, device=dev)
+        per_sample = torch.empty((samples, h, w, 3), dtype=torch.float32, device=dev)
+        side, cur = _enter(dev)
         renderer.set_stream(side.cuda_stream)
         renderer.render_diff(scene, first_iteration, samples, image.data_ptr(), per_sample.data_ptr())
         _leave(side, cur)
-        ctx.save_for_backward(albedo, roughness, per_sample)
+        ctx.save_for_backward(roughness, per_sample)
+        ctx.albedo, ctx.color = albedo, color
         ctx.rough_sampling = rs
         ctx.renderer, ctx.scene, ctx.slots = renderer, scene, material_slot
         ctx.first_iteration, ctx.samples = first_iteration, samples
@@ -64,27 +75,31 @@ class _DiffRender(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, d_image):
-        albedo, roughness, per_sample = ctx.saved_tensors
+        roughness, per_sample = ctx.saved_tensors
+        albedo, color = ctx.albedo, ctx.color
         r, sc = ctx.renderer, ctx.scene
-        ah, aw, _ = albedo.shape
         # the parameters the forward pass read (the caller may have rebound them since)
-        rs = ctx.rough_sampling
-        sc.set_diff_params(albedo.data_ptr(), aw, ah, roughness.data_ptr(), roughness.numel(), ctx.slots,
-                           rs.data_ptr() if rs is not None else 0)
+        _bind(sc, albedo, roughness, ctx.slots, ctx.rough_sampling, color)
         d = d_image.detach().contiguous().float()
-        g_albedo = torch.zeros_like(albedo)
+        g_albedo = torch.zeros_like(albedo) if albedo is not None else None
         g_rough = torch.zeros_like(roughness)
-        side, cur = _enter(albedo.device)
+        g_color = torch.zeros_like(color) if color is not None else None
+        side, cur = _enter(roughness.device)
         r.set_stream(side.cuda_stream)
-        r.render_adjoint(sc, ctx.first_iteration, ctx.samples, per_sample.data_ptr(), d.data_ptr(), g_albedo.data_ptr(), g_rough.data_ptr())
+        r.render_adjoint(sc, ctx.first_iteration, ctx.samples, per_sample.data_ptr(), d.data_ptr(),
+                         g_albedo.data_ptr() if g_albedo is not None else 0, g_rough.data_ptr(),
+                         g_color.data_ptr() if g_color is not None else 0)
         _leave(side, cur)
-        return g_albedo, g_rough, None, None, None, None, None, None
+        return g_albedo, g_rough, g_color, None, None, None, None, None, None
 
 
-def render(albedo: torch.Tensor, roughness: torch.Tensor, renderer: api.Renderer, scene: api.Scene, material_slot,
-           first_iteration: int = 1, samples: int = 8, roughness_sampling: torch.Tensor | None = None) -> torch.Tensor:
+def render(albedo: torch.Tensor | None, roughness: torch.Tensor, renderer: api.Renderer, scene: api.Scene, material_slot,
+           first_iteration: int = 1, samples: int = 8, roughness_sampling: torch.Tensor | None = None,
+           color: torch.Tensor | None = None) -> torch.Tensor:
     """The (h, w, 3) mean of `samples` samples (iterations first_iteration ..)
     of scene's current camera with the differentiable parameters albedo
-    (ah, aw, 3) and roughness (n,); differentiable with respect to both.
+    (ah, aw, 3; None when no RAY_MAT_PRINCIPLED material has a slot),
+    roughness (n,) and color (n, 3: the RAY_MAT_DIFFUSE slots' main colours;
+    None: the materials' own); differentiable with respect to all three.
     roughness_sampling: frozen roughness for direction sampling and pdfs."""
-    return _DiffRender.apply(albedo, roughness, renderer, scene, material_slot, first_iteration, samples, roughness_sampling)
+    return _DiffRender.apply(albedo, roughness, color, renderer, scene, material_slot, first_iteration, samples, roughness_sampling)
