@@ -21,7 +21,7 @@ pytestmark = pytest.mark.gpu
 
 SPP = 4
 H_FD = 1e-3
-SLOTTED = (0, 5)  # the floor and the tall box
+SLOTTED = (5, 6)  # the two boxes
 ROUGH = (0.45, 0.7)
 
 
