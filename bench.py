@@ -597,8 +597,8 @@ def diff_frames(args, dev, stream, rank: int, world: int) -> dict:
     """The differentiable configuration: forward (ray_render_diff) and adjoint
     (ray_render_adjoint) times through the torch harness, the adjoint's
     gradients against central differences (h = 1e-3) of this renderer and of
-    the oracle, and 200 Adam steps of inverse rendering from albedo 0.5 and
-    roughness 0.5 towards the hidden parameters."""
+    the oracle, and Adam steps of inverse rendering from albedo 0.5 and
+    roughness 0.5 towards a 1,024-sample image of the hidden parameters."""
     import torch
 
     from raydemo_b200 import api, diff, scenes
@@ -710,50 +710,67 @@ def diff_frames(args, dev, stream, rank: int, world: int) -> dict:
         out["oracle_fd"] = {"roughness_max_rel_err": round(float(max(oerr_r)), 5), "albedo_texels": len(oerr_a),
                             "albedo_max_rel_err": round(float(max(oerr_a)), 5), "seconds": round(time.perf_counter() - t0, 1),
                             "threads": threads}
-    # inverse rendering: 200 Adam steps towards a 64-sample target. Each step takes the residual from one
-    # render and the adjoint from an independent one (other samples): with the same samples for both, the
-    # gradient would also follow the estimator's variance, which pulls the parameters away from the truth.
+    # inverse rendering: Adam steps (cosine-decayed learning rates) towards a 1,024-sample target, whose noise
+    # floor sits far below the per-step loss. Each step takes the residual from one render and the adjoint from
+    # an independent one (other samples): with the same samples for both, the gradient would also follow the
+    # estimator's variance, which pulls the parameters away from the truth. A call's samples stay inside one
+    # block of 256 iterations of the sample tables, so the target is 16 calls of 64 samples over four blocks, the
+    # optimisation draws from a fifth and the 64-sample loss checks from a sixth.
+    ispp = args.diff_inverse_spp
     with torch.no_grad():
-        target = diff.render(tgt_a, tgt_r, r, sc, slots, 1, 64).clone()
+        firsts = [1, 65, 129] + [256 * b + 64 * k for b in (1, 2, 3) for k in range(4)] + [1024]
+        acc = torch.zeros_like(target)
+        for f in firsts:
+            acc += diff.render(tgt_a, tgt_r, r, sc, slots, f, 64)
+        target = acc / len(firsts)
     albedo = torch.full_like(tgt_a, 0.5).requires_grad_(True)
     rough = torch.full_like(tgt_r, 0.5).requires_grad_(True)
     opt = torch.optim.Adam([{"params": [albedo], "lr": args.diff_lr_albedo}, {"params": [rough], "lr": args.diff_lr_rough}])
+    sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, max(1, args.diff_steps))
 
-    def loss64():  # the image loss at 64 samples (its noise floor far below the 8-sample loss's)
+    def loss64():  # the image loss at 64 samples (its noise floor far below the per-step loss's)
         with torch.no_grad():
-            return float(((diff.render(albedo, rough, r, sc, slots, 129, 64) - target) ** 2).sum())
+            return float(((diff.render(albedo, rough, r, sc, slots, 1600, 64) - target) ** 2).sum())
 
     with torch.no_grad():  # the floor: another 64-sample render at the hidden parameters
-        loss64_truth = float(((diff.render(tgt_a, tgt_r, r, sc, slots, 129, 64) - target) ** 2).sum())
+        loss64_truth = float(((diff.render(tgt_a, tgt_r, r, sc, slots, 1600, 64) - target) ** 2).sum())
     loss64_start = loss64()
     losses = []
     t0 = time.perf_counter()
     for step in range(args.diff_steps):
         opt.zero_grad()
-        first = 1 + (2 * spp * step) % (256 - 2 * spp)
+        first = 1280 + (2 * ispp * step) % (256 - 2 * ispp)
         with torch.no_grad():
-            resid = diff.render(albedo, rough, r, sc, slots, first, spp) - target
-        img = diff.render(albedo, rough, r, sc, slots, first + spp, spp)
+            resid = diff.render(albedo, rough, r, sc, slots, first, ispp) - target
+        img = diff.render(albedo, rough, r, sc, slots, first + ispp, ispp)
         (2.0 * resid * img).sum().backward()  # gradient 2 (I_a - T) dI_b
         opt.step()
+        sched.step()
         with torch.no_grad():
             albedo.clamp_(0.0, 1.0)
             rough.clamp_(0.05, 1.0)
         losses.append(float((resid ** 2).sum()))
     torch.cuda.synchronize(dev)
-    seen_mask = torch.zeros(tgt_a.numel(), dtype=torch.bool, device=dev)
-    seen_mask[torch.as_tensor(seen, device=dev)] = True
-    a_err0 = float(((0.5 - tgt_a.reshape(-1)[seen_mask]) ** 2).mean().sqrt())
-    a_err = float(((albedo.detach().reshape(-1) - tgt_a.reshape(-1))[seen_mask] ** 2).mean().sqrt())
+
+    def rmse(values, idx):
+        mask = torch.zeros(tgt_a.numel(), dtype=torch.bool, device=dev)
+        mask[torch.as_tensor(idx, device=dev)] = True
+        return float(((values.reshape(-1) - tgt_a.reshape(-1))[mask] ** 2).mean().sqrt())
+
+    half = torch.full_like(tgt_a, 0.5)
     secs = time.perf_counter() - t0
     loss64_end = loss64()
-    out["inverse"] = {"steps": args.diff_steps, "seconds": round(secs, 2), "lr": [args.diff_lr_albedo, args.diff_lr_rough],
-                      "loss8_first": round(losses[0], 3), "loss8_last": round(losses[-1], 3),
+    out["inverse"] = {"steps": args.diff_steps, "seconds": round(secs, 2), "samples_per_render": ispp,
+                      "lr": [args.diff_lr_albedo, args.diff_lr_rough], "lr_schedule": "cosine", "target_samples": 64 * len(firsts),
+                      "loss_first": round(losses[0], 3), "loss_last": round(losses[-1], 3),
                       "loss64_start": round(loss64_start, 3), "loss64_end": round(loss64_end, 3),
                       "loss64_ratio": round(loss64_end / loss64_start, 5), "loss64_at_hidden_parameters": round(loss64_truth, 3),
                       "roughness_mae_start": round(float((0.5 - tgt_r).abs().mean()), 4),
                       "roughness_mae_end": round(float((rough.detach() - tgt_r).abs().mean()), 4),
-                      "albedo_rmse_seen_start": round(a_err0, 4), "albedo_rmse_seen_end": round(a_err, 4)}
+                      "albedo_rmse_seen_start": round(rmse(half, seen), 4), "albedo_rmse_seen_end": round(rmse(albedo.detach(), seen), 4),
+                      "albedo_texels_well_seen": int(len(well)),
+                      "albedo_rmse_well_seen_start": round(rmse(half, well), 4),
+                      "albedo_rmse_well_seen_end": round(rmse(albedo.detach(), well), 4)}
     r.set_stream(0)
     return out
 
@@ -1016,8 +1033,9 @@ def main() -> None:
     ap.add_argument("--sort-only", action="store_true", help="only the ray sort")
     ap.add_argument("--no-sort", action="store_true", help="skip the ray sort measurement")
     ap.add_argument("--diff-steps", type=int, default=200, help="Adam steps of the inverse-rendering run")
+    ap.add_argument("--diff-inverse-spp", type=int, default=32, help="samples per render in an inverse-rendering step")
     ap.add_argument("--diff-lr-albedo", type=float, default=2e-3)
-    ap.add_argument("--diff-lr-rough", type=float, default=1e-2)
+    ap.add_argument("--diff-lr-rough", type=float, default=2e-3)
     ap.add_argument("--no-diff-oracle-fd", dest="diff_oracle_fd", action="store_false",
                     help="skip the oracle's finite differences in the differentiable form")
     ap.add_argument("--trace-tuning", default="auto", choices=["auto", "default"],

@@ -21,13 +21,13 @@ pytestmark = pytest.mark.gpu
 
 SPP = 4
 H_FD = 1e-3
-SLOTTED = (5, 6)  # the two boxes
+SLOTTED = (5, 8)  # the tall box and the icosphere
 ROUGH = (0.45, 0.7)
 
 
 def _spec(colors=None, rough=ROUGH):
     spec = scenes.cornell_box(0, 40, 32, max_bounces=3)
-    spec["lights"] = [{"type": api.PointLight, "position": (0.3, 0.8, 0.4), "radius": 0.05, "color": (2.0, 1.8, 1.6)}]
+    spec["lights"] = [{"type": api.PointLight, "position": (0.5, 0.6, 0.0), "radius": 0.05, "color": (2.0, 1.8, 1.6)}]
     for k, m in enumerate(SLOTTED):
         spec["materials"][m] = dict(spec["materials"][m], roughness=float(rough[k]))
         if colors is not None:
