@@ -279,8 +279,11 @@ int ray_scene_last_trace_info(ray_scene *s, ray_trace_info *out);
 /* Traversal kernel choice for this scene (no counterpart in the reference,
  * which has one CPU loop): kernel 1 = one thread per ray, 2 = resident grid
  * whose lanes take new rays as theirs finish (refill once at least
- * refill_min lanes of a warp are idle, 1..32). kernel 0 or refill_min <= 0
- * keep the current setting. deep_stack: 0 = size the traversal stack by the
+ * refill_min lanes of a warp are idle, 1..32) and test the triangles of a
+ * node step at once, 3 (the default, with refill_min 4) = the same grid
+ * testing one triangle per lane and step (a lane takes its next node once the
+ * last one's triangles are done), the warp meeting again after each phase.
+ * kernel 0 or refill_min <= 0 keep the current setting. deep_stack: 0 = size the traversal stack by the
  * BVH depth (shared memory only unless a tree is deeper than it holds),
  * 1 = always continue it in local memory. reorder: 0 = trace the rays in
  * their input order; 1 = first sort them (stably) by the reference's ray hash
@@ -290,8 +293,8 @@ int ray_scene_last_trace_info(ray_scene *s, ray_trace_info *out);
  * above the direction sector. The hits are written at each ray's input
  * position either way, and do not depend on the order. reorder_bits: how many
  * of the key's top bits the sort uses (8..32; 0 = 32). Calls of fewer than
- * 65,536 rays are not reordered. block (64, 128, 256; 0 = 128) and smem_stack
- * (16, 24, 32 entries per thread; 0 = 24; not 32 with 256 threads): threads
+ * 65,536 rays are not reordered. block (64, 128, 256; 0 = 64) and smem_stack
+ * (16, 24, 32 entries per thread; 0 = 16; not 32 with 256 threads): threads
  * per block of the persistent kernel and the depth of its shared-memory stack
  * (a deeper tree continues in local memory). stream_hint: 1 = the persistent
  * kernel reads rays and writes hits with the streaming (evict-first) cache

@@ -260,10 +260,10 @@ class Scene:
     def set_trace_tuning(self, kernel: int = 0, refill_min: int = 0, deep_stack: int = 0, reorder: int = 0, reorder_bits: int = 0,
                          block: int = 0, smem_stack: int = 0, stream_hint: int = 0, l2_persist: int = 0,
                          instance_tree: int = 0) -> None:
-        """ray_scene_set_trace_tuning: kernel (1 per ray, 2 persistent; 0
-        keeps), refill threshold (0 keeps), deep stack, trace order (0 input,
+        """ray_scene_set_trace_tuning: kernel (1 per ray, 2 persistent, 3
+        persistent with one triangle test per step; 0 keeps), refill threshold (0 keeps), deep stack, trace order (0 input,
         1 ray hash, 2 origin cell first), the key bits it sorts on, threads
-        per block and shared stack entries (0: 128 and 24), streaming cache
+        per block and shared stack entries (0: 64 and 16), streaming cache
         hint on rays and hits, L2 residency (1 nodes, 2 leaf triangles),
         instance tree (0 from 32 instances, 1 always, -1 never)."""
         t = capi.TraceTuning(kernel, refill_min, deep_stack, reorder, reorder_bits, block, smem_stack, stream_hint, l2_persist,

@@ -1070,7 +1070,7 @@ int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t) {
     RG_API_LOCK;
     RG_CHECK(!s || live_scene(s), "unknown or destroyed scene handle");
     RG_CHECK(s && t, "null argument");
-    RG_CHECK(t->kernel >= 0 && t->kernel <= 2, "kernel must be 1 (per ray) or 2 (persistent)");
+    RG_CHECK(t->kernel >= 0 && t->kernel <= 3, "kernel must be 1 (per ray), 2 (persistent) or 3 (persistent, one triangle per step)");
     RG_CHECK(t->refill_min <= 32, "refill_min is a lane count, at most 32");
     RG_CHECK(t->deep_stack == 0 || t->deep_stack == 1, "deep_stack is 0 or 1");
     RG_CHECK(t->reorder >= 0 && t->reorder <= 2, "reorder is 0 (input order), 1 (ray hash) or 2 (origin cell first)");
@@ -1086,8 +1086,8 @@ int ray_scene_set_trace_tuning(ray_scene *s, const ray_trace_tuning *t) {
     s->tuning.deep_stack = t->deep_stack;
     s->tuning.reorder = t->reorder;
     s->tuning.reorder_bits = t->reorder_bits ? t->reorder_bits : 32;
-    s->tuning.block = t->block ? t->block : 128;
-    s->tuning.smem_stack = t->smem_stack ? t->smem_stack : 24;
+    s->tuning.block = t->block ? t->block : 64;
+    s->tuning.smem_stack = t->smem_stack ? t->smem_stack : 16;
     s->tuning.stream_hint = t->stream_hint;
     s->tuning.l2_persist = t->l2_persist;
     if (t->instance_tree != s->tuning.instance_tree) s->inst_dirty = true; // built or dropped at the next commit
@@ -1231,7 +1231,8 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
                  static_cast<const InstanceRec *>(s->d_inst.p), s->n_inst_dev, s->tlas.nodes};
     RG_CUDA_TRY(s->d_next_ray.ensure(8)); // a work counter for each of two concurrent traces
     TraceParams tp;
-    tp.persistent = s->tuning.kernel == 2;
+    tp.persistent = s->tuning.kernel >= 2;
+    tp.one_tri = s->tuning.kernel == 3;
     tp.refill_min = s->tuning.refill_min;
     tp.block = s->tuning.block;
     tp.smem_stack = s->tuning.smem_stack;
@@ -1467,13 +1468,14 @@ int ray_scene_tune_trace(ray_scene *s, const float *rays, uint64_t n, ray_hit *h
         // one setting at a time, each stage starting from the best so far
         using Mut = std::function<void(ray_trace_tuning &)>;
         std::vector<std::vector<Mut>> stages = {
-            {[](ray_trace_tuning &t) { t.kernel = 2; }, [](ray_trace_tuning &t) { t.kernel = 1; }},
+            {[](ray_trace_tuning &t) { t.kernel = 2; }, [](ray_trace_tuning &t) { t.kernel = 3; }, [](ray_trace_tuning &t) { t.kernel = 1; }},
             {[](ray_trace_tuning &t) { t.l2_persist = 0; }, [](ray_trace_tuning &t) { t.l2_persist = 1; },
              [](ray_trace_tuning &t) { t.l2_persist = 2; }},
             {[](ray_trace_tuning &t) { t.stream_hint = 0; }, [](ray_trace_tuning &t) { t.stream_hint = 1; }},
             {[](ray_trace_tuning &t) { t.refill_min = 4; }, [](ray_trace_tuning &t) { t.refill_min = 8; },
              [](ray_trace_tuning &t) { t.refill_min = 12; }, [](ray_trace_tuning &t) { t.refill_min = 16; }},
-            {[](ray_trace_tuning &t) { t.block = 128; t.smem_stack = 24; }, [](ray_trace_tuning &t) { t.block = 64; t.smem_stack = 24; },
+            {[](ray_trace_tuning &t) { t.block = 64; t.smem_stack = 16; }, [](ray_trace_tuning &t) { t.block = 128; t.smem_stack = 24; },
+             [](ray_trace_tuning &t) { t.block = 64; t.smem_stack = 24; },
              [](ray_trace_tuning &t) { t.block = 256; t.smem_stack = 24; }, [](ray_trace_tuning &t) { t.block = 128; t.smem_stack = 16; },
              [](ray_trace_tuning &t) { t.block = 64; t.smem_stack = 32; }, [](ray_trace_tuning &t) { t.block = 256; t.smem_stack = 16; }},
             {[](ray_trace_tuning &t) { t.reorder = 0; t.reorder_bits = 32; }, [](ray_trace_tuning &t) { t.reorder = 1; t.reorder_bits = 32; },

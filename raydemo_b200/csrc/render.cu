@@ -565,7 +565,8 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
     const int n_jobs = (int)jobs.size();
     int bounces = 0;
     TraceParams tp;
-    tp.persistent = scn[0]->tuning.kernel == 2;
+    tp.persistent = scn[0]->tuning.kernel >= 2;
+    tp.one_tri = scn[0]->tuning.kernel == 3;
     tp.refill_min = scn[0]->tuning.refill_min;
     for (int j = 0; j < n_jobs; j++) {
         bounces = std::max(bounces, jobs[j].bounces);
@@ -678,7 +679,7 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
     for (int q = 0; q < 2; q++) key.add(rays[q]).add(pay[q]).add(job[q]);
     key.add(hits).add(obj).add(cnt).add(shadow.recs).add(shadow.rays).add(shadow.job).add(rb->d_loop_sort.p).add(nee).add(ref_lights);
     key.add(sv.nodes).add(sv.leaf_tris).add(sv.inst).add(sv.n_inst).add(tp.persistent).add(tp.refill_min).add(tp.max_depth).add(tp.views);
-    key.add(sv.tlas).add(tp.tlas).add(tp.block).add(tp.smem_stack);
+    key.add(sv.tlas).add(tp.tlas).add(tp.block).add(tp.smem_stack).add(tp.one_tri);
     key.add(ev).add(geo_best).add(geo_tris).add(persp);
     return graph_run(*gs, key.h, st, enqueue);
 }

@@ -29,6 +29,9 @@ namespace {
 using namespace trav;
 
 
+// Rays a warp of the persistent kernel reserves at a time (prefetched into L2).
+constexpr uint32_t RAY_CHUNK = 16;
+
 template <bool COUNT>
 __device__ __forceinline__ void flush_counters(uint32_t err, uint32_t nvis, uint32_t ntri, uint32_t *err_out, unsigned long long *counters) {
     if (err) atomicOr(err_out, err);
@@ -102,7 +105,13 @@ __global__ void __launch_bounds__(TRACE_BLOCK) k_trace_closest(SceneView sv, con
 // whose SceneView is at views + ray_job[i] * view_stride.
 // ANY: shadow rays -- a ray ends at its first accepted hit on a solid
 // triangle (Traverse_MacroTree_WithStack_AnyHit, CoreRef.cpp:1224-1368).
-template <bool COUNT, bool DEEP, bool MULTI = false, bool ANY = false, int BLOCK = TRACE_BLOCK, int SDEPTH = SMEM_STACK, bool TLAS = false>
+// ONE: a lane tests one triangle per loop iteration and takes its next node
+// only when the triangles of the last one are done, so each iteration is at
+// most one node step and one triangle test per lane; otherwise a lane tests
+// all the triangles of its node step in the same iteration, and the warp's
+// triangle loop runs as long as its longest list.
+template <bool COUNT, bool DEEP, bool MULTI = false, bool ANY = false, int BLOCK = TRACE_BLOCK, int SDEPTH = SMEM_STACK, bool TLAS = false,
+          bool ONE = false>
 __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const float4 *__restrict__ rays, uint32_t n,
                                                                   float4 *__restrict__ hits, int32_t *__restrict__ obj_out,
                                                                   uint32_t *__restrict__ err_out, unsigned long long *__restrict__ counters,
@@ -121,7 +130,7 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
     uint32_t ri = NO_RAY, mi = 0, visits = 0, steps = 0;
     uint32_t tstk[TLAS ? TLAS_STACK : 1]; // the ray's instance-tree stack (scenes with an instance tree)
     int tsp = 0;
-    bool in_mesh = false, pool_empty = false;
+    bool in_mesh = false;
     Best best;
     best.t = 0.0f;
     best.u = best.v = 0.0f;
@@ -129,18 +138,32 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
     LocalRay r = make_local_ray(0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f);
     MeshRef mr{};
     uint32_t ng_base = 0, ng_bits = 0, tg_base = 0, tg_bits = 0;
+    // The warp takes rays in chunks of RAY_CHUNK from the global counter: the
+    // current chunk [c_lo, c_hi) and the next one [n_lo, n_hi), whose rays are
+    // prefetched into L2 when it is reserved, so that a refilled lane's ray
+    // load does not wait on DRAM. Values are warp-uniform.
+    uint32_t c_lo, c_hi, n_lo, n_hi;
+    auto reserve = [&](uint32_t &lo, uint32_t &hi) {
+        uint32_t b = 0;
+        if (lane == 0) b = atomicAdd(next_ray, RAY_CHUNK);
+        b = __shfl_sync(0xffffffffu, b, 0);
+        lo = min(b, n);
+        hi = (uint32_t)min((unsigned long long)b + RAY_CHUNK, (unsigned long long)n);
+        const uint32_t i = lo + 4u * lane; // one 128-byte line holds four rays
+        if (!order && i < hi) asm volatile("prefetch.global.L2 [%0];" ::"l"(rays + 2ull * i));
+    };
+    reserve(c_lo, c_hi);
+    reserve(n_lo, n_hi);
     while (true) {
         // ---- refill lanes that have no ray
         const uint32_t need = __ballot_sync(0xffffffffu, ri == NO_RAY);
-        if (!pool_empty && need != 0 && (__popc(need) >= refill_min || need == 0xffffffffu)) {
-            const uint32_t leader = __ffs(need) - 1;
-            uint32_t base = 0;
-            if (lane == leader) base = atomicAdd(next_ray, (uint32_t)__popc(need));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            if (base + __popc(need) >= n) pool_empty = true;
+        const uint32_t cur = c_hi - c_lo, avail = cur + (n_hi - n_lo);
+        if (avail != 0 && need != 0 && (__popc(need) >= refill_min || need == 0xffffffffu)) {
+            const uint32_t taken = min((uint32_t)__popc(need), avail);
             if (ri == NO_RAY) {
-                const uint32_t idx = base + __popc(need & lanemask_lt);
-                if (idx < n) {
+                const uint32_t k = __popc(need & lanemask_lt);
+                if (k < avail) {
+                    const uint32_t idx = k < cur ? c_lo + k : n_lo + (k - cur);
                     ri = order ? __ldg(order + idx) : idx;
                     mi = 0;
                     if (TLAS) {
@@ -153,11 +176,26 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
                     best.prim = best.obj = -1;
                 }
             }
+            if (taken >= cur) { // the current chunk is used up: the next one takes its place
+                c_lo = n_lo + (taken - cur);
+                c_hi = n_hi;
+                reserve(n_lo, n_hi);
+            } else {
+                c_lo += taken;
+            }
         }
-        if (pool_empty && __all_sync(0xffffffffu, ri == NO_RAY)) break;
-        if (ri == NO_RAY) continue;
+        if (c_lo == c_hi && n_lo == n_hi && __all_sync(0xffffffffu, ri == NO_RAY)) break;
+        // A lane without work this iteration falls through to the next one;
+        // with ONE the warp meets again (__syncwarp) after each phase, which
+        // keeps lanes that took different branches from drifting into
+        // different iterations (measured: 4.28 ms without, 3.7 ms with, per
+        // 4M-ray launch of the microbench on B200)
+        bool idle = ri == NO_RAY;
         // ---- next instance whose box the ray enters, or the end of the ray
-        if (!in_mesh) {
+        // (a ray whose scene has no instance left is done without reading it
+        // again; a multi-scene ray reads its scene view first)
+        if (!idle && !in_mesh) {
+          if (MULTI || (TLAS && sv.tlas ? tsp > 0 : mi < sv.n_inst)) {
             // streaming hint: the ray is read once per instance pass and the
             // hit written once, so they may leave L1/L2 first (evict-first),
             // which keeps more of the BVH resident
@@ -203,56 +241,79 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
                 in_mesh = true;
                 break;
             }
+          }
             if (!in_mesh) {
                 const float4 h = make_float4(__int_as_float(best.prim), best.t, best.prim >= 0 ? best.u : 0.0f, best.prim >= 0 ? best.v : 0.0f);
                 if (stream_hint) __stcs(hits + ri, h);
                 else hits[ri] = h;
                 if (obj_out) obj_out[ri] = best.obj;
                 ri = NO_RAY;
-                continue;
+                idle = true;
             }
         }
+        if (ONE) __syncwarp();
         // ---- one traversal step: a node visit and the triangles it hits. A
         // mesh takes at most node_count steps; more means a corrupt structure.
         // Every group pushed today has a node bit, so the else branch (a group
         // of triangles only, tested as such) does not run; keeping the node
         // step under this test measured 4.8 ms instead of 6.9 ms per 4M-ray
         // launch on B200, the compiler keeping the warp converged around it.
-        bool ok = ++steps <= mr.node_count + 8u;
-        if (!ok) err |= TRACE_ERR_LIMIT;
-        if (ok && ng_bits > 0x00FFFFFFu) {
-            ok = node_step<COUNT>(mr, r, best.t, ng_base, ng_bits, tg_base, tg_bits, st, visits, err, nvis);
-        } else if (ok) {
-            tg_base = ng_base;
-            tg_bits = ng_bits;
-            ng_bits = 0;
-        }
-        if (!ok) {
-            in_mesh = false;
-            mi = 0xffffffffu; // abandon the ray; the error flag reports it
-            tsp = 0;
-            continue;
-        }
-        bool stop = false;
-        while (tg_bits) {
-            const uint32_t k = __ffs(tg_bits) - 1;
-            tg_bits &= tg_bits - 1;
-            if (ANY) {
-                if (tri_test<COUNT, true>(mr, r, tg_base + k, best, err, ntri)) {
-                    stop = true;
-                    tg_bits = 0;
-                }
-            } else {
-                tri_test<COUNT>(mr, r, tg_base + k, best, err, ntri);
+        if (!idle && (!ONE || tg_bits == 0)) {
+            bool ok = ++steps <= mr.node_count + 8u;
+            if (!ok) err |= TRACE_ERR_LIMIT;
+            if (ok && ng_bits > 0x00FFFFFFu) {
+                ok = node_step<COUNT>(mr, r, best.t, ng_base, ng_bits, tg_base, tg_bits, st, visits, err, nvis);
+            } else if (ok) {
+                tg_base = ng_base;
+                tg_bits = ng_bits;
+                ng_bits = 0;
+            }
+            if (!ok) {
+                in_mesh = false;
+                mi = 0xffffffffu; // abandon the ray; the error flag reports it
+                tsp = 0;
+                tg_bits = 0;
+                idle = true;
             }
         }
+        if (ONE) __syncwarp();
+        bool stop = false;
+        if (ONE) {
+            if (!idle && tg_bits) {
+                const uint32_t k = __ffs(tg_bits) - 1;
+                tg_bits &= tg_bits - 1;
+                if (ANY) {
+                    if (tri_test<COUNT, true>(mr, r, tg_base + k, best, err, ntri)) {
+                        stop = true;
+                        tg_bits = 0;
+                    }
+                } else {
+                    tri_test<COUNT>(mr, r, tg_base + k, best, err, ntri);
+                }
+            }
+        } else {
+            while (!idle && tg_bits) {
+                const uint32_t k = __ffs(tg_bits) - 1;
+                tg_bits &= tg_bits - 1;
+                if (ANY) {
+                    if (tri_test<COUNT, true>(mr, r, tg_base + k, best, err, ntri)) {
+                        stop = true;
+                        tg_bits = 0;
+                    }
+                } else {
+                    tri_test<COUNT>(mr, r, tg_base + k, best, err, ntri);
+                }
+            }
+        }
+        if (ONE) __syncwarp();
+        if (idle) continue;
         if (ANY && stop) { // a solid triangle blocks the ray: no further instance
             in_mesh = false;
             mi = 0xffffffffu;
             tsp = 0;
             continue;
         }
-        if (ng_bits <= 0x00FFFFFFu) {
+        if (tg_bits == 0 && ng_bits <= 0x00FFFFFFu) {
             if (st.sp == 0) {
                 in_mesh = false;
             } else {
@@ -269,7 +330,7 @@ int g_persistent_blocks[2][2] = {{0, 0}, {0, 0}}; // [DEEP][TLAS]
 
 // The closest-hit persistent kernel with a tuned block size and shared stack
 // depth (one resident grid: the SM count times the blocks that fit per SM).
-template <bool DEEP, bool TLAS, int BLOCK, int SDEPTH>
+template <bool DEEP, bool TLAS, int BLOCK, int SDEPTH, bool ONE>
 cudaError_t launch_tuned(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
                          unsigned long long *counters, cudaStream_t st, const TraceParams &tp) {
     static_assert(SDEPTH * BLOCK * 8 <= 48 * 1024, "static shared memory limit");
@@ -279,14 +340,14 @@ cudaError_t launch_tuned(const SceneView &sv, const float4 *rays, uint32_t n, fl
         cudaError_t e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_persistent<false, DEEP, false, false, BLOCK, SDEPTH, TLAS>,
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_persistent<false, DEEP, false, false, BLOCK, SDEPTH, TLAS, ONE>,
                                                               BLOCK, 0);
         if (e != cudaSuccess) return e;
         blocks = sms * (per_sm > 0 ? per_sm : 1);
     }
     cudaError_t e = cudaMemsetAsync(tp.next_ray, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
-    k_trace_persistent<false, DEEP, false, false, BLOCK, SDEPTH, TLAS><<<blocks, BLOCK, 0, st>>>(
+    k_trace_persistent<false, DEEP, false, false, BLOCK, SDEPTH, TLAS, ONE><<<blocks, BLOCK, 0, st>>>(
         sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min, tp.count, nullptr, 0, nullptr, tp.order, tp.stream_hint);
     return cudaGetLastError();
 }
@@ -295,9 +356,11 @@ template <bool DEEP, bool TLAS>
 cudaError_t launch_tuned_dispatch(const SceneView &sv, const float4 *rays, uint32_t n, float4 *hits, int32_t *obj, uint32_t *err,
                                   unsigned long long *counters, cudaStream_t st, const TraceParams &tp) {
 #define RG_TUNED(B, D)                                                                                                                  \
-    if (tp.block == B && tp.smem_stack == D) return launch_tuned<DEEP, TLAS, B, D>(sv, rays, n, hits, obj, err, counters, st, tp);
+    if (tp.block == B && tp.smem_stack == D)                                                                                            \
+        return tp.one_tri ? launch_tuned<DEEP, TLAS, B, D, true>(sv, rays, n, hits, obj, err, counters, st, tp)                          \
+                          : launch_tuned<DEEP, TLAS, B, D, false>(sv, rays, n, hits, obj, err, counters, st, tp);
     RG_TUNED(64, 16) RG_TUNED(64, 24) RG_TUNED(64, 32)
-    RG_TUNED(128, 16) RG_TUNED(128, 32)
+    RG_TUNED(128, 16) RG_TUNED(128, 24) RG_TUNED(128, 32)
     RG_TUNED(256, 16) RG_TUNED(256, 24)
 #undef RG_TUNED
     return cudaErrorInvalidValue;
@@ -316,7 +379,7 @@ cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, flo
         return cudaGetLastError();
     }
     if (!tp.next_ray) return cudaErrorInvalidValue;
-    if (!count && !tp.views && !tp.any && !(tp.block == TRACE_BLOCK && tp.smem_stack == SMEM_STACK))
+    if (!count && !tp.views && !tp.any && (tp.one_tri || !(tp.block == TRACE_BLOCK && tp.smem_stack == SMEM_STACK)))
         return launch_tuned_dispatch<DEEP, TLAS>(sv, rays, n, hits, obj, err, counters, st, tp);
     int &blocks = g_persistent_blocks[DEEP ? 1 : 0][TLAS ? 1 : 0];
     if (blocks == 0) {
@@ -330,20 +393,27 @@ cudaError_t launch_impl(const SceneView &sv, const float4 *rays, uint32_t n, flo
     }
     cudaError_t e = cudaMemsetAsync(tp.next_ray, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
-    if (tp.any) { // shadow rays (no counting variant)
-        if (tp.views)
-            k_trace_persistent<false, DEEP, true, true, B, D, TLAS><<<blocks, TRACE_BLOCK, 0, st>>>(
-                sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min, tp.count, tp.views, tp.view_stride, tp.ray_job);
-        else
-            k_trace_persistent<false, DEEP, false, true, B, D, TLAS><<<blocks, TRACE_BLOCK, 0, st>>>(sv, rays, n, hits, obj, err, counters,
-                                                                                                 tp.next_ray, tp.refill_min, tp.count);
+    // shadow rays and rays of several scenes (no counting variants), with one
+    // triangle test per step or a node's triangles at once
+#define RG_LAUNCH_P(MULTI_, ANY_, ONE_)                                                                                                 \
+    k_trace_persistent<false, DEEP, MULTI_, ANY_, B, D, TLAS, ONE_><<<blocks, TRACE_BLOCK, 0, st>>>(                                    \
+        sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min, tp.count, tp.views, tp.view_stride, tp.ray_job)
+    if (tp.any) {
+        if (tp.views) {
+            if (tp.one_tri) RG_LAUNCH_P(true, true, true);
+            else RG_LAUNCH_P(true, true, false);
+        } else {
+            if (tp.one_tri) RG_LAUNCH_P(false, true, true);
+            else RG_LAUNCH_P(false, true, false);
+        }
         return cudaGetLastError();
     }
-    if (tp.views) { // rays of several scenes (no counting variant)
-        k_trace_persistent<false, DEEP, true, false, B, D, TLAS><<<blocks, TRACE_BLOCK, 0, st>>>(
-            sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min, tp.count, tp.views, tp.view_stride, tp.ray_job);
+    if (tp.views) {
+        if (tp.one_tri) RG_LAUNCH_P(true, false, true);
+        else RG_LAUNCH_P(true, false, false);
         return cudaGetLastError();
     }
+#undef RG_LAUNCH_P
     if (count)
         k_trace_persistent<true, DEEP, false, false, B, D, TLAS><<<blocks, TRACE_BLOCK, 0, st>>>(
             sv, rays, n, hits, obj, err, counters, tp.next_ray, tp.refill_min, tp.count, nullptr, 0, nullptr, tp.order);

@@ -323,6 +323,31 @@ __device__ __forceinline__ bool node_step(const MeshRef &mr, const LocalRay &r, 
     return true;
 }
 
+// The reference's triangle arithmetic (_IntersectTri, CoreRef.cpp:18-40) on
+// one precomputed record (t0, t1, t2) and a ray given by origin and
+// direction: true when the ray's line passes the edge tests; then
+// t = dett / det, u = detu / det and v = detv / det, each as the product with
+// the correctly rounded reciprocal rdet, as the reference computes them.
+__device__ __forceinline__ bool tri_core(const float4 &t0, const float4 &t1, const float4 &t2, float ox, float oy, float oz, float dx,
+                                         float dy, float dz, float &rdet, float &dett, float &detu, float &detv) {
+    const float nu = t0.x, nv = t0.y, npl = t0.z, pu = t0.w, pv = t1.x, e0u = t1.z, e0v = t1.w, e1u = t2.x, e1v = t2.y;
+    const int iw = __float_as_int(t1.y) & TRI_W_BITS;
+    const float du = iw == 0 ? dy : dx, dv = iw == 2 ? dy : dz, dw = iw == 0 ? dx : (iw == 1 ? dy : dz);
+    const float ou = iw == 0 ? oy : ox, ov = iw == 2 ? oy : oz, ow = iw == 0 ? ox : (iw == 1 ? oy : oz);
+    const float det = __fadd_rn(__fadd_rn(__fmul_rn(du, nu), __fmul_rn(dv, nv)), dw);
+    dett = __fsub_rn(npl, __fadd_rn(__fadd_rn(__fmul_rn(ou, nu), __fmul_rn(ov, nv)), ow));
+    const float Du = __fsub_rn(__fmul_rn(du, dett), __fmul_rn(__fsub_rn(pu, ou), det));
+    const float Dv = __fsub_rn(__fmul_rn(dv, dett), __fmul_rn(__fsub_rn(pv, ov), det));
+    detu = __fsub_rn(__fmul_rn(e1v, Du), __fmul_rn(e1u, Dv));
+    detv = __fsub_rn(__fmul_rn(e0u, Dv), __fmul_rn(e0v, Du));
+    const float tmpdet0 = __fsub_rn(__fsub_rn(det, detu), detv);
+    if ((tmpdet0 > -HIT_EPS && detu > -HIT_EPS && detv > -HIT_EPS) || (tmpdet0 < HIT_EPS && detu < HIT_EPS && detv < HIT_EPS)) {
+        rdet = __frcp_rn(det); // 1.0f / det, correctly rounded
+        return true;
+    }
+    return false;
+}
+
 // One triangle test; updates best when it is the closer hit. With SOLID,
 // returns whether that hit is on a solid triangle (TRI_SOLID_BIT), which ends
 // a shadow ray's search (IntersectTris_AnyHit, CoreRef.cpp:804-829).
@@ -335,20 +360,8 @@ __device__ __forceinline__ bool tri_test(const MeshRef &mr, const LocalRay &r, u
     const float4 *tp = reinterpret_cast<const float4 *>(mr.tris + li);
     const float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
     if (COUNT) ntri++;
-    const float nu = t0.x, nv = t0.y, npl = t0.z, pu = t0.w, pv = t1.x, e0u = t1.z, e0v = t1.w, e1u = t2.x, e1v = t2.y;
-    const int iw = __float_as_int(t1.y) & TRI_W_BITS;
-    const float du = iw == 0 ? r.dy : r.dx, dv = iw == 2 ? r.dy : r.dz, dw = iw == 0 ? r.dx : (iw == 1 ? r.dy : r.dz);
-    const float ou = iw == 0 ? r.oy : r.ox, ov = iw == 2 ? r.oy : r.oz, ow = iw == 0 ? r.ox : (iw == 1 ? r.oy : r.oz);
-    // _IntersectTri, CoreRef.cpp:18-40
-    const float det = __fadd_rn(__fadd_rn(__fmul_rn(du, nu), __fmul_rn(dv, nv)), dw);
-    const float dett = __fsub_rn(npl, __fadd_rn(__fadd_rn(__fmul_rn(ou, nu), __fmul_rn(ov, nv)), ow));
-    const float Du = __fsub_rn(__fmul_rn(du, dett), __fmul_rn(__fsub_rn(pu, ou), det));
-    const float Dv = __fsub_rn(__fmul_rn(dv, dett), __fmul_rn(__fsub_rn(pv, ov), det));
-    const float detu = __fsub_rn(__fmul_rn(e1v, Du), __fmul_rn(e1u, Dv));
-    const float detv = __fsub_rn(__fmul_rn(e0u, Dv), __fmul_rn(e0v, Du));
-    const float tmpdet0 = __fsub_rn(__fsub_rn(det, detu), detv);
-    if ((tmpdet0 > -HIT_EPS && detu > -HIT_EPS && detv > -HIT_EPS) || (tmpdet0 < HIT_EPS && detu < HIT_EPS && detv < HIT_EPS)) {
-        const float rdet = __frcp_rn(det); // 1.0f / det, correctly rounded
+    float rdet, dett, detu, detv;
+    if (tri_core(t0, t1, t2, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, rdet, dett, detu, detv)) {
         const float t = __fmul_rn(dett, rdet);
         const int gp = (int)(mr.prim_base + __float_as_uint(t2.z));
         if (t > 0.0f && (t < best.t || (t == best.t && best.prim >= 0 && gp < best.prim))) {

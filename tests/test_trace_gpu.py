@@ -207,7 +207,9 @@ def variants_case(renderer, oracle):
     (1, 8, 0, 0, 32, 128, 24), (1, 8, 1, 0, 32, 128, 24), (2, 1, 0, 0, 32, 128, 24), (2, 8, 0, 0, 32, 128, 24),
     (2, 32, 0, 0, 32, 128, 24), (2, 8, 1, 0, 32, 128, 24), (2, 8, 0, 1, 32, 128, 24), (2, 8, 0, 2, 24, 128, 24),
     (1, 8, 0, 1, 16, 128, 24), (2, 4, 1, 2, 32, 128, 24), (2, 8, 0, 0, 32, 64, 16), (2, 8, 0, 1, 32, 64, 32),
-    (2, 8, 1, 0, 32, 256, 16), (2, 16, 0, 0, 32, 256, 24), (2, 8, 0, 0, 32, 128, 16), (2, 8, 1, 0, 32, 128, 32)])
+    (2, 8, 1, 0, 32, 256, 16), (2, 16, 0, 0, 32, 256, 24), (2, 8, 0, 0, 32, 128, 16), (2, 8, 1, 0, 32, 128, 32),
+    (3, 4, 0, 0, 32, 64, 16), (3, 1, 0, 0, 32, 64, 16), (3, 8, 1, 0, 32, 128, 24), (3, 32, 0, 1, 32, 256, 16),
+    (3, 4, 1, 2, 24, 64, 32), (3, 16, 0, 0, 32, 256, 24)])
 @pytest.mark.parametrize("hint,persist", [(0, 0), (1, 1), (1, 2)])
 def test_kernel_variants_agree(variants_case, kernel, refill, deep, reorder, bits, block, sdepth, hint, persist):
     """Every traversal kernel, block size, stack placement and depth, trace
