@@ -170,7 +170,7 @@ def tuned_tuple(info) -> dict:
     """The frame tuner's choice as the renderer reports it after a frame."""
     return {"kernel": {1: "wavefront", 2: "path"}.get(info.kernel, "?"), "sort_mask": f"0x{info.sort_mask:03x}",
             "trace_variant": int(info.trace_variant), "refill": int(info.trace_refill), "block": int(info.trace_block),
-            "smem_stack": int(info.trace_stack)}
+            "smem_stack": int(info.trace_stack), "one_triangle_per_step": int(info.trace_one_tri)}
 
 
 def make_workload(rank: int, n_tris: int = N_TRIS, n_rays: int = N_RAYS):

@@ -395,7 +395,7 @@ typedef struct ray_frame_info {
     int32_t kernel; /* the kernel that rendered it: 1 wavefront, 2 path kernel */
     uint64_t rays, shadow_rays;
     uint32_t sort_mask; /* wavefront: bounces whose rays were sorted first (bit b: secondary bounce b) */
-    uint32_t reserved;
+    uint32_t trace_one_tri; /* wavefront: 1 = its traces tested one triangle per lane and step */
     /* wavefront: the trace settings it ran with (ray_renderer_set_trace_variant):
      * their index, refill threshold, threads per block and shared stack entries
      * (0 for each of the three: the scene's own settings) */
@@ -406,9 +406,10 @@ int ray_renderer_frame_info(ray_renderer *r, ray_frame_info *out);
 /* The wavefront's trace settings (no counterpart in the reference): -1 (the
  * default) = the frame tuner times them with the kernel and the sort mask on
  * the first frames of each frame configuration -- index 0 is the scene's own
- * settings, 1..5 are refill threshold / threads per block / shared stack
- * entries of (4, 128, 24), (16, 128, 24), (8, 64, 24), (8, 256, 24),
- * (8, 128, 16) -- and keeps the fastest; the choice is also kept per frame
+ * refill threshold, threads per block and shared stack entries with a node's
+ * triangles tested at once, 1..3 are (8, 128, 24), (16, 128, 24), (8, 64, 24)
+ * the same way, 4..5 are (4, 64, 16), (8, 128, 16) with one triangle test per
+ * lane and step -- and keeps the fastest; the choice is also kept per frame
  * signature (triangle and light counts, pixels, bounces, settings) for every
  * renderer of the process; 0..5 = that setting. Every setting renders the
  * same image. */

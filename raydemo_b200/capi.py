@@ -97,7 +97,7 @@ class TraceInfo(C.Structure):
 
 class FrameInfo(C.Structure):
     _fields_ = [("error_flags", C.c_uint32), ("kernel", C.c_int32), ("rays", C.c_uint64), ("shadow_rays", C.c_uint64),
-                ("sort_mask", C.c_uint32), ("reserved", C.c_uint32), ("trace_variant", C.c_int32), ("trace_refill", C.c_int32),
+                ("sort_mask", C.c_uint32), ("trace_one_tri", C.c_uint32), ("trace_variant", C.c_int32), ("trace_refill", C.c_int32),
                 ("trace_block", C.c_int32), ("trace_stack", C.c_int32)]
 
 

@@ -29,9 +29,6 @@ namespace {
 using namespace trav;
 
 
-// Rays a warp of the persistent kernel reserves at a time (prefetched into L2).
-constexpr uint32_t RAY_CHUNK = 16;
-
 template <bool COUNT>
 __device__ __forceinline__ void flush_counters(uint32_t err, uint32_t nvis, uint32_t ntri, uint32_t *err_out, unsigned long long *counters) {
     if (err) atomicOr(err_out, err);
@@ -138,32 +135,19 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
     LocalRay r = make_local_ray(0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f);
     MeshRef mr{};
     uint32_t ng_base = 0, ng_bits = 0, tg_base = 0, tg_bits = 0;
-    // The warp takes rays in chunks of RAY_CHUNK from the global counter: the
-    // current chunk [c_lo, c_hi) and the next one [n_lo, n_hi), whose rays are
-    // prefetched into L2 when it is reserved, so that a refilled lane's ray
-    // load does not wait on DRAM. Values are warp-uniform.
-    uint32_t c_lo, c_hi, n_lo, n_hi;
-    auto reserve = [&](uint32_t &lo, uint32_t &hi) {
-        uint32_t b = 0;
-        if (lane == 0) b = atomicAdd(next_ray, RAY_CHUNK);
-        b = __shfl_sync(0xffffffffu, b, 0);
-        lo = min(b, n);
-        hi = (uint32_t)min((unsigned long long)b + RAY_CHUNK, (unsigned long long)n);
-        const uint32_t i = lo + 4u * lane; // one 128-byte line holds four rays
-        if (!order && i < hi) asm volatile("prefetch.global.L2 [%0];" ::"l"(rays + 2ull * i));
-    };
-    reserve(c_lo, c_hi);
-    reserve(n_lo, n_hi);
+    bool pool_empty = false;
     while (true) {
         // ---- refill lanes that have no ray
         const uint32_t need = __ballot_sync(0xffffffffu, ri == NO_RAY);
-        const uint32_t cur = c_hi - c_lo, avail = cur + (n_hi - n_lo);
-        if (avail != 0 && need != 0 && (__popc(need) >= refill_min || need == 0xffffffffu)) {
-            const uint32_t taken = min((uint32_t)__popc(need), avail);
+        if (!pool_empty && need != 0 && (__popc(need) >= refill_min || need == 0xffffffffu)) {
+            const uint32_t leader = __ffs(need) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(next_ray, (uint32_t)__popc(need));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + __popc(need) >= n) pool_empty = true;
             if (ri == NO_RAY) {
-                const uint32_t k = __popc(need & lanemask_lt);
-                if (k < avail) {
-                    const uint32_t idx = k < cur ? c_lo + k : n_lo + (k - cur);
+                const uint32_t idx = base + __popc(need & lanemask_lt);
+                if (idx < n) {
                     ri = order ? __ldg(order + idx) : idx;
                     mi = 0;
                     if (TLAS) {
@@ -176,21 +160,15 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
                     best.prim = best.obj = -1;
                 }
             }
-            if (taken >= cur) { // the current chunk is used up: the next one takes its place
-                c_lo = n_lo + (taken - cur);
-                c_hi = n_hi;
-                reserve(n_lo, n_hi);
-            } else {
-                c_lo += taken;
-            }
         }
-        if (c_lo == c_hi && n_lo == n_hi && __all_sync(0xffffffffu, ri == NO_RAY)) break;
+        if (pool_empty && __all_sync(0xffffffffu, ri == NO_RAY)) break;
         // A lane without work this iteration falls through to the next one;
         // with ONE the warp meets again (__syncwarp) after each phase, which
         // keeps lanes that took different branches from drifting into
         // different iterations (measured: 4.28 ms without, 3.7 ms with, per
         // 4M-ray launch of the microbench on B200)
         bool idle = ri == NO_RAY;
+        if (!ONE && idle) continue;
         // ---- next instance whose box the ray enters, or the end of the ray
         // (a ray whose scene has no instance left is done without reading it
         // again; a multi-scene ray reads its scene view first)
@@ -249,6 +227,7 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
                 if (obj_out) obj_out[ri] = best.obj;
                 ri = NO_RAY;
                 idle = true;
+                if (!ONE) continue;
             }
         }
         if (ONE) __syncwarp();
@@ -274,6 +253,7 @@ __global__ void __launch_bounds__(BLOCK) k_trace_persistent(SceneView sv, const 
                 tsp = 0;
                 tg_bits = 0;
                 idle = true;
+                if (!ONE) continue;
             }
         }
         if (ONE) __syncwarp();
