@@ -280,7 +280,7 @@ int ray_scene_last_trace_info(ray_scene *s, ray_trace_info *out);
  * which has one CPU loop): kernel 1 = one thread per ray, 2 = resident grid
  * whose lanes take new rays as theirs finish (refill once at least
  * refill_min lanes of a warp are idle, 1..32) and test the triangles of a
- * node step at once, 3 (the default, with refill_min 4) = the same grid
+ * node step at once, 3 (the default, with refill_min 8) = the same grid
  * testing one triangle per lane and step (a lane takes its next node once the
  * last one's triangles are done), the warp meeting again after each phase.
  * kernel 0 or refill_min <= 0 keep the current setting. deep_stack: 0 = size the traversal stack by the

@@ -144,7 +144,7 @@ struct ray_scene {
     // batch-trace staging and diagnostics
     rg::DeviceBuf d_rays, d_hits, d_obj, d_err, d_counters, d_next_ray;
     rg::DeviceBuf d_order[2]; // reordered traces: keys, order and sort scratch of each of two concurrent chunks
-    ray_trace_tuning tuning{3, 4, 0, 0, 32, 64, 16, 0, 0, 0};
+    ray_trace_tuning tuning{3, 8, 0, 0, 32, 64, 16, 0, 0, 0};
     bool counting = false;
     ray_trace_info last_info{};
     bool info_pending = false;
