@@ -239,6 +239,7 @@ std::unordered_set<const void *> &live_handles() {
 } // namespace
 
 bool live_scene(const ray_scene *s) { return live_handles().count(s) != 0; }
+thread_local int t_api_depth = 0;
 bool live_renderer(const ray_renderer *r) { return live_handles().count(r) != 0; }
 
 cudaError_t note_use(ray_scene *s, cudaStream_t st) {
@@ -434,6 +435,7 @@ ray_scene::~ray_scene() {
     for (cudaEvent_t e : pipe_ev)
         if (e) cudaEventDestroy(e);
     for (auto &u : users) cudaEventDestroy(u.second);
+    if (h_info) cudaFreeHost(h_info);
 }
 
 extern "C" {
@@ -1170,6 +1172,27 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
     RG_CHECK(mem == RAY_MEM_HOST || mem == RAY_MEM_DEVICE, "invalid memory space");
     RG_CHECK(n <= 0xffffffffull, "too many rays in one call");
     RG_GUARD_BEGIN
+    // host-buffer traces of one scene run one at a time; a caller that has to
+    // wait for another thread's lets the API lock go meanwhile (the scene's
+    // mutex first, then the API lock: the order every such call takes them)
+    std::shared_ptr<std::mutex> host_mu;
+    std::unique_lock<std::mutex> host_lock;
+    if (mem == RAY_MEM_HOST) {
+        host_mu = s->host_mu;
+        host_lock = std::unique_lock<std::mutex>(*host_mu, std::try_to_lock);
+        if (!host_lock.owns_lock()) {
+            RG_CHECK(t_api_depth == 1, "a host-buffer trace of this scene is already running on this thread");
+            api_mutex().unlock();
+            try {
+                host_lock.lock();
+            } catch (...) {
+                api_mutex().lock();
+                throw;
+            }
+            api_mutex().lock();
+            RG_CHECK(live_scene(s), "scene destroyed while the call waited for it");
+        }
+    }
     RG_CUDA_TRY(cudaSetDevice(s->device));
     int rc = commit(s);
     if (rc != RAY_OK) return rc;
@@ -1300,11 +1323,9 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
             cudaStreamAttrValue off{};
             RG_CUDA_TRY(cudaStreamSetAttribute(ts, cudaStreamAttributeAccessPolicyWindow, &off));
         }
-        if (mem == RAY_MEM_HOST && m) {
-            if (piped) {
-                RG_CUDA_TRY(cudaEventRecord(s->pipe_ev[2], ts));
-                RG_CUDA_TRY(cudaStreamWaitEvent(down, s->pipe_ev[2], 0));
-            }
+        if (mem == RAY_MEM_HOST && m && piped) { // (pageable buffers: the download below, without the API lock)
+            RG_CUDA_TRY(cudaEventRecord(s->pipe_ev[2], ts));
+            RG_CUDA_TRY(cudaStreamWaitEvent(down, s->pipe_ev[2], 0));
             RG_CUDA_TRY(cudaMemcpyAsync(hits + b, d_hits + b, m * 16, cudaMemcpyDeviceToHost, down));
             if (obj) RG_CUDA_TRY(cudaMemcpyAsync(obj + b, d_obj + b, m * 4, cudaMemcpyDeviceToHost, down));
         }
@@ -1317,10 +1338,36 @@ int ray_scene_trace_closest(ray_scene *s, const float *rays, uint64_t n, ray_hit
     RG_CUDA_TRY(note_use(s, st));
     s->info_pending = true;
     s->info_stream = st;
+    const uint64_t seq = ++s->trace_seq;
     if (mem == RAY_MEM_HOST) {
+        // this call's error word and counters, copied behind its work (another
+        // thread's trace of the scene may reset the device words meanwhile)
+        if (!s->h_info) RG_CUDA_TRY(cudaHostAlloc(reinterpret_cast<void **>(&s->h_info), 32, cudaHostAllocDefault));
+        RG_CUDA_TRY(cudaMemcpyAsync(s->h_info, s->d_err.p, 4, cudaMemcpyDeviceToHost, st));
+        RG_CUDA_TRY(cudaMemcpyAsync(s->h_info + 2, s->d_counters.p, 16, cudaMemcpyDeviceToHost, st));
+        // the download of pageable buffers and the wait for the GPU work, without
+        // the API lock when this is the outermost entry point of the thread
+        const bool release = t_api_depth == 1;
+        if (release) api_mutex().unlock();
+        cudaError_t we = cudaSuccess;
+        if (!piped && n) {
+            we = cudaMemcpyAsync(hits, d_hits, n * 16, cudaMemcpyDeviceToHost, st);
+            if (we == cudaSuccess && obj) we = cudaMemcpyAsync(obj, d_obj, n * 4, cudaMemcpyDeviceToHost, st);
+        }
+        if (we == cudaSuccess) we = wait_stream(st);
+        if (release) api_mutex().lock();
+        RG_CHECK(live_scene(s), "scene destroyed while the call waited for its GPU work");
+        RG_CUDA_TRY(we);
         ray_trace_info info;
-        rc = ray_scene_last_trace_info(s, &info);
-        if (rc != RAY_OK) return rc;
+        info.error_flags = s->h_info[0];
+        unsigned long long cnt[2];
+        memcpy(cnt, s->h_info + 2, 16);
+        info.node_visits = cnt[0];
+        info.tri_tests = cnt[1];
+        if (s->trace_seq == seq) { // no later trace of the scene was enqueued meanwhile
+            s->last_info = info;
+            s->info_pending = false;
+        }
         if (info.error_flags & TRACE_ERR_STACK) {
             set_error("traversal stack overflow");
             return RAY_ERR_STACK_OVERFLOW;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <utility>
@@ -78,7 +79,18 @@ std::recursive_mutex &api_mutex();
 // other pointer returns RAY_ERR_INVALID_ARG instead of dereferencing it.
 bool live_scene(const ray_scene *s);
 bool live_renderer(const ray_renderer *r);
-#define RG_API_LOCK std::lock_guard<std::recursive_mutex> rg_api_lock_(rg::api_mutex())
+// The process-wide API lock, with the calling thread's nesting depth (an
+// entry point called from another holds it twice); a host-buffer trace lets
+// it go while it waits for its GPU work when it holds it once.
+extern thread_local int t_api_depth;
+struct ApiLock {
+    std::lock_guard<std::recursive_mutex> g;
+    ApiLock() : g(api_mutex()) { ++t_api_depth; }
+    ~ApiLock() { --t_api_depth; }
+    ApiLock(const ApiLock &) = delete;
+    ApiLock &operator=(const ApiLock &) = delete;
+};
+#define RG_API_LOCK rg::ApiLock rg_api_lock_
 
 // api.cu: builds pending BVHs and uploads pending scene data, after the
 // kernels already enqueued that read the arrays it overwrites
@@ -149,10 +161,16 @@ struct ray_scene {
     ray_trace_info last_info{};
     bool info_pending = false;
     cudaStream_t info_stream = nullptr;
+    uint64_t trace_seq = 0; // traces enqueued on the scene so far
     // host-buffer traces: the chunk pipeline's upload, download and second trace
     // streams and its events (created on first use)
     cudaStream_t copy_st[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t pipe_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // host-buffer traces of this scene run one at a time (they share the
+    // staging buffers and events above); a shared pointer, so that a caller
+    // can wait for it without holding the API lock while the scene lives on
+    std::shared_ptr<std::mutex> host_mu = std::make_shared<std::mutex>();
+    uint32_t *h_info = nullptr; // page-locked copy of the error word and counters of the last host-buffer trace
 
     ~ray_scene();
 };

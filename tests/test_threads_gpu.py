@@ -57,3 +57,66 @@ def test_concurrent_traces_of_one_scene(cuda_device):
         together = list(pool.map(sc.trace_closest, sets))
     for a, b in zip(alone, together):
         assert np.array_equal(np.asarray(a).view(np.uint32), np.asarray(b).view(np.uint32))
+
+
+def _soup_scene(r, n_tris, seed):
+    sc = r.CreateScene()
+    attrs, idx = scenes.triangle_soup_mesh(scenes.random_triangles(n_tris, seed=seed, mean_edge=0.01))
+    m = sc.AddMaterial()
+    sc.AddMeshInstance(sc.AddMesh(attrs, idx, [(m, 0, len(idx))]))
+    return sc
+
+
+def test_host_trace_waits_without_the_api_lock(cuda_device):
+    """A host-buffer trace holds the process-wide lock only while it enqueues
+    its work: while one thread waits for a long trace, another thread's calls
+    go through (the longest pause between them stays far below the trace's
+    duration), and both threads' results equal the one-thread results."""
+    import threading
+    import time
+
+    import torch
+
+    from raydemo_b200 import capi
+
+    r = api.Renderer(8, 8)
+    big, small = _soup_scene(r, 400000, 61), _soup_scene(r, 20000, 62)
+    n = 8 * 1024 * 1024
+    rays = torch.from_numpy(scenes.incoherent_rays(n, seed=63)).pin_memory()
+    hits = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+    L = capi.lib()
+
+    def trace_big():
+        capi.check(L.ray_scene_trace_closest(big.handle, rays.data_ptr(), n, hits.data_ptr(), None, capi.RAY_MEM_HOST, None))
+
+    trace_big()
+    expect = hits.clone()
+    t0 = time.perf_counter()
+    trace_big()
+    t_one = time.perf_counter() - t0
+    small_rays = scenes.incoherent_rays(2000, seed=64)
+    small_expect = np.asarray(small.trace_closest(small_rays)).view(np.uint32).copy()
+
+    done = threading.Event()
+
+    def worker():
+        for _ in range(6):
+            trace_big()
+        done.set()
+
+    th = threading.Thread(target=worker)
+    stamps, small_results = [], []
+    th.start()
+    while not done.is_set():
+        small.get_trace_tuning()
+        stamps.append(time.perf_counter())
+        if len(small_results) < 20:
+            small_results.append(np.asarray(small.trace_closest(small_rays)).view(np.uint32).copy())
+    th.join()
+    gaps = np.diff(np.asarray(stamps))
+    print(f"one trace {t_one * 1e3:.2f} ms; {len(stamps)} calls from the other thread meanwhile, longest pause {gaps.max() * 1e3:.2f} ms")
+    assert len(stamps) > 50
+    assert gaps.max() < 0.5 * t_one, (gaps.max(), t_one)
+    assert torch.equal(hits.view(torch.int32), expect.view(torch.int32))
+    for s in small_results:
+        assert np.array_equal(s, small_expect)
