@@ -395,7 +395,7 @@ typedef struct ray_frame_info {
     int32_t kernel; /* the kernel that rendered it: 1 wavefront, 2 path kernel */
     uint64_t rays, shadow_rays;
     uint32_t sort_mask; /* wavefront: bounces whose rays were sorted first (bit b: secondary bounce b) */
-    uint32_t trace_one_tri; /* wavefront: 1 = its traces tested one triangle per lane and step */
+    uint32_t trace_one_tri; /* wavefront: one triangle test per lane and step in its closest-hit traces (bit 0), shadow-ray traces (bit 1) */
     /* wavefront: the trace settings it ran with (ray_renderer_set_trace_variant):
      * their index, refill threshold, threads per block and shared stack entries
      * (0 for each of the three: the scene's own settings) */

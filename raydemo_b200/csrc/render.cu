@@ -118,17 +118,20 @@ int ensure_frame_state(ray_renderer *r) {
 }
 
 // Trace settings the frame tuner times for the wavefront: one triangle test
-// per lane and step (1) or a node's triangles at once (0), a refill
+// per lane and step (bit 0: in the closest-hit traces, bit 1: in the
+// shadow-ray traces) or a node's triangles at once, a refill
 // threshold, threads per block and shared stack entries (the block and stack
 // apply to one-scene closest-hit launches). Index 0 takes the scene's refill,
 // block and stack (ray_scene_set_trace_tuning) with a node's triangles at
-// once: measured on the atrium (1280x720, 16 spp), one triangle per step
-// traced its bounces 12 % slower, while it is the faster form for the
-// incoherent rays of ray_scene_trace_closest.
+// once: measured on the atrium (1280x720, 16 spp; refill 16, 128 threads, 24
+// entries), one triangle per step made the closest-hit traces 2.5 ms and the
+// shadow-ray traces 1.7 ms per frame slower (62.7 ms per frame with neither,
+// 67.7 with both), while it is the faster form for the incoherent rays of
+// ray_scene_trace_closest.
 struct TraceVariant {
     int one, refill, block, stack;
 };
-constexpr TraceVariant TRACE_VARIANTS[] = {{0, 0, 0, 0}, {0, 8, 128, 24}, {0, 16, 128, 24}, {0, 8, 64, 24}, {1, 4, 64, 16}, {1, 8, 128, 16}};
+constexpr TraceVariant TRACE_VARIANTS[] = {{0, 0, 0, 0}, {0, 8, 128, 24}, {0, 16, 128, 24}, {0, 8, 64, 24}, {3, 4, 64, 16}, {3, 8, 128, 16}};
 constexpr int N_TRACE_VARIANTS = (int)(sizeof(TRACE_VARIANTS) / sizeof(TRACE_VARIANTS[0]));
 static_assert(3 + N_TRACE_VARIANTS - 1 == ray_renderer::N_VARIANTS, "frame variants: 3 plus the trace variants after the first");
 
@@ -578,11 +581,13 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
     }
     tp.block = scn[0]->tuning.block;
     tp.smem_stack = scn[0]->tuning.smem_stack;
+    bool one_any = false; // shadow-ray traces: one triangle test per step
     if (trace_var > 0 && trace_var < N_TRACE_VARIANTS) { // the frame tuner's trace settings
         tp.refill_min = TRACE_VARIANTS[trace_var].refill;
         tp.block = TRACE_VARIANTS[trace_var].block;
         tp.smem_stack = TRACE_VARIANTS[trace_var].stack;
-        tp.one_tri = TRACE_VARIANTS[trace_var].one != 0;
+        tp.one_tri = (TRACE_VARIANTS[trace_var].one & 1) != 0;
+        one_any = (TRACE_VARIANTS[trace_var].one & 2) != 0;
     }
     tp.next_ray = cnt + 2;
     if (n_jobs > 1) { // each ray traced in its job's scene
@@ -620,6 +625,7 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
         // shadow rays of the light samples: the persistent kernel in any-hit mode (the hits buffer is free again)
         TraceParams tps = tp;
         tps.any = true;
+        tps.one_tri = one_any;
         tps.count = shadow_cnt;
         tps.ray_job = shadow.job;
         // shading of the rays in buffer `in` (bounce b), continuation rays to `out`, then the light samples'
