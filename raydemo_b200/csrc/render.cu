@@ -544,10 +544,11 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
     if (sort_mask) RG_CUDA_TRY(rb->d_loop_sort.ensure(loop_sort_scratch_bytes(std::max<size_t>(total, 1), (int)jobs.size())));
     // light samples of RAY_MAT_PRINCIPLED vertices wait in d_shadow (count in counter [8])
     // for their shadow rays; the reference's own lights are traced inside the shading
-    bool ref_lights = false, nee = false;
+    bool ref_lights = false, nee = false, principled_only = true;
     for (const FrameJob &J : jobs) {
         ref_lights = ref_lights || J.sc.n_lights > 0;
         nee = nee || J.sc.n_area_lights > 0;
+        principled_only = principled_only && J.sc.principled_only;
     }
     ShadowQueue shadow{nullptr, nullptr, nullptr, nullptr};
     if (nee || adj) {
@@ -639,7 +640,7 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
                                          job[out], adj->state[out], cnt + out, shadow, adj->args, err, st, ref_lights);
             else
                 e = launch_shade_jobs(d_jobs, sample, b, rays[in], pay[in], job[in], hits, obj, cnt + in, total, rays[out], pay[out], job[out],
-                                      cnt + out, shadow, ref_lights, err, ray_stats, st);
+                                      cnt + out, shadow, ref_lights, principled_only, err, ray_stats, st);
             if (e != cudaSuccess || !(nee || adj)) return e;
             e = launch_trace_closest(sv, shadow.rays, total, hits, nullptr, err, nullptr, false, st, tps);
             if (e != cudaSuccess) return e;
@@ -687,7 +688,7 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
     GraphKey key;
     key.add(d_jobs).add(n_jobs).add(total).add(sample0).add(samples).add(sort_mask).add(bounces).add(resolve).add(adj).add(st);
     for (int q = 0; q < 2; q++) key.add(rays[q]).add(pay[q]).add(job[q]);
-    key.add(hits).add(obj).add(cnt).add(shadow.recs).add(shadow.rays).add(shadow.job).add(rb->d_loop_sort.p).add(nee).add(ref_lights);
+    key.add(hits).add(obj).add(cnt).add(shadow.recs).add(shadow.rays).add(shadow.job).add(rb->d_loop_sort.p).add(nee).add(ref_lights).add(principled_only);
     key.add(sv.nodes).add(sv.leaf_tris).add(sv.inst).add(sv.n_inst).add(tp.persistent).add(tp.refill_min).add(tp.max_depth).add(tp.views);
     key.add(sv.tlas).add(tp.tlas).add(tp.block).add(tp.smem_stack).add(tp.one_tri);
     key.add(ev).add(geo_best).add(geo_tris).add(persp);

@@ -82,6 +82,7 @@ struct RenderScene {
     const LightRec *lights;
     const AreaLight *area_lights;
     uint32_t n_tris, n_materials, n_textures, n_lights, n_area_lights;
+    uint32_t principled_only; // every material is RAY_MAT_PRINCIPLED (host-side choice of the shading kernel)
     float env_col[3], env_clamp;
     uint32_t env_map;
     // differentiable parameters (ray_scene_set_diff_params): a float RGB
@@ -258,7 +259,7 @@ cudaError_t launch_geo_rays(const FrameJob *jobs, int n_jobs, uint32_t total, in
 cudaError_t launch_shade_jobs(const FrameJob *jobs, int sample, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
                               const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays, float4 *out_rays,
                               RayPayload *out_pay, uint32_t *out_job, uint32_t *out_count, const ShadowQueue &shadow, bool ref_lights,
-                              uint32_t *err, unsigned long long *ray_stats, cudaStream_t st);
+                              bool principled_only, uint32_t *err, unsigned long long *ray_stats, cudaStream_t st);
 // After the any-hit trace of a shading launch's shadow rays (hits): adds the
 // colour of each unblocked light sample to its pixel. A ray whose first hit
 // is on a non-solid triangle takes the full visibility walk through the

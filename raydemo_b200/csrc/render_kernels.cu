@@ -371,7 +371,7 @@ __device__ __forceinline__ void set3(float *dst, V3 v) {
 // RAY_MAT_PRINCIPLED vertex's light sample. REF_LIGHTS: the scene may have
 // the reference's point/spot/directional lights (their shadow rays are traced
 // here); without, the kernel carries no traversal code.
-template <bool REF_LIGHTS>
+template <bool REF_LIGHTS, bool PONLY = false>
 __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_index, const float *halton, float4 hit, int obj,
                         float4 r0, float4 r1, const RayPayload &ray, NewRay &nr, bool &emit, ShadowReq &sr, Stack<true> &st,
                         uint32_t &err, uint32_t &nshadow, VertexGrad *vg = nullptr) {
@@ -440,7 +440,7 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
             return F4{0.0f, 0.0f, 0.0f, 0.0f};
         }
         const MaterialRec &mat = sc.materials[mi];
-        if (mat.type != (uint32_t)RAY_MAT_MIX) break;
+        if (PONLY || mat.type != (uint32_t)RAY_MAT_MIX) break;
         if (++nest > MAX_MIX_NESTING) {
             err |= SHADE_ERR_MIX_LOOP;
             return F4{0.0f, 0.0f, 0.0f, 0.0f};
@@ -479,7 +479,7 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
     // the reference's materials: normal map and main texture (RAY_MAT_PRINCIPLED reads neither)
     V3 B = v3(0.0f, 0.0f, 0.0f), T = v3(0.0f, 0.0f, 0.0f), alb = v3(0.0f, 0.0f, 0.0f);
     float sigma_d = mat.roughness_or_strength; // the diffuse material's Oren-Nayar roughness
-    if (mat.type != (uint32_t)RAY_MAT_PRINCIPLED) {
+    if (!PONLY && mat.type != (uint32_t)RAY_MAT_PRINCIPLED) {
         B = v3(v1.b) * w + v3(v2.b) * hu + v3(v3v.b) * hv;
         T = cross(B, N);
         F4 nm = sample_bilinear(sc, mat.textures[0], uvx, uvy, 0);
@@ -528,7 +528,7 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
     nr.p.pad[0] = nr.p.pad[1] = nr.p.pad[2] = 0;
     const float dot_I_pN = dot(I, plane_N);
 
-    if (mat.type == (uint32_t)RAY_MAT_DIFFUSE) {
+    if (!PONLY && mat.type == (uint32_t)RAY_MAT_DIFFUSE) {
         const bool dgrad = vg && vg->diffuse;
         if (dgrad) vg->albedo_on = consider_albedo;
         if (!(pi.flags & PASS_SKIP_DIRECT) || pi.bounce > 2) {
@@ -581,7 +581,7 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
             emit = roulette(nr, cant_terminate, frac_modf(halton[hi + 0] + rand_offset3));
             if (dgrad) vg->cont = emit;
         }
-    } else if (mat.type == (uint32_t)RAY_MAT_GLOSSY) {
+    } else if (!PONLY && mat.type == (uint32_t)RAY_MAT_GLOSSY) {
         if (gloss_depth < pi.max_glossy_depth && total_depth < pi.max_total_depth) {
             V3 V = reflect(I, N);
             const float rough = mat.roughness_or_strength;
@@ -615,7 +615,7 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
             set3(nr.p.dd_dy, der.dd_dy - 2 * (dot_I_pN * der.dndy + der.ddn_dy * plane_N));
             emit = roulette(nr, cant_terminate, frac_modf(halton[hi + 0] + rand_offset3));
         }
-    } else if (mat.type == (uint32_t)RAY_MAT_REFRACTIVE) {
+    } else if (!PONLY && mat.type == (uint32_t)RAY_MAT_REFRACTIVE) {
         if (refr_depth < pi.max_refr_depth && total_depth < pi.max_total_depth) {
             const float ior = is_backfacing ? mat.ext_ior : mat.int_ior;
             const float eta = ray.ior / ior;
@@ -648,7 +648,7 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
             set3(nr.p.dd_dy, eta * der.dd_dy - (m * der.dndy + dmdy * plane_N));
             emit = roulette(nr, cant_terminate, frac_modf(halton[hi + 0] + rand_offset3));
         }
-    } else if (mat.type == (uint32_t)RAY_MAT_PRINCIPLED) {
+    } else if (PONLY || mat.type == (uint32_t)RAY_MAT_PRINCIPLED) {
         // metallic-roughness material: next-event estimation + a sampled continuation ray
         const V3 wo = normalize(-I);
         V3 Ns = normalize(transform_normal(N_vertex, inv));
@@ -800,11 +800,11 @@ __device__ F4 shade_hit(const RenderScene &sc, const PassInfo &pi, int rand_inde
 // the hit: weight 1 for rays whose last vertex did not sample quad lights
 // (pdf 0 in the payload), else the power heuristic against the light pdf that
 // next-event estimation at that vertex used.
-template <bool REF_LIGHTS>
+template <bool REF_LIGHTS, bool PONLY = false>
 __device__ __forceinline__ F4 shade_surface(const RenderScene &sc, const PassInfo &pi, int rand_index, const float *halton, float4 hit,
                                             int obj, float4 r0, float4 r1, const RayPayload &ray, NewRay &nr, bool &emit, ShadowReq &sr,
                                             Stack<true> &st, uint32_t &err, uint32_t &nshadow, VertexGrad *vg = nullptr) {
-    F4 c = shade_hit<REF_LIGHTS>(sc, pi, rand_index, halton, hit, obj, r0, r1, ray, nr, emit, sr, st, err, nshadow, vg);
+    F4 c = shade_hit<REF_LIGHTS, PONLY>(sc, pi, rand_index, halton, hit, obj, r0, r1, ray, nr, emit, sr, st, err, nshadow, vg);
     if (sc.n_area_lights == 0) return c;
     const V3 o = v3(r0.x, r0.y, r0.z), d = v3(r1.x, r1.y, r1.z);
     const float tmax = __float_as_int(hit.x) >= 0 ? hit.y : MAX_DIST;
@@ -1071,8 +1071,10 @@ __global__ void k_geo_rays(const FrameJob *__restrict__ jobs, int n_jobs, uint32
 // Shading of *in_count rays of any jobs (bounce: pass_info_t::bounce, 2 for
 // primary rays). PRIMARY: SetPixel into the job's sample buffer, else AddPixel
 // with alpha 0. A continuation ray is appended where the path goes on and its
-// job traces another bounce.
-template <bool PRIMARY, bool REF_LIGHTS>
+// job traces another bounce. PONLY: every material of every job's scene is
+// RAY_MAT_PRINCIPLED (and no scene has the reference's lights), so the
+// kernel carries none of the other materials' code.
+template <bool PRIMARY, bool REF_LIGHTS, bool PONLY = false>
 __global__ void __launch_bounds__(SHADE_BLOCK, REF_LIGHTS ? 3 : 4) k_shade_jobs(const FrameJob *__restrict__ jobs, int sample, int bounce,
                                                             const float4 *__restrict__ rays, const RayPayload *__restrict__ pay,
                                                             const uint32_t *__restrict__ ray_job, const float4 *__restrict__ hits,
@@ -1109,7 +1111,8 @@ __global__ void __launch_bounds__(SHADE_BLOCK, REF_LIGHTS ? 3 : 4) k_shade_jobs(
             pi.bounce = bounce;
             const int rand_index = (pi.flags & PASS_COHERENT) ? c_sampling_pattern[(y % 8) * 8 + (x % 8)] : index;
             bool emit = false;
-            const F4 c = shade_surface<REF_LIGHTS>(J.sc, pi, rand_index, J.halton, hits[i], obj[i], r0, r1, p, nr, emit, sr, st, err, nshadow);
+            const F4 c = shade_surface<REF_LIGHTS, PONLY>(J.sc, pi, rand_index, J.halton, hits[i], obj[i], r0, r1, p, nr, emit, sr, st, err,
+                                                          nshadow);
             sr_index = (uint32_t)index;
             sr_rand = (uint32_t)rand_index;
             append = emit && bounce - 2 < J.bounces;
@@ -1718,21 +1721,26 @@ static int resident_blocks(K kernel, int fallback_per_sm) {
 cudaError_t launch_shade_jobs(const FrameJob *jobs, int sample, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
                               const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays, float4 *out_rays,
                               RayPayload *out_pay, uint32_t *out_job, uint32_t *out_count, const ShadowQueue &shadow, bool ref_lights,
-                              uint32_t *err, unsigned long long *ray_stats, cudaStream_t st) {
-    static int resident[2] = {0, 0};
-    int &res = resident[ref_lights ? 1 : 0];
-    if (res == 0) res = ref_lights ? resident_blocks(k_shade_jobs<false, true>, 4) : resident_blocks(k_shade_jobs<false, false>, 4);
+                              bool principled_only, uint32_t *err, unsigned long long *ray_stats, cudaStream_t st) {
+    const bool ponly = principled_only && !ref_lights;
+    static int resident[3] = {0, 0, 0};
+    int &res = resident[ref_lights ? 1 : (ponly ? 2 : 0)];
+    if (res == 0)
+        res = ref_lights ? resident_blocks(k_shade_jobs<false, true>, 4)
+                         : (ponly ? resident_blocks(k_shade_jobs<false, false, true>, 4) : resident_blocks(k_shade_jobs<false, false>, 4));
     const uint32_t need = (max_rays + SHADE_BLOCK - 1) / SHADE_BLOCK;
     const uint32_t blocks = need < (uint32_t)res ? (need > 0 ? need : 1) : (uint32_t)res;
-#define RG_SHADE(P, R)                                                                                                                     \
-    k_shade_jobs<P, R><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, sample, bounce, rays, pay, ray_job, hits, obj, in_count, max_rays, out_rays, \
-                                                       out_pay, out_job, out_count, shadow, err, ray_stats)
+#define RG_SHADE(P, R, O)                                                                                                                  \
+    k_shade_jobs<P, R, O><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, sample, bounce, rays, pay, ray_job, hits, obj, in_count, max_rays, out_rays, \
+                                                          out_pay, out_job, out_count, shadow, err, ray_stats)
     if (bounce == 2) {
-        if (ref_lights) RG_SHADE(true, true);
-        else RG_SHADE(true, false);
+        if (ref_lights) RG_SHADE(true, true, false);
+        else if (ponly) RG_SHADE(true, false, true);
+        else RG_SHADE(true, false, false);
     } else {
-        if (ref_lights) RG_SHADE(false, true);
-        else RG_SHADE(false, false);
+        if (ref_lights) RG_SHADE(false, true, false);
+        else if (ponly) RG_SHADE(false, false, true);
+        else RG_SHADE(false, false, false);
     }
 #undef RG_SHADE
     return cudaGetLastError();

@@ -357,6 +357,9 @@ RenderScene render_scene_view(const ray_scene *s) {
     r.n_materials = (uint32_t)s->materials.size();
     r.n_textures = (uint32_t)s->textures.size();
     r.n_lights = (uint32_t)s->lights.size();
+    r.principled_only = s->materials.empty() ? 0u : 1u;
+    for (const MaterialRec &m : s->materials)
+        if (m.type != (uint32_t)RAY_MAT_PRINCIPLED) r.principled_only = 0u;
     for (int k = 0; k < 3; k++) r.env_col[k] = s->env.env_col[k];
     r.env_clamp = s->env.env_clamp;
     r.env_map = s->env.env_map;
