@@ -240,6 +240,14 @@ std::unordered_set<const void *> &live_handles() {
 
 bool live_scene(const ray_scene *s) { return live_handles().count(s) != 0; }
 thread_local int t_api_depth = 0;
+
+cudaError_t wait_stream_unlocked(cudaStream_t st) {
+    if (t_api_depth != 1) return wait_stream(st);
+    api_mutex().unlock();
+    const cudaError_t e = wait_stream(st);
+    api_mutex().lock();
+    return e;
+}
 bool live_renderer(const ray_renderer *r) { return live_handles().count(r) != 0; }
 
 cudaError_t note_use(ray_scene *s, cudaStream_t st) {

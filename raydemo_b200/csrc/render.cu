@@ -1154,7 +1154,12 @@ int ray_get_pixels(ray_renderer *r, const ray_pixel **out, int on_device) {
     RG_CUDA_TRY(cudaSetDevice(r->device));
     int rc = ensure_frame_buffers(r, false);
     if (rc != RAY_OK) return rc;
-    RG_CUDA_TRY(wait_stream(r->stream));
+    RG_CUDA_TRY(wait_stream_unlocked(r->stream));
+    RG_CHECK(live_renderer(r), "renderer destroyed while the call waited for its GPU work");
+    RG_CUDA_TRY(cudaSetDevice(r->device));
+    rc = ensure_frame_buffers(r, false);
+    if (rc != RAY_OK) return rc;
+    RG_CUDA_TRY(wait_stream(r->stream)); // work another thread enqueued meanwhile
     if (on_device) {
         *out = static_cast<const ray_pixel *>(r->d_final.p);
         return RAY_OK;
@@ -1181,7 +1186,14 @@ int ray_get_sh_data(ray_renderer *r, const ray_shl1 **out) {
         return RAY_OK;
     }
     RG_CUDA_TRY(cudaSetDevice(r->device));
-    RG_CUDA_TRY(wait_stream(r->stream));
+    RG_CUDA_TRY(wait_stream_unlocked(r->stream));
+    RG_CHECK(live_renderer(r), "renderer destroyed while the call waited for its GPU work");
+    RG_CUDA_TRY(cudaSetDevice(r->device));
+    RG_CUDA_TRY(wait_stream(r->stream)); // work another thread enqueued meanwhile
+    if (!r->d_clean_sh.p) {
+        *out = nullptr;
+        return RAY_OK;
+    }
     const size_t n = (size_t)r->w * r->h;
     if (!r->sh_on_host || r->host_sh.size() != n) {
         r->host_sh.resize(n);

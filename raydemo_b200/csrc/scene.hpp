@@ -91,6 +91,11 @@ struct ApiLock {
     ApiLock &operator=(const ApiLock &) = delete;
 };
 #define RG_API_LOCK rg::ApiLock rg_api_lock_
+// Waits (bounded) for st's work with the API lock let go meanwhile, when the
+// calling thread holds it once; the caller re-checks its handles afterwards
+// (another thread may have changed or destroyed them) and waits again under
+// the lock for work enqueued in between.
+cudaError_t wait_stream_unlocked(cudaStream_t st);
 
 // api.cu: builds pending BVHs and uploads pending scene data, after the
 // kernels already enqueued that read the arrays it overwrites

@@ -120,3 +120,55 @@ def test_host_trace_waits_without_the_api_lock(cuda_device):
     assert torch.equal(hits.view(torch.int32), expect.view(torch.int32))
     for s in small_results:
         assert np.array_equal(s, small_expect)
+
+
+def test_pixel_read_back_waits_without_the_api_lock(cuda_device):
+    """ray_get_pixels waits for the renderer's frames with the process-wide
+    lock let go: while one thread renders and reads back large frames, another
+    thread's calls keep going through, and the read-back image equals the
+    one-thread one."""
+    import threading
+    import time
+
+    spec = scenes.cornell_box(0, 1024, 1024, max_bounces=6)
+    w, h = spec["size"]
+    r = api.Renderer(w, h)
+    sc = build_gpu(r, spec)
+    r.set_kernel(1)  # fixed settings: no timed tuning frames
+    r.set_ray_sort(0)
+    r.set_trace_variant(0)
+    other = _soup_scene(api.Renderer(8, 8), 20000, 65)
+
+    def frames():
+        r.Clear()
+        reg = api.RegionContext()
+        for _ in range(4):
+            r.RenderScene(sc, reg)
+        return r.get_pixels_ref().copy()
+
+    expect = frames()
+    t0 = time.perf_counter()
+    frames()
+    t_one = time.perf_counter() - t0
+    done = threading.Event()
+    got = []
+
+    def worker():
+        for _ in range(4):
+            got.append(frames())
+        done.set()
+
+    th = threading.Thread(target=worker)
+    stamps = []
+    th.start()
+    while not done.is_set():
+        other.get_trace_tuning()
+        stamps.append(time.perf_counter())
+    th.join()
+    gaps = np.diff(np.asarray(stamps))
+    print(f"4 frames + read-back {t_one * 1e3:.2f} ms; {len(stamps)} calls from the other thread meanwhile, "
+          f"longest pause {gaps.max() * 1e3:.2f} ms")
+    assert len(stamps) > 50
+    assert gaps.max() < 0.5 * t_one, (gaps.max(), t_one)
+    for img in got:
+        assert np.array_equal(img.view(np.uint32), expect.view(np.uint32))
