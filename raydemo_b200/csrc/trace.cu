@@ -11,12 +11,14 @@
 // and sum rounded on its own, so t, u, v are bit-exact; a tie on t goes to the
 // lower triangle index, which makes the result independent of visiting order.
 //
-// Two kernels share the traversal step:
-//   k_trace_closest     one thread per ray (a grid over the rays)
-//   k_trace_persistent  a resident grid; a lane whose ray is done takes the
-//                       next one from a global counter (warp-aggregated), so
-//                       more lanes do useful work per instruction on
-//                       incoherent rays of very different lengths.
+// The kernels share the traversal step:
+//   k_trace_closest      one thread per ray (a grid over the rays)
+//   k_trace_persistent   a resident grid; a lane whose ray is done takes the
+//                        next one from a global counter (warp-aggregated), so
+//                        more lanes do useful work per instruction on
+//                        incoherent rays of very different lengths
+//   k_trace_closest_one  its closest-hit, one-triangle-per-step form for
+//                        scenes without an instance tree, register-bounded
 // The stack holds one node group per tree level at most. It lives in shared
 // memory; meshes deeper than that use the DEEP instances, which continue it
 // in a local array.
