@@ -637,7 +637,7 @@ int run_wavefront(ray_renderer *rb, const FrameJob *d_jobs, const std::vector<Fr
             if (e != cudaSuccess) return e;
             if (adj)
                 e = launch_adjoint_shade(d_jobs, b, rays[in], pay[in], job[in], adj->state[in], hits, obj, cnt + in, total, rays[out], pay[out],
-                                         job[out], adj->state[out], cnt + out, shadow, adj->args, err, st, ref_lights);
+                                         job[out], adj->state[out], cnt + out, shadow, adj->args, err, st, ref_lights, principled_only);
             else
                 e = launch_shade_jobs(d_jobs, sample, b, rays[in], pay[in], job[in], hits, obj, cnt + in, total, rays[out], pay[out], job[out],
                                       cnt + out, shadow, ref_lights, principled_only, err, ray_stats, st);

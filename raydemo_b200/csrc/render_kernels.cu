@@ -1424,7 +1424,7 @@ __device__ __forceinline__ void flush_slots(float *s_gr, float *grad_rough, uint
 
 // REF_LIGHTS: the scene has the reference's point/spot/directional lights
 // (the replayed shading traces their shadow rays again, as the forward did).
-template <bool PRIMARY, bool REF_LIGHTS>
+template <bool PRIMARY, bool REF_LIGHTS, bool PONLY = false>
 __global__ void __launch_bounds__(SHADE_BLOCK, 3) k_adjoint_shade(const FrameJob *__restrict__ jobs, int bounce,
                                                                   const float4 *__restrict__ rays, const RayPayload *__restrict__ pay,
                                                                   const uint32_t *__restrict__ ray_job, const AdjState *__restrict__ adj_in,
@@ -1495,8 +1495,8 @@ __global__ void __launch_bounds__(SHADE_BLOCK, 3) k_adjoint_shade(const FrameJob
             const int rand_index = (pi.flags & PASS_COHERENT) ? c_sampling_pattern[(y % 8) * 8 + (x % 8)] : index;
             bool emit = false;
             VertexGrad vg;
-            const F4 c = shade_surface<REF_LIGHTS>(sc, pi, rand_index, J.halton, hits[i], obj[i], r0, r1, p, nr, emit, sr, st, err, nshadow,
-                                                   &vg);
+            const F4 c = shade_surface<REF_LIGHTS, PONLY>(sc, pi, rand_index, J.halton, hits[i], obj[i], r0, r1, p, nr, emit, sr, st, err,
+                                                          nshadow, &vg);
             // the sum as the sample buffer takes it (SetPixel on camera rays, AddPixel after)
             if (PRIMARY) {
                 a0 = c.x;
@@ -1789,22 +1789,27 @@ cudaError_t launch_diff_collect(const FrameJob *jobs, int n_jobs, uint32_t n_pix
 cudaError_t launch_adjoint_shade(const FrameJob *jobs, int bounce, const float4 *rays, const RayPayload *pay, const uint32_t *ray_job,
                                  const AdjState *adj_in, const float4 *hits, const int32_t *obj, const uint32_t *in_count, uint32_t max_rays,
                                  float4 *out_rays, RayPayload *out_pay, uint32_t *out_job, AdjState *adj_out, uint32_t *out_count,
-                                 const ShadowQueue &shadow, const AdjArgs &args, uint32_t *err, cudaStream_t st, bool ref_lights) {
-    static int resident[2] = {0, 0};
+                                 const ShadowQueue &shadow, const AdjArgs &args, uint32_t *err, cudaStream_t st, bool ref_lights,
+                                 bool principled_only) {
+    const bool ponly = principled_only && !ref_lights;
+    static int resident[3] = {0, 0, 0};
     if (resident[0] == 0) resident[0] = resident_blocks(k_adjoint_shade<false, false>, 3);
     if (resident[1] == 0) resident[1] = resident_blocks(k_adjoint_shade<false, true>, 3);
-    const int res = resident[ref_lights ? 1 : 0];
+    if (resident[2] == 0) resident[2] = resident_blocks(k_adjoint_shade<false, false, true>, 3);
+    const int res = resident[ref_lights ? 1 : (ponly ? 2 : 0)];
     const uint32_t need = (max_rays + SHADE_BLOCK - 1) / SHADE_BLOCK;
     const uint32_t blocks = need < (uint32_t)res ? (need > 0 ? need : 1) : (uint32_t)res;
-#define RG_ADJ(P, L)                                                                                                                    \
-    k_adjoint_shade<P, L><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, bounce, rays, pay, ray_job, adj_in, hits, obj, in_count, max_rays, out_rays, \
-                                                          out_pay, out_job, adj_out, out_count, shadow, args, err)
+#define RG_ADJ(P, L, O)                                                                                                                 \
+    k_adjoint_shade<P, L, O><<<blocks, SHADE_BLOCK, 0, st>>>(jobs, bounce, rays, pay, ray_job, adj_in, hits, obj, in_count, max_rays,       \
+                                                             out_rays, out_pay, out_job, adj_out, out_count, shadow, args, err)
     if (bounce == 2) {
-        if (ref_lights) RG_ADJ(true, true);
-        else RG_ADJ(true, false);
+        if (ref_lights) RG_ADJ(true, true, false);
+        else if (ponly) RG_ADJ(true, false, true);
+        else RG_ADJ(true, false, false);
     } else {
-        if (ref_lights) RG_ADJ(false, true);
-        else RG_ADJ(false, false);
+        if (ref_lights) RG_ADJ(false, true, false);
+        else if (ponly) RG_ADJ(false, false, true);
+        else RG_ADJ(false, false, false);
     }
 #undef RG_ADJ
     return cudaGetLastError();
