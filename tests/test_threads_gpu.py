@@ -142,7 +142,7 @@ def test_pixel_read_back_waits_without_the_api_lock(cuda_device):
     def frames():
         r.Clear()
         reg = api.RegionContext()
-        for _ in range(4):
+        for _ in range(8):
             r.RenderScene(sc, reg)
         return r.get_pixels_ref().copy()
 
@@ -166,7 +166,7 @@ def test_pixel_read_back_waits_without_the_api_lock(cuda_device):
         stamps.append(time.perf_counter())
     th.join()
     gaps = np.diff(np.asarray(stamps))
-    print(f"4 frames + read-back {t_one * 1e3:.2f} ms; {len(stamps)} calls from the other thread meanwhile, "
+    print(f"8 samples + read-back {t_one * 1e3:.2f} ms; {len(stamps)} calls from the other thread meanwhile, "
           f"longest pause {gaps.max() * 1e3:.2f} ms")
     assert len(stamps) > 50
     assert gaps.max() < 0.5 * t_one, (gaps.max(), t_one)
