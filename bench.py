@@ -527,6 +527,16 @@ def atrium_frames(args, dev, stream, rank: int, world: int) -> dict:
                                                               "sort_mask": f"0x{chosen.sort_mask:03x}"},
            "e2e_ms_per_frame": round(ms_e2e, 3), "e2e_d2h_bytes_per_frame": w * h * 16, "data": "synthetic (seeded procedural scene)",
            "stats_us": {k: int(v) for k, v in stats.items()}}
+    # ray sorting before every bounce against none: its cost in the sort phase and what it changes in the
+    # secondary traces (the phase events of the two variants' timed frames)
+    po, pa = phase_us.get((1, 0)) or {}, phase_us.get((1, 0x3FF)) or {}
+    if po and pa:
+        sort_ms = pa.get("time_secondary_sort_us", 0) / 1e3 - po.get("time_secondary_sort_us", 0) / 1e3
+        tr_off, tr_all = po.get("time_secondary_trace_us", 0) / 1e3, pa.get("time_secondary_trace_us", 0) / 1e3
+        out["ray_sorting"] = {"sort_ms_per_frame": round(sort_ms, 2), "secondary_trace_ms_unsorted": round(tr_off, 2),
+                              "secondary_trace_ms_sorted": round(tr_all, 2),
+                              "reading": ("sorting every bounce costs more than the sorted order saves in the secondary traces"
+                                          if sort_ms > tr_off - tr_all else "the sorted order saves more than the sort costs")}
     del img_h
     if rank == 0 and world == 1 and args.atrium_oracle_spp > 0:
         from oracle.oracle import Oracle
