@@ -30,9 +30,9 @@ constexpr uint32_t TRACE_ERR_TLAS = 16u;  // the instance tree's stack overflowe
 // Kernel choice and its knobs (picked by the tuner).
 struct TraceParams {
     bool persistent = true; // resident grid with per-lane ray refill
-    // closest hit on the persistent grid: one triangle test per lane and loop
-    // iteration (the next node once the last one's triangles are done); the
-    // any-hit, multi-scene and counting launches test a node's triangles at once
+    // persistent grid: one triangle test per lane and loop iteration (the next
+    // node once the last one's triangles are done), else a node's triangles at
+    // once; counting launches always take the latter
     bool one_tri = false;
     int refill_min = 8;     // refill a warp's idle lanes once at least this many are idle
     // closest-hit persistent kernel only: threads per block (64, 128, 256) and
